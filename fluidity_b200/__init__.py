@@ -1,0 +1,364 @@
+"""fluidity_b200: B200-native APIC transfers and MGPCG pressure projection.
+
+The compute path is the CUDA library ``_lib/libfluidity_b200.so`` (sm_100a),
+reached through its C-ABI (``include/fluidity_b200.h``). This module is a thin
+ctypes mirror of that interface plus host helpers (scene generation, sparse to
+dense field views). There is no CPU fallback: importing works without a GPU,
+but every compute call raises ``FluidityError`` unless the CUDA library loads
+and a B200 is present.
+
+Reference-shaped operators mirror FluidiTy's operator API
+(native/include/fluidity/host/transfers_3d.h:23-61):
+
+* :func:`deposit_mac_3d`        <-> ``DepositMac3D``
+* :func:`deposit_mac_quanta_3d` <-> ``DepositMacQuanta3D`` / ``CudaDepositMacQuanta3D``
+* :func:`gather_mac_3d`         <-> ``GatherMac3D`` / ``CudaGatherMac3D``
+
+and :class:`LiquidContext` drives the resident substep
+(topology -> sort -> P2G -> pressure -> G2P) the way the reference's
+``LiquidSubstepBackend3D`` table does (liquid_substep_backend_3d.h:47-260).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from . import scenes  # noqa: F401  (re-exported helper)
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_lib" / "libfluidity_b200.so"
+
+OK, INVALID_ARGUMENT, RESOURCE_EXHAUSTED, FAILED_PRECONDITION, ABORTED, OUT_OF_RANGE, INTERNAL = 0, 3, 8, 9, 10, 11, 13
+STATUS_NAMES = {0: "OK", 3: "INVALID_ARGUMENT", 8: "RESOURCE_EXHAUSTED", 9: "FAILED_PRECONDITION", 10: "ABORTED",
+                11: "OUT_OF_RANGE", 13: "INTERNAL"}
+
+
+class FluidityError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what}: {STATUS_NAMES.get(code, code)} ({code})")
+        self.code = code
+
+
+_fp = ctypes.POINTER(ctypes.c_float)
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_lp = ctypes.POINTER(ctypes.c_int64)
+
+
+class Report(ctypes.Structure):
+    _fields_ = [("compiled_architecture", ctypes.c_int), ("error", ctypes.c_int),
+                ("first_bad_index", ctypes.c_ulonglong)]
+
+
+class Measurement(ctypes.Structure):
+    _fields_ = [("compiled_architecture", ctypes.c_int), ("kernel_ms", ctypes.c_float)]
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("origin", ctypes.c_double * 3), ("h", ctypes.c_double), ("block_lo", ctypes.c_int32 * 3),
+                ("block_dim", ctypes.c_int32 * 3), ("solid_lo", ctypes.c_int32 * 3), ("solid_hi", ctypes.c_int32 * 3)]
+
+
+class Particles(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_void_p * 3), ("v", ctypes.c_void_p * 3), ("c", ctypes.c_void_p * 9),
+                ("mass", ctypes.c_void_p), ("count", ctypes.c_uint64)]
+
+
+class TransferParams(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_float), ("particle_mass", ctypes.c_float), ("gravity", ctypes.c_float * 3),
+                ("min_face_mass", ctypes.c_float), ("density", ctypes.c_float)]
+
+
+class PressureOptions(ctypes.Structure):
+    _fields_ = [("levels", ctypes.c_int), ("pre_sweeps", ctypes.c_int), ("post_sweeps", ctypes.c_int),
+                ("coarse_sweeps", ctypes.c_int), ("precision", ctypes.c_int), ("max_iterations", ctypes.c_int),
+                ("max_refinements", ctypes.c_int), ("pad", ctypes.c_int), ("rel_tol", ctypes.c_double),
+                ("inner_rtol", ctypes.c_double)]
+
+
+class PressureDiagnostics(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iterations", ctypes.c_int), ("refinements", ctypes.c_int),
+                ("levels", ctypes.c_int), ("fluid_cells", ctypes.c_int), ("active_blocks", ctypes.c_int),
+                ("rhs_l2", ctypes.c_double), ("true_residual_l2", ctypes.c_double),
+                ("relative_residual", ctypes.c_double), ("reference_limit", ctypes.c_double),
+                ("max_volume_residual", ctypes.c_double), ("max_divergence", ctypes.c_double),
+                ("solve_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+EXPORTS = [
+    "fl_context_create", "fl_context_destroy", "fl_topology_from_particles", "fl_topology_from_blocks",
+    "fl_active_blocks", "fl_sort_particles_by_block", "fl_p2g", "fl_pressure_project", "fl_g2p", "fl_step",
+    "fl_upload_particles", "fl_download_particles", "fl_state_particles", "fl_state_fields", "fl_step_host",
+    "fl_deposit_mac_3d", "fl_deposit_mac_quanta_3d", "fl_gather_mac_3d", "fl_copy_to_host", "fl_copy_to_device",
+    "fl_runtime_info", "fl_apply_vcycle",
+]
+
+_lib = None
+
+
+def library():
+    """Load the CUDA library (raises FluidityError when it is missing)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FluidityError(FAILED_PRECONDITION, f"CUDA library not built: {LIB_PATH}")
+        lib = ctypes.CDLL(str(LIB_PATH))
+        vp = ctypes.c_void_p
+        lib.fl_context_create.argtypes = [ctypes.POINTER(GridDesc), ctypes.c_uint64, ctypes.POINTER(vp)]
+        lib.fl_context_destroy.argtypes = [vp]
+        lib.fl_topology_from_particles.argtypes = [vp, ctypes.POINTER(Particles), vp, ctypes.POINTER(Report)]
+        lib.fl_topology_from_blocks.argtypes = [vp, _ip, ctypes.c_uint64]
+        lib.fl_active_blocks.argtypes = [vp, _ip, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
+        lib.fl_sort_particles_by_block.argtypes = [vp, ctypes.POINTER(Particles), ctypes.POINTER(Particles), vp,
+                                                   ctypes.POINTER(Report)]
+        lib.fl_p2g.argtypes = [vp, ctypes.POINTER(Particles), ctypes.POINTER(TransferParams), ctypes.c_int,
+                               vp * 3, vp * 3, vp, ctypes.POINTER(Report)]
+        lib.fl_pressure_project.argtypes = [vp, vp * 3, vp * 3, ctypes.POINTER(TransferParams),
+                                            ctypes.POINTER(PressureOptions), ctypes.POINTER(PressureDiagnostics),
+                                            vp, vp]
+        lib.fl_g2p.argtypes = [vp, ctypes.POINTER(Particles), vp * 3, vp * 3, ctypes.c_float, vp, vp,
+                               ctypes.POINTER(Report)]
+        lib.fl_step.argtypes = [vp, ctypes.POINTER(TransferParams), ctypes.POINTER(PressureOptions),
+                                ctypes.POINTER(PressureDiagnostics), vp, ctypes.POINTER(Report)]
+        lib.fl_upload_particles.argtypes = [vp, _fp, ctypes.c_uint64, vp]
+        lib.fl_download_particles.argtypes = [vp, _fp, vp]
+        lib.fl_state_particles.argtypes = [vp, ctypes.POINTER(Particles)]
+        lib.fl_state_fields.argtypes = [vp, vp * 3, vp * 3, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                        ctypes.POINTER(vp)]
+        lib.fl_step_host.argtypes = [vp, _fp, _fp, ctypes.c_uint64, ctypes.POINTER(TransferParams),
+                                     ctypes.POINTER(PressureOptions), ctypes.POINTER(PressureDiagnostics), vp]
+        lib.fl_deposit_mac_3d.argtypes = [_dp, ctypes.c_double, _ip, ctypes.c_uint64, _dp, ctypes.c_uint64, _dp, _dp,
+                                          ctypes.POINTER(Measurement)]
+        lib.fl_deposit_mac_quanta_3d.argtypes = [_dp, ctypes.c_double, _ip, ctypes.c_uint64, _dp, ctypes.c_uint64,
+                                                 ctypes.c_double, ctypes.c_double, ctypes.c_uint64, _lp, _lp,
+                                                 ctypes.POINTER(Measurement)]
+        lib.fl_gather_mac_3d.argtypes = [_dp, ctypes.c_double, _ip, ctypes.c_uint64, _dp, ctypes.c_uint64, _dp, _dp,
+                                         _dp, ctypes.POINTER(Measurement)]
+        lib.fl_copy_to_host.argtypes = [vp, vp, ctypes.c_uint64]
+        lib.fl_copy_to_device.argtypes = [vp, vp, ctypes.c_uint64]
+        lib.fl_runtime_info.argtypes = [ctypes.POINTER(ctypes.c_int)] * 4
+        lib.fl_apply_vcycle.argtypes = [vp, vp, vp, ctypes.POINTER(PressureOptions), vp]
+        _lib = lib
+    return _lib
+
+
+def _check(code: int, what: str):
+    if code != OK:
+        raise FluidityError(code, what)
+
+
+def runtime_info():
+    vals = [ctypes.c_int() for _ in range(4)]
+    library().fl_runtime_info(*[ctypes.byref(v) for v in vals])
+    return dict(compiled_architecture=vals[0].value, device_count=vals[1].value, major=vals[2].value,
+                minor=vals[3].value)
+
+
+def default_pressure_options(precision: int = 0, rel_tol: float = 1e-6, levels: int = 0, pre: int = 2,
+                             post: int = 2, coarse_sweeps: int = 16, max_iterations: int = 400,
+                             max_refinements: int = 6, inner_rtol: float = 1e-4) -> PressureOptions:
+    o = PressureOptions()
+    o.levels, o.pre_sweeps, o.post_sweeps, o.coarse_sweeps = levels, pre, post, coarse_sweeps
+    o.precision, o.max_iterations, o.max_refinements = precision, max_iterations, max_refinements
+    o.rel_tol, o.inner_rtol = rel_tol, inner_rtol
+    return o
+
+
+def transfer_params(dt: float, particle_mass: float, gravity=(0.0, -9.81, 0.0), min_face_mass: float = 0.0,
+                    density: float = 1000.0) -> TransferParams:
+    t = TransferParams()
+    t.dt, t.particle_mass = dt, particle_mass
+    t.gravity[:] = list(gravity)
+    t.min_face_mass, t.density = min_face_mass, density
+    return t
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+# ----------------------------------------------------------------------------- reference-shaped operators
+
+
+def deposit_mac_3d(origin, h, blocks, particles):
+    """GPU DepositMac3D: returns (face_mass, face_pure_momentum) in the
+    reference's owned 4^3 slot order, plus the CUDA-event measurement."""
+    blocks = np.ascontiguousarray(blocks, np.int32)
+    parts = _f64(particles)
+    fc = 192 * len(blocks)
+    m, q = np.zeros(fc), np.zeros(fc)
+    meas = Measurement()
+    _check(library().fl_deposit_mac_3d(_d(_f64(origin)), float(h), blocks.ctypes.data_as(_ip), len(blocks), _d(parts),
+                                       len(parts), _d(m), _d(q), ctypes.byref(meas)), "fl_deposit_mac_3d")
+    return m, q, meas
+
+
+def deposit_mac_quanta_3d(origin, h, blocks, particles, mass_per_quantum, momentum_per_quantum, capacity):
+    blocks = np.ascontiguousarray(blocks, np.int32)
+    parts = _f64(particles)
+    fc = 192 * len(blocks)
+    m, q = np.zeros(fc, np.int64), np.zeros(fc, np.int64)
+    meas = Measurement()
+    _check(library().fl_deposit_mac_quanta_3d(_d(_f64(origin)), float(h), blocks.ctypes.data_as(_ip), len(blocks),
+                                              _d(parts), len(parts), float(mass_per_quantum),
+                                              float(momentum_per_quantum), int(capacity), m.ctypes.data_as(_lp),
+                                              q.ctypes.data_as(_lp), ctypes.byref(meas)), "fl_deposit_mac_quanta_3d")
+    return m, q, meas
+
+
+def gather_mac_3d(origin, h, blocks, particles, old_u, new_u):
+    blocks = np.ascontiguousarray(blocks, np.int32)
+    parts = _f64(particles)
+    out = np.zeros((len(parts), 24))
+    meas = Measurement()
+    _check(library().fl_gather_mac_3d(_d(_f64(origin)), float(h), blocks.ctypes.data_as(_ip), len(blocks), _d(parts),
+                                      len(parts), _d(_f64(old_u)), _d(_f64(new_u)), _d(out), ctypes.byref(meas)),
+           "fl_gather_mac_3d")
+    return out, meas
+
+
+# ----------------------------------------------------------------------------- resident liquid context
+
+
+class LiquidContext:
+    """Resident device arena for the box scene: particles, sparse 8^3-block grid,
+    solver buffers (fl_context_* in the C-ABI)."""
+
+    def __init__(self, n, h=None, capacity=0, origin=(0.0, 0.0, 0.0), walls=True):
+        n = tuple(int(v) for v in (n if np.iterable(n) else (n, n, n)))
+        if any(v % 8 for v in n):
+            raise ValueError("box cells per axis must be a multiple of 8")
+        self.n = n
+        self.h = float(h if h is not None else 1.0 / n[0])
+        self.origin = tuple(float(v) for v in origin)
+        d = GridDesc()
+        d.origin[:] = list(self.origin)
+        d.h = self.h
+        d.block_lo[:] = [0, 0, 0]
+        d.block_dim[:] = [v // 8 for v in n]
+        if walls:
+            d.solid_lo[:] = [1, 1, 1]
+            d.solid_hi[:] = [v - 2 for v in n]
+        else:
+            d.solid_lo[:] = [-(2 ** 31)] * 3
+            d.solid_hi[:] = [2 ** 31 - 1] * 3
+        self.desc = d
+        self.capacity = int(capacity)
+        self._ctx = ctypes.c_void_p()
+        _check(library().fl_context_create(ctypes.byref(d), self.capacity, ctypes.byref(self._ctx)),
+               "fl_context_create")
+        self.count = 0
+
+    def close(self):
+        if self._ctx:
+            library().fl_context_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._ctx
+
+    def upload(self, soa: np.ndarray, stream=None):
+        """soa: float32 array (15, count): x, y, z, vx, vy, vz, C rows."""
+        soa = np.ascontiguousarray(soa, np.float32)
+        self.count = soa.shape[1]
+        _check(library().fl_upload_particles(self._ctx, soa.ctypes.data_as(_fp), self.count, stream),
+               "fl_upload_particles")
+
+    def download(self, stream=None) -> np.ndarray:
+        out = np.zeros((15, self.count), np.float32)
+        _check(library().fl_download_particles(self._ctx, out.ctypes.data_as(_fp), stream), "fl_download_particles")
+        return out
+
+    def step(self, params: TransferParams, options: PressureOptions, stream=None):
+        diag = PressureDiagnostics()
+        rep = Report()
+        code = library().fl_step(self._ctx, ctypes.byref(params), ctypes.byref(options), ctypes.byref(diag), stream,
+                                 ctypes.byref(rep))
+        if code not in (OK, ABORTED):
+            raise FluidityError(code, f"fl_step (report error {rep.error} at {rep.first_bad_index})")
+        return code, diag
+
+    def step_host(self, host_in: np.ndarray, host_out: np.ndarray, params, options, stream=None):
+        diag = PressureDiagnostics()
+        code = library().fl_step_host(self._ctx, host_in.ctypes.data_as(_fp), host_out.ctypes.data_as(_fp),
+                                      host_in.shape[1], ctypes.byref(params), ctypes.byref(options),
+                                      ctypes.byref(diag), stream)
+        if code not in (OK, ABORTED):
+            raise FluidityError(code, "fl_step_host")
+        return code, diag
+
+    def active_blocks(self) -> np.ndarray:
+        cnt = ctypes.c_uint64()
+        library().fl_active_blocks(self._ctx, None, 0, ctypes.byref(cnt))
+        out = np.zeros((cnt.value, 3), np.int32)
+        if cnt.value:
+            _check(library().fl_active_blocks(self._ctx, out.ctypes.data_as(_ip), cnt.value, ctypes.byref(cnt)),
+                   "fl_active_blocks")
+        return out
+
+    def fields(self):
+        """Device pointers of the last step's face fields, pressure, cell type and cell ranges."""
+        up, un = (ctypes.c_void_p * 3)(), (ctypes.c_void_p * 3)()
+        p, t, cs = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        _check(library().fl_state_fields(self._ctx, up, un, ctypes.byref(p), ctypes.byref(t), ctypes.byref(cs)),
+               "fl_state_fields")
+        return dict(u_pred=list(up), u_new=list(un), pressure=p.value, cell_type=t.value, cell_start=cs.value)
+
+    def particles_view(self) -> Particles:
+        p = Particles()
+        _check(library().fl_state_particles(self._ctx, ctypes.byref(p)), "fl_state_particles")
+        return p
+
+
+def copy_to_host(ptr, count, dtype) -> np.ndarray:
+    out = np.zeros(count, dtype)
+    if count:
+        _check(library().fl_copy_to_host(out.ctypes.data, ptr, out.nbytes), "fl_copy_to_host")
+    return out
+
+
+def sparse_faces_to_dense(blocks: np.ndarray, sparse: np.ndarray, n, axis: int, fill=0.0) -> np.ndarray:
+    """Scatter an owned-face array (nb*512, 8^3 layout) into a dense (z,y,x) box
+    array with n[axis]+1 faces along the normal."""
+    n = tuple(n)
+    shape = [n[2], n[1], n[0]]
+    shape[2 - axis] += 1
+    dense = np.full(shape, fill, dtype=sparse.dtype)
+    nb = len(blocks)
+    loc = np.arange(512)
+    lx, ly, lz = loc & 7, (loc >> 3) & 7, loc >> 6
+    gx = (blocks[:, 0:1] * 8 + lx[None, :]).ravel()
+    gy = (blocks[:, 1:2] * 8 + ly[None, :]).ravel()
+    gz = (blocks[:, 2:3] * 8 + lz[None, :]).ravel()
+    ok = (gx < shape[2]) & (gy < shape[1]) & (gz < shape[0])
+    dense[gz[ok], gy[ok], gx[ok]] = sparse[: nb * 512][ok]
+    return dense
+
+
+def sparse_cells_to_dense(blocks: np.ndarray, sparse: np.ndarray, n, fill=0) -> np.ndarray:
+    n = tuple(n)
+    dense = np.full((n[2], n[1], n[0]), fill, dtype=sparse.dtype)
+    loc = np.arange(512)
+    lx, ly, lz = loc & 7, (loc >> 3) & 7, loc >> 6
+    gx = (blocks[:, 0:1] * 8 + lx[None, :]).ravel()
+    gy = (blocks[:, 1:2] * 8 + ly[None, :]).ravel()
+    gz = (blocks[:, 2:3] * 8 + lz[None, :]).ravel()
+    dense[gz, gy, gx] = sparse[: len(blocks) * 512]
+    return dense

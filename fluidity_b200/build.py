@@ -1,0 +1,69 @@
+"""Builds the CUDA library fluidity_b200/_lib/libfluidity_b200.so for sm_100a.
+
+Every translation unit is compiled by nvcc with
+``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` and linked into one
+shared object with a C-ABI (include/fluidity_b200.h). The library is built in
+tree so it travels with the working copy; nothing is installed.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+SRC = HERE / "csrc"
+OUT = HERE / "_lib"
+LIB = OUT / "libfluidity_b200.so"
+SOURCES = ["fl_grid.cu", "fl_p2g.cu", "fl_g2p.cu", "fl_pressure.cu", "fl_quanta.cu", "fl_context.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(obj: Path, deps) -> bool:
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    OUT.mkdir(exist_ok=True)
+    objdir = OUT / "obj"
+    objdir.mkdir(exist_ok=True)
+    headers = list(SRC.glob("*.h")) + list(SRC.glob("*.cuh")) + [HERE.parent / "include" / "fluidity_b200.h"]
+    objs = []
+    procs = []
+    for src in SOURCES:
+        s = SRC / src
+        o = objdir / (src + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + headers):
+            cmd = [nvcc(), "-std=c++17", *ARCH, "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-c", str(s), "-o", str(o)]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+    for cmd, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            sys.stderr.write(out.decode())
+            raise RuntimeError("nvcc failed: " + " ".join(cmd))
+        if verbose:
+            sys.stdout.write(out.decode())
+    if force or _stale(LIB, objs):
+        cmd = [nvcc(), "-shared", *ARCH, "-o", str(LIB), *map(str, objs), "-lcudart"]
+        subprocess.check_call(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

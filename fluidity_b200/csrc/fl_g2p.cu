@@ -1,0 +1,189 @@
+// APIC grid-to-particle transfer with fused advection.
+//
+// Semantics follow GatherMac3D / GatherMacVelocityComponentFromSlots
+// (native/src/transfers_3d.cc:199-261; native/src/mac_gather_3d_internal.h:15-69):
+//   v_a          = sum_n w_n u_n
+//   increment_a  = v_a - sum_n w_n u_old_n
+//   C_a (fitted) = 4 * sum_n w_n u_n (x_n - x_p)/h  /  h
+//   grad_a       = sum_n grad(w_n) u_n
+// The step mode keeps (v, C) and advects x += dt v with a clamp to the
+// non-solid box (the reference's contact-constrained update,
+// liquid_boundary_transfer_3d.cu:544, is out of scope; a plain clamp stands in).
+//
+// B200 design: one CTA per non-empty 8^3 block. The CTA stages the block's
+// 11x10x10 halo tile of each face component in shared memory (coalesced from
+// the owned-face arrays of the 27 neighbouring blocks), then its threads stride
+// over the block's contiguous particle range, gather all 81 samples from
+// shared memory and keep C in registers.
+#include "fl_internal.cuh"
+#include "fl_kernels.h"
+
+namespace fl {
+
+constexpr int kG2PThreads = 256;
+
+__device__ __forceinline__ int tile_ext0(int a) { return a == 0 ? 11 : 10; }
+__device__ __forceinline__ int tile_ext1(int a) { return a == 1 ? 11 : 10; }
+
+__device__ void load_tile(const GridView& g, int b, const float* const u[3], float* tile, int t) {
+  for (int n = t; n < 3 * kTileFaces; n += kG2PThreads) {
+    const int a = n / kTileFaces, idx = n % kTileFaces;
+    const int e0 = tile_ext0(a), e1 = tile_ext1(a);
+    const int nx = idx % e0 - 1, ny = (idx / e0) % e1 - 1, nz = idx / (e0 * e1) - 1;
+    const int dx = nx < 0 ? -1 : (nx > 7 ? 1 : 0), dy = ny < 0 ? -1 : (ny > 7 ? 1 : 0),
+              dz = nz < 0 ? -1 : (nz > 7 ? 1 : 0);
+    const int nb = g.nbr27[b * 27 + nbr_index(dx, dy, dz)];
+    float v = 0.0f;
+    if (nb >= 0) {
+      const int l = ((nz - 8 * dz) * 8 + (ny - 8 * dy)) * 8 + (nx - 8 * dx);
+      v = u[a][(size_t)nb * kBlockCells + l];
+    }
+    tile[n] = v;
+  }
+}
+
+template <bool kFull>
+__global__ void __launch_bounds__(kG2PThreads)
+    k_g2p(GridView g, ParticlesView p, const int* cell_start, const float* u0, const float* u1, const float* u2,
+          const float* o0, const float* o1, const float* o2, G2PParams prm, float* full_out, DeviceReport* rep) {
+  __shared__ float tile[3 * kTileFaces];
+  __shared__ float tile_old[kFull ? 3 * kTileFaces : 1];
+  const int b = blockIdx.x, t = threadIdx.x;
+  const int pbeg = cell_start[b * kBlockCells], pend = cell_start[(b + 1) * kBlockCells];
+  if (pbeg == pend) return;
+  const float* un[3] = {u0, u1, u2};
+  load_tile(g, b, un, tile, t);
+  if (kFull) {
+    const float* uo[3] = {o0, o1, o2};
+    if (o0 != nullptr)
+      load_tile(g, b, uo, tile_old, t);
+    else
+      for (int n = t; n < 3 * kTileFaces; n += kG2PThreads) tile_old[n] = 0.0f;
+  }
+  __syncthreads();
+  const int bc[3] = {g.coord[3 * b] * 8, g.coord[3 * b + 1] * 8, g.coord[3 * b + 2] * 8};
+  const float h = g.h;
+  for (int q = pbeg + t; q < pend; q += kG2PThreads) {
+    float xw[3], X[3];
+    int cell[3];
+    bool inside = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      xw[d] = p.x[d][q];
+      X[d] = lattice_coord(g, xw[d], d);
+      cell[d] = __float2int_rd(X[d]);
+      inside = inside && cell[d] >= bc[d] && cell[d] < bc[d] + 8;
+    }
+    if (!inside) {  // the sort binned this particle elsewhere: never index the tile
+      report_error(rep, kInternal, (unsigned long long)q);
+      continue;
+    }
+    float vel[3], fit[9], inc[3], grad[9];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      // Axis factors: first node, weights, normalized derivative and offset/h.
+      int first[3];
+      float w[3][3], dw[3][3], r[3][3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float shift = d == a ? 0.0f : 0.5f;
+        const float fst = floorf(X[d] - shift - 0.5f);
+        first[d] = (int)fst;
+        const float a0 = fst + shift;
+        const float dl = X[d] - (a0 + 0.5f);
+        const float dr = fabsf(X[d] - (a0 + 1.5f));
+        const float c = X[d] - (a0 + 1.0f);
+        w[d][0] = 0.5f * dr * dr;
+        w[d][1] = 0.75f - c * c;
+        w[d][2] = 0.5f * dl * dl;
+        dw[d][0] = -dr;
+        dw[d][1] = -2.0f * c;
+        dw[d][2] = dl;
+#pragma unroll
+        for (int s = 0; s < 3; ++s) r[d][s] = (a0 + (float)s) - X[d];
+      }
+      const int e0 = tile_ext0(a), e1 = tile_ext1(a);
+      const float* ta = tile + a * kTileFaces;
+      float pic = 0.0f, old = 0.0f, m0 = 0.0f, m1 = 0.0f, m2 = 0.0f, g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
+#pragma unroll
+      for (int kz = 0; kz < 3; ++kz) {
+        const int iz = first[2] + kz - bc[2] + 1;
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+          const int iy = first[1] + ky - bc[1] + 1;
+          const float wyz = w[1][ky] * w[2][kz];
+#pragma unroll
+          for (int kx = 0; kx < 3; ++kx) {
+            const int ix = first[0] + kx - bc[0] + 1;
+            const int n = (iz * e1 + iy) * e0 + ix;
+            const float un_v = ta[n];
+            const float wgt = w[0][kx] * wyz;
+            const float wn = wgt * un_v;
+            pic += wn;
+            m0 = fmaf(r[0][kx], wn, m0);
+            m1 = fmaf(r[1][ky], wn, m1);
+            m2 = fmaf(r[2][kz], wn, m2);
+            if (kFull) {
+              old = fmaf(wgt, tile_old[a * kTileFaces + n], old);
+              g0 = fmaf(dw[0][kx] * wyz, un_v, g0);
+              g1 = fmaf(w[0][kx] * dw[1][ky] * w[2][kz], un_v, g1);
+              g2 = fmaf(w[0][kx] * w[1][ky] * dw[2][kz], un_v, g2);
+            }
+          }
+        }
+      }
+      vel[a] = pic;
+      fit[3 * a] = 4.0f * m0 / h;
+      fit[3 * a + 1] = 4.0f * m1 / h;
+      fit[3 * a + 2] = 4.0f * m2 / h;
+      inc[a] = pic - old;
+      grad[3 * a] = g0 / h;
+      grad[3 * a + 1] = g1 / h;
+      grad[3 * a + 2] = g2 / h;
+    }
+    bool finite = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) finite = finite && isfinite(vel[a]);
+    if (!finite) report_error(rep, kOutOfRange, (unsigned long long)q);
+    if (kFull) {
+      float* o = full_out + 24 * (size_t)q;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        o[a] = vel[a];
+        o[3 + a] = inc[a];
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        o[6 + k] = fit[k];
+        o[15 + k] = grad[k];
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        p.v[d][q] = vel[d];
+        float nx = xw[d] + prm.dt * vel[d];
+        nx = fminf(fmaxf(nx, prm.clamp_lo[d]), prm.clamp_hi[d]);
+        p.x[d][q] = nx;
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) p.c[k][q] = fit[k];
+    }
+  }
+}
+
+cudaError_t launch_g2p(const GridView& g, const ParticlesView& p, const int* cell_start, const float* const u[3],
+                       const float* const u_old[3], const G2PParams& prm, float* full_out, DeviceReport* rep,
+                       cudaStream_t s) {
+  if (g.nb == 0 || p.count == 0) return cudaSuccess;
+  if (full_out != nullptr) {
+    k_g2p<true><<<g.nb, kG2PThreads, 0, s>>>(g, p, cell_start, u[0], u[1], u[2], u_old ? u_old[0] : nullptr,
+                                              u_old ? u_old[1] : nullptr, u_old ? u_old[2] : nullptr, prm, full_out,
+                                              rep);
+  } else {
+    k_g2p<false><<<g.nb, kG2PThreads, 0, s>>>(g, p, cell_start, u[0], u[1], u[2], nullptr, nullptr, nullptr, prm,
+                                               nullptr, rep);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace fl

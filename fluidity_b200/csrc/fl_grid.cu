@@ -1,0 +1,199 @@
+// Sparse-grid topology and the per-step particle sort.
+//
+// Topology: blocks holding particles plus a one-block ring become active; the
+// ring guarantees that every stencil node and every neighbour of a fluid cell
+// is stored (the reference requires owner blocks to be allocated,
+// sparse_mac_grid_3d.cc:388-398, and checks support in BuildOwnedMacFaceStencil3D
+// :627-657).
+//
+// Sort: the particle's cell key is (block ordinal * 512 + local cell), local cell
+// = z*64 + y*8 + x. Keys are radix-sorted (stable, so the order is reproducible
+// run to run) and the SoA arrays are permuted once. Cell counts come from an
+// atomic histogram and an exclusive scan gives cell_start. The reference sorts by
+// the signed bin floor((X - 1.5)/4) with CUB (native/cuda/liquid_arena_3d.cu:29-52);
+// with 8^3 blocks and per-step re-binning the bin is simply the containing cell.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include "fl_internal.cuh"
+#include "fl_kernels.h"
+
+namespace fl {
+
+__device__ __forceinline__ bool particle_cell(const GridView& g, const ParticlesView& p, unsigned long long i,
+                                              int cell[3]) {
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float X = lattice_coord(g, p.x[d][i], d);
+    ok = ok && isfinite(X) && fabsf(X) < 1.0e9f;
+    cell[d] = ok ? __float2int_rd(X) : 0;
+  }
+  return ok;
+}
+
+__global__ void k_mark_blocks(GridView g, ParticlesView p, unsigned char* occ, DeviceReport* rep) {
+  const unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  if (i >= p.count) return;
+  int cell[3];
+  if (!particle_cell(g, p, i, cell)) {
+    report_error(rep, kOutOfRange, i);
+    return;
+  }
+  int b[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    b[d] = floor_div8(cell[d]) - g.blo[d];
+    if (b[d] < 0 || b[d] >= g.bdim[d]) {
+      report_error(rep, kFailedPrecondition, i);
+      return;
+    }
+  }
+  occ[((size_t)b[2] * g.bdim[1] + b[1]) * g.bdim[0] + b[0]] = 1;
+}
+
+__global__ void k_flag_active(GridView g, const unsigned char* occ, int* flag, int total) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const int bx = idx % g.bdim[0], by = (idx / g.bdim[0]) % g.bdim[1], bz = idx / (g.bdim[0] * g.bdim[1]);
+  int active = 0;
+  for (int dz = -1; dz <= 1 && !active; ++dz)
+    for (int dy = -1; dy <= 1 && !active; ++dy)
+      for (int dx = -1; dx <= 1 && !active; ++dx) {
+        const int x = bx + dx, y = by + dy, z = bz + dz;
+        if (x < 0 || y < 0 || z < 0 || x >= g.bdim[0] || y >= g.bdim[1] || z >= g.bdim[2]) continue;
+        active = occ[((size_t)z * g.bdim[1] + y) * g.bdim[0] + x];
+      }
+  flag[idx] = active;
+}
+
+__global__ void k_compact(GridView g, const int* flag, const int* ordinal, int* table, int* coord, int total,
+                          int* nb_out) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const int bx = idx % g.bdim[0], by = (idx / g.bdim[0]) % g.bdim[1], bz = idx / (g.bdim[0] * g.bdim[1]);
+  if (flag[idx]) {
+    const int o = ordinal[idx];
+    table[idx] = o;
+    coord[3 * o] = bx + g.blo[0];
+    coord[3 * o + 1] = by + g.blo[1];
+    coord[3 * o + 2] = bz + g.blo[2];
+  } else {
+    table[idx] = -1;
+  }
+  if (idx == total - 1) *nb_out = ordinal[idx] + flag[idx];
+}
+
+__global__ void k_build_nbr27(GridView g, int* nbr27) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nb * 27) return;
+  const int b = i / 27, n = i % 27;
+  const int dx = n % 3 - 1, dy = (n / 3) % 3 - 1, dz = n / 9 - 1;
+  const int x = g.coord[3 * b] + dx - g.blo[0], y = g.coord[3 * b + 1] + dy - g.blo[1],
+            z = g.coord[3 * b + 2] + dz - g.blo[2];
+  int v;
+  if (x < 0 || y < 0 || z < 0 || x >= g.bdim[0] || y >= g.bdim[1] || z >= g.bdim[2])
+    v = -2;
+  else
+    v = g.table[((size_t)z * g.bdim[1] + y) * g.bdim[0] + x];
+  nbr27[i] = v;
+}
+
+__global__ void k_cell_keys(GridView g, ParticlesView p, unsigned int* keys, unsigned int* index, int* counts,
+                            DeviceReport* rep) {
+  const unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  if (i >= p.count) return;
+  int cell[3];
+  unsigned int key = 0xffffffffu;
+  if (particle_cell(g, p, i, cell)) {
+    int b[3], l[3];
+    bool inside = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      b[d] = floor_div8(cell[d]) - g.blo[d];
+      l[d] = cell[d] - 8 * (b[d] + g.blo[d]);
+      inside = inside && b[d] >= 0 && b[d] < g.bdim[d];
+    }
+    const int o = inside ? g.table[((size_t)b[2] * g.bdim[1] + b[1]) * g.bdim[0] + b[0]] : -1;
+    if (o >= 0) {
+      key = (unsigned int)o * 512u + (unsigned int)(l[2] * 64 + l[1] * 8 + l[0]);
+      atomicAdd(&counts[key], 1);
+    } else {
+      report_error(rep, kFailedPrecondition, i);
+    }
+  } else {
+    report_error(rep, kOutOfRange, i);
+  }
+  keys[i] = key;
+  index[i] = (unsigned int)i;
+}
+
+__global__ void k_permute(ParticlesView in, ParticlesView out, const unsigned int* index) {
+  const unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  if (s >= in.count) return;
+  const unsigned int j = index[s];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) out.x[d][s] = in.x[d][j];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) out.v[d][s] = in.v[d][j];
+#pragma unroll
+  for (int d = 0; d < 9; ++d) out.c[d][s] = in.c[d][j];
+  if (in.mass != nullptr) out.mass[s] = in.mass[j];
+}
+
+__global__ void k_write_arch(DeviceReport* rep) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) rep->compiled_architecture = compiled_arch();
+}
+
+// ------------------------------------------------------------------ host side
+
+static inline unsigned int grid_for(unsigned long long n, int threads) {
+  return (unsigned int)((n + threads - 1) / threads);
+}
+
+size_t sort_temp_bytes(size_t particle_capacity, size_t cell_capacity) {
+  size_t a = 0, b = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, a, (unsigned int*)nullptr, (unsigned int*)nullptr,
+                                  (unsigned int*)nullptr, (unsigned int*)nullptr, (int)particle_capacity, 0, 32);
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (int*)nullptr, (int*)nullptr, (int)(cell_capacity + 1));
+  return (a > b ? a : b) + 256;
+}
+
+cudaError_t launch_topology_from_particles(const GridView& g, const ParticlesView& p, unsigned char* occ,
+                                           int* flag, int* ordinal, int* table, int* coord, int* nb_dev,
+                                           void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s) {
+  const int total = g.bdim[0] * g.bdim[1] * g.bdim[2];
+  cudaMemsetAsync(occ, 0, (size_t)total, s);
+  if (p.count > 0) k_mark_blocks<<<grid_for(p.count, 256), 256, 0, s>>>(g, p, occ, rep);
+  k_flag_active<<<grid_for(total, 256), 256, 0, s>>>(g, occ, flag, total);
+  size_t tb = temp_bytes;
+  cub::DeviceScan::ExclusiveSum(temp, tb, flag, ordinal, total, s);
+  k_compact<<<grid_for(total, 256), 256, 0, s>>>(g, flag, ordinal, table, coord, total, nb_dev);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_build_neighbors(const GridView& g, int* nbr27, cudaStream_t s) {
+  if (g.nb > 0) k_build_nbr27<<<grid_for((unsigned long long)g.nb * 27, 256), 256, 0, s>>>(g, nbr27);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const ParticlesView& out, unsigned int* keys,
+                        unsigned int* keys_alt, unsigned int* index, unsigned int* index_alt, int* counts,
+                        int* cell_start, void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s) {
+  const size_t ncell = (size_t)g.nb * 512;
+  cudaMemsetAsync(counts, 0, sizeof(int) * (ncell + 1), s);
+  k_write_arch<<<1, 32, 0, s>>>(rep);
+  if (in.count > 0) {
+    k_cell_keys<<<grid_for(in.count, 256), 256, 0, s>>>(g, in, keys, index, counts, rep);
+    int end_bit = 1;
+    while (end_bit < 32 && ((size_t)1 << end_bit) < ncell + 1) ++end_bit;
+    size_t tb = temp_bytes;
+    cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys_alt, index, index_alt, (int)in.count, 0, end_bit, s);
+    k_permute<<<grid_for(in.count, 256), 256, 0, s>>>(in, out, index_alt);
+  }
+  size_t tb = temp_bytes;
+  cub::DeviceScan::ExclusiveSum(temp, tb, counts, cell_start, (int)(ncell + 1), s);
+  return cudaGetLastError();
+}
+
+}  // namespace fl

@@ -1,0 +1,137 @@
+// Launch-level declarations shared by the CUDA translation units and the host
+// orchestration (fl_context.cu). Not part of the public C-ABI.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "fl_internal.cuh"
+
+namespace fl {
+
+struct P2GMergeParams {
+  int mode;             // 0: raw mass + momentum; 1: normalize + gravity (+ walls)
+  int walls;            // apply the stationary-wall condition on solid-adjacent faces
+  float mass_scale;     // uniform particle mass (1 when masses are per particle)
+  float min_face_mass;  // NormalizeCore threshold
+  float dt;
+  float gravity[3];
+};
+
+struct G2PParams {
+  float dt;
+  float clamp_lo[3];
+  float clamp_hi[3];
+};
+
+// One multigrid level. Sparse levels keep S^3 cells per active block; dense
+// levels cover the block lattice (coarsened by 2 per level above level 3).
+struct LevelDesc {
+  int sparse;
+  int S;
+  int dim[3];
+  long long count;
+  int parity;
+};
+
+template <typename T>
+struct LevelPtrs {
+  unsigned char* fluid;
+  T* k[3];        // coefficient of the cell's low face (to the -e_a neighbour)
+  float* anchor;  // Dirichlet/compliance part of the diagonal
+  float* diag;
+  T* x;
+};
+
+template <typename T>
+struct MgHierarchy {
+  int levels;
+  LevelDesc desc[12];
+  LevelPtrs<T> ptr[12];
+  float* b[12];  // b[0] unused: level 0 reads the CG residual
+};
+
+struct MgOptions {
+  int pre;
+  int post;
+  int coarse_sweeps;
+};
+
+struct SolverState {
+  double b_norm;      // ||b'||
+  double target;      // rel_tol * ||b'||
+  double res64;       // ||b' - A p64|| (FP64)
+  double inner_rtol;  // inner FCG stop, relative to res64
+  double stop2;
+  double rz, rz_prev, beta, alpha, rr;
+  double div_l2, div_max;
+  int converged;
+  int done;
+  int status;
+  int inner_iter;
+  int inner_max;
+  int total_iter;
+  unsigned int ticket;
+  int pad;
+};
+
+__device__ __forceinline__ long long parent_of(const GridView& g, const LevelDesc& F, const LevelDesc& C,
+                                               long long j);
+
+size_t sort_temp_bytes(size_t particle_capacity, size_t cell_capacity);
+cudaError_t launch_topology_from_particles(const GridView& g, const ParticlesView& p, unsigned char* occ, int* flag,
+                                           int* ordinal, int* table, int* coord, int* nb_dev, void* temp,
+                                           size_t temp_bytes, DeviceReport* rep, cudaStream_t s);
+cudaError_t launch_build_neighbors(const GridView& g, int* nbr27, cudaStream_t s);
+cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const ParticlesView& out, unsigned int* keys,
+                        unsigned int* keys_alt, unsigned int* index, unsigned int* index_alt, int* counts,
+                        int* cell_start, void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s);
+cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cell_start, float2* tiles,
+                       const P2GMergeParams& prm, float* const out0[3], float* const out1[3], DeviceReport* rep,
+                       cudaStream_t s);
+cudaError_t launch_g2p(const GridView& g, const ParticlesView& p, const int* cell_start, const float* const u[3],
+                       const float* const u_old[3], const G2PParams& prm, float* full_out, DeviceReport* rep,
+                       cudaStream_t s);
+
+template <typename T>
+cudaError_t launch_pressure_setup(const GridView& g, const int* cell_start, unsigned char* type,
+                                  const float* const u_pred[3], double rhs_scale, MgHierarchy<T>& H, double* b64,
+                                  double* p64, double* partial, SolverState* st, cudaStream_t s);
+template <typename T>
+cudaError_t launch_apply_vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r, const MgOptions& opt,
+                                const int* done, cudaStream_t s);
+template <typename T>
+cudaError_t launch_residual64(const GridView& g, const MgHierarchy<T>& H, const double* b64, const double* p64,
+                              float* r, float* e, double* partial, SolverState* st, cudaStream_t s);
+template <typename T>
+cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, const MgOptions& opt, float* r_cur,
+                                 float* r_prev, float* d_old, float* d_new, float* q, float* e, double* partial,
+                                 SolverState* st, const int* done, cudaStream_t s);
+cudaError_t launch_accumulate(const GridView& g, const float* e, double* p64, cudaStream_t s);
+cudaError_t launch_correct_faces(const GridView& g, const unsigned char* type, const double* p64,
+                                 const float* const u_pred[3], float* const u_new[3], double scale, double* partial,
+                                 SolverState* st, cudaStream_t s);
+
+// ------------------------------------------------------------- device helpers
+
+__device__ __forceinline__ long long parent_of(const GridView& g, const LevelDesc& F, const LevelDesc& C,
+                                               long long j) {
+  if (F.sparse) {
+    const int S = F.S, S3 = S * S * S;
+    const int b = (int)(j / S3);
+    const int l = (int)(j % S3);
+    const int x = l % S, y = (l / S) % S, z = l / (S * S);
+    if (C.sparse) {
+      const int SC = C.S;
+      return (long long)b * SC * SC * SC + ((z >> 1) * SC + (y >> 1)) * SC + (x >> 1);
+    }
+    const int bx = g.coord[3 * b] - g.blo[0], by = g.coord[3 * b + 1] - g.blo[1], bz = g.coord[3 * b + 2] - g.blo[2];
+    return ((long long)bz * C.dim[1] + by) * C.dim[0] + bx;
+  }
+  const int x = (int)(j % F.dim[0]), y = (int)((j / F.dim[0]) % F.dim[1]),
+            z = (int)(j / ((long long)F.dim[0] * F.dim[1]));
+  return ((long long)(z >> 1) * C.dim[1] + (y >> 1)) * C.dim[0] + (x >> 1);
+}
+
+}  // namespace fl

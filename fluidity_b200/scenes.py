@@ -1,0 +1,120 @@
+"""Seeded synthetic liquid scenes on the unit cube (host-side initial state).
+
+Every scene is a box of n^3 MAC cells (h = 1/n, origin 0) with one-cell solid
+walls on all six faces. Fluid cells are the non-wall cells whose centre lies in
+the scene's liquid region; each receives 8 particles, one per 2x2x2 sub-cell
+stratum, uniformly jittered inside its stratum. The jitter is a counter-based
+SplitMix64 stream keyed by (seed, cell linear index, stratum, axis), so the same
+scene is generated bit-for-bit by every consumer (GPU path, oracle, bench).
+
+Scenes (sizes as in the workloads this library is measured on):
+* ``dam_break(n)``: fluid in [0, 0.5]^3, at rest.
+* ``splash(n)``: pool y <= 0.2 over the whole floor plus two spheres of radius
+  0.15 at (0.35, 0.6, 0.5) and (0.65, 0.6, 0.5) moving at +2 and -2 m/s in x.
+* ``column_drop(n)``: column [0.1,0.3]x[0.1,0.8]x[0.1,0.3] over a pool y <= 0.15.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+DENSITY = 1000.0
+DT = 1.0 / 240.0
+GRAVITY = (0.0, -9.81, 0.0)
+
+_M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    with np.errstate(over="ignore"):
+        z = x + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def _uniform(seed: int, key: np.ndarray) -> np.ndarray:
+    """Uniform [0,1) doubles with 53 random bits from (seed, key)."""
+    with np.errstate(over="ignore"):
+        x = _splitmix64(key.astype(np.uint64) * np.uint64(0x2545F4914F6CDD1D) + np.uint64(seed))
+    return (x >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def seed_particles(n: int, cells: np.ndarray, seed: int = 0, velocity=None):
+    """Particles for the given fluid cells ((k, j, i) triples, shape (m, 3)).
+
+    Returns an FP32 SoA array (15, 8m): x, y, z, vx, vy, vz and nine zero
+    affine entries, plus the particle mass rho h^3 / 8.
+    """
+    h = 1.0 / n
+    cells = np.asarray(cells, dtype=np.int64)
+    m = len(cells)
+    k, j, i = cells[:, 0], cells[:, 1], cells[:, 2]
+    lin = (k * n + j) * n + i
+    strata = np.arange(8, dtype=np.int64)
+    sx, sy, sz = strata & 1, (strata >> 1) & 1, strata >> 2
+    key = (lin[:, None] * 8 + strata[None, :]) * 3
+    ux = _uniform(seed, key)
+    uy = _uniform(seed, key + 1)
+    uz = _uniform(seed, key + 2)
+    x = (i[:, None] + (sx[None, :] + ux) * 0.5) * h
+    y = (j[:, None] + (sy[None, :] + uy) * 0.5) * h
+    z = (k[:, None] + (sz[None, :] + uz) * 0.5) * h
+    soa = np.zeros((15, 8 * m), np.float32)
+    soa[0] = x.ravel()
+    soa[1] = y.ravel()
+    soa[2] = z.ravel()
+    if velocity is not None:
+        vel = np.asarray(velocity, np.float64).reshape(-1, 3)
+        if len(vel) == 1:
+            vel = np.repeat(vel, m, axis=0)
+        for d in range(3):
+            soa[3 + d] = np.repeat(vel[:, d], 8)
+    mass = DENSITY * h ** 3 / 8.0
+    return soa, mass
+
+
+def _interior_centres(n: int):
+    idx = np.arange(1, n - 1)
+    c = (idx + 0.5) / n
+    return idx, c
+
+
+def _cells_where(n: int, inside):
+    idx, c = _interior_centres(n)
+    K, J, I = np.meshgrid(idx, idx, idx, indexing="ij")
+    Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+    mask = inside(X, Y, Z)
+    return np.stack([K[mask], J[mask], I[mask]], axis=1), mask, (X, Y, Z)
+
+
+def dam_break(n: int, seed: int = 0):
+    cells, _, _ = _cells_where(n, lambda X, Y, Z: (X <= 0.5) & (Y <= 0.5) & (Z <= 0.5))
+    return seed_particles(n, cells, seed)
+
+
+def splash(n: int, seed: int = 0):
+    c1, c2, r = (0.35, 0.6, 0.5), (0.65, 0.6, 0.5), 0.15
+
+    def in_sphere(X, Y, Z, c):
+        return (X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 <= r * r
+
+    cells, mask, (X, Y, Z) = _cells_where(
+        n, lambda X, Y, Z: (Y <= 0.2) | in_sphere(X, Y, Z, c1) | in_sphere(X, Y, Z, c2))
+    Xs, Ys, Zs = X[mask], Y[mask], Z[mask]
+    vel = np.zeros((len(cells), 3))
+    pool = Ys <= 0.2
+    s1 = in_sphere(Xs, Ys, Zs, c1) & ~pool
+    s2 = in_sphere(Xs, Ys, Zs, c2) & ~pool & ~s1
+    vel[s1, 0] = 2.0
+    vel[s2, 0] = -2.0
+    return seed_particles(n, cells, seed, vel)
+
+
+def column_drop(n: int, seed: int = 0):
+    cells, _, _ = _cells_where(
+        n, lambda X, Y, Z: (Y <= 0.15) | ((X >= 0.1) & (X <= 0.3) & (Y >= 0.1) & (Y <= 0.8) & (Z >= 0.1) & (Z <= 0.3)))
+    return seed_particles(n, cells, seed)
+
+
+SCENES = {"dam_break": dam_break, "splash": splash, "column_drop": column_drop}

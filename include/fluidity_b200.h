@@ -1,0 +1,223 @@
+/* fluidity_b200 -- C-ABI of the B200-native liquid-step hot path.
+ *
+ * One CUDA library (fluidity_b200/_lib/libfluidity_b200.so) exports these
+ * entry points. Signatures use plain pointers, sizes and a cudaStream_t passed
+ * as void*; no C++ or torch types cross the boundary. Every function returns
+ * a status with the reference's absl numbering (FL_OK = 0). There is no CPU
+ * fallback: without a usable sm_100 device the calls return
+ * FL_FAILED_PRECONDITION, as the reference's CUDA operators do
+ * (native/include/fluidity/host/cuda_mac_pressure_3d.h:154-158).
+ *
+ * The path replaces, in the FluidiTy reference (paths inside that project):
+ *   - DepositMac3D / DepositMacQuanta3D / GatherMac3D
+ *       native/include/fluidity/host/transfers_3d.h:23-61
+ *   - CudaDepositMacQuanta3D / CudaGatherMac3D
+ *       native/include/fluidity/host/cuda_transfers_3d.h:18-39
+ *   - ProjectMacPressure3D / CudaProjectMacPressure3D
+ *       native/include/fluidity/host/mac_pressure_3d.h:101-102,
+ *       native/include/fluidity/host/cuda_mac_pressure_3d.h:19-20
+ *   - the thin bridges LaunchDeposit3D / LaunchGather3D
+ *       (native/cuda/transfer_3d_bridge.h:62-83) and LaunchMacPressure3D /
+ *       LaunchMacPressureBatch3D (native/cuda/mac_pressure_3d_bridge.h:115-120)
+ *   - the scheduler backend ops .topology/.deposit/.normalize/.forces/.project/
+ *     .gather of LiquidSubstepBackend3D
+ *       (native/include/fluidity/host/liquid_substep_backend_3d.h:121-194)
+ *
+ * Threading: a context is single-threaded and non-reentrant, like the
+ * reference's backend (liquid_substep_backend_3d.h:37-46). Calls are ordered
+ * on the stream they are given; functions that must read a device value
+ * (block counts, convergence) synchronize that stream.
+ */
+#ifndef FLUIDITY_B200_H_
+#define FLUIDITY_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (absl::StatusCode numbering, as in native/src/*: transfers_3d.h:13-22,
+ * mac_pressure_3d.h:88-100, operator_runtime.h:18-40). */
+#define FL_OK 0
+#define FL_INVALID_ARGUMENT 3
+#define FL_RESOURCE_EXHAUSTED 8
+#define FL_FAILED_PRECONDITION 9
+#define FL_ABORTED 10
+#define FL_OUT_OF_RANGE 11
+#define FL_INTERNAL 13
+
+typedef struct fl_context fl_context;
+
+/* Device kernel report (MacTransferKernelReport3D, native/cuda/transfer_3d_bridge.h:54-57,
+ * plus the first failing index). */
+typedef struct {
+  int compiled_architecture; /* __CUDA_ARCH__ of the image that ran, e.g. 1000 */
+  int error;                 /* FL_* code written by the first failing lane, 0 if none */
+  unsigned long long first_bad_index;
+} fl_report;
+
+/* CudaOperatorMeasurement (native/include/fluidity/host/cuda_measurement.h:4-10). */
+typedef struct {
+  int compiled_architecture;
+  float kernel_ms;
+} fl_measurement;
+
+/* Uniform MAC geometry on a lattice of 8^3-cell blocks. Cells whose index lies
+ * outside [solid_lo, solid_hi] on any axis are solid (stationary walls); use
+ * INT32_MIN / INT32_MAX for a domain without walls. */
+typedef struct {
+  double origin[3]; /* world position of the lower corner of cell (0,0,0), m */
+  double h;         /* cell width, m */
+  int32_t block_lo[3];
+  int32_t block_dim[3];
+  int32_t solid_lo[3];
+  int32_t solid_hi[3];
+} fl_grid_desc;
+
+/* Device particle SoA in FP32 (60 B/particle without per-particle mass). */
+typedef struct {
+  float* x[3]; /* world position, m */
+  float* v[3]; /* velocity, m/s */
+  float* c[9]; /* APIC affine rows C[a][d], 1/s */
+  float* mass; /* kg per particle, or NULL for the uniform mass of the call */
+  uint64_t count;
+} fl_particles;
+
+typedef struct {
+  float dt;            /* s */
+  float particle_mass; /* kg, used when fl_particles.mass is NULL */
+  float gravity[3];    /* m/s^2 */
+  float min_face_mass; /* kg; faces at or below it are low-mass (velocity 0) */
+  float density;       /* kg/m^3 for the pressure conductance */
+} fl_transfer_params;
+
+typedef struct {
+  int levels;         /* multigrid levels (>= 4), 0 = automatic */
+  int pre_sweeps;     /* red-black Gauss-Seidel sweeps before the coarse correction */
+  int post_sweeps;    /* ... and after it */
+  int coarse_sweeps;  /* symmetric sweeps on the coarsest level */
+  int precision;      /* 0: FP32 V-cycle storage; 1: BF16 V-cycle storage */
+  int max_iterations; /* total inner flexible-CG iterations */
+  int max_refinements;
+  int pad;
+  double rel_tol;    /* ||b - A p||_2 <= rel_tol * ||b||_2, checked in FP64 */
+  double inner_rtol; /* inner FP32 solve reduction per refinement */
+} fl_pressure_options;
+
+typedef struct {
+  int status;
+  int iterations;
+  int refinements;
+  int levels;
+  int fluid_cells;
+  int active_blocks;
+  double rhs_l2;                 /* ||b||_2 in reference units, m^3/s */
+  double true_residual_l2;       /* ||b - A p||_2 in FP64, m^3/s */
+  double relative_residual;      /* true_residual_l2 / rhs_l2 */
+  double reference_limit;        /* 2e-6 + 2e-6 ||b||_2 (MacPressureStoppingCriteria) */
+  double max_volume_residual;    /* max |r|/V, 1/s (estimated from the FP64 l2 bound) */
+  double max_divergence;         /* max |div u_new| over fluid cells, 1/s */
+  double solve_ms;
+} fl_pressure_diagnostics;
+
+/* ---- context (the resident device arena) -------------------------------- */
+
+int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_context** out);
+int fl_context_destroy(fl_context* ctx);
+
+/* Active blocks: blocks holding particles plus a one-block ring
+ * (replaces the .topology backend op, liquid_substep_backend_3d.h:121-127). */
+int fl_topology_from_particles(fl_context* ctx, const fl_particles* particles, void* stream, fl_report* report);
+/* Explicit active blocks (8^3-block coordinates). */
+int fl_topology_from_blocks(fl_context* ctx, const int32_t* block_coords, uint64_t block_count);
+/* Copies up to `capacity` active block coordinates (x,y,z per block, ordinal order). */
+int fl_active_blocks(fl_context* ctx, int32_t* coords, uint64_t capacity, uint64_t* block_count);
+
+/* ---- the hot path ---------------------------------------------------- */
+
+/* Stable sort of the particles by (8^3 block, cell) into `out` (a separate
+ * buffer of the same capacity) and per-cell ranges kept in the context. */
+int fl_sort_particles_by_block(fl_context* ctx, const fl_particles* in, fl_particles* out, void* stream,
+                               fl_report* report);
+
+/* APIC P2G over sorted particles (DepositMac3D semantics). mode 0 writes face
+ * mass (out0) and pure momentum (out1); mode 1 writes the normalized velocity
+ * plus dt*gravity with stationary walls (out0, the predicted velocity) and the
+ * face mass (out1, may be NULL). Face arrays hold active_blocks*512 floats per axis. */
+int fl_p2g(fl_context* ctx, const fl_particles* sorted, const fl_transfer_params* params, int mode,
+           float* const out0[3], float* const out1[3], void* stream, fl_report* report);
+
+/* Pressure projection of the predicted face velocities of the box scene:
+ * fluid = non-solid cells holding particles (from the last sort), Dirichlet
+ * p = 0 against air, sealed against solid cells. Writes corrected velocities
+ * and, optionally, the FP64 cell pressure (active_blocks*512 doubles, Pa). */
+int fl_pressure_project(fl_context* ctx, const float* const u_pred[3], float* const u_new[3],
+                        const fl_transfer_params* params, const fl_pressure_options* options,
+                        fl_pressure_diagnostics* diagnostics, double* pressure_out, void* stream);
+
+/* One application of the V-cycle preconditioner z = M^-1 r on the cells of the
+ * last sort (fluid = non-solid cells holding particles), for checking the
+ * multigrid against its FP64 restatement. r and z hold active_blocks*512 floats
+ * in units of the full-face conductance. */
+int fl_apply_vcycle(fl_context* ctx, const float* r, float* z, const fl_pressure_options* options, void* stream);
+
+/* APIC G2P over sorted particles. With full_out == NULL: v <- PIC velocity,
+ * C <- fitted slopes, x <- clamp(x + dt v) in place. Otherwise writes 24 floats
+ * per sorted particle (MacParticleGatherResult3D layout) and leaves the state. */
+int fl_g2p(fl_context* ctx, fl_particles* sorted, const float* const u_new[3], const float* const u_old[3],
+           float dt, float* full_out, void* stream, fl_report* report);
+
+/* One full liquid substep on the context-resident particle state:
+ * topology -> sort -> P2G (+normalize, gravity, walls) -> pressure -> G2P (+advect). */
+int fl_step(fl_context* ctx, const fl_transfer_params* params, const fl_pressure_options* options,
+            fl_pressure_diagnostics* diagnostics, void* stream, fl_report* report);
+
+/* Context-resident particle state and buffers (device pointers). */
+int fl_upload_particles(fl_context* ctx, const float* host_soa, uint64_t count, void* stream);
+int fl_download_particles(fl_context* ctx, float* host_soa, void* stream);
+int fl_state_particles(fl_context* ctx, fl_particles* out);
+/* Face buffers of the last step: u_pred[3], u_new[3] (floats), pressure (doubles), cell type (bytes). */
+int fl_state_fields(fl_context* ctx, float* u_pred[3], float* u_new[3], double** pressure, uint8_t** cell_type,
+                    int32_t** cell_start);
+
+/* End-to-end substep with host buffers: uploads 15 x count FP32 SoA from
+ * host_in (pinned or pageable), runs fl_step and downloads the state to host_out. */
+int fl_step_host(fl_context* ctx, const float* host_in, float* host_out, uint64_t count,
+                 const fl_transfer_params* params, const fl_pressure_options* options,
+                 fl_pressure_diagnostics* diagnostics, void* stream);
+
+/* ---- reference-shaped operators (host FP64 data, reference 4^3 slot order) ---- */
+
+/* DepositMac3D on the GPU: particles are MacTransferParticle3D records of 19
+ * doubles (sorted xyz, trial xyz, mass, velocity xyz, slope rows); blocks are
+ * the reference's 4^3 active blocks; outputs follow the reference's owned-slot
+ * order (192 slots per 4^3 block, blocks sorted by (z,y,x)). FP32 arithmetic. */
+int fl_deposit_mac_3d(const double origin[3], double h, const int32_t* blocks, uint64_t block_count,
+                      const double* particles, uint64_t particle_count, double* face_mass, double* face_momentum,
+                      fl_measurement* measurement);
+
+/* DepositMacQuanta3D / CudaDepositMacQuanta3D: FP64 contributions rounded to
+ * nearest-even quanta and summed with 64-bit integer atomics (order-independent). */
+int fl_deposit_mac_quanta_3d(const double origin[3], double h, const int32_t* blocks, uint64_t block_count,
+                             const double* particles, uint64_t particle_count, double mass_per_quantum,
+                             double momentum_per_quantum, uint64_t declared_capacity, int64_t* mass_quanta,
+                             int64_t* momentum_quanta, fl_measurement* measurement);
+
+/* GatherMac3D / CudaGatherMac3D: 24 doubles per particle in input order. */
+int fl_gather_mac_3d(const double origin[3], double h, const int32_t* blocks, uint64_t block_count,
+                     const double* particles, uint64_t particle_count, const double* old_face_velocities,
+                     const double* new_face_velocities, double* results, fl_measurement* measurement);
+
+/* Plain device<->host copies for callers without their own CUDA runtime binding. */
+int fl_copy_to_host(void* host, const void* device, uint64_t bytes);
+int fl_copy_to_device(void* device, const void* host, uint64_t bytes);
+
+/* Library information: compiled architecture (e.g. 1000) and whether a usable device exists. */
+int fl_runtime_info(int* compiled_architecture, int* device_count, int* device_major, int* device_minor);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
