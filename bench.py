@@ -1,0 +1,359 @@
+"""Benchmark of the liquid substep on B200.
+
+Workload: the sparse 256^3 splash (pool y <= 0.2 over the floor + two
+counter-moving spheres), 8 particles per fluid cell (~29.6M particles), FP32
+transfers, mixed-precision projection (BF16 V-cycle storage, FP32 flexible CG,
+FP64 refinement to a 1e-6 relative residual). One step = topology + sort + P2G
+(+normalize, gravity, walls) + projection + G2P (+advection). Data: seeded
+synthetic scene generated on the host (no dataset involved).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0). With N > 1 (torchrun) every rank runs an
+independent replica: the path has no data exchange between GPUs.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "steps/s at 256^3 APIC (sparse splash, ~29.6M particles, projection to 1e-6 relative residual)"
+UNIT = "steps/s"
+WORKLOAD = {"workload": "splash_256", "grid": 256, "scene": "pool y<=0.2 + two r=0.15 spheres at +-2 m/s",
+            "particles_per_cell": 8, "dt": 1.0 / 240.0, "precision": "fp32 transfers, bf16 V-cycle, fp32 FCG, fp64 refinement",
+            "rel_tol": 1e-6, "l2": "inputs (1.8 GB of particles) larger than the 126 MB L2; no flush"}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = [r.split(",") for r in Path(self.path).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                mx = max(mx, float(r[1]))
+                for k, name in enumerate(names):
+                    if r[3 + k].strip().lower() == "active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _traffic_per_launch(particles: int, cells: int):
+    """DRAM bytes of one P2G launch pair from the committed ncu summary, scaled
+    by the units processed (profiles/p2g_splash.md records bytes per particle)."""
+    prof = ROOT / "profiles" / "p2g_splash.md"
+    if not prof.exists():
+        return None
+    for line in prof.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_particle:"):
+            return float(line.split(":")[1]) * particles
+    return None
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import fluidity_b200 as fb
+    from fluidity_b200 import scenes
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    soa, mass = scenes.splash(args.grid)
+    npart = soa.shape[1]
+    ctx = fb.LiquidContext(args.grid, capacity=npart)
+    tp = fb.transfer_params(scenes.DT, mass)
+    opt = fb.default_pressure_options(precision=1, rel_tol=1e-6)
+    ctx.upload(soa)
+    for _ in range(args.warmup):
+        code, _ = ctx.step(tp, opt)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches0 = fb.kernel_launches()
+    phases = np.zeros(4)
+    iters = []
+    residuals = []
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            code, diag = ctx.step(tp, opt)
+            phases += ctx.step_timings()
+            iters.append(diag.iterations)
+            residuals.append(diag.relative_residual)
+            if code != fb.OK:
+                raise RuntimeError(f"pressure did not converge: {diag.as_dict()}")
+        stop.record()
+        torch.cuda.synchronize()
+    launches1 = fb.kernel_launches()
+    ms = start.elapsed_time(stop)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+    nb = len(ctx.active_blocks())
+    ncell = nb * 512
+    # end-to-end through the C-ABI with pinned host buffers: H2D state, step, D2H state
+    pin_in = torch.from_numpy(soa).pin_memory()
+    pin_out = torch.empty_like(pin_in).pin_memory()
+    host_in, host_out = pin_in.numpy(), pin_out.numpy()
+    e2e_steps = max(2, min(args.steps, 5))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        ctx.step_host(host_in, host_out, tp, opt)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    peak, peak_kind = _peaks()
+    p2g_ms = phases[1] / args.steps
+    p2g_bytes = 60.0 * npart + 24.0 * ncell
+    achieved = p2g_bytes / (p2g_ms / 1e3) / 1e9
+    g2p_ms = phases[3] / args.steps
+    g2p_bytes = 72.0 * npart + 12.0 * ncell
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded splash scene)",
+        "config": dict(WORKLOAD, particles=npart, active_blocks=nb, allocated_cells=ncell,
+                       parallelism=f"replicas{world}"),
+        "e2e": {"value": round(world * 1e3 / e2e_ms, 4), "unit": UNIT, "h2d_bytes_per_step": int(60 * npart),
+                "d2h_bytes_per_step": int(60 * npart)},
+        "roofline": {"kernel": "p2g (k_p2g_tile + k_p2g_merge)", "bound": "hbm", "achieved": round(achieved, 1),
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "algorithmic_bytes": int(p2g_bytes), "traffic": _traffic_per_launch(npart, ncell)},
+        "phases_ms": {"topology_sort": round(phases[0] / args.steps, 4), "p2g": round(p2g_ms, 4),
+                      "pressure": round(phases[2] / args.steps, 4), "g2p": round(g2p_ms, 4)},
+        "g2p_roofline": {"achieved": round(g2p_bytes / (g2p_ms / 1e3) / 1e9, 1), "frac": round(
+            g2p_bytes / (g2p_ms / 1e3) / 1e9 / peak, 4)},
+        "pressure": {"mean_iterations": float(np.mean(iters)), "max_relative_residual": float(max(residuals))},
+        "gpu_launches": int(launches1[0] - launches0[0]),
+        "library_launches": int(launches1[1] - launches0[1]),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(soa, mass, args.grid, npart, ncell, budget_s=args.cpu_budget)
+    ctx.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return line
+
+
+def _sample_cube(soa, grid, sample):
+    """Particles inside an axis-aligned cube in the pool, sized to hold about
+    `sample` particles (8 per cell), centred away from the walls."""
+    half = 0.5 * (sample / (8.0 * grid ** 3)) ** (1.0 / 3.0)
+    centre = np.array([0.5, min(0.1, 0.2 - half), 0.5])
+    x = soa[0:3].T
+    inside = np.all(np.abs(x - centre) <= half, axis=1)
+    return np.nonzero(inside)[0]
+
+
+def _reference_sample_times(soa, mass, grid, sample, threads):
+    """Times the reference's own CPU operators (compiled from source) on a
+    compact particle sample split over `threads` host threads, plus one
+    ProjectMacPressure3D at its 4096-cell capacity."""
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+
+    if oracle.ref() is None:
+        return None
+    h = 1.0 / grid
+    idx = _sample_cube(soa, grid, sample)
+    x = soa[0:3, idx].T.astype(np.float64)
+    v = soa[3:6, idx].T.astype(np.float64)
+    c = soa[6:15, idx].T.astype(np.float64)
+    order = np.argsort(x[:, 0], kind="stable")
+    x, v, c = x[order], v[order], c[order]
+    chunks = [ch for ch in np.array_split(np.arange(len(idx)), threads) if len(ch)]
+    jobs = []
+    for ch in chunks:
+        xs = x[ch]
+        lo = np.floor(xs.min(0) / h / 4).astype(int) - 1
+        hi = np.floor(xs.max(0) / h / 4).astype(int) + 1
+        blocks = np.array([[i, j, k] for k in range(lo[2], hi[2] + 1) for j in range(lo[1], hi[1] + 1)
+                           for i in range(lo[0], hi[0] + 1)], np.int32)
+        jobs.append((blocks, oracle.particles_aos(xs, v[ch], c[ch], mass)))
+
+    def work(job):
+        blocks, parts = job
+        oracle.ref_deposit([0, 0, 0], h, blocks, parts)
+        u = np.zeros(192 * len(blocks))
+        oracle.ref_gather([0, 0, 0], h, blocks, parts, u, u)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(len(jobs)) as ex:
+        list(ex.map(work, jobs))
+    transfer_s = time.perf_counter() - t0
+    pressure_s, cells = _reference_pressure_time()
+    return transfer_s, len(idx), pressure_s, cells
+
+
+def _reference_pressure_time():
+    import oracle
+    from oracle.box_system import box_pressure_system, ref_blocks_for_box
+    from fluidity_b200 import scenes
+
+    n = 32
+    soa, m = scenes.dam_break(n)
+    x = soa[0:3].T.astype(np.float64)
+    v = soa[3:6].T.astype(np.float64)
+    c = soa[6:15].T.astype(np.float64)
+    box = oracle.Box.make([0, 0, 0], 1.0 / n, [0, 0, 0], [n, n, n])
+    fm, fq = oracle.p2g(box, x, v, c, m)
+    u_pred, _ = oracle.normalize_forces(box, fm, fq, 0.0, scenes.DT, scenes.GRAVITY)
+    ct = oracle.classify_cells(box, x)
+    s = box_pressure_system(box, ct, u_pred)
+    t0 = time.perf_counter()
+    oracle.ref_project([0, 0, 0], box.h, ref_blocks_for_box(n), scenes.DT, s["cells_idx"], s["cells_val"],
+                       s["faces_idx"], s["faces_kind"], s["faces_val"], tolerance_scale=1.0)
+    return time.perf_counter() - t0, len(s["cells_idx"])
+
+
+def cpu_baseline(soa, mass, grid, npart, ncell, budget_s=15.0, threads=1):
+    sample = 400000 * threads
+    res = _reference_sample_times(soa, mass, grid, sample, threads)
+    if res is None:
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": "reference operators not built"}
+    transfer_s, nsample, pressure_s, pcells = res
+    fluid_cells = npart / 8
+    step_s = transfer_s * (npart / nsample) + pressure_s * (fluid_cells / pcells)
+    return {"value": round(1.0 / step_s, 8), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": (f"DepositMac3D+GatherMac3D on {nsample} of {npart} particles ({transfer_s:.2f} s), "
+                       f"ProjectMacPressure3D on its 4096-cell cap ({pcells} cells, {pressure_s:.3f} s); "
+                       f"scaled linearly to the full step (pressure scaling is a lower bound)")}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    import oracle
+    from fluidity_b200 import scenes
+
+    if oracle.ref() is None:
+        return {"impl": "reference", "unavailable": "reference CPU operators not built (oracle/ref/Makefile)"}
+    soa, mass = scenes.splash(args.grid)
+    npart = soa.shape[1]
+    threads = max(1, os.cpu_count() or 1)
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        res = _reference_sample_times(soa, mass, args.grid, 20000 * threads, threads)
+        transfer_s, nsample, pressure_s, pcells = res
+        step_s = transfer_s * (npart / nsample) + pressure_s * (npart / 8 / pcells)
+        if k >= args.warmup:
+            times.append(step_s)
+    value = 1.0 / float(np.mean(times))
+    return {"metric": METRIC, "value": round(value, 8), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 / value, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splash scene)",
+            "config": dict(WORKLOAD, particles=npart), "impl": "reference",
+            "cpu_baseline": {"value": round(value, 8), "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"per step: DepositMac3D+GatherMac3D on {20000 * threads} particles over "
+                                       f"{threads} threads + ProjectMacPressure3D at 4096 cells, scaled to "
+                                       f"{npart} particles"},
+            "e2e": {"value": round(value, 8), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--grid", type=int, default=256)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    world, rank, local = _dist()
+    if args.impl == "reference":
+        line = run_reference(args, world, rank)
+    else:
+        line = run_ours(args, world, rank, local)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -68,8 +68,8 @@ class Particles(ctypes.Structure):
 
 
 class TransferParams(ctypes.Structure):
-    _fields_ = [("dt", ctypes.c_float), ("particle_mass", ctypes.c_float), ("gravity", ctypes.c_float * 3),
-                ("min_face_mass", ctypes.c_float), ("density", ctypes.c_float)]
+    _fields_ = [("dt", ctypes.c_double), ("particle_mass", ctypes.c_double), ("gravity", ctypes.c_double * 3),
+                ("min_face_mass", ctypes.c_double), ("density", ctypes.c_double)]
 
 
 class PressureOptions(ctypes.Structure):
@@ -96,7 +96,7 @@ EXPORTS = [
     "fl_active_blocks", "fl_sort_particles_by_block", "fl_p2g", "fl_pressure_project", "fl_g2p", "fl_step",
     "fl_upload_particles", "fl_download_particles", "fl_state_particles", "fl_state_fields", "fl_step_host",
     "fl_deposit_mac_3d", "fl_deposit_mac_quanta_3d", "fl_gather_mac_3d", "fl_copy_to_host", "fl_copy_to_device",
-    "fl_runtime_info", "fl_apply_vcycle",
+    "fl_runtime_info", "fl_apply_vcycle", "fl_step_timings", "fl_kernel_launches",
 ]
 
 _lib = None
@@ -144,6 +144,8 @@ def library():
         lib.fl_copy_to_device.argtypes = [vp, vp, ctypes.c_uint64]
         lib.fl_runtime_info.argtypes = [ctypes.POINTER(ctypes.c_int)] * 4
         lib.fl_apply_vcycle.argtypes = [vp, vp, vp, ctypes.POINTER(PressureOptions), vp]
+        lib.fl_step_timings.argtypes = [vp, _fp]
+        lib.fl_kernel_launches.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]
         _lib = lib
     return _lib
 
@@ -304,6 +306,12 @@ class LiquidContext:
             raise FluidityError(code, "fl_step_host")
         return code, diag
 
+    def step_timings(self):
+        """CUDA-event ms of the last step: topology+sort, P2G, pressure, G2P."""
+        ms = np.zeros(4, np.float32)
+        _check(library().fl_step_timings(self._ctx, ms.ctypes.data_as(_fp)), "fl_step_timings")
+        return ms
+
     def active_blocks(self) -> np.ndarray:
         cnt = ctypes.c_uint64()
         library().fl_active_blocks(self._ctx, None, 0, ctypes.byref(cnt))
@@ -325,6 +333,12 @@ class LiquidContext:
         p = Particles()
         _check(library().fl_state_particles(self._ctx, ctypes.byref(p)), "fl_state_particles")
         return p
+
+
+def kernel_launches():
+    own, libc = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+    library().fl_kernel_launches(ctypes.byref(own), ctypes.byref(libc))
+    return own.value, libc.value
 
 
 def copy_to_host(ptr, count, dtype) -> np.ndarray:

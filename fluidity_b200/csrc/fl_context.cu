@@ -25,6 +25,8 @@
 #include "fl_kernels.h"
 
 namespace fl {
+unsigned long long g_kernel_launches = 0;
+unsigned long long g_library_launches = 0;
 cudaError_t launch_deposit_quanta(const GridView& g, const double* parts, unsigned long long n,
                                   const double origin[3], double h, double mass_per_quantum,
                                   double momentum_per_quantum, double limit, unsigned long long* const mq[3],
@@ -77,6 +79,7 @@ struct fl_context {
   // multigrid storage (x and k sized for FP32; BF16 uses the first half)
   int max_levels = 0;
   unsigned char* lv_fluid[12] = {};
+  unsigned char* lv_mask0 = nullptr;
   void* lv_k[12][3] = {};
   float* lv_anchor[12] = {};
   float* lv_diag[12] = {};
@@ -87,6 +90,8 @@ struct fl_context {
   DeviceReport* rep_host = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool in_step = false;  // fl_step keeps one device report across its stages
+  cudaEvent_t phase[5] = {};  // topology+sort | P2G | pressure | G2P boundaries of the last fl_step
+  bool phases_valid = false;
 };
 
 namespace {
@@ -189,7 +194,7 @@ int auto_levels(const fl_context* c) {
   for (int L = 4; L <= c->max_levels; ++L) {
     long long n = 1;
     for (int d = 0; d < 3; ++d) n *= dense_dim(c->desc.block_dim[d], L - 1);
-    if (n <= 4096) return L;
+    if (n <= 512) return L;
   }
   return c->max_levels;
 }
@@ -220,6 +225,7 @@ int make_hierarchy(fl_context* c, int levels, MgHierarchy<T>& H) {
     }
     H.desc[l] = D;
     LevelPtrs<T> P{};
+    P.mask = l == 0 ? c->lv_mask0 : nullptr;
     P.fluid = c->lv_fluid[l];
     for (int a = 0; a < 3; ++a) P.k[a] = reinterpret_cast<T*>(c->lv_k[l][a]);
     P.anchor = c->lv_anchor[l];
@@ -272,9 +278,11 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   const long long n = (long long)c->nb * kBlockCells;
   MgOptions mo{std::max(1, opt->pre_sweeps), std::max(1, opt->post_sweeps), std::max(1, opt->coarse_sweeps)};
   FL_CUDA(cudaEventRecord(c->ev0, s));
+  ++g_kernel_launches;
   k_init_state<<<1, 1, 0, s>>>(c->st, opt->rel_tol, opt->inner_rtol, opt->max_iterations);
   FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, u_pred, rhs_scale, H, c->b64, c->p64, c->partial,
                                    c->st, s));
+  ++g_kernel_launches;
   k_set_target<<<1, 1, 0, s>>>(c->st, opt->rel_tol);
   FL_CUDA(cudaMemsetAsync(c->lv_x[0], 0, sizeof(T) * (size_t)n, s));
   FL_CUDA(cudaMemsetAsync(c->d[0], 0, sizeof(float) * (size_t)n, s));
@@ -294,6 +302,7 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
     }
     if (outer == max_ref || total >= opt->max_iterations) break;
     ++refinements;
+    ++g_kernel_launches;
     k_set_inner_budget<<<1, 1, 0, s>>>(c->st, opt->max_iterations - total);
     int cur = 0;
     int it = 0;
@@ -348,7 +357,7 @@ __global__ void k_copy_x(long long n, const float* fluid_src, const void* x, int
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   float v = bf16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(x)[i]) : reinterpret_cast<const float*>(x)[i];
-  z[i] = fluid[i] ? v : 0.0f;
+  z[i] = fluid[i] ? v : 0.0f;  // fluid = level-0 flags
   (void)fluid_src;
 }
 
@@ -361,6 +370,7 @@ int apply_vcycle(fl_context* c, const float* r, float* z, const fl_pressure_opti
   if (st != FL_OK) return st;
   MgOptions mo{std::max(1, opt->pre_sweeps), std::max(1, opt->post_sweeps), std::max(1, opt->coarse_sweeps)};
   const long long n = (long long)c->nb * kBlockCells;
+  ++g_kernel_launches;
   k_init_state<<<1, 1, 0, s>>>(c->st, 1e-6, 1e-4, 1);
   const float* up[3] = {c->u_pred[0], c->u_pred[1], c->u_pred[2]};
   FL_CUDA(cudaMemsetAsync(c->u_pred[0], 0, sizeof(float) * n, s));
@@ -369,6 +379,7 @@ int apply_vcycle(fl_context* c, const float* r, float* z, const fl_pressure_opti
   FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, up, 1.0, H, c->b64, c->p64, c->partial, c->st, s));
   FL_CUDA(cudaMemsetAsync(c->lv_x[0], 0, sizeof(T) * (size_t)n, s));
   FL_CUDA(launch_apply_vcycle<T>(g, H, r, mo, &c->st->done, s));
+  ++g_kernel_launches;
   k_copy_x<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, r, c->lv_x[0], sizeof(T) == 2, z, c->lv_fluid[0]);
   FL_CUDA(cudaGetLastError());
   FL_CUDA(cudaStreamSynchronize(s));
@@ -554,7 +565,7 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
   for (int d = 0; d < 3; ++d)
     if (grid->block_dim[d] <= 0 || !std::isfinite(grid->origin[d])) return FL_INVALID_ARGUMENT;
   const long long lattice = (long long)grid->block_dim[0] * grid->block_dim[1] * grid->block_dim[2];
-  if (lattice > (1LL << 22)) return FL_RESOURCE_EXHAUSTED;
+  if (lattice > (1LL << 21)) return FL_RESOURCE_EXHAUSTED;
   if (particle_capacity >= (1ULL << 31)) return FL_RESOURCE_EXHAUSTED;
   int st = device_ready();
   if (st != FL_OK) return st;
@@ -605,6 +616,7 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
   chk(dalloc(&c->rep, 1));
   chk(cudaMallocHost(&c->rep_host, sizeof(DeviceReport)) == cudaSuccess ? FL_OK : FL_RESOURCE_EXHAUSTED);
   // multigrid levels
+  chk(dalloc(&c->lv_mask0, cells));
   int maxbd = std::max(grid->block_dim[0], std::max(grid->block_dim[1], grid->block_dim[2]));
   int L = 4;
   while (L < 12 && dense_dim(maxbd, L - 1) > 1) ++L;
@@ -631,6 +643,8 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
     }
   }
   if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) chk(FL_INTERNAL);
+  for (int k = 0; k < 5; ++k)
+    if (cudaEventCreate(&c->phase[k]) != cudaSuccess) chk(FL_INTERNAL);
   if (e == FL_OK) {
     cudaMemset(c->st, 0, sizeof(SolverState));
     cudaMemset(c->rep, 0, sizeof(DeviceReport));
@@ -683,6 +697,7 @@ int fl_context_destroy(fl_context* c) {
   if (c->st_host) cudaFreeHost(c->st_host);
   cudaFree(c->rep);
   if (c->rep_host) cudaFreeHost(c->rep_host);
+  cudaFree(c->lv_mask0);
   for (int l = 0; l < 12; ++l) {
     cudaFree(c->lv_fluid[l]);
     for (int a = 0; a < 3; ++a) cudaFree(c->lv_k[l][a]);
@@ -693,6 +708,8 @@ int fl_context_destroy(fl_context* c) {
   }
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (int k = 0; k < 5; ++k)
+    if (c->phase[k]) cudaEventDestroy(c->phase[k]);
   delete c;
   return FL_OK;
 }
@@ -780,10 +797,10 @@ int fl_p2g(fl_context* c, const fl_particles* sorted, const fl_transfer_params* 
   P2GMergeParams prm{};
   prm.mode = mode;
   prm.walls = mode == 1 ? 1 : 0;
-  prm.mass_scale = sorted->mass ? 1.0f : tp->particle_mass;
-  prm.min_face_mass = tp->min_face_mass;
-  prm.dt = tp->dt;
-  for (int d = 0; d < 3; ++d) prm.gravity[d] = tp->gravity[d];
+  prm.mass_scale = sorted->mass ? 1.0f : (float)tp->particle_mass;
+  prm.min_face_mass = (float)tp->min_face_mass;
+  prm.dt = (float)tp->dt;
+  for (int d = 0; d < 3; ++d) prm.gravity[d] = (float)tp->gravity[d];
   float* o1[3] = {out1 ? out1[0] : nullptr, out1 ? out1[1] : nullptr, out1 ? out1[2] : nullptr};
   FL_CUDA(launch_p2g(g, pv, c->cell_start, c->tiles, prm, out0, o1, c->rep, s));
   if (report) return read_report(c, s, report);
@@ -878,6 +895,8 @@ int fl_step(fl_context* c, const fl_transfer_params* tp, const fl_pressure_optio
   cudaStream_t s = (cudaStream_t)stream;
   fl_particles A = state_particles(c, c->cur), B = state_particles(c, 1 - c->cur);
   fl_report rep{};
+  c->phases_valid = false;
+  cudaEventRecord(c->phase[0], s);
   int st = fl_topology_from_particles(c, &A, stream, &rep);
   if (st != FL_OK) {
     if (report) *report = rep;
@@ -890,22 +909,41 @@ int fl_step(fl_context* c, const fl_transfer_params* tp, const fl_pressure_optio
   c->in_step = true;
   st = fl_sort_particles_by_block(c, &A, &B, stream, nullptr);
   if (st != FL_OK) return st;
+  cudaEventRecord(c->phase[1], s);
   float* o0[3] = {c->u_pred[0], c->u_pred[1], c->u_pred[2]};
   float* o1[3] = {c->fmass[0], c->fmass[1], c->fmass[2]};
   st = fl_p2g(c, &B, tp, 1, o0, o1, stream, nullptr);
   if (st != FL_OK) return st;
+  cudaEventRecord(c->phase[2], s);
   const float* up[3] = {c->u_pred[0], c->u_pred[1], c->u_pred[2]};
   float* un[3] = {c->u_new[0], c->u_new[1], c->u_new[2]};
   st = fl_pressure_project(c, up, un, tp, opt, diag, nullptr, stream);
   if (st != FL_OK && st != FL_ABORTED) return st;
   const int pressure_status = st;
+  cudaEventRecord(c->phase[3], s);
   const float* unc[3] = {c->u_new[0], c->u_new[1], c->u_new[2]};
-  st = fl_g2p(c, &B, unc, nullptr, tp->dt, nullptr, stream, nullptr);
+  st = fl_g2p(c, &B, unc, nullptr, (float)tp->dt, nullptr, stream, nullptr);
   if (st != FL_OK) return st;
+  cudaEventRecord(c->phase[4], s);
+  c->phases_valid = true;
   c->cur = 1 - c->cur;
   const int err = read_report(c, s, report);
   if (err != FL_OK) return err;
   return pressure_status;
+}
+
+int fl_step_timings(fl_context* c, float* ms) {
+  if (!c || !ms) return FL_INVALID_ARGUMENT;
+  if (!c->phases_valid) return FL_FAILED_PRECONDITION;
+  FL_CUDA(cudaEventSynchronize(c->phase[4]));
+  for (int k = 0; k < 4; ++k) FL_CUDA(cudaEventElapsedTime(&ms[k], c->phase[k], c->phase[k + 1]));
+  return FL_OK;
+}
+
+int fl_kernel_launches(unsigned long long* own, unsigned long long* library) {
+  if (own) *own = g_kernel_launches;
+  if (library) *library = g_library_launches;
+  return FL_OK;
 }
 
 int fl_step_host(fl_context* c, const float* host_in, float* host_out, uint64_t count, const fl_transfer_params* tp,
@@ -1044,7 +1082,7 @@ int fl_deposit_mac_quanta_3d(const double origin[3], double h, const int32_t* bl
       momentum_quanta[sidx] = (int64_t)host[(size_t)(3 + axis[sidx]) * n8 + slot8[sidx]];
     }
     if (meas) {
-      meas->compiled_architecture = rep.compiled_architecture ? rep.compiled_architecture : 1000;
+      meas->compiled_architecture = rep.compiled_architecture;
       cudaEventElapsedTime(&meas->kernel_ms, c->ev0, c->ev1);
     }
   } while (false);

@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(kG2PThreads)
   __shared__ float tile[3 * kTileFaces];
   __shared__ float tile_old[kFull ? 3 * kTileFaces : 1];
   const int b = blockIdx.x, t = threadIdx.x;
+  if (b == 0 && t == 0 && rep != nullptr) rep->compiled_architecture = compiled_arch();
   const int pbeg = cell_start[b * kBlockCells], pend = cell_start[(b + 1) * kBlockCells];
   if (pbeg == pend) return;
   const float* un[3] = {u0, u1, u2};
@@ -176,10 +177,12 @@ cudaError_t launch_g2p(const GridView& g, const ParticlesView& p, const int* cel
                        cudaStream_t s) {
   if (g.nb == 0 || p.count == 0) return cudaSuccess;
   if (full_out != nullptr) {
+    ++g_kernel_launches;
     k_g2p<true><<<g.nb, kG2PThreads, 0, s>>>(g, p, cell_start, u[0], u[1], u[2], u_old ? u_old[0] : nullptr,
                                               u_old ? u_old[1] : nullptr, u_old ? u_old[2] : nullptr, prm, full_out,
                                               rep);
   } else {
+    ++g_kernel_launches;
     k_g2p<false><<<g.nb, kG2PThreads, 0, s>>>(g, p, cell_start, u[0], u[1], u[2], nullptr, nullptr, nullptr, prm,
                                                nullptr, rep);
   }

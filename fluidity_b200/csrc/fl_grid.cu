@@ -164,16 +164,25 @@ cudaError_t launch_topology_from_particles(const GridView& g, const ParticlesVie
                                            void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s) {
   const int total = g.bdim[0] * g.bdim[1] * g.bdim[2];
   cudaMemsetAsync(occ, 0, (size_t)total, s);
-  if (p.count > 0) k_mark_blocks<<<grid_for(p.count, 256), 256, 0, s>>>(g, p, occ, rep);
+  if (p.count > 0) {
+    ++g_kernel_launches;
+    k_mark_blocks<<<grid_for(p.count, 256), 256, 0, s>>>(g, p, occ, rep);
+  }
+  ++g_kernel_launches;
   k_flag_active<<<grid_for(total, 256), 256, 0, s>>>(g, occ, flag, total);
   size_t tb = temp_bytes;
+  ++g_library_launches;
   cub::DeviceScan::ExclusiveSum(temp, tb, flag, ordinal, total, s);
+  ++g_kernel_launches;
   k_compact<<<grid_for(total, 256), 256, 0, s>>>(g, flag, ordinal, table, coord, total, nb_dev);
   return cudaGetLastError();
 }
 
 cudaError_t launch_build_neighbors(const GridView& g, int* nbr27, cudaStream_t s) {
-  if (g.nb > 0) k_build_nbr27<<<grid_for((unsigned long long)g.nb * 27, 256), 256, 0, s>>>(g, nbr27);
+  if (g.nb > 0) {
+    ++g_kernel_launches;
+    k_build_nbr27<<<grid_for((unsigned long long)g.nb * 27, 256), 256, 0, s>>>(g, nbr27);
+  }
   return cudaGetLastError();
 }
 
@@ -182,16 +191,21 @@ cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const Partic
                         int* cell_start, void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s) {
   const size_t ncell = (size_t)g.nb * 512;
   cudaMemsetAsync(counts, 0, sizeof(int) * (ncell + 1), s);
+  ++g_kernel_launches;
   k_write_arch<<<1, 32, 0, s>>>(rep);
   if (in.count > 0) {
+    ++g_kernel_launches;
     k_cell_keys<<<grid_for(in.count, 256), 256, 0, s>>>(g, in, keys, index, counts, rep);
     int end_bit = 1;
     while (end_bit < 32 && ((size_t)1 << end_bit) < ncell + 1) ++end_bit;
     size_t tb = temp_bytes;
+    ++g_library_launches;
     cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys_alt, index, index_alt, (int)in.count, 0, end_bit, s);
+    ++g_kernel_launches;
     k_permute<<<grid_for(in.count, 256), 256, 0, s>>>(in, out, index_alt);
   }
   size_t tb = temp_bytes;
+  ++g_library_launches;
   cub::DeviceScan::ExclusiveSum(temp, tb, counts, cell_start, (int)(ncell + 1), s);
   return cudaGetLastError();
 }

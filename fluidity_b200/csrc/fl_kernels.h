@@ -37,6 +37,7 @@ struct LevelDesc {
 
 template <typename T>
 struct LevelPtrs {
+  unsigned char* mask;  // level 0 only: bit 2a (2a+1) = low (high) face joins two fluid cells; bit 6 = fluid
   unsigned char* fluid;
   T* k[3];        // coefficient of the cell's low face (to the -e_a neighbour)
   float* anchor;  // Dirichlet/compliance part of the diagonal
@@ -78,6 +79,11 @@ struct SolverState {
 
 __device__ __forceinline__ long long parent_of(const GridView& g, const LevelDesc& F, const LevelDesc& C,
                                                long long j);
+
+// Number of this library's own kernels launched so far (host-side count).
+extern unsigned long long g_kernel_launches;
+// Library (CUB) device-wide algorithm invocations so far.
+extern unsigned long long g_library_launches;
 
 size_t sort_temp_bytes(size_t particle_capacity, size_t cell_capacity);
 cudaError_t launch_topology_from_particles(const GridView& g, const ParticlesView& p, unsigned char* occ, int* flag,

@@ -192,6 +192,7 @@ __global__ void k_p2g_merge(GridView g, const int* cell_start, const float2* til
                             float* out0_x, float* out0_y, float* out0_z, float* out1_x, float* out1_y,
                             float* out1_z, DeviceReport* rep) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i == 0 && rep != nullptr) rep->compiled_architecture = compiled_arch();
   if (i >= (long long)g.nb * 3 * kBlockCells) return;
   const int b = (int)(i / (3 * kBlockCells));
   const int a = (int)((i / kBlockCells) % 3);
@@ -249,8 +250,10 @@ cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cel
     cudaFuncSetAttribute(k_p2g_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     configured = true;
   }
+  ++g_kernel_launches;
   k_p2g_tile<<<g.nb, kP2GThreads, smem, s>>>(g, p, cell_start, tiles, rep);
   const long long faces = (long long)g.nb * 3 * kBlockCells;
+  ++g_kernel_launches;
   k_p2g_merge<<<(unsigned)((faces + 255) / 256), 256, 0, s>>>(g, cell_start, tiles, prm, out0[0], out0[1], out0[2],
                                                                out1[0], out1[1], out1[2], rep);
   return cudaGetLastError();

@@ -35,8 +35,13 @@
 namespace fl {
 
 constexpr int kThreads = 256;
+constexpr int kReduceCtas = 4 * 148;  // fixed grid of the reduction kernels (multiple of the SM count)
 
 static inline unsigned blocks_for(long long n, int t = kThreads) { return (unsigned)((n + t - 1) / t); }
+static inline unsigned reduce_grid(long long n) {
+  const unsigned b = blocks_for(n);
+  return b < 1 ? 1u : (b > (unsigned)kReduceCtas ? (unsigned)kReduceCtas : b);
+}
 
 // ----------------------------------------------------------------- neighbours
 
@@ -106,6 +111,36 @@ __device__ __forceinline__ int cell_parity(const GridView& g, const LevelDesc& L
   return (p.x + p.y + p.z + L.parity) & 1;
 }
 
+// ----------------------------------------------------------------- fast in-block neighbours
+
+// Neighbour of local cell l of block b on a sparse level with 2^LS cells per
+// axis (shifts and masks only). Returns the cell id, -1 for an inactive block
+// inside the lattice (air, no unknown) or -2 outside the lattice (solid).
+template <int LS>
+__device__ __forceinline__ int nbr_s(const GridView& g, int b, int l, int a, int dir) {
+  constexpr int S = 1 << LS, S3 = S * S * S;
+  const int c = (l >> (LS * a)) & (S - 1);
+  const int step = 1 << (LS * a);
+  if (dir < 0 ? c > 0 : c < S - 1) return b * S3 + l + dir * step;
+  const int n = g.nbr27[b * 27 + 13 + dir * (a == 0 ? 1 : (a == 1 ? 3 : 9))];
+  if (n < 0) return n;
+  return n * S3 + l - dir * (S - 1) * step;
+}
+
+// Coarse parent of fine cell j on sparse level LS: the next sparse level, or
+// (LS == 1) the dense block-lattice cell of j's block.
+template <int LS>
+__device__ __forceinline__ int parent_s(const GridView& g, int j, int cdx, int cdy) {
+  constexpr int S = 1 << LS, S3 = S * S * S;
+  const int b = j / S3, l = j % S3;
+  if (LS > 1) {
+    constexpr int SC = S / 2;
+    const int x = (l & (S - 1)) >> 1, y = ((l >> LS) & (S - 1)) >> 1, z = (l >> (2 * LS)) >> 1;
+    return b * SC * SC * SC + (z * SC + y) * SC + x;
+  }
+  return ((g.coord[3 * b + 2] - g.blo[2]) * cdy + (g.coord[3 * b + 1] - g.blo[1])) * cdx + (g.coord[3 * b] - g.blo[0]);
+}
+
 // ----------------------------------------------------------------- level-0 setup (box scene)
 
 __device__ __forceinline__ bool last_block(SolverState* st) {
@@ -117,6 +152,12 @@ __device__ __forceinline__ bool last_block(SolverState* st) {
   return last;
 }
 
+// Sum of per-CTA partials by the last CTA, in a fixed order.
+__device__ __forceinline__ double finish_sum(const double* partial, int stride, int offset, double* red) {
+  double t = 0.0;
+  for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) t += partial[stride * k + offset];
+  return block_sum<kThreads>(t, red);
+}
 
 __device__ __forceinline__ bool solid_cell(const GridView& g, int x, int y, int z) {
   return x < g.solid_lo[0] || y < g.solid_lo[1] || z < g.solid_lo[2] || x > g.solid_hi[0] || y > g.solid_hi[1] ||
@@ -124,9 +165,9 @@ __device__ __forceinline__ bool solid_cell(const GridView& g, int x, int y, int 
 }
 
 __global__ void k_classify(GridView g, const int* cell_start, unsigned char* type) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)g.nb * kBlockCells) return;
-  const int b = (int)(i / kBlockCells), l = (int)(i % kBlockCells);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nb * kBlockCells) return;
+  const int b = i >> 9, l = i & 511;
   const int x = g.coord[3 * b] * 8 + (l & 7), y = g.coord[3 * b + 1] * 8 + ((l >> 3) & 7),
             z = g.coord[3 * b + 2] * 8 + (l >> 6);
   unsigned char t;
@@ -139,7 +180,7 @@ __global__ void k_classify(GridView g, const int* cell_start, unsigned char* typ
 
 // Type of a level-0 neighbour: inactive blocks inside the lattice hold no
 // particles and no walls adjacent to fluid, i.e. air; outside the lattice is solid.
-__device__ __forceinline__ int nbr_type(const unsigned char* type, long long id) {
+__device__ __forceinline__ int nbr_type(const unsigned char* type, int id) {
   if (id == -1) return 2;
   if (id < 0) return 0;
   return type[id];
@@ -150,45 +191,42 @@ __global__ void k_setup_level0(GridView g, const unsigned char* type, const floa
                                const float* u2, double rhs_scale, LevelPtrs<T> L0, double* b64, double* p64,
                                double* partial, SolverState* st) {
   __shared__ double red[kThreads / 32];
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long n = (long long)g.nb * kBlockCells;
+  const int n = g.nb * kBlockCells;
+  const float* u[3] = {u0, u1, u2};
   double bb = 0.0;
-  if (i < n) {
-    const int b = (int)(i / kBlockCells), l = (int)(i % kBlockCells);
-    const int lx = l & 7, ly = (l >> 3) & 7, lz = l >> 6;
-    const float* u[3] = {u0, u1, u2};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int b = i >> 9, l = i & 511;
     const bool fluid = type[i] == 1;
-    float anchor = 0.0f, diag = 0.0f;
+    float anchor = 0.0f;
+    unsigned mask = fluid ? 64u : 0u;
     double div = 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const long long lo = sparse_nbr(g, 8, b, lx, ly, lz, a, -1);
-      const long long hi = sparse_nbr(g, 8, b, lx, ly, lz, a, +1);
+      const int lo = nbr_s<3>(g, b, l, a, -1);
+      const int hi = nbr_s<3>(g, b, l, a, +1);
       const int tlo = nbr_type(type, lo), thi = nbr_type(type, hi);
-      const float klo = (fluid && tlo == 1) ? 1.0f : 0.0f;
-      st_T(&L0.k[a][i], klo);
       if (fluid) {
+        mask |= (tlo == 1 ? 1u : 0u) << (2 * a);
+        mask |= (thi == 1 ? 1u : 0u) << (2 * a + 1);
         anchor += (tlo == 2 ? 1.0f : 0.0f) + (thi == 2 ? 1.0f : 0.0f);
-        diag += (tlo != 0 ? 1.0f : 0.0f) + (thi != 0 ? 1.0f : 0.0f);
         const double ulo = (double)u[a][i];
         const double uhi = hi >= 0 ? (double)u[a][hi] : 0.0;
         div += uhi - ulo;
       }
     }
+    L0.mask[i] = (unsigned char)mask;
     L0.fluid[i] = fluid ? 1 : 0;
     L0.anchor[i] = anchor;
-    L0.diag[i] = diag;
+    L0.diag[i] = fluid ? anchor + (float)__popc(mask & 63u) : 1.0f;
     const double rhs = fluid ? -rhs_scale * div : 0.0;
     b64[i] = rhs;
     p64[i] = 0.0;
-    bb = rhs * rhs;
+    bb += rhs * rhs;
   }
   const double s = block_sum<kThreads>(bb, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
   if (last_block(st)) {
-    double t = 0.0;
-    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) t += partial[k];
-    t = block_sum<kThreads>(t, red);
+    const double t = finish_sum(partial, 1, 0, red);
     if (threadIdx.x == 0) {
       st->b_norm = sqrt(t);
       st->ticket = 0;
@@ -196,16 +234,16 @@ __global__ void k_setup_level0(GridView g, const unsigned char* type, const floa
   }
 }
 
-// ----------------------------------------------------------------- coarsening
+// ----------------------------------------------------------------- coarsening (once per solve)
 
 // Child count per axis is 2; for sparse->sparse the block is shared, for
 // sparse(S=2)->dense the block maps to one dense cell, dense->dense halves.
+// Level-0 coefficients come from the neighbour mask.
 template <typename T>
 __global__ void k_coarsen(GridView g, LevelDesc F, LevelPtrs<T> fp, LevelDesc C, LevelPtrs<T> cp) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= C.count) return;
   const CellPos p = cell_pos(C, i);
-  // Locate children.
   long long child[8];
   int nchild = 0;
   int cl[8][3];
@@ -220,11 +258,6 @@ __global__ void k_coarsen(GridView g, LevelDesc F, LevelPtrs<T> fp, LevelDesc C,
           child[nchild++] = (long long)p.b * S * S * S + ((2 * p.z + dz) * S + 2 * p.y + dy) * S + 2 * p.x + dx;
         }
   } else if (F.sparse) {
-    // dense cell = block lattice coordinate; find the block ordinal
-    const int bx = p.x + g.blo[0], by = p.y + g.blo[1], bz = p.z + g.blo[2];
-    (void)bx;
-    (void)by;
-    (void)bz;
     const int o = g.table[((long long)p.z * g.bdim[1] + p.y) * g.bdim[0] + p.x];
     if (o >= 0) {
       for (int dz = 0; dz < 2; ++dz)
@@ -256,7 +289,7 @@ __global__ void k_coarsen(GridView g, LevelDesc F, LevelPtrs<T> fp, LevelDesc C,
     anchor += fp.anchor[id];
 #pragma unroll
     for (int a = 0; a < 3; ++a)
-      if (cl[c][a] == 0) k[a] += ld(&fp.k[a][id]);
+      if (cl[c][a] == 0) k[a] += fp.mask ? (float)((fp.mask[id] >> (2 * a)) & 1u) : ld(&fp.k[a][id]);
   }
   cp.fluid[i] = fluid ? 1 : 0;
   cp.anchor[i] = 0.5f * anchor;
@@ -265,7 +298,7 @@ __global__ void k_coarsen(GridView g, LevelDesc F, LevelPtrs<T> fp, LevelDesc C,
 }
 
 // diag = anchor + sum of the six face coefficients (after coarsening, since a
-// cell's high faces belong to its neighbours).
+// cell's high faces belong to its neighbours). Levels >= 1.
 template <typename T>
 __global__ void k_level_diag(GridView g, LevelDesc L, LevelPtrs<T> lp) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -281,32 +314,53 @@ __global__ void k_level_diag(GridView g, LevelDesc L, LevelPtrs<T> lp) {
   lp.diag[i] = lp.fluid[i] ? d : 1.0f;
 }
 
-// ----------------------------------------------------------------- smoothing
+// ----------------------------------------------------------------- smoothing (sparse levels)
 
-// Gauss-Seidel update of cells of one colour. mode 0: plain; mode 1: first
-// sweep from x = 0 (neighbours read as zero); mode 2: neighbour values include
-// the coarse correction xc[parent] (prolongation fused into the first post sweep).
-template <typename T>
-__global__ void k_smooth(GridView g, LevelDesc L, LevelPtrs<T> lp, const float* b, int color, int mode,
-                         LevelDesc Cd, const T* xc, const int* done) {
+// Gauss-Seidel update of one colour on a sparse level (2^LS cells per block
+// axis). 256 threads per CTA, each owning one cell of the colour; a CTA covers
+// 256/(S^3/2) blocks. MODE 0: plain; 1: first sweep from x = 0 (no neighbour
+// reads); 2: neighbour values include the coarse correction (prolongation
+// fused into the first post-smoothing sweep).
+template <typename T, int LS, int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_smooth_sparse(GridView g, LevelPtrs<T> lp, const float* __restrict__ b, int color, const T* __restrict__ xc,
+                    int cdx, int cdy, const int* done) {
   if (*done) return;
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= L.count) return;
-  if (!lp.fluid[i]) return;
-  const CellPos p = cell_pos(L, i);
-  if (cell_parity(g, L, p) != color) return;
+  constexpr int S = 1 << LS, S3 = S * S * S, HALF = S3 / 2, BPC = kThreads / HALF;
+  const int t = threadIdx.x;
+  const int blk = blockIdx.x * BPC + t / HALF;
+  if (blk >= g.nb) return;
+  const int j = t % HALF;
+  const int z = j / (S * S / 2), rr = j % (S * S / 2), y = rr / (S / 2), xh = rr % (S / 2);
+  const int x = 2 * xh + ((y + z + color) & 1);
+  const int l = (z * S + y) * S + x;
+  const int i = blk * S3 + l;
+  unsigned m = 0;
+  if (LS == 3) {
+    m = lp.mask[i];
+    if (!(m & 64u)) return;
+  } else if (!lp.fluid[i]) {
+    return;
+  }
   float s = b[i];
-  if (mode != 1) {
+  if (MODE != 1) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
 #pragma unroll
       for (int dir = -1; dir <= 1; dir += 2) {
-        const long long j = level_nbr(g, L, p, a, dir);
-        if (j < 0) continue;
-        const float k = dir < 0 ? ld(&lp.k[a][i]) : ld(&lp.k[a][j]);
-        if (k == 0.0f) continue;
-        float xj = ld(&lp.x[j]);
-        if (mode == 2) xj += ld(&xc[parent_of(g, L, Cd, j)]);
+        float k;
+        if (LS == 3) {
+          if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
+          k = 1.0f;
+        }
+        const int jn = nbr_s<LS>(g, blk, l, a, dir);
+        if (jn < 0) continue;
+        if (LS != 3) {
+          k = dir < 0 ? ld(&lp.k[a][i]) : ld(&lp.k[a][jn]);
+          if (k == 0.0f) continue;
+        }
+        float xj = ld(&lp.x[jn]);
+        if (MODE == 2) xj += ld(&xc[parent_s<LS>(g, jn, cdx, cdy)]);
         s = fmaf(k, xj, s);
       }
     }
@@ -314,57 +368,146 @@ __global__ void k_smooth(GridView g, LevelDesc L, LevelPtrs<T> lp, const float* 
   st_T(&lp.x[i], s / lp.diag[i]);
 }
 
-// Residual of the fine level restricted (summed) into the coarse RHS.
-template <typename T>
-__global__ void k_residual_restrict(GridView g, LevelDesc F, LevelPtrs<T> fp, const float* fb, LevelDesc C,
-                                    LevelPtrs<T> cp, float* cb, const int* done) {
+// Residual of a sparse level summed into the next level's RHS. 512 threads per
+// CTA, one per fine cell; 64 threads then sum 2x2x2 children in a fixed order.
+template <typename T, int LS>
+__global__ void __launch_bounds__(512)
+    k_restrict_sparse(GridView g, LevelPtrs<T> fp, const float* __restrict__ fb, float* cb, int cdx, int cdy,
+                      const int* done) {
   if (*done) return;
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= C.count) return;
-  float sum = 0.0f;
-  if (cp.fluid[i]) {
-    const CellPos p = cell_pos(C, i);
-    long long child[8];
-    int nchild = 0;
-    if (C.sparse) {
-      const int S = F.S;
-      for (int dz = 0; dz < 2; ++dz)
-        for (int dy = 0; dy < 2; ++dy)
-          for (int dx = 0; dx < 2; ++dx)
-            child[nchild++] = (long long)p.b * S * S * S + ((2 * p.z + dz) * S + 2 * p.y + dy) * S + 2 * p.x + dx;
-    } else if (F.sparse) {
-      const int o = g.table[((long long)p.z * g.bdim[1] + p.y) * g.bdim[0] + p.x];
-      if (o >= 0)
-        for (int c = 0; c < 8; ++c) child[nchild++] = (long long)o * 8 + c;
+  constexpr int S = 1 << LS, S3 = S * S * S, BPC = 512 / S3;
+  __shared__ float r[512];
+  const int t = threadIdx.x;
+  const int blk = blockIdx.x * BPC + t / S3;
+  const int l = t % S3;
+  float res = 0.0f;
+  if (blk < g.nb) {
+    const int i = blk * S3 + l;
+    unsigned m = 0;
+    bool fluid;
+    if (LS == 3) {
+      m = fp.mask[i];
+      fluid = (m & 64u) != 0;
     } else {
-      for (int dz = 0; dz < 2; ++dz)
-        for (int dy = 0; dy < 2; ++dy)
-          for (int dx = 0; dx < 2; ++dx) {
-            const int x = 2 * p.x + dx, y = 2 * p.y + dy, z = 2 * p.z + dz;
-            if (x >= F.dim[0] || y >= F.dim[1] || z >= F.dim[2]) continue;
-            child[nchild++] = ((long long)z * F.dim[1] + y) * F.dim[0] + x;
-          }
+      fluid = fp.fluid[i] != 0;
     }
-    for (int c = 0; c < nchild; ++c) {
-      const long long id = child[c];
-      if (!fp.fluid[id]) continue;
-      const CellPos q = cell_pos(F, id);
-      const float xi = ld(&fp.x[id]);
-      float ax = fp.diag[id] * xi;
+    if (fluid) {
+      float ax = fp.diag[i] * ld(&fp.x[i]);
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
 #pragma unroll
         for (int dir = -1; dir <= 1; dir += 2) {
-          const long long j = level_nbr(g, F, q, a, dir);
-          if (j < 0) continue;
-          const float k = dir < 0 ? ld(&fp.k[a][id]) : ld(&fp.k[a][j]);
-          if (k == 0.0f) continue;
-          ax = fmaf(-k, ld(&fp.x[j]), ax);
+          float k;
+          if (LS == 3) {
+            if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
+            k = 1.0f;
+          }
+          const int jn = nbr_s<LS>(g, blk, l, a, dir);
+          if (jn < 0) continue;
+          if (LS != 3) {
+            k = dir < 0 ? ld(&fp.k[a][i]) : ld(&fp.k[a][jn]);
+            if (k == 0.0f) continue;
+          }
+          ax = fmaf(-k, ld(&fp.x[jn]), ax);
         }
       }
-      sum += fb[id] - ax;
+      res = fb[i] - ax;
     }
   }
+  r[t] = res;
+  __syncthreads();
+  if (t < 64) {
+    constexpr int SC = S / 2, SC3 = SC * SC * SC;
+    const int bl = t / SC3, cl = t % SC3;
+    const int cblk = blockIdx.x * BPC + bl;
+    if (cblk < g.nb) {
+      const int cx = cl % SC, cy = (cl / SC) % SC, cz = cl / (SC * SC);
+      float sum = 0.0f;
+#pragma unroll
+      for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+          for (int dx = 0; dx < 2; ++dx) sum += r[bl * S3 + ((2 * cz + dz) * S + 2 * cy + dy) * S + 2 * cx + dx];
+      int out;
+      if (LS > 1) {
+        out = cblk * SC3 + cl;
+      } else {
+        out = ((g.coord[3 * cblk + 2] - g.blo[2]) * cdy + (g.coord[3 * cblk + 1] - g.blo[1])) * cdx +
+              (g.coord[3 * cblk] - g.blo[0]);
+      }
+      cb[out] = sum;
+    }
+  }
+}
+
+// ----------------------------------------------------------------- dense levels (>= 3)
+
+__device__ __forceinline__ int dense_id(const LevelDesc& L, int x, int y, int z) {
+  return (z * L.dim[1] + y) * L.dim[0] + x;
+}
+
+template <typename T, int MODE>
+__global__ void k_smooth_dense(LevelDesc L, LevelPtrs<T> lp, const float* __restrict__ b, int color, LevelDesc C,
+                               const T* __restrict__ xc, const int* done) {
+  if (*done) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L.count) return;
+  const int x = i % L.dim[0], y = (i / L.dim[0]) % L.dim[1], z = i / (L.dim[0] * L.dim[1]);
+  if (((x + y + z + L.parity) & 1) != color || !lp.fluid[i]) return;
+  float s = b[i];
+  if (MODE != 1) {
+    const int c[3] = {x, y, z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+      for (int dir = -1; dir <= 1; dir += 2) {
+        int n[3] = {c[0], c[1], c[2]};
+        n[a] += dir;
+        if (n[a] < 0 || n[a] >= L.dim[a]) continue;
+        const int jn = dense_id(L, n[0], n[1], n[2]);
+        const float k = dir < 0 ? ld(&lp.k[a][i]) : ld(&lp.k[a][jn]);
+        if (k == 0.0f) continue;
+        float xj = ld(&lp.x[jn]);
+        if (MODE == 2) xj += ld(&xc[dense_id(C, n[0] >> 1, n[1] >> 1, n[2] >> 1)]);
+        s = fmaf(k, xj, s);
+      }
+    }
+  }
+  st_T(&lp.x[i], s / lp.diag[i]);
+}
+
+template <typename T>
+__global__ void k_restrict_dense(LevelDesc F, LevelPtrs<T> fp, const float* __restrict__ fb, LevelDesc C, float* cb,
+                                 const int* done) {
+  if (*done) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C.count) return;
+  const int X = i % C.dim[0], Y = (i / C.dim[0]) % C.dim[1], Z = i / (C.dim[0] * C.dim[1]);
+  float sum = 0.0f;
+  for (int dz = 0; dz < 2; ++dz)
+    for (int dy = 0; dy < 2; ++dy)
+      for (int dx = 0; dx < 2; ++dx) {
+        const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
+        if (x >= F.dim[0] || y >= F.dim[1] || z >= F.dim[2]) continue;
+        const int id = dense_id(F, x, y, z);
+        if (!fp.fluid[id]) continue;
+        float ax = fp.diag[id] * ld(&fp.x[id]);
+        const int c[3] = {x, y, z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+          for (int dir = -1; dir <= 1; dir += 2) {
+            int n[3] = {c[0], c[1], c[2]};
+            n[a] += dir;
+            if (n[a] < 0 || n[a] >= F.dim[a]) continue;
+            const int jn = dense_id(F, n[0], n[1], n[2]);
+            const float k = dir < 0 ? ld(&fp.k[a][id]) : ld(&fp.k[a][jn]);
+            if (k != 0.0f) ax = fmaf(-k, ld(&fp.x[jn]), ax);
+          }
+        }
+        sum += fb[id] - ax;
+      }
   cb[i] = sum;
 }
 
@@ -413,7 +556,24 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(LevelDesc L, LevelPtrs<T>
   for (int i = threadIdx.x; i < n; i += blockDim.x) st_T(&lp.x[i], lp.fluid[i] ? x[i] : 0.0f);
 }
 
-// ----------------------------------------------------------------- CG kernels (level 0)
+// ----------------------------------------------------------------- CG kernels (level 0, grid-stride)
+
+// (A x)_i on level 0 from the neighbour mask: diag_i x_i - sum of fluid neighbours.
+template <typename T, typename V>
+__device__ __forceinline__ V apply0(const GridView& g, const LevelPtrs<T>& L0, unsigned m, int i, V xi,
+                                    const V* __restrict__ xv) {
+  const int b = i >> 9, l = i & 511;
+  V ax = (V)L0.diag[i] * xi;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+#pragma unroll
+    for (int dir = -1; dir <= 1; dir += 2) {
+      if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
+      ax -= xv[nbr_s<3>(g, b, l, a, dir)];
+    }
+  }
+  return ax;
+}
 
 // r64 = b' - A p64 (FP64); r = (float)r64; e = 0; ||r64||^2. The last block
 // decides whether to stop and arms the inner solve.
@@ -421,37 +581,20 @@ template <typename T>
 __global__ void k_residual64(GridView g, LevelPtrs<T> L0, const double* b64, const double* p64, float* r, float* e,
                              double* partial, SolverState* st) {
   __shared__ double red[kThreads / 32];
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long n = (long long)g.nb * kBlockCells;
+  const int n = g.nb * kBlockCells;
   double rr = 0.0;
-  if (i < n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned m = L0.mask[i];
     double res = 0.0;
-    if (L0.fluid[i]) {
-      const int b = (int)(i / kBlockCells), l = (int)(i % kBlockCells);
-      const int lx = l & 7, ly = (l >> 3) & 7, lz = l >> 6;
-      double ax = (double)L0.diag[i] * p64[i];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-#pragma unroll
-        for (int dir = -1; dir <= 1; dir += 2) {
-          const long long j = sparse_nbr(g, 8, b, lx, ly, lz, a, dir);
-          if (j < 0) continue;
-          const float k = dir < 0 ? ld(&L0.k[a][i]) : ld(&L0.k[a][j]);
-          if (k != 0.0f) ax -= (double)k * p64[j];
-        }
-      }
-      res = b64[i] - ax;
-    }
+    if (m & 64u) res = b64[i] - apply0<T, double>(g, L0, m, i, p64[i], p64);
     r[i] = (float)res;
     e[i] = 0.0f;
-    rr = res * res;
+    rr += res * res;
   }
   const double s = block_sum<kThreads>(rr, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
   if (last_block(st)) {
-    double t = 0.0;
-    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) t += partial[k];
-    t = block_sum<kThreads>(t, red);
+    const double t = finish_sum(partial, 1, 0, red);
     if (threadIdx.x == 0) {
       st->res64 = sqrt(t);
       const double target = st->target;
@@ -467,16 +610,15 @@ __global__ void k_residual64(GridView g, LevelPtrs<T> L0, const double* b64, con
 
 // z.r and z.r_prev -> beta (flexible Polak-Ribiere), rz.
 template <typename T>
-__global__ void k_dots(long long n, const T* z, const float* r, const float* r_prev, double* partial,
-                       SolverState* st) {
+__global__ void k_dots(int n, const T* __restrict__ z, const float* __restrict__ r, const float* __restrict__ r_prev,
+                       double* partial, SolverState* st) {
   if (st->done) return;
   __shared__ double red[kThreads / 32];
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double zr = 0.0, zp = 0.0;
-  if (i < n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double zi = (double)ld(&z[i]);
-    zr = zi * (double)r[i];
-    zp = zi * (double)r_prev[i];
+    zr += zi * (double)r[i];
+    zp += zi * (double)r_prev[i];
   }
   const double s0 = block_sum<kThreads>(zr, red);
   const double s1 = block_sum<kThreads>(zp, red);
@@ -485,13 +627,8 @@ __global__ void k_dots(long long n, const T* z, const float* r, const float* r_p
     partial[2 * blockIdx.x + 1] = s1;
   }
   if (last_block(st)) {
-    double t0 = 0.0, t1 = 0.0;
-    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
-      t0 += partial[2 * k];
-      t1 += partial[2 * k + 1];
-    }
-    t0 = block_sum<kThreads>(t0, red);
-    t1 = block_sum<kThreads>(t1, red);
+    const double t0 = finish_sum(partial, 2, 0, red);
+    const double t1 = finish_sum(partial, 2, 1, red);
     if (threadIdx.x == 0) {
       if (!(t0 > 0.0) || !isfinite(t0)) {
         st->status = kAborted;
@@ -506,36 +643,32 @@ __global__ void k_dots(long long n, const T* z, const float* r, const float* r_p
 
 // d = z + beta d_old; q = A d (neighbours' d formed on the fly); d.q -> alpha.
 template <typename T>
-__global__ void k_direction(GridView g, LevelPtrs<T> L0, const T* z, const float* d_old, float* d_new, float* q,
-                            double* partial, SolverState* st) {
+__global__ void k_direction(GridView g, LevelPtrs<T> L0, const T* __restrict__ z, const float* __restrict__ d_old,
+                            float* __restrict__ d_new, float* __restrict__ q, double* partial, SolverState* st) {
   if (st->done) return;
   __shared__ double red[kThreads / 32];
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long n = (long long)g.nb * kBlockCells;
+  const int n = g.nb * kBlockCells;
   const float beta = (float)st->beta;
   const bool first = st->inner_iter == 0;
   double dq = 0.0;
-  if (i < n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned m = L0.mask[i];
     float di = 0.0f, qi = 0.0f;
-    if (L0.fluid[i]) {
+    if (m & 64u) {
       di = first ? ld(&z[i]) : fmaf(beta, d_old[i], ld(&z[i]));
-      const int b = (int)(i / kBlockCells), l = (int)(i % kBlockCells);
-      const int lx = l & 7, ly = (l >> 3) & 7, lz = l >> 6;
+      const int b = i >> 9, l = i & 511;
       float ax = L0.diag[i] * di;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
 #pragma unroll
         for (int dir = -1; dir <= 1; dir += 2) {
-          const long long j = sparse_nbr(g, 8, b, lx, ly, lz, a, dir);
-          if (j < 0) continue;
-          const float k = dir < 0 ? ld(&L0.k[a][i]) : ld(&L0.k[a][j]);
-          if (k == 0.0f) continue;
-          const float dj = first ? ld(&z[j]) : fmaf(beta, d_old[j], ld(&z[j]));
-          ax = fmaf(-k, dj, ax);
+          if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
+          const int j = nbr_s<3>(g, b, l, a, dir);
+          ax -= first ? ld(&z[j]) : fmaf(beta, d_old[j], ld(&z[j]));
         }
       }
       qi = ax;
-      dq = (double)di * (double)qi;
+      dq += (double)di * (double)qi;
     }
     d_new[i] = di;
     q[i] = qi;
@@ -543,9 +676,7 @@ __global__ void k_direction(GridView g, LevelPtrs<T> L0, const T* z, const float
   const double s = block_sum<kThreads>(dq, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
   if (last_block(st)) {
-    double t = 0.0;
-    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) t += partial[k];
-    t = block_sum<kThreads>(t, red);
+    const double t = finish_sum(partial, 1, 0, red);
     if (threadIdx.x == 0) {
       if (!(t > 0.0) || !isfinite(t)) {
         st->status = kAborted;
@@ -559,25 +690,22 @@ __global__ void k_direction(GridView g, LevelPtrs<T> L0, const T* z, const float
 }
 
 // e += alpha d; r_next = r - alpha q; ||r_next||^2 -> stop test.
-__global__ void k_update(long long n, const float* d, const float* q, const float* r, float* r_next, float* e,
-                         double* partial, SolverState* st) {
+__global__ void k_update(int n, const float* __restrict__ d, const float* __restrict__ q, const float* __restrict__ r,
+                         float* __restrict__ r_next, float* __restrict__ e, double* partial, SolverState* st) {
   if (st->done) return;
   __shared__ double red[kThreads / 32];
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const float alpha = (float)st->alpha;
   double rr = 0.0;
-  if (i < n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     e[i] = fmaf(alpha, d[i], e[i]);
     const float rn = fmaf(-alpha, q[i], r[i]);
     r_next[i] = rn;
-    rr = (double)rn * (double)rn;
+    rr += (double)rn * (double)rn;
   }
   const double s = block_sum<kThreads>(rr, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
   if (last_block(st)) {
-    double t = 0.0;
-    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) t += partial[k];
-    t = block_sum<kThreads>(t, red);
+    const double t = finish_sum(partial, 1, 0, red);
     if (threadIdx.x == 0) {
       st->rr = t;
       st->inner_iter += 1;
@@ -589,24 +717,22 @@ __global__ void k_update(long long n, const float* d, const float* q, const floa
   }
 }
 
-__global__ void k_accumulate(long long n, const float* e, double* p64) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) p64[i] += (double)e[i];
+__global__ void k_accumulate(int n, const float* e, double* p64) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p64[i] += (double)e[i];
 }
 
-// Corrected face velocities and the post-projection divergence in FP64.
-// u_new = u_pred + scale (p_tail - p_head) on faces with a fluid side and no
-// solid side (air pressure 0); other faces keep u_pred.
+// Corrected face velocities: u_new = u_pred + scale (p_tail - p_head) on faces
+// with a fluid side and no solid side (air pressure 0); other faces keep u_pred.
 __global__ void k_correct_faces(GridView g, const unsigned char* type, const double* p64, const float* up0,
                                 const float* up1, const float* up2, float* un0, float* un1, float* un2,
                                 double scale) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)g.nb * 3 * kBlockCells) return;
-  const int b = (int)(i / (3 * kBlockCells));
-  const int a = (int)((i / kBlockCells) % 3);
-  const int l = (int)(i % kBlockCells);
-  const long long head = (long long)b * kBlockCells + l;
-  const long long tail = sparse_nbr(g, 8, b, l & 7, (l >> 3) & 7, l >> 6, a, -1);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nb * 3 * kBlockCells) return;
+  const int b = i / (3 * kBlockCells);
+  const int a = (i >> 9) % 3;
+  const int l = i & 511;
+  const int head = b * kBlockCells + l;
+  const int tail = nbr_s<3>(g, b, l, a, -1);
   const int th = type[head], tt = nbr_type(type, tail);
   const float* up = a == 0 ? up0 : (a == 1 ? up1 : up2);
   float* un = a == 0 ? un0 : (a == 1 ? un1 : un2);
@@ -619,42 +745,37 @@ __global__ void k_correct_faces(GridView g, const unsigned char* type, const dou
   un[head] = (float)u;
 }
 
-// Diagnostics over fluid cells: max |r64| and max |divergence| of the corrected
-// FP64 velocities (pred + scale * dp, per face), both in device units.
-__global__ void k_diagnostics(GridView g, const unsigned char* type, const double* p64, const double* b64,
-                              const float* L0diag, const float* up0, const float* up1, const float* up2,
-                              double scale, double* partial, SolverState* st) {
+// Post-projection divergence over fluid cells from the FP64 correction of the
+// FP32 predicted velocities: l2 and max, in m/s summed over a cell's faces.
+__global__ void k_diagnostics(GridView g, const unsigned char* type, const double* p64, const float* up0,
+                              const float* up1, const float* up2, double scale, double* partial, SolverState* st) {
   __shared__ double red[kThreads / 32];
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long n = (long long)g.nb * kBlockCells;
-  double maxdiv = 0.0, sumsq_div = 0.0;
-  if (i < n && type[i] == 1) {
-    const int b = (int)(i / kBlockCells), l = (int)(i % kBlockCells);
-    const int lx = l & 7, ly = (l >> 3) & 7, lz = l >> 6;
-    const float* up[3] = {up0, up1, up2};
+  __shared__ double mx[kThreads / 32];
+  const int n = g.nb * kBlockCells;
+  const float* up[3] = {up0, up1, up2};
+  double maxdiv = 0.0, sumsq = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (type[i] != 1) continue;
+    const int b = i >> 9, l = i & 511;
     double div = 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const long long lo = sparse_nbr(g, 8, b, lx, ly, lz, a, -1);
-      const long long hi = sparse_nbr(g, 8, b, lx, ly, lz, a, +1);
+      const int lo = nbr_s<3>(g, b, l, a, -1);
+      const int hi = nbr_s<3>(g, b, l, a, +1);
       const int tlo = nbr_type(type, lo), thi = nbr_type(type, hi);
       double ulo = (double)up[a][i], uhi = hi >= 0 ? (double)up[a][hi] : 0.0;
       if (tlo != 0) ulo += scale * ((tlo == 1 ? p64[lo] : 0.0) - p64[i]);
       if (thi != 0) uhi += scale * (p64[i] - (thi == 1 ? p64[hi] : 0.0));
       div += uhi - ulo;
     }
-    maxdiv = fabs(div);
-    sumsq_div = div * div;
+    maxdiv = fmax(maxdiv, fabs(div));
+    sumsq += div * div;
   }
-  (void)b64;
-  (void)L0diag;
-  // max via warp/block: use sum for L2 and a separate max reduction
   double m = maxdiv;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  __shared__ double mx[kThreads / 32];
   if ((threadIdx.x & 31) == 0) mx[threadIdx.x >> 5] = m;
-  const double s = block_sum<kThreads>(sumsq_div, red);
+  const double s = block_sum<kThreads>(sumsq, red);
   __syncthreads();
   if (threadIdx.x == 0) {
     double mm = 0.0;
@@ -663,14 +784,19 @@ __global__ void k_diagnostics(GridView g, const unsigned char* type, const doubl
     partial[2 * blockIdx.x + 1] = mm;
   }
   if (last_block(st)) {
+    const double t = finish_sum(partial, 2, 0, red);
+    double mm = 0.0;
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) mm = fmax(mm, partial[2 * k + 1]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) mx[threadIdx.x >> 5] = mm;
+    __syncthreads();
     if (threadIdx.x == 0) {
-      double t = 0.0, mm = 0.0;
-      for (unsigned k = 0; k < gridDim.x; ++k) {
-        t += partial[2 * k];
-        mm = fmax(mm, partial[2 * k + 1]);
-      }
+      double all = 0.0;
+      for (int w = 0; w < kThreads / 32; ++w) all = fmax(all, mx[w]);
       st->div_l2 = sqrt(t);
-      st->div_max = mm;
+      st->div_max = all;
       st->ticket = 0;
     }
   }
@@ -678,62 +804,117 @@ __global__ void k_diagnostics(GridView g, const unsigned char* type, const doubl
 
 // ----------------------------------------------------------------- host orchestration
 
+template <typename T, int LS>
+static void smooth_sparse(const GridView& g, const MgHierarchy<T>& H, int l, const float* bl, int color, int mode,
+                          const int* done, cudaStream_t s) {
+  constexpr int HALF = (1 << (3 * LS)) / 2, BPC = kThreads / HALF;
+  const unsigned grid = (unsigned)((g.nb + BPC - 1) / BPC);
+  const LevelDesc& C = H.desc[l + 1];
+  const T* xc = H.ptr[l + 1].x;
+  ++g_kernel_launches;
+  if (mode == 1)
+    k_smooth_sparse<T, LS, 1><<<grid, kThreads, 0, s>>>(g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
+  else if (mode == 2)
+    k_smooth_sparse<T, LS, 2><<<grid, kThreads, 0, s>>>(g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
+  else
+    k_smooth_sparse<T, LS, 0><<<grid, kThreads, 0, s>>>(g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
+}
+
+template <typename T>
+static void smooth(const GridView& g, const MgHierarchy<T>& H, int l, const float* bl, int color, int mode,
+                   const int* done, cudaStream_t s) {
+  if (l == 0) return smooth_sparse<T, 3>(g, H, l, bl, color, mode, done, s);
+  if (l == 1) return smooth_sparse<T, 2>(g, H, l, bl, color, mode, done, s);
+  if (l == 2) return smooth_sparse<T, 1>(g, H, l, bl, color, mode, done, s);
+  const LevelDesc& D = H.desc[l];
+  const LevelDesc& C = H.desc[l + 1 < H.levels ? l + 1 : l];
+  const unsigned grid = blocks_for(D.count);
+  ++g_kernel_launches;
+  if (mode == 1)
+    k_smooth_dense<T, 1><<<grid, kThreads, 0, s>>>(D, H.ptr[l], bl, color, C, nullptr, done);
+  else if (mode == 2)
+    k_smooth_dense<T, 2><<<grid, kThreads, 0, s>>>(D, H.ptr[l], bl, color, C, H.ptr[l + 1].x, done);
+  else
+    k_smooth_dense<T, 0><<<grid, kThreads, 0, s>>>(D, H.ptr[l], bl, color, C, nullptr, done);
+}
+
+template <typename T>
+static void restrict_level(const GridView& g, const MgHierarchy<T>& H, int l, const float* bl, const int* done,
+                           cudaStream_t s) {
+  const LevelDesc& C = H.desc[l + 1];
+  ++g_kernel_launches;
+  if (l < 3) {
+    const int S3 = 1 << (3 * (3 - l));
+    const int bpc = 512 / S3;
+    const unsigned grid = (unsigned)((g.nb + bpc - 1) / bpc);
+    if (l == 0)
+      k_restrict_sparse<T, 3><<<grid, 512, 0, s>>>(g, H.ptr[0], bl, H.b[1], C.dim[0], C.dim[1], done);
+    else if (l == 1)
+      k_restrict_sparse<T, 2><<<grid, 512, 0, s>>>(g, H.ptr[1], bl, H.b[2], C.dim[0], C.dim[1], done);
+    else
+      k_restrict_sparse<T, 1><<<grid, 512, 0, s>>>(g, H.ptr[2], bl, H.b[3], C.dim[0], C.dim[1], done);
+    return;
+  }
+  k_restrict_dense<T><<<blocks_for(C.count), kThreads, 0, s>>>(H.desc[l], H.ptr[l], bl, C, H.b[l + 1], done);
+}
+
 template <typename T>
 static void vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r0, const MgOptions& opt,
                    const int* done, cudaStream_t s) {
   const int L = H.levels;
-  const float* b = r0;
   for (int l = 0; l < L - 1; ++l) {
-    const LevelDesc& D = H.desc[l];
-    const unsigned nblk = blocks_for(D.count);
     const float* bl = l == 0 ? r0 : H.b[l];
-    k_smooth<T><<<nblk, kThreads, 0, s>>>(g, D, H.ptr[l], bl, 0, 1, D, nullptr, done);
-    k_smooth<T><<<nblk, kThreads, 0, s>>>(g, D, H.ptr[l], bl, 1, 0, D, nullptr, done);
+    smooth<T>(g, H, l, bl, 0, 1, done, s);
+    smooth<T>(g, H, l, bl, 1, 0, done, s);
     for (int sw = 1; sw < opt.pre; ++sw) {
-      k_smooth<T><<<nblk, kThreads, 0, s>>>(g, D, H.ptr[l], bl, 0, 0, D, nullptr, done);
-      k_smooth<T><<<nblk, kThreads, 0, s>>>(g, D, H.ptr[l], bl, 1, 0, D, nullptr, done);
+      smooth<T>(g, H, l, bl, 0, 0, done, s);
+      smooth<T>(g, H, l, bl, 1, 0, done, s);
     }
-    const LevelDesc& C = H.desc[l + 1];
-    k_residual_restrict<T><<<blocks_for(C.count), kThreads, 0, s>>>(g, D, H.ptr[l], bl, C, H.ptr[l + 1],
-                                                                     H.b[l + 1], done);
+    restrict_level<T>(g, H, l, bl, done, s);
   }
   {
     const LevelDesc& C = H.desc[L - 1];
     const size_t smem = (size_t)C.count * 6 * sizeof(float);
     static bool configured = false;
     if (!configured) {
-      cudaFuncSetAttribute(k_coarse_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 6 * (int)sizeof(float));
+      cudaFuncSetAttribute(k_coarse_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           8192 * 6 * (int)sizeof(float));
       configured = true;
     }
-    k_coarse_solve<T><<<1, 1024, smem, s>>>(C, H.ptr[L - 1], H.b[L - 1], opt.coarse_sweeps, done);
+    const int threads = C.count <= 1024 ? (int)((C.count + 31) / 32 * 32) : 1024;
+    ++g_kernel_launches;
+    k_coarse_solve<T><<<1, threads, smem, s>>>(C, H.ptr[L - 1], H.b[L - 1], opt.coarse_sweeps, done);
   }
   for (int l = L - 2; l >= 0; --l) {
-    const LevelDesc& D = H.desc[l];
-    const unsigned nblk = blocks_for(D.count);
     const float* bl = l == 0 ? r0 : H.b[l];
-    k_smooth<T><<<nblk, kThreads, 0, s>>>(g, D, H.ptr[l], bl, 1, 2, H.desc[l + 1], H.ptr[l + 1].x, done);
-    k_smooth<T><<<nblk, kThreads, 0, s>>>(g, D, H.ptr[l], bl, 0, 0, D, nullptr, done);
+    smooth<T>(g, H, l, bl, 1, 2, done, s);
+    smooth<T>(g, H, l, bl, 0, 0, done, s);
     for (int sw = 1; sw < opt.post; ++sw) {
-      k_smooth<T><<<nblk, kThreads, 0, s>>>(g, D, H.ptr[l], bl, 1, 0, D, nullptr, done);
-      k_smooth<T><<<nblk, kThreads, 0, s>>>(g, D, H.ptr[l], bl, 0, 0, D, nullptr, done);
+      smooth<T>(g, H, l, bl, 1, 0, done, s);
+      smooth<T>(g, H, l, bl, 0, 0, done, s);
     }
   }
-  (void)b;
 }
 
 template <typename T>
 cudaError_t launch_pressure_setup(const GridView& g, const int* cell_start, unsigned char* type,
                                   const float* const u_pred[3], double rhs_scale, MgHierarchy<T>& H, double* b64,
                                   double* p64, double* partial, SolverState* st, cudaStream_t s) {
-  const long long n = (long long)g.nb * kBlockCells;
+  const int n = g.nb * kBlockCells;
+  ++g_kernel_launches;
   k_classify<<<blocks_for(n), kThreads, 0, s>>>(g, cell_start, type);
-  k_setup_level0<T><<<blocks_for(n), kThreads, 0, s>>>(g, type, u_pred[0], u_pred[1], u_pred[2], rhs_scale,
-                                                       H.ptr[0], b64, p64, partial, st);
-  for (int l = 1; l < H.levels; ++l)
+  ++g_kernel_launches;
+  k_setup_level0<T><<<reduce_grid(n), kThreads, 0, s>>>(g, type, u_pred[0], u_pred[1], u_pred[2], rhs_scale,
+                                                         H.ptr[0], b64, p64, partial, st);
+  for (int l = 1; l < H.levels; ++l) {
+    ++g_kernel_launches;
     k_coarsen<T><<<blocks_for(H.desc[l].count), kThreads, 0, s>>>(g, H.desc[l - 1], H.ptr[l - 1], H.desc[l],
                                                                    H.ptr[l]);
-  for (int l = 0; l < H.levels; ++l)
+  }
+  for (int l = 1; l < H.levels; ++l) {
+    ++g_kernel_launches;
     k_level_diag<T><<<blocks_for(H.desc[l].count), kThreads, 0, s>>>(g, H.desc[l], H.ptr[l]);
+  }
   return cudaGetLastError();
 }
 
@@ -747,8 +928,9 @@ cudaError_t launch_apply_vcycle(const GridView& g, const MgHierarchy<T>& H, cons
 template <typename T>
 cudaError_t launch_residual64(const GridView& g, const MgHierarchy<T>& H, const double* b64, const double* p64,
                               float* r, float* e, double* partial, SolverState* st, cudaStream_t s) {
-  const long long n = (long long)g.nb * kBlockCells;
-  k_residual64<T><<<blocks_for(n), kThreads, 0, s>>>(g, H.ptr[0], b64, p64, r, e, partial, st);
+  const int n = g.nb * kBlockCells;
+  ++g_kernel_launches;
+  k_residual64<T><<<reduce_grid(n), kThreads, 0, s>>>(g, H.ptr[0], b64, p64, r, e, partial, st);
   return cudaGetLastError();
 }
 
@@ -756,30 +938,34 @@ template <typename T>
 cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, const MgOptions& opt, float* r_cur,
                                  float* r_prev, float* d_old, float* d_new, float* q, float* e, double* partial,
                                  SolverState* st, const int* done, cudaStream_t s) {
-  const long long n = (long long)g.nb * kBlockCells;
+  const int n = g.nb * kBlockCells;
   vcycle<T>(g, H, r_cur, opt, done, s);
   const T* z = H.ptr[0].x;
-  k_dots<T><<<blocks_for(n), kThreads, 0, s>>>(n, z, r_cur, r_prev, partial, st);
-  k_direction<T><<<blocks_for(n), kThreads, 0, s>>>(g, H.ptr[0], z, d_old, d_new, q, partial, st);
-  k_update<<<blocks_for(n), kThreads, 0, s>>>(n, d_new, q, r_cur, r_prev, e, partial, st);
+  const unsigned grid = reduce_grid(n);
+  g_kernel_launches += 3;
+  k_dots<T><<<grid, kThreads, 0, s>>>(n, z, r_cur, r_prev, partial, st);
+  k_direction<T><<<grid, kThreads, 0, s>>>(g, H.ptr[0], z, d_old, d_new, q, partial, st);
+  k_update<<<grid, kThreads, 0, s>>>(n, d_new, q, r_cur, r_prev, e, partial, st);
   return cudaGetLastError();
 }
 
 cudaError_t launch_accumulate(const GridView& g, const float* e, double* p64, cudaStream_t s) {
-  const long long n = (long long)g.nb * kBlockCells;
-  k_accumulate<<<blocks_for(n), kThreads, 0, s>>>(n, e, p64);
+  const int n = g.nb * kBlockCells;
+  ++g_kernel_launches;
+  k_accumulate<<<reduce_grid(n), kThreads, 0, s>>>(n, e, p64);
   return cudaGetLastError();
 }
 
 cudaError_t launch_correct_faces(const GridView& g, const unsigned char* type, const double* p64,
                                  const float* const u_pred[3], float* const u_new[3], double scale,
                                  double* partial, SolverState* st, cudaStream_t s) {
-  const long long nf = (long long)g.nb * 3 * kBlockCells;
+  const int nf = g.nb * 3 * kBlockCells;
+  g_kernel_launches += 2;
   k_correct_faces<<<blocks_for(nf), kThreads, 0, s>>>(g, type, p64, u_pred[0], u_pred[1], u_pred[2], u_new[0],
                                                       u_new[1], u_new[2], scale);
-  const long long n = (long long)g.nb * kBlockCells;
-  k_diagnostics<<<blocks_for(n), kThreads, 0, s>>>(g, type, p64, nullptr, nullptr, u_pred[0], u_pred[1], u_pred[2],
-                                                   scale, partial, st);
+  const int n = g.nb * kBlockCells;
+  k_diagnostics<<<reduce_grid(n), kThreads, 0, s>>>(g, type, p64, u_pred[0], u_pred[1], u_pred[2], scale, partial,
+                                                    st);
   return cudaGetLastError();
 }
 

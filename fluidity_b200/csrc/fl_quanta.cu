@@ -36,6 +36,7 @@ __global__ void k_deposit_quanta(GridView g, const double* parts, unsigned long 
                                  unsigned long long* pq0, unsigned long long* pq1, unsigned long long* pq2,
                                  DeviceReport* rep) {
   const unsigned long long p = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  if (p == 0) rep->compiled_architecture = compiled_arch();
   if (p >= n) return;
   const double* q = parts + 19 * p;
   const double mass = q[6];
@@ -103,6 +104,7 @@ cudaError_t launch_deposit_quanta(const GridView& g, const double* parts, unsign
   prm.mass_per_quantum = mass_per_quantum;
   prm.momentum_per_quantum = momentum_per_quantum;
   prm.limit = limit;
+  ++g_kernel_launches;
   k_deposit_quanta<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(g, parts, n, prm, mq[0], mq[1], mq[2], pq[0], pq[1],
                                                                 pq[2], rep);
   return cudaGetLastError();

@@ -86,11 +86,11 @@ typedef struct {
 } fl_particles;
 
 typedef struct {
-  float dt;            /* s */
-  float particle_mass; /* kg, used when fl_particles.mass is NULL */
-  float gravity[3];    /* m/s^2 */
-  float min_face_mass; /* kg; faces at or below it are low-mass (velocity 0) */
-  float density;       /* kg/m^3 for the pressure conductance */
+  double dt;            /* s */
+  double particle_mass; /* kg, used when fl_particles.mass is NULL */
+  double gravity[3];    /* m/s^2 */
+  double min_face_mass; /* kg; faces at or below it are low-mass (velocity 0) */
+  double density;       /* kg/m^3 for the pressure conductance */
 } fl_transfer_params;
 
 typedef struct {
@@ -173,6 +173,14 @@ int fl_g2p(fl_context* ctx, fl_particles* sorted, const float* const u_new[3], c
  * topology -> sort -> P2G (+normalize, gravity, walls) -> pressure -> G2P (+advect). */
 int fl_step(fl_context* ctx, const fl_transfer_params* params, const fl_pressure_options* options,
             fl_pressure_diagnostics* diagnostics, void* stream, fl_report* report);
+
+/* CUDA-event durations of the last fl_step's phases, ms:
+ * [0] topology + sort, [1] P2G (tile + merge kernels), [2] pressure, [3] G2P. */
+int fl_step_timings(fl_context* ctx, float* ms);
+
+/* Host-side counts of kernels launched by this library since load: its own
+ * kernels, and device-wide CUB algorithm invocations (radix sort, scans). */
+int fl_kernel_launches(unsigned long long* own, unsigned long long* library);
 
 /* Context-resident particle state and buffers (device pointers). */
 int fl_upload_particles(fl_context* ctx, const float* host_soa, uint64_t count, void* stream);

@@ -893,150 +893,180 @@ int fo_step(const fo_box* b, const fo_step_params* prm, double* x, double* v, do
 
 /* ------------------------------------------------------------------------- */
 /* Geometric V-cycle restatement (no reference counterpart: the reference uses
- * aggregation AMG with weighted Jacobi). Mirrors the CUDA preconditioner:
- * level-l cells are 2^l-aggregates; a coarse cell is fluid if any child is
- * fluid, else air if any child is air, else solid; the level-l operator is
- * 2^l * (sum over non-solid neighbours of (x_i - x_j), x_j = 0 for air);
- * restriction sums the fluid children, prolongation injects. Cells outside the
- * box are solid. Red-black ordering uses the global level-l cell parity.     */
+ * aggregation AMG with weighted Jacobi). Mirrors the CUDA preconditioner.
+ * Level 0 (units of the full-face conductance): k = 1 on faces between two
+ * fluid cells, anchor = number of air neighbours (Dirichlet p = 0), solid
+ * neighbours contribute nothing. Level l+1 aggregates 2x2x2 cells: fluid if
+ * any child is fluid, anchor = (sum of child anchors)/2, the low-face
+ * coefficient = (sum of the four crossing fine coefficients)/2; diag = anchor
+ * + the six face coefficients. Red-black Gauss-Seidel (red = even global
+ * parity), `pre` sweeps red->black, restriction sums fluid-child residuals,
+ * piecewise-constant prolongation, `post` sweeps black->red; the coarsest level
+ * runs `coarse_sweeps` forward and `coarse_sweeps` backward sweeps from zero. */
 
 typedef struct {
   int64_t n[3];
-  uint8_t* type;
+  uint8_t* fluid;
+  double* k[3];
+  double* anchor;
+  double* diag;
   double* x;
   double* b;
 } mg_level;
 
-static inline uint8_t mg_type(const mg_level* L, int64_t i, int64_t j, int64_t k) {
-  if (i < 0 || j < 0 || k < 0 || i >= L->n[0] || j >= L->n[1] || k >= L->n[2]) return 0;
-  return L->type[(k * L->n[1] + j) * L->n[0] + i];
+static inline int64_t mg_id(const mg_level* L, int64_t i, int64_t j, int64_t k) {
+  if (i < 0 || j < 0 || k < 0 || i >= L->n[0] || j >= L->n[1] || k >= L->n[2]) return -1;
+  return (k * L->n[1] + j) * L->n[0] + i;
 }
 
-static void mg_sweep(mg_level* L, double scale, int color, int64_t parity_offset) {
-  static const int off[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+/* sum over the 6 faces of k_f * x_j for fluid neighbours */
+static double mg_offdiag(const mg_level* L, int64_t i, int64_t j, int64_t k, const double* x) {
+  const int64_t id = mg_id(L, i, j, k);
+  double s = 0.0;
+  const int64_t c[3] = {i, j, k};
+  for (int a = 0; a < 3; ++a) {
+    int64_t lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[0], c[1], c[2]};
+    lo[a] -= 1;
+    hi[a] += 1;
+    const int64_t jl = mg_id(L, lo[0], lo[1], lo[2]), jh = mg_id(L, hi[0], hi[1], hi[2]);
+    if (jl >= 0 && L->k[a][id] != 0.0) s += L->k[a][id] * x[jl];
+    if (jh >= 0 && L->k[a][jh] != 0.0) s += L->k[a][jh] * x[jh];
+  }
+  return s;
+}
+
+static void mg_sweep(mg_level* L, int color, int first) {
   for (int64_t k = 0; k < L->n[2]; ++k)
     for (int64_t j = 0; j < L->n[1]; ++j)
       for (int64_t i = 0; i < L->n[0]; ++i) {
-        if (((i + j + k + parity_offset) & 1) != color) continue;
-        const int64_t id = (k * L->n[1] + j) * L->n[0] + i;
-        if (L->type[id] != 1) continue;
-        double sum = L->b[id];
-        int cnt = 0;
-        for (int q = 0; q < 6; ++q) {
-          const int64_t ii = i + off[q][0], jj = j + off[q][1], kk = k + off[q][2];
-          const uint8_t t = mg_type(L, ii, jj, kk);
-          if (t == 0) continue;
-          ++cnt;
-          if (t == 1) sum += scale * L->x[(kk * L->n[1] + jj) * L->n[0] + ii];
-        }
-        L->x[id] = cnt ? sum / (scale * cnt) : 0.0;
+        if (((i + j + k) & 1) != color) continue;
+        const int64_t id = mg_id(L, i, j, k);
+        if (!L->fluid[id]) continue;
+        const double s = L->b[id] + (first ? 0.0 : mg_offdiag(L, i, j, k, L->x));
+        L->x[id] = s / L->diag[id];
       }
 }
 
-static void mg_residual(const mg_level* L, double scale, double* r) {
-  static const int off[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
-  for (int64_t k = 0; k < L->n[2]; ++k)
-    for (int64_t j = 0; j < L->n[1]; ++j)
-      for (int64_t i = 0; i < L->n[0]; ++i) {
-        const int64_t id = (k * L->n[1] + j) * L->n[0] + i;
-        if (L->type[id] != 1) {
-          r[id] = 0.0;
-          continue;
-        }
-        double ax = 0.0;
-        for (int q = 0; q < 6; ++q) {
-          const int64_t ii = i + off[q][0], jj = j + off[q][1], kk = k + off[q][2];
-          const uint8_t t = mg_type(L, ii, jj, kk);
-          if (t == 0) continue;
-          ax += scale * (L->x[id] - (t == 1 ? L->x[(kk * L->n[1] + jj) * L->n[0] + ii] : 0.0));
-        }
-        r[id] = L->b[id] - ax;
-      }
-}
-
-static void mg_vcycle(mg_level* Ls, int l, int levels, int pre, int post, int coarse_sweeps, int64_t parity[]) {
+static void mg_vcycle(mg_level* Ls, int l, int levels, int pre, int post, int coarse_sweeps) {
   mg_level* L = &Ls[l];
   const size_t nc = (size_t)(L->n[0] * L->n[1] * L->n[2]);
-  const double scale = (double)(1 << l);
   memset(L->x, 0, sizeof(double) * nc);
   if (l == levels - 1) {
     for (int s = 0; s < coarse_sweeps; ++s) {
-      mg_sweep(L, scale, 0, parity[l]);
-      mg_sweep(L, scale, 1, parity[l]);
+      mg_sweep(L, 0, 0);
+      mg_sweep(L, 1, 0);
     }
     for (int s = 0; s < coarse_sweeps; ++s) {
-      mg_sweep(L, scale, 1, parity[l]);
-      mg_sweep(L, scale, 0, parity[l]);
+      mg_sweep(L, 1, 0);
+      mg_sweep(L, 0, 0);
     }
     return;
   }
   for (int s = 0; s < pre; ++s) {
-    mg_sweep(L, scale, 0, parity[l]);
-    mg_sweep(L, scale, 1, parity[l]);
+    mg_sweep(L, 0, s == 0);
+    mg_sweep(L, 1, 0);
   }
-  double* r = (double*)malloc(sizeof(double) * nc);
-  mg_residual(L, scale, r);
   mg_level* C = &Ls[l + 1];
-  const size_t ncc = (size_t)(C->n[0] * C->n[1] * C->n[2]);
-  memset(C->b, 0, sizeof(double) * ncc);
+  memset(C->b, 0, sizeof(double) * (size_t)(C->n[0] * C->n[1] * C->n[2]));
   for (int64_t k = 0; k < L->n[2]; ++k)
     for (int64_t j = 0; j < L->n[1]; ++j)
       for (int64_t i = 0; i < L->n[0]; ++i) {
-        const int64_t id = (k * L->n[1] + j) * L->n[0] + i;
-        if (L->type[id] != 1) continue;
-        C->b[((k / 2) * C->n[1] + j / 2) * C->n[0] + i / 2] += r[id];
+        const int64_t id = mg_id(L, i, j, k);
+        if (!L->fluid[id]) continue;
+        const double r = L->b[id] - (L->diag[id] * L->x[id] - mg_offdiag(L, i, j, k, L->x));
+        C->b[mg_id(C, i / 2, j / 2, k / 2)] += r;
       }
-  free(r);
-  mg_vcycle(Ls, l + 1, levels, pre, post, coarse_sweeps, parity);
+  mg_vcycle(Ls, l + 1, levels, pre, post, coarse_sweeps);
   for (int64_t k = 0; k < L->n[2]; ++k)
     for (int64_t j = 0; j < L->n[1]; ++j)
       for (int64_t i = 0; i < L->n[0]; ++i) {
-        const int64_t id = (k * L->n[1] + j) * L->n[0] + i;
-        if (L->type[id] != 1) continue;
-        L->x[id] += C->x[((k / 2) * C->n[1] + j / 2) * C->n[0] + i / 2];
+        const int64_t id = mg_id(L, i, j, k);
+        if (L->fluid[id]) L->x[id] += C->x[mg_id(C, i / 2, j / 2, k / 2)];
       }
   for (int s = 0; s < post; ++s) {
-    mg_sweep(L, scale, 1, parity[l]);
-    mg_sweep(L, scale, 0, parity[l]);
+    mg_sweep(L, 1, 0);
+    mg_sweep(L, 0, 0);
   }
+}
+
+static void mg_finish_diag(mg_level* L) {
+  for (int64_t k = 0; k < L->n[2]; ++k)
+    for (int64_t j = 0; j < L->n[1]; ++j)
+      for (int64_t i = 0; i < L->n[0]; ++i) {
+        const int64_t id = mg_id(L, i, j, k);
+        double d = L->anchor[id];
+        const int64_t c[3] = {i, j, k};
+        for (int a = 0; a < 3; ++a) {
+          int64_t hi[3] = {c[0], c[1], c[2]};
+          hi[a] += 1;
+          const int64_t jh = mg_id(L, hi[0], hi[1], hi[2]);
+          d += L->k[a][id];
+          if (jh >= 0) d += L->k[a][jh];
+        }
+        L->diag[id] = L->fluid[id] ? d : 1.0;
+      }
 }
 
 int fo_vcycle(const fo_box* b, const uint8_t* cell_type, int levels, int pre, int post, int coarse_sweeps,
               const double* r, double* z) {
-  if (levels < 1 || levels > 8) return FO_INVALID;
-  for (int d = 0; d < 3; ++d)
-    if (b->lo[d] % (1 << (levels - 1)) != 0 || b->n[d] % (1 << (levels - 1)) != 0) return FO_INVALID;
+  if (levels < 1 || levels > 8 || pre < 1 || post < 1) return FO_INVALID;
   mg_level Ls[8];
-  int64_t parity[8];
   for (int l = 0; l < levels; ++l) {
-    for (int d = 0; d < 3; ++d) Ls[l].n[d] = b->n[d] >> l;
+    for (int d = 0; d < 3; ++d) Ls[l].n[d] = l == 0 ? b->n[d] : (Ls[l - 1].n[d] + 1) / 2;
     const size_t nc = (size_t)(Ls[l].n[0] * Ls[l].n[1] * Ls[l].n[2]);
-    Ls[l].type = (uint8_t*)calloc(nc, 1);
+    Ls[l].fluid = (uint8_t*)calloc(nc, 1);
+    for (int a = 0; a < 3; ++a) Ls[l].k[a] = (double*)calloc(nc, sizeof(double));
+    Ls[l].anchor = (double*)calloc(nc, sizeof(double));
+    Ls[l].diag = (double*)calloc(nc, sizeof(double));
     Ls[l].x = (double*)calloc(nc, sizeof(double));
     Ls[l].b = (double*)calloc(nc, sizeof(double));
-    parity[l] = ((b->lo[0] >> l) + (b->lo[1] >> l) + (b->lo[2] >> l)) & 1;
   }
-  const size_t n0 = (size_t)(Ls[0].n[0] * Ls[0].n[1] * Ls[0].n[2]);
-  memcpy(Ls[0].type, cell_type, n0);
+  mg_level* L0 = &Ls[0];
+  for (int64_t k = 0; k < L0->n[2]; ++k)
+    for (int64_t j = 0; j < L0->n[1]; ++j)
+      for (int64_t i = 0; i < L0->n[0]; ++i) {
+        const int64_t id = mg_id(L0, i, j, k);
+        const int fl = cell_type[id] == 1;
+        L0->fluid[id] = (uint8_t)fl;
+        if (!fl) continue;
+        const int64_t c[3] = {i, j, k};
+        double anchor = 0.0;
+        for (int a = 0; a < 3; ++a) {
+          int64_t lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[0], c[1], c[2]};
+          lo[a] -= 1;
+          hi[a] += 1;
+          const int64_t jl = mg_id(L0, lo[0], lo[1], lo[2]), jh = mg_id(L0, hi[0], hi[1], hi[2]);
+          const int tl = jl >= 0 ? cell_type[jl] : 0, th = jh >= 0 ? cell_type[jh] : 0;
+          L0->k[a][id] = tl == 1 ? 1.0 : 0.0;
+          anchor += (tl == 2) + (th == 2);
+        }
+        L0->anchor[id] = anchor;
+      }
+  mg_finish_diag(L0);
   for (int l = 1; l < levels; ++l) {
     mg_level* F = &Ls[l - 1];
     mg_level* C = &Ls[l];
     for (int64_t k = 0; k < F->n[2]; ++k)
       for (int64_t j = 0; j < F->n[1]; ++j)
         for (int64_t i = 0; i < F->n[0]; ++i) {
-          const uint8_t t = F->type[(k * F->n[1] + j) * F->n[0] + i];
-          uint8_t* ct = &C->type[((k / 2) * C->n[1] + j / 2) * C->n[0] + i / 2];
-          if (t == 1)
-            *ct = 1;
-          else if (t == 2 && *ct == 0)
-            *ct = 2;
+          const int64_t fid = mg_id(F, i, j, k), cid = mg_id(C, i / 2, j / 2, k / 2);
+          if (F->fluid[fid]) C->fluid[cid] = 1;
+          C->anchor[cid] += 0.5 * F->anchor[fid];
+          const int64_t c[3] = {i, j, k};
+          for (int a = 0; a < 3; ++a)
+            if ((c[a] & 1) == 0) C->k[a][cid] += 0.5 * F->k[a][fid];
         }
+    mg_finish_diag(C);
   }
-  for (size_t i = 0; i < n0; ++i) Ls[0].b[i] = cell_type[i] == 1 ? r[i] : 0.0;
-  mg_vcycle(Ls, 0, levels, pre, post, coarse_sweeps, parity);
-  for (size_t i = 0; i < n0; ++i) z[i] = cell_type[i] == 1 ? Ls[0].x[i] : 0.0;
+  const size_t n0 = (size_t)(L0->n[0] * L0->n[1] * L0->n[2]);
+  for (size_t i = 0; i < n0; ++i) L0->b[i] = L0->fluid[i] ? r[i] : 0.0;
+  mg_vcycle(Ls, 0, levels, pre, post, coarse_sweeps);
+  for (size_t i = 0; i < n0; ++i) z[i] = L0->fluid[i] ? L0->x[i] : 0.0;
   for (int l = 0; l < levels; ++l) {
-    free(Ls[l].type);
+    free(Ls[l].fluid);
+    for (int a = 0; a < 3; ++a) free(Ls[l].k[a]);
+    free(Ls[l].anchor);
+    free(Ls[l].diag);
     free(Ls[l].x);
     free(Ls[l].b);
   }

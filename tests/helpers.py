@@ -1,0 +1,71 @@
+"""Shared test helpers: scene setup, host replica of the stable cell sort, and
+GPU state read-back into dense box arrays for comparison with the oracle."""
+
+import json
+from pathlib import Path
+
+import numpy as np
+
+import fluidity_b200 as fb
+import oracle
+from fluidity_b200 import scenes
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def golden(name):
+    return json.loads((GOLDEN / name).read_text())
+
+
+def soa_to_xvc(soa):
+    x = soa[0:3].T.astype(np.float64)
+    v = soa[3:6].T.astype(np.float64)
+    c = soa[6:15].T.astype(np.float64)
+    return x, v, c
+
+
+def box_for(n):
+    return oracle.Box.make([0.0, 0.0, 0.0], 1.0 / n, [0, 0, 0], [n, n, n])
+
+
+def sort_permutation(soa, n):
+    """Replica of the device's stable sort key (block, local cell) for a box of n cells."""
+    X = soa[0:3].astype(np.float32) * np.float32(n)
+    cell = np.floor(X).astype(np.int64)
+    nbk = n // 8
+    key = ((((cell[2] >> 3) * nbk + (cell[1] >> 3)) * nbk + (cell[0] >> 3)) * 512 + (cell[2] & 7) * 64 +
+           (cell[1] & 7) * 8 + (cell[0] & 7))
+    return np.argsort(key, kind="stable")
+
+
+def read_fields(ctx, n):
+    blocks = ctx.active_blocks()
+    nb = len(blocks)
+    f = ctx.fields()
+    nn = (n, n, n)
+    out = {"blocks": blocks}
+    out["u_pred"] = [fb.sparse_faces_to_dense(blocks, fb.copy_to_host(f["u_pred"][a], nb * 512, np.float32), nn, a,
+                                              fill=np.nan) for a in range(3)]
+    out["u_new"] = [fb.sparse_faces_to_dense(blocks, fb.copy_to_host(f["u_new"][a], nb * 512, np.float32), nn, a,
+                                             fill=np.nan) for a in range(3)]
+    out["pressure"] = fb.sparse_cells_to_dense(blocks, fb.copy_to_host(f["pressure"], nb * 512, np.float64), nn,
+                                               fill=np.nan)
+    out["cell_type"] = fb.sparse_cells_to_dense(blocks, fb.copy_to_host(f["cell_type"], nb * 512, np.uint8), nn,
+                                                fill=255)
+    return out
+
+
+def rel_err(a, b, mask=None):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if mask is not None:
+        a, b = a[mask], b[mask]
+    scale = max(np.abs(b).max(), 1e-300)
+    return float(np.abs(a - b).max() / scale)
+
+
+def dam_break_context(n, capacity=None):
+    soa, m = scenes.dam_break(n)
+    ctx = fb.LiquidContext(n, capacity=capacity or soa.shape[1])
+    ctx.upload(soa)
+    return ctx, soa, m
