@@ -92,6 +92,13 @@ struct fl_context {
   bool in_step = false;  // fl_step keeps one device report across its stages
   cudaEvent_t phase[5] = {};  // topology+sort | P2G | pressure | G2P boundaries of the last fl_step
   bool phases_valid = false;
+  // pressure solver: own stream (graph capture needs a non-legacy stream), the
+  // replayed two-iteration FCG graph, handoff events and the natural-layout pressure
+  cudaStream_t work = nullptr;
+  cudaGraphExec_t fcg_exec = nullptr;
+  unsigned long long fcg_graph_kernels = 0;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  double* p_nat = nullptr;
 };
 
 namespace {
@@ -262,10 +269,51 @@ __global__ void k_set_inner_budget(SolverState* st, int inner_max) {
   st->done = st->converged;
 }
 
+// Captures two flexible-CG iterations (V-cycle + 3 CG kernels each, r/d
+// buffers swapping roles) into one graph and updates the executable graph in
+// place when only launch parameters changed (the block count changes per step).
+template <typename T>
+int capture_fcg(fl_context* c, const GridView& g, const MgHierarchy<T>& H, const MgOptions& mo) {
+  cudaGraph_t graph = nullptr;
+  const unsigned long long before = g_kernel_launches;
+  FL_CUDA(cudaStreamBeginCapture(c->work, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e1 = launch_fcg_iteration<T>(g, H, mo, c->r[0], c->r[1], c->d[0], c->d[1], c->q, c->e, c->partial,
+                                           c->st, &c->st->done, c->work);
+  cudaError_t e2 = launch_fcg_iteration<T>(g, H, mo, c->r[1], c->r[0], c->d[1], c->d[0], c->q, c->e, c->partial,
+                                           c->st, &c->st->done, c->work);
+  cudaError_t e3 = cudaStreamEndCapture(c->work, &graph);
+  c->fcg_graph_kernels = g_kernel_launches - before;
+  g_kernel_launches = before;  // counted again at every replay
+  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return FL_INTERNAL;
+  }
+  bool updated = false;
+  if (c->fcg_exec) {
+    cudaGraphExecUpdateResultInfo info;
+    updated = cudaGraphExecUpdate(c->fcg_exec, graph, &info) == cudaSuccess;
+    if (!updated) {
+      cudaGetLastError();
+      cudaGraphExecDestroy(c->fcg_exec);
+      c->fcg_exec = nullptr;
+    }
+  }
+  if (!updated) {
+    if (cudaGraphInstantiate(&c->fcg_exec, graph, 0) != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      c->fcg_exec = nullptr;
+      return FL_INTERNAL;
+    }
+  }
+  cudaGraphDestroy(graph);
+  return FL_OK;
+}
+
 template <typename T>
 int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_new[3], const fl_transfer_params* tp,
                    const fl_pressure_options* opt, fl_pressure_diagnostics* diag, double* pressure_out,
-                   cudaStream_t s) {
+                   cudaStream_t user) {
   GridView g = view(c);
   MgHierarchy<T> H{};
   const int levels = opt->levels > 0 ? opt->levels : auto_levels(c);
@@ -277,6 +325,9 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   const double vel_scale = dt / (rho * h);    // u += vel_scale * (p_tail - p_head)
   const long long n = (long long)c->nb * kBlockCells;
   MgOptions mo{std::max(1, opt->pre_sweeps), std::max(1, opt->post_sweeps), std::max(1, opt->coarse_sweeps)};
+  cudaStream_t s = c->work;
+  FL_CUDA(cudaEventRecord(c->ev_in, user));
+  FL_CUDA(cudaStreamWaitEvent(s, c->ev_in, 0));
   FL_CUDA(cudaEventRecord(c->ev0, s));
   ++g_kernel_launches;
   k_init_state<<<1, 1, 0, s>>>(c->st, opt->rel_tol, opt->inner_rtol, opt->max_iterations);
@@ -292,6 +343,7 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   bool converged = false;
   int status = FL_OK;
   const int max_ref = std::max(1, opt->max_refinements);
+  bool captured = false;
   for (int outer = 0; outer <= max_ref; ++outer) {
     FL_CUDA(launch_residual64<T>(g, H, c->b64, c->p64, c->r[0], c->e, c->partial, c->st, s));
     FL_CUDA(cudaMemcpyAsync(c->st_host, c->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
@@ -304,16 +356,14 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
     ++refinements;
     ++g_kernel_launches;
     k_set_inner_budget<<<1, 1, 0, s>>>(c->st, opt->max_iterations - total);
-    int cur = 0;
-    int it = 0;
+    if (!captured) {
+      st = capture_fcg<T>(c, g, H, mo);
+      if (st != FL_OK) return st;
+      captured = true;
+    }
     for (;;) {
-      // Two iterations per host check; buffers alternate r/d roles.
-      for (int k = 0; k < 2; ++k) {
-        FL_CUDA(launch_fcg_iteration<T>(g, H, mo, c->r[cur], c->r[1 - cur], c->d[cur], c->d[1 - cur], c->q, c->e,
-                                        c->partial, c->st, &c->st->done, s));
-        cur = 1 - cur;
-        ++it;
-      }
+      FL_CUDA(cudaGraphLaunch(c->fcg_exec, s));
+      g_kernel_launches += c->fcg_graph_kernels;
       FL_CUDA(cudaMemcpyAsync(c->st_host, c->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
       FL_CUDA(cudaStreamSynchronize(s));
       if (c->st_host->done) break;
@@ -326,9 +376,12 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
     FL_CUDA(launch_accumulate(g, c->e, c->p64, s));
   }
   FL_CUDA(launch_correct_faces(g, c->type, c->p64, u_pred, u_new, vel_scale, c->partial, c->st, s));
+  FL_CUDA(launch_export_pressure(g, c->p64, c->p_nat, s));
   FL_CUDA(cudaEventRecord(c->ev1, s));
-  if (pressure_out) FL_CUDA(cudaMemcpyAsync(pressure_out, c->p64, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  if (pressure_out) FL_CUDA(cudaMemcpyAsync(pressure_out, c->p_nat, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   FL_CUDA(cudaMemcpyAsync(c->st_host, c->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
+  FL_CUDA(cudaEventRecord(c->ev_out, s));
+  FL_CUDA(cudaStreamWaitEvent(user, c->ev_out, 0));
   FL_CUDA(cudaStreamSynchronize(s));
   const SolverState& S = *c->st_host;
   if (diag) {
@@ -352,15 +405,6 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   return converged ? FL_OK : FL_ABORTED;
 }
 
-__global__ void k_copy_x(long long n, const float* fluid_src, const void* x, int bf16, float* z,
-                         const unsigned char* fluid) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float v = bf16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(x)[i]) : reinterpret_cast<const float*>(x)[i];
-  z[i] = fluid[i] ? v : 0.0f;  // fluid = level-0 flags
-  (void)fluid_src;
-}
-
 template <typename T>
 int apply_vcycle(fl_context* c, const float* r, float* z, const fl_pressure_options* opt, cudaStream_t s) {
   GridView g = view(c);
@@ -373,15 +417,12 @@ int apply_vcycle(fl_context* c, const float* r, float* z, const fl_pressure_opti
   ++g_kernel_launches;
   k_init_state<<<1, 1, 0, s>>>(c->st, 1e-6, 1e-4, 1);
   const float* up[3] = {c->u_pred[0], c->u_pred[1], c->u_pred[2]};
-  FL_CUDA(cudaMemsetAsync(c->u_pred[0], 0, sizeof(float) * n, s));
-  FL_CUDA(cudaMemsetAsync(c->u_pred[1], 0, sizeof(float) * n, s));
-  FL_CUDA(cudaMemsetAsync(c->u_pred[2], 0, sizeof(float) * n, s));
+  for (int a = 0; a < 3; ++a) FL_CUDA(cudaMemsetAsync(c->u_pred[a], 0, sizeof(float) * n, s));
   FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, up, 1.0, H, c->b64, c->p64, c->partial, c->st, s));
   FL_CUDA(cudaMemsetAsync(c->lv_x[0], 0, sizeof(T) * (size_t)n, s));
-  FL_CUDA(launch_apply_vcycle<T>(g, H, r, mo, &c->st->done, s));
-  ++g_kernel_launches;
-  k_copy_x<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, r, c->lv_x[0], sizeof(T) == 2, z, c->lv_fluid[0]);
-  FL_CUDA(cudaGetLastError());
+  FL_CUDA(launch_to_rb(g, r, c->r[0], s));
+  FL_CUDA(launch_apply_vcycle<T>(g, H, c->r[0], mo, &c->st->done, s));
+  FL_CUDA(launch_to_natural<T>(g, H, z, s));
   FL_CUDA(cudaStreamSynchronize(s));
   return FL_OK;
 }
@@ -604,6 +645,11 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
   chk(dalloc(&c->type, cells));
   chk(dalloc(&c->b64, cells));
   chk(dalloc(&c->p64, cells));
+  chk(dalloc(&c->p_nat, cells));
+  if (cudaStreamCreateWithFlags(&c->work, cudaStreamNonBlocking) != cudaSuccess) chk(FL_INTERNAL);
+  if (cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming) != cudaSuccess) chk(FL_INTERNAL);
+  if (cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess) chk(FL_INTERNAL);
+  configure_pressure_kernels();
   for (int k = 0; k < 2; ++k) {
     chk(dalloc(&c->r[k], cells));
     chk(dalloc(&c->d[k], cells));
@@ -686,6 +732,11 @@ int fl_context_destroy(fl_context* c) {
   cudaFree(c->type);
   cudaFree(c->b64);
   cudaFree(c->p64);
+  cudaFree(c->p_nat);
+  if (c->fcg_exec) cudaGraphExecDestroy(c->fcg_exec);
+  if (c->work) cudaStreamDestroy(c->work);
+  if (c->ev_in) cudaEventDestroy(c->ev_in);
+  if (c->ev_out) cudaEventDestroy(c->ev_out);
   for (int k = 0; k < 2; ++k) {
     cudaFree(c->r[k]);
     cudaFree(c->d[k]);
@@ -883,7 +934,7 @@ int fl_state_fields(fl_context* c, float* u_pred[3], float* u_new[3], double** p
     if (u_pred) u_pred[a] = c->u_pred[a];
     if (u_new) u_new[a] = c->u_new[a];
   }
-  if (pressure) *pressure = c->p64;
+  if (pressure) *pressure = c->p_nat;
   if (cell_type) *cell_type = c->type;
   if (cell_start) *cell_start = c->cell_start;
   return FL_OK;

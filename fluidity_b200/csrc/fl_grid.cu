@@ -49,7 +49,10 @@ __global__ void k_mark_blocks(GridView g, ParticlesView p, unsigned char* occ, D
       return;
     }
   }
-  occ[((size_t)b[2] * g.bdim[1] + b[1]) * g.bdim[0] + b[0]] = 1;
+  // Most particles of a block mark the same byte: read first so only the
+  // first visitors store (contended same-address stores serialize in L2).
+  unsigned char* o = occ + ((size_t)b[2] * g.bdim[1] + b[1]) * g.bdim[0] + b[0];
+  if (*o == 0) *o = 1;
 }
 
 __global__ void k_flag_active(GridView g, const unsigned char* occ, int* flag, int total) {

@@ -114,6 +114,11 @@ template <typename T>
 cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, const MgOptions& opt, float* r_cur,
                                  float* r_prev, float* d_old, float* d_new, float* q, float* e, double* partial,
                                  SolverState* st, const int* done, cudaStream_t s);
+cudaError_t launch_export_pressure(const GridView& g, const double* p64, double* p_nat, cudaStream_t s);
+cudaError_t launch_to_rb(const GridView& g, const float* in_nat, float* out_rb, cudaStream_t s);
+template <typename T>
+cudaError_t launch_to_natural(const GridView& g, const MgHierarchy<T>& H, float* out_nat, cudaStream_t s);
+void configure_pressure_kernels();
 cudaError_t launch_accumulate(const GridView& g, const float* e, double* p64, cudaStream_t s);
 cudaError_t launch_correct_faces(const GridView& g, const unsigned char* type, const double* p64,
                                  const float* const u_pred[3], float* const u_new[3], double scale, double* partial,

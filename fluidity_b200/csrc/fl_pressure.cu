@@ -141,6 +141,23 @@ __device__ __forceinline__ int parent_s(const GridView& g, int j, int cdx, int c
   return ((g.coord[3 * b + 2] - g.blo[2]) * cdy + (g.coord[3 * b + 1] - g.blo[1])) * cdx + (g.coord[3 * b] - g.blo[0]);
 }
 
+// Level-0 solver layout (red-black): inside each block the 256 cells of colour
+// c = (x+y+z)&1 occupy [c*256, c*256+256) in (z, y, x/2) order, so a colour
+// sweep reads and writes contiguous memory. Face and particle arrays keep the
+// natural (z*64 + y*8 + x) order.
+__device__ __forceinline__ int rb_of(int l) {
+  const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
+  return (((x + y + z) & 1) << 8) | (z << 5) | (y << 2) | (x >> 1);
+}
+__device__ __forceinline__ int nat_of(int r) {
+  const int c = r >> 8, j = r & 255;
+  const int z = j >> 5, y = (j >> 2) & 7, xh = j & 3;
+  return (z << 6) | (y << 3) | (2 * xh + ((y + z + c) & 1));
+}
+__device__ __forceinline__ int rb_id(int natural_id) {
+  return natural_id < 0 ? natural_id : ((natural_id & ~511) | rb_of(natural_id & 511));
+}
+
 // ----------------------------------------------------------------- level-0 setup (box scene)
 
 __device__ __forceinline__ bool last_block(SolverState* st) {
@@ -214,13 +231,14 @@ __global__ void k_setup_level0(GridView g, const unsigned char* type, const floa
         div += uhi - ulo;
       }
     }
-    L0.mask[i] = (unsigned char)mask;
-    L0.fluid[i] = fluid ? 1 : 0;
-    L0.anchor[i] = anchor;
-    L0.diag[i] = fluid ? anchor + (float)__popc(mask & 63u) : 1.0f;
+    const int r = rb_id(i);
+    L0.mask[r] = (unsigned char)mask;
+    L0.fluid[r] = fluid ? 1 : 0;
+    L0.anchor[r] = anchor;
+    L0.diag[r] = fluid ? anchor + (float)__popc(mask & 63u) : 1.0f;
     const double rhs = fluid ? -rhs_scale * div : 0.0;
-    b64[i] = rhs;
-    p64[i] = 0.0;
+    b64[r] = rhs;
+    p64[r] = 0.0;
     bb += rhs * rhs;
   }
   const double s = block_sum<kThreads>(bb, red);
@@ -284,7 +302,7 @@ __global__ void k_coarsen(GridView g, LevelDesc F, LevelPtrs<T> fp, LevelDesc C,
   bool fluid = false;
   float anchor = 0.0f, k[3] = {0.0f, 0.0f, 0.0f};
   for (int c = 0; c < nchild; ++c) {
-    const long long id = child[c];
+    const long long id = fp.mask ? (long long)rb_id((int)child[c]) : child[c];
     if (fp.fluid[id]) fluid = true;
     anchor += fp.anchor[id];
 #pragma unroll
@@ -334,7 +352,7 @@ __global__ void __launch_bounds__(kThreads)
   const int z = j / (S * S / 2), rr = j % (S * S / 2), y = rr / (S / 2), xh = rr % (S / 2);
   const int x = 2 * xh + ((y + z + color) & 1);
   const int l = (z * S + y) * S + x;
-  const int i = blk * S3 + l;
+  const int i = LS == 3 ? blk * S3 + (color << 8) + j : blk * S3 + l;
   unsigned m = 0;
   if (LS == 3) {
     m = lp.mask[i];
@@ -359,7 +377,7 @@ __global__ void __launch_bounds__(kThreads)
           k = dir < 0 ? ld(&lp.k[a][i]) : ld(&lp.k[a][jn]);
           if (k == 0.0f) continue;
         }
-        float xj = ld(&lp.x[jn]);
+        float xj = ld(&lp.x[LS == 3 ? rb_id(jn) : jn]);
         if (MODE == 2) xj += ld(&xc[parent_s<LS>(g, jn, cdx, cdy)]);
         s = fmaf(k, xj, s);
       }
@@ -382,7 +400,7 @@ __global__ void __launch_bounds__(512)
   const int l = t % S3;
   float res = 0.0f;
   if (blk < g.nb) {
-    const int i = blk * S3 + l;
+    const int i = LS == 3 ? blk * S3 + rb_of(l) : blk * S3 + l;
     unsigned m = 0;
     bool fluid;
     if (LS == 3) {
@@ -408,7 +426,7 @@ __global__ void __launch_bounds__(512)
             k = dir < 0 ? ld(&fp.k[a][i]) : ld(&fp.k[a][jn]);
             if (k == 0.0f) continue;
           }
-          ax = fmaf(-k, ld(&fp.x[jn]), ax);
+          ax = fmaf(-k, ld(&fp.x[LS == 3 ? rb_id(jn) : jn]), ax);
         }
       }
       res = fb[i] - ax;
@@ -534,6 +552,40 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(LevelDesc L, LevelPtrs<T>
   }
   __syncthreads();
   const int nx = L.dim[0], ny = L.dim[1], nz = L.dim[2];
+  if (n <= (int)blockDim.x) {
+    // One cell per thread: coefficients and neighbour offsets stay in registers.
+    const int i = threadIdx.x;
+    bool active = false;
+    int color = 0;
+    float kk[6] = {0, 0, 0, 0, 0, 0}, inv = 0.0f, bi = 0.0f;
+    int nb[6] = {0, 0, 0, 0, 0, 0};
+    if (i < n && dg[i] != 0.0f) {
+      active = true;
+      const int cx = i % nx, cy = (i / nx) % ny, cz = i / (nx * ny);
+      color = (cx + cy + cz + L.parity) & 1;
+      inv = 1.0f / dg[i];
+      bi = bb[i];
+      if (cx > 0) { kk[0] = k0[i]; nb[0] = i - 1; }
+      if (cx + 1 < nx) { kk[1] = k0[i + 1]; nb[1] = i + 1; }
+      if (cy > 0) { kk[2] = k1[i]; nb[2] = i - nx; }
+      if (cy + 1 < ny) { kk[3] = k1[i + nx]; nb[3] = i + nx; }
+      if (cz > 0) { kk[4] = k2[i]; nb[4] = i - nx * ny; }
+      if (cz + 1 < nz) { kk[5] = k2[i + nx * ny]; nb[5] = i + nx * ny; }
+    }
+    for (int pass = 0; pass < 4 * sweeps; ++pass) {
+      const int half = pass % 2;
+      const int c = pass < 2 * sweeps ? half : 1 - half;
+      if (active && color == c) {
+        float s = bi;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) s = fmaf(kk[q], x[nb[q]], s);
+        x[i] = s * inv;
+      }
+      __syncthreads();
+    }
+    if (i < n) st_T(&lp.x[i], lp.fluid[i] ? x[i] : 0.0f);
+    return;
+  }
   for (int pass = 0; pass < 4 * sweeps; ++pass) {
     // forward sweeps red,black; backward sweeps black,red
     const int half = pass % 2;
@@ -562,14 +614,14 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(LevelDesc L, LevelPtrs<T>
 template <typename T, typename V>
 __device__ __forceinline__ V apply0(const GridView& g, const LevelPtrs<T>& L0, unsigned m, int i, V xi,
                                     const V* __restrict__ xv) {
-  const int b = i >> 9, l = i & 511;
+  const int b = i >> 9, l = nat_of(i & 511);
   V ax = (V)L0.diag[i] * xi;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
 #pragma unroll
     for (int dir = -1; dir <= 1; dir += 2) {
       if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
-      ax -= xv[nbr_s<3>(g, b, l, a, dir)];
+      ax -= xv[rb_id(nbr_s<3>(g, b, l, a, dir))];
     }
   }
   return ax;
@@ -656,14 +708,14 @@ __global__ void k_direction(GridView g, LevelPtrs<T> L0, const T* __restrict__ z
     float di = 0.0f, qi = 0.0f;
     if (m & 64u) {
       di = first ? ld(&z[i]) : fmaf(beta, d_old[i], ld(&z[i]));
-      const int b = i >> 9, l = i & 511;
+      const int b = i >> 9, l = nat_of(i & 511);
       float ax = L0.diag[i] * di;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
 #pragma unroll
         for (int dir = -1; dir <= 1; dir += 2) {
           if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
-          const int j = nbr_s<3>(g, b, l, a, dir);
+          const int j = rb_id(nbr_s<3>(g, b, l, a, dir));
           ax -= first ? ld(&z[j]) : fmaf(beta, d_old[j], ld(&z[j]));
         }
       }
@@ -738,8 +790,8 @@ __global__ void k_correct_faces(GridView g, const unsigned char* type, const dou
   float* un = a == 0 ? un0 : (a == 1 ? un1 : un2);
   double u = (double)up[head];
   if (th != 0 && tt != 0 && (th == 1 || tt == 1)) {
-    const double ph = th == 1 ? p64[head] : 0.0;
-    const double pt = tt == 1 ? p64[tail] : 0.0;
+    const double ph = th == 1 ? p64[rb_id(head)] : 0.0;
+    const double pt = tt == 1 ? p64[rb_id(tail)] : 0.0;
     u += scale * (pt - ph);
   }
   un[head] = (float)u;
@@ -763,9 +815,10 @@ __global__ void k_diagnostics(GridView g, const unsigned char* type, const doubl
       const int lo = nbr_s<3>(g, b, l, a, -1);
       const int hi = nbr_s<3>(g, b, l, a, +1);
       const int tlo = nbr_type(type, lo), thi = nbr_type(type, hi);
+      const double pi = p64[rb_id(i)];
       double ulo = (double)up[a][i], uhi = hi >= 0 ? (double)up[a][hi] : 0.0;
-      if (tlo != 0) ulo += scale * ((tlo == 1 ? p64[lo] : 0.0) - p64[i]);
-      if (thi != 0) uhi += scale * (p64[i] - (thi == 1 ? p64[hi] : 0.0));
+      if (tlo != 0) ulo += scale * ((tlo == 1 ? p64[rb_id(lo)] : 0.0) - pi);
+      if (thi != 0) uhi += scale * (pi - (thi == 1 ? p64[rb_id(hi)] : 0.0));
       div += uhi - ulo;
     }
     maxdiv = fmax(maxdiv, fabs(div));
@@ -800,6 +853,21 @@ __global__ void k_diagnostics(GridView g, const unsigned char* type, const doubl
       st->ticket = 0;
     }
   }
+}
+
+// Solver (red-black) <-> natural level-0 layout conversions.
+__global__ void k_export_pressure(int n, const double* p64_rb, double* p_nat) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p_nat[i] = p64_rb[rb_id(i)];
+}
+template <typename T>
+__global__ void k_to_natural(int n, const T* x_rb, const unsigned char* fluid_rb, float* out_nat) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int r = rb_id(i);
+    out_nat[i] = fluid_rb[r] ? ld(&x_rb[r]) : 0.0f;
+  }
+}
+__global__ void k_to_rb(int n, const float* in_nat, float* out_rb) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out_rb[rb_id(i)] = in_nat[i];
 }
 
 // ----------------------------------------------------------------- host orchestration
@@ -875,12 +943,6 @@ static void vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r0, 
   {
     const LevelDesc& C = H.desc[L - 1];
     const size_t smem = (size_t)C.count * 6 * sizeof(float);
-    static bool configured = false;
-    if (!configured) {
-      cudaFuncSetAttribute(k_coarse_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           8192 * 6 * (int)sizeof(float));
-      configured = true;
-    }
     const int threads = C.count <= 1024 ? (int)((C.count + 31) / 32 * 32) : 1024;
     ++g_kernel_launches;
     k_coarse_solve<T><<<1, threads, smem, s>>>(C, H.ptr[L - 1], H.b[L - 1], opt.coarse_sweeps, done);
@@ -969,6 +1031,37 @@ cudaError_t launch_correct_faces(const GridView& g, const unsigned char* type, c
   return cudaGetLastError();
 }
 
+cudaError_t launch_export_pressure(const GridView& g, const double* p64, double* p_nat, cudaStream_t s) {
+  const int n = g.nb * kBlockCells;
+  ++g_kernel_launches;
+  k_export_pressure<<<reduce_grid(n), kThreads, 0, s>>>(n, p64, p_nat);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_rb(const GridView& g, const float* in_nat, float* out_rb, cudaStream_t s) {
+  const int n = g.nb * kBlockCells;
+  ++g_kernel_launches;
+  k_to_rb<<<reduce_grid(n), kThreads, 0, s>>>(n, in_nat, out_rb);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_to_natural(const GridView& g, const MgHierarchy<T>& H, float* out_nat, cudaStream_t s) {
+  const int n = g.nb * kBlockCells;
+  ++g_kernel_launches;
+  k_to_natural<T><<<reduce_grid(n), kThreads, 0, s>>>(n, H.ptr[0].x, H.ptr[0].fluid, out_nat);
+  return cudaGetLastError();
+}
+
+void configure_pressure_kernels() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(k_coarse_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 6 * (int)sizeof(float));
+  cudaFuncSetAttribute(k_coarse_solve<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       8192 * 6 * (int)sizeof(float));
+  done = true;
+}
+
 #define FL_INSTANTIATE(T)                                                                                         \
   template cudaError_t launch_pressure_setup<T>(const GridView&, const int*, unsigned char*, const float* const[3], \
                                                 double, MgHierarchy<T>&, double*, double*, double*, SolverState*,   \
@@ -979,7 +1072,8 @@ cudaError_t launch_correct_faces(const GridView& g, const unsigned char* type, c
                                             float*, float*, double*, SolverState*, cudaStream_t);                  \
   template cudaError_t launch_fcg_iteration<T>(const GridView&, const MgHierarchy<T>&, const MgOptions&, float*,   \
                                                float*, float*, float*, float*, float*, double*, SolverState*,      \
-                                               const int*, cudaStream_t);
+                                               const int*, cudaStream_t);                                          \
+  template cudaError_t launch_to_natural<T>(const GridView&, const MgHierarchy<T>&, float*, cudaStream_t);
 
 FL_INSTANTIATE(float)
 FL_INSTANTIATE(__nv_bfloat16)
