@@ -218,6 +218,37 @@ int fl_gather_mac_3d(const double origin[3], double h, const int32_t* blocks, ui
                      const double* particles, uint64_t particle_count, const double* old_face_velocities,
                      const double* new_face_velocities, double* results, fl_measurement* measurement);
 
+/* Block layout passed to fl_p2g_static_scratch: device arrays of 8^3-block
+ * coordinates (block_count x 3, ordinal order), 26-neighbourhood ordinals
+ * (block_count x 27, index (dz+1)*9+(dy+1)*3+(dx+1), -1 inactive, -2 outside
+ * the lattice) and per-cell particle ranges (block_count*512 + 1). */
+typedef struct {
+  double origin[3];
+  double h;
+  int32_t solid_lo[3];
+  int32_t solid_hi[3];
+  const int32_t* block_coords;
+  const int32_t* neighbors;
+  const int32_t* cell_start;
+  uint64_t block_count;
+} fl_static_grid;
+
+/* P2G that allocates nothing (no counterpart in the reference). For callers
+ * that cannot call cudaMalloc where they deposit -- a host engine whose
+ * device memory all comes from its own pool, or a substep that must not
+ * allocate once started -- this runs the fl_p2g kernels without a context.
+ * The caller passes layout, sorted particles and output face arrays (same
+ * meaning and modes as fl_p2g); the per-block tile scratch is a file-scope
+ * static device array of at most 512 active blocks (13.5 MB, held on every
+ * GPU that loads the library until exit). More blocks return
+ * FL_RESOURCE_EXHAUSTED. The first call on a device looks up the array's
+ * device address, so make it before any stream capture. All calls on a GPU
+ * share that GPU's array, which keeps the last call's contents: calls that
+ * overlap on the same GPU (for example on concurrent streams) race and must
+ * be serialized by the caller. */
+int fl_p2g_static_scratch(const fl_static_grid* grid, const fl_particles* sorted, const fl_transfer_params* params,
+                          int mode, float* const out0[3], float* const out1[3], void* stream, fl_report* report);
+
 /* Plain device<->host copies for callers without their own CUDA runtime binding. */
 int fl_copy_to_host(void* host, const void* device, uint64_t bytes);
 int fl_copy_to_device(void* device, const void* host, uint64_t bytes);
