@@ -133,7 +133,7 @@ def run_ours(args, world, rank, local):
     npart = soa.shape[1]
     ctx = fb.LiquidContext(args.grid, capacity=npart)
     tp = fb.transfer_params(scenes.DT, mass)
-    opt = fb.default_pressure_options(precision=1, rel_tol=1e-6)
+    opt = fb.default_pressure_options(precision=1, rel_tol=1e-6, warm_start=1)
     ctx.upload(soa)
     for _ in range(args.warmup):
         code, _ = ctx.step(tp, opt)

@@ -75,7 +75,7 @@ class TransferParams(ctypes.Structure):
 class PressureOptions(ctypes.Structure):
     _fields_ = [("levels", ctypes.c_int), ("pre_sweeps", ctypes.c_int), ("post_sweeps", ctypes.c_int),
                 ("coarse_sweeps", ctypes.c_int), ("precision", ctypes.c_int), ("max_iterations", ctypes.c_int),
-                ("max_refinements", ctypes.c_int), ("pad", ctypes.c_int), ("rel_tol", ctypes.c_double),
+                ("max_refinements", ctypes.c_int), ("warm_start", ctypes.c_int), ("rel_tol", ctypes.c_double),
                 ("inner_rtol", ctypes.c_double)]
 
 
@@ -164,8 +164,10 @@ def runtime_info():
 
 def default_pressure_options(precision: int = 0, rel_tol: float = 1e-6, levels: int = 0, pre: int = 2,
                              post: int = 2, coarse_sweeps: int = 16, max_iterations: int = 400,
-                             max_refinements: int = 6, inner_rtol: float = 1e-4) -> PressureOptions:
+                             max_refinements: int = 6, inner_rtol: float = 1e-4,
+                             warm_start: int = 0) -> PressureOptions:
     o = PressureOptions()
+    o.warm_start = warm_start
     o.levels, o.pre_sweeps, o.post_sweeps, o.coarse_sweeps = levels, pre, post, coarse_sweeps
     o.precision, o.max_iterations, o.max_refinements = precision, max_iterations, max_refinements
     o.rel_tol, o.inner_rtol = rel_tol, inner_rtol

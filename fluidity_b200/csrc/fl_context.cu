@@ -99,6 +99,8 @@ struct fl_context {
   unsigned long long fcg_graph_kernels = 0;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   double* p_nat = nullptr;
+  float* p_keep = nullptr;  // last pressure per lattice cell (warm start across topology changes)
+  bool p_keep_valid = false;
 };
 
 namespace {
@@ -331,8 +333,9 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   FL_CUDA(cudaEventRecord(c->ev0, s));
   ++g_kernel_launches;
   k_init_state<<<1, 1, 0, s>>>(c->st, opt->rel_tol, opt->inner_rtol, opt->max_iterations);
-  FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, u_pred, rhs_scale, H, c->b64, c->p64, c->partial,
-                                   c->st, s));
+  const float* p_prev = (opt->warm_start && c->p_keep_valid) ? c->p_keep : nullptr;
+  FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, u_pred, rhs_scale, H, c->b64, c->p64, p_prev,
+                                   c->partial, c->st, s));
   ++g_kernel_launches;
   k_set_target<<<1, 1, 0, s>>>(c->st, opt->rel_tol);
   FL_CUDA(cudaMemsetAsync(c->lv_x[0], 0, sizeof(T) * (size_t)n, s));
@@ -376,7 +379,10 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
     FL_CUDA(launch_accumulate(g, c->e, c->p64, s));
   }
   FL_CUDA(launch_correct_faces(g, c->type, c->p64, u_pred, u_new, vel_scale, c->partial, c->st, s));
-  FL_CUDA(launch_export_pressure(g, c->p64, c->p_nat, s));
+  // The kept copy is rewritten in full: cells that are not fluid now read back as 0.
+  FL_CUDA(cudaMemsetAsync(c->p_keep, 0, sizeof(float) * (size_t)c->lattice * kBlockCells, s));
+  FL_CUDA(launch_export_pressure(g, c->p64, c->p_nat, c->p_keep, s));
+  c->p_keep_valid = true;
   FL_CUDA(cudaEventRecord(c->ev1, s));
   if (pressure_out) FL_CUDA(cudaMemcpyAsync(pressure_out, c->p_nat, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   FL_CUDA(cudaMemcpyAsync(c->st_host, c->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
@@ -418,7 +424,8 @@ int apply_vcycle(fl_context* c, const float* r, float* z, const fl_pressure_opti
   k_init_state<<<1, 1, 0, s>>>(c->st, 1e-6, 1e-4, 1);
   const float* up[3] = {c->u_pred[0], c->u_pred[1], c->u_pred[2]};
   for (int a = 0; a < 3; ++a) FL_CUDA(cudaMemsetAsync(c->u_pred[a], 0, sizeof(float) * n, s));
-  FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, up, 1.0, H, c->b64, c->p64, c->partial, c->st, s));
+  FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, up, 1.0, H, c->b64, c->p64, nullptr, c->partial,
+                                   c->st, s));
   FL_CUDA(cudaMemsetAsync(c->lv_x[0], 0, sizeof(T) * (size_t)n, s));
   FL_CUDA(launch_to_rb(g, r, c->r[0], s));
   FL_CUDA(launch_apply_vcycle<T>(g, H, c->r[0], mo, &c->st->done, s));
@@ -646,6 +653,7 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
   chk(dalloc(&c->b64, cells));
   chk(dalloc(&c->p64, cells));
   chk(dalloc(&c->p_nat, cells));
+  chk(dalloc(&c->p_keep, cells));
   if (cudaStreamCreateWithFlags(&c->work, cudaStreamNonBlocking) != cudaSuccess) chk(FL_INTERNAL);
   if (cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming) != cudaSuccess) chk(FL_INTERNAL);
   if (cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess) chk(FL_INTERNAL);
@@ -733,6 +741,7 @@ int fl_context_destroy(fl_context* c) {
   cudaFree(c->b64);
   cudaFree(c->p64);
   cudaFree(c->p_nat);
+  cudaFree(c->p_keep);
   if (c->fcg_exec) cudaGraphExecDestroy(c->fcg_exec);
   if (c->work) cudaStreamDestroy(c->work);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
@@ -905,6 +914,7 @@ int fl_upload_particles(fl_context* c, const float* host, uint64_t count, void* 
   cudaStream_t s = (cudaStream_t)stream;
   c->cur = 0;
   c->count = count;
+  c->p_keep_valid = false;
   for (int k = 0; k < 15; ++k)
     FL_CUDA(cudaMemcpyAsync(c->pbuf[0] + (size_t)k * c->pcap, host + (size_t)k * count, sizeof(float) * count,
                             cudaMemcpyHostToDevice, s));

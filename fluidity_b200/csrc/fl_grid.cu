@@ -7,9 +7,11 @@
 // :627-657).
 //
 // Sort: the particle's cell key is (block ordinal * 512 + local cell), local cell
-// = z*64 + y*8 + x. Keys are radix-sorted (stable, so the order is reproducible
-// run to run) and the SoA arrays are permuted once. Cell counts come from an
-// atomic histogram and an exclusive scan gives cell_start. The reference sorts by
+// = z*64 + y*8 + x. A counting sort: an atomic histogram gives each particle an
+// arrival rank in its cell, an exclusive scan gives cell_start, original
+// indices are scattered to (cell_start + rank), each cell's indices are sorted
+// ascending -- the result equals a stable sort, so it is reproducible run to
+// run -- and the SoA arrays are gathered once. The reference sorts by
 // the signed bin floor((X - 1.5)/4) with CUB (native/cuda/liquid_arena_3d.cu:29-52);
 // with 8^3 blocks and per-step re-binning the bin is simply the containing cell.
 #include <cub/device/device_radix_sort.cuh>
@@ -51,8 +53,9 @@ __global__ void k_mark_blocks(GridView g, ParticlesView p, unsigned char* occ, D
   }
   // Most particles of a block mark the same byte: read first so only the
   // first visitors store (contended same-address stores serialize in L2).
-  unsigned char* o = occ + ((size_t)b[2] * g.bdim[1] + b[1]) * g.bdim[0] + b[0];
-  if (*o == 0) *o = 1;
+  const unsigned int idx = (unsigned int)(((size_t)b[2] * g.bdim[1] + b[1]) * g.bdim[0] + b[0]);
+  const unsigned int same = __match_any_sync(__activemask(), idx);
+  if ((threadIdx.x & 31) == __ffs(same) - 1 && occ[idx] == 0) occ[idx] = 1;
 }
 
 __global__ void k_flag_active(GridView g, const unsigned char* occ, int* flag, int total) {
@@ -107,7 +110,7 @@ __global__ void k_cell_keys(GridView g, ParticlesView p, unsigned int* keys, uns
   const unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
   if (i >= p.count) return;
   int cell[3];
-  unsigned int key = 0xffffffffu;
+  unsigned int key = 0xffffffffu, rank = 0;
   if (particle_cell(g, p, i, cell)) {
     int b[3], l[3];
     bool inside = true;
@@ -120,7 +123,7 @@ __global__ void k_cell_keys(GridView g, ParticlesView p, unsigned int* keys, uns
     const int o = inside ? g.table[((size_t)b[2] * g.bdim[1] + b[1]) * g.bdim[0] + b[0]] : -1;
     if (o >= 0) {
       key = (unsigned int)o * 512u + (unsigned int)(l[2] * 64 + l[1] * 8 + l[0]);
-      atomicAdd(&counts[key], 1);
+      rank = (unsigned int)atomicAdd(&counts[key], 1);
     } else {
       report_error(rep, kFailedPrecondition, i);
     }
@@ -128,7 +131,51 @@ __global__ void k_cell_keys(GridView g, ParticlesView p, unsigned int* keys, uns
     report_error(rep, kOutOfRange, i);
   }
   keys[i] = key;
-  index[i] = (unsigned int)i;
+  index[i] = rank;  // arrival rank within the cell (order not yet deterministic)
+}
+
+// Places each particle's original index at its cell's range start + arrival rank.
+__global__ void k_scatter_index(unsigned long long n, const unsigned int* keys, const unsigned int* rank,
+                                const int* cell_start, unsigned int* slots) {
+  const unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned int key = keys[i];
+  if (key == 0xffffffffu) return;
+  slots[cell_start[key] + rank[i]] = (unsigned int)i;
+}
+
+// Sorts each cell's original indices ascending, which makes the permutation
+// equal to a stable sort by cell (deterministic whatever the atomic order).
+__global__ void k_sort_cells(int ncell, const int* cell_start, unsigned int* slots) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int b = cell_start[c], e = cell_start[c + 1];
+  if (e - b < 2) return;
+  if (e - b <= 32) {
+    unsigned int v[32];
+    const int n = e - b;
+    for (int k = 0; k < n; ++k) v[k] = slots[b + k];
+    for (int k = 1; k < n; ++k) {
+      const unsigned int key = v[k];
+      int j = k - 1;
+      while (j >= 0 && v[j] > key) {
+        v[j + 1] = v[j];
+        --j;
+      }
+      v[j + 1] = key;
+    }
+    for (int k = 0; k < n; ++k) slots[b + k] = v[k];
+    return;
+  }
+  for (int k = b + 1; k < e; ++k) {  // crowded cell: in-place insertion sort
+    const unsigned int key = slots[k];
+    int j = k - 1;
+    while (j >= b && slots[j] > key) {
+      slots[j + 1] = slots[j];
+      --j;
+    }
+    slots[j + 1] = key;
+  }
 }
 
 __global__ void k_permute(ParticlesView in, ParticlesView out, const unsigned int* index) {
@@ -199,17 +246,17 @@ cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const Partic
   if (in.count > 0) {
     ++g_kernel_launches;
     k_cell_keys<<<grid_for(in.count, 256), 256, 0, s>>>(g, in, keys, index, counts, rep);
-    int end_bit = 1;
-    while (end_bit < 32 && ((size_t)1 << end_bit) < ncell + 1) ++end_bit;
-    size_t tb = temp_bytes;
-    ++g_library_launches;
-    cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys_alt, index, index_alt, (int)in.count, 0, end_bit, s);
-    ++g_kernel_launches;
-    k_permute<<<grid_for(in.count, 256), 256, 0, s>>>(in, out, index_alt);
   }
   size_t tb = temp_bytes;
   ++g_library_launches;
   cub::DeviceScan::ExclusiveSum(temp, tb, counts, cell_start, (int)(ncell + 1), s);
+  if (in.count > 0) {
+    g_kernel_launches += 3;
+    k_scatter_index<<<grid_for(in.count, 256), 256, 0, s>>>(in.count, keys, index, cell_start, index_alt);
+    k_sort_cells<<<grid_for(ncell, 256), 256, 0, s>>>((int)ncell, cell_start, index_alt);
+    k_permute<<<grid_for(in.count, 256), 256, 0, s>>>(in, out, index_alt);
+  }
+  (void)keys_alt;
   return cudaGetLastError();
 }
 

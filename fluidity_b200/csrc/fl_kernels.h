@@ -103,7 +103,8 @@ cudaError_t launch_g2p(const GridView& g, const ParticlesView& p, const int* cel
 template <typename T>
 cudaError_t launch_pressure_setup(const GridView& g, const int* cell_start, unsigned char* type,
                                   const float* const u_pred[3], double rhs_scale, MgHierarchy<T>& H, double* b64,
-                                  double* p64, double* partial, SolverState* st, cudaStream_t s);
+                                  double* p64, const float* p_prev, double* partial, SolverState* st,
+                                  cudaStream_t s);
 template <typename T>
 cudaError_t launch_apply_vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r, const MgOptions& opt,
                                 const int* done, cudaStream_t s);
@@ -114,7 +115,8 @@ template <typename T>
 cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, const MgOptions& opt, float* r_cur,
                                  float* r_prev, float* d_old, float* d_new, float* q, float* e, double* partial,
                                  SolverState* st, const int* done, cudaStream_t s);
-cudaError_t launch_export_pressure(const GridView& g, const double* p64, double* p_nat, cudaStream_t s);
+cudaError_t launch_export_pressure(const GridView& g, const double* p64, double* p_nat, float* p_keep,
+                                   cudaStream_t s);
 cudaError_t launch_to_rb(const GridView& g, const float* in_nat, float* out_rb, cudaStream_t s);
 template <typename T>
 cudaError_t launch_to_natural(const GridView& g, const MgHierarchy<T>& H, float* out_nat, cudaStream_t s);

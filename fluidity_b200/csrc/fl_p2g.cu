@@ -91,12 +91,17 @@ __device__ __forceinline__ void p2g_component(const GridView& g, const Particles
     axis_factors<false>(X[D1], cell[D1], h, __ldg(&p.c[3 * A + D1][q]), w1, t1);
     axis_factors<false>(X[D2], cell[D2], h, __ldg(&p.c[3 * A + D2][q]), w2, t2);
     if (!(isfinite(m) && isfinite(va))) report_error(rep, kInvalidArgument, (unsigned long long)q);
+    // Per node: W += wa*P and Q += wa*(P*q12) + (wa*ta)*P, with P the mass-scaled
+    // transverse weight product and q12 = v_a + the transverse affine terms.
+    float wta[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) wta[s] = wa[s] * ta[s];
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        const float w12 = m * (w1[j] * w2[k]);
-        const float q12 = va + (t1[j] + t2[k]);
+        const float P = m * (w1[j] * w2[k]);
+        const float PQ = P * (va + (t1[j] + t2[k]));
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
           int sx, sy, sz;
@@ -114,9 +119,8 @@ __device__ __forceinline__ void p2g_component(const GridView& g, const Particles
             sz = s;
           }
           const int slot = slot_index<A>(sx, sy, sz);
-          const float ww = w12 * wa[s];
-          accW[slot] += ww;
-          accQ[slot] = fmaf(ww, q12 + ta[s], accQ[slot]);
+          accW[slot] = fmaf(wa[s], P, accW[slot]);
+          accQ[slot] = fmaf(wa[s], PQ, fmaf(wta[s], P, accQ[slot]));
         }
       }
   }

@@ -203,10 +203,18 @@ __device__ __forceinline__ int nbr_type(const unsigned char* type, int id) {
   return type[id];
 }
 
+// Lattice-indexed cell id (stable across steps, unlike block ordinals).
+__device__ __forceinline__ long long lattice_cell(const GridView& g, int b, int l) {
+  const long long lb = ((long long)(g.coord[3 * b + 2] - g.blo[2]) * g.bdim[1] + (g.coord[3 * b + 1] - g.blo[1])) *
+                           g.bdim[0] +
+                       (g.coord[3 * b] - g.blo[0]);
+  return lb * 512 + l;
+}
+
 template <typename T>
 __global__ void k_setup_level0(GridView g, const unsigned char* type, const float* u0, const float* u1,
                                const float* u2, double rhs_scale, LevelPtrs<T> L0, double* b64, double* p64,
-                               double* partial, SolverState* st) {
+                               const float* p_prev, double* partial, SolverState* st) {
   __shared__ double red[kThreads / 32];
   const int n = g.nb * kBlockCells;
   const float* u[3] = {u0, u1, u2};
@@ -238,7 +246,7 @@ __global__ void k_setup_level0(GridView g, const unsigned char* type, const floa
     L0.diag[r] = fluid ? anchor + (float)__popc(mask & 63u) : 1.0f;
     const double rhs = fluid ? -rhs_scale * div : 0.0;
     b64[r] = rhs;
-    p64[r] = 0.0;
+    p64[r] = (fluid && p_prev != nullptr) ? (double)p_prev[lattice_cell(g, b, l)] : 0.0;
     bb += rhs * rhs;
   }
   const double s = block_sum<kThreads>(bb, red);
@@ -455,6 +463,211 @@ __global__ void __launch_bounds__(512)
               (g.coord[3 * cblk] - g.blo[0]);
       }
       cb[out] = sum;
+    }
+  }
+}
+
+
+// ----------------------------------------------------------------- tiled level-0 kernels
+
+// Face halo of block blk on level 0: for face f = 2a + (dir > 0), the 8x8
+// cells of the neighbouring block that touch it, indexed q = w*8 + u with
+// (u, w) the two transverse coordinates in increasing axis order. value(j)
+// maps a neighbour's natural cell id to the loaded value; missing blocks give 0.
+template <typename F>
+__device__ __forceinline__ void load_halo0(const GridView& g, int blk, float (*halo)[64], F value) {
+  for (int e = threadIdx.x; e < 384; e += blockDim.x) {
+    const int f = e >> 6, q = e & 63, a = f >> 1, dir = (f & 1) ? 1 : -1;
+    const int u = q & 7, w = q >> 3;
+    const int nbb = g.nbr27[blk * 27 + 13 + dir * (a == 0 ? 1 : (a == 1 ? 3 : 9))];
+    float v = 0.0f;
+    if (nbb >= 0) {
+      const int c = dir < 0 ? 7 : 0;
+      const int x = a == 0 ? c : u, y = a == 1 ? c : (a == 0 ? u : w), z = a == 2 ? c : w;
+      v = value(nbb * 512 + ((z << 6) | (y << 3) | x));
+    }
+    halo[f][q] = v;
+  }
+}
+
+// Value of the neighbour of natural local cell (x,y,z) across axis a / dir,
+// from the in-block tile or the face halo.
+__device__ __forceinline__ float tile_nbr0(const float* tile, const float (*halo)[64], int x, int y, int z, int a,
+                                           int dir) {
+  const int c = a == 0 ? x : (a == 1 ? y : z);
+  if (dir < 0 ? c > 0 : c < 7) {
+    const int step = 1 << (3 * a);
+    return tile[((z << 6) | (y << 3) | x) + dir * step];
+  }
+  const int q = a == 0 ? (z << 3) | y : (a == 1 ? (z << 3) | x : (y << 3) | x);
+  return halo[2 * a + (dir > 0 ? 1 : 0)][q];
+}
+
+__device__ __forceinline__ int parent1_of_nat(int j) {  // level-1 (4^3 per block) parent of a level-0 natural id
+  const int b = j >> 9, l = j & 511;
+  const int x = (l & 7) >> 1, y = ((l >> 3) & 7) >> 1, z = (l >> 6) >> 1;
+  return b * 64 + (z << 4) + (y << 2) + x;
+}
+
+// Red-black sweep of one colour on level 0 (MODE 0 plain, 2 prolongation
+// fused); MODE 1 (first sweep from zero) needs no neighbour values.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256)
+    k_smooth0_tiled(GridView g, LevelPtrs<T> lp, const float* __restrict__ b, int color, const T* __restrict__ xc,
+                    const int* done) {
+  if (*done) return;
+  __shared__ float tile[512];
+  __shared__ float halo[6][64];
+  const int blk = blockIdx.x, t = threadIdx.x;
+  const T* __restrict__ x = lp.x;
+  if (MODE != 1) {
+    const int oc = 1 - color;
+    const int lo = nat_of((oc << 8) | t);
+    float v = ld(&x[blk * 512 + (oc << 8) + t]);
+    if (MODE == 2) v += ld(&xc[parent1_of_nat(blk * 512 + lo)]);
+    tile[lo] = v;
+    load_halo0(g, blk, halo, [&](int j) {
+      float hv = ld(&x[rb_id(j)]);
+      if (MODE == 2) hv += ld(&xc[parent1_of_nat(j)]);
+      return hv;
+    });
+    __syncthreads();
+  }
+  const int i = blk * 512 + (color << 8) + t;
+  const unsigned m = lp.mask[i];
+  if (!(m & 64u)) return;
+  float s = b[i];
+  if (MODE != 1) {
+    const int l = nat_of((color << 8) | t);
+    const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+      for (int dir = -1; dir <= 1; dir += 2) {
+        if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
+        s += tile_nbr0(tile, halo, cx, cy, cz, a, dir);
+      }
+    }
+  }
+  st_T(&lp.x[i], s / lp.diag[i]);
+}
+
+// Level-0 residual restricted to level 1: all 512 cells of the block and its
+// face halos staged in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(512)
+    k_restrict0_tiled(GridView g, LevelPtrs<T> fp, const float* __restrict__ fb, float* __restrict__ cb,
+                      const int* done) {
+  if (*done) return;
+  __shared__ float tile[512];
+  __shared__ float halo[6][64];
+  __shared__ float r[512];
+  const int blk = blockIdx.x, t = threadIdx.x;
+  const int i = blk * 512 + t;  // solver (red-black) index
+  const int l = nat_of(t);
+  tile[l] = ld(&fp.x[i]);
+  load_halo0(g, blk, halo, [&](int j) { return ld(&fp.x[rb_id(j)]); });
+  __syncthreads();
+  const unsigned m = fp.mask[i];
+  float res = 0.0f;
+  if (m & 64u) {
+    const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
+    float ax = fp.diag[i] * tile[l];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+      for (int dir = -1; dir <= 1; dir += 2) {
+        if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
+        ax -= tile_nbr0(tile, halo, cx, cy, cz, a, dir);
+      }
+    }
+    res = fb[i] - ax;
+  }
+  r[l] = res;
+  __syncthreads();
+  if (t < 64) {
+    const int cx = t & 3, cy = (t >> 2) & 3, cz = t >> 4;
+    float sum = 0.0f;
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < 2; ++dx) sum += r[((2 * cz + dz) << 6) | ((2 * cy + dy) << 3) | (2 * cx + dx)];
+    cb[blk * 64 + t] = sum;
+  }
+}
+
+// d = z + beta d_old and q = A d for one block, d staged with its halo.
+// One CTA per block; d.q partials reduced by the last CTA.
+template <typename T>
+__global__ void __launch_bounds__(512)
+    k_direction_tiled(GridView g, LevelPtrs<T> L0, const T* __restrict__ z, const float* __restrict__ d_old,
+                      float* __restrict__ d_new, float* __restrict__ q, double* partial, SolverState* st) {
+  if (st->done) return;
+  __shared__ float tile[512];
+  __shared__ float halo[6][64];
+  __shared__ double red[16];
+  const int blk = blockIdx.x, t = threadIdx.x;
+  const float beta = (float)st->beta;
+  const bool first = st->inner_iter == 0;
+  const int i = blk * 512 + t;
+  const int l = nat_of(t);
+  const unsigned m = L0.mask[i];
+  const float di = (m & 64u) ? (first ? ld(&z[i]) : fmaf(beta, d_old[i], ld(&z[i]))) : 0.0f;
+  tile[l] = di;
+  load_halo0(g, blk, halo, [&](int j) {
+    const int r = rb_id(j);
+    return first ? ld(&z[r]) : fmaf(beta, d_old[r], ld(&z[r]));
+  });
+  __syncthreads();
+  float qi = 0.0f;
+  if (m & 64u) {
+    const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
+    float ax = L0.diag[i] * di;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+      for (int dir = -1; dir <= 1; dir += 2) {
+        if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
+        ax -= tile_nbr0(tile, halo, cx, cy, cz, a, dir);
+      }
+    }
+    qi = ax;
+  }
+  d_new[i] = di;
+  q[i] = qi;
+  double dq = (double)di * (double)qi;
+  dq = warp_sum(dq);
+  if ((t & 31) == 0) red[t >> 5] = dq;
+  __syncthreads();
+  if (t < 32) {
+    double v = t < 16 ? red[t] : 0.0;
+    v = warp_sum(v);
+    if (t == 0) partial[blk] = v;
+  }
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (t == 0) last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last) {
+    double acc = 0.0;
+    for (unsigned k = t; k < gridDim.x; k += blockDim.x) acc += partial[k];
+    acc = warp_sum(acc);
+    __syncthreads();
+    if ((t & 31) == 0) red[t >> 5] = acc;
+    __syncthreads();
+    if (t == 0) {
+      double tot = 0.0;
+      for (int w = 0; w < 16; ++w) tot += red[w];
+      if (!(tot > 0.0) || !isfinite(tot)) {
+        st->status = kAborted;
+        st->done = 1;
+      }
+      st->alpha = st->rz / tot;
+      st->rz_prev = st->rz;
+      st->ticket = 0;
     }
   }
 }
@@ -856,8 +1069,12 @@ __global__ void k_diagnostics(GridView g, const unsigned char* type, const doubl
 }
 
 // Solver (red-black) <-> natural level-0 layout conversions.
-__global__ void k_export_pressure(int n, const double* p64_rb, double* p_nat) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p_nat[i] = p64_rb[rb_id(i)];
+__global__ void k_export_pressure(GridView g, int n, const double* p64_rb, double* p_nat, float* p_keep) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double p = p64_rb[rb_id(i)];
+    p_nat[i] = p;
+    if (p_keep != nullptr) p_keep[lattice_cell(g, i >> 9, i & 511)] = (float)p;
+  }
 }
 template <typename T>
 __global__ void k_to_natural(int n, const T* x_rb, const unsigned char* fluid_rb, float* out_nat) {
@@ -891,7 +1108,17 @@ static void smooth_sparse(const GridView& g, const MgHierarchy<T>& H, int l, con
 template <typename T>
 static void smooth(const GridView& g, const MgHierarchy<T>& H, int l, const float* bl, int color, int mode,
                    const int* done, cudaStream_t s) {
-  if (l == 0) return smooth_sparse<T, 3>(g, H, l, bl, color, mode, done, s);
+  if (l == 0) {
+    ++g_kernel_launches;
+    const T* xc = H.ptr[1].x;
+    if (mode == 1)
+      k_smooth0_tiled<T, 1><<<g.nb, 256, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
+    else if (mode == 2)
+      k_smooth0_tiled<T, 2><<<g.nb, 256, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
+    else
+      k_smooth0_tiled<T, 0><<<g.nb, 256, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
+    return;
+  }
   if (l == 1) return smooth_sparse<T, 2>(g, H, l, bl, color, mode, done, s);
   if (l == 2) return smooth_sparse<T, 1>(g, H, l, bl, color, mode, done, s);
   const LevelDesc& D = H.desc[l];
@@ -916,7 +1143,7 @@ static void restrict_level(const GridView& g, const MgHierarchy<T>& H, int l, co
     const int bpc = 512 / S3;
     const unsigned grid = (unsigned)((g.nb + bpc - 1) / bpc);
     if (l == 0)
-      k_restrict_sparse<T, 3><<<grid, 512, 0, s>>>(g, H.ptr[0], bl, H.b[1], C.dim[0], C.dim[1], done);
+      k_restrict0_tiled<T><<<g.nb, 512, 0, s>>>(g, H.ptr[0], bl, H.b[1], done);
     else if (l == 1)
       k_restrict_sparse<T, 2><<<grid, 512, 0, s>>>(g, H.ptr[1], bl, H.b[2], C.dim[0], C.dim[1], done);
     else
@@ -961,13 +1188,14 @@ static void vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r0, 
 template <typename T>
 cudaError_t launch_pressure_setup(const GridView& g, const int* cell_start, unsigned char* type,
                                   const float* const u_pred[3], double rhs_scale, MgHierarchy<T>& H, double* b64,
-                                  double* p64, double* partial, SolverState* st, cudaStream_t s) {
+                                  double* p64, const float* p_prev, double* partial, SolverState* st,
+                                  cudaStream_t s) {
   const int n = g.nb * kBlockCells;
   ++g_kernel_launches;
   k_classify<<<blocks_for(n), kThreads, 0, s>>>(g, cell_start, type);
   ++g_kernel_launches;
   k_setup_level0<T><<<reduce_grid(n), kThreads, 0, s>>>(g, type, u_pred[0], u_pred[1], u_pred[2], rhs_scale,
-                                                         H.ptr[0], b64, p64, partial, st);
+                                                         H.ptr[0], b64, p64, p_prev, partial, st);
   for (int l = 1; l < H.levels; ++l) {
     ++g_kernel_launches;
     k_coarsen<T><<<blocks_for(H.desc[l].count), kThreads, 0, s>>>(g, H.desc[l - 1], H.ptr[l - 1], H.desc[l],
@@ -1006,7 +1234,7 @@ cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, con
   const unsigned grid = reduce_grid(n);
   g_kernel_launches += 3;
   k_dots<T><<<grid, kThreads, 0, s>>>(n, z, r_cur, r_prev, partial, st);
-  k_direction<T><<<grid, kThreads, 0, s>>>(g, H.ptr[0], z, d_old, d_new, q, partial, st);
+  k_direction_tiled<T><<<g.nb, 512, 0, s>>>(g, H.ptr[0], z, d_old, d_new, q, partial, st);
   k_update<<<grid, kThreads, 0, s>>>(n, d_new, q, r_cur, r_prev, e, partial, st);
   return cudaGetLastError();
 }
@@ -1031,10 +1259,11 @@ cudaError_t launch_correct_faces(const GridView& g, const unsigned char* type, c
   return cudaGetLastError();
 }
 
-cudaError_t launch_export_pressure(const GridView& g, const double* p64, double* p_nat, cudaStream_t s) {
+cudaError_t launch_export_pressure(const GridView& g, const double* p64, double* p_nat, float* p_keep,
+                                   cudaStream_t s) {
   const int n = g.nb * kBlockCells;
   ++g_kernel_launches;
-  k_export_pressure<<<reduce_grid(n), kThreads, 0, s>>>(n, p64, p_nat);
+  k_export_pressure<<<reduce_grid(n), kThreads, 0, s>>>(g, n, p64, p_nat, p_keep);
   return cudaGetLastError();
 }
 
@@ -1064,8 +1293,8 @@ void configure_pressure_kernels() {
 
 #define FL_INSTANTIATE(T)                                                                                         \
   template cudaError_t launch_pressure_setup<T>(const GridView&, const int*, unsigned char*, const float* const[3], \
-                                                double, MgHierarchy<T>&, double*, double*, double*, SolverState*,   \
-                                                cudaStream_t);                                                      \
+                                                double, MgHierarchy<T>&, double*, double*, const float*, double*,   \
+                                                SolverState*, cudaStream_t);                                        \
   template cudaError_t launch_apply_vcycle<T>(const GridView&, const MgHierarchy<T>&, const float*,                \
                                               const MgOptions&, const int*, cudaStream_t);                         \
   template cudaError_t launch_residual64<T>(const GridView&, const MgHierarchy<T>&, const double*, const double*,  \

@@ -101,7 +101,7 @@ typedef struct {
   int precision;      /* 0: FP32 V-cycle storage; 1: BF16 V-cycle storage */
   int max_iterations; /* total inner flexible-CG iterations */
   int max_refinements;
-  int pad;
+  int warm_start;     /* 1: start from the previous projection's pressure (InitializeMacPressure3D) */
   double rel_tol;    /* ||b - A p||_2 <= rel_tol * ||b||_2, checked in FP64 */
   double inner_rtol; /* inner FP32 solve reduction per refinement */
 } fl_pressure_options;
