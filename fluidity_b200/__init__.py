@@ -76,7 +76,8 @@ class PressureOptions(ctypes.Structure):
     _fields_ = [("levels", ctypes.c_int), ("pre_sweeps", ctypes.c_int), ("post_sweeps", ctypes.c_int),
                 ("coarse_sweeps", ctypes.c_int), ("precision", ctypes.c_int), ("max_iterations", ctypes.c_int),
                 ("max_refinements", ctypes.c_int), ("warm_start", ctypes.c_int), ("rel_tol", ctypes.c_double),
-                ("inner_rtol", ctypes.c_double)]
+                ("inner_rtol", ctypes.c_double), ("preconditioner", ctypes.c_int), ("stall_limit", ctypes.c_int),
+                ("stall_ratio", ctypes.c_double)]
 
 
 class PressureDiagnostics(ctypes.Structure):
@@ -85,7 +86,7 @@ class PressureDiagnostics(ctypes.Structure):
                 ("rhs_l2", ctypes.c_double), ("true_residual_l2", ctypes.c_double),
                 ("relative_residual", ctypes.c_double), ("reference_limit", ctypes.c_double),
                 ("max_volume_residual", ctypes.c_double), ("max_divergence", ctypes.c_double),
-                ("solve_ms", ctypes.c_double)]
+                ("solve_ms", ctypes.c_double), ("learned_iterations", ctypes.c_int), ("fell_back", ctypes.c_int)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -96,7 +97,10 @@ EXPORTS = [
     "fl_active_blocks", "fl_sort_particles_by_block", "fl_p2g", "fl_pressure_project", "fl_g2p", "fl_step",
     "fl_upload_particles", "fl_download_particles", "fl_state_particles", "fl_state_fields", "fl_step_host",
     "fl_deposit_mac_3d", "fl_deposit_mac_quanta_3d", "fl_gather_mac_3d", "fl_copy_to_host", "fl_copy_to_device",
-    "fl_runtime_info", "fl_apply_vcycle", "fl_step_timings", "fl_kernel_launches",
+    "fl_runtime_info", "fl_apply_vcycle", "fl_step_timings", "fl_kernel_launches", "fl_unet_param_count",
+    "fl_unet_create", "fl_unet_destroy", "fl_unet_init_params", "fl_unet_forward", "fl_unet_backward",
+    "fl_unet_masked_mse", "fl_adam_step", "fl_collect_training_pairs", "fl_set_learned_preconditioner",
+    "fl_apply_learned",
 ]
 
 _lib = None
@@ -146,6 +150,21 @@ def library():
         lib.fl_apply_vcycle.argtypes = [vp, vp, vp, ctypes.POINTER(PressureOptions), vp]
         lib.fl_step_timings.argtypes = [vp, _fp]
         lib.fl_kernel_launches.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_ulonglong)]
+        lib.fl_unet_param_count.restype = ctypes.c_int64
+        lib.fl_unet_param_count.argtypes = []
+        lib.fl_unet_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+        lib.fl_unet_destroy.argtypes = [vp]
+        lib.fl_unet_init_params.argtypes = [vp, ctypes.c_uint64, vp]
+        lib.fl_unet_forward.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
+        lib.fl_unet_backward.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
+        lib.fl_unet_masked_mse.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp, vp]
+        lib.fl_adam_step.argtypes = [vp, vp, vp, vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                     ctypes.c_float, ctypes.c_float, vp]
+        lib.fl_collect_training_pairs.argtypes = [vp, ctypes.POINTER(TransferParams), ctypes.POINTER(PressureOptions),
+                                                  _ip, ctypes.c_int, vp, vp, vp, ctypes.c_uint64,
+                                                  ctypes.POINTER(ctypes.c_uint64)]
+        lib.fl_set_learned_preconditioner.argtypes = [vp, vp, vp]
+        lib.fl_apply_learned.argtypes = [vp, vp, vp, vp]
         _lib = lib
     return _lib
 
@@ -165,9 +184,11 @@ def runtime_info():
 def default_pressure_options(precision: int = 0, rel_tol: float = 1e-6, levels: int = 0, pre: int = 2,
                              post: int = 2, coarse_sweeps: int = 16, max_iterations: int = 400,
                              max_refinements: int = 6, inner_rtol: float = 1e-4,
-                             warm_start: int = 0) -> PressureOptions:
+                             warm_start: int = 0, preconditioner: int = 0, stall_limit: int = 3,
+                             stall_ratio: float = 0.9) -> PressureOptions:
     o = PressureOptions()
     o.warm_start = warm_start
+    o.preconditioner, o.stall_limit, o.stall_ratio = preconditioner, stall_limit, stall_ratio
     o.levels, o.pre_sweeps, o.post_sweeps, o.coarse_sweeps = levels, pre, post, coarse_sweeps
     o.precision, o.max_iterations, o.max_refinements = precision, max_iterations, max_refinements
     o.rel_tol, o.inner_rtol = rel_tol, inner_rtol
@@ -335,6 +356,77 @@ class LiquidContext:
         p = Particles()
         _check(library().fl_state_particles(self._ctx, ctypes.byref(p)), "fl_state_particles")
         return p
+
+    def collect_training_pairs(self, params: TransferParams, options: PressureOptions, iterations, inputs, targets,
+                               masks) -> int:
+        """(residual, error) items of the last step's projection into device tensors
+        inputs (cap, 2, 10, 10, 10), targets and masks (cap, 512); returns the count."""
+        its = np.ascontiguousarray(iterations, np.int32)
+        cap = min(inputs.shape[0], targets.shape[0], masks.shape[0])
+        written = ctypes.c_uint64()
+        _check(library().fl_collect_training_pairs(self._ctx, ctypes.byref(params), ctypes.byref(options),
+                                                   its.ctypes.data_as(_ip), len(its), inputs.data_ptr(),
+                                                   targets.data_ptr(), masks.data_ptr(), cap, ctypes.byref(written)),
+               "fl_collect_training_pairs")
+        return written.value
+
+    def set_learned_preconditioner(self, params, stream=None):
+        """Loads FP32 network parameters (a device tensor) for options.preconditioner = 1."""
+        _check(library().fl_set_learned_preconditioner(self._ctx, params.data_ptr(), stream),
+               "fl_set_learned_preconditioner")
+
+    def apply_learned(self, r, z, stream=None):
+        """z = U(r) on the cells of the last sort (device tensors, active_blocks*512 floats, natural order)."""
+        _check(library().fl_apply_learned(self._ctx, r.data_ptr(), z.data_ptr(), stream), "fl_apply_learned")
+
+
+class UNet:
+    """Training handle of the learned block preconditioner (fl_unet_*). Tensors are
+    device tensors (torch, float32, contiguous); calls are ordered on `stream`."""
+
+    def __init__(self, max_batch: int):
+        h = ctypes.c_void_p()
+        _check(library().fl_unet_create(int(max_batch), ctypes.byref(h)), "fl_unet_create")
+        self._h = h
+        self.max_batch = int(max_batch)
+
+    @staticmethod
+    def param_count() -> int:
+        return int(library().fl_unet_param_count())
+
+    @staticmethod
+    def init_params(params, seed: int = 0, stream=None):
+        _check(library().fl_unet_init_params(params.data_ptr(), int(seed), stream), "fl_unet_init_params")
+
+    def forward(self, params, inputs, outputs, stream=None):
+        _check(library().fl_unet_forward(self._h, params.data_ptr(), inputs.data_ptr(), inputs.shape[0],
+                                         outputs.data_ptr(), stream), "fl_unet_forward")
+
+    def backward(self, params, grad_outputs, grads, stream=None):
+        _check(library().fl_unet_backward(self._h, params.data_ptr(), grad_outputs.data_ptr(), grad_outputs.shape[0],
+                                          grads.data_ptr(), stream), "fl_unet_backward")
+
+    @staticmethod
+    def masked_mse(outputs, targets, masks, loss, grad_outputs, stream=None):
+        _check(library().fl_unet_masked_mse(outputs.data_ptr(), targets.data_ptr(), masks.data_ptr(), outputs.shape[0],
+                                            loss.data_ptr(), grad_outputs.data_ptr(), stream), "fl_unet_masked_mse")
+
+    @staticmethod
+    def adam_step(params, grads, m, v, step: int, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999,
+                  eps: float = 1e-8, stream=None):
+        _check(library().fl_adam_step(params.data_ptr(), grads.data_ptr(), m.data_ptr(), v.data_ptr(), params.numel(),
+                                      int(step), lr, beta1, beta2, eps, stream), "fl_adam_step")
+
+    def close(self):
+        if self._h:
+            library().fl_unet_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def kernel_launches():

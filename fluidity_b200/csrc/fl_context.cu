@@ -23,6 +23,7 @@
 #include "../../include/fluidity_b200.h"
 #include "fl_internal.cuh"
 #include "fl_kernels.h"
+#include "fl_unet.h"
 
 namespace fl {
 unsigned long long g_kernel_launches = 0;
@@ -101,6 +102,17 @@ struct fl_context {
   double* p_nat = nullptr;
   float* p_keep = nullptr;  // last pressure per lattice cell (warm start across topology changes)
   bool p_keep_valid = false;
+  // learned preconditioner: FP32 parameters, per-block scales, the inference
+  // activations (grown on demand to the active block count) and its own
+  // one-iteration FCG graph
+  float* nn_params = nullptr;
+  bool nn_ready = false;
+  float* nn_scale = nullptr;
+  float* nn_act = nullptr;
+  long long nn_act_items = 0;
+  cudaGraphExec_t fcg_nn_exec = nullptr;
+  unsigned long long fcg_nn_kernels = 0;
+  PrecondHook nn_hook{};
 };
 
 namespace {
@@ -248,7 +260,15 @@ int make_hierarchy(fl_context* c, int levels, MgHierarchy<T>& H) {
   return FL_OK;
 }
 
-__global__ void k_init_state(SolverState* st, double rel_tol, double inner_rtol, int inner_max) {
+__global__ void k_init_state(SolverState* st, double rel_tol, double inner_rtol, int inner_max, int learned,
+                             int stall_limit, double stall_ratio) {
+  st->rr_best = INFINITY;
+  st->stall_ratio2 = stall_ratio * stall_ratio;
+  st->learned = learned;
+  st->stall_limit = stall_limit;
+  st->stalls = 0;
+  st->fallback = 0;
+  st->learned_iter = 0;
   st->target = 0.0;
   st->inner_rtol = inner_rtol;
   st->inner_max = inner_max;
@@ -274,17 +294,30 @@ __global__ void k_set_inner_budget(SolverState* st, int inner_max) {
 // Captures two flexible-CG iterations (V-cycle + 3 CG kernels each, r/d
 // buffers swapping roles) into one graph and updates the executable graph in
 // place when only launch parameters changed (the block count changes per step).
+// The learned variant runs the network in place of the V-cycle. The host picks
+// the graph per replay, so the V-cycle takes over at the first replay after the
+// device flags the fallback (at most one further learned iteration).
 template <typename T>
-int capture_fcg(fl_context* c, const GridView& g, const MgHierarchy<T>& H, const MgOptions& mo) {
+int capture_fcg(fl_context* c, const GridView& g, const MgHierarchy<T>& H, const MgOptions& mo, bool learned,
+                cudaGraphExec_t* exec, unsigned long long* kernels) {
   cudaGraph_t graph = nullptr;
   const unsigned long long before = g_kernel_launches;
+  const int a = 0, b = 1;
   FL_CUDA(cudaStreamBeginCapture(c->work, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e1 = launch_fcg_iteration<T>(g, H, mo, c->r[0], c->r[1], c->d[0], c->d[1], c->q, c->e, c->partial,
-                                           c->st, &c->st->done, c->work);
-  cudaError_t e2 = launch_fcg_iteration<T>(g, H, mo, c->r[1], c->r[0], c->d[1], c->d[0], c->q, c->e, c->partial,
-                                           c->st, &c->st->done, c->work);
+  cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
+  if (learned) {
+    e1 = launch_fcg_iteration<T>(g, H, mo, c->r[a], c->r[b], c->d[a], c->d[b], c->q, c->e, c->partial, c->st,
+                                 &c->st->done, c->work, &c->nn_hook);
+    e2 = launch_fcg_iteration<T>(g, H, mo, c->r[b], c->r[a], c->d[b], c->d[a], c->q, c->e, c->partial, c->st,
+                                 &c->st->done, c->work, &c->nn_hook);
+  } else {
+    e1 = launch_fcg_iteration<T>(g, H, mo, c->r[a], c->r[b], c->d[a], c->d[b], c->q, c->e, c->partial, c->st,
+                                 &c->st->done, c->work);
+    e2 = launch_fcg_iteration<T>(g, H, mo, c->r[b], c->r[a], c->d[b], c->d[a], c->q, c->e, c->partial, c->st,
+                                 &c->st->done, c->work);
+  }
   cudaError_t e3 = cudaStreamEndCapture(c->work, &graph);
-  c->fcg_graph_kernels = g_kernel_launches - before;
+  *kernels = g_kernel_launches - before;
   g_kernel_launches = before;  // counted again at every replay
   if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
     if (graph) cudaGraphDestroy(graph);
@@ -292,23 +325,52 @@ int capture_fcg(fl_context* c, const GridView& g, const MgHierarchy<T>& H, const
     return FL_INTERNAL;
   }
   bool updated = false;
-  if (c->fcg_exec) {
+  if (*exec) {
     cudaGraphExecUpdateResultInfo info;
-    updated = cudaGraphExecUpdate(c->fcg_exec, graph, &info) == cudaSuccess;
+    updated = cudaGraphExecUpdate(*exec, graph, &info) == cudaSuccess;
     if (!updated) {
       cudaGetLastError();
-      cudaGraphExecDestroy(c->fcg_exec);
-      c->fcg_exec = nullptr;
+      cudaGraphExecDestroy(*exec);
+      *exec = nullptr;
     }
   }
   if (!updated) {
-    if (cudaGraphInstantiate(&c->fcg_exec, graph, 0) != cudaSuccess) {
+    if (cudaGraphInstantiate(exec, graph, 0) != cudaSuccess) {
       cudaGraphDestroy(graph);
-      c->fcg_exec = nullptr;
+      *exec = nullptr;
       return FL_INTERNAL;
     }
   }
   cudaGraphDestroy(graph);
+  return FL_OK;
+}
+
+// Learned preconditioner application z = s * U(r / s) per block (gather of the
+// block + halo window, batched forward over all active blocks, scatter to the
+// level-0 layout). Captured into the learned FCG graph.
+template <typename T>
+cudaError_t nn_apply(void* vc, const float* r, void* z, cudaStream_t s) {
+  fl_context* c = static_cast<fl_context*>(vc);
+  const GridView g = view(c);
+  const UNetCache C = unet_cache_layout(g.nb);
+  float* x = c->nn_act + C.x;
+  cudaError_t e = unet_gather(g, r, c->type, nullptr, g.nb, x, c->nn_scale, s);
+  if (e == cudaSuccess) e = unet_forward(c->nn_params, x, g.nb, c->nn_act, nullptr, s);
+  if (e == cudaSuccess) e = unet_scatter<T>(g.nb, c->nn_act + C.y, c->nn_scale, c->type, static_cast<T*>(z), true, s);
+  return e;
+}
+
+int nn_reserve(fl_context* c, long long items) {
+  if (items <= c->nn_act_items) return FL_OK;
+  cudaFree(c->nn_act);
+  c->nn_act = nullptr;
+  c->nn_act_items = 0;
+  const long long want = std::min<long long>(items + items / 4 + 16, c->lattice);
+  if (cudaMalloc(&c->nn_act, sizeof(float) * (size_t)unet_cache_layout((int)want).activations) != cudaSuccess) {
+    cudaGetLastError();
+    return FL_RESOURCE_EXHAUSTED;
+  }
+  c->nn_act_items = want;
   return FL_OK;
 }
 
@@ -327,12 +389,24 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   const double vel_scale = dt / (rho * h);    // u += vel_scale * (p_tail - p_head)
   const long long n = (long long)c->nb * kBlockCells;
   MgOptions mo{std::max(1, opt->pre_sweeps), std::max(1, opt->post_sweeps), std::max(1, opt->coarse_sweeps)};
+  const bool use_nn = opt->preconditioner == 1;
+  if (opt->preconditioner != 0 && !use_nn) return FL_INVALID_ARGUMENT;
+  if (use_nn) {
+    if (!c->nn_ready) return FL_FAILED_PRECONDITION;
+    st = nn_reserve(c, c->nb);
+    if (st != FL_OK) return st;
+    c->nn_hook.apply = nn_apply<T>;
+    c->nn_hook.ctx = c;
+  }
+  const int stall_limit = opt->stall_limit > 0 ? opt->stall_limit : 3;
+  const double stall_ratio = opt->stall_ratio > 0.0 ? opt->stall_ratio : 0.9;
   cudaStream_t s = c->work;
   FL_CUDA(cudaEventRecord(c->ev_in, user));
   FL_CUDA(cudaStreamWaitEvent(s, c->ev_in, 0));
   FL_CUDA(cudaEventRecord(c->ev0, s));
   ++g_kernel_launches;
-  k_init_state<<<1, 1, 0, s>>>(c->st, opt->rel_tol, opt->inner_rtol, opt->max_iterations);
+  k_init_state<<<1, 1, 0, s>>>(c->st, opt->rel_tol, opt->inner_rtol, opt->max_iterations, use_nn ? 1 : 0,
+                               stall_limit, stall_ratio);
   const float* p_prev = (opt->warm_start && c->p_keep_valid) ? c->p_keep : nullptr;
   FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, u_pred, rhs_scale, H, c->b64, c->p64, p_prev,
                                    c->partial, c->st, s));
@@ -360,13 +434,15 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
     ++g_kernel_launches;
     k_set_inner_budget<<<1, 1, 0, s>>>(c->st, opt->max_iterations - total);
     if (!captured) {
-      st = capture_fcg<T>(c, g, H, mo);
+      st = capture_fcg<T>(c, g, H, mo, false, &c->fcg_exec, &c->fcg_graph_kernels);
+      if (st == FL_OK && use_nn) st = capture_fcg<T>(c, g, H, mo, true, &c->fcg_nn_exec, &c->fcg_nn_kernels);
       if (st != FL_OK) return st;
       captured = true;
     }
     for (;;) {
-      FL_CUDA(cudaGraphLaunch(c->fcg_exec, s));
-      g_kernel_launches += c->fcg_graph_kernels;
+      const bool nn_now = use_nn && !c->st_host->fallback;
+      FL_CUDA(cudaGraphLaunch(nn_now ? c->fcg_nn_exec : c->fcg_exec, s));
+      g_kernel_launches += nn_now ? c->fcg_nn_kernels : c->fcg_graph_kernels;
       FL_CUDA(cudaMemcpyAsync(c->st_host, c->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
       FL_CUDA(cudaStreamSynchronize(s));
       if (c->st_host->done) break;
@@ -406,6 +482,8 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
     diag->max_volume_residual = S.res64 * k_ref / (h * h * h);
     diag->max_divergence = S.div_max / h;
     diag->solve_ms = ms;
+    diag->learned_iterations = S.learned_iter;
+    diag->fell_back = S.fallback;
   }
   if (status != FL_OK) return status;
   return converged ? FL_OK : FL_ABORTED;
@@ -421,7 +499,7 @@ int apply_vcycle(fl_context* c, const float* r, float* z, const fl_pressure_opti
   MgOptions mo{std::max(1, opt->pre_sweeps), std::max(1, opt->post_sweeps), std::max(1, opt->coarse_sweeps)};
   const long long n = (long long)c->nb * kBlockCells;
   ++g_kernel_launches;
-  k_init_state<<<1, 1, 0, s>>>(c->st, 1e-6, 1e-4, 1);
+  k_init_state<<<1, 1, 0, s>>>(c->st, 1e-6, 1e-4, 1, 0, 3, 0.9);
   const float* up[3] = {c->u_pred[0], c->u_pred[1], c->u_pred[2]};
   for (int a = 0; a < 3; ++a) FL_CUDA(cudaMemsetAsync(c->u_pred[a], 0, sizeof(float) * n, s));
   FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, up, 1.0, H, c->b64, c->p64, nullptr, c->partial,
@@ -743,6 +821,10 @@ int fl_context_destroy(fl_context* c) {
   cudaFree(c->p_nat);
   cudaFree(c->p_keep);
   if (c->fcg_exec) cudaGraphExecDestroy(c->fcg_exec);
+  if (c->fcg_nn_exec) cudaGraphExecDestroy(c->fcg_nn_exec);
+  cudaFree(c->nn_params);
+  cudaFree(c->nn_scale);
+  cudaFree(c->nn_act);
   if (c->work) cudaStreamDestroy(c->work);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
@@ -1212,6 +1294,109 @@ int fl_gather_mac_3d(const double origin[3], double h, const int32_t* blocks, ui
   }
   cudaFree(out);
   return st;
+}
+
+int fl_set_learned_preconditioner(fl_context* c, const float* params, void* stream) {
+  if (!c || !params) return FL_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long np = unet_layout().total;
+  if (!c->nn_params && cudaMalloc(&c->nn_params, sizeof(float) * np) != cudaSuccess) {
+    cudaGetLastError();
+    return FL_RESOURCE_EXHAUSTED;
+  }
+  if (!c->nn_scale && cudaMalloc(&c->nn_scale, sizeof(float) * (size_t)c->lattice) != cudaSuccess) {
+    cudaGetLastError();
+    return FL_RESOURCE_EXHAUSTED;
+  }
+  configure_unet_kernels();
+  FL_CUDA(cudaMemcpyAsync(c->nn_params, params, sizeof(float) * np, cudaMemcpyDeviceToDevice, s));
+  FL_CUDA(cudaStreamSynchronize(s));
+  c->nn_ready = true;
+  return FL_OK;
+}
+
+int fl_apply_learned(fl_context* c, const float* r, float* z, void* stream) {
+  if (!c || !r || !z) return FL_INVALID_ARGUMENT;
+  if (!c->nn_ready) return FL_FAILED_PRECONDITION;
+  if (c->nb == 0) return FL_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = nn_reserve(c, c->nb);
+  if (st != FL_OK) return st;
+  GridView g = view(c);
+  const UNetCache C = unet_cache_layout(g.nb);
+  FL_CUDA(launch_classify(g, c->cell_start, c->type, s));
+  FL_CUDA(launch_to_rb(g, r, c->r[0], s));
+  FL_CUDA(unet_gather(g, c->r[0], c->type, nullptr, g.nb, c->nn_act + C.x, c->nn_scale, s));
+  FL_CUDA(unet_forward(c->nn_params, c->nn_act + C.x, g.nb, c->nn_act, nullptr, s));
+  FL_CUDA(unet_scatter<float>(g.nb, c->nn_act + C.y, c->nn_scale, c->type, z, false, s));
+  FL_CUDA(cudaStreamSynchronize(s));
+  return FL_OK;
+}
+
+int fl_collect_training_pairs(fl_context* c, const fl_transfer_params* tp, const fl_pressure_options* opt,
+                              const int32_t* iterations, int iteration_count, float* inputs, float* targets,
+                              float* target_mask, uint64_t capacity, uint64_t* written) {
+  if (!c || !tp || !opt || !iterations || iteration_count <= 0 || !inputs || !targets || !target_mask || !written)
+    return FL_INVALID_ARGUMENT;
+  *written = 0;
+  if (c->nb == 0 || capacity == 0) return FL_OK;
+  fl_pressure_options o = *opt;
+  o.warm_start = 0;
+  o.preconditioner = 0;
+  const float* up[3] = {c->u_pred[0], c->u_pred[1], c->u_pred[2]};
+  float* un[3] = {c->u_new[0], c->u_new[1], c->u_new[2]};
+  int st = fl_pressure_project(c, up, un, tp, &o, nullptr, nullptr, nullptr);
+  if (st != FL_OK) return st;
+  const int nb = c->nb;
+  const size_t n = (size_t)nb * kBlockCells;
+  double* p_star = nullptr;
+  int* dlist = nullptr;
+  float* scale = nullptr;
+  if (cudaMalloc(&p_star, sizeof(double) * n) != cudaSuccess || cudaMalloc(&dlist, sizeof(int) * nb) != cudaSuccess ||
+      cudaMalloc(&scale, sizeof(float) * nb) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(p_star);
+    cudaFree(dlist);
+    return FL_RESOURCE_EXHAUSTED;
+  }
+  cudaStream_t s = c->work;
+  GridView g = view(c);
+  std::vector<int> flags(nb), list;
+  cudaError_t e = cudaMemcpyAsync(p_star, c->p64, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = unet_block_has_fluid(nb, c->type, dlist, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(flags.data(), dlist, sizeof(int) * nb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  for (int b = 0; b < nb; ++b)
+    if (flags[b]) list.push_back(b);
+  if (e == cudaSuccess && !list.empty())
+    e = cudaMemcpy(dlist, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice);
+  uint64_t w = 0;
+  for (int k = 0; k < iteration_count && e == cudaSuccess && st == FL_OK && w < capacity && !list.empty(); ++k) {
+    fl_pressure_options ok = o;
+    ok.max_iterations = std::max(0, (int)iterations[k]);
+    const int rc = fl_pressure_project(c, up, un, tp, &ok, nullptr, nullptr, nullptr);
+    if (rc != FL_OK && rc != FL_ABORTED) {
+      st = rc;
+      break;
+    }
+    // r[0] holds b - A p_k of the capped solve (its last residual evaluation)
+    const int take = (int)std::min<uint64_t>(list.size(), capacity - w);
+    e = unet_gather(g, c->r[0], c->type, dlist, take, inputs + w * 2000, scale, s);
+    if (e == cudaSuccess)
+      e = unet_targets(g, p_star, c->p64, c->type, dlist, take, scale, targets + w * 512, target_mask + w * 512, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    w += take;
+  }
+  cudaFree(p_star);
+  cudaFree(dlist);
+  cudaFree(scale);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return FL_INTERNAL;
+  }
+  if (st != FL_OK) return st;
+  *written = w;
+  return FL_OK;
 }
 
 }  // extern "C"

@@ -90,6 +90,23 @@ __device__ __forceinline__ int compiled_arch() {
 #endif
 }
 
+// Level-0 solver layout (red-black): inside each block the 256 cells of colour
+// c = (x+y+z)&1 occupy [c*256, c*256+256) in (z, y, x/2) order, so a colour
+// sweep reads and writes contiguous memory. Face and particle arrays keep the
+// natural (z*64 + y*8 + x) order.
+__device__ __forceinline__ int rb_of(int l) {
+  const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
+  return (((x + y + z) & 1) << 8) | (z << 5) | (y << 2) | (x >> 1);
+}
+__device__ __forceinline__ int nat_of(int r) {
+  const int c = r >> 8, j = r & 255;
+  const int z = j >> 5, y = (j >> 2) & 7, xh = j & 3;
+  return (z << 6) | (y << 3) | (2 * xh + ((y + z + c) & 1));
+}
+__device__ __forceinline__ int rb_id(int natural_id) {
+  return natural_id < 0 ? natural_id : ((natural_id & ~511) | rb_of(natural_id & 511));
+}
+
 // Storage helpers for FP32 or BF16 V-cycle vectors.
 template <typename T>
 __device__ __forceinline__ float ld(const T* p) {

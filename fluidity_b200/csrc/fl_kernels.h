@@ -67,6 +67,14 @@ struct SolverState {
   double stop2;
   double rz, rz_prev, beta, alpha, rr;
   double div_l2, div_max;
+  double rr_best;       // learned preconditioner: best ||r||^2 so far
+  double stall_ratio2;  // an iteration stalls unless ||r||^2 < stall_ratio2 * rr_best
+  int learned;          // 1: the learned preconditioner is active until `fallback`
+  int stall_limit;
+  int stalls;
+  int fallback;
+  int learned_iter;
+  int pad2;
   int converged;
   int done;
   int status;
@@ -111,13 +119,22 @@ cudaError_t launch_apply_vcycle(const GridView& g, const MgHierarchy<T>& H, cons
 template <typename T>
 cudaError_t launch_residual64(const GridView& g, const MgHierarchy<T>& H, const double* b64, const double* p64,
                               float* r, float* e, double* partial, SolverState* st, cudaStream_t s);
+// Replacement preconditioner z = M(r) launched in place of the V-cycle (z is the
+// level-0 vector H.ptr[0].x, of the hierarchy's storage type).
+struct PrecondHook {
+  cudaError_t (*apply)(void* ctx, const float* r, void* z, cudaStream_t s);
+  void* ctx;
+};
+
 template <typename T>
 cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, const MgOptions& opt, float* r_cur,
                                  float* r_prev, float* d_old, float* d_new, float* q, float* e, double* partial,
-                                 SolverState* st, const int* done, cudaStream_t s);
+                                 SolverState* st, const int* done, cudaStream_t s, const PrecondHook* hook = nullptr);
 cudaError_t launch_export_pressure(const GridView& g, const double* p64, double* p_nat, float* p_keep,
                                    cudaStream_t s);
 cudaError_t launch_to_rb(const GridView& g, const float* in_nat, float* out_rb, cudaStream_t s);
+// Cell types of the last sort: 0 solid, 1 fluid (holds particles), 2 air.
+cudaError_t launch_classify(const GridView& g, const int* cell_start, unsigned char* type, cudaStream_t s);
 template <typename T>
 cudaError_t launch_to_natural(const GridView& g, const MgHierarchy<T>& H, float* out_nat, cudaStream_t s);
 void configure_pressure_kernels();

@@ -141,22 +141,6 @@ __device__ __forceinline__ int parent_s(const GridView& g, int j, int cdx, int c
   return ((g.coord[3 * b + 2] - g.blo[2]) * cdy + (g.coord[3 * b + 1] - g.blo[1])) * cdx + (g.coord[3 * b] - g.blo[0]);
 }
 
-// Level-0 solver layout (red-black): inside each block the 256 cells of colour
-// c = (x+y+z)&1 occupy [c*256, c*256+256) in (z, y, x/2) order, so a colour
-// sweep reads and writes contiguous memory. Face and particle arrays keep the
-// natural (z*64 + y*8 + x) order.
-__device__ __forceinline__ int rb_of(int l) {
-  const int x = l & 7, y = (l >> 3) & 7, z = l >> 6;
-  return (((x + y + z) & 1) << 8) | (z << 5) | (y << 2) | (x >> 1);
-}
-__device__ __forceinline__ int nat_of(int r) {
-  const int c = r >> 8, j = r & 255;
-  const int z = j >> 5, y = (j >> 2) & 7, xh = j & 3;
-  return (z << 6) | (y << 3) | (2 * xh + ((y + z + c) & 1));
-}
-__device__ __forceinline__ int rb_id(int natural_id) {
-  return natural_id < 0 ? natural_id : ((natural_id & ~511) | rb_of(natural_id & 511));
-}
 
 // ----------------------------------------------------------------- level-0 setup (box scene)
 
@@ -868,6 +852,7 @@ __global__ void k_residual64(GridView g, LevelPtrs<T> L0, const double* b64, con
       st->stop2 = stop * stop;
       st->inner_iter = 0;
       st->done = st->converged;
+      if (t < st->rr_best) st->rr_best = t;
       st->ticket = 0;
     }
   }
@@ -896,7 +881,12 @@ __global__ void k_dots(int n, const T* __restrict__ z, const float* __restrict__
     const double t1 = finish_sum(partial, 2, 1, red);
     if (threadIdx.x == 0) {
       if (!(t0 > 0.0) || !isfinite(t0)) {
-        st->status = kAborted;
+        // A learned correction that is not a descent direction ends this inner
+        // solve and hands the rest of the projection to the V-cycle.
+        if (st->learned && !st->fallback)
+          st->fallback = 1;
+        else
+          st->status = kAborted;
         st->done = 1;
       }
       st->beta = st->inner_iter == 0 ? 0.0 : (t0 - t1) / st->rz_prev;
@@ -975,6 +965,12 @@ __global__ void k_update(int n, const float* __restrict__ d, const float* __rest
       st->rr = t;
       st->inner_iter += 1;
       st->total_iter += 1;
+      if (st->learned && !st->fallback) {
+        st->learned_iter += 1;
+        st->stalls = t < st->stall_ratio2 * st->rr_best ? 0 : st->stalls + 1;
+        if (st->stalls >= st->stall_limit) st->fallback = 1;
+      }
+      if (t < st->rr_best) st->rr_best = t;
       if (t <= st->stop2 || !isfinite(t) || st->inner_iter >= st->inner_max) st->done = 1;
       if (!isfinite(t)) st->status = kOutOfRange;
       st->ticket = 0;
@@ -1185,6 +1181,13 @@ static void vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r0, 
   }
 }
 
+cudaError_t launch_classify(const GridView& g, const int* cell_start, unsigned char* type, cudaStream_t s) {
+  const int n = g.nb * kBlockCells;
+  ++g_kernel_launches;
+  k_classify<<<blocks_for(n), kThreads, 0, s>>>(g, cell_start, type);
+  return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_pressure_setup(const GridView& g, const int* cell_start, unsigned char* type,
                                   const float* const u_pred[3], double rhs_scale, MgHierarchy<T>& H, double* b64,
@@ -1227,9 +1230,14 @@ cudaError_t launch_residual64(const GridView& g, const MgHierarchy<T>& H, const 
 template <typename T>
 cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, const MgOptions& opt, float* r_cur,
                                  float* r_prev, float* d_old, float* d_new, float* q, float* e, double* partial,
-                                 SolverState* st, const int* done, cudaStream_t s) {
+                                 SolverState* st, const int* done, cudaStream_t s, const PrecondHook* hook) {
   const int n = g.nb * kBlockCells;
-  vcycle<T>(g, H, r_cur, opt, done, s);
+  if (hook != nullptr) {
+    const cudaError_t e = hook->apply(hook->ctx, r_cur, H.ptr[0].x, s);
+    if (e != cudaSuccess) return e;
+  } else {
+    vcycle<T>(g, H, r_cur, opt, done, s);
+  }
   const T* z = H.ptr[0].x;
   const unsigned grid = reduce_grid(n);
   g_kernel_launches += 3;
@@ -1301,7 +1309,7 @@ void configure_pressure_kernels() {
                                             float*, float*, double*, SolverState*, cudaStream_t);                  \
   template cudaError_t launch_fcg_iteration<T>(const GridView&, const MgHierarchy<T>&, const MgOptions&, float*,   \
                                                float*, float*, float*, float*, float*, double*, SolverState*,      \
-                                               const int*, cudaStream_t);                                          \
+                                               const int*, cudaStream_t, const PrecondHook*);                      \
   template cudaError_t launch_to_natural<T>(const GridView&, const MgHierarchy<T>&, float*, cudaStream_t);
 
 FL_INSTANTIATE(float)

@@ -1,0 +1,54 @@
+// Learned block preconditioner: parameter layout, training cache layout and launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fl_internal.cuh"
+
+namespace fl {
+
+constexpr int kUNetLayers = 10;  // e1a e1b e2a e2b bt u2 d2 u1 d1 out
+
+struct UNetLayout {
+  int cin[kUNetLayers];
+  int cout[kUNetLayers];
+  int taps[kUNetLayers];          // 27 (3x3x3) or 1 (1x1)
+  long long offset[kUNetLayers];  // weight offset (floats)
+  long long bias[kUNetLayers];    // bias offset (floats)
+  long long total;
+};
+
+// Offsets (floats) of each activation / scratch tensor in a training cache of `batch` items.
+struct UNetCache {
+  long long x, e1a, s1, p1, e2a, s2, p2, bt, c2, u2, d2, c1, u1, d1, y;
+  long long activations;
+  long long g8a, g8b, g8c, g4a, g4b, g4c, g2a, g2b;
+  long long total;
+};
+
+UNetLayout unet_layout();
+// Opts the convolution kernels into large dynamic shared memory (call before any stream capture).
+void configure_unet_kernels();
+UNetCache unet_cache_layout(int batch);
+
+cudaError_t unet_forward(const float* params, const float* x, int batch, float* cache, float* y, cudaStream_t s);
+cudaError_t unet_backward(const float* params, float* cache, const float* grad_y, int batch, float* grad_params,
+                          cudaStream_t s);
+cudaError_t unet_masked_mse(const float* y, const float* target, const float* mask, int n, float* loss, float* grad,
+                            cudaStream_t s);
+cudaError_t adam_step(float* p, const float* g, float* m, float* v, long long n, int step, float lr, float b1,
+                      float b2, float eps, cudaStream_t s);
+cudaError_t unet_init_params(float* p, unsigned long long seed, cudaStream_t s);
+
+// Solver-side data movement (level-0 vectors in the red-black block layout, cell types natural).
+cudaError_t unet_gather(const GridView& g, const float* r_rb, const unsigned char* type, const int* blocks, int count,
+                        float* inputs, float* scale, cudaStream_t s);
+cudaError_t unet_targets(const GridView& g, const double* p_star, const double* p_k, const unsigned char* type,
+                         const int* blocks, int count, const float* scale, float* targets, float* masks,
+                         cudaStream_t s);
+template <typename T>
+cudaError_t unet_scatter(int nb, const float* y, const float* scale, const unsigned char* type, T* z, bool rb,
+                         cudaStream_t s);
+cudaError_t unet_block_has_fluid(int nb, const unsigned char* type, int* flags, cudaStream_t s);
+
+}  // namespace fl

@@ -104,6 +104,9 @@ typedef struct {
   int warm_start;     /* 1: start from the previous projection's pressure (InitializeMacPressure3D) */
   double rel_tol;    /* ||b - A p||_2 <= rel_tol * ||b||_2, checked in FP64 */
   double inner_rtol; /* inner FP32 solve reduction per refinement */
+  int preconditioner; /* 0: V-cycle; 1: learned block U-Net (fl_set_learned_preconditioner), V-cycle fallback */
+  int stall_limit;    /* learned: consecutive stalled iterations before the V-cycle takes over (0 -> 3) */
+  double stall_ratio; /* learned: an iteration stalls unless ||r||_2 < stall_ratio * best so far (0 -> 0.9) */
 } fl_pressure_options;
 
 typedef struct {
@@ -120,6 +123,8 @@ typedef struct {
   double max_volume_residual;    /* max |r|/V, 1/s (estimated from the FP64 l2 bound) */
   double max_divergence;         /* max |div u_new| over fluid cells, 1/s */
   double solve_ms;
+  int learned_iterations; /* iterations preconditioned by the learned network */
+  int fell_back;          /* 1: the V-cycle took over after stalled learned iterations */
 } fl_pressure_diagnostics;
 
 /* ---- context (the resident device arena) -------------------------------- */
@@ -248,6 +253,50 @@ typedef struct {
  * be serialized by the caller. */
 int fl_p2g_static_scratch(const fl_static_grid* grid, const fl_particles* sorted, const fl_transfer_params* params,
                           int mode, float* const out0[3], float* const out1[3], void* stream, fl_report* report);
+
+/* ---- learned block preconditioner (no counterpart in the reference) -------
+ * A 3D U-Net over one 8^3 pressure block plus a one-cell halo (channels
+ * 16/32/64, 3x3x3 convolutions, 141,937 FP32 parameters flattened layer by
+ * layer as weight [Cout][Cin][taps] then bias). Input item: 2 x 10^3 floats
+ * (residual / block scale, cell mask 1 fluid, 0 air, -1 solid), output item: 512
+ * floats (correction / block scale), both [channel][z][y][x]. All pointers are
+ * device pointers; calls are stream-ordered and allocate nothing. */
+typedef struct fl_unet fl_unet;
+int64_t fl_unet_param_count(void);
+/* Training workspace for up to max_batch items (all activations of one forward). */
+int fl_unet_create(int max_batch, fl_unet** out);
+int fl_unet_destroy(fl_unet* net);
+/* He-uniform weights from a counter-based stream (SplitMix64 of seed and index), zero biases. */
+int fl_unet_init_params(float* params, uint64_t seed, void* stream);
+/* FP32 forward pass; keeps the activations for fl_unet_backward. */
+int fl_unet_forward(fl_unet* net, const float* params, const float* input, int batch, float* output, void* stream);
+/* Gradient of sum(grad_output * output) of the last forward with respect to the parameters. */
+int fl_unet_backward(fl_unet* net, const float* params, const float* grad_output, int batch, float* grad_params,
+                     void* stream);
+/* loss = sum mask (output - target)^2 / max(1, sum mask) over batch*512 cells, and d loss / d output. */
+int fl_unet_masked_mse(const float* output, const float* target, const float* mask, int batch, float* loss,
+                       float* grad_output, void* stream);
+/* Adam with bias correction at step >= 1: m, v updated in place, params -= lr mhat / (sqrt(vhat) + eps). */
+int fl_adam_step(float* params, const float* grads, float* m, float* v, uint64_t count, int step, float lr,
+                 float beta1, float beta2, float eps, void* stream);
+
+/* Training pairs from the context's current projection (the last step's
+ * predicted velocities and cells): a converged solve gives p*, then for each
+ * iteration cap k in `iterations` the solve from p = 0 is stopped after k
+ * flexible-CG iterations and every block holding fluid yields one item:
+ * input = (r_k / s, mask) on the block plus halo, target = (p* - p_k) / s,
+ * target_mask = fluid cells, with r_k = b - A p_k and s = max |r_k| over the
+ * input window. Writes at most `capacity` items; `written` gets the count. */
+int fl_collect_training_pairs(fl_context* ctx, const fl_transfer_params* params, const fl_pressure_options* options,
+                              const int32_t* iterations, int iteration_count, float* inputs, float* targets,
+                              float* target_mask, uint64_t capacity, uint64_t* written);
+/* Loads trained FP32 parameters (device pointer) into the context's BF16
+ * inference weights used when fl_pressure_options.preconditioner == 1. */
+int fl_set_learned_preconditioner(fl_context* ctx, const float* params, void* stream);
+/* One application z = U(r) of the learned preconditioner on the cells of the
+ * last sort (r, z: active_blocks*512 floats, natural layout), for checking the
+ * inference kernels against the training forward pass. */
+int fl_apply_learned(fl_context* ctx, const float* r, float* z, void* stream);
 
 /* Plain device<->host copies for callers without their own CUDA runtime binding. */
 int fl_copy_to_host(void* host, const void* device, uint64_t bytes);

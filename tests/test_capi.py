@@ -14,7 +14,7 @@ HEADER = Path(__file__).resolve().parent.parent / "include" / "fluidity_b200.h"
 
 def declared_symbols():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^int\s+(fl_\w+)\s*\(", text, flags=re.M)))
+    return sorted(set(re.findall(r"^(?:int|int64_t)\s+(fl_\w+)\s*\(", text, flags=re.M)))
 
 
 def test_header_declares_the_hot_path():

@@ -1,0 +1,197 @@
+"""GPU checks of the learned block preconditioner through the C-ABI.
+
+* forward, backward (parameter gradients), masked MSE and Adam of the FP32
+  training kernels against the FP64 numpy oracle (oracle/unet.py), which is
+  itself pinned by finite differences: 1e-4 max-norm relative per layer;
+* a training step is bitwise reproducible (fixed-order reductions);
+* training on pairs from the context's own MGPCG solves lowers the loss;
+* flexible CG preconditioned by the trained network reaches the 1e-6 relative
+  FP64 residual, and an untrained network stalls and falls back to the V-cycle
+  (still converging)."""
+
+import numpy as np
+import pytest
+
+import fluidity_b200 as fb
+from fluidity_b200 import learned, scenes
+from helpers import dam_break_context
+from oracle import unet as U
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def _t(a):
+    import torch
+
+    return torch.tensor(np.ascontiguousarray(a, np.float32), device="cuda")
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def _inputs(rng, n):
+    x = rng.normal(size=(n, 2, 10, 10, 10))
+    x[:, 1] = rng.integers(-1, 2, size=(n, 10, 10, 10))
+    return x
+
+
+@pytest.fixture(scope="module")
+def net():
+    n = fb.UNet(8)
+    yield n
+    n.close()
+
+
+def test_forward_and_backward_match_oracle(net):
+    import torch
+
+    rng = np.random.default_rng(0)
+    th = U.init_params(5) + 0.02 * rng.normal(size=U.param_count())
+    x = _inputs(rng, 5)
+    y_ref, cache = U.forward(th, x)
+    dy = rng.normal(size=y_ref.shape)
+    g_ref = U.backward(th, cache, dy)
+    P, X = _t(th), _t(x)
+    Y = torch.zeros((5, 512), device="cuda")
+    G = torch.zeros_like(P)
+    net.forward(P, X, Y)
+    net.backward(P, _t(dy.reshape(5, 512)), G)
+    torch.cuda.synchronize()
+    assert _rel(Y.cpu().numpy(), y_ref.reshape(5, 512)) <= TOL
+    g = G.cpu().numpy()
+    off = 0
+    for name, nw, nb in U.layer_sizes():
+        assert _rel(g[off:off + nw], g_ref[off:off + nw]) <= TOL, name
+        assert _rel(g[off + nw:off + nw + nb], g_ref[off + nw:off + nw + nb]) <= TOL, name
+        off += nw + nb
+
+
+def test_masked_mse_and_adam_match_oracle():
+    import torch
+
+    rng = np.random.default_rng(1)
+    y, t = rng.normal(size=(3, 512)), rng.normal(size=(3, 512))
+    m = (rng.uniform(size=(3, 512)) > 0.4).astype(np.float64)
+    loss_ref, grad_ref = U.masked_mse(y, t, m)
+    loss = torch.zeros(1, device="cuda")
+    grad = torch.zeros((3, 512), device="cuda")
+    fb.UNet.masked_mse(_t(y), _t(t), _t(m), loss, grad)
+    assert abs(loss.item() - loss_ref) <= 1e-6 * loss_ref
+    assert _rel(grad.cpu().numpy(), grad_ref) <= 1e-6
+    th, gr = rng.normal(size=1000), rng.normal(size=1000)
+    mm, vv = np.zeros(1000), np.zeros(1000)
+    P, G, M, V = _t(th), _t(gr), _t(mm), _t(vv)
+    for step in (1, 2, 3):
+        th, mm, vv = U.adam(th, gr, mm, vv, step)
+        fb.UNet.adam_step(P, G, M, V, step)
+    np.testing.assert_allclose(P.cpu().numpy(), th, rtol=0, atol=1e-6)
+
+
+def test_init_params_follow_he_uniform_rule():
+    import torch
+
+    P = torch.empty(fb.UNet.param_count(), device="cuda")
+    fb.UNet.init_params(P, 7)
+    p = P.cpu().numpy()
+    off = 0
+    for (name, kind, cin, cout), (_, nw, nb) in zip(U.LAYERS, U.layer_sizes()):
+        bound = np.sqrt(6.0 / (cin * (27 if kind.startswith("conv3") else 1)))
+        w = p[off:off + nw]
+        assert np.all(np.abs(w) <= bound) and np.all(p[off + nw:off + nw + nb] == 0.0), name
+        if nw >= 1000:
+            assert abs(w.std() - bound / np.sqrt(3)) < 0.05 * bound, name
+        off += nw + nb
+
+
+def test_training_step_is_bitwise_reproducible():
+    import torch
+
+    rng = np.random.default_rng(2)
+    x = _t(_inputs(rng, 64))
+    t = _t(rng.normal(size=(64, 512)))
+    m = _t((rng.uniform(size=(64, 512)) > 0.5).astype(np.float32))
+    outs = []
+    for _ in range(2):
+        P, losses = learned.train(x, t, m, steps=3, batch=64, seed=3)
+        outs.append((P.cpu().numpy(), losses))
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+
+
+@pytest.fixture(scope="module")
+def trained():
+    x, t, m = learned.collect_pairs(64, pairs=3000, steps_between=3, seed_steps=2, max_states=6)
+    P, losses = learned.train(x, t, m, steps=400, batch=64, seed=0)
+    return x.shape[0], P, losses
+
+
+def test_training_on_solver_pairs_lowers_the_loss(trained):
+    count, P, losses = trained
+    assert count >= 500
+    assert np.all(np.isfinite(losses))
+    assert losses[-40:].mean() < 0.7 * losses[:40].mean()
+
+
+def test_learned_fcg_reaches_fp64_residual(trained):
+    _, P, _ = trained
+    ctx, _, m = dam_break_context(64)
+    params = fb.transfer_params(scenes.DT, m)
+    ctx.step(params, fb.default_pressure_options())
+    ctx.set_learned_preconditioner(P)
+    for prec in (0, 1):
+        opt = fb.default_pressure_options(precision=prec, preconditioner=1, max_iterations=2000)
+        code, d = ctx.step(params, opt)
+        assert code == fb.OK, d.as_dict()
+        assert d.relative_residual <= 1e-6 and d.learned_iterations > 0
+    ctx.close()
+
+
+def _identity_params():
+    """Weights for which the network returns its residual input (z = r): a
+    correction no better than plain CG."""
+    P = {name: [w.copy(), b.copy()] for name, (w, b) in U.unpack(np.zeros(U.param_count())).items()}
+    P["e1a"][0][0, 0, 1, 1, 1], P["e1a"][0][1, 0, 1, 1, 1] = 1.0, -1.0
+    for name in ("e1b", "d1"):
+        P[name][0][0, 0, 1, 1, 1] = P[name][0][1, 1, 1, 1, 1] = 1.0
+    P["out"][0][0, 0], P["out"][0][0, 1] = 1.0, -1.0
+    return U.pack(P)
+
+
+def test_identity_network_is_exact_through_the_kernels(net):
+    import torch
+
+    rng = np.random.default_rng(4)
+    x = _inputs(rng, 3)
+    Y = torch.zeros((3, 512), device="cuda")
+    net.forward(_t(_identity_params()), _t(x), Y)
+    np.testing.assert_allclose(Y.cpu().numpy().reshape(3, 8, 8, 8), x[:, 0, 1:9, 1:9, 1:9], rtol=1e-6, atol=1e-6)
+
+
+def test_stalled_network_falls_back_to_the_vcycle():
+    ctx, _, m = dam_break_context(32)
+    params = fb.transfer_params(scenes.DT, m)
+    ctx.step(params, fb.default_pressure_options())
+    ctx.set_learned_preconditioner(_t(_identity_params()))
+    # stall_ratio 0.01: every learned iteration counts as stalled -> fallback after exactly 3
+    code, d = ctx.step(params, fb.default_pressure_options(preconditioner=1, stall_ratio=0.01))
+    assert code == fb.OK
+    assert d.fell_back == 1 and d.learned_iterations == 3
+    assert d.relative_residual <= 1e-6
+    ctx.close()
+
+
+def test_zero_network_breaks_down_and_falls_back_at_once():
+    import torch
+
+    ctx, _, m = dam_break_context(32)
+    params = fb.transfer_params(scenes.DT, m)
+    ctx.step(params, fb.default_pressure_options())
+    ctx.set_learned_preconditioner(torch.zeros(fb.UNet.param_count(), device="cuda"))  # z = 0, z.r = 0
+    code, d = ctx.step(params, fb.default_pressure_options(preconditioner=1))
+    assert code == fb.OK
+    assert d.fell_back == 1 and d.learned_iterations == 0
+    assert d.relative_residual <= 1e-6
+    ctx.close()

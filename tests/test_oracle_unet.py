@@ -1,0 +1,60 @@
+"""The FP64 numpy restatement of the learned block preconditioner (oracle/unet.py)
+against central finite differences, layer by layer. No reference counterpart
+exists, so these checks are what pin the oracle that the GPU kernels are tested
+against. CPU only."""
+
+import numpy as np
+
+from oracle import unet as U
+
+
+def test_parameter_count_and_layout():
+    assert U.param_count() == 141937
+    th = U.init_params(3)
+    P = U.unpack(th)
+    assert P["e1a"][0].shape == (16, 2, 3, 3, 3) and P["bt"][0].shape == (64, 32, 3, 3, 3)
+    assert P["out"][0].shape == (1, 16) and np.all(P["d1"][1] == 0.0)
+    np.testing.assert_array_equal(U.pack({k: v for k, v in P.items()}), th)
+
+
+def test_forward_shapes_and_positive_homogeneity_without_bias():
+    rng = np.random.default_rng(1)
+    th = U.init_params(1)  # zero biases: the network is positively homogeneous of degree 1
+    x = rng.normal(size=(2, 2, 10, 10, 10))
+    y, _ = U.forward(th, x)
+    assert y.shape == (2, 1, 8, 8, 8)
+    y2, _ = U.forward(th, 2.5 * x)
+    np.testing.assert_allclose(y2, 2.5 * y, rtol=1e-12, atol=1e-12)
+
+
+def test_backward_matches_finite_differences_per_layer():
+    rng = np.random.default_rng(0)
+    th = U.init_params(1) + 0.01 * rng.normal(size=U.param_count())  # non-zero biases too
+    x = rng.normal(size=(1, 2, 10, 10, 10))
+    y, cache = U.forward(th, x)
+    dy = rng.normal(size=y.shape)
+    g = U.backward(th, cache, dy)
+    off = 0
+    eps = 1e-6
+    for _, nw, nb in U.layer_sizes():
+        for lo, hi in ((off, off + nw), (off + nw, off + nw + nb)):
+            d = np.zeros_like(th)
+            d[lo:hi] = rng.normal(size=hi - lo)
+            fd = ((U.forward(th + eps * d, x)[0] * dy).sum() - (U.forward(th - eps * d, x)[0] * dy).sum()) / (2 * eps)
+            assert abs(fd - g @ d) <= 1e-6 * max(1.0, abs(fd)), (lo, hi, fd, g @ d)
+        off += nw + nb
+
+
+def test_masked_mse_gradient_and_adam():
+    rng = np.random.default_rng(2)
+    y, t = rng.normal(size=(3, 512)), rng.normal(size=(3, 512))
+    m = (rng.uniform(size=(3, 512)) > 0.3).astype(float)
+    loss, grad = U.masked_mse(y, t, m)
+    assert np.isclose(loss, ((y - t) ** 2 * m).sum() / m.sum())
+    eps = 1e-6
+    d = rng.normal(size=y.shape)
+    fd = (U.masked_mse(y + eps * d, t, m)[0] - U.masked_mse(y - eps * d, t, m)[0]) / (2 * eps)
+    assert np.isclose(fd, (grad * d).sum(), rtol=1e-7)
+    th, gr = rng.normal(size=10), rng.normal(size=10)
+    th1, m1, v1 = U.adam(th, gr, np.zeros(10), np.zeros(10), 1)
+    np.testing.assert_allclose(th1, th - 1e-3 * np.sign(gr), rtol=0, atol=1e-9)  # first step moves lr*sign(g)
