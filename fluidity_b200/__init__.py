@@ -157,7 +157,7 @@ def library():
         lib.fl_unet_init_params.argtypes = [vp, ctypes.c_uint64, vp]
         lib.fl_unet_forward.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
         lib.fl_unet_backward.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
-        lib.fl_unet_masked_mse.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp, vp]
+        lib.fl_unet_masked_mse.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp]
         lib.fl_adam_step.argtypes = [vp, vp, vp, vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                      ctypes.c_float, ctypes.c_float, vp]
         lib.fl_collect_training_pairs.argtypes = [vp, ctypes.POINTER(TransferParams), ctypes.POINTER(PressureOptions),
@@ -407,9 +407,10 @@ class UNet:
                                           grads.data_ptr(), stream), "fl_unet_backward")
 
     @staticmethod
-    def masked_mse(outputs, targets, masks, loss, grad_outputs, stream=None):
+    def masked_mse(outputs, targets, masks, loss, grad_outputs, relative: int = 0, stream=None):
         _check(library().fl_unet_masked_mse(outputs.data_ptr(), targets.data_ptr(), masks.data_ptr(), outputs.shape[0],
-                                            loss.data_ptr(), grad_outputs.data_ptr(), stream), "fl_unet_masked_mse")
+                                            int(relative), loss.data_ptr(), grad_outputs.data_ptr(), stream),
+               "fl_unet_masked_mse")
 
     @staticmethod
     def adam_step(params, grads, m, v, step: int, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999,

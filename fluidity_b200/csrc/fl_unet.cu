@@ -324,40 +324,55 @@ __global__ void k_pool_back_add_mask(const float* __restrict__ ga, const float* 
   }
 }
 
-// Masked mean squared error over the batch in one CTA (fixed order):
-// loss = sum m (y - t)^2 / max(1, sum m), grad = 2 m (y - t) / max(1, sum m).
+// Masked squared error in one CTA (fixed order). relative == 0:
+//   loss = sum m (y - t)^2 / max(1, sum m), grad = 2 m (y - t) / max(1, sum m);
+// relative == 1 (every item weighs the same whatever its scale):
+//   loss = (1/V) sum_items [sum m (y - t)^2 / sum m t^2] over the V items with
+//   sum m t^2 > 0 (items without target energy add nothing), grad likewise.
 __global__ void __launch_bounds__(1024) k_masked_mse(const float* __restrict__ y, const float* __restrict__ t,
-                                                     const float* __restrict__ m, int n, float* __restrict__ loss,
-                                                     float* __restrict__ grad) {
+                                                     const float* __restrict__ m, int batch, int relative,
+                                                     float* __restrict__ loss, float* __restrict__ grad) {
   __shared__ double red[2 * 32];
-  double s = 0.0, c = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double d = (double)y[i] - (double)t[i];
-    s += m[i] * d * d;
-    c += m[i];
-  }
-  s = warp_sum(s);
-  c = warp_sum(c);
-  if ((threadIdx.x & 31) == 0) {
-    red[threadIdx.x >> 5] = s;
-    red[32 + (threadIdx.x >> 5)] = c;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double ts = 0.0, tc = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
-      ts += red[k];
-      tc += red[32 + k];
+  __shared__ double item_den[1024];
+  const int n = batch * 512;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  // per-item denominators (one warp per item, items in order)
+  for (int b = warp; b < batch; b += nwarps) {
+    double s = 0.0, c = 0.0;
+    for (int k = lane; k < 512; k += 32) {
+      const double tv = t[b * 512 + k];
+      s += m[b * 512 + k] * tv * tv;
+      c += m[b * 512 + k];
     }
-    red[0] = ts;
-    red[32] = tc > 1.0 ? tc : 1.0;
+    s = warp_sum(s);
+    c = warp_sum(c);
+    if (lane == 0) item_den[b] = relative ? s : c;
   }
   __syncthreads();
-  const double cnt = red[32];
-  if (threadIdx.x == 0 && loss) *loss = (float)(red[0] / cnt);
-  if (grad)
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-      grad[i] = (float)(2.0 * m[i] * ((double)y[i] - (double)t[i]) / cnt);
+  double global_den = 0.0;
+  int valid = 0;
+  for (int b = 0; b < batch; ++b) {
+    global_den += item_den[b];
+    valid += item_den[b] > 0.0;
+  }
+  global_den = global_den > 1.0 ? global_den : 1.0;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int b = i >> 9;
+    const double den = relative ? item_den[b] * valid : global_den;
+    const double d = (double)y[i] - (double)t[i];
+    const double w = relative && !(item_den[b] > 0.0) ? 0.0 : m[i] / den;
+    acc += w * d * d;
+    if (grad) grad[i] = (float)(2.0 * w * d);
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) red[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0 && loss) {
+    double total = 0.0;
+    for (int k = 0; k < nwarps; ++k) total += red[k];
+    *loss = (float)total;
+  }
 }
 
 __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
@@ -587,10 +602,10 @@ cudaError_t unet_backward(const float* P, float* cache, const float* gy, int bat
   return cudaGetLastError();
 }
 
-cudaError_t unet_masked_mse(const float* y, const float* t, const float* m, int n, float* loss, float* grad,
-                            cudaStream_t s) {
+cudaError_t unet_masked_mse(const float* y, const float* t, const float* m, int batch, int relative, float* loss,
+                            float* grad, cudaStream_t s) {
   ++g_kernel_launches;
-  k_masked_mse<<<1, 1024, 0, s>>>(y, t, m, n, loss, grad);
+  k_masked_mse<<<1, 1024, 0, s>>>(y, t, m, batch, relative, loss, grad);
   return cudaGetLastError();
 }
 
@@ -819,10 +834,12 @@ int fl_unet_backward(fl_unet* u, const float* params, const float* grad_output, 
                                      static_cast<cudaStream_t>(stream)));
 }
 
-int fl_unet_masked_mse(const float* output, const float* target, const float* mask, int batch, float* loss,
-                       float* grad_output, void* stream) {
-  if (output == nullptr || target == nullptr || mask == nullptr || batch <= 0) return FL_INVALID_ARGUMENT;
-  return unet_code(fl::unet_masked_mse(output, target, mask, batch * 512, loss, grad_output,
+int fl_unet_masked_mse(const float* output, const float* target, const float* mask, int batch, int relative,
+                       float* loss, float* grad_output, void* stream) {
+  if (output == nullptr || target == nullptr || mask == nullptr || batch <= 0 || batch > 1024 ||
+      (relative != 0 && relative != 1))
+    return FL_INVALID_ARGUMENT;
+  return unet_code(fl::unet_masked_mse(output, target, mask, batch, relative, loss, grad_output,
                                        static_cast<cudaStream_t>(stream)));
 }
 

@@ -34,8 +34,8 @@ UNetCache unet_cache_layout(int batch);
 cudaError_t unet_forward(const float* params, const float* x, int batch, float* cache, float* y, cudaStream_t s);
 cudaError_t unet_backward(const float* params, float* cache, const float* grad_y, int batch, float* grad_params,
                           cudaStream_t s);
-cudaError_t unet_masked_mse(const float* y, const float* target, const float* mask, int n, float* loss, float* grad,
-                            cudaStream_t s);
+cudaError_t unet_masked_mse(const float* y, const float* target, const float* mask, int batch, int relative,
+                            float* loss, float* grad, cudaStream_t s);
 cudaError_t adam_step(float* p, const float* g, float* m, float* v, long long n, int step, float lr, float b1,
                       float b2, float eps, cudaStream_t s);
 cudaError_t unet_init_params(float* p, unsigned long long seed, cudaStream_t s);

@@ -6,8 +6,9 @@ after k flexible-CG iterations give, per block holding fluid, the input
 (r_k / s, cell mask) on the block plus a one-cell halo and the target
 (p* - p_k) / s, s = max |r_k| over the window. Training runs entirely in the
 library's kernels (fl_unet_forward / fl_unet_backward / fl_unet_masked_mse /
-fl_adam_step) on batches of 64 items with Adam at lr 1e-3; torch only holds the
-device buffers and draws the batch indices.
+fl_adam_step) on batches of 64 items with Adam at lr 1e-3 on the per-item
+relative squared error (items whose errors differ by orders of magnitude weigh
+the same); torch only holds the device buffers and draws the batch indices.
 
     python -m fluidity_b200.learned --grid 128 --pairs 10000 --steps 2000 --out weights.npy
 """
@@ -86,7 +87,7 @@ def train(inputs, targets, masks, steps: int = 2000, batch: int = 64, lr: float 
         torch.index_select(targets, 0, idx, out=tb)
         torch.index_select(masks, 0, idx, out=mb)
         net.forward(P, xb, y)
-        fb.UNet.masked_mse(y, tb, mb, loss[step - 1:step], gy)
+        fb.UNet.masked_mse(y, tb, mb, loss[step - 1:step], gy, relative=1)
         net.backward(P, gy, G)
         fb.UNet.adam_step(P, G, M, V, step, lr=lr)
     torch.cuda.synchronize()

@@ -273,9 +273,12 @@ int fl_unet_forward(fl_unet* net, const float* params, const float* input, int b
 /* Gradient of sum(grad_output * output) of the last forward with respect to the parameters. */
 int fl_unet_backward(fl_unet* net, const float* params, const float* grad_output, int batch, float* grad_params,
                      void* stream);
-/* loss = sum mask (output - target)^2 / max(1, sum mask) over batch*512 cells, and d loss / d output. */
-int fl_unet_masked_mse(const float* output, const float* target, const float* mask, int batch, float* loss,
-                       float* grad_output, void* stream);
+/* Masked squared error of batch (<= 1024) items of 512 cells and d loss / d output.
+ * relative 0: loss = sum mask (output - target)^2 / max(1, sum mask);
+ * relative 1: loss = mean over the items with sum mask target^2 > 0 of
+ *             sum mask (output - target)^2 / sum mask target^2. */
+int fl_unet_masked_mse(const float* output, const float* target, const float* mask, int batch, int relative,
+                       float* loss, float* grad_output, void* stream);
 /* Adam with bias correction at step >= 1: m, v updated in place, params -= lr mhat / (sqrt(vhat) + eps). */
 int fl_adam_step(float* params, const float* grads, float* m, float* v, uint64_t count, int step, float lr,
                  float beta1, float beta2, float eps, void* stream);

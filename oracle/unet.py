@@ -194,11 +194,19 @@ def backward(theta, cache, dy):
     return pack(g)
 
 
-def masked_mse(y, target, mask):
-    """Loss and dL/dy of mean((y - t)^2) over cells where mask > 0."""
-    cnt = max(1.0, float(mask.sum()))
+def masked_mse(y, target, mask, relative=False):
+    """Loss and dL/dy of the masked squared error over items of 512 cells:
+    global mean over masked cells, or (relative) the mean over the items with
+    target energy sum m t^2 > 0 of sum m (y - t)^2 / sum m t^2."""
+    y, target, mask = (np.asarray(a, np.float64).reshape(-1, 512) for a in (y, target, mask))
     d = (y - target) * mask
-    return float((d * d).sum() / cnt), 2.0 * d / cnt
+    if relative:
+        energy = (mask * target * target).sum(axis=1, keepdims=True)
+        valid = energy > 0
+        w = np.where(valid, 1.0 / np.where(valid, energy, 1.0), 0.0) / max(1, int(valid.sum()))
+    else:
+        w = 1.0 / max(1.0, float(mask.sum()))
+    return float((d * d * w).sum()), 2.0 * d * w
 
 
 def adam(theta, grad, m, v, step, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):

@@ -75,12 +75,14 @@ def test_masked_mse_and_adam_match_oracle():
     rng = np.random.default_rng(1)
     y, t = rng.normal(size=(3, 512)), rng.normal(size=(3, 512))
     m = (rng.uniform(size=(3, 512)) > 0.4).astype(np.float64)
-    loss_ref, grad_ref = U.masked_mse(y, t, m)
-    loss = torch.zeros(1, device="cuda")
-    grad = torch.zeros((3, 512), device="cuda")
-    fb.UNet.masked_mse(_t(y), _t(t), _t(m), loss, grad)
-    assert abs(loss.item() - loss_ref) <= 1e-6 * loss_ref
-    assert _rel(grad.cpu().numpy(), grad_ref) <= 1e-6
+    t[1] = 0.0  # an item without target energy
+    for relative in (0, 1):
+        loss_ref, grad_ref = U.masked_mse(y, t, m, relative=bool(relative))
+        loss = torch.zeros(1, device="cuda")
+        grad = torch.zeros((3, 512), device="cuda")
+        fb.UNet.masked_mse(_t(y), _t(t), _t(m), loss, grad, relative=relative)
+        assert abs(loss.item() - loss_ref) <= 1e-6 * loss_ref
+        assert _rel(grad.cpu().numpy(), grad_ref) <= 1e-6
     th, gr = rng.normal(size=1000), rng.normal(size=1000)
     mm, vv = np.zeros(1000), np.zeros(1000)
     P, G, M, V = _t(th), _t(gr), _t(mm), _t(vv)

@@ -55,6 +55,15 @@ def test_masked_mse_gradient_and_adam():
     d = rng.normal(size=y.shape)
     fd = (U.masked_mse(y + eps * d, t, m)[0] - U.masked_mse(y - eps * d, t, m)[0]) / (2 * eps)
     assert np.isclose(fd, (grad * d).sum(), rtol=1e-7)
+    loss, grad = U.masked_mse(y, t, m, relative=True)
+    per_item = [((y[b] - t[b]) ** 2 * m[b]).sum() / (m[b] * t[b] ** 2).sum() for b in range(3)]
+    assert np.isclose(loss, np.mean(per_item))
+    fd = (U.masked_mse(y + eps * d, t, m, True)[0] - U.masked_mse(y - eps * d, t, m, True)[0]) / (2 * eps)
+    assert np.isclose(fd, (grad * d).sum(), rtol=1e-7)
+    t0 = t.copy()
+    t0[2] = 0.0  # no target energy: the item is left out
+    loss, grad = U.masked_mse(y, t0, m, relative=True)
+    assert np.isclose(loss, np.mean(per_item[:2])) and np.all(grad[2] == 0.0)
     th, gr = rng.normal(size=10), rng.normal(size=10)
     th1, m1, v1 = U.adam(th, gr, np.zeros(10), np.zeros(10), 1)
     np.testing.assert_allclose(th1, th - 1e-3 * np.sign(gr), rtol=0, atol=1e-9)  # first step moves lr*sign(g)
