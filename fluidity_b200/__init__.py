@@ -164,7 +164,7 @@ def library():
                                                   _ip, ctypes.c_int, vp, vp, vp, ctypes.c_uint64,
                                                   ctypes.POINTER(ctypes.c_uint64)]
         lib.fl_set_learned_preconditioner.argtypes = [vp, vp, vp]
-        lib.fl_apply_learned.argtypes = [vp, vp, vp, vp]
+        lib.fl_apply_learned.argtypes = [vp, vp, vp, ctypes.c_int, vp]
         _lib = lib
     return _lib
 
@@ -375,9 +375,11 @@ class LiquidContext:
         _check(library().fl_set_learned_preconditioner(self._ctx, params.data_ptr(), stream),
                "fl_set_learned_preconditioner")
 
-    def apply_learned(self, r, z, stream=None):
-        """z = U(r) on the cells of the last sort (device tensors, active_blocks*512 floats, natural order)."""
-        _check(library().fl_apply_learned(self._ctx, r.data_ptr(), z.data_ptr(), stream), "fl_apply_learned")
+    def apply_learned(self, r, z, kernels: int = 0, stream=None):
+        """z = U(r) on the cells of the last sort (device tensors, active_blocks*512 floats, natural
+        order); kernels 0 = tensor-core inference, 1 = FP32 training forward."""
+        _check(library().fl_apply_learned(self._ctx, r.data_ptr(), z.data_ptr(), int(kernels), stream),
+               "fl_apply_learned")
 
 
 class UNet:

@@ -108,8 +108,13 @@ struct fl_context {
   float* nn_params = nullptr;
   bool nn_ready = false;
   float* nn_scale = nullptr;
-  float* nn_act = nullptr;
+  float* nn_act = nullptr;  // FP32 training-forward activations (checking path)
   long long nn_act_items = 0;
+  __nv_bfloat16* nn_packed = nullptr;  // BF16 conv weights for the tensor-core kernels
+  uint4* nn_tc = nullptr;              // BF16 activation columns, zeroed at allocation
+  float* nn_bt = nullptr;
+  long long nn_tc_items = 0;
+  int sms = 0;
   cudaGraphExec_t fcg_nn_exec = nullptr;
   unsigned long long fcg_nn_kernels = 0;
   PrecondHook nn_hook{};
@@ -269,6 +274,7 @@ __global__ void k_init_state(SolverState* st, double rel_tol, double inner_rtol,
   st->stalls = 0;
   st->fallback = 0;
   st->learned_iter = 0;
+  st->nn_error = 0;
   st->target = 0.0;
   st->inner_rtol = inner_rtol;
   st->inner_max = inner_max;
@@ -345,21 +351,41 @@ int capture_fcg(fl_context* c, const GridView& g, const MgHierarchy<T>& H, const
   return FL_OK;
 }
 
-// Learned preconditioner application z = s * U(r / s) per block (gather of the
-// block + halo window, batched forward over all active blocks, scatter to the
-// level-0 layout). Captured into the learned FCG graph.
+// Learned preconditioner application z = s * U(r / s) per block: the
+// tensor-core kernels (BF16 activations, FP32 accumulation) on the solver's
+// vectors. Captured into the learned FCG graph.
 template <typename T>
 cudaError_t nn_apply(void* vc, const float* r, void* z, cudaStream_t s) {
   fl_context* c = static_cast<fl_context*>(vc);
   const GridView g = view(c);
-  const UNetCache C = unet_cache_layout(g.nb);
-  float* x = c->nn_act + C.x;
-  cudaError_t e = unet_gather(g, r, c->type, nullptr, g.nb, x, c->nn_scale, s);
-  if (e == cudaSuccess) e = unet_forward(c->nn_params, x, g.nb, c->nn_act, nullptr, s);
-  if (e == cudaSuccess) e = unet_scatter<T>(g.nb, c->nn_act + C.y, c->nn_scale, c->type, static_cast<T*>(z), true, s);
-  return e;
+  return unet_tc_apply<T>(g, c->nn_params, c->nn_packed, c->nn_tc, c->nn_tc_items, c->nn_bt, c->nn_scale, c->type,
+                          r, static_cast<T*>(z), &c->st->nn_error, c->sms, s);
 }
 
+int nn_reserve_tc(fl_context* c, long long items) {
+  if (items <= c->nn_tc_items) return FL_OK;
+  cudaFree(c->nn_tc);
+  cudaFree(c->nn_bt);
+  c->nn_tc = nullptr;
+  c->nn_bt = nullptr;
+  c->nn_tc_items = 0;
+  const long long want = std::min<long long>(items + items / 4 + 16, c->lattice);
+  const UNetTcLayout L = unet_tc_layout();
+  const size_t bytes = sizeof(uint4) * (size_t)(L.rows_per_block * want);
+  if (cudaMalloc(&c->nn_tc, bytes) != cudaSuccess ||
+      cudaMalloc(&c->nn_bt, sizeof(float) * (size_t)(L.bt_floats_per_block * want)) != cudaSuccess) {
+    cudaGetLastError();
+    return FL_RESOURCE_EXHAUSTED;
+  }
+  // pads are read as zeros and never written (tensors are based on the allocated
+  // capacity, so their columns never move while this allocation lives)
+  if (cudaMemset(c->nn_tc, 0, bytes) != cudaSuccess) return FL_INTERNAL;
+  c->nn_tc_items = want;
+  return FL_OK;
+}
+
+// FP32 training-forward path over the same gathered windows (for checking the
+// tensor-core kernels).
 int nn_reserve(fl_context* c, long long items) {
   if (items <= c->nn_act_items) return FL_OK;
   cudaFree(c->nn_act);
@@ -393,7 +419,7 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   if (opt->preconditioner != 0 && !use_nn) return FL_INVALID_ARGUMENT;
   if (use_nn) {
     if (!c->nn_ready) return FL_FAILED_PRECONDITION;
-    st = nn_reserve(c, c->nb);
+    st = nn_reserve_tc(c, c->nb);
     if (st != FL_OK) return st;
     c->nn_hook.apply = nn_apply<T>;
     c->nn_hook.ctx = c;
@@ -448,6 +474,10 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
       if (c->st_host->done) break;
     }
     total = c->st_host->total_iter;
+    if (c->st_host->nn_error) {
+      status = FL_INTERNAL;
+      break;
+    }
     if (c->st_host->status != 0) {
       status = c->st_host->status;
       break;
@@ -825,6 +855,9 @@ int fl_context_destroy(fl_context* c) {
   cudaFree(c->nn_params);
   cudaFree(c->nn_scale);
   cudaFree(c->nn_act);
+  cudaFree(c->nn_packed);
+  cudaFree(c->nn_tc);
+  cudaFree(c->nn_bt);
   if (c->work) cudaStreamDestroy(c->work);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
@@ -1308,24 +1341,41 @@ int fl_set_learned_preconditioner(fl_context* c, const float* params, void* stre
     cudaGetLastError();
     return FL_RESOURCE_EXHAUSTED;
   }
+  if (!c->nn_packed &&
+      cudaMalloc(&c->nn_packed, sizeof(__nv_bfloat16) * (size_t)unet_tc_layout().w_total) != cudaSuccess) {
+    cudaGetLastError();
+    return FL_RESOURCE_EXHAUSTED;
+  }
+  if (c->sms == 0) cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
   configure_unet_kernels();
   FL_CUDA(cudaMemcpyAsync(c->nn_params, params, sizeof(float) * np, cudaMemcpyDeviceToDevice, s));
+  FL_CUDA(unet_tc_pack(c->nn_params, c->nn_packed, s));
   FL_CUDA(cudaStreamSynchronize(s));
   c->nn_ready = true;
   return FL_OK;
 }
 
-int fl_apply_learned(fl_context* c, const float* r, float* z, void* stream) {
-  if (!c || !r || !z) return FL_INVALID_ARGUMENT;
+int fl_apply_learned(fl_context* c, const float* r, float* z, int kernels, void* stream) {
+  if (!c || !r || !z || (kernels != 0 && kernels != 1)) return FL_INVALID_ARGUMENT;
   if (!c->nn_ready) return FL_FAILED_PRECONDITION;
   if (c->nb == 0) return FL_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  int st = nn_reserve(c, c->nb);
+  int st = kernels == 0 ? nn_reserve_tc(c, c->nb) : nn_reserve(c, c->nb);
   if (st != FL_OK) return st;
   GridView g = view(c);
-  const UNetCache C = unet_cache_layout(g.nb);
   FL_CUDA(launch_classify(g, c->cell_start, c->type, s));
   FL_CUDA(launch_to_rb(g, r, c->r[0], s));
+  if (kernels == 0) {
+    FL_CUDA(cudaMemsetAsync(&c->st->nn_error, 0, sizeof(int), s));
+    FL_CUDA(unet_tc_apply<float>(g, c->nn_params, c->nn_packed, c->nn_tc, c->nn_tc_items, c->nn_bt, c->nn_scale,
+                                 c->type, c->r[0], c->q, &c->st->nn_error, c->sms, s));
+    FL_CUDA(launch_to_natural_f32(g, c->q, z, s));
+    FL_CUDA(cudaMemcpyAsync(c->st_host, c->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
+    FL_CUDA(cudaStreamSynchronize(s));
+    if (c->st_host->nn_error) return FL_INTERNAL;
+    return FL_OK;
+  }
+  const UNetCache C = unet_cache_layout(g.nb);
   FL_CUDA(unet_gather(g, c->r[0], c->type, nullptr, g.nb, c->nn_act + C.x, c->nn_scale, s));
   FL_CUDA(unet_forward(c->nn_params, c->nn_act + C.x, g.nb, c->nn_act, nullptr, s));
   FL_CUDA(unet_scatter<float>(g.nb, c->nn_act + C.y, c->nn_scale, c->type, z, false, s));

@@ -74,7 +74,7 @@ struct SolverState {
   int stalls;
   int fallback;
   int learned_iter;
-  int pad2;
+  int nn_error;         // the learned preconditioner's kernels gave up waiting
   int converged;
   int done;
   int status;
@@ -133,6 +133,8 @@ cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, con
 cudaError_t launch_export_pressure(const GridView& g, const double* p64, double* p_nat, float* p_keep,
                                    cudaStream_t s);
 cudaError_t launch_to_rb(const GridView& g, const float* in_nat, float* out_rb, cudaStream_t s);
+// Level-0 float vector from the red-black block layout to natural cell order.
+cudaError_t launch_to_natural_f32(const GridView& g, const float* in_rb, float* out_nat, cudaStream_t s);
 // Cell types of the last sort: 0 solid, 1 fluid (holds particles), 2 air.
 cudaError_t launch_classify(const GridView& g, const int* cell_start, unsigned char* type, cudaStream_t s);
 template <typename T>

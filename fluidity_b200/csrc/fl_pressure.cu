@@ -1082,6 +1082,9 @@ __global__ void k_to_natural(int n, const T* x_rb, const unsigned char* fluid_rb
 __global__ void k_to_rb(int n, const float* in_nat, float* out_rb) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out_rb[rb_id(i)] = in_nat[i];
 }
+__global__ void k_from_rb(int n, const float* in_rb, float* out_nat) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out_nat[i] = in_rb[rb_id(i)];
+}
 
 // ----------------------------------------------------------------- host orchestration
 
@@ -1279,6 +1282,13 @@ cudaError_t launch_to_rb(const GridView& g, const float* in_nat, float* out_rb, 
   const int n = g.nb * kBlockCells;
   ++g_kernel_launches;
   k_to_rb<<<reduce_grid(n), kThreads, 0, s>>>(n, in_nat, out_rb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_natural_f32(const GridView& g, const float* in_rb, float* out_nat, cudaStream_t s) {
+  const int n = g.nb * kBlockCells;
+  ++g_kernel_launches;
+  k_from_rb<<<reduce_grid(n), kThreads, 0, s>>>(n, in_rb, out_nat);
   return cudaGetLastError();
 }
 

@@ -1,6 +1,7 @@
 // Learned block preconditioner: parameter layout, training cache layout and launchers.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "fl_internal.cuh"
@@ -50,5 +51,26 @@ template <typename T>
 cudaError_t unet_scatter(int nb, const float* y, const float* scale, const unsigned char* type, T* z, bool rb,
                          cudaStream_t s);
 cudaError_t unet_block_has_fluid(int nb, const unsigned char* type, int* flags, cudaStream_t s);
+
+// Tensor-core inference: per-block offsets (in 16-byte rows) of the BF16
+// activation columns, stored tensor-major ([tensor][block][rows]); the packed
+// BF16 conv weights (e1a e1b e2a e2b bt d2 d1) and their element offsets.
+struct UNetTcLayout {
+  long long x, t8, s1, p1, e2a, s2, p2, u2, d2;
+  long long rows_per_block;
+  long long bt_floats_per_block;
+  long long w_off[7];
+  long long w_total;
+};
+UNetTcLayout unet_tc_layout();
+cudaError_t unet_tc_pack(const float* params, __nv_bfloat16* packed, cudaStream_t s);
+// z = s * U(r / s) on fluid cells of every active block (r, z: level-0 layout).
+// `act` holds rows_per_block * cap 16-byte rows (cap >= active blocks) and must
+// be zeroed once when allocated: the pads of every column are read as zeros and
+// never written.
+template <typename T>
+cudaError_t unet_tc_apply(const GridView& g, const float* params, const __nv_bfloat16* packed, uint4* act,
+                          long long cap, float* bt, float* scale, const unsigned char* type, const float* r_rb, T* z,
+                          int* error, int sms, cudaStream_t s);
 
 }  // namespace fl

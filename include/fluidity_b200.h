@@ -297,9 +297,10 @@ int fl_collect_training_pairs(fl_context* ctx, const fl_transfer_params* params,
  * inference weights used when fl_pressure_options.preconditioner == 1. */
 int fl_set_learned_preconditioner(fl_context* ctx, const float* params, void* stream);
 /* One application z = U(r) of the learned preconditioner on the cells of the
- * last sort (r, z: active_blocks*512 floats, natural layout), for checking the
- * inference kernels against the training forward pass. */
-int fl_apply_learned(fl_context* ctx, const float* r, float* z, void* stream);
+ * last sort (r, z: active_blocks*512 floats, natural layout). kernels 0: the
+ * tensor-core inference used inside the solver (BF16 activations, FP32
+ * accumulation); 1: the FP32 training forward pass, for checking the former. */
+int fl_apply_learned(fl_context* ctx, const float* r, float* z, int kernels, void* stream);
 
 /* Plain device<->host copies for callers without their own CUDA runtime binding. */
 int fl_copy_to_host(void* host, const void* device, uint64_t bytes);

@@ -172,6 +172,39 @@ def test_identity_network_is_exact_through_the_kernels(net):
     np.testing.assert_allclose(Y.cpu().numpy().reshape(3, 8, 8, 8), x[:, 0, 1:9, 1:9, 1:9], rtol=1e-6, atol=1e-6)
 
 
+def test_tensor_core_inference_matches_fp32_forward():
+    """The tcgen05 implicit-GEMM inference (BF16 activations, FP32 accumulation)
+    against the FP32 training forward on the same solver windows: 3e-2 max-norm
+    relative for a random network; the identity network returns r on fluid cells
+    to BF16 rounding (4e-3 of max |r|)."""
+    import torch
+
+    ctx, _, m = dam_break_context(32)
+    params = fb.transfer_params(scenes.DT, m)
+    ctx.step(params, fb.default_pressure_options())
+    nb = len(ctx.active_blocks())
+    rng = np.random.default_rng(6)
+    r = _t(rng.normal(size=nb * 512))
+    z_tc = torch.zeros(nb * 512, device="cuda")
+    z_ref = torch.zeros_like(z_tc)
+    th = U.init_params(9) + 0.01 * rng.normal(size=U.param_count())
+    ctx.set_learned_preconditioner(_t(th))
+    ctx.apply_learned(r, z_tc, kernels=0)
+    ctx.apply_learned(r, z_ref, kernels=1)
+    a, b = z_tc.cpu().numpy(), z_ref.cpu().numpy()
+    assert np.any(b != 0.0)
+    assert _rel(a, b) <= 3e-2
+    ctx.set_learned_preconditioner(_t(_identity_params()))
+    ctx.apply_learned(r, z_tc, kernels=0)
+    ctx.apply_learned(r, z_ref, kernels=1)
+    a, b = z_tc.cpu().numpy(), z_ref.cpu().numpy()
+    fluid = b != 0.0
+    np.testing.assert_allclose(b[fluid], r.cpu().numpy()[fluid], rtol=1e-6, atol=1e-6)
+    assert np.all(a[~fluid] == 0.0)
+    assert np.abs(a - b).max() <= 4e-3 * np.abs(b).max()
+    ctx.close()
+
+
 def test_stalled_network_falls_back_to_the_vcycle():
     ctx, _, m = dam_break_context(32)
     params = fb.transfer_params(scenes.DT, m)
