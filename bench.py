@@ -210,6 +210,8 @@ def run_ours(args, world, rank, local):
         "library_launches": int(launches1[1] - launches0[1]),
         "clocks": clocks.summary(),
     }
+    if not args.no_learned:
+        line["pressure_solve_ms"] = pressure_comparison(ctx, tp, args.grid)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(soa, mass, args.grid, npart, ncell, budget_s=args.cpu_budget)
     ctx.close()
@@ -217,6 +219,47 @@ def run_ours(args, world, rank, local):
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return line
+
+
+def pressure_comparison(ctx, tp, grid, repeats=2):
+    """Pressure-solve time to a 1e-6 relative FP64 residual on the last step's
+    projection, each variant from p = 0 (no warm start): plain FP32 MGPCG, the
+    BF16-storage V-cycle, and the learned block preconditioner (trained here on
+    (residual, error) pairs of 128^3 dam-break solves) with the BF16 V-cycle as
+    its fallback. Times are the solver's own CUDA events (setup + iterations +
+    velocity correction); the minimum over `repeats` runs."""
+    import time
+
+    import fluidity_b200 as fb
+    from fluidity_b200 import learned
+
+    t0 = time.time()
+    x, t, m = learned.collect_pairs(128, 10000)
+    P, losses = learned.train(x, t, m, steps=2000, batch=64, lr=1e-3)
+    train_s = time.time() - t0
+    ctx.set_learned_preconditioner(P)
+    variants = {
+        "mgpcg_fp32": dict(precision=0),
+        "mgpcg_bf16": dict(precision=1),
+        "learned_bf16": dict(precision=1, preconditioner=1),
+    }
+    out = {"unit": "ms", "relative_residual": 1e-6, "start": "p = 0", "grid": grid}
+    for name, kw in variants.items():
+        best = None
+        for _ in range(repeats):
+            code, d = ctx.project(tp, fb.default_pressure_options(rel_tol=1e-6, warm_start=0, **kw))
+            if code != fb.OK:
+                raise RuntimeError(f"{name}: pressure did not converge: {d.as_dict()}")
+            if best is None or d.solve_ms < best.solve_ms:
+                best = d
+        out[name] = {"ms": round(best.solve_ms, 3), "iterations": best.iterations,
+                     "learned_iterations": best.learned_iterations, "fell_back": best.fell_back,
+                     "relative_residual": best.relative_residual}
+    out["learned_vs_fp32_mgpcg_speedup"] = round(out["mgpcg_fp32"]["ms"] / out["learned_bf16"]["ms"], 3)
+    out["training"] = {"pairs": int(x.shape[0]), "adam_steps": 2000, "batch": 64, "lr": 1e-3,
+                       "seconds": round(train_s, 1), "loss_first": float(losses[:20].mean()),
+                       "loss_last": float(losses[-20:].mean())}
+    return out
 
 
 def _sample_cube(soa, grid, sample):
@@ -344,6 +387,7 @@ def main():
     ap.add_argument("--grid", type=int, default=256)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-MGPCG pressure comparison")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     args = ap.parse_args()
     world, rank, local = _dist()

@@ -357,6 +357,19 @@ class LiquidContext:
         _check(library().fl_state_particles(self._ctx, ctypes.byref(p)), "fl_state_particles")
         return p
 
+    def project(self, params: TransferParams, options: PressureOptions, stream=None):
+        """Re-runs the pressure projection of the last step (its predicted velocities and
+        cells) with `options`; returns (status code, diagnostics)."""
+        f = self.fields()
+        up = (ctypes.c_void_p * 3)(*f["u_pred"])
+        un = (ctypes.c_void_p * 3)(*f["u_new"])
+        diag = PressureDiagnostics()
+        code = library().fl_pressure_project(self._ctx, up, un, ctypes.byref(params), ctypes.byref(options),
+                                             ctypes.byref(diag), None, stream)
+        if code not in (OK, ABORTED):
+            raise FluidityError(code, "fl_pressure_project")
+        return code, diag
+
     def collect_training_pairs(self, params: TransferParams, options: PressureOptions, iterations, inputs, targets,
                                masks) -> int:
         """(residual, error) items of the last step's projection into device tensors
