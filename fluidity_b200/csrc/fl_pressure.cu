@@ -493,8 +493,30 @@ __device__ __forceinline__ int parent1_of_nat(int j) {  // level-1 (4^3 per bloc
   return b * 64 + (z << 4) + (y << 2) + x;
 }
 
+// Face halo of one colour: the 32 cells of each face of the neighbouring blocks
+// whose colour is `oc` (the only ones a sweep of colour 1 - oc reads), 192 in
+// all, one per thread for threads < 192; halo[f][q] as in load_halo0.
+template <typename F>
+__device__ __forceinline__ void load_halo0_colour(const GridView& g, int blk, int oc, float (*halo)[64], F value) {
+  const int e = threadIdx.x;
+  if (e >= 192) return;
+  const int f = e >> 5, k = e & 31, a = f >> 1, dir = (f & 1) ? 1 : -1;
+  const int c = dir < 0 ? 7 : 0;  // plane of the neighbour block next to this face
+  const int w = k >> 2;
+  const int u = 2 * (k & 3) + ((oc + c + w) & 1);  // (c + u + w) & 1 == oc
+  const int nbb = g.nbr27[blk * 27 + 13 + dir * (a == 0 ? 1 : (a == 1 ? 3 : 9))];
+  float v = 0.0f;
+  if (nbb >= 0) {
+    const int x = a == 0 ? c : u, y = a == 1 ? c : (a == 0 ? u : w), z = a == 2 ? c : w;
+    v = value(nbb * 512 + ((z << 6) | (y << 3) | x));
+  }
+  halo[f][(w << 3) | u] = v;
+}
+
 // Red-black sweep of one colour on level 0 (MODE 0 plain, 2 prolongation
-// fused); MODE 1 (first sweep from zero) needs no neighbour values.
+// fused); MODE 1 (first sweep from zero) needs no neighbour values. The cell's
+// mask, right-hand side and diagonal are loaded before the neighbour values so
+// their latencies overlap.
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256)
     k_smooth0_tiled(GridView g, LevelPtrs<T> lp, const float* __restrict__ b, int color, const T* __restrict__ xc,
@@ -503,6 +525,10 @@ __global__ void __launch_bounds__(256)
   __shared__ float tile[512];
   __shared__ float halo[6][64];
   const int blk = blockIdx.x, t = threadIdx.x;
+  const int i = blk * 512 + (color << 8) + t;
+  const unsigned m = lp.mask[i];
+  const float bi = b[i];
+  const float di = lp.diag[i];
   const T* __restrict__ x = lp.x;
   if (MODE != 1) {
     const int oc = 1 - color;
@@ -510,17 +536,15 @@ __global__ void __launch_bounds__(256)
     float v = ld(&x[blk * 512 + (oc << 8) + t]);
     if (MODE == 2) v += ld(&xc[parent1_of_nat(blk * 512 + lo)]);
     tile[lo] = v;
-    load_halo0(g, blk, halo, [&](int j) {
+    load_halo0_colour(g, blk, oc, halo, [&](int j) {
       float hv = ld(&x[rb_id(j)]);
       if (MODE == 2) hv += ld(&xc[parent1_of_nat(j)]);
       return hv;
     });
     __syncthreads();
   }
-  const int i = blk * 512 + (color << 8) + t;
-  const unsigned m = lp.mask[i];
   if (!(m & 64u)) return;
-  float s = b[i];
+  float s = bi;
   if (MODE != 1) {
     const int l = nat_of((color << 8) | t);
     const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
@@ -533,7 +557,7 @@ __global__ void __launch_bounds__(256)
       }
     }
   }
-  st_T(&lp.x[i], s / lp.diag[i]);
+  st_T(&lp.x[i], s / di);
 }
 
 // Level-0 residual restricted to level 1: all 512 cells of the block and its
@@ -549,14 +573,16 @@ __global__ void __launch_bounds__(512)
   const int blk = blockIdx.x, t = threadIdx.x;
   const int i = blk * 512 + t;  // solver (red-black) index
   const int l = nat_of(t);
+  const unsigned m = fp.mask[i];
+  const float di = fp.diag[i];
+  const float bi = fb[i];
   tile[l] = ld(&fp.x[i]);
   load_halo0(g, blk, halo, [&](int j) { return ld(&fp.x[rb_id(j)]); });
   __syncthreads();
-  const unsigned m = fp.mask[i];
   float res = 0.0f;
   if (m & 64u) {
     const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
-    float ax = fp.diag[i] * tile[l];
+    float ax = di * tile[l];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
 #pragma unroll
@@ -565,7 +591,7 @@ __global__ void __launch_bounds__(512)
         ax -= tile_nbr0(tile, halo, cx, cy, cz, a, dir);
       }
     }
-    res = fb[i] - ax;
+    res = bi - ax;
   }
   r[l] = res;
   __syncthreads();
@@ -598,7 +624,9 @@ __global__ void __launch_bounds__(512)
   const int i = blk * 512 + t;
   const int l = nat_of(t);
   const unsigned m = L0.mask[i];
-  const float di = (m & 64u) ? (first ? ld(&z[i]) : fmaf(beta, d_old[i], ld(&z[i]))) : 0.0f;
+  const float dg = L0.diag[i];
+  const float zi = ld(&z[i]);
+  const float di = (m & 64u) ? (first ? zi : fmaf(beta, d_old[i], zi)) : 0.0f;
   tile[l] = di;
   load_halo0(g, blk, halo, [&](int j) {
     const int r = rb_id(j);
@@ -608,7 +636,7 @@ __global__ void __launch_bounds__(512)
   float qi = 0.0f;
   if (m & 64u) {
     const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
-    float ax = L0.diag[i] * di;
+    float ax = dg * di;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
 #pragma unroll
@@ -630,29 +658,27 @@ __global__ void __launch_bounds__(512)
     v = warp_sum(v);
     if (t == 0) partial[blk] = v;
   }
-  __shared__ bool last;
-  __threadfence();
+}
+
+// d.q over the per-block partials of k_direction_tiled, in block order, -> alpha.
+__global__ void __launch_bounds__(1024) k_direction_finish(int nb, const double* __restrict__ partial,
+                                                           SolverState* st) {
+  if (st->done) return;
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) acc += partial[k];
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
-  if (t == 0) last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (last) {
-    double acc = 0.0;
-    for (unsigned k = t; k < gridDim.x; k += blockDim.x) acc += partial[k];
-    acc = warp_sum(acc);
-    __syncthreads();
-    if ((t & 31) == 0) red[t >> 5] = acc;
-    __syncthreads();
-    if (t == 0) {
-      double tot = 0.0;
-      for (int w = 0; w < 16; ++w) tot += red[w];
-      if (!(tot > 0.0) || !isfinite(tot)) {
-        st->status = kAborted;
-        st->done = 1;
-      }
-      st->alpha = st->rz / tot;
-      st->rz_prev = st->rz;
-      st->ticket = 0;
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+    if (!(tot > 0.0) || !isfinite(tot)) {
+      st->status = kAborted;
+      st->done = 1;
     }
+    st->alpha = st->rz / tot;
+    st->rz_prev = st->rz;
   }
 }
 
@@ -1243,9 +1269,10 @@ cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, con
   }
   const T* z = H.ptr[0].x;
   const unsigned grid = reduce_grid(n);
-  g_kernel_launches += 3;
+  g_kernel_launches += 4;
   k_dots<T><<<grid, kThreads, 0, s>>>(n, z, r_cur, r_prev, partial, st);
   k_direction_tiled<T><<<g.nb, 512, 0, s>>>(g, H.ptr[0], z, d_old, d_new, q, partial, st);
+  k_direction_finish<<<1, 1024, 0, s>>>(g.nb, partial, st);
   k_update<<<grid, kThreads, 0, s>>>(n, d_new, q, r_cur, r_prev, e, partial, st);
   return cudaGetLastError();
 }
