@@ -34,7 +34,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "steps/s at 256^3 APIC (sparse splash, ~29.6M particles, projection to 1e-6 relative residual)"
 UNIT = "steps/s"
 WORKLOAD = {"workload": "splash_256", "grid": 256, "scene": "pool y<=0.2 + two r=0.15 spheres at +-2 m/s",
-            "particles_per_cell": 8, "dt": 1.0 / 240.0, "precision": "fp32 transfers, bf16 V-cycle, fp32 FCG, fp64 refinement",
+            "particles_per_cell": 8, "dt": 1.0 / 240.0,
+            "precision": "fp32 transfers, fp32 V-cycle storage (bf16 measured beside), fp32 FCG, fp64 refinement",
             "rel_tol": 1e-6, "l2": "inputs (1.8 GB of particles) larger than the 126 MB L2; no flush"}
 FALLBACK_HBM_GBS = 6650.0
 
@@ -133,7 +134,7 @@ def run_ours(args, world, rank, local):
     npart = soa.shape[1]
     ctx = fb.LiquidContext(args.grid, capacity=npart)
     tp = fb.transfer_params(scenes.DT, mass)
-    opt = fb.default_pressure_options(precision=1, rel_tol=1e-6, warm_start=1)
+    opt = fb.default_pressure_options(precision=args.precision, rel_tol=1e-6, warm_start=1, inner_rtol=1e-3)
     ctx.upload(soa)
     for _ in range(args.warmup):
         code, _ = ctx.step(tp, opt)
@@ -159,6 +160,24 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
     launches1 = fb.kernel_launches()
     ms = start.elapsed_time(stop)
+    # the other V-cycle storage precision, same scene continued, for comparison
+    alt_prec = 1 - args.precision
+    alt_opt = fb.default_pressure_options(precision=alt_prec, rel_tol=1e-6, warm_start=1, inner_rtol=1e-3)
+    alt_phases, alt_iters = np.zeros(4), []
+    for _ in range(2):
+        ctx.step(tp, alt_opt)
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a0.record()
+    for _ in range(args.steps):
+        code, diag = ctx.step(tp, alt_opt)
+        alt_phases += ctx.step_timings()
+        alt_iters.append(diag.iterations)
+        if code != fb.OK:
+            raise RuntimeError(f"pressure did not converge: {diag.as_dict()}")
+    a1.record()
+    torch.cuda.synchronize()
+    alt_ms = a0.elapsed_time(a1) / args.steps
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -205,7 +224,11 @@ def run_ours(args, world, rank, local):
                       "pressure": round(phases[2] / args.steps, 4), "g2p": round(g2p_ms, 4)},
         "g2p_roofline": {"achieved": round(g2p_bytes / (g2p_ms / 1e3) / 1e9, 1), "frac": round(
             g2p_bytes / (g2p_ms / 1e3) / 1e9 / peak, 4)},
-        "pressure": {"mean_iterations": float(np.mean(iters)), "max_relative_residual": float(max(residuals))},
+        "pressure": {"mean_iterations": float(np.mean(iters)), "max_relative_residual": float(max(residuals)),
+                     "vcycle_storage": "bf16" if args.precision == 1 else "fp32", "inner_rtol": 1e-3},
+        "vcycle_" + ("bf16" if alt_prec == 1 else "fp32"): {
+            "steps_per_s": round(1e3 / alt_ms, 4), "ms_per_step": round(alt_ms, 4),
+            "pressure_ms": round(alt_phases[2] / args.steps, 4), "mean_iterations": float(np.mean(alt_iters))},
         "gpu_launches": int(launches1[0] - launches0[0]),
         "library_launches": int(launches1[1] - launches0[1]),
         "clocks": clocks.summary(),
@@ -385,6 +408,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--grid", type=int, default=256)
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
+                    help="V-cycle storage: 0 FP32 (default, fewer FCG iterations), 1 BF16")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-MGPCG pressure comparison")

@@ -1,6 +1,7 @@
 """Runs a few liquid substeps of a seeded scene, for profiling (ncu, CUDA events).
 
     python -m fluidity_b200.profile_step --scene splash --grid 256 --steps 2 [--precision 1] [--levels 0]
+        [--warm-start 1] [--inner-rtol 1e-3]
 
 Prints, per step, the status, FCG iterations, FP64 relative residual, the
 CUDA-event phase times (topology+sort, P2G, pressure, G2P; ms) and the running
@@ -20,15 +21,17 @@ def main():
     ap.add_argument("--scene", default="splash", choices=sorted(scenes.SCENES))
     ap.add_argument("--grid", type=int, default=256)
     ap.add_argument("--steps", type=int, default=2)
-    ap.add_argument("--precision", type=int, default=1)
+    ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--levels", type=int, default=0)
     ap.add_argument("--warm-start", type=int, default=1)
+    ap.add_argument("--inner-rtol", type=float, default=1e-3)
     args = ap.parse_args()
     soa, mass = scenes.SCENES[args.scene](args.grid)
     ctx = fb.LiquidContext(args.grid, capacity=soa.shape[1])
     ctx.upload(soa)
     tp = fb.transfer_params(scenes.DT, mass)
-    opt = fb.default_pressure_options(precision=args.precision, levels=args.levels, warm_start=args.warm_start)
+    opt = fb.default_pressure_options(precision=args.precision, levels=args.levels, warm_start=args.warm_start,
+                                      inner_rtol=args.inner_rtol)
     for s in range(args.steps):
         code, d = ctx.step(tp, opt)
         print(s, code, d.iterations, f"{d.relative_residual:.3e}", ctx.step_timings().round(4).tolist(),
