@@ -96,6 +96,9 @@ struct fl_context {
   // pressure solver: own stream (graph capture needs a non-legacy stream), the
   // replayed two-iteration FCG graph, handoff events and the natural-layout pressure
   cudaStream_t work = nullptr;
+  cudaStream_t cap = nullptr;  // graph capture only (overlaps the solver's setup on `work`)
+  long long fcg_key[8] = {};   // what the executable graphs were captured for
+  long long fcg_nn_key[8] = {};
   cudaGraphExec_t fcg_exec = nullptr;
   unsigned long long fcg_graph_kernels = 0;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -309,20 +312,20 @@ int capture_fcg(fl_context* c, const GridView& g, const MgHierarchy<T>& H, const
   cudaGraph_t graph = nullptr;
   const unsigned long long before = g_kernel_launches;
   const int a = 0, b = 1;
-  FL_CUDA(cudaStreamBeginCapture(c->work, cudaStreamCaptureModeThreadLocal));
+  FL_CUDA(cudaStreamBeginCapture(c->cap, cudaStreamCaptureModeThreadLocal));
   cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
   if (learned) {
     e1 = launch_fcg_iteration<T>(g, H, mo, c->r[a], c->r[b], c->d[a], c->d[b], c->q, c->e, c->partial, c->st,
-                                 &c->st->done, c->work, &c->nn_hook);
+                                 &c->st->done, c->cap, &c->nn_hook);
     e2 = launch_fcg_iteration<T>(g, H, mo, c->r[b], c->r[a], c->d[b], c->d[a], c->q, c->e, c->partial, c->st,
-                                 &c->st->done, c->work, &c->nn_hook);
+                                 &c->st->done, c->cap, &c->nn_hook);
   } else {
     e1 = launch_fcg_iteration<T>(g, H, mo, c->r[a], c->r[b], c->d[a], c->d[b], c->q, c->e, c->partial, c->st,
-                                 &c->st->done, c->work);
+                                 &c->st->done, c->cap);
     e2 = launch_fcg_iteration<T>(g, H, mo, c->r[b], c->r[a], c->d[b], c->d[a], c->q, c->e, c->partial, c->st,
-                                 &c->st->done, c->work);
+                                 &c->st->done, c->cap);
   }
-  cudaError_t e3 = cudaStreamEndCapture(c->work, &graph);
+  cudaError_t e3 = cudaStreamEndCapture(c->cap, &graph);
   *kernels = g_kernel_launches - before;
   g_kernel_launches = before;  // counted again at every replay
   if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
@@ -446,7 +449,26 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   bool converged = false;
   int status = FL_OK;
   const int max_ref = std::max(1, opt->max_refinements);
-  bool captured = false;
+  // (Re)capture the FCG graphs on the capture stream while `work` runs the
+  // setup; skipped when the block count and options match the last capture
+  // (pointers are fixed for the context's lifetime, grid sizes follow nb).
+  {
+    const long long key[8] = {c->nb, levels, mo.pre, mo.post, mo.coarse_sweeps, (long long)sizeof(T), 1, 0};
+    if (!c->fcg_exec || std::memcmp(key, c->fcg_key, sizeof(key)) != 0) {
+      st = capture_fcg<T>(c, g, H, mo, false, &c->fcg_exec, &c->fcg_graph_kernels);
+      if (st != FL_OK) return st;
+      std::memcpy(c->fcg_key, key, sizeof(key));
+    }
+    if (use_nn) {
+      const long long nkey[8] = {c->nb, levels, mo.pre, mo.post, mo.coarse_sweeps, (long long)sizeof(T),
+                                 (long long)(uintptr_t)c->nn_tc, c->nn_tc_items};
+      if (!c->fcg_nn_exec || std::memcmp(nkey, c->fcg_nn_key, sizeof(nkey)) != 0) {
+        st = capture_fcg<T>(c, g, H, mo, true, &c->fcg_nn_exec, &c->fcg_nn_kernels);
+        if (st != FL_OK) return st;
+        std::memcpy(c->fcg_nn_key, nkey, sizeof(nkey));
+      }
+    }
+  }
   for (int outer = 0; outer <= max_ref; ++outer) {
     FL_CUDA(launch_residual64<T>(g, H, c->b64, c->p64, c->r[0], c->e, c->partial, c->st, s));
     FL_CUDA(cudaMemcpyAsync(c->st_host, c->st, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
@@ -459,12 +481,6 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
     ++refinements;
     ++g_kernel_launches;
     k_set_inner_budget<<<1, 1, 0, s>>>(c->st, opt->max_iterations - total);
-    if (!captured) {
-      st = capture_fcg<T>(c, g, H, mo, false, &c->fcg_exec, &c->fcg_graph_kernels);
-      if (st == FL_OK && use_nn) st = capture_fcg<T>(c, g, H, mo, true, &c->fcg_nn_exec, &c->fcg_nn_kernels);
-      if (st != FL_OK) return st;
-      captured = true;
-    }
     for (;;) {
       const bool nn_now = use_nn && !c->st_host->fallback;
       FL_CUDA(cudaGraphLaunch(nn_now ? c->fcg_nn_exec : c->fcg_exec, s));
@@ -763,6 +779,7 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
   chk(dalloc(&c->p_nat, cells));
   chk(dalloc(&c->p_keep, cells));
   if (cudaStreamCreateWithFlags(&c->work, cudaStreamNonBlocking) != cudaSuccess) chk(FL_INTERNAL);
+  if (cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking) != cudaSuccess) chk(FL_INTERNAL);
   if (cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming) != cudaSuccess) chk(FL_INTERNAL);
   if (cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess) chk(FL_INTERNAL);
   configure_pressure_kernels();
@@ -859,6 +876,7 @@ int fl_context_destroy(fl_context* c) {
   cudaFree(c->nn_tc);
   cudaFree(c->nn_bt);
   if (c->work) cudaStreamDestroy(c->work);
+  if (c->cap) cudaStreamDestroy(c->cap);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
   for (int k = 0; k < 2; ++k) {
