@@ -33,10 +33,18 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "steps/s at 256^3 APIC (sparse splash, ~29.6M particles, projection to 1e-6 relative residual)"
 UNIT = "steps/s"
-WORKLOAD = {"workload": "splash_256", "grid": 256, "scene": "pool y<=0.2 + two r=0.15 spheres at +-2 m/s",
-            "particles_per_cell": 8, "dt": 1.0 / 240.0,
-            "precision": "fp32 transfers, fp32 V-cycle storage (bf16 measured beside), fp32 FCG, fp64 refinement",
-            "rel_tol": 1e-6, "l2": "inputs (1.8 GB of particles) larger than the 126 MB L2; no flush"}
+SCENES = {
+    "splash": "pool y<=0.2 + two r=0.15 spheres at +-2 m/s",
+    "column_drop": "column [0.1,0.3]x[0.1,0.8]x[0.1,0.3] falling into a pool y<=0.15",
+}
+
+
+def workload(scene: str, grid: int, precision: int):
+    return {"workload": f"{scene}_{grid}", "grid": grid, "scene": SCENES[scene], "particles_per_cell": 8,
+            "dt": 1.0 / 240.0,
+            "precision": "fp32 transfers, " + ("bf16" if precision else "fp32") + " V-cycle storage (the other "
+                         "measured beside), fp32 FCG, fp64 refinement",
+            "rel_tol": 1e-6, "l2": "inputs (particles, GBs) larger than the 126 MB L2; no flush"}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -130,7 +138,7 @@ def run_ours(args, world, rank, local):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    soa, mass = scenes.splash(args.grid)
+    soa, mass = scenes.SCENES[args.scene](args.grid)
     npart = soa.shape[1]
     ctx = fb.LiquidContext(args.grid, capacity=npart)
     tp = fb.transfer_params(scenes.DT, mass)
@@ -212,8 +220,9 @@ def run_ours(args, world, rank, local):
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded splash scene)",
-        "config": dict(WORKLOAD, particles=npart, active_blocks=nb, allocated_cells=ncell,
+        "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.scene} scene)",
+        "config": dict(workload(args.scene, args.grid, args.precision), particles=npart, active_blocks=nb,
+                       allocated_cells=ncell,
                        parallelism=f"replicas{world}"),
         "e2e": {"value": round(world * 1e3 / e2e_ms, 4), "unit": UNIT, "h2d_bytes_per_step": int(60 * npart),
                 "d2h_bytes_per_step": int(60 * npart)},
@@ -379,7 +388,7 @@ def run_reference(args, world, rank):
 
     if oracle.ref() is None:
         return {"impl": "reference", "unavailable": "reference CPU operators not built (oracle/ref/Makefile)"}
-    soa, mass = scenes.splash(args.grid)
+    soa, mass = scenes.SCENES[args.scene](args.grid)
     npart = soa.shape[1]
     threads = max(1, os.cpu_count() or 1)
     times = []
@@ -393,8 +402,8 @@ def run_reference(args, world, rank):
     value = 1.0 / float(np.mean(times))
     return {"metric": METRIC, "value": round(value, 8), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 / value, 2), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splash scene)",
-            "config": dict(WORKLOAD, particles=npart), "impl": "reference",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": f"synthetic (seeded {args.scene} scene)",
+            "config": dict(workload(args.scene, args.grid, args.precision), particles=npart), "impl": "reference",
             "cpu_baseline": {"value": round(value, 8), "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"per step: DepositMac3D+GatherMac3D on {20000 * threads} particles over "
                                        f"{threads} threads + ProjectMacPressure3D at 4096 cells, scaled to "
@@ -408,6 +417,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--grid", type=int, default=256)
+    ap.add_argument("--scene", default="splash", choices=sorted(SCENES),
+                    help="splash (256^3 headline) or column_drop (the 512^3 configuration)")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
                     help="V-cycle storage: 0 FP32 (default, fewer FCG iterations), 1 BF16")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])

@@ -72,6 +72,39 @@ def test_dam_break_32_step_10_matches_oracle_replay():
         assert e <= TOL, (k, e, errs)
 
 
+def test_dam_break_32_step_100_matches_oracle_replay():
+    """Config 1 runs 100 steps: the 100th step, replayed by the oracle from the GPU state."""
+    ctx, soa, m = dam_break_context(32)
+    tp = fb.transfer_params(scenes.DT, m)
+    opt = fb.default_pressure_options()
+    for _ in range(99):
+        code, _ = ctx.step(tp, opt)
+        assert code == fb.OK
+    errs, diag, _, _ = _compare_step(ctx, 32, ctx.download())
+    assert diag.relative_residual <= 1e-6
+    for k, e in errs.items():
+        assert e <= TOL, (k, e, errs)
+
+
+def test_dam_break_128_steps_10_and_200_match_oracle_replay():
+    """Config 2 (128^3, 4-level V-cycle): steps 10 and 200, each replayed by the
+    oracle from the GPU state of the step before."""
+    ctx, soa, m = dam_break_context(128)
+    tp = fb.transfer_params(scenes.DT, m)
+    opt = fb.default_pressure_options(levels=4)
+    done = 0
+    for check in (10, 200):
+        while done < check - 1:
+            code, _ = ctx.step(tp, opt)
+            assert code == fb.OK
+            done += 1
+        errs, diag, _, _ = _compare_step(ctx, 128, ctx.download(), levels=4)
+        done += 1
+        assert diag.relative_residual <= 1e-6
+        for k, e in errs.items():
+            assert e <= TOL, (check, k, e, errs)
+
+
 def test_dam_break_128_first_step_matches_oracle():
     """128^3 with the 4-level V-cycle (2 pre + 2 post red-black sweeps)."""
     ctx, soa, _ = dam_break_context(128)
