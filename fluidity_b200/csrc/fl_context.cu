@@ -105,6 +105,7 @@ struct fl_context {
   double* p_nat = nullptr;
   float* p_keep = nullptr;  // last pressure per lattice cell (warm start across topology changes)
   bool p_keep_valid = false;
+  bool occ_ready = false;  // occ holds the blocks of the current state (marked by the last fl_step's G2P)
   // learned preconditioner: FP32 parameters, per-block scales, the inference
   // activations (grown on demand to the active block count) and its own
   // one-iteration FCG graph
@@ -695,6 +696,46 @@ int upload_ref_particles(fl_context* c, const double* parts, uint64_t np, cudaSt
 
 // ======================================================================= C-ABI
 
+// G2P on sorted particles; occ_next (step mode only) receives the blocks of the
+// advected positions for the next topology.
+int g2p_impl(fl_context* c, fl_particles* sorted, const float* const u_new[3], const float* const u_old[3], float dt,
+             float* full_out, cudaStream_t s, fl_report* report, unsigned char* occ_next) {
+  reset_report(c, s);
+  GridView g = view(c);
+  ParticlesView pv = pview(sorted);
+  G2PParams prm{};
+  prm.dt = dt;
+  prm.occ_next = full_out ? nullptr : occ_next;
+  for (int d = 0; d < 3; ++d) {
+    const double lo = c->desc.solid_lo[d] == INT_MIN ? -1e30 : c->desc.origin[d] + (c->desc.solid_lo[d] + 1e-3) * c->desc.h;
+    const double hi =
+        c->desc.solid_hi[d] == INT_MAX ? 1e30 : c->desc.origin[d] + (c->desc.solid_hi[d] + 1 - 1e-3) * c->desc.h;
+    prm.clamp_lo[d] = (float)lo;
+    prm.clamp_hi[d] = (float)hi;
+  }
+  FL_CUDA(launch_g2p(g, pv, c->cell_start, u_new, u_old, prm, full_out, c->rep, s));
+  if (report) return read_report(c, s, report);
+  return FL_OK;
+}
+
+// Active blocks of the state about to be stepped: from the occupancy the last
+// step's G2P marked when it is current, else by marking the particles; then
+// occ is cleared for this step's G2P to mark.
+int step_topology(fl_context* c, const fl_particles* p, cudaStream_t s, fl_report* report) {
+  if (!c->occ_ready) return fl_topology_from_particles(c, p, s, report);
+  reset_report(c, s);
+  GridView g = view(c);
+  FL_CUDA(launch_topology_from_occupancy(g, c->occ, c->flag, c->ordinal, c->table, c->coord, c->nb_dev, c->temp,
+                                         c->temp_bytes, s));
+  FL_CUDA(cudaMemcpyAsync(c->nb_host, c->nb_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
+  const int err = read_report(c, s, report);
+  if (err != FL_OK) return err;
+  c->nb = *c->nb_host;
+  g = view(c);
+  FL_CUDA(launch_build_neighbors(g, c->nbr27, s));
+  return FL_OK;
+}
+
 extern "C" {
 
 int fl_runtime_info(int* compiled_architecture, int* device_count, int* device_major, int* device_minor) {
@@ -910,6 +951,7 @@ int fl_context_destroy(fl_context* c) {
 int fl_topology_from_particles(fl_context* c, const fl_particles* p, void* stream, fl_report* report) {
   if (!c || !p) return FL_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
+  c->occ_ready = false;
   reset_report(c, s);
   GridView g = view(c);
   ParticlesView pv = pview(p);
@@ -1023,22 +1065,8 @@ int fl_apply_vcycle(fl_context* c, const float* r, float* z, const fl_pressure_o
 int fl_g2p(fl_context* c, fl_particles* sorted, const float* const u_new[3], const float* const u_old[3], float dt,
            float* full_out, void* stream, fl_report* report) {
   if (!c || !sorted || !u_new) return FL_INVALID_ARGUMENT;
-  cudaStream_t s = (cudaStream_t)stream;
-  reset_report(c, s);
-  GridView g = view(c);
-  ParticlesView pv = pview(sorted);
-  G2PParams prm{};
-  prm.dt = dt;
-  for (int d = 0; d < 3; ++d) {
-    const double lo = c->desc.solid_lo[d] == INT_MIN ? -1e30 : c->desc.origin[d] + (c->desc.solid_lo[d] + 1e-3) * c->desc.h;
-    const double hi =
-        c->desc.solid_hi[d] == INT_MAX ? 1e30 : c->desc.origin[d] + (c->desc.solid_hi[d] + 1 - 1e-3) * c->desc.h;
-    prm.clamp_lo[d] = (float)lo;
-    prm.clamp_hi[d] = (float)hi;
-  }
-  FL_CUDA(launch_g2p(g, pv, c->cell_start, u_new, u_old, prm, full_out, c->rep, s));
-  if (report) return read_report(c, s, report);
-  return FL_OK;
+  if (!full_out) c->occ_ready = false;  // positions may move: the next topology marks again
+  return g2p_impl(c, sorted, u_new, u_old, dt, full_out, (cudaStream_t)stream, report, nullptr);
 }
 
 int fl_upload_particles(fl_context* c, const float* host, uint64_t count, void* stream) {
@@ -1048,6 +1076,7 @@ int fl_upload_particles(fl_context* c, const float* host, uint64_t count, void* 
   c->cur = 0;
   c->count = count;
   c->p_keep_valid = false;
+  c->occ_ready = false;
   for (int k = 0; k < 15; ++k)
     FL_CUDA(cudaMemcpyAsync(c->pbuf[0] + (size_t)k * c->pcap, host + (size_t)k * count, sizeof(float) * count,
                             cudaMemcpyHostToDevice, s));
@@ -1091,11 +1120,13 @@ int fl_step(fl_context* c, const fl_transfer_params* tp, const fl_pressure_optio
   fl_report rep{};
   c->phases_valid = false;
   cudaEventRecord(c->phase[0], s);
-  int st = fl_topology_from_particles(c, &A, stream, &rep);
+  int st = step_topology(c, &A, s, &rep);
   if (st != FL_OK) {
     if (report) *report = rep;
     return st;
   }
+  c->occ_ready = false;
+  FL_CUDA(cudaMemsetAsync(c->occ, 0, (size_t)c->lattice, s));  // this step's G2P marks the next topology
   struct StepScope {
     fl_context* c;
     ~StepScope() { c->in_step = false; }
@@ -1116,13 +1147,14 @@ int fl_step(fl_context* c, const fl_transfer_params* tp, const fl_pressure_optio
   const int pressure_status = st;
   cudaEventRecord(c->phase[3], s);
   const float* unc[3] = {c->u_new[0], c->u_new[1], c->u_new[2]};
-  st = fl_g2p(c, &B, unc, nullptr, (float)tp->dt, nullptr, stream, nullptr);
+  st = g2p_impl(c, &B, unc, nullptr, (float)tp->dt, nullptr, s, nullptr, c->occ);
   if (st != FL_OK) return st;
   cudaEventRecord(c->phase[4], s);
   c->phases_valid = true;
   c->cur = 1 - c->cur;
   const int err = read_report(c, s, report);
   if (err != FL_OK) return err;
+  c->occ_ready = true;
   return pressure_status;
 }
 

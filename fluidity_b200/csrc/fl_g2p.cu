@@ -48,10 +48,12 @@ __global__ void __launch_bounds__(kG2PThreads)
           const float* o0, const float* o1, const float* o2, G2PParams prm, float* full_out, DeviceReport* rep) {
   __shared__ float tile[3 * kTileFaces];
   __shared__ float tile_old[kFull ? 3 * kTileFaces : 1];
+  __shared__ unsigned int next_blocks;  // step mode: neighbouring blocks the advected particles land in
   const int b = blockIdx.x, t = threadIdx.x;
   if (b == 0 && t == 0 && rep != nullptr) rep->compiled_architecture = compiled_arch();
   const int pbeg = cell_start[b * kBlockCells], pend = cell_start[(b + 1) * kBlockCells];
   if (pbeg == pend) return;
+  if (t == 0) next_blocks = 0u;
   const float* un[3] = {u0, u1, u2};
   load_tile(g, b, un, tile, t);
   if (kFull) {
@@ -159,15 +161,42 @@ __global__ void __launch_bounds__(kG2PThreads)
         o[15 + k] = grad[k];
       }
     } else {
+      int off[3];
+      bool near = true, valid = true;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         p.v[d][q] = vel[d];
         float nx = xw[d] + prm.dt * vel[d];
         nx = fminf(fmaxf(nx, prm.clamp_lo[d]), prm.clamp_hi[d]);
         p.x[d][q] = nx;
+        // the next step's block of this particle (the cell rule of the sort)
+        const float Xn = lattice_coord(g, nx, d);
+        valid = valid && isfinite(Xn) && fabsf(Xn) < 1.0e9f;
+        const int nb_d = floor_div8(valid ? __float2int_rd(Xn) : 0);
+        off[d] = nb_d - bc[d] / 8;
+        near = near && off[d] >= -1 && off[d] <= 1;
+        valid = valid && nb_d - g.blo[d] >= 0 && nb_d - g.blo[d] < g.bdim[d];
       }
 #pragma unroll
       for (int k = 0; k < 9; ++k) p.c[k][q] = fit[k];
+      // Particles that leave the lattice are reported by the next sort; here they mark nothing.
+      if (prm.occ_next != nullptr && valid) {
+        if (near) {
+          atomicOr(&next_blocks, 1u << nbr_index(off[0], off[1], off[2]));
+        } else {
+          const int bx = bc[0] / 8 + off[0] - g.blo[0], by = bc[1] / 8 + off[1] - g.blo[1],
+                    bz = bc[2] / 8 + off[2] - g.blo[2];
+          prm.occ_next[((size_t)bz * g.bdim[1] + by) * g.bdim[0] + bx] = 1;
+        }
+      }
+    }
+  }
+  if (!kFull && prm.occ_next != nullptr) {
+    __syncthreads();
+    if (t < 27 && ((next_blocks >> t) & 1u)) {
+      const int bx = bc[0] / 8 + t % 3 - 1 - g.blo[0], by = bc[1] / 8 + (t / 3) % 3 - 1 - g.blo[1],
+                bz = bc[2] / 8 + t / 9 - 1 - g.blo[2];
+      prm.occ_next[((size_t)bz * g.bdim[1] + by) * g.bdim[0] + bx] = 1;
     }
   }
 }

@@ -178,17 +178,29 @@ __global__ void k_sort_cells(int ncell, const int* cell_start, unsigned int* slo
   }
 }
 
+// Gathers every attribute of particle index[s] into slot s. All 15 (16) loads
+// are issued before any store: the buffers may not be declared disjoint to the
+// compiler, and interleaving each load with its store would serialize 15 memory
+// round trips per particle.
 __global__ void k_permute(ParticlesView in, ParticlesView out, const unsigned int* index) {
   const unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
   if (s >= in.count) return;
   const unsigned int j = index[s];
+  float v[16];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) out.x[d][s] = in.x[d][j];
+  for (int d = 0; d < 3; ++d) v[d] = in.x[d][j];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) out.v[d][s] = in.v[d][j];
+  for (int d = 0; d < 3; ++d) v[3 + d] = in.v[d][j];
 #pragma unroll
-  for (int d = 0; d < 9; ++d) out.c[d][s] = in.c[d][j];
-  if (in.mass != nullptr) out.mass[s] = in.mass[j];
+  for (int d = 0; d < 9; ++d) v[6 + d] = in.c[d][j];
+  v[15] = in.mass != nullptr ? in.mass[j] : 0.0f;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) out.x[d][s] = v[d];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) out.v[d][s] = v[3 + d];
+#pragma unroll
+  for (int d = 0; d < 9; ++d) out.c[d][s] = v[6 + d];
+  if (in.mass != nullptr) out.mass[s] = v[15];
 }
 
 __global__ void k_write_arch(DeviceReport* rep) {
@@ -218,6 +230,20 @@ cudaError_t launch_topology_from_particles(const GridView& g, const ParticlesVie
     ++g_kernel_launches;
     k_mark_blocks<<<grid_for(p.count, 256), 256, 0, s>>>(g, p, occ, rep);
   }
+  ++g_kernel_launches;
+  k_flag_active<<<grid_for(total, 256), 256, 0, s>>>(g, occ, flag, total);
+  size_t tb = temp_bytes;
+  ++g_library_launches;
+  cub::DeviceScan::ExclusiveSum(temp, tb, flag, ordinal, total, s);
+  ++g_kernel_launches;
+  k_compact<<<grid_for(total, 256), 256, 0, s>>>(g, flag, ordinal, table, coord, total, nb_dev);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_topology_from_occupancy(const GridView& g, const unsigned char* occ, int* flag, int* ordinal,
+                                           int* table, int* coord, int* nb_dev, void* temp, size_t temp_bytes,
+                                           cudaStream_t s) {
+  const int total = g.bdim[0] * g.bdim[1] * g.bdim[2];
   ++g_kernel_launches;
   k_flag_active<<<grid_for(total, 256), 256, 0, s>>>(g, occ, flag, total);
   size_t tb = temp_bytes;

@@ -23,6 +23,9 @@ struct G2PParams {
   float dt;
   float clamp_lo[3];
   float clamp_hi[3];
+  // step mode: when set, the blocks of the advected positions are marked here
+  // (zeroed beforehand) for the next step's topology
+  unsigned char* occ_next = nullptr;
 };
 
 // One multigrid level. Sparse levels keep S^3 cells per active block; dense
@@ -94,6 +97,11 @@ extern unsigned long long g_kernel_launches;
 extern unsigned long long g_library_launches;
 
 size_t sort_temp_bytes(size_t particle_capacity, size_t cell_capacity);
+// Topology from an occupancy already marked (by the previous step's G2P): the
+// active blocks (occupied + one-block ring), their ordinals and coordinates.
+cudaError_t launch_topology_from_occupancy(const GridView& g, const unsigned char* occ, int* flag, int* ordinal,
+                                           int* table, int* coord, int* nb_dev, void* temp, size_t temp_bytes,
+                                           cudaStream_t s);
 cudaError_t launch_topology_from_particles(const GridView& g, const ParticlesView& p, unsigned char* occ, int* flag,
                                            int* ordinal, int* table, int* coord, int* nb_dev, void* temp,
                                            size_t temp_bytes, DeviceReport* rep, cudaStream_t s);

@@ -187,7 +187,11 @@ int fl_step_timings(fl_context* ctx, float* ms);
  * kernels, and device-wide CUB algorithm invocations (radix sort, scans). */
 int fl_kernel_launches(unsigned long long* own, unsigned long long* library);
 
-/* Context-resident particle state and buffers (device pointers). */
+/* Context-resident particle state and buffers (device pointers). fl_step
+ * records, in its G2P, which blocks the advected particles occupy and the next
+ * fl_step builds its topology from that record; a caller that writes positions
+ * through fl_state_particles' pointers between steps calls
+ * fl_topology_from_particles afterwards so the record is rebuilt. */
 int fl_upload_particles(fl_context* ctx, const float* host_soa, uint64_t count, void* stream);
 int fl_download_particles(fl_context* ctx, float* host_soa, void* stream);
 int fl_state_particles(fl_context* ctx, fl_particles* out);
