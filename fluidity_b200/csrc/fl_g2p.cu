@@ -180,10 +180,13 @@ __global__ void __launch_bounds__(kG2PThreads)
 #pragma unroll
       for (int k = 0; k < 9; ++k) p.c[k][q] = fit[k];
       // Particles that leave the lattice are reported by the next sort; here they mark nothing.
-      if (prm.occ_next != nullptr && valid) {
-        if (near) {
-          atomicOr(&next_blocks, 1u << nbr_index(off[0], off[1], off[2]));
-        } else {
+      if (prm.occ_next != nullptr) {
+        // one shared-memory OR per warp for the neighbouring blocks
+        const unsigned bit = valid && near ? 1u << nbr_index(off[0], off[1], off[2]) : 0u;
+        const unsigned active = __activemask();
+        const unsigned bits = __reduce_or_sync(active, bit);
+        if (bits != 0u && (threadIdx.x & 31) == __ffs(active) - 1) atomicOr(&next_blocks, bits);
+        if (valid && !near) {
           const int bx = bc[0] / 8 + off[0] - g.blo[0], by = bc[1] / 8 + off[1] - g.blo[1],
                     bz = bc[2] / 8 + off[2] - g.blo[2];
           prm.occ_next[((size_t)bz * g.bdim[1] + by) * g.bdim[0] + bx] = 1;

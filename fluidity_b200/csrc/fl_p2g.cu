@@ -167,7 +167,11 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
   const int b = blockIdx.x;
   const int t = threadIdx.x;
   const int base = b * kBlockCells;
-  if (cell_start[base] == cell_start[base + kBlockCells]) return;  // no particles: tile never read
+  float2* tile0 = tiles + (size_t)b * 3 * kTileFaces;
+  if (cell_start[base] == cell_start[base + kBlockCells]) {  // no particles: a zero tile for the merge
+    for (int n = t; n < 3 * kTileFaces; n += kP2GThreads) tile0[n] = make_float2(0.0f, 0.0f);
+    return;
+  }
   const int pbeg = cell_start[base + t], pend = cell_start[base + t + 1];
   const int cell[3] = {g.coord[3 * b] * 8 + (t & 7), g.coord[3 * b + 1] * 8 + ((t >> 3) & 7),
                        g.coord[3 * b + 2] * 8 + (t >> 6)};
@@ -190,6 +194,45 @@ __device__ __forceinline__ bool is_solid(const GridView& g, int x, int y, int z)
          z > g.solid_hi[2];
 }
 
+// Sum, in a fixed order, of the tile entries of the (at most 8) blocks whose
+// halo tile covers face `loc` of normal axis A in block b. Along each axis the
+// covering blocks are the face's own block and at most one neighbour: the lower
+// one when loc is within the neighbour tile's upper halo (loc <= 1 along the
+// normal axis, loc == 0 across it), the upper one when loc == 7. All candidate
+// loads are issued before the sum.
+template <int A>
+__device__ __forceinline__ float2 merge_face(const GridView& g, const float2* __restrict__ tiles, int b,
+                                             const int loc[3]) {
+  int alt[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) alt[d] = loc[d] <= (d == A ? 1 : 0) ? -1 : (loc[d] == 7 ? 1 : 0);
+  constexpr int e0 = A == 0 ? 11 : 10, e1 = A == 1 ? 11 : 10;
+  float2 v[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int sx = k & 1, sy = (k >> 1) & 1, sz = k >> 2;
+    const bool use = (!sx || alt[0] != 0) && (!sy || alt[1] != 0) && (!sz || alt[2] != 0);
+    const int dx = sx ? alt[0] : 0, dy = sy ? alt[1] : 0, dz = sz ? alt[2] : 0;
+    int nb = -1;
+    if (k == 0)
+      nb = b;
+    else if (use)
+      nb = g.nbr27[b * 27 + nbr_index(dx, dy, dz)];
+    v[k] = make_float2(0.0f, 0.0f);
+    if (nb >= 0) {
+      const int n = ((loc[2] - 8 * dz + 1) * e1 + (loc[1] - 8 * dy + 1)) * e0 + (loc[0] - 8 * dx + 1);
+      v[k] = tiles[((size_t)nb * 3 + A) * kTileFaces + n];
+    }
+  }
+  float2 r = make_float2(0.0f, 0.0f);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    r.x += v[k].x;
+    r.y += v[k].y;
+  }
+  return r;
+}
+
 // One thread per owned face: fixed-order sum of the covering tiles, then either
 // raw mass/momentum or normalize + gravity + stationary walls.
 __global__ void k_p2g_merge(GridView g, const int* cell_start, const float2* tiles, P2GMergeParams prm,
@@ -202,27 +245,9 @@ __global__ void k_p2g_merge(GridView g, const int* cell_start, const float2* til
   const int a = (int)((i / kBlockCells) % 3);
   const int l = (int)(i % kBlockCells);
   const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
-  float W = 0.0f, Q = 0.0f;
-  for (int dz = -1; dz <= 1; ++dz) {
-    const int nz = loc[2] - 8 * dz;
-    if (nz < -1 || nz > (a == 2 ? 9 : 8)) continue;
-    for (int dy = -1; dy <= 1; ++dy) {
-      const int ny = loc[1] - 8 * dy;
-      if (ny < -1 || ny > (a == 1 ? 9 : 8)) continue;
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int nx = loc[0] - 8 * dx;
-        if (nx < -1 || nx > (a == 0 ? 9 : 8)) continue;
-        const int nb = g.nbr27[b * 27 + nbr_index(dx, dy, dz)];
-        if (nb < 0) continue;
-        if (cell_start[nb * kBlockCells] == cell_start[(nb + 1) * kBlockCells]) continue;
-        const int e0 = a == 0 ? 11 : 10, e1 = a == 1 ? 11 : 10;
-        const int n = ((nz + 1) * e1 + (ny + 1)) * e0 + (nx + 1);
-        const float2 v = tiles[((size_t)nb * 3 + a) * kTileFaces + n];
-        W += v.x;
-        Q += v.y;
-      }
-    }
-  }
+  const float2 wq = a == 0 ? merge_face<0>(g, tiles, b, loc) : (a == 1 ? merge_face<1>(g, tiles, b, loc)
+                                                                       : merge_face<2>(g, tiles, b, loc));
+  const float W = wq.x, Q = wq.y;
   float* out0 = a == 0 ? out0_x : (a == 1 ? out0_y : out0_z);
   float* out1 = a == 0 ? out1_x : (a == 1 ? out1_y : out1_z);
   const size_t slot = (size_t)b * kBlockCells + l;
