@@ -55,6 +55,26 @@ def _dist():
     return world, rank, local
 
 
+def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's time: every rank contributes its own device-timed
+    milliseconds and all receive the maximum (identity on one rank). Replicas
+    exchange nothing else."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, steps: int, max_ms: float) -> float:
+    """Weak-scaling throughput: every replica advances `steps` steps of its own
+    scene, so the job completes world * steps steps in the slowest rank's time."""
+    return world * steps / (max_ms / 1e3)
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -186,12 +206,9 @@ def run_ours(args, world, rank, local):
     a1.record()
     torch.cuda.synchronize()
     alt_ms = a0.elapsed_time(a1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world)
     ms_per_step = ms / args.steps
-    value = world * args.steps / (ms / 1e3)
+    value = whole_job_rate(world, args.steps, ms)
     nb = len(ctx.active_blocks())
     ncell = nb * 512
     # end-to-end through the C-ABI with pinned host buffers: H2D state, step, D2H state
@@ -207,10 +224,7 @@ def run_ours(args, world, rank, local):
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, world)
     peak, peak_kind = _peaks()
     p2g_ms = phases[1] / args.steps
     p2g_bytes = 60.0 * npart + 24.0 * ncell
