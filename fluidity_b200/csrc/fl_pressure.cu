@@ -331,10 +331,17 @@ __global__ void k_level_diag(GridView g, LevelDesc L, LevelPtrs<T> lp) {
 // 256/(S^3/2) blocks. MODE 0: plain; 1: first sweep from x = 0 (no neighbour
 // reads); 2: neighbour values include the coarse correction (prolongation
 // fused into the first post-smoothing sweep).
+// Colour sweep on an in-block level (LS = 2: 4^3, LS = 1: 2^3 cells per block).
+// Every load a cell needs is issued before any result is used -- the cell's
+// flag, right-hand side and diagonal, the neighbour ordinals, then the
+// coefficients and neighbour values -- and neighbours with k == 0 are masked
+// rather than skipped, so a sweep costs one or two memory round trips instead of
+// four. The arithmetic (order of the fused multiply-adds) is unchanged.
 template <typename T, int LS, int MODE>
 __global__ void __launch_bounds__(kThreads)
     k_smooth_sparse(GridView g, LevelPtrs<T> lp, const float* __restrict__ b, int color, const T* __restrict__ xc,
                     int cdx, int cdy, const int* done) {
+  static_assert(LS == 1 || LS == 2, "level 0 has its own kernel");
   if (*done) return;
   constexpr int S = 1 << LS, S3 = S * S * S, HALF = S3 / 2, BPC = kThreads / HALF;
   const int t = threadIdx.x;
@@ -344,38 +351,30 @@ __global__ void __launch_bounds__(kThreads)
   const int z = j / (S * S / 2), rr = j % (S * S / 2), y = rr / (S / 2), xh = rr % (S / 2);
   const int x = 2 * xh + ((y + z + color) & 1);
   const int l = (z * S + y) * S + x;
-  const int i = LS == 3 ? blk * S3 + (color << 8) + j : blk * S3 + l;
-  unsigned m = 0;
-  if (LS == 3) {
-    m = lp.mask[i];
-    if (!(m & 64u)) return;
-  } else if (!lp.fluid[i]) {
-    return;
-  }
-  float s = b[i];
+  const int i = blk * S3 + l;
+  const bool fluid = lp.fluid[i] != 0;
+  const float bi = b[i];
+  const float di = lp.diag[i];
+  float s = bi;
   if (MODE != 1) {
+    int jn[6];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
+    for (int q = 0; q < 6; ++q) jn[q] = nbr_s<LS>(g, blk, l, q >> 1, (q & 1) ? 1 : -1);
+    float kq[6], xq[6];
 #pragma unroll
-      for (int dir = -1; dir <= 1; dir += 2) {
-        float k;
-        if (LS == 3) {
-          if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
-          k = 1.0f;
-        }
-        const int jn = nbr_s<LS>(g, blk, l, a, dir);
-        if (jn < 0) continue;
-        if (LS != 3) {
-          k = dir < 0 ? ld(&lp.k[a][i]) : ld(&lp.k[a][jn]);
-          if (k == 0.0f) continue;
-        }
-        float xj = ld(&lp.x[LS == 3 ? rb_id(jn) : jn]);
-        if (MODE == 2) xj += ld(&xc[parent_s<LS>(g, jn, cdx, cdy)]);
-        s = fmaf(k, xj, s);
-      }
+    for (int q = 0; q < 6; ++q) {
+      const int a = q >> 1;
+      const bool ok = jn[q] >= 0;
+      kq[q] = ok ? ((q & 1) ? ld(&lp.k[a][jn[q]]) : ld(&lp.k[a][i])) : 0.0f;
+      float xv = ok ? ld(&lp.x[jn[q]]) : 0.0f;
+      if (MODE == 2 && ok) xv += ld(&xc[parent_s<LS>(g, jn[q], cdx, cdy)]);
+      xq[q] = xv;
     }
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+      if (kq[q] != 0.0f) s = fmaf(kq[q], xq[q], s);
   }
-  st_T(&lp.x[i], s / lp.diag[i]);
+  if (fluid) st_T(&lp.x[i], s / di);
 }
 
 // Residual of a sparse level summed into the next level's RHS. 512 threads per
@@ -384,6 +383,7 @@ template <typename T, int LS>
 __global__ void __launch_bounds__(512)
     k_restrict_sparse(GridView g, LevelPtrs<T> fp, const float* __restrict__ fb, float* cb, int cdx, int cdy,
                       const int* done) {
+  static_assert(LS == 1 || LS == 2, "level 0 has its own kernel");
   if (*done) return;
   constexpr int S = 1 << LS, S3 = S * S * S, BPC = 512 / S3;
   __shared__ float r[512];
@@ -392,36 +392,28 @@ __global__ void __launch_bounds__(512)
   const int l = t % S3;
   float res = 0.0f;
   if (blk < g.nb) {
-    const int i = LS == 3 ? blk * S3 + rb_of(l) : blk * S3 + l;
-    unsigned m = 0;
-    bool fluid;
-    if (LS == 3) {
-      m = fp.mask[i];
-      fluid = (m & 64u) != 0;
-    } else {
-      fluid = fp.fluid[i] != 0;
+    const int i = blk * S3 + l;
+    const bool fluid = fp.fluid[i] != 0;
+    const float di = fp.diag[i];
+    const float xi = ld(&fp.x[i]);
+    const float bi = fb[i];
+    int jn[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) jn[q] = nbr_s<LS>(g, blk, l, q >> 1, (q & 1) ? 1 : -1);
+    float kq[6], xq[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const int a = q >> 1;
+      const bool ok = jn[q] >= 0;
+      kq[q] = ok ? ((q & 1) ? ld(&fp.k[a][jn[q]]) : ld(&fp.k[a][i])) : 0.0f;
+      xq[q] = ok ? ld(&fp.x[jn[q]]) : 0.0f;
     }
     if (fluid) {
-      float ax = fp.diag[i] * ld(&fp.x[i]);
+      float ax = di * xi;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-#pragma unroll
-        for (int dir = -1; dir <= 1; dir += 2) {
-          float k;
-          if (LS == 3) {
-            if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
-            k = 1.0f;
-          }
-          const int jn = nbr_s<LS>(g, blk, l, a, dir);
-          if (jn < 0) continue;
-          if (LS != 3) {
-            k = dir < 0 ? ld(&fp.k[a][i]) : ld(&fp.k[a][jn]);
-            if (k == 0.0f) continue;
-          }
-          ax = fmaf(-k, ld(&fp.x[LS == 3 ? rb_id(jn) : jn]), ax);
-        }
-      }
-      res = fb[i] - ax;
+      for (int q = 0; q < 6; ++q)
+        if (kq[q] != 0.0f) ax = fmaf(-kq[q], xq[q], ax);
+      res = bi - ax;
     }
   }
   r[t] = res;
@@ -688,6 +680,7 @@ __device__ __forceinline__ int dense_id(const LevelDesc& L, int x, int y, int z)
   return (z * L.dim[1] + y) * L.dim[0] + x;
 }
 
+// Colour sweep on a dense level (loads issued before use, as on the in-block levels).
 template <typename T, int MODE>
 __global__ void k_smooth_dense(LevelDesc L, LevelPtrs<T> lp, const float* __restrict__ b, int color, LevelDesc C,
                                const T* __restrict__ xc, const int* done) {
@@ -695,29 +688,36 @@ __global__ void k_smooth_dense(LevelDesc L, LevelPtrs<T> lp, const float* __rest
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L.count) return;
   const int x = i % L.dim[0], y = (i / L.dim[0]) % L.dim[1], z = i / (L.dim[0] * L.dim[1]);
-  if (((x + y + z + L.parity) & 1) != color || !lp.fluid[i]) return;
-  float s = b[i];
+  if (((x + y + z + L.parity) & 1) != color) return;
+  const bool fluid = lp.fluid[i] != 0;
+  const float bi = b[i];
+  const float di = lp.diag[i];
+  float s = bi;
   if (MODE != 1) {
     const int c[3] = {x, y, z};
+    float kq[6], xq[6];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-#pragma unroll
-      for (int dir = -1; dir <= 1; dir += 2) {
-        int n[3] = {c[0], c[1], c[2]};
-        n[a] += dir;
-        if (n[a] < 0 || n[a] >= L.dim[a]) continue;
-        const int jn = dense_id(L, n[0], n[1], n[2]);
-        const float k = dir < 0 ? ld(&lp.k[a][i]) : ld(&lp.k[a][jn]);
-        if (k == 0.0f) continue;
-        float xj = ld(&lp.x[jn]);
-        if (MODE == 2) xj += ld(&xc[dense_id(C, n[0] >> 1, n[1] >> 1, n[2] >> 1)]);
-        s = fmaf(k, xj, s);
-      }
+    for (int q = 0; q < 6; ++q) {
+      const int a = q >> 1, dir = (q & 1) ? 1 : -1;
+      int n[3] = {c[0], c[1], c[2]};
+      n[a] += dir;
+      const bool ok = n[a] >= 0 && n[a] < L.dim[a];
+      const int jn = ok ? dense_id(L, n[0], n[1], n[2]) : i;
+      kq[q] = ok ? (dir < 0 ? ld(&lp.k[a][i]) : ld(&lp.k[a][jn])) : 0.0f;
+      float xv = ok ? ld(&lp.x[jn]) : 0.0f;
+      if (MODE == 2 && ok) xv += ld(&xc[dense_id(C, n[0] >> 1, n[1] >> 1, n[2] >> 1)]);
+      xq[q] = xv;
     }
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+      if (kq[q] != 0.0f) s = fmaf(kq[q], xq[q], s);
   }
-  st_T(&lp.x[i], s / lp.diag[i]);
+  if (fluid) st_T(&lp.x[i], s / di);
 }
 
+// Dense-level residual restricted to the next level: one thread per coarse
+// cell sums its (up to 8) children's residuals in a fixed order; all child and
+// neighbour loads are issued before the sum.
 template <typename T>
 __global__ void k_restrict_dense(LevelDesc F, LevelPtrs<T> fp, const float* __restrict__ fb, LevelDesc C, float* cb,
                                  const int* done) {
@@ -726,29 +726,35 @@ __global__ void k_restrict_dense(LevelDesc F, LevelPtrs<T> fp, const float* __re
   if (i >= C.count) return;
   const int X = i % C.dim[0], Y = (i / C.dim[0]) % C.dim[1], Z = i / (C.dim[0] * C.dim[1]);
   float sum = 0.0f;
-  for (int dz = 0; dz < 2; ++dz)
-    for (int dy = 0; dy < 2; ++dy)
-      for (int dx = 0; dx < 2; ++dx) {
-        const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
-        if (x >= F.dim[0] || y >= F.dim[1] || z >= F.dim[2]) continue;
-        const int id = dense_id(F, x, y, z);
-        if (!fp.fluid[id]) continue;
-        float ax = fp.diag[id] * ld(&fp.x[id]);
-        const int c[3] = {x, y, z};
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
+  for (int ch = 0; ch < 8; ++ch) {
+    const int x = 2 * X + (ch & 1), y = 2 * Y + ((ch >> 1) & 1), z = 2 * Z + (ch >> 2);
+    const bool inside = x < F.dim[0] && y < F.dim[1] && z < F.dim[2];
+    const int id = inside ? dense_id(F, x, y, z) : 0;
+    const bool fluid = inside && fp.fluid[id] != 0;
+    const float di = inside ? fp.diag[id] : 0.0f;
+    const float xi = inside ? ld(&fp.x[id]) : 0.0f;
+    const float bi = inside ? fb[id] : 0.0f;
+    const int c[3] = {x, y, z};
+    float kq[6], xq[6];
 #pragma unroll
-          for (int dir = -1; dir <= 1; dir += 2) {
-            int n[3] = {c[0], c[1], c[2]};
-            n[a] += dir;
-            if (n[a] < 0 || n[a] >= F.dim[a]) continue;
-            const int jn = dense_id(F, n[0], n[1], n[2]);
-            const float k = dir < 0 ? ld(&fp.k[a][id]) : ld(&fp.k[a][jn]);
-            if (k != 0.0f) ax = fmaf(-k, ld(&fp.x[jn]), ax);
-          }
-        }
-        sum += fb[id] - ax;
-      }
+    for (int q = 0; q < 6; ++q) {
+      const int a = q >> 1, dir = (q & 1) ? 1 : -1;
+      int n[3] = {c[0], c[1], c[2]};
+      n[a] += dir;
+      const bool ok = inside && n[a] >= 0 && n[a] < F.dim[a];
+      const int jn = ok ? dense_id(F, n[0], n[1], n[2]) : 0;
+      kq[q] = ok ? (dir < 0 ? ld(&fp.k[a][id]) : ld(&fp.k[a][jn])) : 0.0f;
+      xq[q] = ok ? ld(&fp.x[jn]) : 0.0f;
+    }
+    if (fluid) {
+      float ax = di * xi;
+#pragma unroll
+      for (int q = 0; q < 6; ++q)
+        if (kq[q] != 0.0f) ax = fmaf(-kq[q], xq[q], ax);
+      sum += bi - ax;
+    }
+  }
   cb[i] = sum;
 }
 
