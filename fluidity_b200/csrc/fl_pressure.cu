@@ -205,22 +205,30 @@ __global__ void k_setup_level0(GridView g, const unsigned char* type, const floa
   double bb = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int b = i >> 9, l = i & 511;
+    // loads first (whatever the cell type), then the fluid cell's row
     const bool fluid = type[i] == 1;
+    const float pp = p_prev != nullptr ? p_prev[lattice_cell(g, b, l)] : 0.0f;
+    int tlo[3], thi[3];
+    float ul[3], uh[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int lo = nbr_s<3>(g, b, l, a, -1);
+      const int hi = nbr_s<3>(g, b, l, a, +1);
+      tlo[a] = nbr_type(type, lo);
+      thi[a] = nbr_type(type, hi);
+      ul[a] = u[a][i];
+      uh[a] = hi >= 0 ? u[a][hi] : 0.0f;
+    }
     float anchor = 0.0f;
     unsigned mask = fluid ? 64u : 0u;
     double div = 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const int lo = nbr_s<3>(g, b, l, a, -1);
-      const int hi = nbr_s<3>(g, b, l, a, +1);
-      const int tlo = nbr_type(type, lo), thi = nbr_type(type, hi);
       if (fluid) {
-        mask |= (tlo == 1 ? 1u : 0u) << (2 * a);
-        mask |= (thi == 1 ? 1u : 0u) << (2 * a + 1);
-        anchor += (tlo == 2 ? 1.0f : 0.0f) + (thi == 2 ? 1.0f : 0.0f);
-        const double ulo = (double)u[a][i];
-        const double uhi = hi >= 0 ? (double)u[a][hi] : 0.0;
-        div += uhi - ulo;
+        mask |= (tlo[a] == 1 ? 1u : 0u) << (2 * a);
+        mask |= (thi[a] == 1 ? 1u : 0u) << (2 * a + 1);
+        anchor += (tlo[a] == 2 ? 1.0f : 0.0f) + (thi[a] == 2 ? 1.0f : 0.0f);
+        div += (double)uh[a] - (double)ul[a];
       }
     }
     const int r = rb_id(i);
@@ -230,7 +238,7 @@ __global__ void k_setup_level0(GridView g, const unsigned char* type, const floa
     L0.diag[r] = fluid ? anchor + (float)__popc(mask & 63u) : 1.0f;
     const double rhs = fluid ? -rhs_scale * div : 0.0;
     b64[r] = rhs;
-    p64[r] = (fluid && p_prev != nullptr) ? (double)p_prev[lattice_cell(g, b, l)] : 0.0;
+    p64[r] = (fluid && p_prev != nullptr) ? (double)pp : 0.0;
     bb += rhs * rhs;
   }
   const double s = block_sum<kThreads>(bb, red);
@@ -859,15 +867,33 @@ __device__ __forceinline__ V apply0(const GridView& g, const LevelPtrs<T>& L0, u
 // r64 = b' - A p64 (FP64); r = (float)r64; e = 0; ||r64||^2. The last block
 // decides whether to stop and arms the inner solve.
 template <typename T>
-__global__ void k_residual64(GridView g, LevelPtrs<T> L0, const double* b64, const double* p64, float* r, float* e,
+__global__ void k_residual64(GridView g, LevelPtrs<T> L0, const double* __restrict__ b64,
+                             const double* __restrict__ p64, float* __restrict__ r, float* __restrict__ e,
                              double* partial, SolverState* st) {
   __shared__ double red[kThreads / 32];
   const int n = g.nb * kBlockCells;
   double rr = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    // all loads first (neighbour values whatever the mask says), then the
+    // same arithmetic as apply0: diag p_i minus the fluid neighbours in order
     const unsigned m = L0.mask[i];
+    const double bi = b64[i], pi = p64[i];
+    const double dg = (double)L0.diag[i];
+    const int b = i >> 9, l = nat_of(i & 511);
+    double pn[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const int jn = nbr_s<3>(g, b, l, q >> 1, (q & 1) ? 1 : -1);
+      pn[q] = jn >= 0 ? p64[rb_id(jn)] : 0.0;
+    }
     double res = 0.0;
-    if (m & 64u) res = b64[i] - apply0<T, double>(g, L0, m, i, p64[i], p64);
+    if (m & 64u) {
+      double ax = dg * pi;
+#pragma unroll
+      for (int q = 0; q < 6; ++q)
+        if ((m >> q) & 1u) ax -= pn[q];
+      res = bi - ax;
+    }
     r[i] = (float)res;
     e[i] = 0.0f;
     rr += res * res;
@@ -1026,13 +1052,16 @@ __global__ void k_correct_faces(GridView g, const unsigned char* type, const dou
   const int l = i & 511;
   const int head = b * kBlockCells + l;
   const int tail = nbr_s<3>(g, b, l, a, -1);
-  const int th = type[head], tt = nbr_type(type, tail);
   const float* up = a == 0 ? up0 : (a == 1 ? up1 : up2);
   float* un = a == 0 ? un0 : (a == 1 ? un1 : un2);
+  // loads first: types, velocity and both pressures (used only where fluid)
+  const int th = type[head], tt = nbr_type(type, tail);
   double u = (double)up[head];
+  const double ph_v = p64[rb_id(head)];
+  const double pt_v = tail >= 0 ? p64[rb_id(tail)] : 0.0;
   if (th != 0 && tt != 0 && (th == 1 || tt == 1)) {
-    const double ph = th == 1 ? p64[rb_id(head)] : 0.0;
-    const double pt = tt == 1 ? p64[rb_id(tail)] : 0.0;
+    const double ph = th == 1 ? ph_v : 0.0;
+    const double pt = tt == 1 ? pt_v : 0.0;
     u += scale * (pt - ph);
   }
   un[head] = (float)u;
@@ -1048,18 +1077,34 @@ __global__ void k_diagnostics(GridView g, const unsigned char* type, const doubl
   const float* up[3] = {up0, up1, up2};
   double maxdiv = 0.0, sumsq = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (type[i] != 1) continue;
+    const int ti = type[i];
     const int b = i >> 9, l = i & 511;
+    // loads first (whatever the cell types), then the divergence of fluid cells
+    int lo[3], hi[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = nbr_s<3>(g, b, l, a, -1);
+      hi[a] = nbr_s<3>(g, b, l, a, +1);
+    }
+    const double pi = p64[rb_id(i)];
+    int tlo[3], thi[3];
+    double ul[3], uh[3], pl[3], ph[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      tlo[a] = nbr_type(type, lo[a]);
+      thi[a] = nbr_type(type, hi[a]);
+      ul[a] = (double)up[a][i];
+      uh[a] = hi[a] >= 0 ? (double)up[a][hi[a]] : 0.0;
+      pl[a] = lo[a] >= 0 ? p64[rb_id(lo[a])] : 0.0;
+      ph[a] = hi[a] >= 0 ? p64[rb_id(hi[a])] : 0.0;
+    }
+    if (ti != 1) continue;
     double div = 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const int lo = nbr_s<3>(g, b, l, a, -1);
-      const int hi = nbr_s<3>(g, b, l, a, +1);
-      const int tlo = nbr_type(type, lo), thi = nbr_type(type, hi);
-      const double pi = p64[rb_id(i)];
-      double ulo = (double)up[a][i], uhi = hi >= 0 ? (double)up[a][hi] : 0.0;
-      if (tlo != 0) ulo += scale * ((tlo == 1 ? p64[rb_id(lo)] : 0.0) - pi);
-      if (thi != 0) uhi += scale * (pi - (thi == 1 ? p64[rb_id(hi)] : 0.0));
+      double ulo = ul[a], uhi = uh[a];
+      if (tlo[a] != 0) ulo += scale * ((tlo[a] == 1 ? pl[a] : 0.0) - pi);
+      if (thi[a] != 0) uhi += scale * (pi - (thi[a] == 1 ? ph[a] : 0.0));
       div += uhi - ulo;
     }
     maxdiv = fmax(maxdiv, fabs(div));
