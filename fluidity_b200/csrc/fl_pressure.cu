@@ -847,22 +847,6 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(LevelDesc L, LevelPtrs<T>
 
 // ----------------------------------------------------------------- CG kernels (level 0, grid-stride)
 
-// (A x)_i on level 0 from the neighbour mask: diag_i x_i - sum of fluid neighbours.
-template <typename T, typename V>
-__device__ __forceinline__ V apply0(const GridView& g, const LevelPtrs<T>& L0, unsigned m, int i, V xi,
-                                    const V* __restrict__ xv) {
-  const int b = i >> 9, l = nat_of(i & 511);
-  V ax = (V)L0.diag[i] * xi;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-#pragma unroll
-    for (int dir = -1; dir <= 1; dir += 2) {
-      if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
-      ax -= xv[rb_id(nbr_s<3>(g, b, l, a, dir))];
-    }
-  }
-  return ax;
-}
 
 // r64 = b' - A p64 (FP64); r = (float)r64; e = 0; ||r64||^2. The last block
 // decides whether to stop and arms the inner solve.
@@ -875,7 +859,7 @@ __global__ void k_residual64(GridView g, LevelPtrs<T> L0, const double* __restri
   double rr = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     // all loads first (neighbour values whatever the mask says), then the
-    // same arithmetic as apply0: diag p_i minus the fluid neighbours in order
+    // (A p)_i = diag_i p_i - sum of the fluid neighbours, in axis/direction order
     const unsigned m = L0.mask[i];
     const double bi = b64[i], pi = p64[i];
     const double dg = (double)L0.diag[i];
@@ -949,54 +933,6 @@ __global__ void k_dots(int n, const T* __restrict__ z, const float* __restrict__
       }
       st->beta = st->inner_iter == 0 ? 0.0 : (t0 - t1) / st->rz_prev;
       st->rz = t0;
-      st->ticket = 0;
-    }
-  }
-}
-
-// d = z + beta d_old; q = A d (neighbours' d formed on the fly); d.q -> alpha.
-template <typename T>
-__global__ void k_direction(GridView g, LevelPtrs<T> L0, const T* __restrict__ z, const float* __restrict__ d_old,
-                            float* __restrict__ d_new, float* __restrict__ q, double* partial, SolverState* st) {
-  if (st->done) return;
-  __shared__ double red[kThreads / 32];
-  const int n = g.nb * kBlockCells;
-  const float beta = (float)st->beta;
-  const bool first = st->inner_iter == 0;
-  double dq = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const unsigned m = L0.mask[i];
-    float di = 0.0f, qi = 0.0f;
-    if (m & 64u) {
-      di = first ? ld(&z[i]) : fmaf(beta, d_old[i], ld(&z[i]));
-      const int b = i >> 9, l = nat_of(i & 511);
-      float ax = L0.diag[i] * di;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-#pragma unroll
-        for (int dir = -1; dir <= 1; dir += 2) {
-          if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
-          const int j = rb_id(nbr_s<3>(g, b, l, a, dir));
-          ax -= first ? ld(&z[j]) : fmaf(beta, d_old[j], ld(&z[j]));
-        }
-      }
-      qi = ax;
-      dq += (double)di * (double)qi;
-    }
-    d_new[i] = di;
-    q[i] = qi;
-  }
-  const double s = block_sum<kThreads>(dq, red);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
-  if (last_block(st)) {
-    const double t = finish_sum(partial, 1, 0, red);
-    if (threadIdx.x == 0) {
-      if (!(t > 0.0) || !isfinite(t)) {
-        st->status = kAborted;
-        st->done = 1;
-      }
-      st->alpha = st->rz / t;
-      st->rz_prev = st->rz;
       st->ticket = 0;
     }
   }
