@@ -16,6 +16,8 @@ independent replica: the path has no data exchange between GPUs.
 from __future__ import annotations
 
 import argparse
+import atexit
+import datetime
 import json
 import os
 import statistics
@@ -84,12 +86,16 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons every 50 ms. The
+    sampler starts before the warm-up (nvidia-smi takes a moment to come up) and
+    only the samples stamped inside the timed window (mark_start / mark_stop)
+    are summarised."""
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -97,22 +103,30 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu),
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "--query-gpu=timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
                  "clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
         return self
 
+    def mark_start(self):
+        self.t0 = datetime.datetime.now()
+
+    def mark_stop(self):
+        self.t1 = datetime.datetime.now()
+
     def __exit__(self, *exc):
-        if self.proc is not None:
+        if self.proc is not None:  # idempotent: also called on error paths
+            time.sleep(0.1)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+            self.proc = None
 
     def summary(self):
         if not self.path or not os.path.exists(self.path):
@@ -123,10 +137,13 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             try:
-                sm.append(float(r[0]))
-                mx = max(mx, float(r[1]))
+                ts = datetime.datetime.strptime(r[0].strip(), "%Y/%m/%d %H:%M:%S.%f")
+                if self.t0 is not None and self.t1 is not None and not (self.t0 <= ts <= self.t1):
+                    continue
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
                 for k, name in enumerate(names):
-                    if r[3 + k].strip().lower() == "active":
+                    if r[4 + k].strip().lower() == "active":
                         reasons.add(name)
             except (ValueError, IndexError):
                 continue
@@ -164,6 +181,8 @@ def run_ours(args, world, rank, local):
     tp = fb.transfer_params(scenes.DT, mass)
     opt = fb.default_pressure_options(precision=args.precision, rel_tol=1e-6, warm_start=1, inner_rtol=1e-3)
     ctx.upload(soa)
+    clocks = ClockSampler(local).__enter__()
+    atexit.register(clocks.__exit__, None, None, None)  # never leave nvidia-smi running
     for _ in range(args.warmup):
         code, _ = ctx.step(tp, opt)
     torch.cuda.synchronize()
@@ -175,18 +194,20 @@ def run_ours(args, world, rank, local):
     iters = []
     residuals = []
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        torch.cuda.synchronize()
-        start.record()
-        for _ in range(args.steps):
-            code, diag = ctx.step(tp, opt)
-            phases += ctx.step_timings()
-            iters.append(diag.iterations)
-            residuals.append(diag.relative_residual)
-            if code != fb.OK:
-                raise RuntimeError(f"pressure did not converge: {diag.as_dict()}")
-        stop.record()
-        torch.cuda.synchronize()
+    torch.cuda.synchronize()
+    clocks.mark_start()
+    start.record()
+    for _ in range(args.steps):
+        code, diag = ctx.step(tp, opt)
+        phases += ctx.step_timings()
+        iters.append(diag.iterations)
+        residuals.append(diag.relative_residual)
+        if code != fb.OK:
+            raise RuntimeError(f"pressure did not converge: {diag.as_dict()}")
+    stop.record()
+    torch.cuda.synchronize()
+    clocks.mark_stop()
+    clocks.__exit__(None, None, None)
     launches1 = fb.kernel_launches()
     ms = start.elapsed_time(stop)
     nb_last = len(ctx.active_blocks())
