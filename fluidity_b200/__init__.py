@@ -182,7 +182,7 @@ def runtime_info():
 
 
 def default_pressure_options(precision: int = 0, rel_tol: float = 1e-6, levels: int = 0, pre: int = 2,
-                             post: int = 2, coarse_sweeps: int = 16, max_iterations: int = 400,
+                             post: int = 2, coarse_sweeps: int = 4, max_iterations: int = 400,
                              max_refinements: int = 6, inner_rtol: float = 1e-3,
                              warm_start: int = 0, preconditioner: int = 0, stall_limit: int = 3,
                              stall_ratio: float = 0.9) -> PressureOptions:
