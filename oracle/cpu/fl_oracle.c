@@ -897,12 +897,14 @@ int fo_step(const fo_box* b, const fo_step_params* prm, double* x, double* v, do
  * Level 0 (units of the full-face conductance): k = 1 on faces between two
  * fluid cells, anchor = number of air neighbours (Dirichlet p = 0), solid
  * neighbours contribute nothing. Level l+1 aggregates 2x2x2 cells: fluid if
- * any child is fluid, anchor = (sum of child anchors)/2, the low-face
+ * any child is fluid, anchor = 0.8 * (sum of child anchors), the low-face
  * coefficient = (sum of the four crossing fine coefficients)/2; diag = anchor
  * + the six face coefficients. Red-black Gauss-Seidel (red = even global
  * parity), `pre` sweeps red->black, restriction sums fluid-child residuals,
  * piecewise-constant prolongation, `post` sweeps black->red; the coarsest level
  * runs `coarse_sweeps` forward and `coarse_sweeps` backward sweeps from zero. */
+
+#define FO_COARSE_ANCHOR_SCALE 0.8
 
 typedef struct {
   int64_t n[3];
@@ -1051,7 +1053,7 @@ int fo_vcycle(const fo_box* b, const uint8_t* cell_type, int levels, int pre, in
         for (int64_t i = 0; i < F->n[0]; ++i) {
           const int64_t fid = mg_id(F, i, j, k), cid = mg_id(C, i / 2, j / 2, k / 2);
           if (F->fluid[fid]) C->fluid[cid] = 1;
-          C->anchor[cid] += 0.5 * F->anchor[fid];
+          C->anchor[cid] += FO_COARSE_ANCHOR_SCALE * F->anchor[fid];
           const int64_t c[3] = {i, j, k};
           for (int a = 0; a < 3; ++a)
             if ((c[a] & 1) == 0) C->k[a][cid] += 0.5 * F->k[a][fid];
