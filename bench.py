@@ -458,8 +458,8 @@ def main():
     ap.add_argument("--grid", type=int, default=256)
     ap.add_argument("--scene", default="splash", choices=sorted(SCENES),
                     help="splash (256^3 headline) or column_drop (the 512^3 configuration)")
-    ap.add_argument("--precision", type=int, default=0, choices=[0, 1],
-                    help="V-cycle storage: 0 FP32 (default, fewer FCG iterations), 1 BF16")
+    ap.add_argument("--precision", type=int, default=1, choices=[0, 1],
+                    help="V-cycle storage: 1 BF16 (default, the configured mixed precision), 0 FP32")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-MGPCG pressure comparison")
