@@ -106,33 +106,48 @@ __global__ void __launch_bounds__(kG2PThreads)
         for (int s = 0; s < 3; ++s) r[d][s] = (a0 + (float)s) - X[d];
       }
       const int e0 = tile_ext0(a), e1 = tile_ext1(a);
-      const float* ta = tile + a * kTileFaces;
+      const int n0 = ((first[2] - bc[2] + 1) * e1 + (first[1] - bc[1] + 1)) * e0 + (first[0] - bc[0] + 1);
+      const float* ta = tile + a * kTileFaces + n0;
+      const float* to = tile_old + (kFull ? a * kTileFaces + n0 : 0);
+      // The 27-node sums factor by axis: contract x (weights w0 and w0*r0, and
+      // for the full gather dw0 and the old field), then y, then z. Every
+      // output is the same sum of w-products times node values as the direct
+      // 27-term form, with about half the FP32 operations.
+      float wr[3][3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int s = 0; s < 3; ++s) wr[d][s] = w[d][s] * r[d][s];
       float pic = 0.0f, old = 0.0f, m0 = 0.0f, m1 = 0.0f, m2 = 0.0f, g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
 #pragma unroll
       for (int kz = 0; kz < 3; ++kz) {
-        const int iz = first[2] + kz - bc[2] + 1;
+        float V0 = 0.0f, V1 = 0.0f, V2 = 0.0f, V3 = 0.0f, V4 = 0.0f, V5 = 0.0f;
 #pragma unroll
         for (int ky = 0; ky < 3; ++ky) {
-          const int iy = first[1] + ky - bc[1] + 1;
-          const float wyz = w[1][ky] * w[2][kz];
-#pragma unroll
-          for (int kx = 0; kx < 3; ++kx) {
-            const int ix = first[0] + kx - bc[0] + 1;
-            const int n = (iz * e1 + iy) * e0 + ix;
-            const float un_v = ta[n];
-            const float wgt = w[0][kx] * wyz;
-            const float wn = wgt * un_v;
-            pic += wn;
-            m0 = fmaf(r[0][kx], wn, m0);
-            m1 = fmaf(r[1][ky], wn, m1);
-            m2 = fmaf(r[2][kz], wn, m2);
-            if (kFull) {
-              old = fmaf(wgt, tile_old[a * kTileFaces + n], old);
-              g0 = fmaf(dw[0][kx] * wyz, un_v, g0);
-              g1 = fmaf(w[0][kx] * dw[1][ky] * w[2][kz], un_v, g1);
-              g2 = fmaf(w[0][kx] * w[1][ky] * dw[2][kz], un_v, g2);
-            }
+          const int row = (kz * e1 + ky) * e0;
+          const float u0 = ta[row], u1 = ta[row + 1], u2 = ta[row + 2];
+          const float U0 = fmaf(w[0][2], u2, fmaf(w[0][1], u1, w[0][0] * u0));
+          const float U1 = fmaf(wr[0][2], u2, fmaf(wr[0][1], u1, wr[0][0] * u0));
+          V0 = fmaf(w[1][ky], U0, V0);
+          V1 = fmaf(w[1][ky], U1, V1);
+          V2 = fmaf(wr[1][ky], U0, V2);
+          if (kFull) {
+            const float Ud = fmaf(dw[0][2], u2, fmaf(dw[0][1], u1, dw[0][0] * u0));
+            const float O = fmaf(w[0][2], to[row + 2], fmaf(w[0][1], to[row + 1], w[0][0] * to[row]));
+            V3 = fmaf(w[1][ky], Ud, V3);
+            V4 = fmaf(dw[1][ky], U0, V4);
+            V5 = fmaf(w[1][ky], O, V5);
           }
+        }
+        pic = fmaf(w[2][kz], V0, pic);
+        m0 = fmaf(w[2][kz], V1, m0);
+        m1 = fmaf(w[2][kz], V2, m1);
+        m2 = fmaf(wr[2][kz], V0, m2);
+        if (kFull) {
+          g0 = fmaf(w[2][kz], V3, g0);
+          g1 = fmaf(w[2][kz], V4, g1);
+          g2 = fmaf(dw[2][kz], V0, g2);
+          old = fmaf(w[2][kz], V5, old);
         }
       }
       vel[a] = pic;

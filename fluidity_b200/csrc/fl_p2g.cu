@@ -73,11 +73,15 @@ __device__ __forceinline__ void p2g_component(const GridView& g, const Particles
                                               const int cell[3], float* part, int t, DeviceReport* rep) {
   constexpr int D1 = A == 0 ? 1 : 0;
   constexpr int D2 = A == 2 ? 1 : 2;
-  float accW[kSlots], accQ[kSlots];
+  // Accumulators in normal-axis slot pairs: entry (k * 3 + j) * 2 + hp holds
+  // normal slots 2hp (x) and 2hp + 1 (y) of transverse node (j, k). Each pair
+  // is updated by one packed FP32 FMA (fma.rn.f32x2), which rounds every lane
+  // exactly as fmaf does, so the sums are bitwise those of the scalar form.
+  float2 accW[kSlots / 2], accQ[kSlots / 2];
 #pragma unroll
-  for (int s = 0; s < kSlots; ++s) {
-    accW[s] = 0.0f;
-    accQ[s] = 0.0f;
+  for (int s = 0; s < kSlots / 2; ++s) {
+    accW[s] = make_float2(0.0f, 0.0f);
+    accQ[s] = make_float2(0.0f, 0.0f);
   }
   const float h = g.h;
   for (int q = pbeg; q < pend; ++q) {
@@ -93,42 +97,35 @@ __device__ __forceinline__ void p2g_component(const GridView& g, const Particles
     if (!(isfinite(m) && isfinite(va))) report_error(rep, kInvalidArgument, (unsigned long long)q);
     // Per node: W += wa*P and Q += wa*(P*q12) + (wa*ta)*P, with P the mass-scaled
     // transverse weight product and q12 = v_a + the transverse affine terms.
-    float wta[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) wta[s] = wa[s] * ta[s];
+    const float2 wa2[2] = {make_float2(wa[0], wa[1]), make_float2(wa[2], wa[3])};
+    const float2 wta2[2] = {__fmul2_rn(wa2[0], make_float2(ta[0], ta[1])),
+                            __fmul2_rn(wa2[1], make_float2(ta[2], ta[3]))};
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
         const float P = m * (w1[j] * w2[k]);
         const float PQ = P * (va + (t1[j] + t2[k]));
+        const float2 P2 = make_float2(P, P), PQ2 = make_float2(PQ, PQ);
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
-          int sx, sy, sz;
-          if (A == 0) {
-            sx = s;
-            sy = j;
-            sz = k;
-          } else if (A == 1) {
-            sx = j;
-            sy = s;
-            sz = k;
-          } else {
-            sx = j;
-            sy = k;
-            sz = s;
-          }
-          const int slot = slot_index<A>(sx, sy, sz);
-          accW[slot] = fmaf(wa[s], P, accW[slot]);
-          accQ[slot] = fmaf(wa[s], PQ, fmaf(wta[s], P, accQ[slot]));
+        for (int hp = 0; hp < 2; ++hp) {
+          const int e = (k * 3 + j) * 2 + hp;
+          accW[e] = __ffma2_rn(wa2[hp], P2, accW[e]);
+          accQ[e] = __ffma2_rn(wa2[hp], PQ2, __ffma2_rn(wta2[hp], P2, accQ[e]));
         }
       }
   }
 #pragma unroll
-  for (int s = 0; s < kSlots; ++s) {
-    part[s * kP2GThreads + t] = accW[s];
-    part[(kSlots + s) * kP2GThreads + t] = accQ[s];
-  }
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int slot = A == 0 ? slot_index<A>(s, j, k) : A == 1 ? slot_index<A>(j, s, k) : slot_index<A>(j, k, s);
+        const int e = (k * 3 + j) * 2 + (s >> 1);
+        part[slot * kP2GThreads + t] = (s & 1) ? accW[e].y : accW[e].x;
+        part[(kSlots + slot) * kP2GThreads + t] = (s & 1) ? accQ[e].y : accQ[e].x;
+      }
 }
 
 template <int A>
