@@ -465,23 +465,58 @@ __global__ void __launch_bounds__(512)
 // ----------------------------------------------------------------- tiled level-0 kernels
 
 // Face halo of block blk on level 0: for face f = 2a + (dir > 0), the 8x8
-// cells of the neighbouring block that touch it, indexed q = w*8 + u with
-// (u, w) the two transverse coordinates in increasing axis order. value(j)
-// maps a neighbour's natural cell id to the loaded value; missing blocks give 0.
-template <typename F>
-__device__ __forceinline__ void load_halo0(const GridView& g, int blk, float (*halo)[64], F value) {
-  for (int e = threadIdx.x; e < 384; e += blockDim.x) {
-    const int f = e >> 6, q = e & 63, a = f >> 1, dir = (f & 1) ? 1 : -1;
-    const int u = q & 7, w = q >> 3;
-    const int nbb = g.nbr27[blk * 27 + 13 + dir * (a == 0 ? 1 : (a == 1 ? 3 : 9))];
-    float v = 0.0f;
-    if (nbb >= 0) {
-      const int c = dir < 0 ? 7 : 0;
-      const int x = a == 0 ? c : u, y = a == 1 ? c : (a == 0 ? u : w), z = a == 2 ? c : w;
-      v = value(nbb * 512 + ((z << 6) | (y << 3) | x));
-    }
-    halo[f][q] = v;
+// cells of the neighbouring block that touch it, stored at f * 64 + w * 8 + u
+// with (u, w) the two transverse coordinates in increasing axis order. For
+// halo entry e in [0, 384) this gives the entry's slot and the natural id of
+// the neighbour cell it holds (-1 where the neighbouring block is missing).
+__device__ __forceinline__ int halo_src0(const GridView& g, int blk, int e, int* slot) {
+  const int f = e >> 6, q = e & 63, a = f >> 1, dir = (f & 1) ? 1 : -1;
+  const int u = q & 7, w = q >> 3;
+  *slot = e;
+  const int nbb = g.nbr27[blk * 27 + 13 + dir * (a == 0 ? 1 : (a == 1 ? 3 : 9))];
+  if (nbb < 0) return -1;
+  const int c = dir < 0 ? 7 : 0;
+  const int x = a == 0 ? c : u, y = a == 1 ? c : (a == 0 ? u : w), z = a == 2 ? c : w;
+  return nbb * 512 + ((z << 6) | (y << 3) | x);
+}
+
+// One-colour face halo: entry e in [0, 192) is one of the 32 cells of colour
+// oc on each face of the neighbouring blocks (the only ones a sweep of colour
+// 1 - oc reads), stored at the same slot as in the full halo.
+__device__ __forceinline__ int halo_src0_colour(const GridView& g, int blk, int oc, int e, int* slot) {
+  const int f = e >> 5, k = e & 31, a = f >> 1, dir = (f & 1) ? 1 : -1;
+  const int c = dir < 0 ? 7 : 0;  // plane of the neighbour block next to this face
+  const int w = k >> 2;
+  const int u = 2 * (k & 3) + ((oc + c + w) & 1);  // (c + u + w) & 1 == oc
+  *slot = f * 64 + ((w << 3) | u);
+  const int nbb = g.nbr27[blk * 27 + 13 + dir * (a == 0 ? 1 : (a == 1 ? 3 : 9))];
+  if (nbb < 0) return -1;
+  const int x = a == 0 ? c : u, y = a == 1 ? c : (a == 0 ? u : w), z = a == 2 ? c : w;
+  return nbb * 512 + ((z << 6) | (y << 3) | x);
+}
+
+// The halo entries e = t + k * NT (< COUNT) of thread t, loaded in two batches
+// (every neighbour-block lookup, then every value) before any shared store, so
+// a CTA waits for two memory round trips whatever its cells per thread.
+// value(j) maps a neighbour's natural cell id to the staged value.
+template <int NT, int COUNT, bool kColour, typename F>
+__device__ __forceinline__ void load_halo0(const GridView& g, int blk, int oc, float* halo, F value) {
+  constexpr int PER = (COUNT + NT - 1) / NT;
+  const int t = threadIdx.x;
+  int src[PER], slot[PER];
+  float v[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int e = t + k * NT;
+    src[k] = -1;
+    slot[k] = -1;
+    if (e < COUNT) src[k] = kColour ? halo_src0_colour(g, blk, oc, e, &slot[k]) : halo_src0(g, blk, e, &slot[k]);
   }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) v[k] = src[k] >= 0 ? value(src[k]) : 0.0f;
+#pragma unroll
+  for (int k = 0; k < PER; ++k)
+    if (slot[k] >= 0) halo[slot[k]] = v[k];
 }
 
 // Value of the neighbour of natural local cell (x,y,z) across axis a / dir,
@@ -497,113 +532,120 @@ __device__ __forceinline__ float tile_nbr0(const float* tile, const float (*halo
   return halo[2 * a + (dir > 0 ? 1 : 0)][q];
 }
 
+// A (natural local cell l) applied to the staged tile and halo, minus the
+// diagonal term: the sum of the neighbour values across the open faces in m.
+__device__ __forceinline__ float nbr_sum0(const float* tile, const float (*halo)[64], int l, unsigned m) {
+  const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
+  float s = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+#pragma unroll
+    for (int dir = -1; dir <= 1; dir += 2) {
+      if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
+      s += tile_nbr0(tile, halo, cx, cy, cz, a, dir);
+    }
+  }
+  return s;
+}
+
 __device__ __forceinline__ int parent1_of_nat(int j) {  // level-1 (4^3 per block) parent of a level-0 natural id
   const int b = j >> 9, l = j & 511;
   const int x = (l & 7) >> 1, y = ((l >> 3) & 7) >> 1, z = (l >> 6) >> 1;
   return b * 64 + (z << 4) + (y << 2) + x;
 }
 
-// Face halo of one colour: the 32 cells of each face of the neighbouring blocks
-// whose colour is `oc` (the only ones a sweep of colour 1 - oc reads), 192 in
-// all, one per thread for threads < 192; halo[f][q] as in load_halo0.
-template <typename F>
-__device__ __forceinline__ void load_halo0_colour(const GridView& g, int blk, int oc, float (*halo)[64], F value) {
-  const int e = threadIdx.x;
-  if (e >= 192) return;
-  const int f = e >> 5, k = e & 31, a = f >> 1, dir = (f & 1) ? 1 : -1;
-  const int c = dir < 0 ? 7 : 0;  // plane of the neighbour block next to this face
-  const int w = k >> 2;
-  const int u = 2 * (k & 3) + ((oc + c + w) & 1);  // (c + u + w) & 1 == oc
-  const int nbb = g.nbr27[blk * 27 + 13 + dir * (a == 0 ? 1 : (a == 1 ? 3 : 9))];
-  float v = 0.0f;
-  if (nbb >= 0) {
-    const int x = a == 0 ? c : u, y = a == 1 ? c : (a == 0 ? u : w), z = a == 2 ? c : w;
-    v = value(nbb * 512 + ((z << 6) | (y << 3) | x));
-  }
-  halo[f][(w << 3) | u] = v;
-}
+// Cells per thread of the tiled level-0 kernels. One CTA still covers one 8^3
+// block, so with fewer threads per block more blocks are resident per SM and
+// each thread keeps CPT independent loads in flight.
+constexpr int kSmooth0Cpt = 4;    // k_smooth0_tiled: 64 threads for the 256 cells of a colour
+constexpr int kRestrict0Cpt = 4;  // k_restrict0_tiled: 128 threads
+constexpr int kDirectionCpt = 4;  // k_direction_tiled: 128 threads
 
 // Red-black sweep of one colour on level 0 (MODE 0 plain, 2 prolongation
-// fused); MODE 1 (first sweep from zero) needs no neighbour values. The cell's
-// mask, right-hand side and diagonal are loaded before the neighbour values so
-// their latencies overlap.
-template <typename T, int MODE>
-__global__ void __launch_bounds__(256)
+// fused); MODE 1 (first sweep from zero) needs no neighbour values. The cells'
+// masks, right-hand sides and diagonals are loaded with the other colour's
+// values and the halo lookups, so their latencies overlap.
+template <typename T, int MODE, int CPT>
+__global__ void __launch_bounds__(256 / CPT)
     k_smooth0_tiled(GridView g, LevelPtrs<T> lp, const float* __restrict__ b, int color, const T* __restrict__ xc,
                     const int* done) {
+  constexpr int NT = 256 / CPT;
   if (*done) return;
   __shared__ float tile[512];
   __shared__ float halo[6][64];
   const int blk = blockIdx.x, t = threadIdx.x;
-  const int i = blk * 512 + (color << 8) + t;
-  const unsigned m = lp.mask[i];
-  const float bi = b[i];
-  const float di = lp.diag[i];
   const T* __restrict__ x = lp.x;
+  unsigned m[CPT];
+  float bi[CPT], di[CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int i = blk * 512 + (color << 8) + t + k * NT;
+    m[k] = lp.mask[i];
+    bi[k] = b[i];
+    di[k] = lp.diag[i];
+  }
   if (MODE != 1) {
     const int oc = 1 - color;
-    const int lo = nat_of((oc << 8) | t);
-    float v = ld(&x[blk * 512 + (oc << 8) + t]);
-    if (MODE == 2) v += ld(&xc[parent1_of_nat(blk * 512 + lo)]);
-    tile[lo] = v;
-    load_halo0_colour(g, blk, oc, halo, [&](int j) {
+    float v[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+      const int c = (oc << 8) + t + k * NT;
+      v[k] = ld(&x[blk * 512 + c]);
+      if (MODE == 2) v[k] += ld(&xc[parent1_of_nat(blk * 512 + nat_of(c))]);
+    }
+    load_halo0<NT, 192, true>(g, blk, oc, &halo[0][0], [&](int j) {
       float hv = ld(&x[rb_id(j)]);
       if (MODE == 2) hv += ld(&xc[parent1_of_nat(j)]);
       return hv;
     });
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) tile[nat_of((oc << 8) + t + k * NT)] = v[k];
     __syncthreads();
   }
-  if (!(m & 64u)) return;
-  float s = bi;
-  if (MODE != 1) {
-    const int l = nat_of((color << 8) | t);
-    const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-#pragma unroll
-      for (int dir = -1; dir <= 1; dir += 2) {
-        if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
-        s += tile_nbr0(tile, halo, cx, cy, cz, a, dir);
-      }
-    }
+  for (int k = 0; k < CPT; ++k) {
+    if (!(m[k] & 64u)) continue;
+    const int c = (color << 8) + t + k * NT;
+    float s = bi[k];
+    if (MODE != 1) s += nbr_sum0(tile, halo, nat_of(c), m[k]);
+    st_T(&lp.x[blk * 512 + c], s / di[k]);
   }
-  st_T(&lp.x[i], s / di);
 }
 
 // Level-0 residual restricted to level 1: all 512 cells of the block and its
 // face halos staged in shared memory.
-template <typename T>
-__global__ void __launch_bounds__(512)
+template <typename T, int CPT>
+__global__ void __launch_bounds__(512 / CPT)
     k_restrict0_tiled(GridView g, LevelPtrs<T> fp, const float* __restrict__ fb, float* __restrict__ cb,
                       const int* done) {
+  constexpr int NT = 512 / CPT;
+  static_assert(NT >= 64, "one thread per level-1 cell of the block");
   if (*done) return;
   __shared__ float tile[512];
   __shared__ float halo[6][64];
   __shared__ float r[512];
   const int blk = blockIdx.x, t = threadIdx.x;
-  const int i = blk * 512 + t;  // solver (red-black) index
-  const int l = nat_of(t);
-  const unsigned m = fp.mask[i];
-  const float di = fp.diag[i];
-  const float bi = fb[i];
-  tile[l] = ld(&fp.x[i]);
-  load_halo0(g, blk, halo, [&](int j) { return ld(&fp.x[rb_id(j)]); });
-  __syncthreads();
-  float res = 0.0f;
-  if (m & 64u) {
-    const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
-    float ax = di * tile[l];
+  unsigned m[CPT];
+  float di[CPT], bi[CPT], xv[CPT];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-#pragma unroll
-      for (int dir = -1; dir <= 1; dir += 2) {
-        if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
-        ax -= tile_nbr0(tile, halo, cx, cy, cz, a, dir);
-      }
-    }
-    res = bi - ax;
+  for (int k = 0; k < CPT; ++k) {
+    const int i = blk * 512 + t + k * NT;  // solver (red-black) index
+    m[k] = fp.mask[i];
+    di[k] = fp.diag[i];
+    bi[k] = fb[i];
+    xv[k] = ld(&fp.x[i]);
   }
-  r[l] = res;
+  load_halo0<NT, 384, false>(g, blk, 0, &halo[0][0], [&](int j) { return ld(&fp.x[rb_id(j)]); });
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) tile[nat_of(t + k * NT)] = xv[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int l = nat_of(t + k * NT);
+    float res = 0.0f;
+    if (m[k] & 64u) res = bi[k] - (di[k] * xv[k] - nbr_sum0(tile, halo, l, m[k]));
+    r[l] = res;
+  }
   __syncthreads();
   if (t < 64) {
     const int cx = t & 3, cy = (t >> 2) & 3, cz = t >> 4;
@@ -618,53 +660,52 @@ __global__ void __launch_bounds__(512)
   }
 }
 
-// d = z + beta d_old and q = A d for one block, d staged with its halo.
-// One CTA per block; d.q partials reduced by the last CTA.
-template <typename T>
-__global__ void __launch_bounds__(512)
+// d = z + beta d_old and q = A d for one block, d staged with its halo; the
+// block's d.q partial goes to partial[blk].
+template <typename T, int CPT>
+__global__ void __launch_bounds__(512 / CPT)
     k_direction_tiled(GridView g, LevelPtrs<T> L0, const T* __restrict__ z, const float* __restrict__ d_old,
                       float* __restrict__ d_new, float* __restrict__ q, double* partial, SolverState* st) {
+  constexpr int NT = 512 / CPT;
   if (st->done) return;
   __shared__ float tile[512];
   __shared__ float halo[6][64];
-  __shared__ double red[16];
+  __shared__ double red[NT / 32];
   const int blk = blockIdx.x, t = threadIdx.x;
   const float beta = (float)st->beta;
   const bool first = st->inner_iter == 0;
-  const int i = blk * 512 + t;
-  const int l = nat_of(t);
-  const unsigned m = L0.mask[i];
-  const float dg = L0.diag[i];
-  const float zi = ld(&z[i]);
-  const float di = (m & 64u) ? (first ? zi : fmaf(beta, d_old[i], zi)) : 0.0f;
-  tile[l] = di;
-  load_halo0(g, blk, halo, [&](int j) {
+  unsigned m[CPT];
+  float dg[CPT], di[CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int i = blk * 512 + t + k * NT;
+    m[k] = L0.mask[i];
+    dg[k] = L0.diag[i];
+    const float zi = ld(&z[i]), dold = d_old[i];
+    di[k] = (m[k] & 64u) ? (first ? zi : fmaf(beta, dold, zi)) : 0.0f;
+  }
+  load_halo0<NT, 384, false>(g, blk, 0, &halo[0][0], [&](int j) {
     const int r = rb_id(j);
     return first ? ld(&z[r]) : fmaf(beta, d_old[r], ld(&z[r]));
   });
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) tile[nat_of(t + k * NT)] = di[k];
   __syncthreads();
-  float qi = 0.0f;
-  if (m & 64u) {
-    const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
-    float ax = dg * di;
+  double dq = 0.0;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-#pragma unroll
-      for (int dir = -1; dir <= 1; dir += 2) {
-        if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
-        ax -= tile_nbr0(tile, halo, cx, cy, cz, a, dir);
-      }
-    }
-    qi = ax;
+  for (int k = 0; k < CPT; ++k) {
+    const int i = blk * 512 + t + k * NT;
+    float qi = 0.0f;
+    if (m[k] & 64u) qi = dg[k] * di[k] - nbr_sum0(tile, halo, nat_of(t + k * NT), m[k]);
+    d_new[i] = di[k];
+    q[i] = qi;
+    dq += (double)di[k] * (double)qi;
   }
-  d_new[i] = di;
-  q[i] = qi;
-  double dq = (double)di * (double)qi;
   dq = warp_sum(dq);
   if ((t & 31) == 0) red[t >> 5] = dq;
   __syncthreads();
   if (t < 32) {
-    double v = t < 16 ? red[t] : 0.0;
+    double v = t < NT / 32 ? red[t] : 0.0;
     v = warp_sum(v);
     if (t == 0) partial[blk] = v;
   }
@@ -917,10 +958,18 @@ __global__ void k_dots(int n, const T* __restrict__ z, const float* __restrict__
   if (st->done) return;
   __shared__ double red[kThreads / 32];
   double zr = 0.0, zp = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double zi = (double)ld(&z[i]);
-    zr += zi * (double)r[i];
-    zp += zi * (double)r_prev[i];
+  // Four cells per thread and iteration (n is a multiple of 512): 16-byte loads.
+  const float4* r4 = reinterpret_cast<const float4*>(r);
+  const float4* p4 = reinterpret_cast<const float4*>(r_prev);
+#pragma unroll 2
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n >> 2); i += gridDim.x * blockDim.x) {
+    float zv[4];
+    ld4(z + 4 * i, zv);
+    const float4 rv = r4[i], pv = p4[i];
+    zr += (double)zv[0] * (double)rv.x + (double)zv[1] * (double)rv.y + (double)zv[2] * (double)rv.z +
+          (double)zv[3] * (double)rv.w;
+    zp += (double)zv[0] * (double)pv.x + (double)zv[1] * (double)pv.y + (double)zv[2] * (double)pv.z +
+          (double)zv[3] * (double)pv.w;
   }
   const double s0 = block_sum<kThreads>(zr, red);
   const double s1 = block_sum<kThreads>(zp, red);
@@ -955,11 +1004,26 @@ __global__ void k_update(int n, const float* __restrict__ d, const float* __rest
   __shared__ double red[kThreads / 32];
   const float alpha = (float)st->alpha;
   double rr = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    e[i] = fmaf(alpha, d[i], e[i]);
-    const float rn = fmaf(-alpha, q[i], r[i]);
-    r_next[i] = rn;
-    rr += (double)rn * (double)rn;
+  // Four cells per thread and iteration (n is a multiple of 512): 16-byte accesses.
+  const float4* d4 = reinterpret_cast<const float4*>(d);
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  const float4* r4 = reinterpret_cast<const float4*>(r);
+  float4* e4 = reinterpret_cast<float4*>(e);
+  float4* n4 = reinterpret_cast<float4*>(r_next);
+#pragma unroll 2
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n >> 2); i += gridDim.x * blockDim.x) {
+    const float4 dv = d4[i], qv = q4[i], rv = r4[i];
+    float4 ev = e4[i];
+    ev.x = fmaf(alpha, dv.x, ev.x);
+    ev.y = fmaf(alpha, dv.y, ev.y);
+    ev.z = fmaf(alpha, dv.z, ev.z);
+    ev.w = fmaf(alpha, dv.w, ev.w);
+    const float4 rn = make_float4(fmaf(-alpha, qv.x, rv.x), fmaf(-alpha, qv.y, rv.y), fmaf(-alpha, qv.z, rv.z),
+                                  fmaf(-alpha, qv.w, rv.w));
+    e4[i] = ev;
+    n4[i] = rn;
+    rr += (double)rn.x * (double)rn.x + (double)rn.y * (double)rn.y + (double)rn.z * (double)rn.z +
+          (double)rn.w * (double)rn.w;
   }
   const double s = block_sum<kThreads>(rr, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
@@ -972,7 +1036,12 @@ __global__ void k_update(int n, const float* __restrict__ d, const float* __rest
       if (st->learned && !st->fallback) {
         st->learned_iter += 1;
         st->stalls = t < st->stall_ratio2 * st->rr_best ? 0 : st->stalls + 1;
-        if (st->stalls >= st->stall_limit) st->fallback = 1;
+        // A stalled learned solve ends here, like a breakdown in k_dots: the
+        // rest of the replayed graph would still apply the network.
+        if (st->stalls >= st->stall_limit) {
+          st->fallback = 1;
+          st->done = 1;
+        }
       }
       if (t < st->rr_best) st->rr_best = t;
       if (t <= st->stop2 || !isfinite(t) || st->inner_iter >= st->inner_max) st->done = 1;
@@ -1133,12 +1202,13 @@ static void smooth(const GridView& g, const MgHierarchy<T>& H, int l, const floa
   if (l == 0) {
     ++g_kernel_launches;
     const T* xc = H.ptr[1].x;
+    constexpr int C = kSmooth0Cpt, NT = 256 / C;
     if (mode == 1)
-      k_smooth0_tiled<T, 1><<<g.nb, 256, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
+      k_smooth0_tiled<T, 1, C><<<g.nb, NT, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
     else if (mode == 2)
-      k_smooth0_tiled<T, 2><<<g.nb, 256, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
+      k_smooth0_tiled<T, 2, C><<<g.nb, NT, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
     else
-      k_smooth0_tiled<T, 0><<<g.nb, 256, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
+      k_smooth0_tiled<T, 0, C><<<g.nb, NT, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
     return;
   }
   if (l == 1) return smooth_sparse<T, 2>(g, H, l, bl, color, mode, done, s);
@@ -1165,7 +1235,7 @@ static void restrict_level(const GridView& g, const MgHierarchy<T>& H, int l, co
     const int bpc = 512 / S3;
     const unsigned grid = (unsigned)((g.nb + bpc - 1) / bpc);
     if (l == 0)
-      k_restrict0_tiled<T><<<g.nb, 512, 0, s>>>(g, H.ptr[0], bl, H.b[1], done);
+      k_restrict0_tiled<T, kRestrict0Cpt><<<g.nb, 512 / kRestrict0Cpt, 0, s>>>(g, H.ptr[0], bl, H.b[1], done);
     else if (l == 1)
       k_restrict_sparse<T, 2><<<grid, 512, 0, s>>>(g, H.ptr[1], bl, H.b[2], C.dim[0], C.dim[1], done);
     else
@@ -1268,7 +1338,7 @@ cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, con
   const unsigned grid = reduce_grid(n);
   g_kernel_launches += 4;
   k_dots<T><<<grid, kThreads, 0, s>>>(n, z, r_cur, r_prev, partial, st);
-  k_direction_tiled<T><<<g.nb, 512, 0, s>>>(g, H.ptr[0], z, d_old, d_new, q, partial, st);
+  k_direction_tiled<T, kDirectionCpt><<<g.nb, 512 / kDirectionCpt, 0, s>>>(g, H.ptr[0], z, d_old, d_new, q, partial, st);
   k_direction_finish<<<1, 1024, 0, s>>>(g.nb, partial, st);
   k_update<<<grid, kThreads, 0, s>>>(n, d_new, q, r_cur, r_prev, e, partial, st);
   return cudaGetLastError();
