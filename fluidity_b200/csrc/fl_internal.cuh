@@ -116,6 +116,12 @@ template <>
 __device__ __forceinline__ float ld<__nv_bfloat16>(const __nv_bfloat16* p) {
   return __bfloat162float(*p);
 }
+// Programmatic dependent launch: blocks until the grid this kernel depends on
+// has completed and its writes are visible. A kernel launched with
+// programmatic stream serialization calls it first, before any early return;
+// launched without that attribute, it returns at once.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Four consecutive values from a 4-element-aligned position (16 B for FP32, 8 B for BF16).
 template <typename T>
 __device__ __forceinline__ void ld4(const T* p, float v[4]) {

@@ -360,6 +360,7 @@ __global__ void __launch_bounds__(kThreads)
     k_smooth_sparse(GridView g, LevelPtrs<T> lp, const float* __restrict__ b, int color, const T* __restrict__ xc,
                     int cdx, int cdy, const int* done) {
   static_assert(LS == 1 || LS == 2, "level 0 has its own kernel");
+  grid_dependency_wait();
   if (*done) return;
   constexpr int S = 1 << LS, S3 = S * S * S, HALF = S3 / 2, BPC = kThreads / HALF;
   const int t = threadIdx.x;
@@ -402,6 +403,7 @@ __global__ void __launch_bounds__(512)
     k_restrict_sparse(GridView g, LevelPtrs<T> fp, const float* __restrict__ fb, float* cb, int cdx, int cdy,
                       const int* done) {
   static_assert(LS == 1 || LS == 2, "level 0 has its own kernel");
+  grid_dependency_wait();
   if (*done) return;
   constexpr int S = 1 << LS, S3 = S * S * S, BPC = 512 / S3;
   __shared__ float r[512];
@@ -570,6 +572,7 @@ __global__ void __launch_bounds__(256 / CPT)
     k_smooth0_tiled(GridView g, LevelPtrs<T> lp, const float* __restrict__ b, int color, const T* __restrict__ xc,
                     const int* done) {
   constexpr int NT = 256 / CPT;
+  grid_dependency_wait();
   if (*done) return;
   __shared__ float tile[512];
   __shared__ float halo[6][64];
@@ -620,6 +623,7 @@ __global__ void __launch_bounds__(512 / CPT)
                       const int* done) {
   constexpr int NT = 512 / CPT;
   static_assert(NT >= 64, "one thread per level-1 cell of the block");
+  grid_dependency_wait();
   if (*done) return;
   __shared__ float tile[512];
   __shared__ float halo[6][64];
@@ -667,6 +671,7 @@ __global__ void __launch_bounds__(512 / CPT)
     k_direction_tiled(GridView g, LevelPtrs<T> L0, const T* __restrict__ z, const float* __restrict__ d_old,
                       float* __restrict__ d_new, float* __restrict__ q, double* partial, SolverState* st) {
   constexpr int NT = 512 / CPT;
+  grid_dependency_wait();
   if (st->done) return;
   __shared__ float tile[512];
   __shared__ float halo[6][64];
@@ -714,6 +719,7 @@ __global__ void __launch_bounds__(512 / CPT)
 // d.q over the per-block partials of k_direction_tiled, in block order, -> alpha.
 __global__ void __launch_bounds__(1024) k_direction_finish(int nb, const double* __restrict__ partial,
                                                            SolverState* st) {
+  grid_dependency_wait();
   if (st->done) return;
   __shared__ double red[32];
   double acc = 0.0;
@@ -743,6 +749,7 @@ __device__ __forceinline__ int dense_id(const LevelDesc& L, int x, int y, int z)
 template <typename T, int MODE>
 __global__ void k_smooth_dense(LevelDesc L, LevelPtrs<T> lp, const float* __restrict__ b, int color, LevelDesc C,
                                const T* __restrict__ xc, const int* done) {
+  grid_dependency_wait();
   if (*done) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L.count) return;
@@ -780,6 +787,7 @@ __global__ void k_smooth_dense(LevelDesc L, LevelPtrs<T> lp, const float* __rest
 template <typename T>
 __global__ void k_restrict_dense(LevelDesc F, LevelPtrs<T> fp, const float* __restrict__ fb, LevelDesc C, float* cb,
                                  const int* done) {
+  grid_dependency_wait();
   if (*done) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= C.count) return;
@@ -821,6 +829,7 @@ __global__ void k_restrict_dense(LevelDesc F, LevelPtrs<T> fp, const float* __re
 template <typename T>
 __global__ void __launch_bounds__(1024) k_coarse_solve(LevelDesc L, LevelPtrs<T> lp, const float* b, int sweeps,
                                                        const int* done) {
+  grid_dependency_wait();
   if (*done) return;
   extern __shared__ float sm[];
   const int n = (int)L.count;
@@ -955,6 +964,7 @@ __global__ void k_residual64(GridView g, LevelPtrs<T> L0, const double* __restri
 template <typename T>
 __global__ void k_dots(int n, const T* __restrict__ z, const float* __restrict__ r, const float* __restrict__ r_prev,
                        double* partial, SolverState* st) {
+  grid_dependency_wait();
   if (st->done) return;
   __shared__ double red[kThreads / 32];
   double zr = 0.0, zp = 0.0;
@@ -1000,6 +1010,7 @@ __global__ void k_dots(int n, const T* __restrict__ z, const float* __restrict__
 // e += alpha d; r_next = r - alpha q; ||r_next||^2 -> stop test.
 __global__ void k_update(int n, const float* __restrict__ d, const float* __restrict__ q, const float* __restrict__ r,
                          float* __restrict__ r_next, float* __restrict__ e, double* partial, SolverState* st) {
+  grid_dependency_wait();
   if (st->done) return;
   __shared__ double red[kThreads / 32];
   const float alpha = (float)st->alpha;
@@ -1180,6 +1191,28 @@ __global__ void k_from_rb(int n, const float* in_rb, float* out_nat) {
 
 // ----------------------------------------------------------------- host orchestration
 
+// Launch with programmatic stream serialization: the kernel may be scheduled
+// while its predecessor on the stream drains, hiding the launch gap between
+// the many short kernels of a V-cycle. Every kernel launched this way calls
+// grid_dependency_wait() before anything else, so it reads no input before the
+// predecessor grid has completed (and, the wait being unconditional, each
+// grid completes only after its own predecessor: the ordering is transitive).
+template <typename... P, typename... A>
+static void launch_dep(void (*kernel)(P...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                       A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<P>(args)...);  // a failure is left for cudaGetLastError()
+}
+
 template <typename T, int LS>
 static void smooth_sparse(const GridView& g, const MgHierarchy<T>& H, int l, const float* bl, int color, int mode,
                           const int* done, cudaStream_t s) {
@@ -1189,11 +1222,11 @@ static void smooth_sparse(const GridView& g, const MgHierarchy<T>& H, int l, con
   const T* xc = H.ptr[l + 1].x;
   ++g_kernel_launches;
   if (mode == 1)
-    k_smooth_sparse<T, LS, 1><<<grid, kThreads, 0, s>>>(g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
+    launch_dep(k_smooth_sparse<T, LS, 1>, grid, kThreads, 0, s, g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
   else if (mode == 2)
-    k_smooth_sparse<T, LS, 2><<<grid, kThreads, 0, s>>>(g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
+    launch_dep(k_smooth_sparse<T, LS, 2>, grid, kThreads, 0, s, g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
   else
-    k_smooth_sparse<T, LS, 0><<<grid, kThreads, 0, s>>>(g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
+    launch_dep(k_smooth_sparse<T, LS, 0>, grid, kThreads, 0, s, g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
 }
 
 template <typename T>
@@ -1204,11 +1237,11 @@ static void smooth(const GridView& g, const MgHierarchy<T>& H, int l, const floa
     const T* xc = H.ptr[1].x;
     constexpr int C = kSmooth0Cpt, NT = 256 / C;
     if (mode == 1)
-      k_smooth0_tiled<T, 1, C><<<g.nb, NT, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
+      launch_dep(k_smooth0_tiled<T, 1, C>, g.nb, NT, 0, s, g, H.ptr[0], bl, color, xc, done);
     else if (mode == 2)
-      k_smooth0_tiled<T, 2, C><<<g.nb, NT, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
+      launch_dep(k_smooth0_tiled<T, 2, C>, g.nb, NT, 0, s, g, H.ptr[0], bl, color, xc, done);
     else
-      k_smooth0_tiled<T, 0, C><<<g.nb, NT, 0, s>>>(g, H.ptr[0], bl, color, xc, done);
+      launch_dep(k_smooth0_tiled<T, 0, C>, g.nb, NT, 0, s, g, H.ptr[0], bl, color, xc, done);
     return;
   }
   if (l == 1) return smooth_sparse<T, 2>(g, H, l, bl, color, mode, done, s);
@@ -1218,11 +1251,11 @@ static void smooth(const GridView& g, const MgHierarchy<T>& H, int l, const floa
   const unsigned grid = blocks_for(D.count);
   ++g_kernel_launches;
   if (mode == 1)
-    k_smooth_dense<T, 1><<<grid, kThreads, 0, s>>>(D, H.ptr[l], bl, color, C, nullptr, done);
+    launch_dep(k_smooth_dense<T, 1>, grid, kThreads, 0, s, D, H.ptr[l], bl, color, C, nullptr, done);
   else if (mode == 2)
-    k_smooth_dense<T, 2><<<grid, kThreads, 0, s>>>(D, H.ptr[l], bl, color, C, H.ptr[l + 1].x, done);
+    launch_dep(k_smooth_dense<T, 2>, grid, kThreads, 0, s, D, H.ptr[l], bl, color, C, H.ptr[l + 1].x, done);
   else
-    k_smooth_dense<T, 0><<<grid, kThreads, 0, s>>>(D, H.ptr[l], bl, color, C, nullptr, done);
+    launch_dep(k_smooth_dense<T, 0>, grid, kThreads, 0, s, D, H.ptr[l], bl, color, C, nullptr, done);
 }
 
 template <typename T>
@@ -1235,14 +1268,14 @@ static void restrict_level(const GridView& g, const MgHierarchy<T>& H, int l, co
     const int bpc = 512 / S3;
     const unsigned grid = (unsigned)((g.nb + bpc - 1) / bpc);
     if (l == 0)
-      k_restrict0_tiled<T, kRestrict0Cpt><<<g.nb, 512 / kRestrict0Cpt, 0, s>>>(g, H.ptr[0], bl, H.b[1], done);
+      launch_dep(k_restrict0_tiled<T, kRestrict0Cpt>, g.nb, 512 / kRestrict0Cpt, 0, s, g, H.ptr[0], bl, H.b[1], done);
     else if (l == 1)
-      k_restrict_sparse<T, 2><<<grid, 512, 0, s>>>(g, H.ptr[1], bl, H.b[2], C.dim[0], C.dim[1], done);
+      launch_dep(k_restrict_sparse<T, 2>, grid, 512, 0, s, g, H.ptr[1], bl, H.b[2], C.dim[0], C.dim[1], done);
     else
-      k_restrict_sparse<T, 1><<<grid, 512, 0, s>>>(g, H.ptr[2], bl, H.b[3], C.dim[0], C.dim[1], done);
+      launch_dep(k_restrict_sparse<T, 1>, grid, 512, 0, s, g, H.ptr[2], bl, H.b[3], C.dim[0], C.dim[1], done);
     return;
   }
-  k_restrict_dense<T><<<blocks_for(C.count), kThreads, 0, s>>>(H.desc[l], H.ptr[l], bl, C, H.b[l + 1], done);
+  launch_dep(k_restrict_dense<T>, blocks_for(C.count), kThreads, 0, s, H.desc[l], H.ptr[l], bl, C, H.b[l + 1], done);
 }
 
 template <typename T>
@@ -1264,7 +1297,7 @@ static void vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r0, 
     const size_t smem = (size_t)C.count * 6 * sizeof(float);
     const int threads = C.count <= 1024 ? (int)((C.count + 31) / 32 * 32) : 1024;
     ++g_kernel_launches;
-    k_coarse_solve<T><<<1, threads, smem, s>>>(C, H.ptr[L - 1], H.b[L - 1], opt.coarse_sweeps, done);
+    launch_dep(k_coarse_solve<T>, 1, threads, smem, s, C, H.ptr[L - 1], H.b[L - 1], opt.coarse_sweeps, done);
   }
   for (int l = L - 2; l >= 0; --l) {
     const float* bl = l == 0 ? r0 : H.b[l];
@@ -1337,10 +1370,10 @@ cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, con
   const T* z = H.ptr[0].x;
   const unsigned grid = reduce_grid(n);
   g_kernel_launches += 4;
-  k_dots<T><<<grid, kThreads, 0, s>>>(n, z, r_cur, r_prev, partial, st);
-  k_direction_tiled<T, kDirectionCpt><<<g.nb, 512 / kDirectionCpt, 0, s>>>(g, H.ptr[0], z, d_old, d_new, q, partial, st);
-  k_direction_finish<<<1, 1024, 0, s>>>(g.nb, partial, st);
-  k_update<<<grid, kThreads, 0, s>>>(n, d_new, q, r_cur, r_prev, e, partial, st);
+  launch_dep(k_dots<T>, grid, kThreads, 0, s, n, z, r_cur, r_prev, partial, st);
+  launch_dep(k_direction_tiled<T, kDirectionCpt>, g.nb, 512 / kDirectionCpt, 0, s, g, H.ptr[0], z, d_old, d_new, q, partial, st);
+  launch_dep(k_direction_finish, 1, 1024, 0, s, g.nb, partial, st);
+  launch_dep(k_update, grid, kThreads, 0, s, n, d_new, q, r_cur, r_prev, e, partial, st);
   return cudaGetLastError();
 }
 
