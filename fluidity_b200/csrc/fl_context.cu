@@ -698,14 +698,21 @@ int upload_ref_particles(fl_context* c, const double* parts, uint64_t np, cudaSt
 
 // G2P on sorted particles; occ_next (step mode only) receives the blocks of the
 // advected positions for the next topology.
+// With `order` (step mode), particle q of the cell order is read from `in` at
+// order[q] and written to `sorted` at q.
 int g2p_impl(fl_context* c, fl_particles* sorted, const float* const u_new[3], const float* const u_old[3], float dt,
-             float* full_out, cudaStream_t s, fl_report* report, unsigned char* occ_next) {
+             float* full_out, cudaStream_t s, fl_report* report, unsigned char* occ_next,
+             const unsigned int* order = nullptr, const fl_particles* in = nullptr) {
   reset_report(c, s);
   GridView g = view(c);
   ParticlesView pv = pview(sorted);
   G2PParams prm{};
   prm.dt = dt;
   prm.occ_next = full_out ? nullptr : occ_next;
+  if (order != nullptr && in != nullptr && full_out == nullptr) {
+    prm.order = order;
+    for (int d = 0; d < 3; ++d) prm.x_in[d] = in->x[d];
+  }
   for (int d = 0; d < 3; ++d) {
     const double lo = c->desc.solid_lo[d] == INT_MIN ? -1e30 : c->desc.origin[d] + (c->desc.solid_lo[d] + 1e-3) * c->desc.h;
     const double hi =
@@ -1005,19 +1012,45 @@ int fl_active_blocks(fl_context* c, int32_t* coords, uint64_t capacity, uint64_t
   return FL_OK;
 }
 
-int fl_sort_particles_by_block(fl_context* c, const fl_particles* in, fl_particles* out, void* stream,
-                               fl_report* report) {
-  if (!c || !in || !out) return FL_INVALID_ARGUMENT;
-  if (in->count > c->pcap) return FL_RESOURCE_EXHAUSTED;
-  if ((in->mass == nullptr) != (out->mass == nullptr)) return FL_INVALID_ARGUMENT;
-  cudaStream_t s = (cudaStream_t)stream;
+// Sort by block and cell. permute = false (the step) leaves `out` unwritten:
+// c->index_alt then holds, for every cell-order slot, the particle of `in`.
+static int sort_impl(fl_context* c, const fl_particles* in, fl_particles* out, bool permute, cudaStream_t s,
+                     fl_report* report) {
   reset_report(c, s);
   GridView g = view(c);
   ParticlesView iv = pview(in), ov = pview(out);
   ov.count = in->count;
   FL_CUDA(launch_sort(g, iv, ov, c->keys, c->keys_alt, c->index, c->index_alt, c->counts, c->cell_start, c->temp,
-                      c->temp_bytes, c->rep, s));
+                      c->temp_bytes, c->rep, s, permute));
   out->count = in->count;
+  if (report) return read_report(c, s, report);
+  return FL_OK;
+}
+
+int fl_sort_particles_by_block(fl_context* c, const fl_particles* in, fl_particles* out, void* stream,
+                               fl_report* report) {
+  if (!c || !in || !out) return FL_INVALID_ARGUMENT;
+  if (in->count > c->pcap) return FL_RESOURCE_EXHAUSTED;
+  if ((in->mass == nullptr) != (out->mass == nullptr)) return FL_INVALID_ARGUMENT;
+  return sort_impl(c, in, out, true, (cudaStream_t)stream, report);
+}
+
+// P2G of the particles in cell order: slot q is particle q of `parts`, or
+// particle order[q] when an order is given (the step, which skips the permutation).
+static int p2g_impl(fl_context* c, const fl_particles* parts, const unsigned int* order, const fl_transfer_params* tp,
+                    int mode, float* const out0[3], float* const out1[3], cudaStream_t s, fl_report* report) {
+  reset_report(c, s);
+  GridView g = view(c);
+  ParticlesView pv = pview(parts);
+  P2GMergeParams prm{};
+  prm.mode = mode;
+  prm.walls = mode == 1 ? 1 : 0;
+  prm.mass_scale = parts->mass ? 1.0f : (float)tp->particle_mass;
+  prm.min_face_mass = (float)tp->min_face_mass;
+  prm.dt = (float)tp->dt;
+  for (int d = 0; d < 3; ++d) prm.gravity[d] = (float)tp->gravity[d];
+  float* o1[3] = {out1 ? out1[0] : nullptr, out1 ? out1[1] : nullptr, out1 ? out1[2] : nullptr};
+  FL_CUDA(launch_p2g(g, pv, c->cell_start, c->tiles, prm, out0, o1, c->rep, s, order));
   if (report) return read_report(c, s, report);
   return FL_OK;
 }
@@ -1025,21 +1058,7 @@ int fl_sort_particles_by_block(fl_context* c, const fl_particles* in, fl_particl
 int fl_p2g(fl_context* c, const fl_particles* sorted, const fl_transfer_params* tp, int mode, float* const out0[3],
            float* const out1[3], void* stream, fl_report* report) {
   if (!c || !sorted || !tp || !out0 || (mode == 0 && !out1)) return FL_INVALID_ARGUMENT;
-  cudaStream_t s = (cudaStream_t)stream;
-  reset_report(c, s);
-  GridView g = view(c);
-  ParticlesView pv = pview(sorted);
-  P2GMergeParams prm{};
-  prm.mode = mode;
-  prm.walls = mode == 1 ? 1 : 0;
-  prm.mass_scale = sorted->mass ? 1.0f : (float)tp->particle_mass;
-  prm.min_face_mass = (float)tp->min_face_mass;
-  prm.dt = (float)tp->dt;
-  for (int d = 0; d < 3; ++d) prm.gravity[d] = (float)tp->gravity[d];
-  float* o1[3] = {out1 ? out1[0] : nullptr, out1 ? out1[1] : nullptr, out1 ? out1[2] : nullptr};
-  FL_CUDA(launch_p2g(g, pv, c->cell_start, c->tiles, prm, out0, o1, c->rep, s));
-  if (report) return read_report(c, s, report);
-  return FL_OK;
+  return p2g_impl(c, sorted, nullptr, tp, mode, out0, out1, (cudaStream_t)stream, report);
 }
 
 int fl_pressure_project(fl_context* c, const float* const u_pred[3], float* const u_new[3],
@@ -1132,12 +1151,14 @@ int fl_step(fl_context* c, const fl_transfer_params* tp, const fl_pressure_optio
     ~StepScope() { c->in_step = false; }
   } scope{c};
   c->in_step = true;
-  st = fl_sort_particles_by_block(c, &A, &B, stream, nullptr);
+  // The particles are not permuted: P2G reads state A through the cell order
+  // and G2P writes the advected state into B in that order.
+  st = sort_impl(c, &A, &B, false, s, nullptr);
   if (st != FL_OK) return st;
   cudaEventRecord(c->phase[1], s);
   float* o0[3] = {c->u_pred[0], c->u_pred[1], c->u_pred[2]};
   float* o1[3] = {c->fmass[0], c->fmass[1], c->fmass[2]};
-  st = fl_p2g(c, &B, tp, 1, o0, o1, stream, nullptr);
+  st = p2g_impl(c, &A, c->index_alt, tp, 1, o0, o1, s, nullptr);
   if (st != FL_OK) return st;
   cudaEventRecord(c->phase[2], s);
   const float* up[3] = {c->u_pred[0], c->u_pred[1], c->u_pred[2]};
@@ -1147,7 +1168,7 @@ int fl_step(fl_context* c, const fl_transfer_params* tp, const fl_pressure_optio
   const int pressure_status = st;
   cudaEventRecord(c->phase[3], s);
   const float* unc[3] = {c->u_new[0], c->u_new[1], c->u_new[2]};
-  st = g2p_impl(c, &B, unc, nullptr, (float)tp->dt, nullptr, s, nullptr, c->occ);
+  st = g2p_impl(c, &B, unc, nullptr, (float)tp->dt, nullptr, s, nullptr, c->occ, c->index_alt, &A);
   if (st != FL_OK) return st;
   cudaEventRecord(c->phase[4], s);
   c->phases_valid = true;

@@ -70,9 +70,10 @@ __global__ void __launch_bounds__(kG2PThreads)
     float xw[3], X[3];
     int cell[3];
     bool inside = true;
+    const int src = (!kFull && prm.order != nullptr) ? (int)prm.order[q] : -1;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      xw[d] = p.x[d][q];
+      xw[d] = src >= 0 ? prm.x_in[d][src] : p.x[d][q];
       X[d] = lattice_coord(g, xw[d], d);
       cell[d] = __float2int_rd(X[d]);
       inside = inside && cell[d] >= bc[d] && cell[d] < bc[d] + 8;

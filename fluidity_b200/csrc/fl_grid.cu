@@ -264,7 +264,8 @@ cudaError_t launch_build_neighbors(const GridView& g, int* nbr27, cudaStream_t s
 
 cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const ParticlesView& out, unsigned int* keys,
                         unsigned int* keys_alt, unsigned int* index, unsigned int* index_alt, int* counts,
-                        int* cell_start, void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s) {
+                        int* cell_start, void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s,
+                        bool permute) {
   const size_t ncell = (size_t)g.nb * 512;
   cudaMemsetAsync(counts, 0, sizeof(int) * (ncell + 1), s);
   ++g_kernel_launches;
@@ -277,10 +278,10 @@ cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const Partic
   ++g_library_launches;
   cub::DeviceScan::ExclusiveSum(temp, tb, counts, cell_start, (int)(ncell + 1), s);
   if (in.count > 0) {
-    g_kernel_launches += 3;
+    g_kernel_launches += permute ? 3 : 2;
     k_scatter_index<<<grid_for(in.count, 256), 256, 0, s>>>(in.count, keys, index, cell_start, index_alt);
     k_sort_cells<<<grid_for(ncell, 256), 256, 0, s>>>((int)ncell, cell_start, index_alt);
-    k_permute<<<grid_for(in.count, 256), 256, 0, s>>>(in, out, index_alt);
+    if (permute) k_permute<<<grid_for(in.count, 256), 256, 0, s>>>(in, out, index_alt);
   }
   (void)keys_alt;
   return cudaGetLastError();

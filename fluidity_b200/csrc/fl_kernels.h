@@ -26,6 +26,11 @@ struct G2PParams {
   // step mode: when set, the blocks of the advected positions are marked here
   // (zeroed beforehand) for the next step's topology
   unsigned char* occ_next = nullptr;
+  // step mode: when set, particle q (in cell order) is read from x_in at
+  // order[q] (the unpermuted state) and written to the output view at q, so the
+  // step needs no separate permutation pass
+  const unsigned int* order = nullptr;
+  const float* x_in[3] = {nullptr, nullptr, nullptr};
 };
 
 // One multigrid level. Sparse levels keep S^3 cells per active block; dense
@@ -108,10 +113,11 @@ cudaError_t launch_topology_from_particles(const GridView& g, const ParticlesVie
 cudaError_t launch_build_neighbors(const GridView& g, int* nbr27, cudaStream_t s);
 cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const ParticlesView& out, unsigned int* keys,
                         unsigned int* keys_alt, unsigned int* index, unsigned int* index_alt, int* counts,
-                        int* cell_start, void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s);
+                        int* cell_start, void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s,
+                        bool permute = true);  // false: index_alt holds the cell order, `out` is not written
 cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cell_start, float2* tiles,
                        const P2GMergeParams& prm, float* const out0[3], float* const out1[3], DeviceReport* rep,
-                       cudaStream_t s);
+                       cudaStream_t s, const unsigned int* order = nullptr);  // order: particle of cell-order slot q
 cudaError_t launch_g2p(const GridView& g, const ParticlesView& p, const int* cell_start, const float* const u[3],
                        const float* const u_old[3], const G2PParams& prm, float* full_out, DeviceReport* rep,
                        cudaStream_t s);

@@ -69,8 +69,9 @@ __device__ __forceinline__ void axis_factors(float X, int cell, float h, float c
 }
 
 template <int A>
-__device__ __forceinline__ void p2g_component(const GridView& g, const ParticlesView& p, int pbeg, int pend,
-                                              const int cell[3], float* part, int t, DeviceReport* rep) {
+__device__ __forceinline__ void p2g_component(const GridView& g, const ParticlesView& p, const unsigned int* order,
+                                              int pbeg, int pend, const int cell[3], float* part, int t,
+                                              DeviceReport* rep) {
   constexpr int D1 = A == 0 ? 1 : 0;
   constexpr int D2 = A == 2 ? 1 : 2;
   // Accumulators in normal-axis slot pairs: entry (k * 3 + j) * 2 + hp holds
@@ -84,17 +85,22 @@ __device__ __forceinline__ void p2g_component(const GridView& g, const Particles
     accQ[s] = make_float2(0.0f, 0.0f);
   }
   const float h = g.h;
+  // The particle of cell-order slot q, with the next slot's entry loaded one
+  // iteration ahead so the order lookup overlaps the particle loads.
+  int next = order != nullptr && pbeg < pend ? (int)__ldg(&order[pbeg]) : pbeg;
   for (int q = pbeg; q < pend; ++q) {
+    const int i = next;
+    next = order != nullptr ? (q + 1 < pend ? (int)__ldg(&order[q + 1]) : 0) : q + 1;
     float X[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) X[d] = lattice_coord(g, __ldg(&p.x[d][q]), d);
-    const float m = p.mass ? __ldg(&p.mass[q]) : 1.0f;
-    const float va = __ldg(&p.v[A][q]);
+    for (int d = 0; d < 3; ++d) X[d] = lattice_coord(g, __ldg(&p.x[d][i]), d);
+    const float m = p.mass ? __ldg(&p.mass[i]) : 1.0f;
+    const float va = __ldg(&p.v[A][i]);
     float wa[4], ta[4], w1[4], t1[4], w2[4], t2[4];
-    axis_factors<true>(X[A], cell[A], h, __ldg(&p.c[3 * A + A][q]), wa, ta);
-    axis_factors<false>(X[D1], cell[D1], h, __ldg(&p.c[3 * A + D1][q]), w1, t1);
-    axis_factors<false>(X[D2], cell[D2], h, __ldg(&p.c[3 * A + D2][q]), w2, t2);
-    if (!(isfinite(m) && isfinite(va))) report_error(rep, kInvalidArgument, (unsigned long long)q);
+    axis_factors<true>(X[A], cell[A], h, __ldg(&p.c[3 * A + A][i]), wa, ta);
+    axis_factors<false>(X[D1], cell[D1], h, __ldg(&p.c[3 * A + D1][i]), w1, t1);
+    axis_factors<false>(X[D2], cell[D2], h, __ldg(&p.c[3 * A + D2][i]), w2, t2);
+    if (!(isfinite(m) && isfinite(va))) report_error(rep, kInvalidArgument, (unsigned long long)i);
     // Per node: W += wa*P and Q += wa*(P*q12) + (wa*ta)*P, with P the mass-scaled
     // transverse weight product and q12 = v_a + the transverse affine terms.
     const float2 wa2[2] = {make_float2(wa[0], wa[1]), make_float2(wa[2], wa[3])};
@@ -159,7 +165,8 @@ __device__ __forceinline__ void reduce_tile(const float* part, float2* tile, int
 }
 
 __global__ void __launch_bounds__(kP2GThreads, 1)
-    k_p2g_tile(GridView g, ParticlesView p, const int* cell_start, float2* tiles, DeviceReport* rep) {
+    k_p2g_tile(GridView g, ParticlesView p, const unsigned int* order, const int* cell_start, float2* tiles,
+               DeviceReport* rep) {
   extern __shared__ float part[];
   const int b = blockIdx.x;
   const int t = threadIdx.x;
@@ -173,15 +180,15 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
   const int cell[3] = {g.coord[3 * b] * 8 + (t & 7), g.coord[3 * b + 1] * 8 + ((t >> 3) & 7),
                        g.coord[3 * b + 2] * 8 + (t >> 6)};
   float2* tile = tiles + (size_t)b * 3 * kTileFaces;
-  p2g_component<0>(g, p, pbeg, pend, cell, part, t, rep);
+  p2g_component<0>(g, p, order, pbeg, pend, cell, part, t, rep);
   __syncthreads();
   reduce_tile<0>(part, tile, t);
   __syncthreads();
-  p2g_component<1>(g, p, pbeg, pend, cell, part, t, rep);
+  p2g_component<1>(g, p, order, pbeg, pend, cell, part, t, rep);
   __syncthreads();
   reduce_tile<1>(part, tile + kTileFaces, t);
   __syncthreads();
-  p2g_component<2>(g, p, pbeg, pend, cell, part, t, rep);
+  p2g_component<2>(g, p, order, pbeg, pend, cell, part, t, rep);
   __syncthreads();
   reduce_tile<2>(part, tile + 2 * kTileFaces, t);
 }
@@ -268,7 +275,7 @@ __global__ void k_p2g_merge(GridView g, const int* cell_start, const float2* til
 
 cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cell_start, float2* tiles,
                        const P2GMergeParams& prm, float* const out0[3], float* const out1[3], DeviceReport* rep,
-                       cudaStream_t s) {
+                       cudaStream_t s, const unsigned int* order) {
   if (g.nb == 0) return cudaSuccess;
   const size_t smem = sizeof(float) * 2 * kSlots * kP2GThreads;
   static bool configured = false;
@@ -277,7 +284,7 @@ cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cel
     configured = true;
   }
   ++g_kernel_launches;
-  k_p2g_tile<<<g.nb, kP2GThreads, smem, s>>>(g, p, cell_start, tiles, rep);
+  k_p2g_tile<<<g.nb, kP2GThreads, smem, s>>>(g, p, order, cell_start, tiles, rep);
   const long long faces = (long long)g.nb * 3 * kBlockCells;
   ++g_kernel_launches;
   k_p2g_merge<<<(unsigned)((faces + 255) / 256), 256, 0, s>>>(g, cell_start, tiles, prm, out0[0], out0[1], out0[2],
