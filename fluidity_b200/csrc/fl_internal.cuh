@@ -22,6 +22,22 @@
 
 namespace fl {
 
+// Host-side once-per-device flag: true the first time it is asked for the
+// current device (bit d of `mask` records device d). Set-up such as a
+// function's shared-memory attribute applies to the current device only, so
+// a process that drives several GPUs repeats it on each.
+inline bool first_on_device(unsigned long long& mask) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return true;
+  }
+  const unsigned long long bit = 1ull << dev;
+  if (mask & bit) return false;
+  mask |= bit;
+  return true;
+}
+
 constexpr int kBlockAxis = 8;
 constexpr int kBlockCells = 512;
 constexpr int kTileFaces = 1100;  // 11 x 10 x 10 faces per normal component

@@ -74,8 +74,8 @@ extern "C" int fl_p2g_static_scratch(const fl_static_grid* grid, const fl_partic
   if (st != FL_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
   // The report starts at zero for every call; the tiles need no clearing: the
-  // merge reads only tiles of blocks that hold particles, and the tile kernel
-  // overwrites all of those before the merge runs.
+  // tile kernel writes the tile of every block of this call (a zero tile for a
+  // block without particles) before the merge reads any of them.
   if (cudaMemsetAsync(rep, 0, sizeof(DeviceReport), s) != cudaSuccess) return FL_INTERNAL;
   GridView g{};
   for (int d = 0; d < 3; ++d) {

@@ -278,11 +278,9 @@ cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cel
                        cudaStream_t s, const unsigned int* order) {
   if (g.nb == 0) return cudaSuccess;
   const size_t smem = sizeof(float) * 2 * kSlots * kP2GThreads;
-  static bool configured = false;
-  if (!configured) {
+  static unsigned long long configured = 0;
+  if (first_on_device(configured))
     cudaFuncSetAttribute(k_p2g_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = true;
-  }
   ++g_kernel_launches;
   k_p2g_tile<<<g.nb, kP2GThreads, smem, s>>>(g, p, order, cell_start, tiles, rep);
   const long long faces = (long long)g.nb * 3 * kBlockCells;

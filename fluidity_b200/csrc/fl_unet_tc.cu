@@ -463,11 +463,9 @@ template <int KG, int N, int MODE, int IN_KIND, int OUT_KIND>
 cudaError_t launch_conv(const ConvArgs& a, int sms, cudaStream_t s) {
   constexpr size_t smem = conv_smem<KG, N, MODE, IN_KIND, OUT_KIND>();
   auto kern = k_conv_tc<KG, N, MODE, IN_KIND, OUT_KIND>;
-  static bool configured = false;
-  if (!configured) {
+  static unsigned long long configured = 0;
+  if (first_on_device(configured))
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = true;
-  }
   const int per_sm = (int)((227 * 1024) / smem);
   const int grid = a.nb < sms * per_sm ? a.nb : sms * per_sm;
   ++g_kernel_launches;
