@@ -123,12 +123,23 @@ __global__ void k_cell_keys(GridView g, ParticlesView p, unsigned int* keys, uns
     const int o = inside ? g.table[((size_t)b[2] * g.bdim[1] + b[1]) * g.bdim[0] + b[0]] : -1;
     if (o >= 0) {
       key = (unsigned int)o * 512u + (unsigned int)(l[2] * 64 + l[1] * 8 + l[0]);
-      rank = (unsigned int)atomicAdd(&counts[key], 1);
     } else {
       report_error(rep, kFailedPrecondition, i);
     }
   } else {
     report_error(rep, kOutOfRange, i);
+  }
+  // One counter update per cell present in the warp: particles arrive nearly in
+  // cell order (the previous step's), so most lanes share a few cells. Each lane
+  // of a group takes the group's base plus its position among the group's lanes;
+  // ranks within a cell are unique, and k_sort_cells fixes their final order.
+  const unsigned peers = __match_any_sync(__activemask(), key);
+  if (key != 0xffffffffu) {
+    const int lane = (int)(threadIdx.x & 31), leader = __ffs(peers) - 1;
+    unsigned int base = 0;
+    if (lane == leader) base = (unsigned int)atomicAdd(&counts[key], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    rank = base + (unsigned int)__popc(peers & ((1u << lane) - 1u));
   }
   keys[i] = key;
   index[i] = rank;  // arrival rank within the cell (order not yet deterministic)

@@ -101,17 +101,22 @@ __device__ __forceinline__ void p2g_component(const GridView& g, const Particles
     axis_factors<false>(X[D1], cell[D1], h, __ldg(&p.c[3 * A + D1][i]), w1, t1);
     axis_factors<false>(X[D2], cell[D2], h, __ldg(&p.c[3 * A + D2][i]), w2, t2);
     if (!(isfinite(m) && isfinite(va))) report_error(rep, kInvalidArgument, (unsigned long long)i);
-    // Per node: W += wa*P and Q += wa*(P*q12) + (wa*ta)*P, with P the mass-scaled
-    // transverse weight product and q12 = v_a + the transverse affine terms.
-    const float2 wa2[2] = {make_float2(wa[0], wa[1]), make_float2(wa[2], wa[3])};
+    // Per node: W += wa*P and Q += wa*(P*q12) + (wa*ta)*P, with wa the
+    // mass-scaled normal weight, P the transverse weight product and q12 = v_a
+    // plus the transverse affine terms (v_a + t1[j] formed once per j).
+    const float2 m2 = make_float2(m, m);
+    const float2 wa2[2] = {__fmul2_rn(m2, make_float2(wa[0], wa[1])), __fmul2_rn(m2, make_float2(wa[2], wa[3]))};
     const float2 wta2[2] = {__fmul2_rn(wa2[0], make_float2(ta[0], ta[1])),
                             __fmul2_rn(wa2[1], make_float2(ta[2], ta[3]))};
+    float q1[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) q1[j] = va + t1[j];
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        const float P = m * (w1[j] * w2[k]);
-        const float PQ = P * (va + (t1[j] + t2[k]));
+        const float P = w1[j] * w2[k];
+        const float PQ = P * (q1[j] + t2[k]);
         const float2 P2 = make_float2(P, P), PQ2 = make_float2(PQ, PQ);
 #pragma unroll
         for (int hp = 0; hp < 2; ++hp) {
