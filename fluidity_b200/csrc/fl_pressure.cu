@@ -470,13 +470,14 @@ __global__ void __launch_bounds__(512)
 // cells of the neighbouring block that touch it, stored at f * 64 + w * 8 + u
 // with (u, w) the two transverse coordinates in increasing axis order. For
 // halo entry e in [0, 384) this gives the entry's slot and the natural id of
-// the neighbour cell it holds (-1 where the neighbouring block is missing).
+// the neighbour cell it holds (where the neighbouring block is missing, its
+// nbr27 code: -1 inactive, -2 outside the lattice).
 __device__ __forceinline__ int halo_src0(const GridView& g, int blk, int e, int* slot) {
   const int f = e >> 6, q = e & 63, a = f >> 1, dir = (f & 1) ? 1 : -1;
   const int u = q & 7, w = q >> 3;
   *slot = e;
   const int nbb = g.nbr27[blk * 27 + 13 + dir * (a == 0 ? 1 : (a == 1 ? 3 : 9))];
-  if (nbb < 0) return -1;
+  if (nbb < 0) return nbb;  // -1 inactive block (air), -2 outside the lattice (solid)
   const int c = dir < 0 ? 7 : 0;
   const int x = a == 0 ? c : u, y = a == 1 ? c : (a == 0 ? u : w), z = a == 2 ? c : w;
   return nbb * 512 + ((z << 6) | (y << 3) | x);
@@ -501,12 +502,12 @@ __device__ __forceinline__ int halo_src0_colour(const GridView& g, int blk, int 
 // (every neighbour-block lookup, then every value) before any shared store, so
 // a CTA waits for two memory round trips whatever its cells per thread.
 // value(j) maps a neighbour's natural cell id to the staged value.
-template <int NT, int COUNT, bool kColour, typename F>
-__device__ __forceinline__ void load_halo0(const GridView& g, int blk, int oc, float* halo, F value) {
+template <int NT, int COUNT, bool kColour, typename V, typename F>
+__device__ __forceinline__ void load_halo0(const GridView& g, int blk, int oc, V* halo, F value) {
   constexpr int PER = (COUNT + NT - 1) / NT;
   const int t = threadIdx.x;
   int src[PER], slot[PER];
-  float v[PER];
+  V v[PER];
 #pragma unroll
   for (int k = 0; k < PER; ++k) {
     const int e = t + k * NT;
@@ -515,7 +516,7 @@ __device__ __forceinline__ void load_halo0(const GridView& g, int blk, int oc, f
     if (e < COUNT) src[k] = kColour ? halo_src0_colour(g, blk, oc, e, &slot[k]) : halo_src0(g, blk, e, &slot[k]);
   }
 #pragma unroll
-  for (int k = 0; k < PER; ++k) v[k] = src[k] >= 0 ? value(src[k]) : 0.0f;
+  for (int k = 0; k < PER; ++k) v[k] = src[k] >= 0 ? value(src[k]) : V(0);
 #pragma unroll
   for (int k = 0; k < PER; ++k)
     if (slot[k] >= 0) halo[slot[k]] = v[k];
@@ -523,8 +524,8 @@ __device__ __forceinline__ void load_halo0(const GridView& g, int blk, int oc, f
 
 // Value of the neighbour of natural local cell (x,y,z) across axis a / dir,
 // from the in-block tile or the face halo.
-__device__ __forceinline__ float tile_nbr0(const float* tile, const float (*halo)[64], int x, int y, int z, int a,
-                                           int dir) {
+template <typename V>
+__device__ __forceinline__ V tile_nbr0(const V* tile, const V (*halo)[64], int x, int y, int z, int a, int dir) {
   const int c = a == 0 ? x : (a == 1 ? y : z);
   if (dir < 0 ? c > 0 : c < 7) {
     const int step = 1 << (3 * a);
@@ -562,6 +563,8 @@ __device__ __forceinline__ int parent1_of_nat(int j) {  // level-1 (4^3 per bloc
 constexpr int kSmooth0Cpt = 4;    // k_smooth0_tiled: 64 threads for the 256 cells of a colour
 constexpr int kRestrict0Cpt = 4;  // k_restrict0_tiled: 128 threads
 constexpr int kDirectionCpt = 4;  // k_direction_tiled: 128 threads
+constexpr int kResidualCpt = 4;   // k_residual64_tiled: 128 threads
+constexpr int kCorrectCpt = 4;    // k_correct_tiled: 128 threads
 
 // Red-black sweep of one colour on level 0 (MODE 0 plain, 2 prolongation
 // fused); MODE 1 (first sweep from zero) needs no neighbour values. The cells'
@@ -908,55 +911,80 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(LevelDesc L, LevelPtrs<T>
 // ----------------------------------------------------------------- CG kernels (level 0, grid-stride)
 
 
-// r64 = b' - A p64 (FP64); r = (float)r64; e = 0; ||r64||^2. The last block
-// decides whether to stop and arms the inner solve.
-template <typename T>
-__global__ void k_residual64(GridView g, LevelPtrs<T> L0, const double* __restrict__ b64,
-                             const double* __restrict__ p64, float* __restrict__ r, float* __restrict__ e,
-                             double* partial, SolverState* st) {
-  __shared__ double red[kThreads / 32];
-  const int n = g.nb * kBlockCells;
-  double rr = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    // all loads first (neighbour values whatever the mask says), then the
-    // (A p)_i = diag_i p_i - sum of the fluid neighbours, in axis/direction order
-    const unsigned m = L0.mask[i];
-    const double bi = b64[i], pi = p64[i];
-    const double dg = (double)L0.diag[i];
-    const int b = i >> 9, l = nat_of(i & 511);
-    double pn[6];
+// r64 = b' - A p64 (FP64) for one 8^3 block; r = (float)r64; e = 0; the
+// block's ||r64||^2 goes to partial[blk]. One CTA per block with CPT cells per
+// thread, p64 staged with its face halo (every load issued before any store).
+template <typename T, int CPT>
+__global__ void __launch_bounds__(512 / CPT)
+    k_residual64_tiled(GridView g, LevelPtrs<T> L0, const double* __restrict__ b64, const double* __restrict__ p64,
+                       float* __restrict__ r, float* __restrict__ e, double* partial) {
+  constexpr int NT = 512 / CPT;
+  __shared__ double tile[512];
+  __shared__ double halo[6][64];
+  __shared__ double red[NT / 32];
+  const int blk = blockIdx.x, t = threadIdx.x;
+  unsigned m[CPT];
+  double bi[CPT], pi[CPT], dg[CPT];
 #pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      const int jn = nbr_s<3>(g, b, l, q >> 1, (q & 1) ? 1 : -1);
-      pn[q] = jn >= 0 ? p64[rb_id(jn)] : 0.0;
-    }
+  for (int k = 0; k < CPT; ++k) {
+    const int i = blk * 512 + t + k * NT;  // solver (red-black) index
+    m[k] = L0.mask[i];
+    bi[k] = b64[i];
+    pi[k] = p64[i];
+    dg[k] = (double)L0.diag[i];
+  }
+  load_halo0<NT, 384, false>(g, blk, 0, &halo[0][0], [&](int j) { return p64[rb_id(j)]; });
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) tile[nat_of(t + k * NT)] = pi[k];
+  __syncthreads();
+  double rr = 0.0;
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int i = blk * 512 + t + k * NT, l = nat_of(t + k * NT);
+    const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
     double res = 0.0;
-    if (m & 64u) {
-      double ax = dg * pi;
+    if (m[k] & 64u) {  // (A p)_i = diag_i p_i - the fluid neighbours, in axis/direction order
+      double ax = dg[k] * pi[k];
 #pragma unroll
       for (int q = 0; q < 6; ++q)
-        if ((m >> q) & 1u) ax -= pn[q];
-      res = bi - ax;
+        if ((m[k] >> q) & 1u) ax -= tile_nbr0(tile, halo, cx, cy, cz, q >> 1, (q & 1) ? 1 : -1);
+      res = bi[k] - ax;
     }
     r[i] = (float)res;
     e[i] = 0.0f;
     rr += res * res;
   }
-  const double s = block_sum<kThreads>(rr, red);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
-  if (last_block(st)) {
-    const double t = finish_sum(partial, 1, 0, red);
-    if (threadIdx.x == 0) {
-      st->res64 = sqrt(t);
-      const double target = st->target;
-      st->converged = st->res64 <= target ? 1 : 0;
-      const double stop = fmax(st->inner_rtol * st->res64, 0.5 * target);
-      st->stop2 = stop * stop;
-      st->inner_iter = 0;
-      st->done = st->converged;
-      if (t < st->rr_best) st->rr_best = t;
-      st->ticket = 0;
-    }
+  rr = warp_sum(rr);
+  if ((t & 31) == 0) red[t >> 5] = rr;
+  __syncthreads();
+  if (t < 32) {
+    double v = t < NT / 32 ? red[t] : 0.0;
+    v = warp_sum(v);
+    if (t == 0) partial[blk] = v;
+  }
+}
+
+// ||r64|| over the per-block partials, in block order; decides whether to stop
+// and arms the inner solve.
+__global__ void __launch_bounds__(1024) k_residual64_finish(int nb, const double* __restrict__ partial,
+                                                            SolverState* st) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) acc += partial[k];
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    st->res64 = sqrt(t);
+    const double target = st->target;
+    st->converged = st->res64 <= target ? 1 : 0;
+    const double stop = fmax(st->inner_rtol * st->res64, 0.5 * target);
+    st->stop2 = stop * stop;
+    st->inner_iter = 0;
+    st->done = st->converged;
+    if (t < st->rr_best) st->rr_best = t;
   }
 }
 
@@ -1066,104 +1094,153 @@ __global__ void k_accumulate(int n, const float* e, double* p64) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p64[i] += (double)e[i];
 }
 
-// Corrected face velocities: u_new = u_pred + scale (p_tail - p_head) on faces
-// with a fluid side and no solid side (air pressure 0); other faces keep u_pred.
-__global__ void k_correct_faces(GridView g, const unsigned char* type, const double* p64, const float* up0,
-                                const float* up1, const float* up2, float* un0, float* un1, float* un2,
-                                double scale) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.nb * 3 * kBlockCells) return;
-  const int b = i / (3 * kBlockCells);
-  const int a = (i >> 9) % 3;
-  const int l = i & 511;
-  const int head = b * kBlockCells + l;
-  const int tail = nbr_s<3>(g, b, l, a, -1);
-  const float* up = a == 0 ? up0 : (a == 1 ? up1 : up2);
-  float* un = a == 0 ? un0 : (a == 1 ? un1 : un2);
-  // loads first: types, velocity and both pressures (used only where fluid)
-  const int th = type[head], tt = nbr_type(type, tail);
-  double u = (double)up[head];
-  const double ph_v = p64[rb_id(head)];
-  const double pt_v = tail >= 0 ? p64[rb_id(tail)] : 0.0;
-  if (th != 0 && tt != 0 && (th == 1 || tt == 1)) {
-    const double ph = th == 1 ? ph_v : 0.0;
-    const double pt = tt == 1 ? pt_v : 0.0;
-    u += scale * (pt - ph);
-  }
-  un[head] = (float)u;
-}
-
-// Post-projection divergence over fluid cells from the FP64 correction of the
-// FP32 predicted velocities: l2 and max, in m/s summed over a cell's faces.
-__global__ void k_diagnostics(GridView g, const unsigned char* type, const double* p64, const float* up0,
-                              const float* up1, const float* up2, double scale, double* partial, SolverState* st) {
-  __shared__ double red[kThreads / 32];
-  __shared__ double mx[kThreads / 32];
-  const int n = g.nb * kBlockCells;
+// Corrected face velocities and the post-projection divergence, one CTA per
+// 8^3 block with CPT cells per thread. Each owned (low) face gets
+// u_new = u_pred + scale (p_tail - p_head) where it has a fluid side and no
+// solid side (air pressure 0); other faces keep u_pred. The divergence of each
+// fluid cell is taken from the FP64 correction of its six FP32 predicted face
+// velocities (l2 and max, m/s summed over the cell's faces); the block's sum of
+// squares and maximum go to partial[2 blk] and partial[2 blk + 1]. Types,
+// pressures and predicted velocities are staged with their face halos (the
+// upper faces of the block's last planes are owned by the upper neighbours).
+template <int CPT>
+__global__ void __launch_bounds__(512 / CPT)
+    k_correct_tiled(GridView g, const unsigned char* __restrict__ type, const double* __restrict__ p64,
+                    const float* __restrict__ up0, const float* __restrict__ up1, const float* __restrict__ up2,
+                    float* __restrict__ un0, float* __restrict__ un1, float* __restrict__ un2, double scale,
+                    double* partial) {
+  constexpr int NT = 512 / CPT;
+  constexpr int PER = 384 / NT;
+  static_assert(384 % NT == 0, "whole halo entries per thread");
+  __shared__ double ptile[512];
+  __shared__ double phalo[6][64];
+  __shared__ unsigned char ttile[512];
+  __shared__ unsigned char thalo[6][64];
+  __shared__ float utile[3][512];
+  __shared__ float uhalo[6][64];  // entries of the upper faces (odd f) only
+  __shared__ double red[NT / 32], mx[NT / 32];
+  const int blk = blockIdx.x, t = threadIdx.x;
   const float* up[3] = {up0, up1, up2};
+  float* un[3] = {un0, un1, un2};
+  // loads first: the block's cells, then the halo (lookups, then values)
+  unsigned char tv[CPT];
+  double pv[CPT];
+  float uv[3][CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int l = t + k * NT, i = blk * 512 + l;  // natural order
+    tv[k] = type[i];
+    pv[k] = p64[blk * 512 + rb_of(l)];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) uv[a][k] = up[a][i];
+  }
+  int src[PER], slot[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) src[k] = halo_src0(g, blk, t + k * NT, &slot[k]);
+  unsigned char th[PER];
+  double ph[PER];
+  float uh[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int f = slot[k] >> 6, a = f >> 1;
+    th[k] = (unsigned char)nbr_type(type, src[k]);
+    ph[k] = src[k] >= 0 ? p64[rb_id(src[k])] : 0.0;
+    uh[k] = ((f & 1) && src[k] >= 0) ? up[a][src[k]] : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int l = t + k * NT;
+    ttile[l] = tv[k];
+    ptile[l] = pv[k];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) utile[a][l] = uv[a][k];
+  }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    (&thalo[0][0])[slot[k]] = th[k];
+    (&phalo[0][0])[slot[k]] = ph[k];
+    (&uhalo[0][0])[slot[k]] = uh[k];
+  }
+  __syncthreads();
   double maxdiv = 0.0, sumsq = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int ti = type[i];
-    const int b = i >> 9, l = i & 511;
-    // loads first (whatever the cell types), then the divergence of fluid cells
-    int lo[3], hi[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      lo[a] = nbr_s<3>(g, b, l, a, -1);
-      hi[a] = nbr_s<3>(g, b, l, a, +1);
-    }
-    const double pi = p64[rb_id(i)];
-    int tlo[3], thi[3];
-    double ul[3], uh[3], pl[3], ph[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      tlo[a] = nbr_type(type, lo[a]);
-      thi[a] = nbr_type(type, hi[a]);
-      ul[a] = (double)up[a][i];
-      uh[a] = hi[a] >= 0 ? (double)up[a][hi[a]] : 0.0;
-      pl[a] = lo[a] >= 0 ? p64[rb_id(lo[a])] : 0.0;
-      ph[a] = hi[a] >= 0 ? p64[rb_id(hi[a])] : 0.0;
-    }
-    if (ti != 1) continue;
+  for (int k = 0; k < CPT; ++k) {
+    const int l = t + k * NT, i = blk * 512 + l;
+    const int c[3] = {l & 7, (l >> 3) & 7, l >> 6};
+    const int ti = tv[k];
+    const double pi = pv[k];
     double div = 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      double ulo = ul[a], uhi = uh[a];
-      if (tlo[a] != 0) ulo += scale * ((tlo[a] == 1 ? pl[a] : 0.0) - pi);
-      if (thi[a] != 0) uhi += scale * (pi - (thi[a] == 1 ? ph[a] : 0.0));
-      div += uhi - ulo;
+      const int step = 1 << (3 * a);
+      const int q = a == 0 ? (c[2] << 3) | c[1] : (a == 1 ? (c[2] << 3) | c[0] : (c[1] << 3) | c[0]);
+      // lower neighbour (tail of the owned face) and upper neighbour
+      const bool lo_in = c[a] > 0, hi_in = c[a] < 7;
+      const int tlo = lo_in ? ttile[l - step] : thalo[2 * a][q];
+      const int thi = hi_in ? ttile[l + step] : thalo[2 * a + 1][q];
+      const double plo = lo_in ? ptile[l - step] : phalo[2 * a][q];
+      const double phi = hi_in ? ptile[l + step] : phalo[2 * a + 1][q];
+      const double uhi_pred = hi_in ? (double)utile[a][l + step] : (double)uhalo[2 * a + 1][q];
+      // owned face: head = this cell, tail = the lower neighbour
+      double u = (double)uv[a][k];
+      if (ti != 0 && tlo != 0 && (ti == 1 || tlo == 1)) u += scale * ((tlo == 1 ? plo : 0.0) - (ti == 1 ? pi : 0.0));
+      un[a][i] = (float)u;
+      if (ti == 1) {
+        double ulo = (double)uv[a][k], uhi = uhi_pred;
+        if (tlo != 0) ulo += scale * ((tlo == 1 ? plo : 0.0) - pi);
+        if (thi != 0) uhi += scale * (pi - (thi == 1 ? phi : 0.0));
+        div += uhi - ulo;
+      }
     }
-    maxdiv = fmax(maxdiv, fabs(div));
-    sumsq += div * div;
+    if (ti == 1) {
+      maxdiv = fmax(maxdiv, fabs(div));
+      sumsq += div * div;
+    }
   }
-  double m = maxdiv;
+  sumsq = warp_sum(sumsq);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) mx[threadIdx.x >> 5] = m;
-  const double s = block_sum<kThreads>(sumsq, red);
+  for (int o = 16; o > 0; o >>= 1) maxdiv = fmax(maxdiv, __shfl_xor_sync(0xffffffffu, maxdiv, o));
+  if ((t & 31) == 0) {
+    red[t >> 5] = sumsq;
+    mx[t >> 5] = maxdiv;
+  }
+  __syncthreads();
+  if (t == 0) {
+    double s2 = 0.0, m2 = 0.0;
+    for (int w = 0; w < NT / 32; ++w) {
+      s2 += red[w];
+      m2 = fmax(m2, mx[w]);
+    }
+    partial[2 * blk] = s2;
+    partial[2 * blk + 1] = m2;
+  }
+}
+
+// Divergence l2 and max over the per-block partials, in block order.
+__global__ void __launch_bounds__(1024) k_correct_finish(int nb, const double* __restrict__ partial,
+                                                         SolverState* st) {
+  __shared__ double red[32], mx[32];
+  double acc = 0.0, mm = 0.0;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    acc += partial[2 * k];
+    mm = fmax(mm, partial[2 * k + 1]);
+  }
+  acc = warp_sum(acc);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = acc;
+    mx[threadIdx.x >> 5] = mm;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double mm = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) mm = fmax(mm, mx[w]);
-    partial[2 * blockIdx.x] = s;
-    partial[2 * blockIdx.x + 1] = mm;
-  }
-  if (last_block(st)) {
-    const double t = finish_sum(partial, 2, 0, red);
-    double mm = 0.0;
-    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) mm = fmax(mm, partial[2 * k + 1]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, o));
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) mx[threadIdx.x >> 5] = mm;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double all = 0.0;
-      for (int w = 0; w < kThreads / 32; ++w) all = fmax(all, mx[w]);
-      st->div_l2 = sqrt(t);
-      st->div_max = all;
-      st->ticket = 0;
+    double t = 0.0, all = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      t += red[w];
+      all = fmax(all, mx[w]);
     }
+    st->div_l2 = sqrt(t);
+    st->div_max = all;
   }
 }
 
@@ -1350,9 +1427,9 @@ cudaError_t launch_apply_vcycle(const GridView& g, const MgHierarchy<T>& H, cons
 template <typename T>
 cudaError_t launch_residual64(const GridView& g, const MgHierarchy<T>& H, const double* b64, const double* p64,
                               float* r, float* e, double* partial, SolverState* st, cudaStream_t s) {
-  const int n = g.nb * kBlockCells;
-  ++g_kernel_launches;
-  k_residual64<T><<<reduce_grid(n), kThreads, 0, s>>>(g, H.ptr[0], b64, p64, r, e, partial, st);
+  g_kernel_launches += 2;
+  k_residual64_tiled<T, kResidualCpt><<<g.nb, 512 / kResidualCpt, 0, s>>>(g, H.ptr[0], b64, p64, r, e, partial);
+  k_residual64_finish<<<1, 1024, 0, s>>>(g.nb, partial, st);
   return cudaGetLastError();
 }
 
@@ -1387,13 +1464,10 @@ cudaError_t launch_accumulate(const GridView& g, const float* e, double* p64, cu
 cudaError_t launch_correct_faces(const GridView& g, const unsigned char* type, const double* p64,
                                  const float* const u_pred[3], float* const u_new[3], double scale,
                                  double* partial, SolverState* st, cudaStream_t s) {
-  const int nf = g.nb * 3 * kBlockCells;
   g_kernel_launches += 2;
-  k_correct_faces<<<blocks_for(nf), kThreads, 0, s>>>(g, type, p64, u_pred[0], u_pred[1], u_pred[2], u_new[0],
-                                                      u_new[1], u_new[2], scale);
-  const int n = g.nb * kBlockCells;
-  k_diagnostics<<<reduce_grid(n), kThreads, 0, s>>>(g, type, p64, u_pred[0], u_pred[1], u_pred[2], scale, partial,
-                                                    st);
+  k_correct_tiled<kCorrectCpt><<<g.nb, 512 / kCorrectCpt, 0, s>>>(g, type, p64, u_pred[0], u_pred[1], u_pred[2],
+                                                                  u_new[0], u_new[1], u_new[2], scale, partial);
+  k_correct_finish<<<1, 1024, 0, s>>>(g.nb, partial, st);
   return cudaGetLastError();
 }
 
