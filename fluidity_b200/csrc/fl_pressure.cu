@@ -195,60 +195,18 @@ __device__ __forceinline__ long long lattice_cell(const GridView& g, int b, int 
   return lb * 512 + l;
 }
 
-template <typename T>
-__global__ void k_setup_level0(GridView g, const unsigned char* type, const float* u0, const float* u1,
-                               const float* u2, double rhs_scale, LevelPtrs<T> L0, double* b64, double* p64,
-                               const float* p_prev, double* partial, SolverState* st) {
-  __shared__ double red[kThreads / 32];
-  const int n = g.nb * kBlockCells;
-  const float* u[3] = {u0, u1, u2};
-  double bb = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int b = i >> 9, l = i & 511;
-    // loads first (whatever the cell type), then the fluid cell's row
-    const bool fluid = type[i] == 1;
-    const float pp = p_prev != nullptr ? p_prev[lattice_cell(g, b, l)] : 0.0f;
-    int tlo[3], thi[3];
-    float ul[3], uh[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const int lo = nbr_s<3>(g, b, l, a, -1);
-      const int hi = nbr_s<3>(g, b, l, a, +1);
-      tlo[a] = nbr_type(type, lo);
-      thi[a] = nbr_type(type, hi);
-      ul[a] = u[a][i];
-      uh[a] = hi >= 0 ? u[a][hi] : 0.0f;
-    }
-    float anchor = 0.0f;
-    unsigned mask = fluid ? 64u : 0u;
-    double div = 0.0;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      if (fluid) {
-        mask |= (tlo[a] == 1 ? 1u : 0u) << (2 * a);
-        mask |= (thi[a] == 1 ? 1u : 0u) << (2 * a + 1);
-        anchor += (tlo[a] == 2 ? 1.0f : 0.0f) + (thi[a] == 2 ? 1.0f : 0.0f);
-        div += (double)uh[a] - (double)ul[a];
-      }
-    }
-    const int r = rb_id(i);
-    L0.mask[r] = (unsigned char)mask;
-    L0.fluid[r] = fluid ? 1 : 0;
-    L0.anchor[r] = anchor;
-    L0.diag[r] = fluid ? anchor + (float)__popc(mask & 63u) : 1.0f;
-    const double rhs = fluid ? -rhs_scale * div : 0.0;
-    b64[r] = rhs;
-    p64[r] = (fluid && p_prev != nullptr) ? (double)pp : 0.0;
-    bb += rhs * rhs;
-  }
-  const double s = block_sum<kThreads>(bb, red);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
-  if (last_block(st)) {
-    const double t = finish_sum(partial, 1, 0, red);
-    if (threadIdx.x == 0) {
-      st->b_norm = sqrt(t);
-      st->ticket = 0;
-    }
+// ||b'|| over the per-block partials, in block order.
+__global__ void __launch_bounds__(1024) k_setup_finish(int nb, const double* __restrict__ partial, SolverState* st) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) acc += partial[k];
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    st->b_norm = sqrt(t);
   }
 }
 
@@ -565,6 +523,7 @@ constexpr int kRestrict0Cpt = 4;  // k_restrict0_tiled: 128 threads
 constexpr int kDirectionCpt = 4;  // k_direction_tiled: 128 threads
 constexpr int kResidualCpt = 4;   // k_residual64_tiled: 128 threads
 constexpr int kCorrectCpt = 4;    // k_correct_tiled: 128 threads
+constexpr int kSetupCpt = 4;      // k_setup_level0_tiled: 128 threads
 
 // Red-black sweep of one colour on level 0 (MODE 0 plain, 2 prolongation
 // fused); MODE 1 (first sweep from zero) needs no neighbour values. The cells'
@@ -1244,6 +1203,107 @@ __global__ void __launch_bounds__(1024) k_correct_finish(int nb, const double* _
   }
 }
 
+// Level-0 operator and right-hand side for one 8^3 block, one CTA per block
+// with CPT cells per thread: for each fluid cell the fluid-neighbour mask, the
+// air anchor (count of air neighbours), the diagonal, b' = -rhs_scale div u
+// and the warm-start pressure; the block's ||b'||^2 goes to partial[blk].
+// Types and predicted velocities are staged with their face halos (the upper
+// faces of the block's last planes are owned by the upper neighbours).
+template <typename T, int CPT>
+__global__ void __launch_bounds__(512 / CPT)
+    k_setup_level0_tiled(GridView g, const unsigned char* __restrict__ type, const float* __restrict__ u0,
+                         const float* __restrict__ u1, const float* __restrict__ u2, double rhs_scale,
+                         LevelPtrs<T> L0, double* __restrict__ b64, double* __restrict__ p64,
+                         const float* __restrict__ p_prev, double* partial) {
+  constexpr int NT = 512 / CPT;
+  constexpr int PER = 384 / NT;
+  static_assert(384 % NT == 0, "whole halo entries per thread");
+  __shared__ unsigned char ttile[512];
+  __shared__ unsigned char thalo[6][64];
+  __shared__ float utile[3][512];
+  __shared__ float uhalo[6][64];  // entries of the upper faces (odd f) only
+  __shared__ double red[NT / 32];
+  const int blk = blockIdx.x, t = threadIdx.x;
+  const float* u[3] = {u0, u1, u2};
+  // loads first (whatever the cell type): the block's cells, then the halo
+  unsigned char tv[CPT];
+  float pp[CPT], uv[3][CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int l = t + k * NT, i = blk * 512 + l;  // natural order
+    tv[k] = type[i];
+    pp[k] = p_prev != nullptr ? p_prev[lattice_cell(g, blk, l)] : 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) uv[a][k] = u[a][i];
+  }
+  int src[PER], slot[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) src[k] = halo_src0(g, blk, t + k * NT, &slot[k]);
+  unsigned char th[PER];
+  float uh[PER];
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int f = slot[k] >> 6, a = f >> 1;
+    th[k] = (unsigned char)nbr_type(type, src[k]);
+    uh[k] = ((f & 1) && src[k] >= 0) ? u[a][src[k]] : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int l = t + k * NT;
+    ttile[l] = tv[k];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) utile[a][l] = uv[a][k];
+  }
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    (&thalo[0][0])[slot[k]] = th[k];
+    (&uhalo[0][0])[slot[k]] = uh[k];
+  }
+  __syncthreads();
+  double bb = 0.0;
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int l = t + k * NT;
+    const int c[3] = {l & 7, (l >> 3) & 7, l >> 6};
+    const bool fluid = tv[k] == 1;
+    float anchor = 0.0f;
+    unsigned mask = fluid ? 64u : 0u;
+    double div = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int step = 1 << (3 * a);
+      const int q = a == 0 ? (c[2] << 3) | c[1] : (a == 1 ? (c[2] << 3) | c[0] : (c[1] << 3) | c[0]);
+      const bool lo_in = c[a] > 0, hi_in = c[a] < 7;
+      const int tlo = lo_in ? ttile[l - step] : thalo[2 * a][q];
+      const int thi = hi_in ? ttile[l + step] : thalo[2 * a + 1][q];
+      const float uh_a = hi_in ? utile[a][l + step] : uhalo[2 * a + 1][q];
+      if (fluid) {
+        mask |= (tlo == 1 ? 1u : 0u) << (2 * a);
+        mask |= (thi == 1 ? 1u : 0u) << (2 * a + 1);
+        anchor += (tlo == 2 ? 1.0f : 0.0f) + (thi == 2 ? 1.0f : 0.0f);
+        div += (double)uh_a - (double)uv[a][k];
+      }
+    }
+    const int r = blk * 512 + rb_of(l);
+    L0.mask[r] = (unsigned char)mask;
+    L0.fluid[r] = fluid ? 1 : 0;
+    L0.anchor[r] = anchor;
+    L0.diag[r] = fluid ? anchor + (float)__popc(mask & 63u) : 1.0f;
+    const double rhs = fluid ? -rhs_scale * div : 0.0;
+    b64[r] = rhs;
+    p64[r] = (fluid && p_prev != nullptr) ? (double)pp[k] : 0.0;
+    bb += rhs * rhs;
+  }
+  bb = warp_sum(bb);
+  if ((t & 31) == 0) red[t >> 5] = bb;
+  __syncthreads();
+  if (t < 32) {
+    double v = t < NT / 32 ? red[t] : 0.0;
+    v = warp_sum(v);
+    if (t == 0) partial[blk] = v;
+  }
+}
+
 // Solver (red-black) <-> natural level-0 layout conversions.
 __global__ void k_export_pressure(GridView g, int n, const double* p64_rb, double* p_nat, float* p_keep) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -1403,8 +1463,11 @@ cudaError_t launch_pressure_setup(const GridView& g, const int* cell_start, unsi
   ++g_kernel_launches;
   k_classify<<<blocks_for(n), kThreads, 0, s>>>(g, cell_start, type);
   ++g_kernel_launches;
-  k_setup_level0<T><<<reduce_grid(n), kThreads, 0, s>>>(g, type, u_pred[0], u_pred[1], u_pred[2], rhs_scale,
-                                                         H.ptr[0], b64, p64, p_prev, partial, st);
+  k_setup_level0_tiled<T, kSetupCpt><<<g.nb, 512 / kSetupCpt, 0, s>>>(g, type, u_pred[0], u_pred[1], u_pred[2],
+                                                                      rhs_scale, H.ptr[0], b64, p64, p_prev,
+                                                                      partial);
+  ++g_kernel_launches;
+  k_setup_finish<<<1, 1024, 0, s>>>(g.nb, partial, st);
   for (int l = 1; l < H.levels; ++l) {
     ++g_kernel_launches;
     k_coarsen<T><<<blocks_for(H.desc[l].count), kThreads, 0, s>>>(g, H.desc[l - 1], H.ptr[l - 1], H.desc[l],
