@@ -867,6 +867,168 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(LevelDesc L, LevelPtrs<T>
   for (int i = threadIdx.x; i < n; i += blockDim.x) st_T(&lp.x[i], lp.fluid[i] ? x[i] : 0.0f);
 }
 
+// Coarse tail of the V-cycle in one CTA: the last dense level F (at most
+// kTailMaxCells cells) pre-smoothed, its residual restricted to the coarsest
+// level C, C solved by symmetric sweeps, then F corrected and post-smoothed,
+// all in shared memory. The sweeps, restriction and coarsest solve are those
+// of k_smooth_dense, k_restrict_dense and k_coarse_solve, in the same order;
+// F's iterate stays in FP32 between them (one launch instead of ten).
+constexpr int kTailMaxCells = 4096;
+constexpr int kTailThreads = 1024;
+constexpr int kTailCpt = kTailMaxCells / kTailThreads;
+
+__host__ __device__ constexpr size_t tail_smem_bytes(int nf, int nc) {
+  return sizeof(float) * (6 * (size_t)nf + 6 * (size_t)nc) + (size_t)nf;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTailThreads)
+    k_coarse_tail(LevelDesc F, LevelPtrs<T> fp, const float* __restrict__ fb, LevelDesc C, LevelPtrs<T> cp,
+                  float* __restrict__ cb, int pre, int post, int sweeps, const int* done) {
+  grid_dependency_wait();
+  if (*done) return;
+  extern __shared__ float sm[];
+  const int nf = (int)F.count, nc = (int)C.count;
+  float* x = sm;                 // F iterate
+  float* bf = x + nf;            // F right-hand side
+  float* df = bf + nf;           // F diagonal
+  float* kf[3] = {df + nf, df + 2 * nf, df + 3 * nf};
+  float* xc = df + 4 * nf;       // C iterate
+  float* bc = xc + nc;           // C right-hand side
+  float* dc = bc + nc;           // C diagonal of fluid cells, 0 elsewhere
+  float* kc[3] = {dc + nc, dc + 2 * nc, dc + 3 * nc};
+  unsigned char* ff = reinterpret_cast<unsigned char*>(kc[2] + nc);  // F fluid flags
+  const int t = threadIdx.x;
+  for (int i = t; i < nf; i += kTailThreads) {
+    x[i] = 0.0f;
+    bf[i] = fb[i];
+    df[i] = fp.diag[i];
+    ff[i] = fp.fluid[i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) kf[a][i] = ld(&fp.k[a][i]);
+  }
+  for (int i = t; i < nc; i += kTailThreads) {
+    xc[i] = 0.0f;
+    dc[i] = cp.fluid[i] ? cp.diag[i] : 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) kc[a][i] = ld(&cp.k[a][i]);
+  }
+  // This thread's F cells: coordinates and colour.
+  int cx[kTailCpt], cy[kTailCpt], cz[kTailCpt], col[kTailCpt];
+#pragma unroll
+  for (int j = 0; j < kTailCpt; ++j) {
+    const int i = t + j * kTailThreads;
+    cx[j] = i % F.dim[0];
+    cy[j] = (i / F.dim[0]) % F.dim[1];
+    cz[j] = i / (F.dim[0] * F.dim[1]);
+    col[j] = (cx[j] + cy[j] + cz[j] + F.parity) & 1;
+  }
+  __syncthreads();
+  // One colour sweep on F: mode 1 from zero, mode 2 with the coarse correction
+  // added to the neighbour values read (as k_smooth_dense).
+  auto sweep = [&](int color, int mode) {
+#pragma unroll
+    for (int j = 0; j < kTailCpt; ++j) {
+      const int i = t + j * kTailThreads;
+      if (i >= nf || col[j] != color || !ff[i]) continue;
+      float s = bf[i];
+      if (mode != 1) {
+        const int c[3] = {cx[j], cy[j], cz[j]};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const int a = q >> 1, dir = (q & 1) ? 1 : -1;
+          int n[3] = {c[0], c[1], c[2]};
+          n[a] += dir;
+          if (n[a] < 0 || n[a] >= F.dim[a]) continue;
+          const int jn = dense_id(F, n[0], n[1], n[2]);
+          const float kq = dir < 0 ? kf[a][i] : kf[a][jn];
+          float xv = x[jn];
+          if (mode == 2) xv += xc[dense_id(C, n[0] >> 1, n[1] >> 1, n[2] >> 1)];
+          if (kq != 0.0f) s = fmaf(kq, xv, s);
+        }
+      }
+      x[i] = s / df[i];
+    }
+    __syncthreads();
+  };
+  sweep(0, 1);
+  sweep(1, 0);
+  for (int sw = 1; sw < pre; ++sw) {
+    sweep(0, 0);
+    sweep(1, 0);
+  }
+  // Residual of F restricted to C (as k_restrict_dense), one thread per C cell.
+  for (int I = t; I < nc; I += kTailThreads) {
+    const int X = I % C.dim[0], Y = (I / C.dim[0]) % C.dim[1], Z = I / (C.dim[0] * C.dim[1]);
+    float sum = 0.0f;
+#pragma unroll
+    for (int ch = 0; ch < 8; ++ch) {
+      const int c[3] = {2 * X + (ch & 1), 2 * Y + ((ch >> 1) & 1), 2 * Z + (ch >> 2)};
+      if (c[0] >= F.dim[0] || c[1] >= F.dim[1] || c[2] >= F.dim[2]) continue;
+      const int id = dense_id(F, c[0], c[1], c[2]);
+      if (!ff[id]) continue;
+      float ax = df[id] * x[id];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const int a = q >> 1, dir = (q & 1) ? 1 : -1;
+        int n[3] = {c[0], c[1], c[2]};
+        n[a] += dir;
+        if (n[a] < 0 || n[a] >= F.dim[a]) continue;
+        const int jn = dense_id(F, n[0], n[1], n[2]);
+        const float kq = dir < 0 ? kf[a][id] : kf[a][jn];
+        if (kq != 0.0f) ax = fmaf(-kq, x[jn], ax);
+      }
+      sum += bf[id] - ax;
+    }
+    bc[I] = sum;
+    cb[I] = sum;
+  }
+  __syncthreads();
+  // Coarsest level: symmetric red-black sweeps, one cell per thread (as k_coarse_solve).
+  {
+    const int i = t;
+    bool active = false;
+    int color = 0;
+    float kk[6] = {0, 0, 0, 0, 0, 0}, inv = 0.0f, bi = 0.0f;
+    int nb[6] = {0, 0, 0, 0, 0, 0};
+    const int nx = C.dim[0], ny = C.dim[1], nz = C.dim[2];
+    if (i < nc && dc[i] != 0.0f) {
+      active = true;
+      const int X = i % nx, Y = (i / nx) % ny, Z = i / (nx * ny);
+      color = (X + Y + Z + C.parity) & 1;
+      inv = 1.0f / dc[i];
+      bi = bc[i];
+      if (X > 0) { kk[0] = kc[0][i]; nb[0] = i - 1; }
+      if (X + 1 < nx) { kk[1] = kc[0][i + 1]; nb[1] = i + 1; }
+      if (Y > 0) { kk[2] = kc[1][i]; nb[2] = i - nx; }
+      if (Y + 1 < ny) { kk[3] = kc[1][i + nx]; nb[3] = i + nx; }
+      if (Z > 0) { kk[4] = kc[2][i]; nb[4] = i - nx * ny; }
+      if (Z + 1 < nz) { kk[5] = kc[2][i + nx * ny]; nb[5] = i + nx * ny; }
+    }
+    for (int pass = 0; pass < 4 * sweeps; ++pass) {
+      const int half = pass % 2;
+      const int c = pass < 2 * sweeps ? half : 1 - half;
+      if (active && color == c) {
+        float sacc = bi;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) sacc = fmaf(kk[q], xc[nb[q]], sacc);
+        xc[i] = sacc * inv;
+      }
+      __syncthreads();
+    }
+    if (i < nc) st_T(&cp.x[i], cp.fluid[i] ? xc[i] : 0.0f);
+  }
+  __syncthreads();
+  sweep(1, 2);
+  sweep(0, 0);
+  for (int sw = 1; sw < post; ++sw) {
+    sweep(1, 0);
+    sweep(0, 0);
+  }
+  for (int i = t; i < nf; i += kTailThreads)
+    if (ff[i]) st_T(&fp.x[i], x[i]);
+}
+
 // ----------------------------------------------------------------- CG kernels (level 0, grid-stride)
 
 
@@ -1419,7 +1581,11 @@ template <typename T>
 static void vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r0, const MgOptions& opt,
                    const int* done, cudaStream_t s) {
   const int L = H.levels;
-  for (int l = 0; l < L - 1; ++l) {
+  // The last dense level and the coarsest in one CTA when both fit.
+  const bool tail = L >= 2 && !H.desc[L - 2].sparse && H.desc[L - 2].count <= kTailMaxCells &&
+                    H.desc[L - 1].count <= kTailThreads;
+  const int top = tail ? L - 2 : L - 1;  // levels smoothed by the per-level kernels: [0, top)
+  for (int l = 0; l < top; ++l) {
     const float* bl = l == 0 ? r0 : H.b[l];
     smooth<T>(g, H, l, bl, 0, 1, done, s);
     smooth<T>(g, H, l, bl, 1, 0, done, s);
@@ -1429,14 +1595,25 @@ static void vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r0, 
     }
     restrict_level<T>(g, H, l, bl, done, s);
   }
-  {
+  if (tail) {
+    const LevelDesc& F = H.desc[L - 2];
+    const LevelDesc& C = H.desc[L - 1];
+    const size_t smem = tail_smem_bytes((int)F.count, (int)C.count);
+    static unsigned long long configured = 0;
+    if (first_on_device(configured))
+      cudaFuncSetAttribute(k_coarse_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)tail_smem_bytes(kTailMaxCells, kTailThreads));
+    ++g_kernel_launches;
+    launch_dep(k_coarse_tail<T>, 1, kTailThreads, smem, s, F, H.ptr[L - 2], (const float*)H.b[L - 2], C,
+               H.ptr[L - 1], H.b[L - 1], opt.pre, opt.post, opt.coarse_sweeps, done);
+  } else {
     const LevelDesc& C = H.desc[L - 1];
     const size_t smem = (size_t)C.count * 6 * sizeof(float);
     const int threads = C.count <= 1024 ? (int)((C.count + 31) / 32 * 32) : 1024;
     ++g_kernel_launches;
     launch_dep(k_coarse_solve<T>, 1, threads, smem, s, C, H.ptr[L - 1], H.b[L - 1], opt.coarse_sweeps, done);
   }
-  for (int l = L - 2; l >= 0; --l) {
+  for (int l = top - 1; l >= 0; --l) {
     const float* bl = l == 0 ? r0 : H.b[l];
     smooth<T>(g, H, l, bl, 1, 2, done, s);
     smooth<T>(g, H, l, bl, 0, 0, done, s);
