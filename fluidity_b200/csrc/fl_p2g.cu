@@ -15,7 +15,7 @@
 // accumulates into registers: along the normal axis a particle of the cell
 // touches nodes cell-1..cell+1 or cell..cell+2, so 4 x 3 x 3 = 36 slots per
 // channel cover every particle of the cell with static register indexing.
-// Register partials go to shared memory ([channel][slot][cell]); each tile node
+// Register partials go to shared memory ([slot][cell] mass/momentum pairs); each tile node
 // then sums its (at most 36) contributing (cell, slot) entries in a fixed
 // order. The 11x10x10 tile (normal extent 11, transverse 10) is written to a
 // per-block scratch tile and a second kernel sums, for every owned face, the
@@ -70,7 +70,7 @@ __device__ __forceinline__ void axis_factors(float X, int cell, float h, float c
 
 template <int A>
 __device__ __forceinline__ void p2g_component(const GridView& g, const ParticlesView& p, const unsigned int* order,
-                                              int pbeg, int pend, const int cell[3], float* part, int t,
+                                              int pbeg, int pend, const int cell[3], float2* part, int t,
                                               DeviceReport* rep) {
   constexpr int D1 = A == 0 ? 1 : 0;
   constexpr int D2 = A == 2 ? 1 : 2;
@@ -134,18 +134,18 @@ __device__ __forceinline__ void p2g_component(const GridView& g, const Particles
       for (int s = 0; s < 4; ++s) {
         const int slot = A == 0 ? slot_index<A>(s, j, k) : A == 1 ? slot_index<A>(j, s, k) : slot_index<A>(j, k, s);
         const int e = (k * 3 + j) * 2 + (s >> 1);
-        part[slot * kP2GThreads + t] = (s & 1) ? accW[e].y : accW[e].x;
-        part[(kSlots + slot) * kP2GThreads + t] = (s & 1) ? accQ[e].y : accQ[e].x;
+        part[slot * kP2GThreads + t] =
+            (s & 1) ? make_float2(accW[e].y, accQ[e].y) : make_float2(accW[e].x, accQ[e].x);
       }
 }
 
 template <int A>
-__device__ __forceinline__ void reduce_tile(const float* part, float2* tile, int t) {
+__device__ __forceinline__ void reduce_tile(const float2* part, float2* tile, int t) {
   constexpr int e0 = A == 0 ? 11 : 10, e1 = A == 1 ? 11 : 10;
   constexpr int ex = A == 0 ? 4 : 3, ey = A == 1 ? 4 : 3, ez = A == 2 ? 4 : 3;
   for (int n = t; n < kTileFaces; n += kP2GThreads) {
     const int nx = n % e0 - 1, ny = (n / e0) % e1 - 1, nz = n / (e0 * e1) - 1;
-    float W = 0.0f, Q = 0.0f;
+    float2 WQ = make_float2(0.0f, 0.0f);  // (mass, momentum), each lane summed in the same order
 #pragma unroll
     for (int sz = 0; sz < ez; ++sz) {
       const int cz = nz + 1 - sz;
@@ -160,19 +160,18 @@ __device__ __forceinline__ void reduce_tile(const float* part, float2* tile, int
           if (cx < 0 || cx > 7) continue;
           const int c = cz * 64 + cy * 8 + cx;
           const int s = (sz * ey + sy) * ex + sx;
-          W += part[s * kP2GThreads + c];
-          Q += part[(kSlots + s) * kP2GThreads + c];
+          WQ = __fadd2_rn(WQ, part[s * kP2GThreads + c]);
         }
       }
     }
-    tile[n] = make_float2(W, Q);
+    tile[n] = WQ;
   }
 }
 
 __global__ void __launch_bounds__(kP2GThreads, 1)
     k_p2g_tile(GridView g, ParticlesView p, const unsigned int* order, const int* cell_start, float2* tiles,
                DeviceReport* rep) {
-  extern __shared__ float part[];
+  extern __shared__ float2 part[];  // [slot][cell] (mass, momentum) partials
   const int b = blockIdx.x;
   const int t = threadIdx.x;
   const int base = b * kBlockCells;
@@ -282,7 +281,7 @@ cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cel
                        const P2GMergeParams& prm, float* const out0[3], float* const out1[3], DeviceReport* rep,
                        cudaStream_t s, const unsigned int* order) {
   if (g.nb == 0) return cudaSuccess;
-  const size_t smem = sizeof(float) * 2 * kSlots * kP2GThreads;
+  const size_t smem = sizeof(float2) * kSlots * kP2GThreads;
   static unsigned long long configured = 0;
   if (first_on_device(configured))
     cudaFuncSetAttribute(k_p2g_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
