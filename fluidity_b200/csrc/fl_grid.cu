@@ -132,7 +132,7 @@ __global__ void k_cell_keys(GridView g, ParticlesView p, unsigned int* keys, uns
   // One counter update per cell present in the warp: particles arrive nearly in
   // cell order (the previous step's), so most lanes share a few cells. Each lane
   // of a group takes the group's base plus its position among the group's lanes;
-  // ranks within a cell are unique, and k_sort_cells fixes their final order.
+  // ranks within a cell are unique, and k_sort_cells_block fixes their final order.
   const unsigned peers = __match_any_sync(__activemask(), key);
   if (key != 0xffffffffu) {
     const int lane = (int)(threadIdx.x & 31), leader = __ffs(peers) - 1;
@@ -157,37 +157,40 @@ __global__ void k_scatter_index(unsigned long long n, const unsigned int* keys, 
 
 // Sorts each cell's original indices ascending, which makes the permutation
 // equal to a stable sort by cell (deterministic whatever the atomic order).
-__global__ void k_sort_cells(int ncell, const int* cell_start, unsigned int* slots) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncell) return;
-  const int b = cell_start[c], e = cell_start[c + 1];
-  if (e - b < 2) return;
-  if (e - b <= 32) {
-    unsigned int v[32];
-    const int n = e - b;
-    for (int k = 0; k < n; ++k) v[k] = slots[b + k];
-    for (int k = 1; k < n; ++k) {
-      const unsigned int key = v[k];
-      int j = k - 1;
-      while (j >= 0 && v[j] > key) {
-        v[j + 1] = v[j];
-        --j;
-      }
-      v[j + 1] = key;
-    }
-    for (int k = 0; k < n; ++k) slots[b + k] = v[k];
-    return;
-  }
-  for (int k = b + 1; k < e; ++k) {  // crowded cell: in-place insertion sort
-    const unsigned int key = slots[k];
+// One CTA per 8^3 block: the block's slots are staged in shared memory
+// (coalesced in and out) and each thread insertion-sorts its cell there; a
+// block holding more than kSortBlockCap particles sorts its cells in place.
+constexpr int kSortBlockCap = 12288;  // 48 KB of staged slots
+
+__device__ __forceinline__ void insertion_sort(unsigned int* v, int n) {
+  for (int k = 1; k < n; ++k) {
+    const unsigned int key = v[k];
     int j = k - 1;
-    while (j >= b && slots[j] > key) {
-      slots[j + 1] = slots[j];
+    while (j >= 0 && v[j] > key) {
+      v[j + 1] = v[j];
       --j;
     }
-    slots[j + 1] = key;
+    v[j + 1] = key;
   }
 }
+
+__global__ void __launch_bounds__(512) k_sort_cells_block(const int* cell_start, unsigned int* slots) {
+  __shared__ unsigned int buf[kSortBlockCap];
+  const int b = blockIdx.x, t = threadIdx.x;
+  const int beg = cell_start[b * 512], end = cell_start[b * 512 + 512];
+  const int cb = cell_start[b * 512 + t], ce = cell_start[b * 512 + t + 1];
+  const int n = end - beg;
+  if (n > kSortBlockCap) {
+    insertion_sort(slots + cb, ce - cb);
+    return;
+  }
+  for (int i = t; i < n; i += 512) buf[i] = slots[beg + i];
+  __syncthreads();
+  insertion_sort(buf + (cb - beg), ce - cb);
+  __syncthreads();
+  for (int i = t; i < n; i += 512) slots[beg + i] = buf[i];
+}
+
 
 // Gathers every attribute of particle index[s] into slot s. All 15 (16) loads
 // are issued before any store: the buffers may not be declared disjoint to the
@@ -291,7 +294,7 @@ cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const Partic
   if (in.count > 0) {
     g_kernel_launches += permute ? 3 : 2;
     k_scatter_index<<<grid_for(in.count, 256), 256, 0, s>>>(in.count, keys, index, cell_start, index_alt);
-    k_sort_cells<<<grid_for(ncell, 256), 256, 0, s>>>((int)ncell, cell_start, index_alt);
+    k_sort_cells_block<<<(unsigned)(ncell / 512), 512, 0, s>>>(cell_start, index_alt);
     if (permute) k_permute<<<grid_for(in.count, 256), 256, 0, s>>>(in, out, index_alt);
   }
   (void)keys_alt;
