@@ -105,6 +105,8 @@ struct fl_context {
   double* p_nat = nullptr;
   float* p_keep = nullptr;  // last pressure per lattice cell (warm start across topology changes)
   bool p_keep_valid = false;
+  float* p_keep_prev = nullptr;  // the one before it (warm start by linear extrapolation)
+  bool p_keep_prev_valid = false;
   bool occ_ready = false;  // occ holds the blocks of the current state (marked by the last fl_step's G2P)
   // learned preconditioner: FP32 parameters, per-block scales, the inference
   // activations (grown on demand to the active block count) and its own
@@ -438,7 +440,8 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   k_init_state<<<1, 1, 0, s>>>(c->st, opt->rel_tol, opt->inner_rtol, opt->max_iterations, use_nn ? 1 : 0,
                                stall_limit, stall_ratio);
   const float* p_prev = (opt->warm_start && c->p_keep_valid) ? c->p_keep : nullptr;
-  FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, u_pred, rhs_scale, H, c->b64, c->p64, p_prev,
+  const float* p_prev2 = (opt->warm_start == 2 && p_prev && c->p_keep_prev_valid) ? c->p_keep_prev : nullptr;
+  FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, u_pred, rhs_scale, H, c->b64, c->p64, p_prev, p_prev2,
                                    c->partial, c->st, s));
   ++g_kernel_launches;
   k_set_target<<<1, 1, 0, s>>>(c->st, opt->rel_tol);
@@ -503,6 +506,8 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   }
   FL_CUDA(launch_correct_faces(g, c->type, c->p64, u_pred, u_new, vel_scale, c->partial, c->st, s));
   // The kept copy is rewritten in full: cells that are not fluid now read back as 0.
+  std::swap(c->p_keep, c->p_keep_prev);  // the last pressure becomes the one before
+  c->p_keep_prev_valid = c->p_keep_valid;
   FL_CUDA(cudaMemsetAsync(c->p_keep, 0, sizeof(float) * (size_t)c->lattice * kBlockCells, s));
   FL_CUDA(launch_export_pressure(g, c->p64, c->p_nat, c->p_keep, s));
   c->p_keep_valid = true;
@@ -549,7 +554,7 @@ int apply_vcycle(fl_context* c, const float* r, float* z, const fl_pressure_opti
   k_init_state<<<1, 1, 0, s>>>(c->st, 1e-6, 1e-4, 1, 0, 3, 0.9);
   const float* up[3] = {c->u_pred[0], c->u_pred[1], c->u_pred[2]};
   for (int a = 0; a < 3; ++a) FL_CUDA(cudaMemsetAsync(c->u_pred[a], 0, sizeof(float) * n, s));
-  FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, up, 1.0, H, c->b64, c->p64, nullptr, c->partial,
+  FL_CUDA(launch_pressure_setup<T>(g, c->cell_start, c->type, up, 1.0, H, c->b64, c->p64, nullptr, nullptr, c->partial,
                                    c->st, s));
   FL_CUDA(cudaMemsetAsync(c->lv_x[0], 0, sizeof(T) * (size_t)n, s));
   FL_CUDA(launch_to_rb(g, r, c->r[0], s));
@@ -826,6 +831,7 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
   chk(dalloc(&c->p64, cells));
   chk(dalloc(&c->p_nat, cells));
   chk(dalloc(&c->p_keep, cells));
+  chk(dalloc(&c->p_keep_prev, cells));
   if (cudaStreamCreateWithFlags(&c->work, cudaStreamNonBlocking) != cudaSuccess) chk(FL_INTERNAL);
   if (cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking) != cudaSuccess) chk(FL_INTERNAL);
   if (cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming) != cudaSuccess) chk(FL_INTERNAL);
@@ -915,6 +921,7 @@ int fl_context_destroy(fl_context* c) {
   cudaFree(c->p64);
   cudaFree(c->p_nat);
   cudaFree(c->p_keep);
+  cudaFree(c->p_keep_prev);
   if (c->fcg_exec) cudaGraphExecDestroy(c->fcg_exec);
   if (c->fcg_nn_exec) cudaGraphExecDestroy(c->fcg_nn_exec);
   cudaFree(c->nn_params);
@@ -1095,6 +1102,7 @@ int fl_upload_particles(fl_context* c, const float* host, uint64_t count, void* 
   c->cur = 0;
   c->count = count;
   c->p_keep_valid = false;
+  c->p_keep_prev_valid = false;
   c->occ_ready = false;
   for (int k = 0; k < 15; ++k)
     FL_CUDA(cudaMemcpyAsync(c->pbuf[0] + (size_t)k * c->pcap, host + (size_t)k * count, sizeof(float) * count,

@@ -125,7 +125,8 @@ cudaError_t launch_g2p(const GridView& g, const ParticlesView& p, const int* cel
 template <typename T>
 cudaError_t launch_pressure_setup(const GridView& g, const int* cell_start, unsigned char* type,
                                   const float* const u_pred[3], double rhs_scale, MgHierarchy<T>& H, double* b64,
-                                  double* p64, const float* p_prev, double* partial, SolverState* st,
+                                  double* p64, const float* p_prev,
+                                  const float* p_prev2, double* partial, SolverState* st,
                                   cudaStream_t s);
 template <typename T>
 cudaError_t launch_apply_vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r, const MgOptions& opt,

@@ -1368,7 +1368,8 @@ __global__ void __launch_bounds__(1024) k_correct_finish(int nb, const double* _
 // Level-0 operator and right-hand side for one 8^3 block, one CTA per block
 // with CPT cells per thread: for each fluid cell the fluid-neighbour mask, the
 // air anchor (count of air neighbours), the diagonal, b' = -rhs_scale div u
-// and the warm-start pressure; the block's ||b'||^2 goes to partial[blk].
+// and the warm-start pressure (p_prev, or 2 p_prev - p_prev2 when both are
+// given); the block's ||b'||^2 goes to partial[blk].
 // Types and predicted velocities are staged with their face halos (the upper
 // faces of the block's last planes are owned by the upper neighbours).
 template <typename T, int CPT>
@@ -1376,7 +1377,7 @@ __global__ void __launch_bounds__(512 / CPT)
     k_setup_level0_tiled(GridView g, const unsigned char* __restrict__ type, const float* __restrict__ u0,
                          const float* __restrict__ u1, const float* __restrict__ u2, double rhs_scale,
                          LevelPtrs<T> L0, double* __restrict__ b64, double* __restrict__ p64,
-                         const float* __restrict__ p_prev, double* partial) {
+                         const float* __restrict__ p_prev, const float* __restrict__ p_prev2, double* partial) {
   constexpr int NT = 512 / CPT;
   constexpr int PER = 384 / NT;
   static_assert(384 % NT == 0, "whole halo entries per thread");
@@ -1394,7 +1395,9 @@ __global__ void __launch_bounds__(512 / CPT)
   for (int k = 0; k < CPT; ++k) {
     const int l = t + k * NT, i = blk * 512 + l;  // natural order
     tv[k] = type[i];
-    pp[k] = p_prev != nullptr ? p_prev[lattice_cell(g, blk, l)] : 0.0f;
+    // warm start: the previous pressure, or extrapolated from the last two
+    const int lc = lattice_cell(g, blk, l);
+    pp[k] = p_prev != nullptr ? (p_prev2 != nullptr ? 2.0f * p_prev[lc] - p_prev2[lc] : p_prev[lc]) : 0.0f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) uv[a][k] = u[a][i];
   }
@@ -1634,15 +1637,15 @@ cudaError_t launch_classify(const GridView& g, const int* cell_start, unsigned c
 template <typename T>
 cudaError_t launch_pressure_setup(const GridView& g, const int* cell_start, unsigned char* type,
                                   const float* const u_pred[3], double rhs_scale, MgHierarchy<T>& H, double* b64,
-                                  double* p64, const float* p_prev, double* partial, SolverState* st,
-                                  cudaStream_t s) {
+                                  double* p64, const float* p_prev, const float* p_prev2, double* partial,
+                                  SolverState* st, cudaStream_t s) {
   const int n = g.nb * kBlockCells;
   ++g_kernel_launches;
   k_classify<<<blocks_for(n), kThreads, 0, s>>>(g, cell_start, type);
   ++g_kernel_launches;
   k_setup_level0_tiled<T, kSetupCpt><<<g.nb, 512 / kSetupCpt, 0, s>>>(g, type, u_pred[0], u_pred[1], u_pred[2],
                                                                       rhs_scale, H.ptr[0], b64, p64, p_prev,
-                                                                      partial);
+                                                                      p_prev2, partial);
   ++g_kernel_launches;
   k_setup_finish<<<1, 1024, 0, s>>>(g.nb, partial, st);
   for (int l = 1; l < H.levels; ++l) {
@@ -1752,8 +1755,8 @@ void configure_pressure_kernels() {
 
 #define FL_INSTANTIATE(T)                                                                                         \
   template cudaError_t launch_pressure_setup<T>(const GridView&, const int*, unsigned char*, const float* const[3], \
-                                                double, MgHierarchy<T>&, double*, double*, const float*, double*,   \
-                                                SolverState*, cudaStream_t);                                        \
+                                                double, MgHierarchy<T>&, double*, double*, const float*,            \
+                                                const float*, double*, SolverState*, cudaStream_t);                 \
   template cudaError_t launch_apply_vcycle<T>(const GridView&, const MgHierarchy<T>&, const float*,                \
                                               const MgOptions&, const int*, cudaStream_t);                         \
   template cudaError_t launch_residual64<T>(const GridView&, const MgHierarchy<T>&, const double*, const double*,  \

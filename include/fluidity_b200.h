@@ -101,7 +101,8 @@ typedef struct {
   int precision;      /* 0: FP32 V-cycle storage; 1: BF16 V-cycle storage */
   int max_iterations; /* total inner flexible-CG iterations */
   int max_refinements;
-  int warm_start;     /* 1: start from the previous projection's pressure (InitializeMacPressure3D) */
+  int warm_start;     /* 1: start from the previous projection's pressure (InitializeMacPressure3D);
+                         2: from 2 p(n) - p(n-1), the last two projections' pressures (falls back to 1) */
   double rel_tol;    /* ||b - A p||_2 <= rel_tol * ||b||_2, checked in FP64 */
   double inner_rtol; /* inner FP32 solve reduction per refinement */
   int preconditioner; /* 0: V-cycle; 1: learned block U-Net (fl_set_learned_preconditioner), V-cycle fallback */

@@ -115,15 +115,18 @@ def test_dam_break_128_first_step_matches_oracle():
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_pressure_meets_fp64_residual_checked_by_oracle(precision):
+@pytest.mark.parametrize("warm_start", [0, 2])
+def test_pressure_meets_fp64_residual_checked_by_oracle(precision, warm_start):
     """The GPU pressure, re-evaluated in FP64 by the oracle on the same system
     (built from the GPU's own predicted velocities), meets 1e-6 ||b||, and the
-    reference's own gate is reported."""
+    reference's own gate is reported; from p = 0 and from the pressure
+    extrapolated from the last two projections."""
     n = 64
     ctx, soa, m = dam_break_context(n)
+    opt = fb.default_pressure_options(precision=precision, warm_start=warm_start)
     for _ in range(3):
-        ctx.step(fb.transfer_params(scenes.DT, m), fb.default_pressure_options(precision=precision))
-    code, diag = ctx.step(fb.transfer_params(scenes.DT, m), fb.default_pressure_options(precision=precision))
+        ctx.step(fb.transfer_params(scenes.DT, m), opt)
+    code, diag = ctx.step(fb.transfer_params(scenes.DT, m), opt)
     assert code == fb.OK
     f = read_fields(ctx, n)
     box = box_for(n)
