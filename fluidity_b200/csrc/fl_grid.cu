@@ -105,54 +105,92 @@ __global__ void k_build_nbr27(GridView g, int* nbr27) {
   nbr27[i] = v;
 }
 
-__global__ void k_cell_keys(GridView g, ParticlesView p, unsigned int* keys, unsigned int* index, int* counts,
-                            DeviceReport* rep) {
-  const unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
-  if (i >= p.count) return;
-  int cell[3];
-  unsigned int key = 0xffffffffu, rank = 0;
-  if (particle_cell(g, p, i, cell)) {
-    int b[3], l[3];
-    bool inside = true;
+// Particles per thread in k_cell_keys and k_scatter_index: a CTA of 256
+// threads covers 1024 consecutive particles, particle k * 256 + t of the CTA's
+// range on thread t, with every independent load of the four issued together.
+constexpr int kSortIlp = 4;
+constexpr int kSortThreads = 256;
+
+__global__ void __launch_bounds__(kSortThreads)
+    k_cell_keys(GridView g, ParticlesView p, unsigned int* keys, unsigned int* index, int* counts,
+                DeviceReport* rep) {
+  const unsigned long long i0 = (unsigned long long)blockIdx.x * (kSortIlp * kSortThreads) + threadIdx.x;
+  float X[kSortIlp][3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      b[d] = floor_div8(cell[d]) - g.blo[d];
-      l[d] = cell[d] - 8 * (b[d] + g.blo[d]);
-      inside = inside && b[d] >= 0 && b[d] < g.bdim[d];
-    }
-    const int o = inside ? g.table[((size_t)b[2] * g.bdim[1] + b[1]) * g.bdim[0] + b[0]] : -1;
-    if (o >= 0) {
-      key = (unsigned int)o * 512u + (unsigned int)(l[2] * 64 + l[1] * 8 + l[0]);
-    } else {
-      report_error(rep, kFailedPrecondition, i);
-    }
-  } else {
-    report_error(rep, kOutOfRange, i);
+  for (int k = 0; k < kSortIlp; ++k) {
+    const unsigned long long i = i0 + (unsigned long long)k * kSortThreads;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) X[k][d] = i < p.count ? lattice_coord(g, p.x[d][i], d) : 0.0f;
   }
-  // One counter update per cell present in the warp: particles arrive nearly in
-  // cell order (the previous step's), so most lanes share a few cells. Each lane
-  // of a group takes the group's base plus its position among the group's lanes;
-  // ranks within a cell are unique, and k_sort_cells_block fixes their final order.
-  const unsigned peers = __match_any_sync(__activemask(), key);
-  if (key != 0xffffffffu) {
-    const int lane = (int)(threadIdx.x & 31), leader = __ffs(peers) - 1;
-    unsigned int base = 0;
-    if (lane == leader) base = (unsigned int)atomicAdd(&counts[key], __popc(peers));
-    base = __shfl_sync(peers, base, leader);
-    rank = base + (unsigned int)__popc(peers & ((1u << lane) - 1u));
+  int o[kSortIlp], lcell[kSortIlp];
+  bool fin_k[kSortIlp];
+#pragma unroll
+  for (int k = 0; k < kSortIlp; ++k) {
+    const unsigned long long i = i0 + (unsigned long long)k * kSortThreads;
+    bool fin = true, inside = true;
+    int bidx = 0, l = 0;
+    if (i < p.count) {
+      int b[3], c[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        fin = fin && isfinite(X[k][d]) && fabsf(X[k][d]) < 1.0e9f;
+        c[d] = fin ? __float2int_rd(X[k][d]) : 0;
+        b[d] = floor_div8(c[d]) - g.blo[d];
+        inside = inside && b[d] >= 0 && b[d] < g.bdim[d];
+      }
+      l = (c[2] - 8 * (b[2] + g.blo[2])) * 64 + (c[1] - 8 * (b[1] + g.blo[1])) * 8 + (c[0] - 8 * (b[0] + g.blo[0]));
+      bidx = (int)(((size_t)b[2] * g.bdim[1] + b[1]) * g.bdim[0] + b[0]);
+    }
+    fin_k[k] = fin;
+    o[k] = (i < p.count && fin && inside) ? g.table[bidx] : -1;
+    lcell[k] = l;
   }
-  keys[i] = key;
-  index[i] = rank;  // arrival rank within the cell (order not yet deterministic)
+#pragma unroll
+  for (int k = 0; k < kSortIlp; ++k) {
+    const unsigned long long i = i0 + (unsigned long long)k * kSortThreads;
+    unsigned int key = 0xffffffffu, rank = 0;
+    if (o[k] >= 0)
+      key = (unsigned int)o[k] * 512u + (unsigned int)lcell[k];
+    else if (i < p.count)  // not finite: out of range; else outside the lattice or in an inactive block
+      report_error(rep, fin_k[k] ? kFailedPrecondition : kOutOfRange, i);
+    // One counter update per cell present in the warp: particles arrive nearly
+    // in cell order (the previous step's), so most lanes share a few cells.
+    // Each lane of a group takes the group's base plus its position among the
+    // group's lanes; ranks within a cell are unique, and k_sort_cells_block
+    // fixes their final order.
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    if (key != 0xffffffffu) {
+      const int lane = (int)(threadIdx.x & 31), leader = __ffs(peers) - 1;
+      unsigned int base = 0;
+      if (lane == leader) base = (unsigned int)atomicAdd(&counts[key], __popc(peers));
+      base = __shfl_sync(peers, base, leader);
+      rank = base + (unsigned int)__popc(peers & ((1u << lane) - 1u));
+    }
+    if (i < p.count) {
+      keys[i] = key;
+      index[i] = rank;  // arrival rank within the cell (order not yet deterministic)
+    }
+  }
 }
 
 // Places each particle's original index at its cell's range start + arrival rank.
-__global__ void k_scatter_index(unsigned long long n, const unsigned int* keys, const unsigned int* rank,
-                                const int* cell_start, unsigned int* slots) {
-  const unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const unsigned int key = keys[i];
-  if (key == 0xffffffffu) return;
-  slots[cell_start[key] + rank[i]] = (unsigned int)i;
+__global__ void __launch_bounds__(kSortThreads)
+    k_scatter_index(unsigned long long n, const unsigned int* keys, const unsigned int* rank, const int* cell_start,
+                    unsigned int* slots) {
+  const unsigned long long i0 = (unsigned long long)blockIdx.x * (kSortIlp * kSortThreads) + threadIdx.x;
+  unsigned int key[kSortIlp], rk[kSortIlp];
+#pragma unroll
+  for (int k = 0; k < kSortIlp; ++k) {
+    const unsigned long long i = i0 + (unsigned long long)k * kSortThreads;
+    key[k] = i < n ? keys[i] : 0xffffffffu;
+    rk[k] = i < n ? rank[i] : 0u;
+  }
+  int start[kSortIlp];
+#pragma unroll
+  for (int k = 0; k < kSortIlp; ++k) start[k] = key[k] != 0xffffffffu ? cell_start[key[k]] : 0;
+#pragma unroll
+  for (int k = 0; k < kSortIlp; ++k)
+    if (key[k] != 0xffffffffu) slots[start[k] + rk[k]] = (unsigned int)(i0 + (unsigned long long)k * kSortThreads);
 }
 
 // Sorts each cell's original indices ascending, which makes the permutation
@@ -286,14 +324,15 @@ cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const Partic
   k_write_arch<<<1, 32, 0, s>>>(rep);
   if (in.count > 0) {
     ++g_kernel_launches;
-    k_cell_keys<<<grid_for(in.count, 256), 256, 0, s>>>(g, in, keys, index, counts, rep);
+    k_cell_keys<<<grid_for(in.count, kSortIlp * kSortThreads), kSortThreads, 0, s>>>(g, in, keys, index, counts, rep);
   }
   size_t tb = temp_bytes;
   ++g_library_launches;
   cub::DeviceScan::ExclusiveSum(temp, tb, counts, cell_start, (int)(ncell + 1), s);
   if (in.count > 0) {
     g_kernel_launches += permute ? 3 : 2;
-    k_scatter_index<<<grid_for(in.count, 256), 256, 0, s>>>(in.count, keys, index, cell_start, index_alt);
+    k_scatter_index<<<grid_for(in.count, kSortIlp * kSortThreads), kSortThreads, 0, s>>>(in.count, keys, index,
+                                                                                          cell_start, index_alt);
     k_sort_cells_block<<<(unsigned)(ncell / 512), 512, 0, s>>>(cell_start, index_alt);
     if (permute) k_permute<<<grid_for(in.count, 256), 256, 0, s>>>(in, out, index_alt);
   }

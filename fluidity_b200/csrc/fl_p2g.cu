@@ -241,17 +241,14 @@ __device__ __forceinline__ float2 merge_face(const GridView& g, const float2* __
   return r;
 }
 
-// One thread per owned face: fixed-order sum of the covering tiles, then either
-// raw mass/momentum or normalize + gravity + stationary walls.
-__global__ void k_p2g_merge(GridView g, const int* cell_start, const float2* tiles, P2GMergeParams prm,
-                            float* out0_x, float* out0_y, float* out0_z, float* out1_x, float* out1_y,
-                            float* out1_z, DeviceReport* rep) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i == 0 && rep != nullptr) rep->compiled_architecture = compiled_arch();
-  if (i >= (long long)g.nb * 3 * kBlockCells) return;
-  const int b = (int)(i / (3 * kBlockCells));
-  const int a = (int)((i / kBlockCells) % 3);
-  const int l = (int)(i % kBlockCells);
+// One thread per owned face (CTA = one block and normal axis, thread = cell):
+// fixed-order sum of the covering tiles, then either raw mass/momentum or
+// normalize + gravity + stationary walls.
+__global__ void __launch_bounds__(kBlockCells)
+    k_p2g_merge(GridView g, const int* cell_start, const float2* tiles, P2GMergeParams prm, float* out0_x,
+                float* out0_y, float* out0_z, float* out1_x, float* out1_y, float* out1_z, DeviceReport* rep) {
+  const int b = blockIdx.x, a = blockIdx.y, l = threadIdx.x;
+  if (b == 0 && a == 0 && l == 0 && rep != nullptr) rep->compiled_architecture = compiled_arch();
   const int loc[3] = {l & 7, (l >> 3) & 7, l >> 6};
   const float2 wq = a == 0 ? merge_face<0>(g, tiles, b, loc) : (a == 1 ? merge_face<1>(g, tiles, b, loc)
                                                                        : merge_face<2>(g, tiles, b, loc));
@@ -287,10 +284,9 @@ cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cel
     cudaFuncSetAttribute(k_p2g_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   ++g_kernel_launches;
   k_p2g_tile<<<g.nb, kP2GThreads, smem, s>>>(g, p, order, cell_start, tiles, rep);
-  const long long faces = (long long)g.nb * 3 * kBlockCells;
   ++g_kernel_launches;
-  k_p2g_merge<<<(unsigned)((faces + 255) / 256), 256, 0, s>>>(g, cell_start, tiles, prm, out0[0], out0[1], out0[2],
-                                                               out1[0], out1[1], out1[2], rep);
+  k_p2g_merge<<<dim3(g.nb, 3), kBlockCells, 0, s>>>(g, cell_start, tiles, prm, out0[0], out0[1], out0[2], out1[0],
+                                                    out1[1], out1[2], rep);
   return cudaGetLastError();
 }
 
