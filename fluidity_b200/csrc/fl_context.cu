@@ -52,7 +52,7 @@ struct fl_context {
   int* nb_dev = nullptr;
   int* nb_host = nullptr;
   // sort
-  unsigned int *keys = nullptr, *keys_alt = nullptr, *index = nullptr, *index_alt = nullptr;
+  unsigned int *keys = nullptr, *index = nullptr, *index_alt = nullptr;
   int* counts = nullptr;
   int* cell_start = nullptr;
   void* temp = nullptr;
@@ -812,7 +812,6 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
   chk(dalloc(&c->nb_dev, 1));
   chk(cudaMallocHost(&c->nb_host, sizeof(int)) == cudaSuccess ? FL_OK : FL_RESOURCE_EXHAUSTED);
   chk(dalloc(&c->keys, c->pcap));
-  chk(dalloc(&c->keys_alt, c->pcap));
   chk(dalloc(&c->index, c->pcap));
   chk(dalloc(&c->index_alt, c->pcap));
   chk(dalloc(&c->counts, cells + 1));
@@ -903,7 +902,6 @@ int fl_context_destroy(fl_context* c) {
   cudaFree(c->nb_dev);
   if (c->nb_host) cudaFreeHost(c->nb_host);
   cudaFree(c->keys);
-  cudaFree(c->keys_alt);
   cudaFree(c->index);
   cudaFree(c->index_alt);
   cudaFree(c->counts);
@@ -1027,7 +1025,7 @@ static int sort_impl(fl_context* c, const fl_particles* in, fl_particles* out, b
   GridView g = view(c);
   ParticlesView iv = pview(in), ov = pview(out);
   ov.count = in->count;
-  FL_CUDA(launch_sort(g, iv, ov, c->keys, c->keys_alt, c->index, c->index_alt, c->counts, c->cell_start, c->temp,
+  FL_CUDA(launch_sort(g, iv, ov, c->keys, c->index, c->index_alt, c->counts, c->cell_start, c->temp,
                       c->temp_bytes, c->rep, s, permute));
   out->count = in->count;
   if (report) return read_report(c, s, report);

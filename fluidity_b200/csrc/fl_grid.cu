@@ -14,7 +14,6 @@
 // run -- and the SoA arrays are gathered once. The reference sorts by
 // the signed bin floor((X - 1.5)/4) with CUB (native/cuda/liquid_arena_3d.cu:29-52);
 // with 8^3 blocks and per-step re-binning the bin is simply the containing cell.
-#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "fl_internal.cuh"
@@ -265,12 +264,12 @@ static inline unsigned int grid_for(unsigned long long n, int threads) {
   return (unsigned int)((n + threads - 1) / threads);
 }
 
+// Scratch of the exclusive scans (the largest runs over every cell + 1).
 size_t sort_temp_bytes(size_t particle_capacity, size_t cell_capacity) {
-  size_t a = 0, b = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, a, (unsigned int*)nullptr, (unsigned int*)nullptr,
-                                  (unsigned int*)nullptr, (unsigned int*)nullptr, (int)particle_capacity, 0, 32);
+  (void)particle_capacity;
+  size_t b = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, b, (int*)nullptr, (int*)nullptr, (int)(cell_capacity + 1));
-  return (a > b ? a : b) + 256;
+  return b + 256;
 }
 
 cudaError_t launch_topology_from_particles(const GridView& g, const ParticlesView& p, unsigned char* occ,
@@ -315,7 +314,7 @@ cudaError_t launch_build_neighbors(const GridView& g, int* nbr27, cudaStream_t s
 }
 
 cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const ParticlesView& out, unsigned int* keys,
-                        unsigned int* keys_alt, unsigned int* index, unsigned int* index_alt, int* counts,
+                        unsigned int* index, unsigned int* index_alt, int* counts,
                         int* cell_start, void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s,
                         bool permute) {
   const size_t ncell = (size_t)g.nb * 512;
@@ -336,7 +335,6 @@ cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const Partic
     k_sort_cells_block<<<(unsigned)(ncell / 512), 512, 0, s>>>(cell_start, index_alt);
     if (permute) k_permute<<<grid_for(in.count, 256), 256, 0, s>>>(in, out, index_alt);
   }
-  (void)keys_alt;
   return cudaGetLastError();
 }
 

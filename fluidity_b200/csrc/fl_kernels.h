@@ -112,7 +112,7 @@ cudaError_t launch_topology_from_particles(const GridView& g, const ParticlesVie
                                            size_t temp_bytes, DeviceReport* rep, cudaStream_t s);
 cudaError_t launch_build_neighbors(const GridView& g, int* nbr27, cudaStream_t s);
 cudaError_t launch_sort(const GridView& g, const ParticlesView& in, const ParticlesView& out, unsigned int* keys,
-                        unsigned int* keys_alt, unsigned int* index, unsigned int* index_alt, int* counts,
+                        unsigned int* index, unsigned int* index_alt, int* counts,
                         int* cell_start, void* temp, size_t temp_bytes, DeviceReport* rep, cudaStream_t s,
                         bool permute = true);  // false: index_alt holds the cell order, `out` is not written
 cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cell_start, float2* tiles,
