@@ -359,15 +359,40 @@ __global__ void __launch_bounds__(kThreads)
 template <typename T, int LS>
 __global__ void __launch_bounds__(512)
     k_restrict_sparse(GridView g, LevelPtrs<T> fp, const float* __restrict__ fb, float* cb, int cdx, int cdy,
-                      const int* done) {
+                      LevelPtrs<T> cp, int cparity, int seed, const int* done) {
   static_assert(LS == 1 || LS == 2, "level 0 has its own kernel");
   grid_dependency_wait();
   if (*done) return;
   constexpr int S = 1 << LS, S3 = S * S * S, BPC = 512 / S3;
+  constexpr int SC = S / 2, SC3 = SC * SC * SC;
   __shared__ float r[512];
   const int t = threadIdx.x;
   const int blk = blockIdx.x * BPC + t / S3;
   const int l = t % S3;
+  // Coarse cell of thread t < 64, and (seed) its colour-0 first sweep inputs,
+  // loaded with the fine inputs below.
+  const int cbl = t / SC3, ccl = t % SC3, cblk = blockIdx.x * BPC + cbl;
+  const bool cown = t < 64 && cblk < g.nb;
+  int out = 0;
+  bool cseed = false;
+  unsigned char cfl = 0;
+  float cdg = 1.0f;
+  if (cown) {
+    const int cx = ccl % SC, cy = (ccl / SC) % SC, cz = ccl / (SC * SC);
+    if (LS > 1) {
+      out = cblk * SC3 + ccl;
+      cseed = seed && ((cx + cy + cz) & 1) == 0;
+    } else {
+      const int X = g.coord[3 * cblk] - g.blo[0], Y = g.coord[3 * cblk + 1] - g.blo[1],
+                Z = g.coord[3 * cblk + 2] - g.blo[2];
+      out = (Z * cdy + Y) * cdx + X;
+      cseed = seed && ((X + Y + Z + cparity) & 1) == 0;
+    }
+    if (cseed) {
+      cfl = cp.fluid[out];
+      cdg = cp.diag[out];
+    }
+  }
   float res = 0.0f;
   if (blk < g.nb) {
     const int i = blk * S3 + l;
@@ -396,28 +421,17 @@ __global__ void __launch_bounds__(512)
   }
   r[t] = res;
   __syncthreads();
-  if (t < 64) {
-    constexpr int SC = S / 2, SC3 = SC * SC * SC;
-    const int bl = t / SC3, cl = t % SC3;
-    const int cblk = blockIdx.x * BPC + bl;
-    if (cblk < g.nb) {
-      const int cx = cl % SC, cy = (cl / SC) % SC, cz = cl / (SC * SC);
-      float sum = 0.0f;
+  if (cown) {
+    const int cx = ccl % SC, cy = (ccl / SC) % SC, cz = ccl / (SC * SC);
+    float sum = 0.0f;
 #pragma unroll
-      for (int dz = 0; dz < 2; ++dz)
+    for (int dz = 0; dz < 2; ++dz)
 #pragma unroll
-        for (int dy = 0; dy < 2; ++dy)
+      for (int dy = 0; dy < 2; ++dy)
 #pragma unroll
-          for (int dx = 0; dx < 2; ++dx) sum += r[bl * S3 + ((2 * cz + dz) * S + 2 * cy + dy) * S + 2 * cx + dx];
-      int out;
-      if (LS > 1) {
-        out = cblk * SC3 + cl;
-      } else {
-        out = ((g.coord[3 * cblk + 2] - g.blo[2]) * cdy + (g.coord[3 * cblk + 1] - g.blo[1])) * cdx +
-              (g.coord[3 * cblk] - g.blo[0]);
-      }
-      cb[out] = sum;
-    }
+        for (int dx = 0; dx < 2; ++dx) sum += r[cbl * S3 + ((2 * cz + dz) * S + 2 * cy + dy) * S + 2 * cx + dx];
+    cb[out] = sum;
+    if (cseed && cfl) st_T(&cp.x[out], sum / cdg);  // the coarse level's first sweep (from zero), colour 0
   }
 }
 
@@ -582,7 +596,7 @@ __global__ void __launch_bounds__(256 / CPT)
 template <typename T, int CPT>
 __global__ void __launch_bounds__(512 / CPT)
     k_restrict0_tiled(GridView g, LevelPtrs<T> fp, const float* __restrict__ fb, float* __restrict__ cb,
-                      const int* done) {
+                      LevelPtrs<T> cp, int seed, const int* done) {
   constexpr int NT = 512 / CPT;
   static_assert(NT >= 64, "one thread per level-1 cell of the block");
   grid_dependency_wait();
@@ -601,6 +615,10 @@ __global__ void __launch_bounds__(512 / CPT)
     bi[k] = fb[i];
     xv[k] = ld(&fp.x[i]);
   }
+  // (seed) level-1 cell t < 64: colour-0 first-sweep inputs, loaded with the rest
+  const bool cseed = seed && t < 64 && (((t & 3) + ((t >> 2) & 3) + (t >> 4)) & 1) == 0;
+  const unsigned char cfl = cseed ? cp.fluid[blk * 64 + t] : 0;
+  const float cdg = cseed ? cp.diag[blk * 64 + t] : 1.0f;
   load_halo0<NT, 384, false>(g, blk, 0, &halo[0][0], [&](int j) { return ld(&fp.x[rb_id(j)]); });
 #pragma unroll
   for (int k = 0; k < CPT; ++k) tile[nat_of(t + k * NT)] = xv[k];
@@ -623,6 +641,7 @@ __global__ void __launch_bounds__(512 / CPT)
 #pragma unroll
         for (int dx = 0; dx < 2; ++dx) sum += r[((2 * cz + dz) << 6) | ((2 * cy + dy) << 3) | (2 * cx + dx)];
     cb[blk * 64 + t] = sum;
+    if (cseed && cfl) st_T(&cp.x[blk * 64 + t], sum / cdg);  // level 1's first sweep (from zero), colour 0
   }
 }
 
@@ -748,12 +767,16 @@ __global__ void k_smooth_dense(LevelDesc L, LevelPtrs<T> lp, const float* __rest
 // neighbour loads are issued before the sum.
 template <typename T>
 __global__ void k_restrict_dense(LevelDesc F, LevelPtrs<T> fp, const float* __restrict__ fb, LevelDesc C, float* cb,
-                                 const int* done) {
+                                 LevelPtrs<T> cp, int seed, const int* done) {
   grid_dependency_wait();
   if (*done) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= C.count) return;
   const int X = i % C.dim[0], Y = (i / C.dim[0]) % C.dim[1], Z = i / (C.dim[0] * C.dim[1]);
+  // (seed) the coarse level's colour-0 first sweep inputs, loaded with the children's
+  const bool cseed = seed && ((X + Y + Z + C.parity) & 1) == 0;
+  const unsigned char cfl = cseed ? cp.fluid[i] : 0;
+  const float cdg = cseed ? cp.diag[i] : 1.0f;
   float sum = 0.0f;
 #pragma unroll
   for (int ch = 0; ch < 8; ++ch) {
@@ -785,6 +808,7 @@ __global__ void k_restrict_dense(LevelDesc F, LevelPtrs<T> fp, const float* __re
     }
   }
   cb[i] = sum;
+  if (cseed && cfl) st_T(&cp.x[i], sum / cdg);  // the coarse level's first sweep (from zero), colour 0
 }
 
 // Coarsest level: symmetric red-black sweeps in shared memory, one CTA.
@@ -1560,9 +1584,12 @@ static void smooth(const GridView& g, const MgHierarchy<T>& H, int l, const floa
     launch_dep(k_smooth_dense<T, 0>, grid, kThreads, 0, s, D, H.ptr[l], bl, color, C, nullptr, done);
 }
 
+// Residual of level l restricted to level l + 1; with `seed`, the restriction
+// also performs level l + 1's first pre-smoothing sweep (colour 0 from zero:
+// x = b / diag on fluid cells), which then needs no launch of its own.
 template <typename T>
-static void restrict_level(const GridView& g, const MgHierarchy<T>& H, int l, const float* bl, const int* done,
-                           cudaStream_t s) {
+static void restrict_level(const GridView& g, const MgHierarchy<T>& H, int l, const float* bl, bool seed,
+                           const int* done, cudaStream_t s) {
   const LevelDesc& C = H.desc[l + 1];
   ++g_kernel_launches;
   if (l < 3) {
@@ -1570,14 +1597,18 @@ static void restrict_level(const GridView& g, const MgHierarchy<T>& H, int l, co
     const int bpc = 512 / S3;
     const unsigned grid = (unsigned)((g.nb + bpc - 1) / bpc);
     if (l == 0)
-      launch_dep(k_restrict0_tiled<T, kRestrict0Cpt>, g.nb, 512 / kRestrict0Cpt, 0, s, g, H.ptr[0], bl, H.b[1], done);
+      launch_dep(k_restrict0_tiled<T, kRestrict0Cpt>, g.nb, 512 / kRestrict0Cpt, 0, s, g, H.ptr[0], bl, H.b[1],
+                 H.ptr[1], (int)seed, done);
     else if (l == 1)
-      launch_dep(k_restrict_sparse<T, 2>, grid, 512, 0, s, g, H.ptr[1], bl, H.b[2], C.dim[0], C.dim[1], done);
+      launch_dep(k_restrict_sparse<T, 2>, grid, 512, 0, s, g, H.ptr[1], bl, H.b[2], C.dim[0], C.dim[1], H.ptr[2],
+                 C.parity, (int)seed, done);
     else
-      launch_dep(k_restrict_sparse<T, 1>, grid, 512, 0, s, g, H.ptr[2], bl, H.b[3], C.dim[0], C.dim[1], done);
+      launch_dep(k_restrict_sparse<T, 1>, grid, 512, 0, s, g, H.ptr[2], bl, H.b[3], C.dim[0], C.dim[1], H.ptr[3],
+                 C.parity, (int)seed, done);
     return;
   }
-  launch_dep(k_restrict_dense<T>, blocks_for(C.count), kThreads, 0, s, H.desc[l], H.ptr[l], bl, C, H.b[l + 1], done);
+  launch_dep(k_restrict_dense<T>, blocks_for(C.count), kThreads, 0, s, H.desc[l], H.ptr[l], bl, C, H.b[l + 1],
+             H.ptr[l + 1], (int)seed, done);
 }
 
 template <typename T>
@@ -1590,13 +1621,13 @@ static void vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r0, 
   const int top = tail ? L - 2 : L - 1;  // levels smoothed by the per-level kernels: [0, top)
   for (int l = 0; l < top; ++l) {
     const float* bl = l == 0 ? r0 : H.b[l];
-    smooth<T>(g, H, l, bl, 0, 1, done, s);
+    if (l == 0) smooth<T>(g, H, l, bl, 0, 1, done, s);  // above level 0, the restriction did this sweep
     smooth<T>(g, H, l, bl, 1, 0, done, s);
     for (int sw = 1; sw < opt.pre; ++sw) {
       smooth<T>(g, H, l, bl, 0, 0, done, s);
       smooth<T>(g, H, l, bl, 1, 0, done, s);
     }
-    restrict_level<T>(g, H, l, bl, done, s);
+    restrict_level<T>(g, H, l, bl, l + 1 < top, done, s);
   }
   if (tail) {
     const LevelDesc& F = H.desc[L - 2];
