@@ -71,14 +71,23 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
   __syncthreads();
   const int bc[3] = {g.coord[3 * b] * 8, g.coord[3 * b + 1] * 8, g.coord[3 * b + 2] * 8};
   const float four_inv_h = 4.0f * g.inv_h;  // fitted slopes 4 sum w u r / h (one multiply instead of a division)
-  for (int q = pbeg + t; q < pend; q += kG2PThreads) {
-    float xw[3], X[3];
-    int cell[3];
-    bool inside = true;
+  // Position of particle q (read through the cell order in step mode); the
+  // next particle's is loaded one iteration ahead, so its two dependent loads
+  // overlap the current particle's work.
+  auto load_x = [&](int q, float out[3]) {
     const int src = (!kFull && prm.order != nullptr) ? (int)prm.order[q] : -1;
 #pragma unroll
+    for (int d = 0; d < 3; ++d) out[d] = src >= 0 ? prm.x_in[d][src] : p.x[d][q];
+  };
+  float xnext[3] = {0.0f, 0.0f, 0.0f};
+  if (pbeg + t < pend) load_x(pbeg + t, xnext);
+  for (int q = pbeg + t; q < pend; q += kG2PThreads) {
+    float xw[3] = {xnext[0], xnext[1], xnext[2]}, X[3];
+    if (q + kG2PThreads < pend) load_x(q + kG2PThreads, xnext);
+    int cell[3];
+    bool inside = true;
+#pragma unroll
     for (int d = 0; d < 3; ++d) {
-      xw[d] = src >= 0 ? prm.x_in[d][src] : p.x[d][q];
       X[d] = lattice_coord(g, xw[d], d);
       cell[d] = __float2int_rd(X[d]);
       inside = inside && cell[d] >= bc[d] && cell[d] < bc[d] + 8;
