@@ -159,8 +159,10 @@ def test_step_is_bitwise_reproducible():
 
 
 @pytest.mark.parametrize("precision,tol", [(0, 1e-5), (1, 3e-2)])
-def test_vcycle_matches_fp64_restatement(precision, tol):
-    n = 32
+@pytest.mark.parametrize("n,levels", [(32, 4), (64, 5)])
+def test_vcycle_matches_fp64_restatement(precision, tol, n, levels):
+    """One V-cycle against the FP64 restatement. At 64^3 with 5 levels the last
+    dense level (8^3) and the coarsest (4^3) run in the one-CTA coarse tail."""
     ctx, soa, m = dam_break_context(n)
     ctx.step(fb.transfer_params(scenes.DT, m), fb.default_pressure_options())
     blocks = ctx.active_blocks()
@@ -179,12 +181,12 @@ def test_vcycle_matches_fp64_restatement(precision, tol):
     import torch
     r_dev = torch.from_numpy(r_sparse).cuda()
     z_dev = torch.zeros_like(r_dev)
-    opt = fb.default_pressure_options(precision=precision)
+    opt = fb.default_pressure_options(precision=precision, levels=levels)
     assert lib.fl_apply_vcycle(ctx.handle, ctypes.c_void_p(r_dev.data_ptr()), ctypes.c_void_p(z_dev.data_ptr()),
                                ctypes.byref(opt), None) == fb.OK
     torch.cuda.synchronize()
     z = fb.sparse_cells_to_dense(blocks, z_dev.cpu().numpy(), (n, n, n))
-    zo = oracle.vcycle(box_for(n), ct, r_dense, levels=4, pre=opt.pre_sweeps, post=opt.post_sweeps,
+    zo = oracle.vcycle(box_for(n), ct, r_dense, levels=levels, pre=opt.pre_sweeps, post=opt.post_sweeps,
                        coarse_sweeps=opt.coarse_sweeps)
     assert rel_err(z, zo, ct == 1) <= tol
 
