@@ -176,7 +176,11 @@ int fl_g2p(fl_context* ctx, fl_particles* sorted, const float* const u_new[3], c
            float dt, float* full_out, void* stream, fl_report* report);
 
 /* One full liquid substep on the context-resident particle state:
- * topology -> sort -> P2G (+normalize, gravity, walls) -> pressure -> G2P (+advect). */
+ * topology -> sort -> P2G (+normalize, gravity, walls) -> pressure -> G2P (+advect).
+ * The sort computes the cell order without moving the particles; P2G reads the
+ * state through it and G2P writes the advected state, in cell order, into the
+ * context's other particle buffer, which is the state after the call (take
+ * fresh pointers from fl_state_particles after each step). */
 int fl_step(fl_context* ctx, const fl_transfer_params* params, const fl_pressure_options* options,
             fl_pressure_diagnostics* diagnostics, void* stream, fl_report* report);
 
@@ -185,7 +189,7 @@ int fl_step(fl_context* ctx, const fl_transfer_params* params, const fl_pressure
 int fl_step_timings(fl_context* ctx, float* ms);
 
 /* Host-side counts of kernels launched by this library since load: its own
- * kernels, and device-wide CUB algorithm invocations (radix sort, scans). */
+ * kernels, and device-wide CUB algorithm invocations (exclusive scans). */
 int fl_kernel_launches(unsigned long long* own, unsigned long long* library);
 
 /* Context-resident particle state and buffers (device pointers). fl_step
