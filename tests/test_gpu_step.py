@@ -208,6 +208,34 @@ def test_sort_is_a_stable_cell_permutation():
     assert cs[0] == 0 and cs[-1] == soa.shape[1] and np.all(np.diff(cs) >= 0)
 
 
+def test_sort_handles_crowded_blocks():
+    """A block holding more particles than the sort stages in shared memory
+    (12,288) sorts its cells in place; the order is still the stable cell sort,
+    next to a block that takes the staged path."""
+    n = 32
+    rng = np.random.default_rng(5)
+    crowded, normal = 20000, 3000
+    x = np.concatenate([rng.uniform(8.0 / n, 16.0 / n, size=(3, crowded)),
+                        rng.uniform([[16.0 / n], [8.0 / n], [8.0 / n]], [[24.0 / n], [16.0 / n], [16.0 / n]],
+                                    size=(3, normal))], axis=1)
+    soa = np.zeros((15, crowded + normal), np.float32)
+    soa[0:3] = x[:, rng.permutation(x.shape[1])]
+    soa[3:6] = rng.normal(scale=0.1, size=(3, soa.shape[1]))
+    ctx = fb.LiquidContext(n, capacity=soa.shape[1])
+    ctx.upload(soa)
+    code, diag = ctx.step(fb.transfer_params(0.0, 1.0 / (8 * n ** 3), gravity=(0, 0, 0)),
+                          fb.default_pressure_options())
+    assert code == fb.OK
+    out = ctx.download()
+    perm = sort_permutation(soa, n)
+    np.testing.assert_array_equal(out[0:3], soa[0:3, perm])  # dt = 0, far from the walls: x unchanged
+    f = ctx.fields()
+    nb = len(ctx.active_blocks())
+    cs = fb.copy_to_host(f["cell_start"], nb * 512 + 1, np.int32)
+    assert cs[0] == 0 and cs[-1] == soa.shape[1] and np.all(np.diff(cs) >= 0)
+    ctx.close()
+
+
 def test_empty_and_invalid_particles():
     ctx = fb.LiquidContext(32, capacity=64)
     ctx.upload(np.zeros((15, 0), np.float32))
