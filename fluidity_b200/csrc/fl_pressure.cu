@@ -1547,9 +1547,8 @@ static void smooth_sparse(const GridView& g, const MgHierarchy<T>& H, int l, con
   const LevelDesc& C = H.desc[l + 1];
   const T* xc = H.ptr[l + 1].x;
   ++g_kernel_launches;
-  if (mode == 1)
-    launch_dep(k_smooth_sparse<T, LS, 1>, grid, kThreads, 0, s, g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
-  else if (mode == 2)
+  // (mode 1, the first sweep from zero, is done by the restriction into this level)
+  if (mode == 2)
     launch_dep(k_smooth_sparse<T, LS, 2>, grid, kThreads, 0, s, g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
   else
     launch_dep(k_smooth_sparse<T, LS, 0>, grid, kThreads, 0, s, g, H.ptr[l], bl, color, xc, C.dim[0], C.dim[1], done);
@@ -1576,9 +1575,8 @@ static void smooth(const GridView& g, const MgHierarchy<T>& H, int l, const floa
   const LevelDesc& C = H.desc[l + 1 < H.levels ? l + 1 : l];
   const unsigned grid = blocks_for(D.count);
   ++g_kernel_launches;
-  if (mode == 1)
-    launch_dep(k_smooth_dense<T, 1>, grid, kThreads, 0, s, D, H.ptr[l], bl, color, C, nullptr, done);
-  else if (mode == 2)
+  // (mode 1, the first sweep from zero, is done by the restriction into this level)
+  if (mode == 2)
     launch_dep(k_smooth_dense<T, 2>, grid, kThreads, 0, s, D, H.ptr[l], bl, color, C, H.ptr[l + 1].x, done);
   else
     launch_dep(k_smooth_dense<T, 0>, grid, kThreads, 0, s, D, H.ptr[l], bl, color, C, nullptr, done);
