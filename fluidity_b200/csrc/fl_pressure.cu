@@ -470,12 +470,28 @@ __device__ __forceinline__ int halo_src0_colour(const GridView& g, int blk, int 
   return nbb * 512 + ((z << 6) | (y << 3) | x);
 }
 
+// Level-0 staging in shared memory: a 10^3 shell around the 8^3 block. Natural
+// local cell (x,y,z) sits at (z+1)*100 + (y+1)*10 + x+1; the face cells of the
+// six neighbouring blocks fill the outer layer (edges and corners stay unused),
+// so every face neighbour is at a constant offset: +-1, +-10, +-100.
+constexpr int kShell0 = 1000;
+__device__ __forceinline__ int sidx(int l) { return ((l >> 6) + 1) * 100 + (((l >> 3) & 7) + 1) * 10 + (l & 7) + 1; }
+
+// Shell position of halo slot f * 64 + w * 8 + u (face f = 2a + (dir > 0);
+// (u, w) the two transverse coordinates in increasing axis order).
+__device__ __forceinline__ int shell_of_slot(int slot) {
+  const int f = slot >> 6, q = slot & 63, a = f >> 1, c = (f & 1) ? 9 : 0;
+  const int u = (q & 7) + 1, w = (q >> 3) + 1;
+  return a == 0 ? w * 100 + u * 10 + c : (a == 1 ? w * 100 + c * 10 + u : c * 100 + w * 10 + u);
+}
+
 // The halo entries e = t + k * NT (< COUNT) of thread t, loaded in two batches
 // (every neighbour-block lookup, then every value) before any shared store, so
-// a CTA waits for two memory round trips whatever its cells per thread.
-// value(j) maps a neighbour's natural cell id to the staged value.
+// a CTA waits for two memory round trips whatever its cells per thread; each
+// value goes to its place in the shell. value(j) maps a neighbour's natural
+// cell id to the staged value.
 template <int NT, int COUNT, bool kColour, typename V, typename F>
-__device__ __forceinline__ void load_halo0(const GridView& g, int blk, int oc, V* halo, F value) {
+__device__ __forceinline__ void load_halo0(const GridView& g, int blk, int oc, V* shell, F value) {
   constexpr int PER = (COUNT + NT - 1) / NT;
   const int t = threadIdx.x;
   int src[PER], slot[PER];
@@ -491,35 +507,23 @@ __device__ __forceinline__ void load_halo0(const GridView& g, int blk, int oc, V
   for (int k = 0; k < PER; ++k) v[k] = src[k] >= 0 ? value(src[k]) : V(0);
 #pragma unroll
   for (int k = 0; k < PER; ++k)
-    if (slot[k] >= 0) halo[slot[k]] = v[k];
+    if (slot[k] >= 0) shell[shell_of_slot(slot[k])] = v[k];
 }
 
-// Value of the neighbour of natural local cell (x,y,z) across axis a / dir,
-// from the in-block tile or the face halo.
+// Offsets of the six face neighbours in the shell, in axis/direction order.
+__device__ __forceinline__ int shell_off(int q) {
+  return (q & 1 ? 1 : -1) * (q < 2 ? 1 : (q < 4 ? 10 : 100));
+}
+
+// A (natural local cell at shell position i) applied to the staged shell minus
+// the diagonal term: the sum of the neighbour values across the open faces in
+// m, in axis/direction order.
 template <typename V>
-__device__ __forceinline__ V tile_nbr0(const V* tile, const V (*halo)[64], int x, int y, int z, int a, int dir) {
-  const int c = a == 0 ? x : (a == 1 ? y : z);
-  if (dir < 0 ? c > 0 : c < 7) {
-    const int step = 1 << (3 * a);
-    return tile[((z << 6) | (y << 3) | x) + dir * step];
-  }
-  const int q = a == 0 ? (z << 3) | y : (a == 1 ? (z << 3) | x : (y << 3) | x);
-  return halo[2 * a + (dir > 0 ? 1 : 0)][q];
-}
-
-// A (natural local cell l) applied to the staged tile and halo, minus the
-// diagonal term: the sum of the neighbour values across the open faces in m.
-__device__ __forceinline__ float nbr_sum0(const float* tile, const float (*halo)[64], int l, unsigned m) {
-  const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
-  float s = 0.0f;
+__device__ __forceinline__ V nbr_sum0(const V* sh, int i, unsigned m) {
+  V s = V(0);
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-#pragma unroll
-    for (int dir = -1; dir <= 1; dir += 2) {
-      if (!((m >> (2 * a + (dir > 0 ? 1 : 0))) & 1u)) continue;
-      s += tile_nbr0(tile, halo, cx, cy, cz, a, dir);
-    }
-  }
+  for (int q = 0; q < 6; ++q)
+    if ((m >> q) & 1u) s += sh[i + shell_off(q)];
   return s;
 }
 
@@ -550,8 +554,7 @@ __global__ void __launch_bounds__(256 / CPT)
   constexpr int NT = 256 / CPT;
   grid_dependency_wait();
   if (*done) return;
-  __shared__ float tile[512];
-  __shared__ float halo[6][64];
+  __shared__ float sh[kShell0];
   const int blk = blockIdx.x, t = threadIdx.x;
   const T* __restrict__ x = lp.x;
   unsigned m[CPT];
@@ -572,13 +575,13 @@ __global__ void __launch_bounds__(256 / CPT)
       v[k] = ld(&x[blk * 512 + c]);
       if (MODE == 2) v[k] += ld(&xc[parent1_of_nat(blk * 512 + nat_of(c))]);
     }
-    load_halo0<NT, 192, true>(g, blk, oc, &halo[0][0], [&](int j) {
+    load_halo0<NT, 192, true>(g, blk, oc, sh, [&](int j) {
       float hv = ld(&x[rb_id(j)]);
       if (MODE == 2) hv += ld(&xc[parent1_of_nat(j)]);
       return hv;
     });
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) tile[nat_of((oc << 8) + t + k * NT)] = v[k];
+    for (int k = 0; k < CPT; ++k) sh[sidx(nat_of((oc << 8) + t + k * NT))] = v[k];
     __syncthreads();
   }
 #pragma unroll
@@ -586,7 +589,7 @@ __global__ void __launch_bounds__(256 / CPT)
     if (!(m[k] & 64u)) continue;
     const int c = (color << 8) + t + k * NT;
     float s = bi[k];
-    if (MODE != 1) s += nbr_sum0(tile, halo, nat_of(c), m[k]);
+    if (MODE != 1) s += nbr_sum0(sh, sidx(nat_of(c)), m[k]);
     st_T(&lp.x[blk * 512 + c], s / di[k]);
   }
 }
@@ -601,8 +604,7 @@ __global__ void __launch_bounds__(512 / CPT)
   static_assert(NT >= 64, "one thread per level-1 cell of the block");
   grid_dependency_wait();
   if (*done) return;
-  __shared__ float tile[512];
-  __shared__ float halo[6][64];
+  __shared__ float sh[kShell0];
   __shared__ float r[512];
   const int blk = blockIdx.x, t = threadIdx.x;
   unsigned m[CPT];
@@ -619,15 +621,15 @@ __global__ void __launch_bounds__(512 / CPT)
   const bool cseed = seed && t < 64 && (((t & 3) + ((t >> 2) & 3) + (t >> 4)) & 1) == 0;
   const unsigned char cfl = cseed ? cp.fluid[blk * 64 + t] : 0;
   const float cdg = cseed ? cp.diag[blk * 64 + t] : 1.0f;
-  load_halo0<NT, 384, false>(g, blk, 0, &halo[0][0], [&](int j) { return ld(&fp.x[rb_id(j)]); });
+  load_halo0<NT, 384, false>(g, blk, 0, sh, [&](int j) { return ld(&fp.x[rb_id(j)]); });
 #pragma unroll
-  for (int k = 0; k < CPT; ++k) tile[nat_of(t + k * NT)] = xv[k];
+  for (int k = 0; k < CPT; ++k) sh[sidx(nat_of(t + k * NT))] = xv[k];
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < CPT; ++k) {
     const int l = nat_of(t + k * NT);
     float res = 0.0f;
-    if (m[k] & 64u) res = bi[k] - (di[k] * xv[k] - nbr_sum0(tile, halo, l, m[k]));
+    if (m[k] & 64u) res = bi[k] - (di[k] * xv[k] - nbr_sum0(sh, sidx(l), m[k]));
     r[l] = res;
   }
   __syncthreads();
@@ -654,8 +656,7 @@ __global__ void __launch_bounds__(512 / CPT)
   constexpr int NT = 512 / CPT;
   grid_dependency_wait();
   if (st->done) return;
-  __shared__ float tile[512];
-  __shared__ float halo[6][64];
+  __shared__ float sh[kShell0];
   __shared__ double red[NT / 32];
   const int blk = blockIdx.x, t = threadIdx.x;
   const float beta = (float)st->beta;
@@ -670,19 +671,19 @@ __global__ void __launch_bounds__(512 / CPT)
     const float zi = ld(&z[i]), dold = d_old[i];
     di[k] = (m[k] & 64u) ? (first ? zi : fmaf(beta, dold, zi)) : 0.0f;
   }
-  load_halo0<NT, 384, false>(g, blk, 0, &halo[0][0], [&](int j) {
+  load_halo0<NT, 384, false>(g, blk, 0, sh, [&](int j) {
     const int r = rb_id(j);
     return first ? ld(&z[r]) : fmaf(beta, d_old[r], ld(&z[r]));
   });
 #pragma unroll
-  for (int k = 0; k < CPT; ++k) tile[nat_of(t + k * NT)] = di[k];
+  for (int k = 0; k < CPT; ++k) sh[sidx(nat_of(t + k * NT))] = di[k];
   __syncthreads();
   double dq = 0.0;
 #pragma unroll
   for (int k = 0; k < CPT; ++k) {
     const int i = blk * 512 + t + k * NT;
     float qi = 0.0f;
-    if (m[k] & 64u) qi = dg[k] * di[k] - nbr_sum0(tile, halo, nat_of(t + k * NT), m[k]);
+    if (m[k] & 64u) qi = dg[k] * di[k] - nbr_sum0(sh, sidx(nat_of(t + k * NT)), m[k]);
     d_new[i] = di[k];
     q[i] = qi;
     dq += (double)di[k] * (double)qi;
@@ -1064,8 +1065,7 @@ __global__ void __launch_bounds__(512 / CPT)
     k_residual64_tiled(GridView g, LevelPtrs<T> L0, const double* __restrict__ b64, const double* __restrict__ p64,
                        float* __restrict__ r, float* __restrict__ e, double* partial) {
   constexpr int NT = 512 / CPT;
-  __shared__ double tile[512];
-  __shared__ double halo[6][64];
+  __shared__ double sh[kShell0];
   __shared__ double red[NT / 32];
   const int blk = blockIdx.x, t = threadIdx.x;
   unsigned m[CPT];
@@ -1078,21 +1078,20 @@ __global__ void __launch_bounds__(512 / CPT)
     pi[k] = p64[i];
     dg[k] = (double)L0.diag[i];
   }
-  load_halo0<NT, 384, false>(g, blk, 0, &halo[0][0], [&](int j) { return p64[rb_id(j)]; });
+  load_halo0<NT, 384, false>(g, blk, 0, sh, [&](int j) { return p64[rb_id(j)]; });
 #pragma unroll
-  for (int k = 0; k < CPT; ++k) tile[nat_of(t + k * NT)] = pi[k];
+  for (int k = 0; k < CPT; ++k) sh[sidx(nat_of(t + k * NT))] = pi[k];
   __syncthreads();
   double rr = 0.0;
 #pragma unroll
   for (int k = 0; k < CPT; ++k) {
-    const int i = blk * 512 + t + k * NT, l = nat_of(t + k * NT);
-    const int cx = l & 7, cy = (l >> 3) & 7, cz = l >> 6;
+    const int i = blk * 512 + t + k * NT, si = sidx(nat_of(t + k * NT));
     double res = 0.0;
     if (m[k] & 64u) {  // (A p)_i = diag_i p_i - the fluid neighbours, in axis/direction order
       double ax = dg[k] * pi[k];
 #pragma unroll
       for (int q = 0; q < 6; ++q)
-        if ((m[k] >> q) & 1u) ax -= tile_nbr0(tile, halo, cx, cy, cz, q >> 1, (q & 1) ? 1 : -1);
+        if ((m[k] >> q) & 1u) ax -= sh[si + shell_off(q)];
       res = bi[k] - ax;
     }
     r[i] = (float)res;
