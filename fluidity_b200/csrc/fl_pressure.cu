@@ -903,7 +903,7 @@ constexpr int kTailThreads = 1024;
 constexpr int kTailCpt = kTailMaxCells / kTailThreads;
 
 __host__ __device__ constexpr size_t tail_smem_bytes(int nf, int nc) {
-  return sizeof(float) * (6 * (size_t)nf + 6 * (size_t)nc) + (size_t)nf;
+  return sizeof(float) * (7 * (size_t)nf + 6 * (size_t)nc) + (size_t)nf;
 }
 
 template <typename T>
@@ -922,7 +922,8 @@ __global__ void __launch_bounds__(kTailThreads)
   float* bc = xc + nc;           // C right-hand side
   float* dc = bc + nc;           // C diagonal of fluid cells, 0 elsewhere
   float* kc[3] = {dc + nc, dc + 2 * nc, dc + 3 * nc};
-  unsigned char* ff = reinterpret_cast<unsigned char*>(kc[2] + nc);  // F fluid flags
+  float* rf = kc[2] + nc;        // F residual before the restriction
+  unsigned char* ff = reinterpret_cast<unsigned char*>(rf + nf);  // F fluid flags
   const int t = threadIdx.x;
   for (int i = t; i < nf; i += kTailThreads) {
     x[i] = 0.0f;
@@ -938,37 +939,45 @@ __global__ void __launch_bounds__(kTailThreads)
 #pragma unroll
     for (int a = 0; a < 3; ++a) kc[a][i] = ld(&cp.k[a][i]);
   }
-  // This thread's F cells: coordinates and colour.
-  int cx[kTailCpt], cy[kTailCpt], cz[kTailCpt], col[kTailCpt];
+  // This thread's F cells, worked out once (in `info`): the in-range face
+  // neighbours (bits 0-5, axis/direction order), the colour (bit 6) and
+  // whether the cell exists (bit 7).
+  const int nx = F.dim[0], nxy = F.dim[0] * F.dim[1];
+  unsigned info[kTailCpt];
 #pragma unroll
   for (int j = 0; j < kTailCpt; ++j) {
     const int i = t + j * kTailThreads;
-    cx[j] = i % F.dim[0];
-    cy[j] = (i / F.dim[0]) % F.dim[1];
-    cz[j] = i / (F.dim[0] * F.dim[1]);
-    col[j] = (cx[j] + cy[j] + cz[j] + F.parity) & 1;
+    const int c0 = i % nx, c1 = (i / nx) % F.dim[1], c2 = i / nxy;
+    unsigned m = 0;
+    m |= (c0 > 0 ? 1u : 0u) | (c0 + 1 < F.dim[0] ? 2u : 0u);
+    m |= (c1 > 0 ? 4u : 0u) | (c1 + 1 < F.dim[1] ? 8u : 0u);
+    m |= (c2 > 0 ? 16u : 0u) | (c2 + 1 < F.dim[2] ? 32u : 0u);
+    info[j] = m | ((unsigned)((c0 + c1 + c2 + F.parity) & 1) << 6) | (i < nf ? 128u : 0u);
   }
+  const int off[6] = {-1, 1, -nx, nx, -nxy, nxy};  // face neighbours in axis/direction order
   __syncthreads();
   // One colour sweep on F: mode 1 from zero, mode 2 with the coarse correction
   // added to the neighbour values read (as k_smooth_dense).
   auto sweep = [&](int color, int mode) {
 #pragma unroll
     for (int j = 0; j < kTailCpt; ++j) {
+      const unsigned inf = info[j];
       const int i = t + j * kTailThreads;
-      if (i >= nf || col[j] != color || !ff[i]) continue;
+      if (!(inf & 128u) || (int)((inf >> 6) & 1u) != color || !ff[i]) continue;
       float s = bf[i];
       if (mode != 1) {
-        const int c[3] = {cx[j], cy[j], cz[j]};
+        const int c[3] = {i % nx, (i / nx) % F.dim[1], i / nxy};  // used by mode 2 only
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
-          const int a = q >> 1, dir = (q & 1) ? 1 : -1;
-          int n[3] = {c[0], c[1], c[2]};
-          n[a] += dir;
-          if (n[a] < 0 || n[a] >= F.dim[a]) continue;
-          const int jn = dense_id(F, n[0], n[1], n[2]);
-          const float kq = dir < 0 ? kf[a][i] : kf[a][jn];
+          if (!((inf >> q) & 1u)) continue;
+          const int a = q >> 1, jn = i + off[q];
+          const float kq = (q & 1) ? kf[a][jn] : kf[a][i];
           float xv = x[jn];
-          if (mode == 2) xv += xc[dense_id(C, n[0] >> 1, n[1] >> 1, n[2] >> 1)];
+          if (mode == 2) {
+            int n[3] = {c[0], c[1], c[2]};
+            n[a] += (q & 1) ? 1 : -1;
+            xv += xc[dense_id(C, n[0] >> 1, n[1] >> 1, n[2] >> 1)];
+          }
           if (kq != 0.0f) s = fmaf(kq, xv, s);
         }
       }
@@ -982,7 +991,24 @@ __global__ void __launch_bounds__(kTailThreads)
     sweep(0, 0);
     sweep(1, 0);
   }
-  // Residual of F restricted to C (as k_restrict_dense), one thread per C cell.
+  // Residual of F (every cell, all threads), then restricted to C in the
+  // children order of k_restrict_dense, one thread per C cell.
+#pragma unroll
+  for (int j = 0; j < kTailCpt; ++j) {
+    const unsigned inf = info[j];
+    const int i = t + j * kTailThreads;
+    if (!(inf & 128u) || !ff[i]) continue;
+    float ax = df[i] * x[i];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      if (!((inf >> q) & 1u)) continue;
+      const int a = q >> 1, jn = i + off[q];
+      const float kq = (q & 1) ? kf[a][jn] : kf[a][i];
+      if (kq != 0.0f) ax = fmaf(-kq, x[jn], ax);
+    }
+    rf[i] = bf[i] - ax;
+  }
+  __syncthreads();
   for (int I = t; I < nc; I += kTailThreads) {
     const int X = I % C.dim[0], Y = (I / C.dim[0]) % C.dim[1], Z = I / (C.dim[0] * C.dim[1]);
     float sum = 0.0f;
@@ -991,19 +1017,7 @@ __global__ void __launch_bounds__(kTailThreads)
       const int c[3] = {2 * X + (ch & 1), 2 * Y + ((ch >> 1) & 1), 2 * Z + (ch >> 2)};
       if (c[0] >= F.dim[0] || c[1] >= F.dim[1] || c[2] >= F.dim[2]) continue;
       const int id = dense_id(F, c[0], c[1], c[2]);
-      if (!ff[id]) continue;
-      float ax = df[id] * x[id];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        const int a = q >> 1, dir = (q & 1) ? 1 : -1;
-        int n[3] = {c[0], c[1], c[2]};
-        n[a] += dir;
-        if (n[a] < 0 || n[a] >= F.dim[a]) continue;
-        const int jn = dense_id(F, n[0], n[1], n[2]);
-        const float kq = dir < 0 ? kf[a][id] : kf[a][jn];
-        if (kq != 0.0f) ax = fmaf(-kq, x[jn], ax);
-      }
-      sum += bf[id] - ax;
+      if (ff[id]) sum += rf[id];
     }
     bc[I] = sum;
     cb[I] = sum;
