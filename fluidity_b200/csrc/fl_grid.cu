@@ -11,7 +11,8 @@
 // arrival rank in its cell, an exclusive scan gives cell_start, original
 // indices are scattered to (cell_start + rank), each cell's indices are sorted
 // ascending -- the result equals a stable sort, so it is reproducible run to
-// run -- and the SoA arrays are gathered once. The reference sorts by
+// run. The operator-level sort then gathers the SoA arrays once; the step does
+// not move the particles (P2G and G2P read through the cell order). The reference sorts by
 // the signed bin floor((X - 1.5)/4) with CUB (native/cuda/liquid_arena_3d.cu:29-52);
 // with 8^3 blocks and per-step re-binning the bin is simply the containing cell.
 #include <cub/device/device_scan.cuh>

@@ -20,13 +20,15 @@
 //   p64 += e.
 // V-cycle: levels 0-2 live inside each 8^3 block (8^3, 4^3, 2^3 cells), levels
 // >= 3 are dense over the block lattice; piecewise-constant prolongation, sum
-// restriction, coarse coefficients = (sum of crossing fine coefficients)/2 and
-// coarse anchors = (sum of child anchors)/2 (for uniform coefficients this is
-// the rediscretized 2^l-scaled operator); red-black Gauss-Seidel, `pre` sweeps
-// red->black before and `post` sweeps black->red after the coarse correction
-// (symmetric); the coarsest level is solved by `coarse_sweeps` symmetric sweeps
-// inside one CTA's shared memory. x and k are stored as T (FP32 or BF16),
-// arithmetic is FP32.
+// restriction, coarse coefficients = (sum of crossing fine coefficients)/2 (for
+// uniform coefficients the rediscretized 2^l-scaled operator) and coarse
+// anchors = 0.8 x (sum of child anchors) (kCoarseAnchorScale); red-black
+// Gauss-Seidel, `pre` sweeps red->black before and `post` sweeps black->red
+// after the coarse correction (symmetric); the restriction into a level also
+// performs that level's first sweep; the coarsest level is solved by
+// `coarse_sweeps` symmetric sweeps inside one CTA's shared memory, together
+// with the last dense level when both fit (k_coarse_tail). x and k are stored
+// as T (FP32 or BF16), arithmetic is FP32.
 #include <cuda_bf16.h>
 
 #include "fl_internal.cuh"
