@@ -235,20 +235,52 @@ def run_ours(args, world, rank, local):
     value = whole_job_rate(world, args.steps, ms)
     # allocated cells over the timed steps (the splash spreads): the mean of the first and last counts
     ncell = (nb_first + nb_last) // 2 * 512
-    # end-to-end through the C-ABI with pinned host buffers: H2D state, step, D2H state
+    # End to end through the C-ABI from pinned host memory, every step: the H2D
+    # upload of the step's input, the step, and the D2H of its result through the
+    # snapshot queue (device check + copy on the queue's own stream, so the D2H of
+    # step k overlaps the H2D of step k + 1), finished and read on the host.
     pin_in = torch.from_numpy(soa).pin_memory()
     pin_out = torch.empty_like(pin_in).pin_memory()
     host_in, host_out = pin_in.numpy(), pin_out.numpy()
+    queue = fb.SnapshotQueue(ctx)
     e2e_steps = max(2, min(args.steps, 5))
-    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    probe = 0.0
+
+    def take(ticket):
+        nonlocal probe
+        if queue.wait(ticket) != fb.SNAPSHOT_READY:
+            raise RuntimeError("snapshot did not complete")
+        out, _ = queue.finish(ticket)
+        probe += float(out[0, 0]) + float(out[14, -1])  # the host reads the result
+        queue.release(ticket)
+
+    torch.cuda.synchronize()
     e0.record()
-    for _ in range(e2e_steps):
-        ctx.step_host(host_in, host_out, tp, opt)
+    prev = None
+    for k in range(e2e_steps):
+        ctx.upload(host_in)
+        code, diag = ctx.step(tp, opt)
+        if code != fb.OK:
+            raise RuntimeError(f"pressure did not converge: {diag.as_dict()}")
+        ticket = queue.begin(k + 1, k + 1, (k + 1) * scenes.DT)
+        if prev is not None:
+            take(prev)
+        prev = ticket
+    take(prev)
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    e2e_ms = max_over_ranks(e2e_ms, world)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, world)
+    queue.close()
+    # the same through the synchronous host step (fl_step_host: H2D, step, D2H in turn)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s0.record()
+    for _ in range(e2e_steps):
+        ctx.step_host(host_in, host_out, tp, opt)
+    s1.record()
+    torch.cuda.synchronize()
+    e2e_sync_ms = max_over_ranks(s0.elapsed_time(s1) / e2e_steps, world)
     peak, peak_kind = _peaks()
     p2g_ms = phases[1] / args.steps
     p2g_bytes = 60.0 * npart + 24.0 * ncell
@@ -264,7 +296,11 @@ def run_ours(args, world, rank, local):
                                                                                       args.warmup + args.steps],
                        parallelism=f"replicas{world}"),
         "e2e": {"value": round(world * 1e3 / e2e_ms, 4), "unit": UNIT, "h2d_bytes_per_step": int(60 * npart),
-                "d2h_bytes_per_step": int(60 * npart)},
+                "d2h_bytes_per_step": int(60 * npart + 64), "steps": e2e_steps,
+                "path": "fl_upload_particles -> fl_step -> fl_snapshot_begin/wait/finish (D2H overlaps next H2D)"},
+        "e2e_sync": {"value": round(world * 1e3 / e2e_sync_ms, 4), "unit": UNIT,
+                     "h2d_bytes_per_step": int(60 * npart), "d2h_bytes_per_step": int(60 * npart),
+                     "path": "fl_step_host (H2D, step, D2H in turn)"},
         "roofline": {"kernel": "p2g (k_p2g_tile + k_p2g_merge)", "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "algorithmic_bytes": int(p2g_bytes), "traffic": _traffic_per_launch(npart, ncell)},

@@ -32,8 +32,10 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_lib" / "libfluidity_b200.so"
 
 OK, INVALID_ARGUMENT, RESOURCE_EXHAUSTED, FAILED_PRECONDITION, ABORTED, OUT_OF_RANGE, INTERNAL = 0, 3, 8, 9, 10, 11, 13
-STATUS_NAMES = {0: "OK", 3: "INVALID_ARGUMENT", 8: "RESOURCE_EXHAUSTED", 9: "FAILED_PRECONDITION", 10: "ABORTED",
-                11: "OUT_OF_RANGE", 13: "INTERNAL"}
+ALREADY_EXISTS, UNAVAILABLE, DATA_LOSS = 6, 14, 15
+STATUS_NAMES = {0: "OK", 3: "INVALID_ARGUMENT", 6: "ALREADY_EXISTS", 8: "RESOURCE_EXHAUSTED", 9: "FAILED_PRECONDITION",
+                10: "ABORTED", 11: "OUT_OF_RANGE", 13: "INTERNAL", 14: "UNAVAILABLE", 15: "DATA_LOSS"}
+SNAPSHOT_PENDING, SNAPSHOT_READY, SNAPSHOT_CANCELED = 0, 1, 2
 
 
 class FluidityError(RuntimeError):
@@ -103,6 +105,18 @@ EXPORTS = [
     "fl_apply_learned",
 ]
 
+class Epoch(ctypes.Structure):
+    _fields_ = [("generation", ctypes.c_uint64), ("frame_ordinal", ctypes.c_uint64), ("time", ctypes.c_double)]
+
+
+class SnapshotTicket(ctypes.Structure):
+    _fields_ = [("slot", ctypes.c_uint32), ("reservation", ctypes.c_uint64), ("epoch", Epoch)]
+
+
+class SnapshotView(ctypes.Structure):
+    _fields_ = [("soa", ctypes.c_void_p), ("count", ctypes.c_uint64), ("epoch", Epoch), ("copy_ms", ctypes.c_float)]
+
+
 _lib = None
 
 
@@ -165,6 +179,16 @@ def library():
                                                   ctypes.POINTER(ctypes.c_uint64)]
         lib.fl_set_learned_preconditioner.argtypes = [vp, vp, vp]
         lib.fl_apply_learned.argtypes = [vp, vp, vp, ctypes.c_int, vp]
+        tk, ip = ctypes.POINTER(SnapshotTicket), ctypes.POINTER(ctypes.c_int)
+        lib.fl_snapshot_queue_create.argtypes = [vp, ctypes.POINTER(vp)]
+        lib.fl_snapshot_queue_destroy.argtypes = [vp]
+        lib.fl_snapshot_begin.argtypes = [vp, ctypes.POINTER(Epoch), vp, tk]
+        lib.fl_snapshot_poll.argtypes = [vp, tk, ip]
+        lib.fl_snapshot_wait.argtypes = [vp, tk, ip]
+        lib.fl_snapshot_finish.argtypes = [vp, tk, ctypes.POINTER(SnapshotView)]
+        lib.fl_snapshot_release.argtypes = [vp, tk]
+        lib.fl_snapshot_cancel.argtypes = [vp, tk]
+        lib.fl_snapshot_last_valid.argtypes = [vp, ctypes.POINTER(SnapshotView)]
         _lib = lib
     return _lib
 
@@ -286,7 +310,7 @@ class LiquidContext:
 
     def close(self):
         if self._ctx:
-            library().fl_context_destroy(self._ctx)
+            _check(library().fl_context_destroy(self._ctx), "fl_context_destroy (close its snapshot queues first)")
             self._ctx = ctypes.c_void_p()
 
     def __del__(self):
@@ -393,6 +417,79 @@ class LiquidContext:
         order); kernels 0 = tensor-core inference, 1 = FP32 training forward."""
         _check(library().fl_apply_learned(self._ctx, r.data_ptr(), z.data_ptr(), int(kernels), stream),
                "fl_apply_learned")
+
+
+class SnapshotQueue:
+    """Asynchronous device-to-host snapshots of a context's particle state
+    (fl_snapshot_* in the C-ABI; the reference's CudaLiquidSnapshotQueue3D,
+    native/include/fluidity/host/cuda_liquid_snapshot_3d.h:56-110).
+
+    ``begin`` queues the check and the copy of the state after the work queued
+    on ``stream`` and returns a ticket; ``poll``/``wait`` report progress;
+    ``finish`` validates the copy and returns a (15, count) float32 array that
+    views the pinned slot memory until ``release``. The last finished snapshot
+    stays readable through ``last_valid`` until the next finish. Error statuses
+    raise FluidityError with the C-ABI code (UNAVAILABLE: both slots held)."""
+
+    def __init__(self, ctx: LiquidContext):
+        self._q = ctypes.c_void_p()
+        self._ctx = ctx  # the context must outlive the queue
+        _check(library().fl_snapshot_queue_create(ctx.handle, ctypes.byref(self._q)), "fl_snapshot_queue_create")
+
+    def close(self):
+        if self._q:
+            library().fl_snapshot_queue_destroy(self._q)
+            self._q = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def begin(self, generation: int, frame_ordinal: int = 0, time: float = 0.0, stream=None) -> SnapshotTicket:
+        t = SnapshotTicket()
+        e = Epoch(generation, frame_ordinal, time)
+        _check(library().fl_snapshot_begin(self._q, ctypes.byref(e), stream, ctypes.byref(t)), "fl_snapshot_begin")
+        return t
+
+    def poll(self, ticket: SnapshotTicket) -> int:
+        p = ctypes.c_int()
+        _check(library().fl_snapshot_poll(self._q, ctypes.byref(ticket), ctypes.byref(p)), "fl_snapshot_poll")
+        return p.value
+
+    def wait(self, ticket: SnapshotTicket) -> int:
+        p = ctypes.c_int()
+        _check(library().fl_snapshot_wait(self._q, ctypes.byref(ticket), ctypes.byref(p)), "fl_snapshot_wait")
+        return p.value
+
+    @staticmethod
+    def _array(v: SnapshotView) -> np.ndarray:
+        if v.count == 0:
+            return np.zeros((15, 0), np.float32)
+        buf = (ctypes.c_float * (15 * v.count)).from_address(v.soa)
+        return np.ctypeslib.as_array(buf).reshape(15, v.count)
+
+    def finish(self, ticket: SnapshotTicket):
+        """(state view (15, count), SnapshotView) of a READY ticket."""
+        v = SnapshotView()
+        _check(library().fl_snapshot_finish(self._q, ctypes.byref(ticket), ctypes.byref(v)), "fl_snapshot_finish")
+        return self._array(v), v
+
+    def release(self, ticket: SnapshotTicket):
+        _check(library().fl_snapshot_release(self._q, ctypes.byref(ticket)), "fl_snapshot_release")
+
+    def cancel(self, ticket: SnapshotTicket):
+        _check(library().fl_snapshot_cancel(self._q, ctypes.byref(ticket)), "fl_snapshot_cancel")
+
+    def last_valid(self):
+        """(state view, SnapshotView) of the last finished snapshot, or None before the first."""
+        v = SnapshotView()
+        code = library().fl_snapshot_last_valid(self._q, ctypes.byref(v))
+        if code == FAILED_PRECONDITION:
+            return None
+        _check(code, "fl_snapshot_last_valid")
+        return self._array(v), v
 
 
 class UNet:

@@ -19,7 +19,7 @@ SRC = HERE / "csrc"
 OUT = HERE / "_lib"
 LIB = OUT / "libfluidity_b200.so"
 SOURCES = ["fl_grid.cu", "fl_p2g.cu", "fl_g2p.cu", "fl_pressure.cu", "fl_quanta.cu", "fl_context.cu", "fl_noalloc.cu",
-           "fl_unet.cu", "fl_unet_tc.cu"]
+           "fl_unet.cu", "fl_unet_tc.cu", "fl_snapshot.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

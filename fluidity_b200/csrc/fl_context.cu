@@ -60,6 +60,10 @@ struct fl_context {
   // particles (ping-pong, 16 arrays each incl. mass)
   float* pbuf[2] = {nullptr, nullptr};
   int cur = 0;
+  // fence[b]: recorded by a snapshot queue after its copy of buffer b; every
+  // write into buffer b waits on it (a never-recorded event is complete)
+  cudaEvent_t fence[2] = {nullptr, nullptr};
+  int snapshot_queues = 0;  // live fl_snapshot_queue objects over this context
   uint64_t count = 0;
   // faces
   float* u_pred[3] = {};
@@ -197,6 +201,11 @@ fl_particles state_particles(fl_context* c, int which) {
   p.mass = nullptr;
   p.count = c->count;
   return p;
+}
+
+// Orders `s` after every snapshot copy of either particle buffer.
+void wait_state_fences(fl_context* c, cudaStream_t s) {
+  for (int b = 0; b < 2; ++b) cudaStreamWaitEvent(s, c->fence[b], 0);
 }
 
 int read_report(fl_context* c, cudaStream_t s, fl_report* out) {
@@ -795,6 +804,7 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
   int st = device_ready();
   if (st != FL_OK) return st;
   fl_context* c = new fl_context();
+  cudaGetDevice(&c->device);
   c->desc = *grid;
   c->pcap = std::max<uint64_t>(particle_capacity, 1);
   c->lattice = (int)lattice;
@@ -835,6 +845,8 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
   if (cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking) != cudaSuccess) chk(FL_INTERNAL);
   if (cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming) != cudaSuccess) chk(FL_INTERNAL);
   if (cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess) chk(FL_INTERNAL);
+  for (int b = 0; b < 2; ++b)
+    if (cudaEventCreateWithFlags(&c->fence[b], cudaEventDisableTiming) != cudaSuccess) chk(FL_INTERNAL);
   configure_pressure_kernels();
   for (int k = 0; k < 2; ++k) {
     chk(dalloc(&c->r[k], cells));
@@ -893,6 +905,7 @@ int fl_context_create(const fl_grid_desc* grid, uint64_t particle_capacity, fl_c
 
 int fl_context_destroy(fl_context* c) {
   if (!c) return FL_OK;
+  if (c->snapshot_queues > 0) return FL_FAILED_PRECONDITION;  // destroy its snapshot queues first
   cudaFree(c->occ);
   cudaFree(c->flag);
   cudaFree(c->ordinal);
@@ -932,6 +945,8 @@ int fl_context_destroy(fl_context* c) {
   if (c->cap) cudaStreamDestroy(c->cap);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
+  for (int b = 0; b < 2; ++b)
+    if (c->fence[b]) cudaEventDestroy(c->fence[b]);
   for (int k = 0; k < 2; ++k) {
     cudaFree(c->r[k]);
     cudaFree(c->d[k]);
@@ -1037,6 +1052,7 @@ int fl_sort_particles_by_block(fl_context* c, const fl_particles* in, fl_particl
   if (!c || !in || !out) return FL_INVALID_ARGUMENT;
   if (in->count > c->pcap) return FL_RESOURCE_EXHAUSTED;
   if ((in->mass == nullptr) != (out->mass == nullptr)) return FL_INVALID_ARGUMENT;
+  wait_state_fences(c, (cudaStream_t)stream);  // `out` may be a context buffer under a snapshot copy
   return sort_impl(c, in, out, true, (cudaStream_t)stream, report);
 }
 
@@ -1089,7 +1105,10 @@ int fl_apply_vcycle(fl_context* c, const float* r, float* z, const fl_pressure_o
 int fl_g2p(fl_context* c, fl_particles* sorted, const float* const u_new[3], const float* const u_old[3], float dt,
            float* full_out, void* stream, fl_report* report) {
   if (!c || !sorted || !u_new) return FL_INVALID_ARGUMENT;
-  if (!full_out) c->occ_ready = false;  // positions may move: the next topology marks again
+  if (!full_out) {
+    c->occ_ready = false;                       // positions may move: the next topology marks again
+    wait_state_fences(c, (cudaStream_t)stream);  // step mode writes `sorted`, possibly a context buffer
+  }
   return g2p_impl(c, sorted, u_new, u_old, dt, full_out, (cudaStream_t)stream, report, nullptr);
 }
 
@@ -1102,6 +1121,7 @@ int fl_upload_particles(fl_context* c, const float* host, uint64_t count, void* 
   c->p_keep_valid = false;
   c->p_keep_prev_valid = false;
   c->occ_ready = false;
+  FL_CUDA(cudaStreamWaitEvent(s, c->fence[0], 0));  // a snapshot copy of buffer 0 still in flight
   for (int k = 0; k < 15; ++k)
     FL_CUDA(cudaMemcpyAsync(c->pbuf[0] + (size_t)k * c->pcap, host + (size_t)k * count, sizeof(float) * count,
                             cudaMemcpyHostToDevice, s));
@@ -1174,6 +1194,8 @@ int fl_step(fl_context* c, const fl_transfer_params* tp, const fl_pressure_optio
   const int pressure_status = st;
   cudaEventRecord(c->phase[3], s);
   const float* unc[3] = {c->u_new[0], c->u_new[1], c->u_new[2]};
+  // B may still be read by a snapshot of the previous state: only the write into it waits
+  FL_CUDA(cudaStreamWaitEvent(s, c->fence[1 - c->cur], 0));
   st = g2p_impl(c, &B, unc, nullptr, (float)tp->dt, nullptr, s, nullptr, c->occ, c->index_alt, &A);
   if (st != FL_OK) return st;
   cudaEventRecord(c->phase[4], s);
@@ -1527,3 +1549,17 @@ int fl_collect_training_pairs(fl_context* c, const fl_transfer_params* tp, const
 }
 
 }  // extern "C"
+
+// Accessors for the snapshot queue (fl_snapshot.cu).
+namespace fl {
+void context_snapshot_source(fl_context* c, SnapshotSource* out) {
+  out->base = c->pbuf[c->cur];
+  out->pcap = c->pcap;
+  out->count = c->count;
+  out->buffer = c->cur;
+  out->device = c->device;
+  out->g = view(c);
+}
+cudaEvent_t context_buffer_fence(fl_context* c, int buffer) { return c->fence[buffer]; }
+void context_attach_snapshot_queue(fl_context* c, int delta) { c->snapshot_queues += delta; }
+}  // namespace fl

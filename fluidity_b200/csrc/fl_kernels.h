@@ -181,4 +181,22 @@ __device__ __forceinline__ long long parent_of(const GridView& g, const LevelDes
   return ((long long)(z >> 1) * C.dim[1] + (y >> 1)) * C.dim[0] + (x >> 1);
 }
 
+// ---- the context's particle state as seen by the snapshot queue (fl_snapshot.cu)
+struct SnapshotSource {
+  const float* base;  // 15 arrays of pcap floats: x[3], v[3], C rows [9]
+  size_t pcap;
+  unsigned long long count;
+  int buffer;  // which of the context's two particle buffers holds the state
+  int device;
+  GridView g;  // lattice (origin, inv_h, blo, bdim) for the position check
+};
+
+}  // namespace fl
+
+struct fl_context;
+namespace fl {
+void context_snapshot_source(::fl_context* c, SnapshotSource* out);
+// Event recorded after every snapshot copy of particle buffer `buffer`; writes into it wait on it.
+cudaEvent_t context_buffer_fence(::fl_context* c, int buffer);
+void context_attach_snapshot_queue(::fl_context* c, int delta);
 }  // namespace fl

@@ -42,11 +42,14 @@ extern "C" {
  * mac_pressure_3d.h:88-100, operator_runtime.h:18-40). */
 #define FL_OK 0
 #define FL_INVALID_ARGUMENT 3
+#define FL_ALREADY_EXISTS 6
 #define FL_RESOURCE_EXHAUSTED 8
 #define FL_FAILED_PRECONDITION 9
 #define FL_ABORTED 10
 #define FL_OUT_OF_RANGE 11
 #define FL_INTERNAL 13
+#define FL_UNAVAILABLE 14
+#define FL_DATA_LOSS 15
 
 typedef struct fl_context fl_context;
 
@@ -310,6 +313,78 @@ int fl_set_learned_preconditioner(fl_context* ctx, const float* params, void* st
  * tensor-core inference used inside the solver (BF16 activations, FP32
  * accumulation); 1: the FP32 training forward pass, for checking the former. */
 int fl_apply_learned(fl_context* ctx, const float* r, float* z, int kernels, void* stream);
+
+/* ---- asynchronous device-to-host snapshots of the particle state ----
+ *
+ * Replaces CudaLiquidSnapshotQueue3D (native/include/fluidity/host/
+ * cuda_liquid_snapshot_3d.h:56-110, native/cuda/liquid_snapshot_3d_host.cc:
+ * 228-380): two reservations, each with its own non-blocking stream and a pair
+ * of timing events; tickets carry a never-reused reservation number and the
+ * source epoch; a slot goes Pending -> Ready (copy complete) -> Writer
+ * (finished, held by the caller) -> Free. The copy reads the context's current
+ * particle buffer in place: every later write into that buffer (the G2P of the
+ * step after next, an upload, a permuting sort) waits for the copy, so the
+ * steps in between run beside it. A device kernel on the slot's stream checks
+ * the copied state (all 15 values finite, positions inside the block lattice)
+ * and stamps count and epoch into a control record copied behind it; finish
+ * verifies that record (FL_DATA_LOSS, after which the queue only returns
+ * FL_INTERNAL, as the reference's poisoned job). Host memory: three pinned
+ * buffers of 15 x capacity floats, reference-counted between the slots and the
+ * last valid snapshot, so finish copies nothing on the host. A queue and its
+ * context are used from one thread with the context's device current; destroy
+ * the queue before the context (fl_context_destroy returns
+ * FL_FAILED_PRECONDITION while a queue is live). */
+typedef struct fl_snapshot_queue fl_snapshot_queue;
+typedef struct {
+  uint64_t generation;    /* > 0, increasing between finished snapshots */
+  uint64_t frame_ordinal; /* completed frame */
+  double time;            /* s */
+} fl_epoch;
+typedef struct {
+  uint32_t slot;
+  uint64_t reservation;
+  fl_epoch epoch;
+} fl_snapshot_ticket;
+typedef struct {
+  const float* soa; /* host: 15 arrays of `count` floats (x[3], v[3], C rows[9]), in cell order */
+  uint64_t count;
+  fl_epoch epoch;
+  float copy_ms; /* CUDA-event interval around the check and the copy on the slot's stream */
+} fl_snapshot_view;
+#define FL_SNAPSHOT_PENDING 0
+#define FL_SNAPSHOT_READY 1
+#define FL_SNAPSHOT_CANCELED 2
+
+/* Create (CudaLiquidSnapshotQueue3D::Create): pinned buffers for the context's capacity. */
+int fl_snapshot_queue_create(fl_context* ctx, fl_snapshot_queue** out);
+/* Drains the slot streams and frees everything; views from it end. */
+int fl_snapshot_queue_destroy(fl_snapshot_queue* queue);
+/* BeginCopy: snapshot of the context's state after the work queued on `stream`.
+ * FL_INVALID_ARGUMENT: generation 0; FL_FAILED_PRECONDITION: generation not
+ * above the last finished one, or another device current; FL_ALREADY_EXISTS:
+ * the epoch's generation is live in a slot; FL_UNAVAILABLE: both slots held
+ * (poll/finish/release/cancel, then retry); FL_OUT_OF_RANGE: reservations exhausted. */
+int fl_snapshot_begin(fl_snapshot_queue* queue, const fl_epoch* epoch, void* stream, fl_snapshot_ticket* ticket);
+/* Poll: nonblocking; *progress = FL_SNAPSHOT_PENDING, _READY, or _CANCELED (once,
+ * for a canceled copy that has completed; the ticket is stale afterwards).
+ * FL_FAILED_PRECONDITION for a stale ticket or one already finished. */
+int fl_snapshot_poll(fl_snapshot_queue* queue, const fl_snapshot_ticket* ticket, int* progress);
+/* Poll that blocks until the copy has completed. */
+int fl_snapshot_wait(fl_snapshot_queue* queue, const fl_snapshot_ticket* ticket, int* progress);
+/* Finish: requires READY and an epoch not older than the last finished one
+ * (generation above, frame and time not below); validates the control record
+ * and publishes the view (held until fl_snapshot_release) as the last valid
+ * snapshot. FL_FAILED_PRECONDITION for pending/stale/out-of-order/canceled
+ * tickets, FL_DATA_LOSS for a failed check. Failures keep the last valid snapshot. */
+int fl_snapshot_finish(fl_snapshot_queue* queue, const fl_snapshot_ticket* ticket, fl_snapshot_view* out);
+/* Ends a finished snapshot's lease (LiquidSnapshotLease3D destruction); the slot becomes free. */
+int fl_snapshot_release(fl_snapshot_queue* queue, const fl_snapshot_ticket* ticket);
+/* Cancel: a READY slot is freed at once; a PENDING one is freed when poll reports
+ * FL_SNAPSHOT_CANCELED. FL_FAILED_PRECONDITION for stale or finished tickets. */
+int fl_snapshot_cancel(fl_snapshot_queue* queue, const fl_snapshot_ticket* ticket);
+/* LastValidHostSnapshot: the last finished snapshot (kept after its release, until
+ * the next finish); FL_FAILED_PRECONDITION before the first finish. */
+int fl_snapshot_last_valid(fl_snapshot_queue* queue, fl_snapshot_view* out);
 
 /* Plain device<->host copies for callers without their own CUDA runtime binding. */
 int fl_copy_to_host(void* host, const void* device, uint64_t bytes);
