@@ -164,6 +164,29 @@ def _traffic_per_launch(particles: int, cells: int):
     return None
 
 
+# Algorithmic bytes per allocated cell (active blocks x 512) of one flexible-CG
+# iteration, each array element counted once per kernel, V-cycle x and
+# coefficients in BF16 (FP32 storage: 158, the x and k accesses at 4 B):
+#   k_dots 10 (z, r, r_prev) + k_direction_tiled 15 (z, d_old, mask -> d, q)
+#   + k_update 24 (d, q, r, e -> e, r_next)                                   = 49
+#   level 0: from-zero sweep 5.5, six sweeps 6.5, prolongation sweep 6.75
+#            (mask, b, diag of the colour; x of the other colour; x written),
+#            restriction 11.9 (mask, diag, b, x; coarse b and seed)            = 63.2
+#   levels >= 1: ~106 B per coarse cell per V-cycle, 1/8 per level             = 15.5
+_PRESSURE_BYTES_PER_CELL_ITER = {1: 128.0, 0: 158.0}
+
+
+def _pressure_roofline(cells: int, iterations: float, pressure_ms: float, peak: float, precision: int):
+    """Iteration bytes over the whole projection's time (setup, FP64 residuals,
+    correction and export included in the time but not in the bytes): a lower
+    bound on the solver's achieved bandwidth."""
+    per = _PRESSURE_BYTES_PER_CELL_ITER[precision]
+    moved = per * cells * iterations
+    achieved = moved / (pressure_ms / 1e3) / 1e9
+    return {"bytes_per_cell_per_iteration": per, "cells": cells, "iterations": iterations,
+            "algorithmic_bytes": int(moved), "achieved": round(achieved, 1), "frac": round(achieved / peak, 4)}
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -308,6 +331,12 @@ def run_ours(args, world, rank, local):
                       "pressure": round(phases[2] / args.steps, 4), "g2p": round(g2p_ms, 4)},
         "g2p_roofline": {"achieved": round(g2p_bytes / (g2p_ms / 1e3) / 1e9, 1), "frac": round(
             g2p_bytes / (g2p_ms / 1e3) / 1e9 / peak, 4)},
+        "transfers_roofline": {"kernels": "P2G + G2P", "algorithmic_bytes": int(p2g_bytes + g2p_bytes),
+                               "achieved": round((p2g_bytes + g2p_bytes) / ((p2g_ms + g2p_ms) / 1e3) / 1e9, 1),
+                               "frac": round((p2g_bytes + g2p_bytes) / ((p2g_ms + g2p_ms) / 1e3) / 1e9 / peak, 4)},
+        "pressure_roofline": _pressure_roofline(ncell, float(np.mean(iters)), phases[2] / args.steps, peak,
+                                                args.precision),
+        "particles_per_s": round(value * npart, 1),
         "pressure": {"mean_iterations": float(np.mean(iters)), "max_relative_residual": float(max(residuals)),
                      "vcycle_storage": "bf16" if args.precision == 1 else "fp32", "inner_rtol": 1e-3},
         "vcycle_" + ("bf16" if alt_prec == 1 else "fp32"): {
