@@ -163,3 +163,16 @@ def test_snapshot_device_check_reports_data_loss(where):
     assert q.last_valid() is None
     q.close()
     ctx.close()
+
+
+def test_snapshot_of_an_empty_state():
+    ctx, soa, tp, opt = _setup(32)
+    ctx.upload(soa[:, :0])
+    q = fb.SnapshotQueue(ctx)
+    t = q.begin(1)
+    assert q.wait(t) == fb.SNAPSHOT_READY
+    got, view = q.finish(t)
+    assert got.shape == (15, 0) and view.count == 0
+    q.release(t)
+    q.close()
+    ctx.close()
