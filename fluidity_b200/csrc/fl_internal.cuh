@@ -166,6 +166,16 @@ __device__ __forceinline__ void st_T<__nv_bfloat16>(__nv_bfloat16* p, float v) {
   *p = __float2bfloat16_rn(v);
 }
 
+// v as stored in T and read back (the value a sweep that stores v leaves for the next one).
+template <typename T>
+__device__ __forceinline__ float round_T(float v) {
+  return static_cast<float>(static_cast<T>(v));
+}
+template <>
+__device__ __forceinline__ float round_T<__nv_bfloat16>(float v) {
+  return __bfloat162float(__float2bfloat16_rn(v));
+}
+
 // Warp + block reduction of doubles (deterministic order for a fixed launch shape).
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

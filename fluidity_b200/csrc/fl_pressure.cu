@@ -546,9 +546,14 @@ constexpr int kCorrectCpt = 4;    // k_correct_tiled: 128 threads
 constexpr int kSetupCpt = 4;      // k_setup_level0_tiled: 128 threads
 
 // Red-black sweep of one colour on level 0 (MODE 0 plain, 2 prolongation
-// fused); MODE 1 (first sweep from zero) needs no neighbour values. The cells'
-// masks, right-hand sides and diagonals are loaded with the other colour's
-// values and the halo lookups, so their latencies overlap.
+// fused); MODE 1 (first sweep from zero) needs no neighbour values. MODE 3 is
+// colour 1 of the first pre-smoothing pair with colour 0's sweep from zero
+// folded in: the colour-0 neighbour values are formed from b and diag and
+// rounded to the storage type exactly as that sweep stores them, and the
+// block's fluid colour-0 cells are written too, so the pair takes one launch
+// and gives bitwise the two sweeps' result. The cells' masks, right-hand
+// sides and diagonals are loaded with the other colour's values and the halo
+// lookups, so their latencies overlap.
 template <typename T, int MODE, int CPT>
 __global__ void __launch_bounds__(256 / CPT)
     k_smooth0_tiled(GridView g, LevelPtrs<T> lp, const float* __restrict__ b, int color, const T* __restrict__ xc,
@@ -571,17 +576,40 @@ __global__ void __launch_bounds__(256 / CPT)
   if (MODE != 1) {
     const int oc = 1 - color;
     float v[CPT];
+    if (MODE == 3) {
+      unsigned mo[CPT];
+      float bo[CPT], dgo[CPT];
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-      const int c = (oc << 8) + t + k * NT;
-      v[k] = ld(&x[blk * 512 + c]);
-      if (MODE == 2) v[k] += ld(&xc[parent1_of_nat(blk * 512 + nat_of(c))]);
+      for (int k = 0; k < CPT; ++k) {
+        const int i = blk * 512 + (oc << 8) + t + k * NT;
+        mo[k] = lp.mask[i];
+        bo[k] = b[i];
+        dgo[k] = lp.diag[i];
+      }
+      // (a halo cell that is not fluid gets a value no open face ever reads)
+      load_halo0<NT, 192, true>(g, blk, oc, sh, [&](int j) {
+        const int r = rb_id(j);
+        return round_T<T>(b[r] / lp.diag[r]);
+      });
+#pragma unroll
+      for (int k = 0; k < CPT; ++k) {
+        const float s0 = bo[k] / dgo[k];
+        v[k] = round_T<T>(s0);
+        if (mo[k] & 64u) st_T(&lp.x[blk * 512 + (oc << 8) + t + k * NT], s0);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < CPT; ++k) {
+        const int c = (oc << 8) + t + k * NT;
+        v[k] = ld(&x[blk * 512 + c]);
+        if (MODE == 2) v[k] += ld(&xc[parent1_of_nat(blk * 512 + nat_of(c))]);
+      }
+      load_halo0<NT, 192, true>(g, blk, oc, sh, [&](int j) {
+        float hv = ld(&x[rb_id(j)]);
+        if (MODE == 2) hv += ld(&xc[parent1_of_nat(j)]);
+        return hv;
+      });
     }
-    load_halo0<NT, 192, true>(g, blk, oc, sh, [&](int j) {
-      float hv = ld(&x[rb_id(j)]);
-      if (MODE == 2) hv += ld(&xc[parent1_of_nat(j)]);
-      return hv;
-    });
 #pragma unroll
     for (int k = 0; k < CPT; ++k) sh[sidx(nat_of((oc << 8) + t + k * NT))] = v[k];
     __syncthreads();
@@ -1576,7 +1604,9 @@ static void smooth(const GridView& g, const MgHierarchy<T>& H, int l, const floa
     ++g_kernel_launches;
     const T* xc = H.ptr[1].x;
     constexpr int C = kSmooth0Cpt, NT = 256 / C;
-    if (mode == 1)
+    if (mode == 3)
+      launch_dep(k_smooth0_tiled<T, 3, C>, g.nb, NT, 0, s, g, H.ptr[0], bl, color, xc, done);
+    else if (mode == 1)
       launch_dep(k_smooth0_tiled<T, 1, C>, g.nb, NT, 0, s, g, H.ptr[0], bl, color, xc, done);
     else if (mode == 2)
       launch_dep(k_smooth0_tiled<T, 2, C>, g.nb, NT, 0, s, g, H.ptr[0], bl, color, xc, done);
@@ -1634,8 +1664,9 @@ static void vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r0, 
   const int top = tail ? L - 2 : L - 1;  // levels smoothed by the per-level kernels: [0, top)
   for (int l = 0; l < top; ++l) {
     const float* bl = l == 0 ? r0 : H.b[l];
-    if (l == 0) smooth<T>(g, H, l, bl, 0, 1, done, s);  // above level 0, the restriction did this sweep
-    smooth<T>(g, H, l, bl, 1, 0, done, s);
+    // colour 0's first sweep (from zero) is folded into colour 1's kernel on
+    // level 0 and into the restriction that fills each coarser level
+    smooth<T>(g, H, l, bl, 1, l == 0 ? 3 : 0, done, s);
     for (int sw = 1; sw < opt.pre; ++sw) {
       smooth<T>(g, H, l, bl, 0, 0, done, s);
       smooth<T>(g, H, l, bl, 1, 0, done, s);
