@@ -105,6 +105,15 @@ EXPORTS = [
     "fl_apply_learned",
 ]
 
+class MacPressureDiagnostics(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_uint64), ("true_residual_l2", ctypes.c_double),
+                ("max_volume_scaled_residual", ctypes.c_double), ("max_cell_constraint_defect", ctypes.c_double),
+                ("rhs_l2", ctypes.c_double), ("gauge_count", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Epoch(ctypes.Structure):
     _fields_ = [("generation", ctypes.c_uint64), ("frame_ordinal", ctypes.c_uint64), ("time", ctypes.c_double)]
 
@@ -179,6 +188,10 @@ def library():
                                                   ctypes.POINTER(ctypes.c_uint64)]
         lib.fl_set_learned_preconditioner.argtypes = [vp, vp, vp]
         lib.fl_apply_learned.argtypes = [vp, vp, vp, ctypes.c_int, vp]
+        lib.fl_project_mac_pressure_3d.argtypes = [ctypes.c_double, ctypes.c_double, _ip, _dp, ctypes.c_uint64, _ip, _ip,
+                                                   _dp, ctypes.c_uint64, ctypes.c_int, ctypes.c_double, _dp, _dp, _dp,
+                                                   _dp, _dp, ctypes.POINTER(ctypes.c_uint64),
+                                                   ctypes.POINTER(MacPressureDiagnostics), ctypes.POINTER(Measurement)]
         tk, ip = ctypes.POINTER(SnapshotTicket), ctypes.POINTER(ctypes.c_int)
         lib.fl_snapshot_queue_create.argtypes = [vp, ctypes.POINTER(vp)]
         lib.fl_snapshot_queue_destroy.argtypes = [vp]
@@ -263,6 +276,35 @@ def deposit_mac_quanta_3d(origin, h, blocks, particles, mass_per_quantum, moment
                                               float(momentum_per_quantum), int(capacity), m.ctypes.data_as(_lp),
                                               q.ctypes.data_as(_lp), ctypes.byref(meas)), "fl_deposit_mac_quanta_3d")
     return m, q, meas
+
+
+def project_mac_pressure_3d(cells_idx, cells_val, faces_idx, faces_kind, faces_val, h, dt, rel_tol=0.0,
+                            max_iterations=256):
+    """ProjectMacPressure3D on the GPU (fl_project_mac_pressure_3d): cells (n, 3) int32 with
+    (n, 5) values, faces (m, 4) int32 with kinds (m,) and (m, 6) values, in the record
+    layout of include/fluidity_b200.h. Returns pressure, rhs, residual, defect,
+    corrected_u, gauges, diag and kernel_ms; raises FluidityError on a failed status."""
+    ci = np.ascontiguousarray(cells_idx, np.int32)
+    cv = np.ascontiguousarray(cells_val, np.float64)
+    fi = np.ascontiguousarray(faces_idx, np.int32).reshape(-1, 4)
+    fk = np.ascontiguousarray(faces_kind, np.int32).reshape(-1)
+    fv = np.ascontiguousarray(faces_val, np.float64).reshape(-1, 6)
+    nc, nf = ci.shape[0], fi.shape[0]
+    p, b, r, d = np.zeros(nc), np.zeros(nc), np.zeros(nc), np.zeros(nc)
+    u = np.zeros(max(nf, 1))
+    g = np.zeros(max(nc, 1), np.uint64)
+    diag, meas = MacPressureDiagnostics(), Measurement()
+    code = library().fl_project_mac_pressure_3d(float(h), float(dt), ci.ctypes.data_as(_ip), cv.ctypes.data_as(_dp),
+                                                nc, fi.ctypes.data_as(_ip), fk.ctypes.data_as(_ip),
+                                                fv.ctypes.data_as(_dp), nf, int(max_iterations), float(rel_tol),
+                                                p.ctypes.data_as(_dp), u.ctypes.data_as(_dp), b.ctypes.data_as(_dp),
+                                                r.ctypes.data_as(_dp), d.ctypes.data_as(_dp),
+                                                g.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                                ctypes.byref(diag), ctypes.byref(meas))
+    if code != OK:
+        raise FluidityError(code, f"fl_project_mac_pressure_3d ({diag.as_dict()})")
+    return dict(pressure=p, rhs=b, residual=r, defect=d, corrected_u=u[:nf], gauges=g[:diag.gauge_count],
+                diag=diag.as_dict(), kernel_ms=meas.kernel_ms, compiled_architecture=meas.compiled_architecture)
 
 
 def gather_mac_3d(origin, h, blocks, particles, old_u, new_u):

@@ -1,7 +1,8 @@
 """Builds the CUDA library fluidity_b200/_lib/libfluidity_b200.so for sm_100a.
 
 Every translation unit is compiled by nvcc with
-``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` and linked into one
+``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` (plus the per-file
+flags of EXTRA) and linked into one
 shared object with a C-ABI (include/fluidity_b200.h). The library is built in
 tree so it travels with the working copy; nothing is installed.
 """
@@ -19,8 +20,11 @@ SRC = HERE / "csrc"
 OUT = HERE / "_lib"
 LIB = OUT / "libfluidity_b200.so"
 SOURCES = ["fl_grid.cu", "fl_p2g.cu", "fl_g2p.cu", "fl_pressure.cu", "fl_quanta.cu", "fl_context.cu", "fl_noalloc.cu",
-           "fl_unet.cu", "fl_unet_tc.cu", "fl_snapshot.cu"]
+           "fl_unet.cu", "fl_unet_tc.cu", "fl_snapshot.cu", "fl_mac_pressure.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Per-file flags: the reference-shaped pressure operator keeps every FP64
+# product apart from the sum it enters, as the reference's arithmetic does.
+EXTRA = {"fl_mac_pressure.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -49,7 +53,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         o = objdir / (src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            cmd = [nvcc(), "-std=c++17", *ARCH, "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-c", str(s), "-o", str(o)]
+            cmd = [nvcc(), "-std=c++17", *ARCH, "-O3", "-lineinfo", *EXTRA.get(src, []), "-Xcompiler", "-fPIC", "-c",
+                   str(s), "-o", str(o)]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
             procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))

@@ -1562,4 +1562,5 @@ void context_snapshot_source(fl_context* c, SnapshotSource* out) {
 }
 cudaEvent_t context_buffer_fence(fl_context* c, int buffer) { return c->fence[buffer]; }
 void context_attach_snapshot_queue(fl_context* c, int delta) { c->snapshot_queues += delta; }
+int check_device() { return device_ready(); }
 }  // namespace fl

@@ -199,4 +199,6 @@ void context_snapshot_source(::fl_context* c, SnapshotSource* out);
 // Event recorded after every snapshot copy of particle buffer `buffer`; writes into it wait on it.
 cudaEvent_t context_buffer_fence(::fl_context* c, int buffer);
 void context_attach_snapshot_queue(::fl_context* c, int delta);
+// FL_OK when an sm_100 device is current, else FL_FAILED_PRECONDITION.
+int check_device();
 }  // namespace fl

@@ -1,0 +1,623 @@
+// Reference-shaped integrated MAC pressure projection on the GPU.
+//
+// Replaces ProjectMacPressure3D / CudaProjectMacPressure3D
+// (native/include/fluidity/host/mac_pressure_3d.h:14-102,
+// native/include/fluidity/host/cuda_mac_pressure_3d.h:19-20) for the bounded
+// owned-face systems those operators take (1-4096 pressure cells, at most
+// 24576 faces): general fluid volumes, target divergences, compliance (bulk
+// modulus), wall fluxes, apertures, mobilities, pressure-gradient distances,
+// internal pressure jumps, Dirichlet exterior pressures and sealed faces. The
+// arithmetic follows the integrated system of native/src/
+// mac_pressure_3d_arithmetic.h (FreezeCell :110-146, FreezeLinkFromIncidence
+// :174-245, AssembleIntegratedRhsInto :263-313 with compensated sums,
+// SelectGaugesInto :328-399, ApplyOriginalPressureOperatorInto :404-436,
+// CorrectFacesAndAccumulatePhysicalDefectInto :440-503), the warm start of
+// InitializeMacPressure3D (mac_pressure_3d_multigrid.cc:401-419) and the
+// evaluation and identity check of mac_pressure_workspace_3d.cc:399-461.
+//
+// B200 layout. Such a system is a few hundred KB, so one CTA of 1024 threads
+// on one SM does all of it in a single launch, in FP64: per-face
+// coefficients, then per cell the right-hand side and the diagonal summed over
+// its incident faces in increasing face order (the order of the reference's
+// face loop, so the compensated sums are the reference's sums), the gauge
+// balance of every unanchored component, Jacobi-preconditioned CG from the
+// warm start, and the evaluation (corrected face velocities, residuals,
+// physical defects, the residual/defect identity). The host does only index
+// work: face endpoints by binary search, per-cell face lists, connected
+// components and gauges. This file is compiled with -fmad=false so that no
+// product is fused into a sum, as in the reference's FP64 arithmetic.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../include/fluidity_b200.h"
+#include "fl_internal.cuh"
+#include "fl_kernels.h"
+
+namespace fl {
+namespace {
+
+constexpr int kMpThreads = 1024;
+constexpr uint64_t kMpMaxCells = 4096;   // mac_pressure_3d_arithmetic.h:19
+constexpr uint64_t kMpMaxFaces = 24576;  // mac_pressure_3d_arithmetic.h:20
+constexpr int kMpMaxIterations = 65536;
+
+enum { kLinkSealed = 0, kLinkInternal = 1, kLinkDirichlet = 2 };
+
+struct MpStatus {
+  int status;
+  int iterations;
+  int arch;
+  double true_residual_l2, max_volume_scaled_residual, max_defect, rhs_l2;
+};
+
+// Device view of one system. Per-cell face lists hold (face << 1) | side,
+// side 1 when the cell is the face's head; unanchored components list their
+// cells and their faces that do not join two cells of the same component,
+// with the sign of the face's wall flux in the component's balance.
+struct MpSystem {
+  int nc, nf, ncomp;
+  double h, dt, rel_tol;
+  int max_iterations;
+  const double* cell_values;  // nc x 5
+  const double* face_values;  // nf x 6
+  const int* face_kind;
+  const int* tail;
+  const int* head;
+  const int* cell_off;  // nc + 1
+  const int* cell_ent;
+  const int* root;       // component root (smallest ordinal) per cell
+  const unsigned char* pinned;
+  const int* comp_cell_off;  // ncomp + 1 (unanchored components only)
+  const int* comp_cells;
+  const int* comp_face_off;
+  const int* comp_faces;  // (face << 1) | (1 when the component holds the head)
+  // work and results
+  double *scale, *cond, *wall_face;                       // nf
+  double *compliance, *diagA, *rhs, *rhs_abs;             // nc
+  double *p, *r, *z, *d, *q, *residual, *defect;          // nc
+  double* corrected_u;                                    // nf
+  MpStatus* out;
+};
+
+// Neumaier-compensated sum (CompensatedSum, mac_pressure_3d_arithmetic.h:57-74).
+struct NSum {
+  double sum = 0.0, corr = 0.0;
+  __device__ void add(double t) {
+    const double next = sum + t;
+    if (fabs(sum) >= fabs(t))
+      corr += (sum - next) + t;
+    else
+      corr += (t - next) + sum;
+    sum = next;
+  }
+  __device__ double total() const { return sum + corr; }
+};
+struct Row {
+  NSum flux, absolute;
+  __device__ void add(double t) {
+    flux.add(t);
+    absolute.add(fabs(t));
+  }
+};
+
+// Sum of v over the CTA, returned to every thread (fixed order for a fixed launch).
+__device__ double cta_sum(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();  // red may still be read from the previous call
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int k = 0; k < kMpThreads / 32; ++k) s += red[k];
+  return s;
+}
+__device__ double cta_max(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int k = 0; k < kMpThreads / 32; ++k) s = fmax(s, red[k]);
+  return s;
+}
+
+// out_i = (A x)_i: compliance, then each incident face's flux in face order.
+__device__ double apply_row(const MpSystem& S, const double* x, int i) {
+  double out = S.compliance[i] * x[i];
+  for (int e = S.cell_off[i]; e < S.cell_off[i + 1]; ++e) {
+    const int f = S.cell_ent[e] >> 1;
+    const double c = S.cond[f];
+    if (c == 0.0) continue;
+    const int t = S.tail[f], hd = S.head[f];
+    const double pt = t >= 0 ? x[t] : 0.0, ph = hd >= 0 ? x[hd] : 0.0;
+    const double flux = c * (pt - ph);
+    if (S.cell_ent[e] & 1)
+      out -= flux;
+    else
+      out += flux;
+  }
+  return out;
+}
+
+__device__ double corrected_velocity(const MpSystem& S, const double* p, int f) {
+  const double* v = S.face_values + 6 * f;
+  double u = v[3];
+  if (v[0] > 0.0) {
+    const int kind = S.face_kind[f];
+    const double ext = kind == kLinkDirichlet ? v[5] : 0.0;
+    const double jump = kind == kLinkInternal ? v[5] : 0.0;
+    const int t = S.tail[f], hd = S.head[f];
+    const double pt = t >= 0 ? p[t] : ext, ph = hd >= 0 ? p[hd] : ext;
+    u += S.scale[f] * (pt - ph + jump);
+  }
+  return u;
+}
+
+__global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
+  __shared__ double red[kMpThreads / 32];
+  __shared__ int status;
+  const int t = threadIdx.x;
+  const int nc = S.nc, nf = S.nf;
+  if (t == 0) {
+    status = FL_OK;
+    S.out->arch = compiled_arch();
+  }
+  const double full_area = S.h * S.h;
+  // Face coefficients (FreezeLinkFromIncidence).
+  for (int f = t; f < nf; f += kMpThreads) {
+    const double* v = S.face_values + 6 * f;
+    double sc = 0.0, c = 0.0;
+    if (v[0] > 0.0) {
+      sc = (S.dt * v[1]) / v[2];
+      c = v[0] * sc;
+    }
+    S.scale[f] = sc;
+    S.cond[f] = c;
+    S.wall_face[f] = (full_area - v[0]) * v[4];
+  }
+  for (int i = t; i < nc; i += kMpThreads) {
+    const double* v = S.cell_values + 5 * i;
+    S.compliance[i] = v[2] == 0.0 ? 0.0 : v[0] / (v[2] * S.dt);
+  }
+  __syncthreads();
+  // Right-hand side and diagonal (AssembleIntegratedRhsInto): the cell's own
+  // terms, then its faces in increasing face order.
+  for (int i = t; i < nc; i += kMpThreads) {
+    const double* v = S.cell_values + 5 * i;
+    Row row;
+    row.add(v[0] * v[1]);
+    row.add(v[4]);
+    row.add(S.compliance[i] * v[3]);
+    double dg = S.compliance[i];
+    for (int e = S.cell_off[i]; e < S.cell_off[i + 1]; ++e) {
+      const int f = S.cell_ent[e] >> 1;
+      const bool is_head = S.cell_ent[e] & 1;
+      const double* fv = S.face_values + 6 * f;
+      const double fluid_flux = fv[0] * fv[3];
+      const double sgn = is_head ? 1.0 : -1.0;
+      row.add(sgn * fluid_flux);
+      row.add(sgn * S.wall_face[f]);
+      const int kind = S.face_kind[f];
+      if (kind == kLinkInternal)
+        row.add(sgn * (S.cond[f] * fv[5]));
+      else if (kind == kLinkDirichlet)
+        row.add(S.cond[f] * fv[5]);
+      dg += S.cond[f];
+    }
+    S.rhs[i] = row.flux.total();
+    S.rhs_abs[i] = row.absolute.total();
+    S.diagA[i] = dg;
+  }
+  // Gauge balance of each unanchored component (SelectGaugesInto): its cells'
+  // source and wall terms, then the wall flux of its faces, in order.
+  for (int k = t; k < S.ncomp; k += kMpThreads) {
+    Row bal;
+    for (int e = S.comp_cell_off[k]; e < S.comp_cell_off[k + 1]; ++e) {
+      const double* v = S.cell_values + 5 * S.comp_cells[e];
+      bal.add(v[0] * v[1]);
+      bal.add(v[4]);
+    }
+    for (int e = S.comp_face_off[k]; e < S.comp_face_off[k + 1]; ++e) {
+      const int f = S.comp_faces[e] >> 1;
+      bal.add((S.comp_faces[e] & 1) ? S.wall_face[f] : -1.0 * S.wall_face[f]);
+    }
+    if (fabs(bal.flux.total()) > 32.0 * DBL_EPSILON * bal.absolute.total()) atomicExch(&status, FL_FAILED_PRECONDITION);
+  }
+  __syncthreads();
+  if (status != FL_OK) {
+    if (t == 0) S.out->status = status;
+    return;  // (uniform: every thread read the same status after the barrier)
+  }
+  // Warm start: the previous pressure, less the pin's on unanchored components.
+  for (int i = t; i < nc; i += kMpThreads) {
+    const int rt = S.root[i];
+    const double shift = S.pinned[rt] ? S.cell_values[5 * rt + 3] : 0.0;
+    S.p[i] = S.cell_values[5 * i + 3] - shift;
+  }
+  __syncthreads();
+  double bb = 0.0;
+  for (int i = t; i < nc; i += kMpThreads) {
+    const double q = apply_row(S, S.p, i);
+    S.r[i] = S.pinned[i] ? 0.0 : S.rhs[i] - q;
+    bb += S.rhs[i] * S.rhs[i];
+  }
+  const double bnorm = sqrt(cta_sum(bb, red));
+  // ||b - Ap||_2 <= rel_tol ||b||_2, or the reference's gate 2e-6 + 2e-6 ||b||_2
+  const double limit = S.rel_tol > 0.0 ? S.rel_tol * bnorm : 2e-6 + 2e-6 * bnorm;
+  // Jacobi-preconditioned CG; the pinned rows stay at their warm start.
+  double rz_prev = 0.0;
+  int it = 0;
+  for (; it < S.max_iterations; ++it) {
+    double rr = 0.0;
+    for (int i = t; i < nc; i += kMpThreads) rr += S.r[i] * S.r[i];
+    if (sqrt(cta_sum(rr, red)) <= limit) break;
+    double rz = 0.0;
+    for (int i = t; i < nc; i += kMpThreads) {
+      const double zi = (S.pinned[i] || S.diagA[i] == 0.0) ? 0.0 : S.r[i] / S.diagA[i];
+      S.z[i] = zi;
+      rz += S.r[i] * zi;
+    }
+    rz = cta_sum(rz, red);
+    const double beta = it == 0 ? 0.0 : rz / rz_prev;
+    for (int i = t; i < nc; i += kMpThreads) S.d[i] = it == 0 ? S.z[i] : S.z[i] + beta * S.d[i];
+    __syncthreads();
+    double dq = 0.0;
+    for (int i = t; i < nc; i += kMpThreads) {
+      const double qi = S.pinned[i] ? 0.0 : apply_row(S, S.d, i);
+      S.q[i] = qi;
+      dq += S.d[i] * qi;
+    }
+    dq = cta_sum(dq, red);
+    if (!(dq > 0.0)) {
+      if (t == 0) status = FL_ABORTED;
+      break;
+    }
+    const double alpha = rz / dq;
+    for (int i = t; i < nc; i += kMpThreads) {
+      S.p[i] += alpha * S.d[i];
+      S.r[i] -= alpha * S.q[i];
+    }
+    rz_prev = rz;
+  }
+  __syncthreads();
+  // Evaluation: corrected faces, residuals b - Ap, physical defects and the
+  // identity V d + r = 0 within 64 ulp of the terms' magnitudes.
+  for (int f = t; f < nf; f += kMpThreads) {
+    const double u = corrected_velocity(S, S.p, f);
+    if (!isfinite(u)) atomicExch(&status, FL_OUT_OF_RANGE);
+    S.corrected_u[f] = u;
+  }
+  __syncthreads();
+  double l2 = 0.0, bl2 = 0.0, maxr = 0.0, maxd = 0.0;
+  for (int i = t; i < nc; i += kMpThreads) {
+    const double* v = S.cell_values + 5 * i;
+    Row op, ph;
+    op.add(S.compliance[i] * S.p[i]);
+    ph.add(-v[0] * v[1]);
+    ph.add(-v[4]);
+    if (S.compliance[i] > 0.0) ph.add(S.compliance[i] * (S.p[i] - v[3]));
+    for (int e = S.cell_off[i]; e < S.cell_off[i + 1]; ++e) {
+      const int f = S.cell_ent[e] >> 1;
+      const bool is_head = S.cell_ent[e] & 1;
+      const double c = S.cond[f];
+      if (c != 0.0) {
+        const int tl = S.tail[f], hd = S.head[f];
+        const double pt = tl >= 0 ? S.p[tl] : 0.0, phd = hd >= 0 ? S.p[hd] : 0.0;
+        const double flux = c * (pt - phd);
+        op.add(is_head ? -flux : flux);
+      }
+      const double flux = S.face_values[6 * f] * S.corrected_u[f];
+      if (is_head) {
+        ph.add(-flux);
+        ph.add(-S.wall_face[f]);
+      } else {
+        ph.add(flux);
+        ph.add(S.wall_face[f]);
+      }
+    }
+    const double r = S.rhs[i] - op.flux.total();
+    const double dd = ph.flux.total() / v[0];
+    const double ident = v[0] * dd + r;
+    const double absterms = S.rhs_abs[i] + op.absolute.total() + ph.absolute.total();
+    if (fabs(ident) > 64.0 * DBL_EPSILON * absterms) atomicExch(&status, FL_INTERNAL);
+    S.residual[i] = r;
+    S.defect[i] = dd;
+    l2 += r * r;
+    bl2 += S.rhs[i] * S.rhs[i];
+    maxr = fmax(maxr, fabs(r) / v[0]);
+    maxd = fmax(maxd, fabs(dd));
+  }
+  l2 = sqrt(cta_sum(l2, red));
+  bl2 = sqrt(cta_sum(bl2, red));
+  maxr = cta_max(maxr, red);
+  maxd = cta_max(maxd, red);
+  __syncthreads();
+  if (t == 0) {
+    int st = status;
+    if (st == FL_OK && l2 > limit * 1.000001 + 1e-300) st = FL_ABORTED;
+    S.out->status = st;
+    S.out->iterations = it;
+    S.out->true_residual_l2 = l2;
+    S.out->max_volume_scaled_residual = maxr;
+    S.out->max_defect = maxd;
+    S.out->rhs_l2 = bl2;
+  }
+}
+
+int64_t cell_key(const int32_t* c) {
+  return ((int64_t)c[2] << 42) ^ (((int64_t)c[1] & 0x1fffff) << 21) ^ ((int64_t)c[0] & 0x1fffff);
+}
+
+bool cell_less(const int32_t* a, const int32_t* b) {
+  if (a[2] != b[2]) return a[2] < b[2];
+  if (a[1] != b[1]) return a[1] < b[1];
+  return a[0] < b[0];
+}
+
+int find_cell(const int32_t* cells, int nc, int32_t x, int32_t y, int32_t z) {
+  const int32_t key[3] = {x, y, z};
+  int lo = 0, hi = nc;
+  while (lo < hi) {
+    const int mid = (lo + hi) / 2;
+    if (cell_less(cells + 3 * mid, key))
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo < nc && !cell_less(key, cells + 3 * lo)) return lo;
+  return -1;
+}
+
+int find_root(std::vector<int>& parent, int c) {
+  while (parent[c] != c) c = parent[c];
+  return c;
+}
+
+}  // namespace
+}  // namespace fl
+
+using namespace fl;
+
+extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* cell_index, const double* cell_values,
+                                          uint64_t cell_count, const int32_t* face_index, const int32_t* face_kind,
+                                          const double* face_values, uint64_t face_count, int max_iterations,
+                                          double rel_tol, double* pressure, double* corrected_u, double* rhs,
+                                          double* residual, double* defect, uint64_t* gauge_ordinals,
+                                          fl_mac_pressure_diagnostics* diagnostics, fl_measurement* measurement) {
+  if (!(h > 0.0) || !std::isfinite(h) || !(dt > 0.0) || !std::isfinite(dt) || !(rel_tol >= 0.0) ||
+      !std::isfinite(rel_tol))
+    return FL_INVALID_ARGUMENT;
+  if (cell_count == 0 || !cell_index || !cell_values || (face_count && (!face_index || !face_kind || !face_values)))
+    return FL_INVALID_ARGUMENT;
+  if (!pressure || !rhs || !residual || !defect || (face_count && !corrected_u)) return FL_INVALID_ARGUMENT;
+  if (max_iterations < 1 || max_iterations > kMpMaxIterations) return FL_INVALID_ARGUMENT;
+  if (cell_count > kMpMaxCells || face_count > kMpMaxFaces) return FL_RESOURCE_EXHAUSTED;
+  const int nc = (int)cell_count, nf = (int)face_count;
+  for (int i = 0; i < nc; ++i) {
+    if (i > 0 && !cell_less(cell_index + 3 * (i - 1), cell_index + 3 * i)) return FL_INVALID_ARGUMENT;
+    for (int k = 0; k < 5; ++k)
+      if (!std::isfinite(cell_values[5 * i + k])) return FL_INVALID_ARGUMENT;
+    if (!(cell_values[5 * i] > 0.0) || cell_values[5 * i + 2] < 0.0) return FL_INVALID_ARGUMENT;
+  }
+  // Face endpoints and the link rules (internal: two cells; Dirichlet: one
+  // cell and an open aperture; sealed: closed).
+  std::vector<int> tail(nf), head(nf);
+  for (int f = 0; f < nf; ++f) {
+    const int32_t* fi = face_index + 4 * f;
+    const double* v = face_values + 6 * f;
+    if (fi[0] < 0 || fi[0] > 2 || face_kind[f] < kLinkSealed || face_kind[f] > kLinkDirichlet) return FL_INVALID_ARGUMENT;
+    for (int k = 0; k < 6; ++k)
+      if (!std::isfinite(v[k])) return FL_INVALID_ARGUMENT;
+    int32_t tc[3] = {fi[1], fi[2], fi[3]};
+    tc[fi[0]] -= 1;
+    tail[f] = find_cell(cell_index, nc, tc[0], tc[1], tc[2]);
+    head[f] = find_cell(cell_index, nc, fi[1], fi[2], fi[3]);
+    const bool both = tail[f] >= 0 && head[f] >= 0, one = (tail[f] >= 0) != (head[f] >= 0);
+    const int kind = face_kind[f];
+    if (kind == kLinkInternal && !both) return FL_INVALID_ARGUMENT;
+    if (kind == kLinkDirichlet && (!one || v[0] == 0.0)) return FL_INVALID_ARGUMENT;
+    if (kind == kLinkSealed && v[0] != 0.0) return FL_INVALID_ARGUMENT;
+    if (v[0] > 0.0 && !(v[2] > 0.0)) return FL_INVALID_ARGUMENT;
+  }
+  int st = check_device();
+  if (st != FL_OK) return st;
+  // Per-cell face lists in increasing face order.
+  std::vector<int> cell_off(nc + 1, 0), cell_ent;
+  for (int f = 0; f < nf; ++f) {
+    if (tail[f] >= 0) ++cell_off[tail[f] + 1];
+    if (head[f] >= 0) ++cell_off[head[f] + 1];
+  }
+  for (int i = 0; i < nc; ++i) cell_off[i + 1] += cell_off[i];
+  cell_ent.resize(std::max(cell_off[nc], 1));
+  {
+    std::vector<int> fill(cell_off.begin(), cell_off.end() - 1);
+    for (int f = 0; f < nf; ++f) {
+      if (tail[f] >= 0) cell_ent[fill[tail[f]]++] = f << 1;
+      if (head[f] >= 0) cell_ent[fill[head[f]]++] = (f << 1) | 1;
+    }
+  }
+  // Components over conducting two-cell faces (union towards the smaller
+  // ordinal, so a component's root is its first cell); anchors are compliant
+  // cells and Dirichlet faces; every unanchored component pins its root.
+  std::vector<int> parent(nc);
+  for (int i = 0; i < nc; ++i) parent[i] = i;
+  for (int f = 0; f < nf; ++f) {
+    const double* v = face_values + 6 * f;
+    const double cond = v[0] > 0.0 ? v[0] * ((dt * v[1]) / v[2]) : 0.0;
+    if (cond > 0.0 && tail[f] >= 0 && head[f] >= 0) {
+      const int a = find_root(parent, tail[f]), b = find_root(parent, head[f]);
+      parent[std::max(a, b)] = std::min(a, b);
+    }
+  }
+  std::vector<int> root(nc);
+  std::vector<unsigned char> anchored(nc, 0), pinned(nc, 0);
+  for (int i = 0; i < nc; ++i) {
+    root[i] = find_root(parent, i);
+    const double* v = cell_values + 5 * i;
+    if (v[2] != 0.0 && v[0] / (v[2] * dt) > 0.0) anchored[root[i]] = 1;
+  }
+  for (int f = 0; f < nf; ++f)
+    if (face_kind[f] == kLinkDirichlet) anchored[root[tail[f] >= 0 ? tail[f] : head[f]]] = 1;
+  std::vector<int> comp_of(nc, -1), gauges;
+  for (int i = 0; i < nc; ++i)
+    if (root[i] == i && !anchored[i]) {
+      pinned[i] = 1;
+      comp_of[i] = (int)gauges.size();
+      gauges.push_back(i);
+    }
+  const int ncomp = (int)gauges.size();
+  std::vector<int> comp_cell_off(ncomp + 1, 0), comp_cells, comp_face_off(ncomp + 1, 0), comp_faces;
+  {
+    std::vector<std::vector<int>> cc(ncomp), cf(ncomp);
+    for (int i = 0; i < nc; ++i)
+      if (comp_of[root[i]] >= 0) cc[comp_of[root[i]]].push_back(i);
+    for (int f = 0; f < nf; ++f) {
+      const int tl = tail[f], hd = head[f];
+      if (tl >= 0 && hd >= 0 && root[tl] == root[hd]) continue;
+      if (tl >= 0 && comp_of[root[tl]] >= 0) cf[comp_of[root[tl]]].push_back(f << 1);
+      if (hd >= 0 && comp_of[root[hd]] >= 0) cf[comp_of[root[hd]]].push_back((f << 1) | 1);
+    }
+    for (int k = 0; k < ncomp; ++k) {
+      comp_cell_off[k + 1] = comp_cell_off[k] + (int)cc[k].size();
+      comp_face_off[k + 1] = comp_face_off[k] + (int)cf[k].size();
+      comp_cells.insert(comp_cells.end(), cc[k].begin(), cc[k].end());
+      comp_faces.insert(comp_faces.end(), cf[k].begin(), cf[k].end());
+    }
+  }
+  // One device arena: inputs, index lists, work arrays and the status.
+  const size_t nd_in = (size_t)5 * nc + (size_t)6 * nf;
+  const size_t nd_work = (size_t)3 * nf + (size_t)11 * nc + (size_t)nf;
+  const size_t ni = (size_t)3 * nf + (nc + 1) + cell_ent.size() + nc + (ncomp + 1) + comp_cells.size() + (ncomp + 1) +
+                    comp_faces.size();
+  const size_t bytes = sizeof(double) * (nd_in + nd_work) + sizeof(MpStatus) + sizeof(int) * ni + nc + 64;
+  char* arena = nullptr;
+  if (cudaMalloc(&arena, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return FL_RESOURCE_EXHAUSTED;
+  }
+  MpSystem S{};
+  S.nc = nc;
+  S.nf = nf;
+  S.ncomp = ncomp;
+  S.h = h;
+  S.dt = dt;
+  S.rel_tol = rel_tol;
+  S.max_iterations = max_iterations;
+  double* dp = reinterpret_cast<double*>(arena);
+  auto take_d = [&](size_t n) {
+    double* r = dp;
+    dp += n;
+    return r;
+  };
+  double* d_cells = take_d((size_t)5 * nc);
+  double* d_faces = take_d((size_t)6 * nf);
+  S.scale = take_d(nf);
+  S.cond = take_d(nf);
+  S.wall_face = take_d(nf);
+  S.compliance = take_d(nc);
+  S.diagA = take_d(nc);
+  S.rhs = take_d(nc);
+  S.rhs_abs = take_d(nc);
+  S.p = take_d(nc);
+  S.r = take_d(nc);
+  S.z = take_d(nc);
+  S.d = take_d(nc);
+  S.q = take_d(nc);
+  S.residual = take_d(nc);
+  S.defect = take_d(nc);
+  S.corrected_u = take_d(nf);
+  S.out = reinterpret_cast<MpStatus*>(dp);
+  int* ip = reinterpret_cast<int*>(S.out + 1);
+  std::vector<int> host_ints;
+  host_ints.reserve(ni);
+  auto put = [&](const int* src, size_t n) {
+    int* r = ip + host_ints.size();
+    host_ints.insert(host_ints.end(), src, src + n);
+    return r;
+  };
+  S.face_kind = put(face_kind, nf);
+  S.tail = put(tail.data(), nf);
+  S.head = put(head.data(), nf);
+  S.cell_off = put(cell_off.data(), nc + 1);
+  S.cell_ent = put(cell_ent.data(), cell_ent.size());
+  S.root = put(root.data(), nc);
+  S.comp_cell_off = put(comp_cell_off.data(), ncomp + 1);
+  S.comp_cells = put(comp_cells.data(), comp_cells.size());
+  S.comp_face_off = put(comp_face_off.data(), ncomp + 1);
+  S.comp_faces = put(comp_faces.data(), comp_faces.size());
+  unsigned char* d_pinned = reinterpret_cast<unsigned char*>(ip + host_ints.size());
+  S.pinned = d_pinned;
+  S.cell_values = d_cells;
+  S.face_values = d_faces;
+  cudaStream_t s = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MpStatus res{};
+  float ms = 0.0f;
+  bool ok = cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess &&
+            cudaMemcpyAsync(d_cells, cell_values, sizeof(double) * 5 * nc, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            (nf == 0 || cudaMemcpyAsync(d_faces, face_values, sizeof(double) * 6 * nf, cudaMemcpyHostToDevice, s) ==
+                            cudaSuccess) &&
+            cudaMemcpyAsync(ip, host_ints.data(), sizeof(int) * host_ints.size(), cudaMemcpyHostToDevice, s) ==
+                cudaSuccess &&
+            cudaMemcpyAsync(d_pinned, pinned.data(), nc, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaEventRecord(e0, s) == cudaSuccess;
+  if (ok) {
+    ++g_kernel_launches;
+    k_mac_pressure<<<1, kMpThreads, 0, s>>>(S);
+    ok = cudaGetLastError() == cudaSuccess && cudaEventRecord(e1, s) == cudaSuccess &&
+         cudaMemcpyAsync(&res, S.out, sizeof(MpStatus), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         cudaStreamSynchronize(s) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+  }
+  std::vector<double> hp, hr, hd, hb, hu;
+  if (ok && res.status == FL_OK) {
+    hp.resize(nc);
+    hr.resize(nc);
+    hd.resize(nc);
+    hb.resize(nc);
+    hu.resize(std::max(nf, 1));
+    ok = cudaMemcpy(hp.data(), S.p, sizeof(double) * nc, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(hr.data(), S.residual, sizeof(double) * nc, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(hd.data(), S.defect, sizeof(double) * nc, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(hb.data(), S.rhs, sizeof(double) * nc, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         (nf == 0 ||
+          cudaMemcpy(hu.data(), S.corrected_u, sizeof(double) * nf, cudaMemcpyDeviceToHost) == cudaSuccess);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(arena);
+  if (!ok) {
+    cudaGetLastError();
+    return FL_INTERNAL;
+  }
+  if (diagnostics) {
+    diagnostics->iterations = (uint64_t)res.iterations;
+    diagnostics->true_residual_l2 = res.true_residual_l2;
+    diagnostics->max_volume_scaled_residual = res.max_volume_scaled_residual;
+    diagnostics->max_cell_constraint_defect = res.max_defect;
+    diagnostics->rhs_l2 = res.rhs_l2;
+    diagnostics->gauge_count = (uint64_t)ncomp;
+  }
+  if (measurement) {
+    measurement->compiled_architecture = res.arch;
+    measurement->kernel_ms = ms;
+  }
+  if (res.status != FL_OK) return res.status;  // no projection is published
+  std::memcpy(pressure, hp.data(), sizeof(double) * nc);
+  std::memcpy(residual, hr.data(), sizeof(double) * nc);
+  std::memcpy(defect, hd.data(), sizeof(double) * nc);
+  std::memcpy(rhs, hb.data(), sizeof(double) * nc);
+  if (nf) std::memcpy(corrected_u, hu.data(), sizeof(double) * nf);
+  if (gauge_ordinals)
+    for (int k = 0; k < ncomp; ++k) gauge_ordinals[k] = (uint64_t)gauges[k];
+  return FL_OK;
+}

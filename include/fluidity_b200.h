@@ -314,6 +314,44 @@ int fl_set_learned_preconditioner(fl_context* ctx, const float* params, void* st
  * accumulation); 1: the FP32 training forward pass, for checking the former. */
 int fl_apply_learned(fl_context* ctx, const float* r, float* z, int kernels, void* stream);
 
+/* ProjectMacPressure3D / CudaProjectMacPressure3D on the GPU
+ * (native/include/fluidity/host/mac_pressure_3d.h:14-102,
+ * native/include/fluidity/host/cuda_mac_pressure_3d.h:19-20) for the bounded
+ * owned-face systems they take: 1-4096 cells in strictly increasing (z,y,x)
+ * order, at most 24576 faces. Host FP64 arrays, one record per cell / face:
+ *   cell_index  3 x int32 (x, y, z)
+ *   cell_values 5 doubles: fluid volume m^3, target divergence 1/s, bulk
+ *               modulus Pa (0 = infinite: no compliance), previous pressure Pa,
+ *               integrated inward wall flux m^3/s
+ *   face_index  4 x int32 (normal axis, x, y, z of the head cell)
+ *   face_kind   0 sealed, 1 internal, 2 Dirichlet (MacPressureFace3D::pressure_link)
+ *   face_values 6 doubles: open area m^2, inverse density m^3/kg, pressure-gradient
+ *               distance m, predicted normal velocity m/s, wall normal velocity m/s,
+ *               pressure lift Pa (the internal jump, or the Dirichlet exterior pressure)
+ * Solves in FP64 to ||b - Ap||_2 <= rel_tol ||b||_2, or the reference's gate
+ * 2e-6 + 2e-6 ||b||_2 when rel_tol == 0, within max_iterations (1-65536), and
+ * evaluates the corrected face velocities, residuals b - Ap and physical defects.
+ * Outputs (pressure, rhs, residual, defect: cell_count; corrected_u: face_count;
+ * gauge_ordinals: up to cell_count, may be NULL) are written only on FL_OK.
+ * FL_INVALID_ARGUMENT for bad data or face topology, FL_RESOURCE_EXHAUSTED above
+ * the caps, FL_FAILED_PRECONDITION for an incompatible unanchored component (or
+ * no device), FL_OUT_OF_RANGE for an unrepresentable velocity, FL_INTERNAL for a
+ * residual/defect identity mismatch, FL_ABORTED when the gate is not met. */
+typedef struct {
+  uint64_t iterations;
+  double true_residual_l2;           /* m^3/s */
+  double max_volume_scaled_residual; /* max |b - Ap| / V, 1/s */
+  double max_cell_constraint_defect; /* 1/s */
+  double rhs_l2;                     /* ||b||_2, m^3/s */
+  uint64_t gauge_count;              /* cells pinned to zero pressure */
+} fl_mac_pressure_diagnostics;
+int fl_project_mac_pressure_3d(double h, double dt, const int32_t* cell_index, const double* cell_values,
+                               uint64_t cell_count, const int32_t* face_index, const int32_t* face_kind,
+                               const double* face_values, uint64_t face_count, int max_iterations, double rel_tol,
+                               double* pressure, double* corrected_u, double* rhs, double* residual, double* defect,
+                               uint64_t* gauge_ordinals, fl_mac_pressure_diagnostics* diagnostics,
+                               fl_measurement* measurement);
+
 /* ---- asynchronous device-to-host snapshots of the particle state ----
  *
  * Replaces CudaLiquidSnapshotQueue3D (native/include/fluidity/host/

@@ -69,3 +69,23 @@ def dam_break_context(n, capacity=None):
     ctx = fb.LiquidContext(n, capacity=capacity or soa.shape[1])
     ctx.upload(soa)
     return ctx, soa, m
+
+
+def pressure_case(arr, case):
+    """One case of tests/golden/pressure_3d.json in the record layout of the oracle and the C-ABI."""
+    co, fo, go = arr["case_cell_offsets"], arr["case_face_offsets"], arr["case_gauge_offsets"]
+    cs, ce, fs, fe = co[case], co[case + 1], fo[case], fo[case + 1]
+    cells_idx = np.array(arr["cell_indices"][cs:ce], np.int32)
+    cells_val = np.stack([arr["cell_fluid_volumes"][cs:ce], arr["target_cell_divergences"][cs:ce],
+                          arr["cell_bulk_moduli"][cs:ce], arr["previous_cell_pressures"][cs:ce],
+                          np.zeros(ce - cs)], 1)
+    faces_idx = np.array(arr["face_indices"][fs:fe], np.int32)
+    faces_kind = np.array(arr["face_link_kinds"][fs:fe], np.int32)
+    faces_val = np.stack([arr["face_open_areas"][fs:fe], arr["face_inverse_densities"][fs:fe],
+                          arr["face_pressure_gradient_distances"][fs:fe], arr["predicted_face_velocities"][fs:fe],
+                          arr["wall_face_velocities"][fs:fe], arr["face_pressure_lifts"][fs:fe]], 1)
+    expect = {k: np.array(arr[k][cs:ce]) for k in ("expected_cell_pressures", "expected_integrated_rhs",
+                                                     "expected_true_residuals", "expected_cell_constraint_defects")}
+    expect["expected_corrected_face_velocities"] = np.array(arr["expected_corrected_face_velocities"][fs:fe])
+    expect["gauges"] = np.array(arr["expected_gauge_cell_ordinals"][go[case]:go[case + 1]])
+    return cells_idx, cells_val, faces_idx, faces_kind, faces_val, arr["step_durations"][case], expect

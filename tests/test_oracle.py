@@ -8,7 +8,7 @@ import pytest
 
 import oracle
 from fluidity_b200 import scenes
-from helpers import box_for, golden, soa_to_xvc
+from helpers import box_for, golden, pressure_case, soa_to_xvc
 from oracle.box_system import box_pressure_system, ref_blocks_for_box
 
 CORNER_BLOCKS = np.array([[0, -1, 0], [1, -1, 0], [0, 0, 0], [1, 0, 0], [0, -1, 1], [1, -1, 1], [0, 0, 1], [1, 0, 1]],
@@ -210,29 +210,10 @@ def test_g2p_restatement_matches_reference_gather():
     np.testing.assert_allclose(out, ref, rtol=1e-12, atol=1e-12)
 
 
-def _pressure_case(arr, case):
-    co, fo, go = arr["case_cell_offsets"], arr["case_face_offsets"], arr["case_gauge_offsets"]
-    cs, ce, fs, fe = co[case], co[case + 1], fo[case], fo[case + 1]
-    cells_idx = np.array(arr["cell_indices"][cs:ce], np.int32)
-    cells_val = np.stack([arr["cell_fluid_volumes"][cs:ce], arr["target_cell_divergences"][cs:ce],
-                          arr["cell_bulk_moduli"][cs:ce], arr["previous_cell_pressures"][cs:ce],
-                          np.zeros(ce - cs)], 1)
-    faces_idx = np.array(arr["face_indices"][fs:fe], np.int32)
-    faces_kind = np.array(arr["face_link_kinds"][fs:fe], np.int32)
-    faces_val = np.stack([arr["face_open_areas"][fs:fe], arr["face_inverse_densities"][fs:fe],
-                          arr["face_pressure_gradient_distances"][fs:fe], arr["predicted_face_velocities"][fs:fe],
-                          arr["wall_face_velocities"][fs:fe], arr["face_pressure_lifts"][fs:fe]], 1)
-    expect = {k: np.array(arr[k][cs:ce]) for k in ("expected_cell_pressures", "expected_integrated_rhs",
-                                                     "expected_true_residuals", "expected_cell_constraint_defects")}
-    expect["expected_corrected_face_velocities"] = np.array(arr["expected_corrected_face_velocities"][fs:fe])
-    expect["gauges"] = np.array(arr["expected_gauge_cell_ordinals"][go[case]:go[case + 1]])
-    return cells_idx, cells_val, faces_idx, faces_kind, faces_val, arr["step_durations"][case], expect
-
-
 @pytest.mark.parametrize("case", range(8))
 def test_pressure_restatement_matches_dense_fixture(case):
     g = golden("pressure_3d.json")
-    ci, cv, fi, fk, fv, dt, ex = _pressure_case(g["arrays"], case)
+    ci, cv, fi, fk, fv, dt, ex = pressure_case(g["arrays"], case)
     out = oracle.pressure_solve(ci, cv, fi, fk, fv, 1.0, dt, rel_tol=1e-15, max_iterations=200)
     tol = dict(rtol=2e-12, atol=2e-12)
     np.testing.assert_allclose(out["pressure"], ex["expected_cell_pressures"], **tol)
@@ -248,7 +229,7 @@ def test_pressure_restatement_matches_dense_fixture(case):
 def test_reference_build_matches_dense_fixture(case):
     """Pins the compiled reference itself (ProjectMacPressure3D) against the Python fixture."""
     g = golden("pressure_3d.json")
-    ci, cv, fi, fk, fv, dt, ex = _pressure_case(g["arrays"], case)
+    ci, cv, fi, fk, fv, dt, ex = pressure_case(g["arrays"], case)
     blocks = sorted({(x // 4, y // 4, z // 4) for (_, x, y, z) in fi} | {(x // 4, y // 4, z // 4) for x, y, z in ci})
     out = oracle.ref_project([0, 0, 0], 1.0, np.array(blocks, np.int32), dt, ci, cv, fi, fk, fv,
                              tolerance_scale=1e-12)
