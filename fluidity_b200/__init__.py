@@ -155,6 +155,7 @@ def library():
                                 ctypes.POINTER(PressureDiagnostics), vp, ctypes.POINTER(Report)]
         lib.fl_upload_particles.argtypes = [vp, _fp, ctypes.c_uint64, vp]
         lib.fl_download_particles.argtypes = [vp, _fp, vp]
+        lib.fl_stage_particles.argtypes = [vp, _fp, ctypes.c_uint64]
         lib.fl_state_particles.argtypes = [vp, ctypes.POINTER(Particles)]
         lib.fl_state_fields.argtypes = [vp, vp * 3, vp * 3, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                         ctypes.POINTER(vp)]
@@ -372,7 +373,16 @@ class LiquidContext:
         _check(library().fl_upload_particles(self._ctx, soa.ctypes.data_as(_fp), self.count, stream),
                "fl_upload_particles")
 
+    def stage(self, soa: np.ndarray):
+        """Queues soa (float32 (15, count), pinned for an asynchronous copy) as the input of
+        the next step that has none staged before it (fl_stage_particles)."""
+        if soa.dtype != np.float32 or not soa.flags.c_contiguous:
+            raise ValueError("stage needs a C-contiguous float32 (15, count) array")
+        _check(library().fl_stage_particles(self._ctx, soa.ctypes.data_as(_fp), soa.shape[1]),
+               "fl_stage_particles")
+
     def download(self, stream=None) -> np.ndarray:
+        self.count = self.particles_view().count  # a staged input may have changed it
         out = np.zeros((15, self.count), np.float32)
         _check(library().fl_download_particles(self._ctx, out.ctypes.data_as(_fp), stream), "fl_download_particles")
         return out

@@ -36,6 +36,8 @@ cudaError_t launch_deposit_quanta(const GridView& g, const double* parts, unsign
 
 using namespace fl;
 
+constexpr int kStateBuffers = 4;
+
 struct fl_context {
   int device = 0;
   fl_grid_desc desc{};
@@ -58,12 +60,21 @@ struct fl_context {
   void* temp = nullptr;
   size_t temp_bytes = 0;
   // particles (ping-pong, 16 arrays each incl. mass)
-  float* pbuf[2] = {nullptr, nullptr};
+  // Particle buffers: two at creation, four once a next input is staged.
+  float* pbuf[kStateBuffers] = {};
+  int nbuf = 2;
   int cur = 0;
   // fence[b]: recorded by a snapshot queue after its copy of buffer b; every
   // write into buffer b waits on it (a never-recorded event is complete)
-  cudaEvent_t fence[2] = {nullptr, nullptr};
+  cudaEvent_t fence[kStateBuffers] = {};
   int snapshot_queues = 0;  // live fl_snapshot_queue objects over this context
+  // Staged next inputs (fl_stage_particles), oldest first: buffer, count, and
+  // the event recorded on the staging stream after the buffer's copies.
+  int stage_buf[2] = {-1, -1};
+  uint64_t stage_count[2] = {0, 0};
+  int nstage = 0;
+  cudaEvent_t staged[kStateBuffers] = {};
+  cudaStream_t stage_stream = nullptr;
   uint64_t count = 0;
   // faces
   float* u_pred[3] = {};
@@ -203,9 +214,30 @@ fl_particles state_particles(fl_context* c, int which) {
   return p;
 }
 
-// Orders `s` after every snapshot copy of either particle buffer.
+// Orders `s` after every snapshot copy of any particle buffer.
 void wait_state_fences(fl_context* c, cudaStream_t s) {
-  for (int b = 0; b < 2; ++b) cudaStreamWaitEvent(s, c->fence[b], 0);
+  for (int b = 0; b < c->nbuf; ++b) cudaStreamWaitEvent(s, c->fence[b], 0);
+}
+
+// A particle buffer to write next: not in `exclude` (bit per buffer),
+// preferring one whose last snapshot copy has finished, so that the write
+// need not wait; otherwise the lowest candidate (its fence orders the write).
+int pick_buffer(fl_context* c, unsigned exclude) {
+  int fallback = -1;
+  for (int b = 0; b < c->nbuf; ++b) {
+    if (exclude & (1u << b)) continue;
+    const cudaError_t q = cudaEventQuery(c->fence[b]);
+    if (q == cudaSuccess) return b;
+    if (q == cudaErrorNotReady && cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();
+    if (fallback < 0) fallback = b;
+  }
+  return fallback;
+}
+
+unsigned staged_mask(const fl_context* c) {
+  unsigned m = 0;
+  for (int k = 0; k < c->nstage; ++k) m |= 1u << c->stage_buf[k];
+  return m;
 }
 
 int read_report(fl_context* c, cudaStream_t s, fl_report* out) {
@@ -920,7 +952,8 @@ int fl_context_destroy(fl_context* c) {
   cudaFree(c->counts);
   cudaFree(c->cell_start);
   cudaFree(c->temp);
-  for (int b = 0; b < 2; ++b) cudaFree(c->pbuf[b]);
+  if (c->stage_stream) cudaStreamSynchronize(c->stage_stream);
+  for (int b = 0; b < kStateBuffers; ++b) cudaFree(c->pbuf[b]);
   for (int a = 0; a < 3; ++a) {
     cudaFree(c->u_pred[a]);
     cudaFree(c->u_new[a]);
@@ -945,8 +978,11 @@ int fl_context_destroy(fl_context* c) {
   if (c->cap) cudaStreamDestroy(c->cap);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
-  for (int b = 0; b < 2; ++b)
+  for (int b = 0; b < kStateBuffers; ++b) {
     if (c->fence[b]) cudaEventDestroy(c->fence[b]);
+    if (c->staged[b]) cudaEventDestroy(c->staged[b]);
+  }
+  if (c->stage_stream) cudaStreamDestroy(c->stage_stream);
   for (int k = 0; k < 2; ++k) {
     cudaFree(c->r[k]);
     cudaFree(c->d[k]);
@@ -1116,15 +1152,44 @@ int fl_upload_particles(fl_context* c, const float* host, uint64_t count, void* 
   if (!c || (!host && count)) return FL_INVALID_ARGUMENT;
   if (count > c->pcap) return FL_RESOURCE_EXHAUSTED;
   cudaStream_t s = (cudaStream_t)stream;
-  c->cur = 0;
+  c->nstage = 0;  // the uploaded state replaces any staged input
+  const int b = pick_buffer(c, 0);
+  c->cur = b;
   c->count = count;
   c->p_keep_valid = false;
   c->p_keep_prev_valid = false;
   c->occ_ready = false;
-  FL_CUDA(cudaStreamWaitEvent(s, c->fence[0], 0));  // a snapshot copy of buffer 0 still in flight
+  FL_CUDA(cudaStreamWaitEvent(s, c->fence[b], 0));  // a snapshot copy of the buffer still in flight
+  if (c->staged[b]) FL_CUDA(cudaStreamWaitEvent(s, c->staged[b], 0));  // a dropped staging copy into it
   for (int k = 0; k < 15; ++k)
-    FL_CUDA(cudaMemcpyAsync(c->pbuf[0] + (size_t)k * c->pcap, host + (size_t)k * count, sizeof(float) * count,
+    FL_CUDA(cudaMemcpyAsync(c->pbuf[b] + (size_t)k * c->pcap, host + (size_t)k * count, sizeof(float) * count,
                             cudaMemcpyHostToDevice, s));
+  return FL_OK;
+}
+
+int fl_stage_particles(fl_context* c, const float* host, uint64_t count) {
+  if (!c || (!host && count)) return FL_INVALID_ARGUMENT;
+  if (count > c->pcap) return FL_RESOURCE_EXHAUSTED;
+  if (c->nstage == 2) return FL_UNAVAILABLE;
+  if (c->nbuf < kStateBuffers) {  // first staging: two more buffers and the staging stream
+    for (int b = c->nbuf; b < kStateBuffers; ++b) {
+      if (dalloc(&c->pbuf[b], 16 * c->pcap) != FL_OK) return FL_RESOURCE_EXHAUSTED;
+      FL_CUDA(cudaEventCreateWithFlags(&c->fence[b], cudaEventDisableTiming));
+    }
+    for (int b = 0; b < kStateBuffers; ++b) FL_CUDA(cudaEventCreateWithFlags(&c->staged[b], cudaEventDisableTiming));
+    FL_CUDA(cudaStreamCreateWithFlags(&c->stage_stream, cudaStreamNonBlocking));
+    c->nbuf = kStateBuffers;
+  }
+  const int b = pick_buffer(c, (1u << c->cur) | staged_mask(c));
+  cudaStream_t s = c->stage_stream;
+  FL_CUDA(cudaStreamWaitEvent(s, c->fence[b], 0));
+  for (int k = 0; k < 15; ++k)
+    FL_CUDA(cudaMemcpyAsync(c->pbuf[b] + (size_t)k * c->pcap, host + (size_t)k * count, sizeof(float) * count,
+                            cudaMemcpyHostToDevice, s));
+  FL_CUDA(cudaEventRecord(c->staged[b], s));
+  c->stage_buf[c->nstage] = b;
+  c->stage_count[c->nstage] = count;
+  ++c->nstage;
   return FL_OK;
 }
 
@@ -1161,7 +1226,20 @@ int fl_step(fl_context* c, const fl_transfer_params* tp, const fl_pressure_optio
             fl_pressure_diagnostics* diag, void* stream, fl_report* report) {
   if (!c || !tp || !opt) return FL_INVALID_ARGUMENT;
   cudaStream_t s = (cudaStream_t)stream;
-  fl_particles A = state_particles(c, c->cur), B = state_particles(c, 1 - c->cur);
+  if (c->nstage > 0) {  // the oldest staged input becomes the state this step advances
+    const int b = c->stage_buf[0];
+    FL_CUDA(cudaStreamWaitEvent(s, c->staged[b], 0));
+    c->cur = b;
+    c->count = c->stage_count[0];
+    c->stage_buf[0] = c->stage_buf[1];
+    c->stage_count[0] = c->stage_count[1];
+    --c->nstage;
+    c->p_keep_valid = false;
+    c->p_keep_prev_valid = false;
+    c->occ_ready = false;
+  }
+  const int out_buf = pick_buffer(c, (1u << c->cur) | staged_mask(c));
+  fl_particles A = state_particles(c, c->cur), B = state_particles(c, out_buf);
   fl_report rep{};
   c->phases_valid = false;
   cudaEventRecord(c->phase[0], s);
@@ -1195,12 +1273,13 @@ int fl_step(fl_context* c, const fl_transfer_params* tp, const fl_pressure_optio
   cudaEventRecord(c->phase[3], s);
   const float* unc[3] = {c->u_new[0], c->u_new[1], c->u_new[2]};
   // B may still be read by a snapshot of the previous state: only the write into it waits
-  FL_CUDA(cudaStreamWaitEvent(s, c->fence[1 - c->cur], 0));
+  FL_CUDA(cudaStreamWaitEvent(s, c->fence[out_buf], 0));
+  if (c->staged[out_buf]) FL_CUDA(cudaStreamWaitEvent(s, c->staged[out_buf], 0));  // a dropped staging copy
   st = g2p_impl(c, &B, unc, nullptr, (float)tp->dt, nullptr, s, nullptr, c->occ, c->index_alt, &A);
   if (st != FL_OK) return st;
   cudaEventRecord(c->phase[4], s);
   c->phases_valid = true;
-  c->cur = 1 - c->cur;
+  c->cur = out_buf;
   const int err = read_report(c, s, report);
   if (err != FL_OK) return err;
   c->occ_ready = true;

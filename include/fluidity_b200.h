@@ -201,6 +201,14 @@ int fl_kernel_launches(unsigned long long* own, unsigned long long* library);
  * through fl_state_particles' pointers between steps calls
  * fl_topology_from_particles afterwards so the record is rebuilt. */
 int fl_upload_particles(fl_context* ctx, const float* host_soa, uint64_t count, void* stream);
+/* Stages a next input: copies 15 x count FP32 SoA from host memory (pinned,
+ * for the copy to run asynchronously) on the context's own non-blocking stream
+ * into a free particle buffer and returns. The next fl_step starts from the
+ * oldest staged input instead of the current state (as if it had been
+ * uploaded), so the input of step k + 1 can be copied while step k runs. At
+ * most two inputs wait (FL_UNAVAILABLE otherwise); fl_upload_particles drops
+ * them. The first call allocates two more particle buffers. */
+int fl_stage_particles(fl_context* ctx, const float* host_soa, uint64_t count);
 int fl_download_particles(fl_context* ctx, float* host_soa, void* stream);
 int fl_state_particles(fl_context* ctx, fl_particles* out);
 /* Face buffers of the last step: u_pred[3], u_new[3] (floats), pressure (doubles), cell type (bytes). */

@@ -176,3 +176,55 @@ def test_snapshot_of_an_empty_state():
     q.release(t)
     q.close()
     ctx.close()
+
+
+def test_staged_inputs_pipeline_matches_the_synchronous_host_step():
+    """stage(k + 1) -> step(k) -> begin(k), finishing snapshot k - 1: each step
+    starts from its staged input (as if uploaded) while the next one is copied."""
+    ctx, soa, tp, opt = _setup(64, "splash")
+    host_in = np.ascontiguousarray(soa, np.float32)
+    want = np.empty_like(host_in)
+    ctx.step_host(host_in, want, tp, opt)
+    q = fb.SnapshotQueue(ctx)
+    ctx.stage(host_in)
+    prev = None
+    for gen in range(1, 6):
+        if gen < 5:
+            ctx.stage(host_in)
+        ctx.step(tp, opt)
+        t = q.begin(gen)
+        if prev is not None:
+            assert q.wait(prev) == fb.SNAPSHOT_READY
+            got, _ = q.finish(prev)
+            np.testing.assert_array_equal(got, want)
+            q.release(prev)
+        prev = t
+    assert q.wait(prev) == fb.SNAPSHOT_READY
+    got, _ = q.finish(prev)
+    np.testing.assert_array_equal(got, want)
+    q.release(prev)
+    # at most two inputs wait; an upload drops them and becomes the state
+    ctx.stage(host_in)
+    ctx.stage(host_in)
+    assert _code(ctx.stage, host_in) == fb.UNAVAILABLE
+    ctx.upload(host_in)
+    ctx.step(tp, opt)
+    np.testing.assert_array_equal(ctx.download(), want)
+    q.close()
+    ctx.close()
+
+
+def test_steps_continue_from_the_state_after_staging():
+    """With four buffers a step without a staged input advances the current
+    state exactly as the two-buffer path does."""
+    ctx, soa, tp, opt = _setup(64, "splash")
+    host_in = np.ascontiguousarray(soa, np.float32)
+    ctx.upload(host_in)
+    for _ in range(3):
+        ctx.step(tp, opt)
+    want = ctx.download()
+    ctx.stage(host_in)
+    for _ in range(3):
+        ctx.step(tp, opt)
+    np.testing.assert_array_equal(ctx.download(), want)
+    ctx.close()
