@@ -267,7 +267,7 @@ def run_ours(args, world, rank, local):
     pin_out = torch.empty_like(pin_in).pin_memory()
     host_in, host_out = pin_in.numpy(), pin_out.numpy()
     queue = fb.SnapshotQueue(ctx)
-    e2e_steps = max(2, min(args.steps, 5))
+    e2e_steps = max(2, min(args.steps, 10))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     probe = 0.0
 
