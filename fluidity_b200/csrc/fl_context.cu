@@ -3,8 +3,9 @@
 // The context is the resident device arena (the role of the reference's
 // CudaLiquidSubstepBackend3D arena, native/include/fluidity/host/
 // cuda_liquid_substep_3d.h:28-81): every buffer is allocated once, at
-// creation, for the full block lattice and the declared particle capacity, so
-// a step allocates nothing. Kernels report arithmetic failures through a
+// creation, for the full block lattice and the declared particle capacity
+// (the two extra particle buffers of staged inputs at the first
+// fl_stage_particles), so a step allocates nothing. Kernels report arithmetic failures through a
 // device report (native/cuda/transfer_3d_bridge.h:49-57) that the host reads
 // after synchronizing, and failing calls publish nothing the caller owns.
 #include <cuda_bf16.h>
