@@ -1,11 +1,12 @@
 """Runs a few liquid substeps of a seeded scene, for profiling (ncu, CUDA events).
 
     python -m fluidity_b200.profile_step --scene splash --grid 256 --steps 2 [--precision 1] [--levels 0]
-        [--warm-start 1] [--inner-rtol 1e-3]
+        [--warm-start 1] [--inner-rtol 1e-3] [--snapshot]
 
 Prints, per step, the status, FCG iterations, FP64 relative residual, the
 CUDA-event phase times (topology+sort, P2G, pressure, G2P; ms) and the running
-kernel-launch counts.
+kernel-launch counts. With --snapshot every step's state also goes through the
+asynchronous snapshot queue (device check + D2H), whose copy time is printed.
 """
 
 from __future__ import annotations
@@ -25,6 +26,7 @@ def main():
     ap.add_argument("--levels", type=int, default=0)
     ap.add_argument("--warm-start", type=int, default=1)
     ap.add_argument("--inner-rtol", type=float, default=1e-3)
+    ap.add_argument("--snapshot", action="store_true")
     args = ap.parse_args()
     soa, mass = scenes.SCENES[args.scene](args.grid)
     ctx = fb.LiquidContext(args.grid, capacity=soa.shape[1])
@@ -32,10 +34,19 @@ def main():
     tp = fb.transfer_params(scenes.DT, mass)
     opt = fb.default_pressure_options(precision=args.precision, levels=args.levels, warm_start=args.warm_start,
                                       inner_rtol=args.inner_rtol)
+    queue = fb.SnapshotQueue(ctx) if args.snapshot else None
     for s in range(args.steps):
         code, d = ctx.step(tp, opt)
         print(s, code, d.iterations, f"{d.relative_residual:.3e}", ctx.step_timings().round(4).tolist(),
               fb.kernel_launches(), flush=True)
+        if queue is not None:
+            t = queue.begin(s + 1, s + 1, (s + 1) * scenes.DT)
+            queue.wait(t)
+            _, view = queue.finish(t)
+            print("  snapshot", view.count, f"{view.copy_ms:.3f} ms", flush=True)
+            queue.release(t)
+    if queue is not None:
+        queue.close()
     ctx.close()
 
 
