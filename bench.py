@@ -279,6 +279,10 @@ def run_ours(args, world, rank, local):
         probe += float(out[0, 0]) + float(out[14, -1])  # the host reads the result
         queue.release(ticket)
 
+    # the first staging allocates the context's two extra particle buffers: done
+    # once before the timed region (the upload drops the staged input)
+    ctx.stage(host_in)
+    ctx.upload(host_in)
     torch.cuda.synchronize()
     e0.record()
     prev = None
