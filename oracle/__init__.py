@@ -40,7 +40,7 @@ _u8p = ctypes.POINTER(ctypes.c_uint8)
 
 def build(force: bool = False) -> None:
     """Compile the C restatement, and the reference operators when the FluidiTy
-    sources are present (the GPU box only uses the prebuilt files)."""
+    sources are present (a machine without those sources uses the prebuilt files)."""
     (HERE / "_lib").mkdir(exist_ok=True)
     src = HERE / "cpu" / "fl_oracle.c"
     if force or not CPU_LIB.exists() or CPU_LIB.stat().st_mtime < src.stat().st_mtime:
