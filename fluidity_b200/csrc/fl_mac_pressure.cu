@@ -235,7 +235,11 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
   }
   __syncthreads();
   if (status != FL_OK) {
-    if (t == 0) S.out->status = status;
+    if (t == 0) {
+      S.out->status = status;
+      S.out->iterations = 0;
+      S.out->true_residual_l2 = S.out->max_volume_scaled_residual = S.out->max_defect = S.out->rhs_l2 = 0.0;
+    }
     return;  // (uniform: every thread read the same status after the barrier)
   }
   // Warm start: the previous pressure, less the pin's on unanchored components.
