@@ -79,6 +79,8 @@ struct MpSystem {
   const int* comp_face_off;
   const int* comp_faces;  // (face << 1) | (1 when the component holds the head)
   // work and results
+  int* ent_other;                                         // per face entry: (other cell << 1) | side
+  double* ent_cond;                                       // per face entry: the face's conductance
   double *scale, *cond, *wall_face;                       // nf
   double *compliance, *diagA, *rhs, *rhs_abs;             // nc
   double *p, *r, *z, *d, *q, *residual, *defect;          // nc
@@ -132,19 +134,22 @@ __device__ double cta_max(double v, double* red) {
 }
 
 // out_i = (A x)_i: compliance, then each incident face's flux in face order.
+// Entries are resolved once (other endpoint, conductance), so a row needs no
+// face lookup; the flux is c (x_tail - x_head) as in the face loop, with a
+// missing endpoint at zero.
 __device__ double apply_row(const MpSystem& S, const double* x, int i) {
-  double out = S.compliance[i] * x[i];
+  const double xi = x[i];
+  double out = S.compliance[i] * xi;
   for (int e = S.cell_off[i]; e < S.cell_off[i + 1]; ++e) {
-    const int f = S.cell_ent[e] >> 1;
-    const double c = S.cond[f];
+    const double c = S.ent_cond[e];
     if (c == 0.0) continue;
-    const int t = S.tail[f], hd = S.head[f];
-    const double pt = t >= 0 ? x[t] : 0.0, ph = hd >= 0 ? x[hd] : 0.0;
-    const double flux = c * (pt - ph);
-    if (S.cell_ent[e] & 1)
-      out -= flux;
+    const int o = S.ent_other[e];
+    const int other = o >> 1;  // -1: no cell at the other end
+    const double xo = other >= 0 ? x[other] : 0.0;
+    if (o & 1)
+      out -= c * (xo - xi);  // this cell is the head
     else
-      out += flux;
+      out += c * (xi - xo);
   }
   return out;
 }
@@ -191,8 +196,15 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
   }
   __syncthreads();
   // Right-hand side and diagonal (AssembleIntegratedRhsInto): the cell's own
-  // terms, then its faces in increasing face order.
+  // terms, then its faces in increasing face order; each face entry resolved
+  // for the operator rows.
   for (int i = t; i < nc; i += kMpThreads) {
+    for (int e = S.cell_off[i]; e < S.cell_off[i + 1]; ++e) {
+      const int f = S.cell_ent[e] >> 1, side = S.cell_ent[e] & 1;
+      const int other = side ? S.tail[f] : S.head[f];
+      S.ent_other[e] = other * 2 + side;  // other = -1 gives -2 + side: >> 1 is -1, & 1 the side
+      S.ent_cond[e] = S.cond[f];
+    }
     const double* v = S.cell_values + 5 * i;
     Row row;
     row.add(v[0] * v[1]);
@@ -500,10 +512,11 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   }
   // One device arena: inputs, index lists, work arrays and the status.
   const size_t nd_in = (size_t)5 * nc + (size_t)6 * nf;
-  const size_t nd_work = (size_t)3 * nf + (size_t)11 * nc + (size_t)nf;
+  const size_t nd_work = (size_t)3 * nf + (size_t)11 * nc + (size_t)nf + cell_ent.size();
   const size_t ni = (size_t)3 * nf + (nc + 1) + cell_ent.size() + nc + (ncomp + 1) + comp_cells.size() + (ncomp + 1) +
                     comp_faces.size();
-  const size_t bytes = sizeof(double) * (nd_in + nd_work) + sizeof(MpStatus) + sizeof(int) * ni + nc + 64;
+  const size_t bytes = sizeof(double) * (nd_in + nd_work) + sizeof(MpStatus) + sizeof(int) * (ni + cell_ent.size()) +
+                       nc + 64;
   char* arena = nullptr;
   if (cudaMalloc(&arena, bytes) != cudaSuccess) {
     cudaGetLastError();
@@ -540,6 +553,7 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   S.residual = take_d(nc);
   S.defect = take_d(nc);
   S.corrected_u = take_d(nf);
+  S.ent_cond = take_d(cell_ent.size());
   S.out = reinterpret_cast<MpStatus*>(dp);
   int* ip = reinterpret_cast<int*>(S.out + 1);
   std::vector<int> host_ints;
@@ -559,7 +573,8 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   S.comp_cells = put(comp_cells.data(), comp_cells.size());
   S.comp_face_off = put(comp_face_off.data(), ncomp + 1);
   S.comp_faces = put(comp_faces.data(), comp_faces.size());
-  unsigned char* d_pinned = reinterpret_cast<unsigned char*>(ip + host_ints.size());
+  S.ent_other = ip + host_ints.size();  // written by the kernel
+  unsigned char* d_pinned = reinterpret_cast<unsigned char*>(S.ent_other + cell_ent.size());
   S.pinned = d_pinned;
   S.cell_values = d_cells;
   S.face_values = d_faces;

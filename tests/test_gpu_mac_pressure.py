@@ -116,3 +116,13 @@ def test_status_codes_and_no_publication_on_failure():
     code, outs = _call_raw(s["cells_idx"], s["cells_val"], s["faces_idx"], s["faces_kind"], s["faces_val"], box.h,
                            scenes.DT, 2, 1e-12)
     assert code == fb.ABORTED and np.all(outs[0] == 7.0) and np.all(outs[4] == 7.0)
+
+
+def test_solves_are_bitwise_reproducible():
+    box, s = _dam_break_system()
+    args = (s["cells_idx"], s["cells_val"], s["faces_idx"], s["faces_kind"], s["faces_val"], box.h, scenes.DT)
+    a = fb.project_mac_pressure_3d(*args, rel_tol=1e-12, max_iterations=4000)
+    b = fb.project_mac_pressure_3d(*args, rel_tol=1e-12, max_iterations=4000)
+    for k in ("pressure", "rhs", "residual", "defect", "corrected_u"):
+        np.testing.assert_array_equal(a[k], b[k])
+    assert a["diag"]["iterations"] == b["diag"]["iterations"] == 95  # as the FP64 oracle
