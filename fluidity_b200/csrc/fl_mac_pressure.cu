@@ -82,8 +82,8 @@ struct MpSystem {
   int* ent_other;                                         // per face entry: (other cell << 1) | side
   double* ent_cond;                                       // per face entry: the face's conductance
   double *scale, *cond, *wall_face;                       // nf
-  double *compliance, *diagA, *rhs, *rhs_abs;             // nc
-  double *p, *r, *z, *d, *q, *residual, *defect;          // nc
+  double *compliance, *rhs, *rhs_abs;                    // nc
+  double *p, *residual, *defect;                          // nc (the solver's vectors are in shared memory)
   double* corrected_u;                                    // nf
   MpStatus* out;
 };
@@ -173,6 +173,15 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
   __shared__ int status;
   const int t = threadIdx.x;
   const int nc = S.nc, nf = S.nf;
+  // The solver's vectors (at most 6 x 4096 doubles) live in shared memory;
+  // the pressure goes to global memory at the end for the host.
+  extern __shared__ double vec[];
+  double* P = vec;
+  double* D = P + nc;
+  double* R = D + nc;
+  double* Q = R + nc;
+  double* Z = Q + nc;
+  double* DG = Z + nc;
   if (t == 0) {
     status = FL_OK;
     S.out->arch = compiled_arch();
@@ -228,7 +237,7 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
     }
     S.rhs[i] = row.flux.total();
     S.rhs_abs[i] = row.absolute.total();
-    S.diagA[i] = dg;
+    DG[i] = dg;
   }
   // Gauge balance of each unanchored component (SelectGaugesInto): its cells'
   // source and wall terms, then the wall flux of its faces, in order.
@@ -258,13 +267,13 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
   for (int i = t; i < nc; i += kMpThreads) {
     const int rt = S.root[i];
     const double shift = S.pinned[rt] ? S.cell_values[5 * rt + 3] : 0.0;
-    S.p[i] = S.cell_values[5 * i + 3] - shift;
+    P[i] = S.cell_values[5 * i + 3] - shift;
   }
   __syncthreads();
   double bb = 0.0;
   for (int i = t; i < nc; i += kMpThreads) {
-    const double q = apply_row(S, S.p, i);
-    S.r[i] = S.pinned[i] ? 0.0 : S.rhs[i] - q;
+    const double q = apply_row(S, P, i);
+    R[i] = S.pinned[i] ? 0.0 : S.rhs[i] - q;
     bb += S.rhs[i] * S.rhs[i];
   }
   const double bnorm = sqrt(cta_sum(bb, red));
@@ -275,23 +284,23 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
   int it = 0;
   for (; it < S.max_iterations; ++it) {
     double rr = 0.0;
-    for (int i = t; i < nc; i += kMpThreads) rr += S.r[i] * S.r[i];
+    for (int i = t; i < nc; i += kMpThreads) rr += R[i] * R[i];
     if (sqrt(cta_sum(rr, red)) <= limit) break;
     double rz = 0.0;
     for (int i = t; i < nc; i += kMpThreads) {
-      const double zi = (S.pinned[i] || S.diagA[i] == 0.0) ? 0.0 : S.r[i] / S.diagA[i];
-      S.z[i] = zi;
-      rz += S.r[i] * zi;
+      const double zi = (S.pinned[i] || DG[i] == 0.0) ? 0.0 : R[i] / DG[i];
+      Z[i] = zi;
+      rz += R[i] * zi;
     }
     rz = cta_sum(rz, red);
     const double beta = it == 0 ? 0.0 : rz / rz_prev;
-    for (int i = t; i < nc; i += kMpThreads) S.d[i] = it == 0 ? S.z[i] : S.z[i] + beta * S.d[i];
+    for (int i = t; i < nc; i += kMpThreads) D[i] = it == 0 ? Z[i] : Z[i] + beta * D[i];
     __syncthreads();
     double dq = 0.0;
     for (int i = t; i < nc; i += kMpThreads) {
-      const double qi = S.pinned[i] ? 0.0 : apply_row(S, S.d, i);
-      S.q[i] = qi;
-      dq += S.d[i] * qi;
+      const double qi = S.pinned[i] ? 0.0 : apply_row(S, D, i);
+      Q[i] = qi;
+      dq += D[i] * qi;
     }
     dq = cta_sum(dq, red);
     if (!(dq > 0.0)) {
@@ -300,8 +309,8 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
     }
     const double alpha = rz / dq;
     for (int i = t; i < nc; i += kMpThreads) {
-      S.p[i] += alpha * S.d[i];
-      S.r[i] -= alpha * S.q[i];
+      P[i] += alpha * D[i];
+      R[i] -= alpha * Q[i];
     }
     rz_prev = rz;
   }
@@ -309,7 +318,7 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
   // Evaluation: corrected faces, residuals b - Ap, physical defects and the
   // identity V d + r = 0 within 64 ulp of the terms' magnitudes.
   for (int f = t; f < nf; f += kMpThreads) {
-    const double u = corrected_velocity(S, S.p, f);
+    const double u = corrected_velocity(S, P, f);
     if (!isfinite(u)) atomicExch(&status, FL_OUT_OF_RANGE);
     S.corrected_u[f] = u;
   }
@@ -318,17 +327,17 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
   for (int i = t; i < nc; i += kMpThreads) {
     const double* v = S.cell_values + 5 * i;
     Row op, ph;
-    op.add(S.compliance[i] * S.p[i]);
+    op.add(S.compliance[i] * P[i]);
     ph.add(-v[0] * v[1]);
     ph.add(-v[4]);
-    if (S.compliance[i] > 0.0) ph.add(S.compliance[i] * (S.p[i] - v[3]));
+    if (S.compliance[i] > 0.0) ph.add(S.compliance[i] * (P[i] - v[3]));
     for (int e = S.cell_off[i]; e < S.cell_off[i + 1]; ++e) {
       const int f = S.cell_ent[e] >> 1;
       const bool is_head = S.cell_ent[e] & 1;
       const double c = S.cond[f];
       if (c != 0.0) {
         const int tl = S.tail[f], hd = S.head[f];
-        const double pt = tl >= 0 ? S.p[tl] : 0.0, phd = hd >= 0 ? S.p[hd] : 0.0;
+        const double pt = tl >= 0 ? P[tl] : 0.0, phd = hd >= 0 ? P[hd] : 0.0;
         const double flux = c * (pt - phd);
         op.add(is_head ? -flux : flux);
       }
@@ -348,6 +357,7 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
     if (fabs(ident) > 64.0 * DBL_EPSILON * absterms) atomicExch(&status, FL_INTERNAL);
     S.residual[i] = r;
     S.defect[i] = dd;
+    S.p[i] = P[i];
     l2 += r * r;
     bl2 += S.rhs[i] * S.rhs[i];
     maxr = fmax(maxr, fabs(r) / v[0]);
@@ -512,7 +522,7 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   }
   // One device arena: inputs, index lists, work arrays and the status.
   const size_t nd_in = (size_t)5 * nc + (size_t)6 * nf;
-  const size_t nd_work = (size_t)3 * nf + (size_t)11 * nc + (size_t)nf + cell_ent.size();
+  const size_t nd_work = (size_t)3 * nf + (size_t)6 * nc + (size_t)nf + cell_ent.size();
   const size_t ni = (size_t)3 * nf + (nc + 1) + cell_ent.size() + nc + (ncomp + 1) + comp_cells.size() + (ncomp + 1) +
                     comp_faces.size();
   const size_t bytes = sizeof(double) * (nd_in + nd_work) + sizeof(MpStatus) + sizeof(int) * (ni + cell_ent.size()) +
@@ -542,14 +552,9 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   S.cond = take_d(nf);
   S.wall_face = take_d(nf);
   S.compliance = take_d(nc);
-  S.diagA = take_d(nc);
   S.rhs = take_d(nc);
   S.rhs_abs = take_d(nc);
   S.p = take_d(nc);
-  S.r = take_d(nc);
-  S.z = take_d(nc);
-  S.d = take_d(nc);
-  S.q = take_d(nc);
   S.residual = take_d(nc);
   S.defect = take_d(nc);
   S.corrected_u = take_d(nf);
@@ -591,8 +596,13 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
             cudaMemcpyAsync(d_pinned, pinned.data(), nc, cudaMemcpyHostToDevice, s) == cudaSuccess &&
             cudaEventRecord(e0, s) == cudaSuccess;
   if (ok) {
+    const size_t vec_bytes = sizeof(double) * 6 * (size_t)nc;
+    static unsigned long long configured = 0;
+    if (first_on_device(configured))
+      cudaFuncSetAttribute(k_mac_pressure, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(double) * 6 * kMpMaxCells));
     ++g_kernel_launches;
-    k_mac_pressure<<<1, kMpThreads, 0, s>>>(S);
+    k_mac_pressure<<<1, kMpThreads, vec_bytes, s>>>(S);
     ok = cudaGetLastError() == cudaSuccess && cudaEventRecord(e1, s) == cudaSuccess &&
          cudaMemcpyAsync(&res, S.out, sizeof(MpStatus), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
          cudaStreamSynchronize(s) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
