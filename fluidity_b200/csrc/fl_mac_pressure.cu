@@ -21,8 +21,10 @@
 // its incident faces in increasing face order (the order of the reference's
 // face loop, so the compensated sums are the reference's sums), the gauge
 // balance of every unanchored component, Jacobi-preconditioned CG from the
-// warm start, and the evaluation (corrected face velocities, residuals,
-// physical defects, the residual/defect identity). The host does only index
+// warm start with its six vectors in shared memory (each face entry resolved
+// once to its other cell and conductance), and the evaluation (corrected face
+// velocities, residuals, physical defects, the residual/defect identity). The
+// host does only index
 // work: face endpoints by binary search, per-cell face lists, connected
 // components and gauges. This file is compiled with -fmad=false so that no
 // product is fused into a sum, as in the reference's FP64 arithmetic.
