@@ -114,6 +114,13 @@ class MacPressureDiagnostics(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class StaticGrid(ctypes.Structure):
+    """fl_static_grid: the caller-owned block layout of fl_p2g_static_scratch."""
+    _fields_ = [("origin", ctypes.c_double * 3), ("h", ctypes.c_double), ("solid_lo", ctypes.c_int32 * 3),
+                ("solid_hi", ctypes.c_int32 * 3), ("block_coords", ctypes.c_void_p), ("neighbors", ctypes.c_void_p),
+                ("cell_start", ctypes.c_void_p), ("block_count", ctypes.c_uint64)]
+
+
 class Epoch(ctypes.Structure):
     _fields_ = [("generation", ctypes.c_uint64), ("frame_ordinal", ctypes.c_uint64), ("time", ctypes.c_double)]
 
@@ -146,6 +153,9 @@ def library():
                                                    ctypes.POINTER(Report)]
         lib.fl_p2g.argtypes = [vp, ctypes.POINTER(Particles), ctypes.POINTER(TransferParams), ctypes.c_int,
                                vp * 3, vp * 3, vp, ctypes.POINTER(Report)]
+        lib.fl_p2g_static_scratch.argtypes = [ctypes.POINTER(StaticGrid), ctypes.POINTER(Particles),
+                                              ctypes.POINTER(TransferParams), ctypes.c_int, vp * 3, vp * 3, vp,
+                                              ctypes.POINTER(Report)]
         lib.fl_pressure_project.argtypes = [vp, vp * 3, vp * 3, ctypes.POINTER(TransferParams),
                                             ctypes.POINTER(PressureOptions), ctypes.POINTER(PressureDiagnostics),
                                             vp, vp]

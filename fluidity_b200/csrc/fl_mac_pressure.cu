@@ -406,6 +406,30 @@ int find_cell(const int32_t* cells, int nc, int32_t x, int32_t y, int32_t z) {
   return -1;
 }
 
+// Owned-slot order of a face in the reference's sparse grid of 4^3 blocks
+// (SparseMacGrid3D::FaceSlot, sparse_mac_grid_3d.cc:388-409): blocks in
+// (z,y,x) order, then the normal axis, then the local (z,y,x) position; the
+// face at lattice index (i,j,k) is owned by the block of cell (i,j,k).
+struct FaceKey {
+  int32_t v[7];
+  bool operator<(const FaceKey& o) const {
+    for (int k = 0; k < 7; ++k)
+      if (v[k] != o.v[k]) return v[k] < o.v[k];
+    return false;
+  }
+  bool operator==(const FaceKey& o) const {
+    for (int k = 0; k < 7; ++k)
+      if (v[k] != o.v[k]) return false;
+    return true;
+  }
+};
+
+FaceKey face_key(int axis, int64_t x, int64_t y, int64_t z) {
+  auto fdiv = [](int64_t a) { return (int32_t)(a >= 0 ? a / 4 : -((-a + 3) / 4)); };
+  auto fmod = [](int64_t a) { return (int32_t)(((a % 4) + 4) % 4); };
+  return FaceKey{{fdiv(z), fdiv(y), fdiv(x), axis, fmod(z), fmod(y), fmod(x)}};
+}
+
 int find_root(std::vector<int>& parent, int c) {
   while (parent[c] != c) c = parent[c];
   return c;
@@ -437,8 +461,33 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
       if (!std::isfinite(cell_values[5 * i + k])) return FL_INVALID_ARGUMENT;
     if (!(cell_values[5 * i] > 0.0) || cell_values[5 * i + 2] < 0.0) return FL_INVALID_ARGUMENT;
   }
+  // The faces must be exactly the cells' incident faces (six per cell, shared
+  // faces once), unique and in the reference's owned-slot order, as
+  // PrepareMacPressureSystem3D requires (mac_pressure_3d_system.cc:223-239).
+  {
+    std::vector<FaceKey> incident;
+    incident.reserve((size_t)6 * nc);
+    for (int i = 0; i < nc; ++i) {
+      const int32_t* c = cell_index + 3 * i;
+      for (int a = 0; a < 3; ++a) {
+        int64_t hi[3] = {c[0], c[1], c[2]};
+        hi[a] += 1;
+        if (hi[a] > INT32_MAX) return FL_OUT_OF_RANGE;
+        incident.push_back(face_key(a, c[0], c[1], c[2]));
+        incident.push_back(face_key(a, hi[0], hi[1], hi[2]));
+      }
+    }
+    std::sort(incident.begin(), incident.end());
+    incident.erase(std::unique(incident.begin(), incident.end()), incident.end());
+    if (incident.size() != (size_t)nf) return FL_INVALID_ARGUMENT;
+    for (int f = 0; f < nf; ++f) {
+      const int32_t* fi = face_index + 4 * f;
+      if (fi[0] < 0 || fi[0] > 2 || !(face_key(fi[0], fi[1], fi[2], fi[3]) == incident[f])) return FL_INVALID_ARGUMENT;
+    }
+  }
   // Face endpoints and the link rules (internal: two cells; Dirichlet: one
-  // cell and an open aperture; sealed: closed).
+  // cell and an open aperture; sealed: closed; the aperture within the full
+  // face, mac_pressure_3d_arithmetic.h:182).
   std::vector<int> tail(nf), head(nf);
   for (int f = 0; f < nf; ++f) {
     const int32_t* fi = face_index + 4 * f;
@@ -446,6 +495,7 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
     if (fi[0] < 0 || fi[0] > 2 || face_kind[f] < kLinkSealed || face_kind[f] > kLinkDirichlet) return FL_INVALID_ARGUMENT;
     for (int k = 0; k < 6; ++k)
       if (!std::isfinite(v[k])) return FL_INVALID_ARGUMENT;
+    if (v[0] < 0.0 || v[0] > h * h) return FL_INVALID_ARGUMENT;
     int32_t tc[3] = {fi[1], fi[2], fi[3]};
     tc[fi[0]] -= 1;
     tail[f] = find_cell(cell_index, nc, tc[0], tc[1], tc[2]);

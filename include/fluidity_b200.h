@@ -27,6 +27,13 @@
  * reference's backend (liquid_substep_backend_3d.h:37-46). Calls are ordered
  * on the stream they are given; functions that must read a device value
  * (block counts, convergence) synchronize that stream.
+ *
+ * Device-side errors: a call that takes an fl_report* and is given one
+ * synchronizes its stream, copies the kernels' report into it and returns its
+ * error code (the reference's checked report, transfer_3d_host.cc:69-92).
+ * Given report == NULL, the call returns after queueing its kernels: it
+ * reports argument and launch errors only, and no device-side error check is
+ * made.
  */
 #ifndef FLUIDITY_B200_H_
 #define FLUIDITY_B200_H_
@@ -264,13 +271,20 @@ typedef struct {
  * allocate once started -- this runs the fl_p2g kernels without a context.
  * The caller passes layout, sorted particles and output face arrays (same
  * meaning and modes as fl_p2g); the per-block tile scratch is a file-scope
- * static device array of at most 512 active blocks (13.5 MB, held on every
- * GPU that loads the library until exit). More blocks return
- * FL_RESOURCE_EXHAUSTED. The first call on a device looks up the array's
- * device address, so make it before any stream capture. All calls on a GPU
- * share that GPU's array, which keeps the last call's contents: calls that
- * overlap on the same GPU (for example on concurrent streams) race and must
- * be serialized by the caller. */
+ * static device array of at most 512 active blocks (13.5 MB, plus 1.1 MB for
+ * a checked copy of the layout, held on every GPU that loads the library
+ * until exit). More blocks return FL_RESOURCE_EXHAUSTED. The layout is
+ * checked on the device first (neighbour ordinals below block_count, cell
+ * ranges non-decreasing inside [0, count]) and the P2G kernels read a copy
+ * forced into range, so a malformed layout cannot make them read or write
+ * out of bounds; with a report the call waits for the check and returns
+ * FL_INVALID_ARGUMENT (first bad entry in first_bad_index: cell_start
+ * index, or block_count*512+1 + neighbour index) without writing any output.
+ * Without an sm_100 device it returns FL_FAILED_PRECONDITION. The first call
+ * on a device looks up the arrays' device addresses, so make it before any
+ * stream capture. All calls on a GPU share that GPU's arrays, which keep the
+ * last call's contents: calls that overlap on the same GPU (for example on
+ * concurrent streams) race and must be serialized by the caller. */
 int fl_p2g_static_scratch(const fl_static_grid* grid, const fl_particles* sorted, const fl_transfer_params* params,
                           int mode, float* const out0[3], float* const out1[3], void* stream, fl_report* report);
 

@@ -27,7 +27,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 CPU_LIB = HERE / "_lib" / "libfl_oracle.so"
 REF_LIB = HERE / "_ref" / "libfluidity_ref.so"
-REFERENCE_ROOT = Path(os.environ.get("FLUIDITY_REFERENCE", "/root/reference"))
+# The FluidiTy sources: $FLUIDITY_REFERENCE, else a checkout beside this repository.
+REFERENCE_ROOT = Path(os.environ.get("FLUIDITY_REFERENCE", str(HERE.parent.parent / "reference")))
 
 _cpu = None
 _ref = None

@@ -47,8 +47,18 @@ def box_pressure_system(box, cell_type, u_pred, density=scenes.DENSITY):
     faces_idx = np.concatenate([f[0] for f in faces]).astype(np.int32)
     faces_kind = np.concatenate([f[1] for f in faces]).astype(np.int32)
     faces_val = np.concatenate([f[2] for f in faces])
+    order = owned_slot_order(faces_idx)
+    faces_idx, faces_kind, faces_val = faces_idx[order], faces_kind[order], faces_val[order]
     return dict(cells_idx=cells_idx, cells_val=cells_val, faces_idx=faces_idx, faces_kind=faces_kind,
                 faces_val=faces_val)
+
+
+def owned_slot_order(faces_idx):
+    """Permutation putting faces (axis, x, y, z) in the reference's owned-slot
+    order: 4^3 block (z, y, x), normal axis, local (z, y, x)
+    (SparseMacGrid3D::FaceSlot, sparse_mac_grid_3d.cc:388-409)."""
+    a, x, y, z = (faces_idx[:, k].astype(np.int64) for k in range(4))
+    return np.lexsort((x % 4, y % 4, z % 4, a, x // 4, y // 4, z // 4))
 
 
 def ref_blocks_for_box(n):

@@ -41,7 +41,8 @@ def _tolist(v):
 
 
 def main():
-    root = Path(os.environ.get("FLUIDITY_REFERENCE", "/root/reference"))
+    # the FluidiTy sources: $FLUIDITY_REFERENCE, else a checkout beside this repository
+    root = Path(os.environ.get("FLUIDITY_REFERENCE", str(HERE.parent.parent.parent / "reference")))
     sys.path.insert(0, str(root / "reference" / "src"))
     from fluidity_reference import mac_transport_3d, pressure_3d_fixtures, transfer_3d_fixtures
 

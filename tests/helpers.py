@@ -89,3 +89,26 @@ def pressure_case(arr, case):
     expect["expected_corrected_face_velocities"] = np.array(arr["expected_corrected_face_velocities"][fs:fe])
     expect["gauges"] = np.array(arr["expected_gauge_cell_ordinals"][go[case]:go[case + 1]])
     return cells_idx, cells_val, faces_idx, faces_kind, faces_val, arr["step_durations"][case], expect
+
+
+def closed_system(cells_idx, open_faces):
+    """Every incident face of the cells (shared faces once) in the reference's
+    owned-slot order: sealed with zero values, except the faces named in
+    open_faces ({(axis, x, y, z): (kind, 6 values)})."""
+    from oracle.box_system import owned_slot_order
+
+    faces = set()
+    for x, y, z in np.asarray(cells_idx).tolist():
+        for a in range(3):
+            hi = [x, y, z]
+            hi[a] += 1
+            faces.add((a, x, y, z))
+            faces.add((a, *hi))
+    fi = np.array(sorted(faces), np.int32)
+    fi = fi[owned_slot_order(fi)]
+    fk = np.zeros(len(fi), np.int32)
+    fv = np.zeros((len(fi), 6))
+    for f, key in enumerate(map(tuple, fi.tolist())):
+        if key in open_faces:
+            fk[f], fv[f] = open_faces[key][0], open_faces[key][1]
+    return fi, fk, fv

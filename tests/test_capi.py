@@ -42,3 +42,19 @@ def test_no_cpu_fallback_without_a_b200():
     with pytest.raises(fb.FluidityError) as e:
         fb.deposit_mac_3d([0, 0, 0], 1.0, [[0, 0, 0]], [[1.5] * 6 + [1.0] + [0.0] * 12])
     assert e.value.code == fb.FAILED_PRECONDITION
+    # the allocation-free P2G refuses too (its pointers are never dereferenced on the host)
+    import ctypes
+
+    grid = fb.StaticGrid()
+    grid.h, grid.block_count = 1.0, 1
+    grid.block_coords = grid.neighbors = grid.cell_start = 16
+    parts = fb.Particles()
+    for d in range(3):
+        parts.x[d] = parts.v[d] = 16
+    for d in range(9):
+        parts.c[d] = 16
+    parts.count = 1
+    outs = (ctypes.c_void_p * 3)(16, 16, 16)
+    tp = fb.transfer_params(1e-3, 1.0)
+    assert fb.library().fl_p2g_static_scratch(ctypes.byref(grid), ctypes.byref(parts), ctypes.byref(tp), 0, outs,
+                                              outs, None, None) == fb.FAILED_PRECONDITION

@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import fluidity_b200 as fb
+from helpers import closed_system
 
 
 def _on_b200():
@@ -17,12 +18,15 @@ def _on_b200():
 
 
 def _two_cells():
+    """Two unit cells joined by one open internal face; their ten other faces sealed."""
     ci = np.array([[0, 0, 0], [1, 0, 0]], np.int32)
     cv = np.array([[1.0, 0.0, 0.0, 0.0, 0.0]] * 2)
-    fi = np.array([[0, 1, 0, 0]], np.int32)
-    fk = np.array([1], np.int32)
-    fv = np.array([[1.0, 1e-3, 1.0, 0.0, 0.0, 0.0]])
+    fi, fk, fv = closed_system(ci, {(0, 1, 0, 0): (1, [1.0, 1e-3, 1.0, 0.0, 0.0, 0.0])})
     return ci, cv, fi, fk, fv
+
+
+def _internal(fi):
+    return int(np.nonzero((fi == [0, 1, 0, 0]).all(1))[0][0])
 
 
 def _code(*args, **kw):
@@ -35,12 +39,25 @@ def test_pressure_operator_rejects_malformed_systems_before_the_device():
     ci, cv, fi, fk, fv = _two_cells()
     assert _code(ci[::-1], cv, fi, fk, fv, 1.0, 0.01) == fb.INVALID_ARGUMENT  # not (z,y,x)-sorted
     assert _code(ci[[0, 0]], cv, fi, fk, fv, 1.0, 0.01) == fb.INVALID_ARGUMENT  # duplicate cell
-    assert _code(ci[:1], cv[:1], fi, fk, fv, 1.0, 0.01) == fb.INVALID_ARGUMENT  # internal face, one cell
-    assert _code(ci, cv, fi, np.array([2], np.int32), fv, 1.0, 0.01) == fb.INVALID_ARGUMENT  # Dirichlet, two cells
-    closed = fv.copy()
-    closed[0, 0] = 0.0
-    assert _code(ci, cv, fi, np.array([2], np.int32), closed, 1.0, 0.01) == fb.INVALID_ARGUMENT
-    assert _code(ci, cv, fi, np.array([0], np.int32), fv, 1.0, 0.01) == fb.INVALID_ARGUMENT  # open sealed face
+    k = _internal(fi)
+    fi1, fk1, fv1 = closed_system(ci[:1], {})
+    fk1[:] = 1
+    assert _code(ci[:1], cv[:1], fi1, fk1, fv1, 1.0, 0.01) == fb.INVALID_ARGUMENT  # internal faces, one cell
+    kind = fk.copy()
+    kind[k] = 2
+    assert _code(ci, cv, fi, kind, fv, 1.0, 0.01) == fb.INVALID_ARGUMENT  # Dirichlet, two cells
+    kind[:] = 0
+    kind[0] = 2
+    assert _code(ci, cv, fi, kind, fv, 1.0, 0.01) == fb.INVALID_ARGUMENT  # Dirichlet with a closed aperture
+    kind = fk.copy()
+    kind[k] = 0
+    assert _code(ci, cv, fi, kind, fv, 1.0, 0.01) == fb.INVALID_ARGUMENT  # open sealed face
+    wide = fv.copy()
+    wide[k, 0] = 1.0 + 1e-9
+    assert _code(ci, cv, fi, fk, wide, 1.0, 0.01) == fb.INVALID_ARGUMENT  # aperture above h^2
+    neg = fv.copy()
+    neg[(k + 1) % len(fv), 0] = -0.0 - 1e-300
+    assert _code(ci, cv, fi, fk, neg, 1.0, 0.01) == fb.INVALID_ARGUMENT  # negative aperture
     bad = cv.copy()
     bad[0, 0] = 0.0
     assert _code(ci, bad, fi, fk, fv, 1.0, 0.01) == fb.INVALID_ARGUMENT  # no fluid volume
@@ -50,6 +67,17 @@ def test_pressure_operator_rejects_malformed_systems_before_the_device():
     assert _code(ci, cv, fi, fk, fv, 1.0, 0.0) == fb.INVALID_ARGUMENT  # dt
     assert _code(ci, cv, fi, fk, fv, 1.0, 0.01, max_iterations=0) == fb.INVALID_ARGUMENT
     assert _code(ci, cv, fi, fk, fv, 1.0, 0.01, rel_tol=-1.0) == fb.INVALID_ARGUMENT
+    # the faces must be exactly the incident faces, unique, in owned-slot order
+    dup = np.concatenate([np.arange(k + 1), np.arange(k, len(fi))])
+    assert _code(ci, cv, fi[dup], fk[dup], fv[dup], 1.0, 0.01) == fb.INVALID_ARGUMENT  # duplicated face
+    miss = np.delete(np.arange(len(fi)), 0)
+    assert _code(ci, cv, fi[miss], fk[miss], fv[miss], 1.0, 0.01) == fb.INVALID_ARGUMENT  # missing face
+    swap = np.arange(len(fi))
+    swap[[0, 1]] = [1, 0]
+    assert _code(ci, cv, fi[swap], fk[swap], fv[swap], 1.0, 0.01) == fb.INVALID_ARGUMENT  # out of slot order
+    extra = np.vstack([fi, [[2, 5, 5, 5]]]).astype(np.int32)
+    assert _code(ci, cv, extra, np.append(fk, 0), np.vstack([fv, np.zeros((1, 6))]), 1.0, 0.01) == \
+        fb.INVALID_ARGUMENT  # a face of no cell
     many = np.stack(np.meshgrid(np.arange(17), np.arange(17), np.arange(15), indexing="ij"), -1).reshape(-1, 3)
     many = many[np.lexsort((many[:, 0], many[:, 1], many[:, 2]))]
     assert _code(many, np.tile(cv[0], (len(many), 1)), fi[:0], fk[:0], fv[:0], 1.0, 0.01) == fb.RESOURCE_EXHAUSTED

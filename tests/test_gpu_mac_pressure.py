@@ -16,7 +16,7 @@ import pytest
 import fluidity_b200 as fb
 import oracle
 from fluidity_b200 import scenes
-from helpers import box_for, golden, pressure_case, soa_to_xvc
+from helpers import box_for, closed_system, golden, pressure_case, soa_to_xvc
 from oracle.box_system import box_pressure_system
 
 pytestmark = pytest.mark.gpu
@@ -85,9 +85,7 @@ def _two_cells(divergence):
     """Two cells joined by one open internal face, every other face sealed."""
     ci = np.array([[0, 0, 0], [1, 0, 0]], np.int32)
     cv = np.array([[1.0, divergence, 0.0, 0.0, 0.0]] * 2)
-    fi = np.array([[0, 1, 0, 0]], np.int32)
-    fk = np.array([1], np.int32)
-    fv = np.array([[1.0, 1e-3, 1.0, 0.0, 0.0, 0.0]])
+    fi, fk, fv = closed_system(ci, {(0, 1, 0, 0): (1, [1.0, 1e-3, 1.0, 0.0, 0.0, 0.0])})
     return ci, cv, fi, fk, fv
 
 
@@ -105,6 +103,10 @@ def test_status_codes_and_no_publication_on_failure():
     assert _call_raw(ci[::-1], cv, fi, fk, fv, 1.0, 0.01, 50, 1e-12)[0] == fb.INVALID_ARGUMENT
     assert _call_raw(ci, cv, fi, fk, fv, 1.0, 0.01, 0, 1e-12)[0] == fb.INVALID_ARGUMENT
     assert _call_raw(ci[:1], cv[:1], fi, fk, fv, 1.0, 0.01, 50, 1e-12)[0] == fb.INVALID_ARGUMENT
+    # a face listed twice, one left out
+    dup = np.concatenate([[0], np.arange(len(fi))])
+    assert _call_raw(ci, cv, fi[dup], fk[dup], fv[dup], 1.0, 0.01, 50, 1e-12)[0] == fb.INVALID_ARGUMENT
+    assert _call_raw(ci, cv, fi[1:], fk[1:], fv[1:], 1.0, 0.01, 50, 1e-12)[0] == fb.INVALID_ARGUMENT
     # above the 4096-cell cap
     big = np.stack(np.meshgrid(np.arange(17), np.arange(17), np.arange(15), indexing="ij"), -1).reshape(-1, 3)
     big = big[np.lexsort((big[:, 0], big[:, 1], big[:, 2]))]

@@ -5,9 +5,11 @@ It exists for callers that cannot call cudaMalloc where they deposit (an
 engine that owns all device memory through its own pool, or a substep that
 must not allocate once started): its tile scratch is a static device array.
 The test runs it twice in a row on the same inputs -- the second call sees
-the first call's leftover scratch -- and compares both results with fl_p2g,
-in both P2G modes, within the 1e-5 relative tolerance of the parity tests.
-It lives in its own file, collected last, and needs a GPU."""
+the first call's leftover scratch -- and requires both results to equal
+fl_p2g's bit for bit, in both P2G modes (the same kernels in the same cell
+order), with the device's free memory unchanged across the second call. A
+malformed layout is refused before any output is written. It lives in its
+own file, collected last, and needs a GPU."""
 
 import ctypes
 
@@ -18,12 +20,6 @@ import fluidity_b200 as fb
 from fluidity_b200 import scenes
 
 pytestmark = pytest.mark.gpu
-
-
-class StaticGrid(ctypes.Structure):
-    _fields_ = [("origin", ctypes.c_double * 3), ("h", ctypes.c_double), ("solid_lo", ctypes.c_int32 * 3),
-                ("solid_hi", ctypes.c_int32 * 3), ("block_coords", ctypes.c_void_p), ("neighbors", ctypes.c_void_p),
-                ("cell_start", ctypes.c_void_p), ("block_count", ctypes.c_uint64)]
 
 
 def _neighbors(blocks, bdim):
@@ -55,9 +51,7 @@ def test_static_scratch_p2g_matches_context_p2g_twice():
     import torch
 
     lib = fb.library()
-    lib.fl_p2g_static_scratch.argtypes = [ctypes.POINTER(StaticGrid), ctypes.POINTER(fb.Particles),
-                                          ctypes.POINTER(fb.TransferParams), ctypes.c_int, ctypes.c_void_p * 3,
-                                          ctypes.c_void_p * 3, ctypes.c_void_p, ctypes.POINTER(fb.Report)]
+    StaticGrid = fb.StaticGrid
     n = 64
     soa, mass = scenes.dam_break(n)
     count = soa.shape[1]
@@ -83,20 +77,47 @@ def test_static_scratch_p2g_matches_context_p2g_twice():
     grid.block_coords, grid.neighbors = coords.data_ptr(), nbrs.data_ptr()
     grid.cell_start, grid.block_count = f["cell_start"], nb
     tp = fb.transfer_params(scenes.DT, mass)
+    arr = lambda ts: (ctypes.c_void_p * 3)(*[t.data_ptr() for t in ts])
     for mode in (0, 1):
         ref = [torch.zeros(nb * 512, device="cuda") for _ in range(6)]
-        arr = lambda ts: (ctypes.c_void_p * 3)(*[t.data_ptr() for t in ts])
         assert lib.fl_p2g(ctx.handle, ctypes.byref(pout), ctypes.byref(tp), mode, arr(ref[:3]), arr(ref[3:]), None,
                           ctypes.byref(rep)) == fb.OK
         for call in range(2):
             got = [torch.full((nb * 512,), float("nan"), device="cuda") for _ in range(6)]
+            torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             code = lib.fl_p2g_static_scratch(ctypes.byref(grid), ctypes.byref(pout), ctypes.byref(tp), mode,
                                              arr(got[:3]), arr(got[3:]), None, ctypes.byref(rep))
+            torch.cuda.synchronize()
+            free_after = torch.cuda.mem_get_info()[0]
             assert code == fb.OK and rep.error == 0 and rep.compiled_architecture == 1000
+            if call == 1:  # the first call on the device may load the module; later ones allocate nothing
+                assert free_after == free_before
             for a in range(6):
-                g, r = got[a].cpu().numpy(), ref[a].cpu().numpy()
-                scale = max(np.abs(r).max(), 1e-30)
-                assert np.abs(g - r).max() <= 1e-5 * scale, (mode, call, a)
+                assert torch.equal(got[a], ref[a]), (mode, call, a)
+    # a neighbour ordinal past the block count: refused, nothing written
+    bad = nbrs.clone()
+    bad[0, 13 + 1] = nb + 5
+    malformed = StaticGrid.from_buffer_copy(grid)
+    malformed.neighbors = bad.data_ptr()
+    got = [torch.full((nb * 512,), 7.0, device="cuda") for _ in range(6)]
+    code = lib.fl_p2g_static_scratch(ctypes.byref(malformed), ctypes.byref(pout), ctypes.byref(tp), 0,
+                                     arr(got[:3]), arr(got[3:]), None, ctypes.byref(rep))
+    assert code == fb.INVALID_ARGUMENT and rep.error == fb.INVALID_ARGUMENT
+    assert rep.first_bad_index == nb * 512 + 1 + 14
+    assert all(bool((t == 7.0).all()) for t in got)
+    # a particle range past the particle count: refused as well
+    host_cs = np.zeros(nb * 512 + 1, np.int32)
+    assert lib.fl_copy_to_host(host_cs.ctypes.data, ctypes.c_void_p(f["cell_start"]), host_cs.nbytes) == fb.OK
+    assert host_cs[-1] == count
+    host_cs[-1] = count + 1000
+    cs = torch.from_numpy(host_cs).cuda()
+    malformed = StaticGrid.from_buffer_copy(grid)
+    malformed.cell_start = cs.data_ptr()
+    code = lib.fl_p2g_static_scratch(ctypes.byref(malformed), ctypes.byref(pout), ctypes.byref(tp), 0,
+                                     arr(got[:3]), arr(got[3:]), None, ctypes.byref(rep))
+    assert code == fb.INVALID_ARGUMENT and rep.first_bad_index == nb * 512
+    assert all(bool((t == 7.0).all()) for t in got)
     too_many = StaticGrid.from_buffer_copy(grid)
     too_many.block_count = 513
     out = [torch.zeros(16, device="cuda") for _ in range(6)]
