@@ -61,9 +61,11 @@ def seed_particles(n: int, cells: np.ndarray, seed: int = 0, velocity=None):
     y = (j[:, None] + (sy[None, :] + uy) * 0.5) * h
     z = (k[:, None] + (sz[None, :] + uz) * 0.5) * h
     soa = np.zeros((15, 8 * m), np.float32)
-    soa[0] = x.ravel()
-    soa[1] = y.ravel()
-    soa[2] = z.ravel()
+    # Rounded to FP32 inside the particle's own cell: a jitter just below the
+    # cell's upper edge would otherwise round onto the edge, into the next cell.
+    for d, (pos, cell) in enumerate(((x, i), (y, j), (z, k))):
+        edge = np.nextafter(((cell[:, None] + 1) * h).astype(np.float32), np.float32(0.0))
+        soa[d] = np.minimum(pos.astype(np.float32), edge).ravel()
     if velocity is not None:
         vel = np.asarray(velocity, np.float64).reshape(-1, 3)
         if len(vel) == 1:

@@ -138,6 +138,9 @@ def cpu():
         lib.fo_classify_cells.argtypes = [ctypes.POINTER(Box), _dp, ctypes.c_size_t, _u8p]
         lib.fo_step.argtypes = [ctypes.POINTER(Box), ctypes.POINTER(StepParams), _dp, _dp, _dp, ctypes.c_size_t,
                                 _dp * 3, _dp * 3, _dp, _u8p, ctypes.POINTER(PressureDiag)]
+        lib.fo_step_replay.argtypes = [ctypes.POINTER(Box), ctypes.POINTER(StepParams), ctypes.POINTER(ctypes.c_float),
+                                       ctypes.c_size_t, _dp, ctypes.c_size_t, ctypes.c_size_t, _dp * 3, _dp * 3, _u8p,
+                                       ctypes.POINTER(PressureDiag), _dp]
         lib.fo_vcycle.argtypes = [ctypes.POINTER(Box), _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int, _dp, _dp]
         _cpu = lib
@@ -310,6 +313,34 @@ def step(box: Box, x, v, c, dt, density=1000.0, gravity=(0.0, -9.81, 0.0), m_min
                          (_dp * 3)(*[_d(a) for a in u_pred]), (_dp * 3)(*[_d(a) for a in u_new]), _d(cp), _u8(ct),
                          ctypes.byref(diag)), "step")
     return dict(x=x, v=v, c=c, u_pred=u_pred, u_new=u_new, pressure=cp, cell_type=ct, diag=diag.as_dict())
+
+
+def step_replay(box: Box, soa, cell_pressure, dt, first=0, stride=1, density=1000.0, gravity=(0.0, -9.81, 0.0),
+                m_min=0.0, clamp_margin=1e-3):
+    """One FP64 step from the FP32 SoA state `soa` (15 x np) with the pressure
+    given (dense over the box) instead of solved: returns the predicted and
+    corrected face velocities, the cell types, the FP64 evaluation of the given
+    pressure on the step's own system (true residual, ||b||), and x, v, C after
+    the step for the particles first, first + stride, ... ((n_sample, 15))."""
+    soa = np.ascontiguousarray(soa, np.float32)
+    np_ = soa.shape[1]
+    prm = StepParams()
+    prm.dt, prm.density = dt, density
+    prm.gravity[:] = list(gravity)
+    prm.m_min, prm.rel_tol, prm.clamp_margin, prm.max_iterations = m_min, 0.0, clamp_margin, 0
+    u_pred = [np.zeros(box.face_shape(a)) for a in range(3)]
+    u_new = [np.zeros(box.face_shape(a)) for a in range(3)]
+    ct = np.zeros((box.n[2], box.n[1], box.n[0]), np.uint8)
+    cp = _f64(cell_pressure)
+    nsample = len(range(first, np_, stride)) if stride > 0 else 0
+    sample = np.zeros((max(nsample, 1), 15))
+    diag = PressureDiag()
+    _check(cpu().fo_step_replay(ctypes.byref(box), ctypes.byref(prm), soa.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                np_, _d(cp), int(first), int(stride), (_dp * 3)(*[_d(a) for a in u_pred]),
+                                (_dp * 3)(*[_d(a) for a in u_new]), _u8(ct), ctypes.byref(diag), _d(sample)),
+           "step_replay")
+    return dict(u_pred=u_pred, u_new=u_new, cell_type=ct, diag=diag.as_dict(), sample=sample[:nsample],
+                sample_index=np.arange(first, np_, stride) if stride > 0 else np.zeros(0, np.int64))
 
 
 def vcycle(box: Box, cell_type, r, levels=4, pre=2, post=2, coarse_sweeps=8):

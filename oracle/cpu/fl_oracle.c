@@ -1074,3 +1074,109 @@ int fo_vcycle(const fo_box* b, const uint8_t* cell_type, int levels, int pre, in
   }
   return FO_OK;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Replay of one device step at full size: fo_step with the pressure given
+ * instead of solved. Reads the state as FP32 SoA (15 x np floats: x[3], v[3],
+ * C rows[9]) and works in FP64: P2G over every particle (in chunks), normalize
+ * + gravity, stationary walls, the box system of the resulting predicted
+ * velocities, its FP64 evaluation at `cell_pressure` (dense over the box:
+ * corrected faces into u_new, the true residual into diag), then G2P and
+ * advection for the sampled particles p = first, first + stride, ...; each
+ * sampled particle gets 15 doubles in `sample_out` (x, v, C rows after the
+ * step). */
+int fo_step_replay(const fo_box* b, const fo_step_params* prm, const float* soa, size_t np, const double* cell_pressure,
+                   size_t first, size_t stride, double* u_pred[3], double* u_new[3], uint8_t* type,
+                   fo_pressure_diag* diag, double* sample_out) {
+  const double h = b->h;
+  const double pmass = prm->density * h * h * h / 8.0;
+  const size_t chunk = (size_t)1 << 20;
+  double* fm[3];
+  double* fq[3];
+  for (int a = 0; a < 3; ++a) {
+    const size_t nf = fo_face_count(b, a);
+    fm[a] = (double*)calloc(nf, sizeof(double));
+    fq[a] = (double*)calloc(nf, sizeof(double));
+  }
+  double* cx = (double*)malloc(sizeof(double) * 3 * chunk);
+  double* cv = (double*)malloc(sizeof(double) * 3 * chunk);
+  double* cc = (double*)malloc(sizeof(double) * 9 * chunk);
+  double* g = (double*)malloc(sizeof(double) * 24 * chunk);
+  dep_ctx dctx = {fm, fq};
+  int st = FO_OK;
+  for (size_t p0 = 0; p0 < np && st == FO_OK; p0 += chunk) {
+    const size_t m = np - p0 < chunk ? np - p0 : chunk;
+    for (size_t p = 0; p < m; ++p) {
+      for (int d = 0; d < 3; ++d) {
+        cx[3 * p + d] = soa[(size_t)d * np + p0 + p];
+        cv[3 * p + d] = soa[(size_t)(3 + d) * np + p0 + p];
+      }
+      for (int q = 0; q < 9; ++q) cc[9 * p + q] = soa[(size_t)(6 + q) * np + p0 + p];
+    }
+    st = deposit_loop(b, cx, cv, cc, &pmass, 0, m, dep_f64, &dctx);
+  }
+  /* cell classification from FP64 positions, as fo_classify_cells does */
+  if (st == FO_OK) {
+    fo_classify_cells(b, NULL, 0, type);
+    for (size_t p = 0; p < np; ++p) {
+      int64_t c[3];
+      for (int d = 0; d < 3; ++d) c[d] = (int64_t)floor(((double)soa[(size_t)d * np + p] - b->origin[d]) / b->h);
+      const int64_t id = cell_at(b, c[0], c[1], c[2]);
+      if (id >= 0 && type[id] == 2) type[id] = 1;
+    }
+    fo_normalize_forces(b, fm, fq, prm->m_min, prm->dt, prm->gravity, u_pred, NULL);
+    apply_wall_bc(b, type, u_pred);
+    for (int a = 0; a < 3; ++a) memcpy(u_new[a], u_pred[a], sizeof(double) * fo_face_count(b, a));
+    box_pressure bp;
+    box_pressure_build(b, type, u_pred, prm->density, &bp);
+    if (bp.nc > 0) {
+      fo_pressure_inputs in = {bp.nc, bp.nf, bp.cell_index, bp.cell_values, bp.face_index, bp.face_kind,
+                               bp.face_values, h, prm->dt};
+      double* p = (double*)malloc(sizeof(double) * bp.nc);
+      double* uc = (double*)malloc(sizeof(double) * bp.nf);
+      for (size_t i = 0; i < bp.nc; ++i) p[i] = cell_pressure[bp.cell_dense[i]];
+      st = fo_pressure_evaluate(&in, p, NULL, NULL, NULL, uc, diag);
+      for (size_t f = 0; f < bp.nf; ++f) u_new[bp.face_index[4 * f]][bp.face_dense[f]] = uc[f];
+      free(p);
+      free(uc);
+    }
+    box_pressure_free(&bp);
+  }
+  if (st == FO_OK && stride > 0) {
+    const double lo_clamp[3] = {b->origin[0] + (b->lo[0] + 1) * h + prm->clamp_margin * h,
+                                b->origin[1] + (b->lo[1] + 1) * h + prm->clamp_margin * h,
+                                b->origin[2] + (b->lo[2] + 1) * h + prm->clamp_margin * h};
+    const double hi_clamp[3] = {b->origin[0] + (b->lo[0] + b->n[0] - 1) * h - prm->clamp_margin * h,
+                                b->origin[1] + (b->lo[1] + b->n[1] - 1) * h - prm->clamp_margin * h,
+                                b->origin[2] + (b->lo[2] + b->n[2] - 1) * h - prm->clamp_margin * h};
+    size_t done = 0;
+    for (size_t p = first; p < np && st == FO_OK;) {
+      size_t m = 0;
+      for (; m < chunk && p < np; ++m, p += stride)
+        for (int d = 0; d < 3; ++d) cx[3 * m + d] = soa[(size_t)d * np + p];
+      st = fo_g2p(b, cx, m, NULL, u_new, g);
+      for (size_t k = 0; k < m && st == FO_OK; ++k) {
+        const double* o = g + 24 * k;
+        double* s = sample_out + 15 * (done + k);
+        for (int d = 0; d < 3; ++d) {
+          double nx = cx[3 * k + d] + prm->dt * o[d];
+          if (nx < lo_clamp[d]) nx = lo_clamp[d];
+          if (nx > hi_clamp[d]) nx = hi_clamp[d];
+          s[d] = nx;
+          s[3 + d] = o[d];
+        }
+        for (int q = 0; q < 9; ++q) s[6 + q] = o[6 + q];
+      }
+      done += m;
+    }
+  }
+  free(cx);
+  free(cv);
+  free(cc);
+  free(g);
+  for (int a = 0; a < 3; ++a) {
+    free(fm[a]);
+    free(fq[a]);
+  }
+  return st;
+}

@@ -95,6 +95,15 @@ typedef struct {
 int fo_step(const fo_box* box, const fo_step_params* params, double* x, double* v, double* c, size_t np,
             double* u_pred[3], double* u_new[3], double* cell_pressure, uint8_t* cell_type, fo_pressure_diag* diag);
 
+/* fo_step with the pressure given instead of solved, for replaying one device
+ * step at full size: FP32 SoA state in (15 x np), cell_pressure dense over the
+ * box, G2P + advection only for particles first, first + stride, ... (15
+ * doubles each into sample_out: x, v, C rows after the step). diag holds the
+ * FP64 evaluation of the given pressure on the step's own system. */
+int fo_step_replay(const fo_box* box, const fo_step_params* params, const float* soa, size_t np,
+                   const double* cell_pressure, size_t first, size_t stride, double* u_pred[3], double* u_new[3],
+                   uint8_t* cell_type, fo_pressure_diag* diag, double* sample_out);
+
 /* Geometric multigrid V-cycle on the box (FP64 restatement of the GPU preconditioner):
  * red-black Gauss-Seidel, `pre`/`post` sweeps, `levels` levels, piecewise-constant
  * transfer with sum restriction and rediscretized coarse operators, `coarse_sweeps`

@@ -1,14 +1,18 @@
-"""The bench workload at full size (256^3 splash, 29.6M particles), checked
-through properties that do not depend on the size: the sort is the stable cell
-order, every projection meets the FP64 gate, and the step is reproducible bit
-for bit. The oracle itself runs only at the smaller sizes of the other tests."""
+"""The bench workload at full size (256^3 splash, 29.6M particles): one step
+after the warm-up replayed field by field by the FP64 oracle (u_pred, u_new,
+v, C, x at 1e-5; the GPU pressure judged by its FP64 true residual on the
+step's own system), for both V-cycle storages; and properties that do not
+depend on the size: the sort is the stable cell order, every projection meets
+the FP64 gate, and the step is reproducible bit for bit."""
 
 import numpy as np
 import pytest
 
 import fluidity_b200 as fb
+import oracle
 from fluidity_b200 import scenes
-from helpers import sort_permutation
+from helpers import read_fields, sort_permutation
+from oracle.replay import step_parity
 
 pytestmark = pytest.mark.gpu
 
@@ -59,3 +63,31 @@ def test_splash_256_projection_gate_and_reproducibility(splash):
         runs.append(out)
     np.testing.assert_array_equal(runs[0], runs[1])
     ctx.close()
+
+
+@pytest.mark.parametrize("precision", [1, 0])
+def test_splash_256_step_matches_fp64_oracle_replay(splash, precision):
+    """Step 6 of the bench scene (after five steps as warm-up), BF16 and FP32
+    V-cycle storage: grid and particle fields within 1e-5 of the FP64 oracle,
+    the GPU pressure meeting 1e-6 ||b|| in FP64."""
+    soa, mass = splash
+    tp = fb.transfer_params(scenes.DT, mass)
+    opt = fb.default_pressure_options(precision=precision, warm_start=1)
+    ctx = fb.LiquidContext(N, capacity=soa.shape[1])
+    ctx.upload(soa)
+    for _ in range(5):
+        code, _ = ctx.step(tp, opt)
+        assert code == fb.OK
+    state = ctx.download()
+    ctx.upload(state)
+    code, diag = ctx.step(tp, opt)
+    assert code == fb.OK and diag.relative_residual <= 1e-6, diag.as_dict()
+    fields = read_fields(ctx, N)
+    out = ctx.download()
+    ctx.close()
+    errs = step_parity(N, state, out, fields, scenes.DT)
+    print(f"splash 256 step 6, precision {precision}: {errs}")
+    assert errs["cell_types_agree"], errs
+    assert errs["pressure_relative_residual"] <= 1.0001e-6, errs
+    for k in ("u_pred0", "u_pred1", "u_pred2", "u_new0", "u_new1", "u_new2", "v", "C", "x_cells"):
+        assert errs[k] <= 1e-5, (k, errs)
