@@ -15,11 +15,15 @@
 // accumulates into registers: along the normal axis a particle of the cell
 // touches nodes cell-1..cell+1 or cell..cell+2, so 4 x 3 x 3 = 36 slots per
 // channel cover every particle of the cell with static register indexing.
-// Register partials go to shared memory ([slot][cell] mass/momentum pairs); each tile node
-// then sums its (at most 36) contributing (cell, slot) entries in a fixed
-// order. The 11x10x10 tile (normal extent 11, transverse 10) is written to a
-// per-block scratch tile and a second kernel sums, for every owned face, the
-// tiles of the (at most 8) blocks whose halo covers it, again in a fixed order.
+// The register partials are then summed across the warp with shuffles: a
+// warp holds one z-plane of four 8-cell rows, so the x-neighbours' slots that
+// land on the same node are combined along each row and then across the rows,
+// giving every warp a small tile of its nodes in shared memory (at most
+// 4 x 6 x 10 entries). Each node of the block's 11x10x10 tile (normal extent 11,
+// transverse 10) sums the (at most 8) warp tiles that cover it in a fixed
+// order. The block tile is written to a per-block scratch tile and a second
+// kernel sums, for every owned face, the tiles of the (at most 8) blocks whose
+// halo covers it, again in a fixed order.
 // No floating-point atomics are used anywhere, so the result is bitwise
 // reproducible run to run for a given particle order (the stable sort fixes it).
 #include "fl_internal.cuh"
@@ -31,60 +35,22 @@ constexpr int kP2GThreads = 512;
 constexpr int kSlots = 36;
 
 template <int A>
-__device__ __forceinline__ int slot_index(int sx, int sy, int sz) {
-  constexpr int ex = A == 0 ? 4 : 3, ey = A == 1 ? 4 : 3;
-  return (sz * ey + sy) * ex + sx;
-}
-
-// Axis factors for one particle coordinate. For the normal axis, 4 slots with
-// node = cell - 1 + s (one slot is zero); for transverse axes, 3 slots with
-// anchor cell - 1 + s + 1/2. affine[s] = C_a,d * (anchor_s - X) * h.
-template <bool kNormal>
-__device__ __forceinline__ void axis_factors(float X, int cell, float h, float cad, float w[4], float affine[4]) {
-  if (kNormal) {
-    const float first = floorf(X - 0.5f);
-    const bool shifted = first > (float)(cell - 1);  // first node is the cell itself
-    const float dl = X - (first + 0.5f);
-    const float dr = fabsf(X - (first + 1.5f));
-    const float c = X - (first + 1.0f);
-    const float w0 = 0.5f * dr * dr, w1 = 0.75f - c * c, w2 = 0.5f * dl * dl;
-    w[0] = shifted ? 0.0f : w0;
-    w[1] = shifted ? w0 : w1;
-    w[2] = shifted ? w1 : w2;
-    w[3] = shifted ? w2 : 0.0f;
-#pragma unroll
-    for (int s = 0; s < 4; ++s) affine[s] = cad * (((float)(cell - 1 + s) - X) * h);
-  } else {
-    const float f = X - (float)cell;
-    const float dr = fabsf(1.0f - f);
-    const float c = f - 0.5f;
-    w[0] = 0.5f * dr * dr;
-    w[1] = 0.75f - c * c;
-    w[2] = 0.5f * f * f;
-    w[3] = 0.0f;
-#pragma unroll
-    for (int s = 0; s < 3; ++s) affine[s] = cad * (((float)(cell - 1 + s) + 0.5f - X) * h);
-    affine[3] = 0.0f;
-  }
-}
-
-template <int A>
 __device__ __forceinline__ void p2g_component(const GridView& g, const ParticlesView& p, const unsigned int* order,
-                                              int pbeg, int pend, const int cell[3], float2* part, int t,
-                                              DeviceReport* rep) {
+                                              int pbeg, int pend, const int cell[3], float2 accW[kSlots / 2],
+                                              float2 accQ[kSlots / 2], DeviceReport* rep) {
   constexpr int D1 = A == 0 ? 1 : 0;
   constexpr int D2 = A == 2 ? 1 : 2;
   // Accumulators in normal-axis slot pairs: entry (k * 3 + j) * 2 + hp holds
   // normal slots 2hp (x) and 2hp + 1 (y) of transverse node (j, k). Each pair
   // is updated by one packed FP32 FMA (fma.rn.f32x2), which rounds every lane
   // exactly as fmaf does, so the sums are bitwise those of the scalar form.
-  float2 accW[kSlots / 2], accQ[kSlots / 2];
 #pragma unroll
   for (int s = 0; s < kSlots / 2; ++s) {
     accW[s] = make_float2(0.0f, 0.0f);
     accQ[s] = make_float2(0.0f, 0.0f);
   }
   const float h = g.h;
+  const float cellf[3] = {(float)cell[0], (float)cell[1], (float)cell[2]};
   // The particle of cell-order slot q, with the next slot's entry loaded one
   // iteration ahead so the order lookup overlaps the particle loads.
   int next = order != nullptr && pbeg < pend ? (int)__ldg(&order[pbeg]) : pbeg;
@@ -96,10 +62,49 @@ __device__ __forceinline__ void p2g_component(const GridView& g, const Particles
     for (int d = 0; d < 3; ++d) X[d] = lattice_coord(g, __ldg(&p.x[d][i]), d);
     const float m = p.mass ? __ldg(&p.mass[i]) : 1.0f;
     const float va = __ldg(&p.v[A][i]);
-    float wa[4], ta[4], w1[4], t1[4], w2[4], t2[4];
-    axis_factors<true>(X[A], cell[A], h, __ldg(&p.c[3 * A + A][i]), wa, ta);
-    axis_factors<false>(X[D1], cell[D1], h, __ldg(&p.c[3 * A + D1][i]), w1, t1);
-    axis_factors<false>(X[D2], cell[D2], h, __ldg(&p.c[3 * A + D2][i]), w2, t2);
+    const float cA = __ldg(&p.c[3 * A + A][i]), c1 = __ldg(&p.c[3 * A + D1][i]), c2 = __ldg(&p.c[3 * A + D2][i]);
+    // Normal axis (face-centred nodes cell-1 .. cell+2): with f = X - cell
+    // (exact) the particle's first node is cell - 1 for f < 1/2, else cell, and
+    // g = X - (first + 1) gives the three weights 0.5 (1/2 - g)^2, 3/4 - g^2,
+    // 0.5 (1/2 + g)^2; the unused slot is zero. Affine terms
+    // ta[s] = C_aa h (s - 1 - f), formed by adding C_aa h slot by slot.
+    float wa[4], ta[4];
+    {
+      const float f = X[A] - cellf[A];
+      const bool shifted = f >= 0.5f;
+      const float gg = shifted ? f - 1.0f : f;
+      const float dm = 0.5f - gg, dp = 0.5f + gg;
+      const float n0 = 0.5f * dm * dm, n1 = fmaf(-gg, gg, 0.75f), n2 = 0.5f * dp * dp;
+      wa[0] = shifted ? 0.0f : n0;
+      wa[1] = shifted ? n0 : n1;
+      wa[2] = shifted ? n1 : n2;
+      wa[3] = shifted ? n2 : 0.0f;
+      const float ch = cA * h;
+      ta[0] = fmaf(-ch, f, -ch);
+      ta[1] = ta[0] + ch;
+      ta[2] = ta[1] + ch;
+      ta[3] = ta[2] + ch;
+    }
+    // Transverse axes D1, D2 as one packed pair (cell-centred nodes
+    // cell-1 .. cell+1): weights 0.5 (1-f)^2, 3/4 - (f - 1/2)^2, 0.5 f^2 and
+    // affine terms C h (s - 1/2 - f).
+    float w1[3], w2[3], t1[3], t2[3];
+    {
+      const float2 f = __fadd2_rn(make_float2(X[D1], X[D2]), make_float2(-cellf[D1], -cellf[D2]));
+      const float2 half = make_float2(0.5f, 0.5f);
+      const float2 d = __fadd2_rn(make_float2(1.0f, 1.0f), make_float2(-f.x, -f.y));
+      const float2 c = __fadd2_rn(f, make_float2(-0.5f, -0.5f));
+      const float2 w0 = __fmul2_rn(__fmul2_rn(half, d), d);
+      const float2 wm = __ffma2_rn(make_float2(-c.x, -c.y), c, make_float2(0.75f, 0.75f));
+      const float2 wp = __fmul2_rn(__fmul2_rn(half, f), f);
+      const float2 ch = __fmul2_rn(make_float2(c1, c2), make_float2(h, h));
+      const float2 a0 = __fmul2_rn(ch, __fadd2_rn(make_float2(-0.5f, -0.5f), make_float2(-f.x, -f.y)));
+      const float2 a1 = __fadd2_rn(a0, ch), a2 = __fadd2_rn(a1, ch);
+      w1[0] = w0.x, w1[1] = wm.x, w1[2] = wp.x;
+      w2[0] = w0.y, w2[1] = wm.y, w2[2] = wp.y;
+      t1[0] = a0.x, t1[1] = a1.x, t1[2] = a2.x;
+      t2[0] = a0.y, t2[1] = a1.y, t2[2] = a2.y;
+    }
     if (!(isfinite(m) && isfinite(va))) report_error(rep, kInvalidArgument, (unsigned long long)i);
     // Per node: W += wa*P and Q += wa*(P*q12) + (wa*ta)*P, with wa the
     // mass-scaled normal weight, P the transverse weight product and q12 = v_a
@@ -126,42 +131,102 @@ __device__ __forceinline__ void p2g_component(const GridView& g, const Particles
         }
       }
   }
-#pragma unroll
-  for (int k = 0; k < 3; ++k)
-#pragma unroll
-    for (int j = 0; j < 3; ++j)
-#pragma unroll
-      for (int s = 0; s < 4; ++s) {
-        const int slot = A == 0 ? slot_index<A>(s, j, k) : A == 1 ? slot_index<A>(j, s, k) : slot_index<A>(j, k, s);
-        const int e = (k * 3 + j) * 2 + (s >> 1);
-        part[slot * kP2GThreads + t] =
-            (s & 1) ? make_float2(accW[e].y, accQ[e].y) : make_float2(accW[e].x, accQ[e].x);
-      }
 }
 
+// Slot (sx, sy, sz) of the accumulators (offsets along x, y, z from the cell's
+// first node), as a (mass, momentum) pair.
 template <int A>
-__device__ __forceinline__ void reduce_tile(const float2* part, float2* tile, int t) {
+__device__ __forceinline__ float2 slot_val(const float2 accW[kSlots / 2], const float2 accQ[kSlots / 2], int sx, int sy,
+                                           int sz) {
+  const int s = A == 0 ? sx : (A == 1 ? sy : sz);
+  const int j = A == 0 ? sy : sx;
+  const int k = A == 2 ? sy : sz;
+  const int e = (k * 3 + j) * 2 + (s >> 1);
+  return (s & 1) ? make_float2(accW[e].y, accQ[e].y) : make_float2(accW[e].x, accQ[e].x);
+}
+
+__device__ __forceinline__ float2 shfl_up2(float2 v, int d) {
+  return make_float2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
+}
+__device__ __forceinline__ float2 shfl_down2(float2 v, int d) {
+  return make_float2(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d));
+}
+
+// Extents of the warp tile of component A: a warp holds the cells of one
+// z-plane and four y-rows of 8, so its slots cover ex + 7 nodes along x,
+// ey + 3 along y and ez along z (node coordinates from the warp's first
+// cell - 1).
+template <int A>
+struct WarpTile {
+  static constexpr int ex = A == 0 ? 4 : 3, ey = A == 1 ? 4 : 3, ez = A == 2 ? 4 : 3;
+  static constexpr int tx = ex + 7, ty = ey + 3, tz = ez;
+  static constexpr int size = tx * ty * tz;
+};
+constexpr int kWarpTileMax = 240;  // max over the three components (10 x 6 x 4)
+constexpr int kP2GWarps = kP2GThreads / 32;
+
+// The warp's partials summed per node, in a fixed order, into its tile:
+// along x within each 8-lane row (a lane keeps node x - 1 and, for x <= ex - 2,
+// node x + 7), then along y across the four rows (node y - 1 and, for
+// y <= ey - 2, node y + 3); every tile entry is written by exactly one lane.
+template <int A>
+__device__ __forceinline__ void warp_tile(const float2 accW[kSlots / 2], const float2 accQ[kSlots / 2], float2* wt,
+                                          int lane) {
+  using W = WarpTile<A>;
+  const int x = lane & 7, y = lane >> 3;
+#pragma unroll
+  for (int sz = 0; sz < W::ez; ++sz) {
+    float2 xf[W::ey], xb[W::ey];
+#pragma unroll
+    for (int sy = 0; sy < W::ey; ++sy) {
+      float2 f = slot_val<A>(accW, accQ, 0, sy, sz), bk = make_float2(0.0f, 0.0f);
+#pragma unroll
+      for (int sx = 1; sx < W::ex; ++sx) {
+        const float2 v = slot_val<A>(accW, accQ, sx, sy, sz);
+        const float2 up = shfl_up2(v, sx), dn = shfl_down2(v, 8 - sx);
+        if (x >= sx) f = __fadd2_rn(f, up);
+        if (sx >= x + 1) bk = __fadd2_rn(bk, dn);
+      }
+      xf[sy] = f;
+      xb[sy] = bk;
+    }
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+      float2 f = part ? xb[0] : xf[0], bk = make_float2(0.0f, 0.0f);
+#pragma unroll
+      for (int sy = 1; sy < W::ey; ++sy) {
+        const float2 v = part ? xb[sy] : xf[sy];
+        const float2 up = shfl_up2(v, 8 * sy), dn = shfl_down2(v, 8 * (4 - sy));
+        if (y >= sy) f = __fadd2_rn(f, up);
+        if (sy >= y + 1) bk = __fadd2_rn(bk, dn);
+      }
+      const int lx = x + 8 * part;
+      if (part == 0 || x <= W::ex - 2) {
+        wt[(sz * W::ty + y) * W::tx + lx] = f;
+        if (y <= W::ey - 2) wt[(sz * W::ty + y + 4) * W::tx + lx] = bk;
+      }
+    }
+  }
+}
+
+// Node n of the block's tile of component A: the sum of the warp tiles that
+// cover it, warps in ascending (z, y-half) order.
+template <int A>
+__device__ __forceinline__ void block_tile(const float2* wtiles, float2* tile, int t) {
+  using W = WarpTile<A>;
   constexpr int e0 = A == 0 ? 11 : 10, e1 = A == 1 ? 11 : 10;
-  constexpr int ex = A == 0 ? 4 : 3, ey = A == 1 ? 4 : 3, ez = A == 2 ? 4 : 3;
   for (int n = t; n < kTileFaces; n += kP2GThreads) {
-    const int nx = n % e0 - 1, ny = (n / e0) % e1 - 1, nz = n / (e0 * e1) - 1;
-    float2 WQ = make_float2(0.0f, 0.0f);  // (mass, momentum), each lane summed in the same order
+    const int lx = n % e0, ny = (n / e0) % e1 - 1, nz = n / (e0 * e1) - 1;
+    float2 WQ = make_float2(0.0f, 0.0f);
 #pragma unroll
-    for (int sz = 0; sz < ez; ++sz) {
-      const int cz = nz + 1 - sz;
-      if (cz < 0 || cz > 7) continue;
+    for (int dz = 0; dz < W::ez; ++dz) {
+      const int wz = nz + 1 - dz;  // warp plane whose local z index is dz
+      if (wz < 0 || wz > 7) continue;
 #pragma unroll
-      for (int sy = 0; sy < ey; ++sy) {
-        const int cy = ny + 1 - sy;
-        if (cy < 0 || cy > 7) continue;
-#pragma unroll
-        for (int sx = 0; sx < ex; ++sx) {
-          const int cx = nx + 1 - sx;
-          if (cx < 0 || cx > 7) continue;
-          const int c = cz * 64 + cy * 8 + cx;
-          const int s = (sz * ey + sy) * ex + sx;
-          WQ = __fadd2_rn(WQ, part[s * kP2GThreads + c]);
-        }
+      for (int wy = 0; wy < 2; ++wy) {
+        const int ly = ny + 1 - 4 * wy;
+        if (ly < 0 || ly >= W::ty) continue;
+        WQ = __fadd2_rn(WQ, wtiles[(wz * 2 + wy) * kWarpTileMax + (dz * W::ty + ly) * W::tx + lx]);
       }
     }
     tile[n] = WQ;
@@ -171,30 +236,46 @@ __device__ __forceinline__ void reduce_tile(const float2* part, float2* tile, in
 __global__ void __launch_bounds__(kP2GThreads, 1)
     k_p2g_tile(GridView g, ParticlesView p, const unsigned int* order, const int* cell_start, float2* tiles,
                DeviceReport* rep) {
-  extern __shared__ float2 part[];  // [slot][cell] (mass, momentum) partials
+  // Two sets of warp tiles, alternating between components, so one barrier
+  // per component separates a set's writers from its readers.
+  extern __shared__ float2 wt_smem[];
+  float2* wtiles[2] = {wt_smem, wt_smem + kP2GWarps * kWarpTileMax};
   const int b = blockIdx.x;
   const int t = threadIdx.x;
   const int base = b * kBlockCells;
-  float2* tile0 = tiles + (size_t)b * 3 * kTileFaces;
+  float2* tile = tiles + (size_t)b * 3 * kTileFaces;
   if (cell_start[base] == cell_start[base + kBlockCells]) {  // no particles: a zero tile for the merge
-    for (int n = t; n < 3 * kTileFaces; n += kP2GThreads) tile0[n] = make_float2(0.0f, 0.0f);
+    for (int n = t; n < 3 * kTileFaces; n += kP2GThreads) tile[n] = make_float2(0.0f, 0.0f);
     return;
   }
   const int pbeg = cell_start[base + t], pend = cell_start[base + t + 1];
   const int cell[3] = {g.coord[3 * b] * 8 + (t & 7), g.coord[3 * b + 1] * 8 + ((t >> 3) & 7),
                        g.coord[3 * b + 2] * 8 + (t >> 6)};
-  float2* tile = tiles + (size_t)b * 3 * kTileFaces;
-  p2g_component<0>(g, p, order, pbeg, pend, cell, part, t, rep);
+  float2* wt = nullptr;
+  {
+    float2 accW[kSlots / 2], accQ[kSlots / 2];
+    p2g_component<0>(g, p, order, pbeg, pend, cell, accW, accQ, rep);
+    wt = wtiles[0] + (t >> 5) * kWarpTileMax;
+    warp_tile<0>(accW, accQ, wt, t & 31);
+  }
   __syncthreads();
-  reduce_tile<0>(part, tile, t);
+  block_tile<0>(wtiles[0], tile, t);
+  {
+    float2 accW[kSlots / 2], accQ[kSlots / 2];
+    p2g_component<1>(g, p, order, pbeg, pend, cell, accW, accQ, rep);
+    wt = wtiles[1] + (t >> 5) * kWarpTileMax;
+    warp_tile<1>(accW, accQ, wt, t & 31);
+  }
   __syncthreads();
-  p2g_component<1>(g, p, order, pbeg, pend, cell, part, t, rep);
+  block_tile<1>(wtiles[1], tile + kTileFaces, t);
+  {
+    float2 accW[kSlots / 2], accQ[kSlots / 2];
+    p2g_component<2>(g, p, order, pbeg, pend, cell, accW, accQ, rep);
+    wt = wtiles[0] + (t >> 5) * kWarpTileMax;
+    warp_tile<2>(accW, accQ, wt, t & 31);
+  }
   __syncthreads();
-  reduce_tile<1>(part, tile + kTileFaces, t);
-  __syncthreads();
-  p2g_component<2>(g, p, order, pbeg, pend, cell, part, t, rep);
-  __syncthreads();
-  reduce_tile<2>(part, tile + 2 * kTileFaces, t);
+  block_tile<2>(wtiles[0], tile + 2 * kTileFaces, t);
 }
 
 __device__ __forceinline__ bool is_solid(const GridView& g, int x, int y, int z) {
@@ -278,7 +359,7 @@ cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cel
                        const P2GMergeParams& prm, float* const out0[3], float* const out1[3], DeviceReport* rep,
                        cudaStream_t s, const unsigned int* order) {
   if (g.nb == 0) return cudaSuccess;
-  const size_t smem = sizeof(float2) * kSlots * kP2GThreads;
+  const size_t smem = sizeof(float2) * 2 * kP2GWarps * kWarpTileMax;
   static unsigned long long configured = 0;
   if (first_on_device(configured))
     cudaFuncSetAttribute(k_p2g_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -89,5 +89,5 @@ def test_splash_256_step_matches_fp64_oracle_replay(splash, precision):
     print(f"splash 256 step 6, precision {precision}: {errs}")
     assert errs["cell_types_agree"], errs
     assert errs["pressure_relative_residual"] <= 1.0001e-6, errs
-    for k in ("u_pred0", "u_pred1", "u_pred2", "u_new0", "u_new1", "u_new2", "v", "C", "x_cells"):
+    for k in ("u_pred0", "u_pred1", "u_pred2", "u_new0", "u_new1", "u_new2", "v", "C", "x"):
         assert errs[k] <= 1e-5, (k, errs)
