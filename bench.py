@@ -354,18 +354,98 @@ def run_ours(args, world, rank, local):
         "library_launches": int(launches1[1] - launches0[1]),
         "clocks": clocks.summary(),
     }
+    learned_params = None
     if not args.no_learned:
-        line["pressure_solve_ms"] = pressure_comparison(ctx, tp, args.grid)
+        line["pressure_solve_ms"], learned_params = pressure_comparison(ctx, tp, args.grid)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(soa, mass, args.grid, npart, ncell, budget_s=args.cpu_budget)
         # One more step of the same run, outside every timed region, replayed
         # field by field by the FP64 oracle on the host (the checker).
         line["parity_vs_fp64"] = parity_vs_fp64(ctx, tp, opt, args.grid, args.warmup + args.steps + 1)
     ctx.close()
+    if world == 1 and not args.no_column_drop:
+        line["column_drop_512"] = column_drop_512(peak, learned_params)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return line
+
+
+def column_drop_512(peak, learned_params, steps=5, warmup=3):
+    """The 512^3 column drop (column [0.1,0.3]x[0.1,0.8]x[0.1,0.3] over a pool
+    y <= 0.15, 8 particles per fluid cell) on the same GPU after the headline:
+    steps/s and particles/s over `steps` CUDA-event-timed steps after `warmup`,
+    the phase times and rooflines as for the headline, and the pressure solve
+    of the last step's projection from p = 0 to a 1e-6 FP64 relative residual
+    with plain FP32 MGPCG, BF16-storage MGPCG and the learned preconditioner."""
+    import torch
+
+    import fluidity_b200 as fb
+    from fluidity_b200 import scenes
+
+    t0 = time.time()
+    soa, mass = scenes.column_drop(512)
+    npart = soa.shape[1]
+    gen_s = time.time() - t0
+    ctx = fb.LiquidContext(512, capacity=npart)
+    tp = fb.transfer_params(scenes.DT, mass)
+    opt = fb.default_pressure_options(precision=1, rel_tol=1e-6, warm_start=1, inner_rtol=1e-3)
+    ctx.upload(soa)
+    fluid_cells = npart // 8
+    del soa
+    for _ in range(warmup):
+        code, _ = ctx.step(tp, opt)
+    nb0 = len(ctx.active_blocks())
+    phases, iters = np.zeros(4), []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        code, d = ctx.step(tp, opt)
+        if code != fb.OK:
+            raise RuntimeError(f"column drop: pressure did not converge: {d.as_dict()}")
+        phases += ctx.step_timings()
+        iters.append(d.iterations)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    nb1 = len(ctx.active_blocks())
+    ncell = (nb0 + nb1) // 2 * 512
+    p2g_ms, g2p_ms, pr_ms = phases[1] / steps, phases[3] / steps, phases[2] / steps
+    tb = 132.0 * npart + 36.0 * ncell
+    out = {"workload": "column_drop_512", "grid": 512, "particles": npart, "fluid_cells_initial": fluid_cells,
+           "active_blocks": [nb0, nb1], "allocated_cells": ncell, "steps": steps, "warmup": warmup,
+           "steps_per_s": round(1e3 / ms, 3), "ms_per_step": round(ms, 3),
+           "particles_per_s": round(npart * 1e3 / ms, 1),
+           "phases_ms": {"topology_sort": round(phases[0] / steps, 3), "p2g": round(p2g_ms, 3),
+                         "pressure": round(pr_ms, 3), "g2p": round(g2p_ms, 3)},
+           "transfers_roofline": {"algorithmic_bytes": int(tb),
+                                  "achieved": round(tb / ((p2g_ms + g2p_ms) / 1e3) / 1e9, 1),
+                                  "frac": round(tb / ((p2g_ms + g2p_ms) / 1e3) / 1e9 / peak, 4)},
+           "pressure_roofline": _pressure_roofline(ncell, float(np.mean(iters)), pr_ms, peak, 1),
+           "mean_iterations": float(np.mean(iters)), "scene_seconds": round(gen_s, 1),
+           "data": "synthetic (seeded column_drop scene, generated on the host z-slab by z-slab)"}
+    variants = {"mgpcg_fp32": dict(precision=0), "mgpcg_bf16": dict(precision=1)}
+    if learned_params is not None:
+        ctx.set_learned_preconditioner(learned_params)
+        variants["learned_bf16"] = dict(precision=1, preconditioner=1)
+    solve = {"unit": "ms", "relative_residual": 1e-6, "start": "p = 0"}
+    for name, kw in variants.items():
+        best = None
+        for _ in range(2):
+            code, d = ctx.project(tp, fb.default_pressure_options(rel_tol=1e-6, warm_start=0, **kw))
+            if code != fb.OK:
+                raise RuntimeError(f"column drop {name}: pressure did not converge: {d.as_dict()}")
+            if best is None or d.solve_ms < best.solve_ms:
+                best = d
+        solve[name] = {"ms": round(best.solve_ms, 3), "iterations": best.iterations,
+                       "learned_iterations": best.learned_iterations, "fell_back": best.fell_back,
+                       "relative_residual": best.relative_residual}
+    if "learned_bf16" in solve:
+        solve["learned_vs_fp32_mgpcg_speedup"] = round(solve["mgpcg_fp32"]["ms"] / solve["learned_bf16"]["ms"], 3)
+    out["pressure_solve_ms"] = solve
+    ctx.close()
+    return out
 
 
 def parity_vs_fp64(ctx, tp, opt, grid, step_number):
@@ -448,7 +528,7 @@ def pressure_comparison(ctx, tp, grid, repeats=2):
     out["training"] = {"pairs": int(x.shape[0]), "adam_steps": 2000, "batch": 64, "lr": 1e-3,
                        "seconds": round(train_s, 1), "loss_first": float(losses[:20].mean()),
                        "loss_last": float(losses[-20:].mean())}
-    return out
+    return out, P
 
 
 def _sample_cube(soa, grid, sample):
@@ -594,6 +674,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-MGPCG pressure comparison")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-column-drop", action="store_true", help="skip the 512^3 column-drop line")
     args = ap.parse_args()
     world, rank, local = _dist()
     if args.impl == "reference":

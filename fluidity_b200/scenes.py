@@ -76,6 +76,45 @@ def seed_particles(n: int, cells: np.ndarray, seed: int = 0, velocity=None):
     return soa, mass
 
 
+def seed_scene(n: int, inside, velocity_of=None, seed: int = 0, slab: int = 32):
+    """Particles of every interior cell whose centre satisfies inside(X, Y, Z),
+    generated z-slab by z-slab into one preallocated FP32 SoA array: the same
+    particles in the same order as seed_particles over all the cells at once,
+    with host memory bounded by one slab (a 512^3 scene holds ~190M particles).
+    velocity_of(X, Y, Z) -> (m, 3) gives the velocity of the selected cells."""
+    h = 1.0 / n
+    idx = np.arange(1, n - 1)
+    c = (idx + 0.5) / n
+    J2, I2 = np.meshgrid(idx, idx, indexing="ij")
+    Y2, X2 = np.meshgrid(c, c, indexing="ij")
+    slabs = [idx[k0:k0 + slab] for k0 in range(0, len(idx), slab)]
+
+    def cells_of(ks):
+        Z = np.repeat(((ks + 0.5) / n)[:, None, None], len(idx), 1).repeat(len(idx), 2)
+        X = np.broadcast_to(X2, Z.shape)
+        Y = np.broadcast_to(Y2, Z.shape)
+        mask = inside(X, Y, Z)
+        K = np.broadcast_to(ks[:, None, None], Z.shape)
+        J = np.broadcast_to(J2, Z.shape)
+        I = np.broadcast_to(I2, Z.shape)
+        return np.stack([K[mask], J[mask], I[mask]], axis=1), (X[mask], Y[mask], Z[mask])
+
+    total = sum(int(inside(np.broadcast_to(X2, (len(ks), *X2.shape)), np.broadcast_to(Y2, (len(ks), *X2.shape)),
+                           np.broadcast_to(((ks + 0.5) / n)[:, None, None], (len(ks), *X2.shape))).sum())
+                for ks in slabs)
+    out = np.zeros((15, 8 * total), np.float32)
+    at = 0
+    for ks in slabs:
+        cells, xyz = cells_of(ks)
+        if len(cells) == 0:
+            continue
+        vel = velocity_of(*xyz) if velocity_of is not None else None
+        part, _ = seed_particles(n, cells, seed, vel)
+        out[:, at:at + part.shape[1]] = part
+        at += part.shape[1]
+    return out, DENSITY * h ** 3 / 8.0
+
+
 def _interior_centres(n: int):
     idx = np.arange(1, n - 1)
     c = (idx + 0.5) / n
@@ -114,9 +153,9 @@ def splash(n: int, seed: int = 0):
 
 
 def column_drop(n: int, seed: int = 0):
-    cells, _, _ = _cells_where(
-        n, lambda X, Y, Z: (Y <= 0.15) | ((X >= 0.1) & (X <= 0.3) & (Y >= 0.1) & (Y <= 0.8) & (Z >= 0.1) & (Z <= 0.3)))
-    return seed_particles(n, cells, seed)
+    return seed_scene(
+        n, lambda X, Y, Z: (Y <= 0.15) | ((X >= 0.1) & (X <= 0.3) & (Y >= 0.1) & (Y <= 0.8) & (Z >= 0.1) & (Z <= 0.3)),
+        seed=seed)
 
 
 SCENES = {"dam_break": dam_break, "splash": splash, "column_drop": column_drop}

@@ -112,3 +112,38 @@ def closed_system(cells_idx, open_faces):
         if key in open_faces:
             fk[f], fv[f] = open_faces[key][0], open_faces[key][1]
     return fi, fk, fv
+
+
+class _DeviceArray:
+    """A raw device pointer seen through __cuda_array_interface__ (for torch views of library buffers)."""
+
+    def __init__(self, ptr, count, dtype):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": np.dtype(dtype).str,
+                                         "data": (int(ptr), False), "version": 3, "strides": None}
+
+
+def device_view(ptr, count, dtype):
+    """A torch tensor aliasing `count` elements of library device memory at `ptr`."""
+    import torch
+
+    return torch.as_tensor(_DeviceArray(ptr, count, dtype), device="cuda")
+
+
+def state_views(ctx):
+    """torch views of the context's current particle state: 15 arrays (x[3], v[3], C[9])."""
+    pv = ctx.particles_view()
+    n = pv.count
+    return [device_view(pv.x[d], n, np.float32) for d in range(3)] + \
+        [device_view(pv.v[d], n, np.float32) for d in range(3)] + [device_view(pv.c[d], n, np.float32) for d in range(9)]
+
+
+def device_cell_order(x, n):
+    """The device's stable sort by (8^3 block, local cell) computed with torch on
+    device positions x (3 tensors): the permutation, as a torch int64 tensor."""
+    import torch
+
+    cell = [torch.floor(x[d] * np.float32(n)).to(torch.int64) for d in range(3)]
+    nbk = n // 8
+    key = ((((cell[2] >> 3) * nbk + (cell[1] >> 3)) * nbk + (cell[0] >> 3)) * 512 + (cell[2] & 7) * 64 +
+           (cell[1] & 7) * 8 + (cell[0] & 7))
+    return torch.sort(key, stable=True).indices
