@@ -192,6 +192,7 @@ def library():
         lib.fl_unet_forward.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
         lib.fl_unet_backward.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
         lib.fl_unet_masked_mse.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp]
+        lib.fl_unet_block_residual_loss.argtypes = [vp, vp, ctypes.c_int, vp, vp, vp]
         lib.fl_adam_step.argtypes = [vp, vp, vp, vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                      ctypes.c_float, ctypes.c_float, vp]
         lib.fl_collect_training_pairs.argtypes = [vp, ctypes.POINTER(TransferParams), ctypes.POINTER(PressureOptions),
@@ -585,6 +586,13 @@ class UNet:
         _check(library().fl_unet_masked_mse(outputs.data_ptr(), targets.data_ptr(), masks.data_ptr(), outputs.shape[0],
                                             int(relative), loss.data_ptr(), grad_outputs.data_ptr(), stream),
                "fl_unet_masked_mse")
+
+    @staticmethod
+    def block_residual_loss(outputs, inputs, loss, grad_outputs, stream=None):
+        """fl_unet_block_residual_loss: |r_b - A_b y|^2 / |r_b|^2 averaged over the items."""
+        _check(library().fl_unet_block_residual_loss(outputs.data_ptr(), inputs.data_ptr(), outputs.shape[0],
+                                                     loss.data_ptr(), grad_outputs.data_ptr(), stream),
+               "fl_unet_block_residual_loss")
 
     @staticmethod
     def adam_step(params, grads, m, v, step: int, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999,

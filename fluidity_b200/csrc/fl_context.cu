@@ -407,7 +407,7 @@ cudaError_t nn_apply(void* vc, const float* r, void* z, cudaStream_t s) {
   fl_context* c = static_cast<fl_context*>(vc);
   const GridView g = view(c);
   return unet_tc_apply<T>(g, c->nn_params, c->nn_packed, c->nn_tc, c->nn_tc_items, c->nn_bt, c->nn_scale, c->type,
-                          r, static_cast<T*>(z), &c->st->nn_error, c->sms, s);
+                          r, static_cast<T*>(z), &c->st->nn_error, c->sms, s, c->nn_hook.compose != 0);
 }
 
 int nn_reserve_tc(fl_context* c, long long items) {
@@ -463,7 +463,7 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
   const double vel_scale = dt / (rho * h);    // u += vel_scale * (p_tail - p_head)
   const long long n = (long long)c->nb * kBlockCells;
   MgOptions mo{std::max(1, opt->pre_sweeps), std::max(1, opt->post_sweeps), std::max(1, opt->coarse_sweeps)};
-  const bool use_nn = opt->preconditioner == 1;
+  const bool use_nn = opt->preconditioner == 1 || opt->preconditioner == 2;
   if (opt->preconditioner != 0 && !use_nn) return FL_INVALID_ARGUMENT;
   if (use_nn) {
     if (!c->nn_ready) return FL_FAILED_PRECONDITION;
@@ -471,6 +471,7 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
     if (st != FL_OK) return st;
     c->nn_hook.apply = nn_apply<T>;
     c->nn_hook.ctx = c;
+    c->nn_hook.compose = opt->preconditioner == 2 ? 1 : 0;
   }
   const int stall_limit = opt->stall_limit > 0 ? opt->stall_limit : 3;
   const double stall_ratio = opt->stall_ratio > 0.0 ? opt->stall_ratio : 0.9;
@@ -506,8 +507,9 @@ int pressure_solve(fl_context* c, const float* const u_pred[3], float* const u_n
       std::memcpy(c->fcg_key, key, sizeof(key));
     }
     if (use_nn) {
-      const long long nkey[8] = {c->nb, levels, mo.pre, mo.post, mo.coarse_sweeps, (long long)sizeof(T),
-                                 (long long)(uintptr_t)c->nn_tc, c->nn_tc_items};
+      const long long nkey[8] = {c->nb, levels, mo.pre, mo.post, mo.coarse_sweeps,
+                                 (long long)sizeof(T) + 16 * c->nn_hook.compose, (long long)(uintptr_t)c->nn_tc,
+                                 c->nn_tc_items};
       if (!c->fcg_nn_exec || std::memcmp(nkey, c->fcg_nn_key, sizeof(nkey)) != 0) {
         st = capture_fcg<T>(c, g, H, mo, true, &c->fcg_nn_exec, &c->fcg_nn_kernels);
         if (st != FL_OK) return st;
@@ -789,6 +791,25 @@ int step_topology(fl_context* c, const fl_particles* p, cudaStream_t s, fl_repor
   FL_CUDA(launch_build_neighbors(g, c->nbr27, s));
   return FL_OK;
 }
+
+namespace fl {
+// The residual the composite preconditioner's network sees: one V-cycle on the
+// current hierarchy from r, then rho = r - A V(r) (rho may be c->q).
+template <typename T>
+int post_vcycle_residual(fl_context* c, const fl_pressure_options* opt, const float* r, float* rho, cudaStream_t s) {
+  GridView g = view(c);
+  MgHierarchy<T> H{};
+  const int levels = opt->levels > 0 ? opt->levels : auto_levels(c);
+  int st = make_hierarchy<T>(c, levels, H);
+  if (st != FL_OK) return st;
+  MgOptions mo{std::max(1, opt->pre_sweeps), std::max(1, opt->post_sweeps), std::max(1, opt->coarse_sweeps)};
+  ++g_kernel_launches;
+  k_init_state<<<1, 1, 0, s>>>(c->st, 1e-6, 1e-4, 1, 0, 3, 0.9);  // clears the done flag of the last solve
+  FL_CUDA(launch_apply_vcycle<T>(g, H, r, mo, &c->st->done, s));
+  FL_CUDA(launch_residual0<T>(g, H, r, rho, &c->st->done, s));
+  return FL_OK;
+}
+}  // namespace fl
 
 extern "C" {
 
@@ -1608,9 +1629,20 @@ int fl_collect_training_pairs(fl_context* c, const fl_transfer_params* tp, const
       st = rc;
       break;
     }
-    // r[0] holds b - A p_k of the capped solve (its last residual evaluation)
+    // r[0] holds b - A p_k of the capped solve (its last residual evaluation);
+    // for the composite preconditioner the input is what follows a V-cycle on it
+    const float* src = c->r[0];
+    if (opt->preconditioner == 2) {
+      const int rc2 = o.precision == 1 ? post_vcycle_residual<__nv_bfloat16>(c, &o, c->r[0], c->q, s)
+                                       : post_vcycle_residual<float>(c, &o, c->r[0], c->q, s);
+      if (rc2 != FL_OK) {
+        st = rc2;
+        break;
+      }
+      src = c->q;
+    }
     const int take = (int)std::min<uint64_t>(list.size(), capacity - w);
-    e = unet_gather(g, c->r[0], c->type, dlist, take, inputs + w * 2000, scale, s);
+    e = unet_gather(g, src, c->type, dlist, take, inputs + w * 2000, scale, s);
     if (e == cudaSuccess)
       e = unet_targets(g, p_star, c->p64, c->type, dlist, take, scale, targets + w * 512, target_mask + w * 512, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

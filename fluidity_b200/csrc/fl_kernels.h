@@ -132,13 +132,20 @@ template <typename T>
 cudaError_t launch_apply_vcycle(const GridView& g, const MgHierarchy<T>& H, const float* r, const MgOptions& opt,
                                 const int* done, cudaStream_t s);
 template <typename T>
+cudaError_t launch_residual0(const GridView& g, const MgHierarchy<T>& H, const float* r, float* rho, const int* done,
+                             cudaStream_t s);
+template <typename T>
 cudaError_t launch_residual64(const GridView& g, const MgHierarchy<T>& H, const double* b64, const double* p64,
                               float* r, float* e, double* partial, SolverState* st, cudaStream_t s);
 // Replacement preconditioner z = M(r) launched in place of the V-cycle (z is the
 // level-0 vector H.ptr[0].x, of the hierarchy's storage type).
+// A learned preconditioner inside the flexible-CG iteration. compose 0: z =
+// apply(r) in place of the V-cycle; compose 1: z = V(r), then apply adds its
+// correction computed from the V-cycle's residual r - A z into z.
 struct PrecondHook {
   cudaError_t (*apply)(void* ctx, const float* r, void* z, cudaStream_t s);
   void* ctx;
+  int compose;
 };
 
 template <typename T>

@@ -677,6 +677,38 @@ __global__ void __launch_bounds__(512 / CPT)
   }
 }
 
+// Level-0 residual of the V-cycle's iterate, rho = r - A x, one block per CTA
+// with x staged with its halo (the input of a learned correction that follows
+// the V-cycle).
+template <typename T, int CPT>
+__global__ void __launch_bounds__(512 / CPT)
+    k_residual0_tiled(GridView g, LevelPtrs<T> fp, const float* __restrict__ r, float* __restrict__ rho,
+                      const int* done) {
+  constexpr int NT = 512 / CPT;
+  if (*done) return;
+  __shared__ float sh[kShell0];
+  const int blk = blockIdx.x, t = threadIdx.x;
+  unsigned m[CPT];
+  float di[CPT], ri[CPT], xv[CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int i = blk * 512 + t + k * NT;
+    m[k] = fp.mask[i];
+    di[k] = fp.diag[i];
+    ri[k] = r[i];
+    xv[k] = ld(&fp.x[i]);
+  }
+  load_halo0<NT, 384, false>(g, blk, 0, sh, [&](int j) { return ld(&fp.x[rb_id(j)]); });
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) sh[sidx(nat_of(t + k * NT))] = xv[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int l = nat_of(t + k * NT);
+    rho[blk * 512 + t + k * NT] = (m[k] & 64u) ? ri[k] - (di[k] * xv[k] - nbr_sum0(sh, sidx(l), m[k])) : 0.0f;
+  }
+}
+
 // d = z + beta d_old and q = A d for one block, d staged with its halo; the
 // block's d.q partial goes to partial[blk].
 template <typename T, int CPT>
@@ -1743,6 +1775,14 @@ cudaError_t launch_apply_vcycle(const GridView& g, const MgHierarchy<T>& H, cons
 }
 
 template <typename T>
+cudaError_t launch_residual0(const GridView& g, const MgHierarchy<T>& H, const float* r, float* rho, const int* done,
+                             cudaStream_t s) {
+  ++g_kernel_launches;
+  k_residual0_tiled<T, kResidualCpt><<<g.nb, 512 / kResidualCpt, 0, s>>>(g, H.ptr[0], r, rho, done);
+  return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t launch_residual64(const GridView& g, const MgHierarchy<T>& H, const double* b64, const double* p64,
                               float* r, float* e, double* partial, SolverState* st, cudaStream_t s) {
   g_kernel_launches += 2;
@@ -1756,11 +1796,17 @@ cudaError_t launch_fcg_iteration(const GridView& g, const MgHierarchy<T>& H, con
                                  float* r_prev, float* d_old, float* d_new, float* q, float* e, double* partial,
                                  SolverState* st, const int* done, cudaStream_t s, const PrecondHook* hook) {
   const int n = g.nb * kBlockCells;
-  if (hook != nullptr) {
+  if (hook != nullptr && !hook->compose) {
     const cudaError_t e = hook->apply(hook->ctx, r_cur, H.ptr[0].x, s);
     if (e != cudaSuccess) return e;
   } else {
     vcycle<T>(g, H, r_cur, opt, done, s);
+    if (hook != nullptr) {  // the learned correction from the V-cycle's residual, added to z (q as scratch)
+      ++g_kernel_launches;
+      k_residual0_tiled<T, kResidualCpt><<<g.nb, 512 / kResidualCpt, 0, s>>>(g, H.ptr[0], r_cur, q, done);
+      const cudaError_t e = hook->apply(hook->ctx, q, H.ptr[0].x, s);
+      if (e != cudaSuccess) return e;
+    }
   }
   const T* z = H.ptr[0].x;
   const unsigned grid = reduce_grid(n);
@@ -1834,6 +1880,8 @@ void configure_pressure_kernels() {
                                                 const float*, double*, SolverState*, cudaStream_t);                 \
   template cudaError_t launch_apply_vcycle<T>(const GridView&, const MgHierarchy<T>&, const float*,                \
                                               const MgOptions&, const int*, cudaStream_t);                         \
+  template cudaError_t launch_residual0<T>(const GridView&, const MgHierarchy<T>&, const float*, float*, const int*, \
+                                           cudaStream_t);                                                          \
   template cudaError_t launch_residual64<T>(const GridView&, const MgHierarchy<T>&, const double*, const double*,  \
                                             float*, float*, double*, SolverState*, cudaStream_t);                  \
   template cudaError_t launch_fcg_iteration<T>(const GridView&, const MgHierarchy<T>&, const MgOptions&, float*,   \

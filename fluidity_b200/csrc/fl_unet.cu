@@ -375,6 +375,94 @@ __global__ void __launch_bounds__(1024) k_masked_mse(const float* __restrict__ y
   }
 }
 
+// Block-residual loss in one CTA of 512 threads (a thread per block cell),
+// items in order. For item b the input window holds r / s (channel 0) and the
+// cell mask (channel 1: fluid 1, air 0, solid -1) on the block plus a one-cell
+// halo; y is the network's correction on the block's 8^3 cells. With A_b the
+// level-0 pressure operator restricted to the block's fluid cells (unit
+// conductance to fluid and air neighbours, none to solid ones, the block's
+// neighbours held at zero):
+//   rho = r_b - A_b y,  loss = (1/V) sum_items |rho|^2 / D_b,
+//   d loss / d y = -(2 / (V D_b)) A_b rho   (A_b is symmetric),
+// with D_b = max(|r_b|^2, 1) (the window is scaled to max |r| = 1, so a block
+// whose residual is mostly in its halo does not weigh more than the rest),
+// over the V items whose block holds residual. The zero correction scores at
+// most 1; a network that inverts A_b on its block scores 0.
+__global__ void __launch_bounds__(512) k_block_residual_loss(const float* __restrict__ y,
+                                                             const float* __restrict__ x, int batch,
+                                                             float* __restrict__ loss, float* __restrict__ grad) {
+  __shared__ float mask[1000];
+  __shared__ float vec[512];
+  __shared__ double item_den[1024];
+  __shared__ double red[16];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int cx = t & 7, cy = (t >> 3) & 7, cz = t >> 6;
+  const int w = ((cz + 1) * 10 + (cy + 1)) * 10 + (cx + 1);
+  const int nb_w[6] = {w - 1, w + 1, w - 10, w + 10, w - 100, w + 100};
+  const bool nb_in[6] = {cx > 0, cx < 7, cy > 0, cy < 7, cz > 0, cz < 7};
+  const int nb_l[6] = {t - 1, t + 1, t - 8, t + 8, t - 64, t + 64};
+  // pass 1: |r_b|^2 per item and the number of items with residual
+  for (int b = 0; b < batch; ++b) {
+    const float* xb = x + (size_t)b * 2000;
+    const double rv = xb[1000 + w] == 1.0f ? (double)xb[w] : 0.0;
+    double v = warp_sum(rv * rv);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (t == 0) {
+      double sum = 0.0;
+      for (int k = 0; k < 16; ++k) sum += red[k];
+      item_den[b] = sum;
+    }
+  }
+  __syncthreads();
+  int valid = 0;
+  for (int b = 0; b < batch; ++b) valid += item_den[b] > 0.0;
+  double acc = 0.0;
+  // pass 2: residual after the correction, the loss and its gradient
+  for (int b = 0; b < batch; ++b) {
+    const float* xb = x + (size_t)b * 2000;
+    for (int i = t; i < 1000; i += 512) mask[i] = xb[1000 + i];
+    __syncthreads();
+    const bool fluid = mask[w] == 1.0f;
+    const float yc = fluid ? y[(size_t)b * 512 + t] : 0.0f;
+    vec[t] = yc;
+    __syncthreads();
+    float diag = 0.0f, off = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float mk = mask[nb_w[k]];
+      diag += mk >= 0.0f ? 1.0f : 0.0f;
+      if (nb_in[k] && mk == 1.0f) off += vec[nb_l[k]];
+    }
+    const float rho = fluid ? xb[w] - (diag * yc - off) : 0.0f;
+    __syncthreads();
+    vec[t] = rho;
+    __syncthreads();
+    float arho = 0.0f;
+    if (fluid) {
+      float o = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 6; ++k)
+        if (nb_in[k] && mask[nb_w[k]] == 1.0f) o += vec[nb_l[k]];
+      arho = diag * rho - o;
+    }
+    const double den = item_den[b];
+    const double scale = den > 0.0 ? 1.0 / (valid * fmax(den, 1.0)) : 0.0;
+    acc += scale * (double)rho * (double)rho;
+    if (grad) grad[(size_t)b * 512 + t] = (float)(-2.0 * scale * (double)arho);
+    __syncthreads();
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) red[warp] = acc;
+  __syncthreads();
+  if (t == 0 && loss) {
+    double total = 0.0;
+    for (int k = 0; k < 16; ++k) total += red[k];
+    *loss = (float)total;
+  }
+}
+
 __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                        float* __restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1,
                        float c2) {
@@ -606,6 +694,13 @@ cudaError_t unet_masked_mse(const float* y, const float* t, const float* m, int 
                             float* grad, cudaStream_t s) {
   ++g_kernel_launches;
   k_masked_mse<<<1, 1024, 0, s>>>(y, t, m, batch, relative, loss, grad);
+  return cudaGetLastError();
+}
+
+cudaError_t unet_block_residual_loss(const float* y, const float* x, int batch, float* loss, float* grad,
+                                     cudaStream_t s) {
+  ++g_kernel_launches;
+  k_block_residual_loss<<<1, 512, 0, s>>>(y, x, batch, loss, grad);
   return cudaGetLastError();
 }
 
@@ -841,6 +936,13 @@ int fl_unet_masked_mse(const float* output, const float* target, const float* ma
     return FL_INVALID_ARGUMENT;
   return unet_code(fl::unet_masked_mse(output, target, mask, batch, relative, loss, grad_output,
                                        static_cast<cudaStream_t>(stream)));
+}
+
+int fl_unet_block_residual_loss(const float* output, const float* input, int batch, float* loss, float* grad_output,
+                                void* stream) {
+  if (output == nullptr || input == nullptr || batch <= 0 || batch > 1024) return FL_INVALID_ARGUMENT;
+  return unet_code(fl::unet_block_residual_loss(output, input, batch, loss, grad_output,
+                                                static_cast<cudaStream_t>(stream)));
 }
 
 int fl_adam_step(float* params, const float* grads, float* m, float* v, uint64_t count, int step, float lr,

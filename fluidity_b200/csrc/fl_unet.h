@@ -37,6 +37,8 @@ cudaError_t unet_backward(const float* params, float* cache, const float* grad_y
                           cudaStream_t s);
 cudaError_t unet_masked_mse(const float* y, const float* target, const float* mask, int batch, int relative,
                             float* loss, float* grad, cudaStream_t s);
+cudaError_t unet_block_residual_loss(const float* y, const float* x, int batch, float* loss, float* grad,
+                                     cudaStream_t s);
 cudaError_t adam_step(float* p, const float* g, float* m, float* v, long long n, int step, float lr, float b1,
                       float b2, float eps, cudaStream_t s);
 cudaError_t unet_init_params(float* p, unsigned long long seed, cudaStream_t s);
@@ -71,6 +73,6 @@ cudaError_t unet_tc_pack(const float* params, __nv_bfloat16* packed, cudaStream_
 template <typename T>
 cudaError_t unet_tc_apply(const GridView& g, const float* params, const __nv_bfloat16* packed, uint4* act,
                           long long cap, float* bt, float* scale, const unsigned char* type, const float* r_rb, T* z,
-                          int* error, int sms, cudaStream_t s);
+                          int* error, int sms, cudaStream_t s, bool accumulate = false);
 
 }  // namespace fl

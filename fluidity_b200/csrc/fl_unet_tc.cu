@@ -166,6 +166,7 @@ struct ConvArgs {
   const unsigned char* type;
   void* z;                // level-0 vector (RB layout), T
   int z_bf16;
+  int z_add;              // 1: z += s y (the correction added to the V-cycle's), 0: z = s y
   int* error;             // set to 1 when an mbarrier wait gives up
 };
 
@@ -276,10 +277,13 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvArgs a) {
         const int l = (z * 8 + y) * 8 + x;
         const float v = a.type[b * 512 + l] == 1 ? a.scale[b] * yv : 0.0f;
         const int zi = b * 512 + rb_of(l);
-        if (a.z_bf16)
-          reinterpret_cast<__nv_bfloat16*>(a.z)[zi] = __float2bfloat16_rn(v);
-        else
-          reinterpret_cast<float*>(a.z)[zi] = v;
+        if (a.z_bf16) {
+          __nv_bfloat16* zp = reinterpret_cast<__nv_bfloat16*>(a.z) + zi;
+          *zp = __float2bfloat16_rn(a.z_add ? __bfloat162float(*zp) + v : v);
+        } else {
+          float* zp = reinterpret_cast<float*>(a.z) + zi;
+          *zp = a.z_add ? *zp + v : v;
+        }
       }
     }
     fence_before_sync();
@@ -520,11 +524,12 @@ cudaError_t unet_tc_pack(const float* params, __nv_bfloat16* packed, cudaStream_
   return cudaGetLastError();
 }
 
-// z = s * U(r / s) per active block through the tensor-core kernels.
+// z = s * U(r / s) per active block through the tensor-core kernels
+// (accumulate: z += s * U(r / s)).
 template <typename T>
 cudaError_t unet_tc_apply(const GridView& g, const float* params, const __nv_bfloat16* packed, uint4* act,
                           long long cap, float* bt, float* scale, const unsigned char* type, const float* r_rb, T* z,
-                          int* error, int sms, cudaStream_t s) {
+                          int* error, int sms, cudaStream_t s, bool accumulate) {
   const int nb = g.nb;
   if (nb <= 0) return cudaSuccess;
   if (nb > cap) return cudaErrorInvalidValue;
@@ -571,14 +576,15 @@ cudaError_t unet_tc_apply(const GridView& g, const float* params, const __nv_bfl
   a.in = base(L.t8); a.weights = wp(6); a.bias = params + P.bias[8]; a.out = nullptr;
   a.w_out = params + P.offset[9]; a.b_out = params + P.bias[9]; a.scale = scale; a.type = type; a.z = z;
   a.z_bf16 = sizeof(T) == 2;
+  a.z_add = accumulate ? 1 : 0;
   return launch_conv<2, 16, kToCorrection, 8, 8>(a, sms, s);
 }
 
 template cudaError_t unet_tc_apply<float>(const GridView&, const float*, const __nv_bfloat16*, uint4*, long long,
                                           float*, float*, const unsigned char*, const float*, float*, int*, int,
-                                          cudaStream_t);
+                                          cudaStream_t, bool);
 template cudaError_t unet_tc_apply<__nv_bfloat16>(const GridView&, const float*, const __nv_bfloat16*, uint4*,
                                                   long long, float*, float*, const unsigned char*, const float*,
-                                                  __nv_bfloat16*, int*, int, cudaStream_t);
+                                                  __nv_bfloat16*, int*, int, cudaStream_t, bool);
 
 }  // namespace fl

@@ -5,10 +5,13 @@ for a dam-break state, the converged pressure p* and the iterates p_k stopped
 after k flexible-CG iterations give, per block holding fluid, the input
 (r_k / s, cell mask) on the block plus a one-cell halo and the target
 (p* - p_k) / s, s = max |r_k| over the window. Training runs entirely in the
-library's kernels (fl_unet_forward / fl_unet_backward / fl_unet_masked_mse /
-fl_adam_step) on batches of 64 items with Adam at lr 1e-3 on the per-item
-relative squared error (items whose errors differ by orders of magnitude weigh
-the same); torch only holds the device buffers and draws the batch indices.
+library's kernels (fl_unet_forward / fl_unet_backward / fl_unet_block_residual_loss
+or fl_unet_masked_mse / fl_adam_step) on batches of 64 items with Adam at lr
+1e-3. The default loss is the block residual |r_b - A_b y|^2 / |r_b|^2: the
+network learns to invert the pressure operator on its block, a target it can
+see in its window (the error p* - p_k is dominated by global modes that a
+block-local network cannot see, and training on it ends at the zero
+predictor). torch only holds the device buffers and draws the batch indices.
 
     python -m fluidity_b200.learned --grid 128 --pairs 10000 --steps 2000 --out weights.npy
 """
@@ -27,10 +30,12 @@ DEFAULT_CAPS = (0, 1, 2, 3, 4, 5, 6, 8, 10, 12)
 
 
 def collect_pairs(n: int = 128, pairs: int = 10000, steps_between: int = 4, caps=DEFAULT_CAPS, precision: int = 0,
-                  seed_steps: int = 2, max_states: int = 40):
+                  seed_steps: int = 2, max_states: int = 40, after_vcycle: bool = False):
     """Dam break at n^3 (the 8-particles-per-cell scene); after `seed_steps` steps and
     then every `steps_between` steps, adds the pairs of that step's projection until
-    `pairs` items are collected. Returns device tensors (inputs, targets, masks)."""
+    `pairs` items are collected. after_vcycle: the inputs are the residuals left by
+    one V-cycle (what the composite preconditioner's network sees). Returns device
+    tensors (inputs, targets, masks)."""
     import torch
 
     soa, m = scenes.dam_break(n)
@@ -38,6 +43,8 @@ def collect_pairs(n: int = 128, pairs: int = 10000, steps_between: int = 4, caps
     ctx.upload(soa)
     params = fb.transfer_params(scenes.DT, m)
     opt = fb.default_pressure_options(precision=precision)
+    collect = fb.default_pressure_options(precision=precision)
+    collect.preconditioner = 2 if after_vcycle else 0
     inputs = torch.zeros((pairs, 2, 10, 10, 10), dtype=torch.float32, device="cuda")
     targets = torch.zeros((pairs, 512), dtype=torch.float32, device="cuda")
     masks = torch.zeros((pairs, 512), dtype=torch.float32, device="cuda")
@@ -47,7 +54,7 @@ def collect_pairs(n: int = 128, pairs: int = 10000, steps_between: int = 4, caps
     for _ in range(max_states):
         if got >= pairs:
             break
-        got += ctx.collect_training_pairs(params, opt, list(caps), inputs[got:], targets[got:], masks[got:])
+        got += ctx.collect_training_pairs(params, collect, list(caps), inputs[got:], targets[got:], masks[got:])
         for _ in range(steps_between):
             ctx.step(params, opt)
     ctx.close()
@@ -55,8 +62,11 @@ def collect_pairs(n: int = 128, pairs: int = 10000, steps_between: int = 4, caps
 
 
 def train(inputs, targets, masks, steps: int = 2000, batch: int = 64, lr: float = 1e-3, seed: int = 0,
-          params=None):
-    """Adam on the masked MSE; returns (params, losses per step)."""
+          params=None, loss_kind: str = "residual"):
+    """Adam on batches of the pairs; returns (params, losses per step).
+    loss_kind "residual": |r_b - A_b y|^2 / |r_b|^2 per item (fl_unet_block_residual_loss: the network
+    learns the inverse of the pressure operator on its block; the zero output scores 1);
+    "error": the per-item relative squared error against the targets p* - p_k (fl_unet_masked_mse)."""
     import torch
 
     n = inputs.shape[0]
@@ -87,7 +97,10 @@ def train(inputs, targets, masks, steps: int = 2000, batch: int = 64, lr: float 
         torch.index_select(targets, 0, idx, out=tb)
         torch.index_select(masks, 0, idx, out=mb)
         net.forward(P, xb, y)
-        fb.UNet.masked_mse(y, tb, mb, loss[step - 1:step], gy, relative=1)
+        if loss_kind == "residual":
+            fb.UNet.block_residual_loss(y, xb, loss[step - 1:step], gy)
+        else:
+            fb.UNet.masked_mse(y, tb, mb, loss[step - 1:step], gy, relative=1)
         net.backward(P, gy, G)
         fb.UNet.adam_step(P, G, M, V, step, lr=lr)
     torch.cuda.synchronize()

@@ -115,7 +115,9 @@ typedef struct {
                          2: from 2 p(n) - p(n-1), the last two projections' pressures (falls back to 1) */
   double rel_tol;    /* ||b - A p||_2 <= rel_tol * ||b||_2, checked in FP64 */
   double inner_rtol; /* inner FP32 solve reduction per refinement */
-  int preconditioner; /* 0: V-cycle; 1: learned block U-Net (fl_set_learned_preconditioner), V-cycle fallback */
+  int preconditioner; /* 0: V-cycle; 1: learned block U-Net (fl_set_learned_preconditioner) in place of the
+                         V-cycle, V-cycle fallback; 2: V-cycle, then the U-Net's correction from the V-cycle's
+                         residual r - A V(r) added to it, V-cycle-only fallback */
   int stall_limit;    /* learned: consecutive stalled iterations before the V-cycle takes over (0 -> 3) */
   double stall_ratio; /* learned: an iteration stalls unless ||r||_2 < stall_ratio * best so far (0 -> 0.9) */
 } fl_pressure_options;
@@ -313,6 +315,15 @@ int fl_unet_backward(fl_unet* net, const float* params, const float* grad_output
  *             sum mask (output - target)^2 / sum mask target^2. */
 int fl_unet_masked_mse(const float* output, const float* target, const float* mask, int batch, int relative,
                        float* loss, float* grad_output, void* stream);
+/* Block-residual loss of batch (<= 1024) items and d loss / d output: with
+ * r_b the input's residual on the block's fluid cells (channel 0 of the 10^3
+ * window, channel 1 the cell mask) and A_b the level-0 pressure operator on
+ * those cells (unit conductance to fluid and air neighbours, the block's
+ * neighbours held at zero), loss = mean over the items with r_b != 0 of
+ * |r_b - A_b output|^2 / max(|r_b|^2, 1) (windows scaled to max |r| = 1). The
+ * zero output scores at most 1; an exact inverse of A_b on the block scores 0. */
+int fl_unet_block_residual_loss(const float* output, const float* input, int batch, float* loss, float* grad_output,
+                                void* stream);
 /* Adam with bias correction at step >= 1: m, v updated in place, params -= lr mhat / (sqrt(vhat) + eps). */
 int fl_adam_step(float* params, const float* grads, float* m, float* v, uint64_t count, int step, float lr,
                  float beta1, float beta2, float eps, void* stream);
@@ -323,7 +334,10 @@ int fl_adam_step(float* params, const float* grads, float* m, float* v, uint64_t
  * flexible-CG iterations and every block holding fluid yields one item:
  * input = (r_k / s, mask) on the block plus halo, target = (p* - p_k) / s,
  * target_mask = fluid cells, with r_k = b - A p_k and s = max |r_k| over the
- * input window. Writes at most `capacity` items; `written` gets the count. */
+ * input window. With options->preconditioner == 2 the input residual is the
+ * one the composite preconditioner's network sees, r_k - A V(r_k) after one
+ * V-cycle V (the target stays p* - p_k). Writes at most `capacity` items;
+ * `written` gets the count. */
 int fl_collect_training_pairs(fl_context* ctx, const fl_transfer_params* params, const fl_pressure_options* options,
                               const int32_t* iterations, int iteration_count, float* inputs, float* targets,
                               float* target_mask, uint64_t capacity, uint64_t* written);

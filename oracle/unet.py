@@ -209,6 +209,54 @@ def masked_mse(y, target, mask, relative=False):
     return float((d * d * w).sum()), 2.0 * d * w
 
 
+def block_operator(mask):
+    """A_b of one item as a dense (512, 512) matrix over the block's cells: the
+    level-0 pressure operator on the block's fluid cells (unit conductance to
+    fluid and air neighbours, none to solid ones), the block's neighbours held
+    at zero; rows and columns of non-fluid cells are zero. mask: (10, 10, 10)."""
+    A = np.zeros((512, 512))
+    for cz in range(8):
+        for cy in range(8):
+            for cx in range(8):
+                c = (cz * 8 + cy) * 8 + cx
+                if mask[cz + 1, cy + 1, cx + 1] != 1.0:
+                    continue
+                for dz, dy, dx in ((0, 0, -1), (0, 0, 1), (0, -1, 0), (0, 1, 0), (-1, 0, 0), (1, 0, 0)):
+                    mk = mask[cz + 1 + dz, cy + 1 + dy, cx + 1 + dx]
+                    if mk >= 0.0:
+                        A[c, c] += 1.0
+                    nz, ny, nx = cz + dz, cy + dy, cx + dx
+                    if mk == 1.0 and 0 <= nz < 8 and 0 <= ny < 8 and 0 <= nx < 8:
+                        A[c, (nz * 8 + ny) * 8 + nx] -= 1.0
+    return A
+
+
+def block_residual_loss(y, x):
+    """Loss (1/V) sum |r_b - A_b y|^2 / max(|r_b|^2, 1) over the V items with
+    r_b != 0 and its gradient with respect to y. y: (batch, 512); x: (batch, 2,
+    10, 10, 10), the window scaled to max |r| = 1."""
+    batch = y.shape[0]
+    ops, rs = [], []
+    for b in range(batch):
+        mask = x[b, 1]
+        r = np.where(mask == 1.0, x[b, 0], 0.0)[1:9, 1:9, 1:9].reshape(512)
+        ops.append(block_operator(mask))
+        rs.append(r)
+    dens = np.array([r @ r for r in rs])
+    valid = int((dens > 0).sum())
+    loss, grad = 0.0, np.zeros_like(y, dtype=np.float64)
+    for b in range(batch):
+        if dens[b] <= 0:
+            continue
+        fluid = np.diag(ops[b]) > 0
+        yb = np.where(fluid, y[b], 0.0)
+        rho = np.where(fluid, rs[b] - ops[b] @ yb, 0.0)
+        den = valid * max(dens[b], 1.0)
+        loss += (rho @ rho) / den
+        grad[b] = -2.0 * (ops[b] @ rho) / den
+    return loss, grad
+
+
 def adam(theta, grad, m, v, step, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
     m = b1 * m + (1 - b1) * grad
     v = b2 * v + (1 - b2) * grad * grad

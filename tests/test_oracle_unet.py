@@ -67,3 +67,25 @@ def test_masked_mse_gradient_and_adam():
     th, gr = rng.normal(size=10), rng.normal(size=10)
     th1, m1, v1 = U.adam(th, gr, np.zeros(10), np.zeros(10), 1)
     np.testing.assert_allclose(th1, th - 1e-3 * np.sign(gr), rtol=0, atol=1e-9)  # first step moves lr*sign(g)
+
+
+def test_block_residual_loss_gradient_matches_finite_differences():
+    """The block-residual loss of the learned preconditioner (oracle restatement
+    of fl_unet_block_residual_loss): gradient by central differences, and the
+    zero correction scores |r_b|^2 / max(|r_b|^2, 1) <= 1."""
+    rng = np.random.default_rng(3)
+    x = np.zeros((3, 2, 10, 10, 10))
+    x[:, 0] = rng.normal(size=(3, 10, 10, 10))
+    x[:, 1] = rng.choice([1.0, 0.0, -1.0], p=[0.7, 0.2, 0.1], size=(3, 10, 10, 10))
+    y = rng.normal(size=(3, 512))
+    loss, grad = U.block_residual_loss(y, x)
+    eps = 1e-6
+    for k in rng.choice(3 * 512, 12, replace=False):
+        b, c = divmod(int(k), 512)
+        yp, ym = y.copy(), y.copy()
+        yp[b, c] += eps
+        ym[b, c] -= eps
+        fd = (U.block_residual_loss(yp, x)[0] - U.block_residual_loss(ym, x)[0]) / (2 * eps)
+        assert abs(fd - grad[b, c]) <= 1e-7 * np.abs(grad).max()
+    zero, _ = U.block_residual_loss(np.zeros_like(y), x)
+    assert 0.0 < zero <= 1.0
