@@ -153,6 +153,8 @@ def library():
                                                    ctypes.POINTER(Report)]
         lib.fl_p2g.argtypes = [vp, ctypes.POINTER(Particles), ctypes.POINTER(TransferParams), ctypes.c_int,
                                vp * 3, vp * 3, vp, ctypes.POINTER(Report)]
+        lib.fl_p2g_normalized.argtypes = [vp, ctypes.POINTER(Particles), ctypes.POINTER(TransferParams), vp * 3,
+                                          vp * 3, vp * 3, vp, ctypes.POINTER(Report)]
         lib.fl_p2g_static_scratch.argtypes = [ctypes.POINTER(StaticGrid), ctypes.POINTER(Particles),
                                               ctypes.POINTER(TransferParams), ctypes.c_int, vp * 3, vp * 3, vp,
                                               ctypes.POINTER(Report)]

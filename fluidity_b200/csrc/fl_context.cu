@@ -1117,7 +1117,8 @@ int fl_sort_particles_by_block(fl_context* c, const fl_particles* in, fl_particl
 // P2G of the particles in cell order: slot q is particle q of `parts`, or
 // particle order[q] when an order is given (the step, which skips the permutation).
 static int p2g_impl(fl_context* c, const fl_particles* parts, const unsigned int* order, const fl_transfer_params* tp,
-                    int mode, float* const out0[3], float* const out1[3], cudaStream_t s, fl_report* report) {
+                    int mode, float* const out0[3], float* const out1[3], cudaStream_t s, fl_report* report,
+                    uint8_t* const validity[3] = nullptr) {
   reset_report(c, s);
   GridView g = view(c);
   ParticlesView pv = pview(parts);
@@ -1128,6 +1129,7 @@ static int p2g_impl(fl_context* c, const fl_particles* parts, const unsigned int
   prm.min_face_mass = (float)tp->min_face_mass;
   prm.dt = (float)tp->dt;
   for (int d = 0; d < 3; ++d) prm.gravity[d] = (float)tp->gravity[d];
+  for (int d = 0; d < 3; ++d) prm.validity[d] = validity ? validity[d] : nullptr;
   float* o1[3] = {out1 ? out1[0] : nullptr, out1 ? out1[1] : nullptr, out1 ? out1[2] : nullptr};
   FL_CUDA(launch_p2g(g, pv, c->cell_start, c->tiles, prm, out0, o1, c->rep, s, order));
   if (report) return read_report(c, s, report);
@@ -1138,6 +1140,14 @@ int fl_p2g(fl_context* c, const fl_particles* sorted, const fl_transfer_params* 
            float* const out1[3], void* stream, fl_report* report) {
   if (!c || !sorted || !tp || !out0 || (mode == 0 && !out1)) return FL_INVALID_ARGUMENT;
   return p2g_impl(c, sorted, nullptr, tp, mode, out0, out1, (cudaStream_t)stream, report);
+}
+
+int fl_p2g_normalized(fl_context* c, const fl_particles* sorted, const fl_transfer_params* tp, float* const u_pred[3],
+                      float* const face_mass[3], uint8_t* const validity[3], void* stream, fl_report* report) {
+  if (!c || !sorted || !tp || !u_pred || !validity) return FL_INVALID_ARGUMENT;
+  for (int a = 0; a < 3; ++a)
+    if (!u_pred[a] || !validity[a] || (face_mass && !face_mass[a])) return FL_INVALID_ARGUMENT;
+  return p2g_impl(c, sorted, nullptr, tp, 1, u_pred, face_mass, (cudaStream_t)stream, report, validity);
 }
 
 int fl_pressure_project(fl_context* c, const float* const u_pred[3], float* const u_new[3],

@@ -17,7 +17,11 @@ struct P2GMergeParams {
   float min_face_mass;  // NormalizeCore threshold
   float dt;
   float gravity[3];
+  unsigned char* validity[3];  // mode 1: NormalizeCore's per-face validity when not null
 };
+
+// LiquidFaceValidity3D (liquid_boundary_transfer_types_3d.h:37-42).
+enum FaceValidity : unsigned char { kFaceMissing = 0, kFaceValid = 1, kFacePredicted = 2, kFaceLowMass = 3 };
 
 struct G2PParams {
   float dt;

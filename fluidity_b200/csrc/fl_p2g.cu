@@ -345,6 +345,10 @@ __global__ void __launch_bounds__(kBlockCells)
   }
   float u = 0.0f;
   if (mass != 0.0f && mass > prm.min_face_mass) u = Q / W;
+  // NormalizeCore's validity (liquid_boundary_transfer_3d.cc:486-510): no
+  // mass -> missing, positive mass at or below the minimum -> low mass
+  if (prm.validity[a] != nullptr)
+    prm.validity[a][slot] = mass == 0.0f ? kFaceMissing : (mass <= prm.min_face_mass ? kFaceLowMass : kFaceValid);
   u += prm.dt * prm.gravity[a];
   const int head[3] = {g.coord[3 * b] * 8 + loc[0], g.coord[3 * b + 1] * 8 + loc[1], g.coord[3 * b + 2] * 8 + loc[2]};
   int tail[3] = {head[0], head[1], head[2]};

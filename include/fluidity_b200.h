@@ -167,6 +167,16 @@ int fl_sort_particles_by_block(fl_context* ctx, const fl_particles* in, fl_parti
 int fl_p2g(fl_context* ctx, const fl_particles* sorted, const fl_transfer_params* params, int mode,
            float* const out0[3], float* const out1[3], void* stream, fl_report* report);
 
+/* fl_p2g mode 1 (NormalizeLiquidMacFaces3D + ApplyForces + stationary walls)
+ * that also writes NormalizeCore's per-face validity, one byte per face
+ * (LiquidFaceValidity3D numbering: 0 missing = no mass, 1 valid, 3 low mass =
+ * positive mass at or below min_face_mass; liquid_boundary_transfer_3d.cc:
+ * 785-805, validity 486-510), so a consumer can tell a face without liquid
+ * from one whose normalized velocity is zero. face_mass may be NULL. */
+int fl_p2g_normalized(fl_context* ctx, const fl_particles* sorted, const fl_transfer_params* params,
+                      float* const u_pred[3], float* const face_mass[3], uint8_t* const validity[3], void* stream,
+                      fl_report* report);
+
 /* Pressure projection of the predicted face velocities of the box scene:
  * fluid = non-solid cells holding particles (from the last sort), Dirichlet
  * p = 0 against air, sealed against solid cells. Writes corrected velocities

@@ -166,6 +166,8 @@ def ref():
                                                   ctypes.c_size_t, _lp, _lp]
         lib.ref_gather_mac_3d.argtypes = [_dp, ctypes.c_double, _ip, ctypes.c_size_t, _dp, ctypes.c_size_t,
                                           _dp, _dp, _dp]
+        lib.ref_normalize_liquid_mac_faces_3d.argtypes = [_lp, _lp, ctypes.c_size_t, ctypes.c_double, ctypes.c_double,
+                                                          ctypes.c_size_t, ctypes.c_double, _dp, _dp, _u8p]
         lib.ref_project_mac_pressure_3d.argtypes = [
             _dp, ctypes.c_double, _ip, ctypes.c_size_t, ctypes.c_double, _ip, _dp, ctypes.c_size_t, _ip, _ip,
             _dp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_double, _dp, _dp, _dp, _dp, _dp, _dp]
@@ -399,6 +401,18 @@ def ref_deposit_quanta(origin, h, blocks, particles, mass_per_quantum, momentum_
                                          float(mass_per_quantum), float(momentum_per_quantum), int(capacity), _l(m),
                                          _l(q)), "DepositMacQuanta3D")
     return m, q
+
+
+def ref_normalize(mass_q, momentum_q, mass_per_quantum, momentum_per_quantum, capacity, minimum_face_mass):
+    """NormalizeLiquidMacFaces3D: decoded face masses, velocities and validity bytes."""
+    lib = ref()
+    mq, pq = np.ascontiguousarray(mass_q, np.int64), np.ascontiguousarray(momentum_q, np.int64)
+    n = len(mq)
+    m, u, val = np.zeros(n), np.zeros(n), np.zeros(n, np.uint8)
+    _check(lib.ref_normalize_liquid_mac_faces_3d(_l(mq), _l(pq), n, float(mass_per_quantum), float(momentum_per_quantum),
+                                                 int(capacity), float(minimum_face_mass), _d(m), _d(u), _u8(val)),
+           "NormalizeLiquidMacFaces3D")
+    return m, u, val
 
 
 def ref_gather(origin, h, blocks, particles, old_u, new_u):

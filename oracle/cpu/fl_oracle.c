@@ -222,13 +222,13 @@ void fo_normalize_forces(const fo_box* b, double* face_mass[3], double* face_mom
     for (size_t f = 0; f < nf; ++f) {
       const double m = face_mass[a][f];
       double u = 0.0;
-      uint8_t valid = 0;
+      uint8_t valid = 0; /* LiquidFaceValidity3D: 0 missing, 1 valid, 3 low mass */
       if (m != 0.0) {
         if (m <= m_min) {
-          valid = 1;
+          valid = 3;
         } else {
           u = face_momentum[a][f] / m;
-          valid = 2;
+          valid = 1;
         }
       }
       if (validity) validity[a][f] = valid;

@@ -48,7 +48,8 @@ int fo_p2g_quanta(const fo_box* box, const double* x, const double* v, const dou
                   int mass_stride, size_t np, double mass_per_quantum, double momentum_per_quantum,
                   int64_t* mass_q[3], int64_t* momentum_q[3]);
 
-/* Normalize (u = q/m when m > m_min) and add dt*g on every face. validity: 0 missing, 1 low mass, 2 valid. */
+/* Normalize (u = q/m when m > m_min) and add dt*g on every face. validity (LiquidFaceValidity3D):
+ * 0 missing (no mass), 1 valid, 3 low mass (positive mass at or below m_min). */
 void fo_normalize_forces(const fo_box* box, double* face_mass[3], double* face_momentum[3], double m_min, double dt,
                          const double g[3], double* u_pred[3], uint8_t* validity[3]);
 

@@ -11,6 +11,7 @@
 //   BuildMacFaceGeometryStencil3D                   native/src/sparse_mac_grid_3d.cc:451-548
 //   DepositMac3D / DepositMacQuanta3D / GatherMac3D native/src/transfers_3d.cc:139-261
 //   ProjectMacPressure3D                            native/src/mac_pressure_3d.cc:6-39
+//   NormalizeLiquidMacFaces3D                       native/src/liquid_boundary_transfer_3d.cc:785-805
 // Every function returns the absl status code as int (0 = OK).
 
 #include <algorithm>
@@ -20,6 +21,7 @@
 #include <span>
 #include <vector>
 
+#include "fluidity/host/liquid_boundary_transfer_3d.h"
 #include "fluidity/host/mac_pressure_3d.h"
 #include "fluidity/host/sparse_mac_grid_3d.h"
 #include "fluidity/host/transfers_3d.h"
@@ -145,6 +147,24 @@ int ref_deposit_mac_quanta_3d(const double origin[3], double h, const int32_t* b
   for (size_t i = 0; i < faces.size(); ++i) {
     out_mass_q[i] = faces[i].mass_quanta_sum;
     out_momentum_q[i] = faces[i].pure_momentum_quanta_sum;
+  }
+  return 0;
+}
+
+// NormalizeLiquidMacFaces3D on per-face quanta (stress channel zero): face
+// masses, velocities and validity (LiquidFaceValidity3D as bytes).
+extern "C" int ref_normalize_liquid_mac_faces_3d(const int64_t* mass_q, const int64_t* momentum_q, size_t nf,
+                                                 double mass_per_quantum, double momentum_per_quantum,
+                                                 size_t capacity, double minimum_face_mass, double* out_mass,
+                                                 double* out_velocity, uint8_t* out_validity) {
+  std::vector<MacFaceDepositQuanta3D> faces(nf);
+  for (size_t i = 0; i < nf; ++i) faces[i] = {mass_q[i], momentum_q[i], 0};
+  auto r = NormalizeLiquidMacFaces3D(faces, {mass_per_quantum, momentum_per_quantum, capacity}, minimum_face_mass);
+  if (!r.ok()) return Code(r.status());
+  for (size_t i = 0; i < nf; ++i) {
+    out_mass[i] = r->face_masses[i];
+    out_velocity[i] = r->face_velocities[i];
+    out_validity[i] = static_cast<uint8_t>(r->validity[i]);
   }
   return 0;
 }

@@ -162,3 +162,65 @@ def test_rejections_preserve_error_codes():
 def test_empty_batch_clears_faces():
     m, q, _ = fb.deposit_mac_3d([0, 0, 0], 1.0, CORNER_BLOCKS, np.zeros((0, 19)))
     assert np.all(m == 0) and np.all(q == 0) and len(m) == 192 * 8
+
+
+def test_normalized_p2g_reports_face_validity():
+    """fl_p2g_normalized on the sorted 32^3 dam break with a minimum face mass
+    that makes part of the faces low-mass: the validity bytes equal the FP64
+    restatement's NormalizeCore validity (pinned against the reference's
+    NormalizeLiquidMacFaces3D), and the velocities the fused normalize's."""
+    import ctypes
+
+    import torch
+
+    from fluidity_b200 import scenes
+    from helpers import box_for, soa_to_xvc
+
+    n = 32
+    soa, mass = scenes.dam_break(n)
+    count = soa.shape[1]
+    ctx = fb.LiquidContext(n, capacity=count)
+    src = [torch.from_numpy(np.ascontiguousarray(soa[k])).cuda() for k in range(15)]
+    dst = [torch.empty_like(t) for t in src]
+
+    def parts(ts):
+        p = fb.Particles()
+        for d in range(3):
+            p.x[d], p.v[d] = ts[d].data_ptr(), ts[3 + d].data_ptr()
+        for d in range(9):
+            p.c[d] = ts[6 + d].data_ptr()
+        p.mass, p.count = None, count
+        return p
+
+    lib, rep = fb.library(), fb.Report()
+    pin, pout = parts(src), parts(dst)
+    assert lib.fl_topology_from_particles(ctx.handle, ctypes.byref(pin), None, ctypes.byref(rep)) == fb.OK
+    assert lib.fl_sort_particles_by_block(ctx.handle, ctypes.byref(pin), ctypes.byref(pout), None,
+                                          ctypes.byref(rep)) == fb.OK
+    blocks = ctx.active_blocks()
+    nb = len(blocks)
+    # the FP64 face masses; a threshold between two well-separated masses
+    x, v, c = soa_to_xvc(soa)
+    box = box_for(n)
+    fm, fq = oracle.p2g(box, x, v, c, mass)
+    masses = np.unique(np.concatenate([a[a > 0] for a in fm]))
+    gaps = np.nonzero(masses[1:] > masses[:-1] * (1 + 1e-3))[0]
+    k = gaps[np.searchsorted(gaps, len(masses) // 4)]
+    m_min = 0.5 * (masses[k] + masses[k + 1])
+    tp = fb.transfer_params(scenes.DT, mass, min_face_mass=m_min)
+    u = [torch.zeros(nb * 512, device="cuda") for _ in range(3)]
+    fmass = [torch.zeros(nb * 512, device="cuda") for _ in range(3)]
+    val = [torch.full((nb * 512,), 200, dtype=torch.uint8, device="cuda") for _ in range(3)]
+    arr = lambda ts: (ctypes.c_void_p * 3)(*[t.data_ptr() for t in ts])
+    assert lib.fl_p2g_normalized(ctx.handle, ctypes.byref(pout), ctypes.byref(tp), arr(u), arr(fmass), arr(val), None,
+                                 ctypes.byref(rep)) == fb.OK and rep.error == 0
+    want_u, want_val = oracle.normalize_forces(box, fm, fq, m_min, scenes.DT, scenes.GRAVITY)
+    seen = set()
+    for a in range(3):
+        got = fb.sparse_faces_to_dense(blocks, val[a].cpu().numpy(), (n, n, n), a, fill=255)
+        have = got != 255
+        np.testing.assert_array_equal(got[have], want_val[a][have])
+        assert np.all(want_val[a][~have] == 0)  # faces outside the active blocks have no mass
+        seen |= set(np.unique(got[have]).tolist())
+    assert seen == {0, 1, 3}
+    ctx.close()

@@ -112,6 +112,31 @@ def test_quanta_restatement_matches_reference_bitwise():
         np.testing.assert_array_equal(pq[a], pq2[a])
 
 
+@needs_ref
+def test_normalize_restatement_matches_reference():
+    """The restatement's normalize (fo_normalize_forces with dt = 0) against the
+    reference's NormalizeLiquidMacFaces3D on the same decoded deposits: equal
+    masses and velocities, and the same per-face validity (0 missing, 1 valid,
+    3 low mass), with a threshold that makes some faces low-mass."""
+    rng = np.random.default_rng(7)
+    x, v, c, m = _random_particles(300, rng)
+    box = oracle.Box.make([0, 0, 0], 1.0, [0, 0, 0], [12, 12, 12])
+    ms, ps = 2.0 ** -30, 2.0 ** -24
+    mq, pq = oracle.p2g_quanta(box, x, v, c, m, ms, ps)
+    m_min = float(np.quantile(np.concatenate([a[a > 0] for a in mq]) * ms, 0.2))
+    fm = [a.astype(np.float64) * ms for a in mq]
+    fq = [a.astype(np.float64) * ps for a in pq]
+    u, valid = oracle.normalize_forces(box, fm, fq, m_min, 0.0, [0.0, 0.0, 0.0])
+    seen = set()
+    for a in range(3):
+        rm, ru, rv = oracle.ref_normalize(mq[a].ravel(), pq[a].ravel(), ms, ps, len(x), m_min)
+        np.testing.assert_array_equal(fm[a].ravel(), rm)
+        np.testing.assert_allclose(u[a].ravel(), ru, rtol=1e-15, atol=0)
+        np.testing.assert_array_equal(valid[a].ravel(), rv)
+        seen |= set(np.unique(rv).tolist())
+    assert seen == {0, 1, 3}
+
+
 def test_quanta_ties_round_to_even():
     """Known answers of the reference's tie test (test_transfers_3d.cc:800-862):
     at the X face (3,-1,3) of a particle at (3.5, 0, 4) each axis weight is 1/2."""
