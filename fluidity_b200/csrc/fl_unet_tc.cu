@@ -217,19 +217,24 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvArgs a) {
     __syncthreads();
     if (tid == 0) {
       fence_after_sync();
+      // The descriptors' start-address field (bits 0-13) counts 16-byte rows,
+      // so each tap's operands are the tile's base descriptors plus constant
+      // row offsets (every address stays below 256 KB: no carry out of the
+      // field; the static_assert above keeps shifted rows inside the column).
+      const uint64_t a0 = smem_desc(a_addr + (uint32_t)IN.r_lo * 16u, KG >= 2 ? GROUP_BYTES : 0u, 128u);
+      const uint64_t b0 = smem_desc(w_addr, N * 16u, 128u);
 #pragma unroll 1
       for (int t = 0; t < TILES; ++t) {
-        const int row0 = IN.r_lo + 128 * t;
-#pragma unroll 1
+        const uint64_t at = a0 + (uint64_t)(128 * t);
+        const uint32_t dt = tmem + (uint32_t)(t * N);
+#pragma unroll
         for (int tap = 0; tap < 27; ++tap) {
-          const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-          const int row = row0 + (dz * IN.Py + dy) * IN.Px + dx;
+          const int shift = ((tap / 9 - 1) * IN.Py + ((tap / 3) % 3 - 1)) * IN.Px + (tap % 3 - 1);
 #pragma unroll
           for (int kc = 0; kc < KC; ++kc) {
-            const uint64_t ad = smem_desc(a_addr + (uint32_t)(2 * kc) * GROUP_BYTES + (uint32_t)row * 16u,
-                                          KG >= 2 ? GROUP_BYTES : 0u, 128u);
-            const uint64_t bd = smem_desc(w_addr + (uint32_t)(tap * KC + kc) * (2u * N * 16u), N * 16u, 128u);
-            mma_bf16(tmem + (uint32_t)(t * N), ad, bd, IDESC, (tap | kc) != 0 ? 1u : 0u);
+            const uint64_t ad = at + (uint64_t)(int64_t)(shift + 2 * kc * IN.rows);
+            const uint64_t bd = b0 + (uint64_t)((tap * KC + kc) * 2 * N);
+            mma_bf16(dt, ad, bd, IDESC, (tap | kc) != 0 ? 1u : 0u);
           }
         }
       }
