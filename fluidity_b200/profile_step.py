@@ -1,12 +1,15 @@
 """Runs a few liquid substeps of a seeded scene, for profiling (ncu, CUDA events).
 
     python -m fluidity_b200.profile_step --scene splash --grid 256 --steps 2 [--precision 1] [--levels 0]
-        [--warm-start 1] [--inner-rtol 1e-3] [--snapshot]
+        [--warm-start 1] [--inner-rtol 1e-3] [--snapshot] [--unet N]
 
 Prints, per step, the status, FCG iterations, FP64 relative residual, the
 CUDA-event phase times (topology+sort, P2G, pressure, G2P; ms) and the running
 kernel-launch counts. With --snapshot every step's state also goes through the
 asynchronous snapshot queue (device check + D2H), whose copy time is printed.
+With --unet N the learned preconditioner (He-uniform weights, seed 1) is then
+applied to a random vector on the last step's cells through the tensor-core
+kernels: 3 untimed applications, then N timed with CUDA events.
 """
 
 from __future__ import annotations
@@ -27,6 +30,7 @@ def main():
     ap.add_argument("--warm-start", type=int, default=1)
     ap.add_argument("--inner-rtol", type=float, default=1e-3)
     ap.add_argument("--snapshot", action="store_true")
+    ap.add_argument("--unet", type=int, default=0)
     args = ap.parse_args()
     soa, mass = scenes.SCENES[args.scene](args.grid)
     ctx = fb.LiquidContext(args.grid, capacity=soa.shape[1])
@@ -47,6 +51,27 @@ def main():
             queue.release(t)
     if queue is not None:
         queue.close()
+    if args.unet > 0:
+        import torch
+
+        params = torch.empty(fb.UNet.param_count(), dtype=torch.float32, device="cuda")
+        fb.UNet.init_params(params, 1)
+        ctx.set_learned_preconditioner(params)
+        nb = len(ctx.active_blocks())
+        r = torch.randn(nb * 512, device="cuda", generator=torch.Generator(device="cuda").manual_seed(0))
+        z = torch.zeros_like(r)
+        for _ in range(3):
+            ctx.apply_learned(r, z, kernels=0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.unet):
+            ctx.apply_learned(r, z, kernels=0)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.unet
+        print(f"unet {nb} blocks {ms:.4f} ms per application, {nb * 25.6e6 / (ms * 1e-3) / 1e12:.1f} TFLOP/s",
+              flush=True)
     ctx.close()
 
 
