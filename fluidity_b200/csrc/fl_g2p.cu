@@ -97,6 +97,27 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
       continue;
     }
     float vel[3], fit[9], inc[3], grad[9];
+    // Step mode: the cell-centred factors of each axis (shift 1/2) serve the
+    // two components transverse to it, so they are formed once per particle;
+    // only the normal axis's face-centred factors are formed per component.
+    int firstC[3];
+    float wC[3][3], wrC[3][3];
+    if (!kFull) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float fst = floorf(X[d] - 1.0f);
+        firstC[d] = (int)fst;
+        const float a0 = fst + 0.5f;
+        const float dl = X[d] - (a0 + 0.5f);
+        const float dr = fabsf(X[d] - (a0 + 1.5f));
+        const float c = X[d] - (a0 + 1.0f);
+        wC[d][0] = 0.5f * dr * dr;
+        wC[d][1] = 0.75f - c * c;
+        wC[d][2] = 0.5f * dl * dl;
+#pragma unroll
+        for (int s = 0; s < 3; ++s) wrC[d][s] = wC[d][s] * ((a0 + (float)s) - X[d]);
+      }
+    }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       // Axis factors: first node, weights, normalized derivative and offset/h.
@@ -104,6 +125,12 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
       float w[3][3], dw[3][3], r[3][3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
+        if (!kFull && d != a) {
+          first[d] = firstC[d];
+#pragma unroll
+          for (int s = 0; s < 3; ++s) w[d][s] = wC[d][s], r[d][s] = 0.0f, dw[d][s] = 0.0f;
+          continue;
+        }
         const float shift = d == a ? 0.0f : 0.5f;
         const float fst = floorf(X[d] - shift - 0.5f);
         first[d] = (int)fst;
@@ -132,7 +159,7 @@ __global__ void __launch_bounds__(kG2PThreads, kG2PMinBlocks)
 #pragma unroll
       for (int d = 0; d < 3; ++d)
 #pragma unroll
-        for (int s = 0; s < 3; ++s) wr[d][s] = w[d][s] * r[d][s];
+        for (int s = 0; s < 3; ++s) wr[d][s] = (!kFull && d != a) ? wrC[d][s] : w[d][s] * r[d][s];
       float pic = 0.0f, old = 0.0f, m0 = 0.0f, m1 = 0.0f, m2 = 0.0f, g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
       if (!kFull) {
         // Step mode, with the pairs (U0, U1), (V0, V1), (pic, m0) and (m1, m2)
