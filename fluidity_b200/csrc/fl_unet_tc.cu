@@ -92,6 +92,16 @@ __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fenc
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// One contiguous global -> shared copy through the bulk-copy engine (no
+// multicast; this GPU's own memory), completing on `mbar` as transaction bytes.
+// Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+
 __device__ __forceinline__ void mbar_init(uint32_t mbar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -194,10 +204,15 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvArgs a) {
   uint4* a_s = reinterpret_cast<uint4*>(smem + W_BYTES);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + W_BYTES + A_BYTES);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + W_BYTES + A_BYTES + 8);
+  uint64_t* abar = reinterpret_cast<uint64_t*>(smem + W_BYTES + A_BYTES + 16);  // operand copy done
+  static_assert(W_BYTES % 16 == 0 && A_BYTES % 16 == 0, "bulk copies need 16-byte alignment and sizes");
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (uint32_t i = tid; i < W_BYTES / 16; i += kTcThreads) w_s[i] = a.weights[i];
-  if (tid == 0) mbar_init(smem_u32(mbar));
+  if (tid == 0) {
+    mbar_init(smem_u32(mbar));
+    mbar_init(smem_u32(abar));
+  }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"((uint32_t)NCOLS));
@@ -208,13 +223,21 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvArgs a) {
   fence_after_sync();
   const uint32_t tmem = *tmem_slot;
   const uint32_t w_addr = smem_u32(w_s), a_addr = smem_u32(a_s), mbar_addr = smem_u32(mbar);
+  const uint32_t abar_addr = smem_u32(abar);
+  fence_async_smem();  // the weights, stored by the threads, before the MMAs read them
 
-  uint32_t parity = 0;
+  uint32_t parity = 0, aparity = 0;
   for (int b = blockIdx.x; b < a.nb; b += gridDim.x) {
-    const uint4* src = a.in + (size_t)b * (KG * IN.rows);
-    for (int i = tid; i < KG * IN.rows; i += kTcThreads) a_s[i] = src[i];
-    fence_async_smem();
-    __syncthreads();
+    // the block's operand columns: one bulk copy (the previous block's MMAs
+    // have completed: their commit was waited for before its epilogue)
+    if (tid == 0) bulk_copy_g2s(a_addr, a.in + (size_t)b * (KG * IN.rows), A_BYTES, abar_addr);
+    const bool copied = mbar_wait(abar_addr, aparity);
+    if (__syncthreads_or(!copied)) {
+      mbar_wait(abar_addr, aparity);  // one more bounded wait for the copy in flight
+      if (tid == 0) atomicExch(a.error, 1);
+      break;
+    }
+    aparity ^= 1u;
     if (tid == 0) {
       fence_after_sync();
       // The descriptors' start-address field (bits 0-13) counts 16-byte rows,
@@ -460,7 +483,7 @@ template <int KG, int N, int MODE, int IN_KIND, int OUT_KIND>
 constexpr size_t conv_smem() {
   constexpr PadGeom IN = IN_KIND == 10 ? geom10() : (IN_KIND == 8 ? geom8() : (IN_KIND == 4 ? geom4() : geom2()));
   constexpr int KC = KG >= 2 ? KG / 2 : 1;
-  constexpr size_t bytes = 27u * KC * 2u * N * 16u + (size_t)KG * IN.rows * 16u + 16;
+  constexpr size_t bytes = 27u * KC * 2u * N * 16u + (size_t)KG * IN.rows * 16u + 32;
   constexpr int COLS = IN.tiles * N;
   // kernels holding 128 TMEM columns ask for enough shared memory that at most
   // four are resident per SM (4 x 128 = the 512 columns), so no allocation waits
