@@ -236,10 +236,11 @@ __device__ __forceinline__ void block_tile(const float2* wtiles, float2* tile, i
 __global__ void __launch_bounds__(kP2GThreads, 1)
     k_p2g_tile(GridView g, ParticlesView p, const unsigned int* order, const int* cell_start, float2* tiles,
                DeviceReport* rep) {
-  // Two sets of warp tiles, alternating between components, so one barrier
-  // per component separates a set's writers from its readers.
+  // One set of warp tiles per component: each warp runs the three components'
+  // particle loops back to back and the CTA meets at a single barrier before
+  // the block tiles are summed, so a warp with few particles does not wait at
+  // every component.
   extern __shared__ float2 wt_smem[];
-  float2* wtiles[2] = {wt_smem, wt_smem + kP2GWarps * kWarpTileMax};
   const int b = blockIdx.x;
   const int t = threadIdx.x;
   const int base = b * kBlockCells;
@@ -251,31 +252,26 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
   const int pbeg = cell_start[base + t], pend = cell_start[base + t + 1];
   const int cell[3] = {g.coord[3 * b] * 8 + (t & 7), g.coord[3 * b + 1] * 8 + ((t >> 3) & 7),
                        g.coord[3 * b + 2] * 8 + (t >> 6)};
-  float2* wt = nullptr;
+  const int wofs = (t >> 5) * kWarpTileMax;
   {
     float2 accW[kSlots / 2], accQ[kSlots / 2];
     p2g_component<0>(g, p, order, pbeg, pend, cell, accW, accQ, rep);
-    wt = wtiles[0] + (t >> 5) * kWarpTileMax;
-    warp_tile<0>(accW, accQ, wt, t & 31);
+    warp_tile<0>(accW, accQ, wt_smem + wofs, t & 31);
   }
-  __syncthreads();
-  block_tile<0>(wtiles[0], tile, t);
   {
     float2 accW[kSlots / 2], accQ[kSlots / 2];
     p2g_component<1>(g, p, order, pbeg, pend, cell, accW, accQ, rep);
-    wt = wtiles[1] + (t >> 5) * kWarpTileMax;
-    warp_tile<1>(accW, accQ, wt, t & 31);
+    warp_tile<1>(accW, accQ, wt_smem + kP2GWarps * kWarpTileMax + wofs, t & 31);
   }
-  __syncthreads();
-  block_tile<1>(wtiles[1], tile + kTileFaces, t);
   {
     float2 accW[kSlots / 2], accQ[kSlots / 2];
     p2g_component<2>(g, p, order, pbeg, pend, cell, accW, accQ, rep);
-    wt = wtiles[0] + (t >> 5) * kWarpTileMax;
-    warp_tile<2>(accW, accQ, wt, t & 31);
+    warp_tile<2>(accW, accQ, wt_smem + 2 * kP2GWarps * kWarpTileMax + wofs, t & 31);
   }
   __syncthreads();
-  block_tile<2>(wtiles[0], tile + 2 * kTileFaces, t);
+  block_tile<0>(wt_smem, tile, t);
+  block_tile<1>(wt_smem + kP2GWarps * kWarpTileMax, tile + kTileFaces, t);
+  block_tile<2>(wt_smem + 2 * kP2GWarps * kWarpTileMax, tile + 2 * kTileFaces, t);
 }
 
 __device__ __forceinline__ bool is_solid(const GridView& g, int x, int y, int z) {
@@ -347,9 +343,10 @@ __global__ void __launch_bounds__(kBlockCells)
   if (mass != 0.0f && mass > prm.min_face_mass) u = Q / W;
   // NormalizeCore's validity (liquid_boundary_transfer_3d.cc:486-510): no
   // mass -> missing, positive mass at or below the minimum -> low mass
-  if (prm.validity[a] != nullptr)
-    prm.validity[a][slot] = mass == 0.0f ? kFaceMissing : (mass <= prm.min_face_mass ? kFaceLowMass : kFaceValid);
-  u += prm.dt * prm.gravity[a];
+  // (selected, not indexed: a dynamic index into the parameter arrays would copy them to local memory)
+  unsigned char* val = a == 0 ? prm.validity[0] : (a == 1 ? prm.validity[1] : prm.validity[2]);
+  if (val != nullptr) val[slot] = mass == 0.0f ? kFaceMissing : (mass <= prm.min_face_mass ? kFaceLowMass : kFaceValid);
+  u += prm.dt * (a == 0 ? prm.gravity[0] : (a == 1 ? prm.gravity[1] : prm.gravity[2]));
   const int head[3] = {g.coord[3 * b] * 8 + loc[0], g.coord[3 * b + 1] * 8 + loc[1], g.coord[3 * b + 2] * 8 + loc[2]};
   int tail[3] = {head[0], head[1], head[2]};
   tail[a] -= 1;
@@ -363,7 +360,7 @@ cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cel
                        const P2GMergeParams& prm, float* const out0[3], float* const out1[3], DeviceReport* rep,
                        cudaStream_t s, const unsigned int* order) {
   if (g.nb == 0) return cudaSuccess;
-  const size_t smem = sizeof(float2) * 2 * kP2GWarps * kWarpTileMax;
+  const size_t smem = sizeof(float2) * 3 * kP2GWarps * kWarpTileMax;
   static unsigned long long configured = 0;
   if (first_on_device(configured))
     cudaFuncSetAttribute(k_p2g_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
