@@ -36,7 +36,7 @@ namespace fl {
 
 namespace {
 
-constexpr int kTcThreads = 128;  // one warpgroup: warp w reads TMEM lanes 32w..32w+31
+constexpr int kTcThreads = 160;  // warps 0-3 read TMEM lanes 32w..32w+31; warp 4 copies and issues MMAs
 constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at 1.9 GHz: mbarrier wait bound
 
 struct PadGeom {
@@ -100,6 +100,14 @@ __device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uin
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(src), "r"(bytes), "r"(mbar)
                : "memory");
+}
+
+// TMEM columns of one accumulator stage (a power of two, at least 32).
+__host__ __device__ constexpr int tc_cols(int used) { return used <= 32 ? 32 : (used <= 64 ? 64 : (used <= 128 ? 128 : 256)); }
+
+__device__ __forceinline__ void mbar_init_count(uint32_t mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t mbar) {
@@ -180,145 +188,184 @@ struct ConvArgs {
   int* error;             // set to 1 when an mbarrier wait gives up
 };
 
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
 // One conv layer over all blocks. IN/OUT: geometry of the input columns and of
 // the output layout (same D except for the valid first layer, whose input is
 // the 10^3 window). KG: input channel groups (1 = the 2-channel window, whose
 // second K half re-reads the first with zero weights). N: output channels.
+//
+// A CTA handles blocks blockIdx.x, blockIdx.x + gridDim.x, ... through a
+// two-stage pipeline. Warp 4's first thread copies block k + 1's operand
+// columns into one shared-memory stage (a bulk copy) while it issues block
+// k's MMAs from the other stage into one of two TMEM accumulator stages;
+// warps 0-3 (TMEM lanes 32w..32w+31) drain the other accumulator stage,
+// block k - 1's, for bias, ReLU and the store. Barriers per stage: operands
+// arrived (full), operands consumed by the MMAs (empty), accumulators written
+// (accf), accumulators read (acce, one arrival per epilogue warp). Every wait
+// is bounded (~1 s); a wait that gives up sets the error flag and its role
+// stops, and the TMEM is released only after a final commit shows every
+// issued MMA complete.
 template <int KG, int N, int MODE, int IN_KIND, int OUT_KIND>
 __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvArgs a) {
   constexpr PadGeom IN = IN_KIND == 10 ? geom10() : (IN_KIND == 8 ? geom8() : (IN_KIND == 4 ? geom4() : geom2()));
   constexpr PadGeom OUT = OUT_KIND == 8 ? geom8() : (OUT_KIND == 4 ? geom4() : geom2());
   constexpr int KC = KG >= 2 ? KG / 2 : 1;
   constexpr int TILES = IN.tiles;
-  constexpr int COLS_USED = TILES * N;
-  constexpr int NCOLS = COLS_USED <= 32 ? 32 : (COLS_USED <= 64 ? 64 : (COLS_USED <= 128 ? 128 : 256));
+  constexpr int NCOLS = tc_cols(TILES * N);
   constexpr uint32_t W_BYTES = 27u * KC * 2u * N * 16u;
   constexpr uint32_t A_BYTES = (uint32_t)KG * IN.rows * 16u;
   constexpr uint32_t GROUP_BYTES = (uint32_t)IN.rows * 16u;
   constexpr uint32_t IDESC = instr_desc(128, N);
   static_assert(IN.rows >= 128 * TILES + 2 * IN.r_lo, "shifted tiles must stay inside the column");
   static_assert(N % 16 == 0 && N >= 16 && N <= 256, "M = 128 needs N in 16..256, multiple of 16");
+  static_assert(W_BYTES % 16 == 0 && A_BYTES % 16 == 0, "bulk copies need 16-byte alignment and sizes");
+  static_assert(2 * NCOLS <= 512, "two accumulator stages within the SM's TMEM");
 
   extern __shared__ __align__(128) unsigned char smem[];
   uint4* w_s = reinterpret_cast<uint4*>(smem);
-  uint4* a_s = reinterpret_cast<uint4*>(smem + W_BYTES);
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + W_BYTES + A_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + W_BYTES + A_BYTES + 8);
-  uint64_t* abar = reinterpret_cast<uint64_t*>(smem + W_BYTES + A_BYTES + 16);  // operand copy done
-  static_assert(W_BYTES % 16 == 0 && A_BYTES % 16 == 0, "bulk copies need 16-byte alignment and sizes");
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + W_BYTES + 2 * A_BYTES);  // 9 barriers
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 9);
+  enum { kFull = 0, kEmpty = 2, kAccF = 4, kAccE = 6, kDrain = 8 };
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (uint32_t i = tid; i < W_BYTES / 16; i += kTcThreads) w_s[i] = a.weights[i];
   if (tid == 0) {
-    mbar_init(smem_u32(mbar));
-    mbar_init(smem_u32(abar));
+#pragma unroll
+    for (int k = 0; k < 9; ++k) mbar_init_count(smem_u32(bars + k), (k == kAccE || k == kAccE + 1) ? 4u : 1u);
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"((uint32_t)NCOLS));
+                 "r"((uint32_t)(2 * NCOLS)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
+  fence_async_smem();  // the weights, stored by every thread, before the MMAs read them
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t w_addr = smem_u32(w_s), a_addr = smem_u32(a_s), mbar_addr = smem_u32(mbar);
-  const uint32_t abar_addr = smem_u32(abar);
-  fence_async_smem();  // the weights, stored by the threads, before the MMAs read them
+  const uint32_t w_addr = smem_u32(w_s), a_addr = smem_u32(smem + W_BYTES);
+  auto bar = [&](int k) { return smem_u32(bars + k); };
+  const int nblk = (int)blockIdx.x < a.nb ? (a.nb - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
 
-  uint32_t parity = 0, aparity = 0;
-  for (int b = blockIdx.x; b < a.nb; b += gridDim.x) {
-    // the block's operand columns: one bulk copy (the previous block's MMAs
-    // have completed: their commit was waited for before its epilogue)
-    if (tid == 0) bulk_copy_g2s(a_addr, a.in + (size_t)b * (KG * IN.rows), A_BYTES, abar_addr);
-    const bool copied = mbar_wait(abar_addr, aparity);
-    if (__syncthreads_or(!copied)) {
-      mbar_wait(abar_addr, aparity);  // one more bounded wait for the copy in flight
-      if (tid == 0) atomicExch(a.error, 1);
-      break;
+  if (warp == 4) {
+    if (lane == 0) {
+      bool ok = true;
+      int issued = -1, arrived = -1;  // last block whose operand copy was issued / was waited for
+      auto copy = [&](int k) {
+        const int st = k & 1;
+        bulk_copy_g2s(a_addr + (uint32_t)st * A_BYTES, a.in + (size_t)(blockIdx.x + k * gridDim.x) * (KG * IN.rows),
+                      A_BYTES, bar(kFull + st));
+        issued = k;
+      };
+      if (nblk > 0) copy(0);
+      for (int k = 0; k < nblk && ok; ++k) {
+        const int st = k & 1;
+        const uint32_t u = (uint32_t)(k >> 1);
+        if (k + 1 < nblk) {  // the other stage is free once block k - 1's MMAs are done
+          if (k >= 1 && !(ok = mbar_wait(bar(kEmpty + (st ^ 1)), (uint32_t)((k - 1) >> 1) & 1u))) break;
+          copy(k + 1);
+        }
+        if (!(ok = mbar_wait(bar(kFull + st), u & 1u))) break;
+        arrived = k;
+        if (k >= 2 && !(ok = mbar_wait(bar(kAccE + st), (u - 1u) & 1u))) break;
+        fence_after_sync();
+        // The descriptors' start-address field (bits 0-13) counts 16-byte rows,
+        // so each tap's operands are the tile's base descriptors plus constant
+        // row offsets (every address stays below 256 KB: no carry out of the
+        // field; the static_assert above keeps shifted rows inside the column).
+        const uint64_t a0 =
+            smem_desc(a_addr + (uint32_t)st * A_BYTES + (uint32_t)IN.r_lo * 16u, KG >= 2 ? GROUP_BYTES : 0u, 128u);
+        const uint64_t b0 = smem_desc(w_addr, N * 16u, 128u);
+#pragma unroll 1
+        for (int t = 0; t < TILES; ++t) {
+          const uint64_t at = a0 + (uint64_t)(128 * t);
+          const uint32_t dt = tmem + (uint32_t)(st * NCOLS + t * N);
+#pragma unroll
+          for (int tap = 0; tap < 27; ++tap) {
+            const int shift = ((tap / 9 - 1) * IN.Py + ((tap / 3) % 3 - 1)) * IN.Px + (tap % 3 - 1);
+#pragma unroll
+            for (int kc = 0; kc < KC; ++kc) {
+              const uint64_t ad = at + (uint64_t)(int64_t)(shift + 2 * kc * IN.rows);
+              const uint64_t bd = b0 + (uint64_t)((tap * KC + kc) * 2 * N);
+              mma_bf16(dt, ad, bd, IDESC, (tap | kc) != 0 ? 1u : 0u);
+            }
+          }
+        }
+        mma_commit(bar(kEmpty + st));
+        mma_commit(bar(kAccF + st));
+      }
+      if (!ok) atomicExch(a.error, 1);
+      // after a wait gave up: one more bounded wait for each copy still in flight
+      for (int j = arrived + 1; j <= issued; ++j) mbar_wait(bar(kFull + (j & 1)), (uint32_t)(j >> 1) & 1u);
+      mma_commit(bar(kDrain));  // arrives once every MMA this thread issued has completed
+      if (!mbar_wait(bar(kDrain), 0u)) atomicExch(a.error, 1);
     }
-    aparity ^= 1u;
-    if (tid == 0) {
+  } else {
+    for (int k = 0; k < nblk; ++k) {
+      const int st = k & 1;
+      const uint32_t u = (uint32_t)(k >> 1);
+      if (!mbar_wait(bar(kAccF + st), u & 1u)) {
+        if (lane == 0) atomicExch(a.error, 1);
+        break;
+      }
       fence_after_sync();
-      // The descriptors' start-address field (bits 0-13) counts 16-byte rows,
-      // so each tap's operands are the tile's base descriptors plus constant
-      // row offsets (every address stays below 256 KB: no carry out of the
-      // field; the static_assert above keeps shifted rows inside the column).
-      const uint64_t a0 = smem_desc(a_addr + (uint32_t)IN.r_lo * 16u, KG >= 2 ? GROUP_BYTES : 0u, 128u);
-      const uint64_t b0 = smem_desc(w_addr, N * 16u, 128u);
+      const int b = blockIdx.x + k * gridDim.x;
+      // warp w owns tile rows 32w..32w+31
 #pragma unroll 1
       for (int t = 0; t < TILES; ++t) {
-        const uint64_t at = a0 + (uint64_t)(128 * t);
-        const uint32_t dt = tmem + (uint32_t)(t * N);
+        const int r = IN.r_lo + 128 * t + 32 * warp + lane;
+        const int px = r % IN.Px, py = (r / IN.Px) % IN.Py, pz = r / (IN.Px * IN.Py);
+        const bool interior = px >= 1 && px <= IN.D && py >= 1 && py <= IN.D && pz >= 1 && pz <= IN.D;
+        const int x = px - 1, y = py - 1, z = pz - 1;
+        float acc[N];
 #pragma unroll
-        for (int tap = 0; tap < 27; ++tap) {
-          const int shift = ((tap / 9 - 1) * IN.Py + ((tap / 3) % 3 - 1)) * IN.Px + (tap % 3 - 1);
+        for (int c = 0; c < N; c += 16) {
+          float v[16];
+          tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(st * NCOLS + t * N + c), v);
 #pragma unroll
-          for (int kc = 0; kc < KC; ++kc) {
-            const uint64_t ad = at + (uint64_t)(int64_t)(shift + 2 * kc * IN.rows);
-            const uint64_t bd = b0 + (uint64_t)((tap * KC + kc) * 2 * N);
-            mma_bf16(dt, ad, bd, IDESC, (tap | kc) != 0 ? 1u : 0u);
+          for (int q = 0; q < 16; ++q) acc[c + q] = fmaxf(v[q] + __ldg(&a.bias[c + q]), 0.0f);
+        }
+        if (!interior) continue;
+        if (MODE == kToPadded) {
+          const int ro = pad_row(OUT, x, y, z);
+          uint4* dst = a.out + (size_t)b * (N / 8) * OUT.rows;
+#pragma unroll
+          for (int g = 0; g < N / 8; ++g) dst[g * OUT.rows + ro] = pack8(acc + 8 * g);
+        } else if (MODE == kToPlain) {
+          float* dst = a.out_plain + ((size_t)b * IN.D * IN.D * IN.D + (z * IN.D + y) * IN.D + x) * N;
+#pragma unroll
+          for (int c = 0; c < N; c += 4)
+            *reinterpret_cast<float4*>(dst + c) = make_float4(acc[c], acc[c + 1], acc[c + 2], acc[c + 3]);
+        } else {
+          float yv = __ldg(a.b_out);
+#pragma unroll
+          for (int c = 0; c < N; ++c) yv = fmaf(__ldg(&a.w_out[c]), acc[c], yv);
+          const int l = (z * 8 + y) * 8 + x;
+          const float v = a.type[b * 512 + l] == 1 ? a.scale[b] * yv : 0.0f;
+          const int zi = b * 512 + rb_of(l);
+          if (a.z_bf16) {
+            __nv_bfloat16* zp = reinterpret_cast<__nv_bfloat16*>(a.z) + zi;
+            *zp = __float2bfloat16_rn(a.z_add ? __bfloat162float(*zp) + v : v);
+          } else {
+            float* zp = reinterpret_cast<float*>(a.z) + zi;
+            *zp = a.z_add ? *zp + v : v;
           }
         }
       }
-      mma_commit(mbar_addr);
+      // this warp's accumulator reads are done (tmem_ld16 waits for them)
+      fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(bar(kAccE + st));
     }
-    __syncwarp();
-    const bool ok = mbar_wait(mbar_addr, parity);
-    if (__syncthreads_or(!ok)) {
-      // give the MMAs in flight one more bounded wait before the TMEM is released
-      mbar_wait(mbar_addr, parity);
-      if (tid == 0) atomicExch(a.error, 1);
-      break;
-    }
-    parity ^= 1u;
-    fence_after_sync();
-    // epilogue: warp w owns tile rows 32w..32w+31
-#pragma unroll 1
-    for (int t = 0; t < TILES; ++t) {
-      const int r = IN.r_lo + 128 * t + 32 * warp + lane;
-      const int px = r % IN.Px, py = (r / IN.Px) % IN.Py, pz = r / (IN.Px * IN.Py);
-      const bool interior = px >= 1 && px <= IN.D && py >= 1 && py <= IN.D && pz >= 1 && pz <= IN.D;
-      const int x = px - 1, y = py - 1, z = pz - 1;
-      float acc[N];
-#pragma unroll
-      for (int c = 0; c < N; c += 16) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(t * N + c), v);
-#pragma unroll
-        for (int k = 0; k < 16; ++k) acc[c + k] = fmaxf(v[k] + __ldg(&a.bias[c + k]), 0.0f);
-      }
-      if (!interior) continue;
-      if (MODE == kToPadded) {
-        const int ro = pad_row(OUT, x, y, z);
-        uint4* dst = a.out + (size_t)b * (N / 8) * OUT.rows;
-#pragma unroll
-        for (int g = 0; g < N / 8; ++g) dst[g * OUT.rows + ro] = pack8(acc + 8 * g);
-      } else if (MODE == kToPlain) {
-        float* dst = a.out_plain + ((size_t)b * IN.D * IN.D * IN.D + (z * IN.D + y) * IN.D + x) * N;
-#pragma unroll
-        for (int c = 0; c < N; c += 4) *reinterpret_cast<float4*>(dst + c) = make_float4(acc[c], acc[c + 1], acc[c + 2], acc[c + 3]);
-      } else {
-        float yv = __ldg(a.b_out);
-#pragma unroll
-        for (int c = 0; c < N; ++c) yv = fmaf(__ldg(&a.w_out[c]), acc[c], yv);
-        const int l = (z * 8 + y) * 8 + x;
-        const float v = a.type[b * 512 + l] == 1 ? a.scale[b] * yv : 0.0f;
-        const int zi = b * 512 + rb_of(l);
-        if (a.z_bf16) {
-          __nv_bfloat16* zp = reinterpret_cast<__nv_bfloat16*>(a.z) + zi;
-          *zp = __float2bfloat16_rn(a.z_add ? __bfloat162float(*zp) + v : v);
-        } else {
-          float* zp = reinterpret_cast<float*>(a.z) + zi;
-          *zp = a.z_add ? *zp + v : v;
-        }
-      }
-    }
-    fence_before_sync();
-    __syncthreads();
   }
+  fence_before_sync();
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)NCOLS));
+  fence_after_sync();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)(2 * NCOLS)));
 }
 
 // Input window of block b in the 10^3 layout (one channel group: residual / s,
@@ -479,16 +526,25 @@ __global__ void k_pack_conv(const float* __restrict__ w, int cin, int cout, int 
   }
 }
 
+// CTAs of one layer per SM: two TMEM accumulator stages each, within the
+// SM's 512 columns.
+template <int KG, int N, int MODE, int IN_KIND, int OUT_KIND>
+constexpr int conv_ctas_per_sm() {
+  constexpr PadGeom IN = IN_KIND == 10 ? geom10() : (IN_KIND == 8 ? geom8() : (IN_KIND == 4 ? geom4() : geom2()));
+  return 512 / (2 * tc_cols(IN.tiles * N));
+}
+
 template <int KG, int N, int MODE, int IN_KIND, int OUT_KIND>
 constexpr size_t conv_smem() {
   constexpr PadGeom IN = IN_KIND == 10 ? geom10() : (IN_KIND == 8 ? geom8() : (IN_KIND == 4 ? geom4() : geom2()));
   constexpr int KC = KG >= 2 ? KG / 2 : 1;
-  constexpr size_t bytes = 27u * KC * 2u * N * 16u + (size_t)KG * IN.rows * 16u + 32;
-  constexpr int COLS = IN.tiles * N;
-  // kernels holding 128 TMEM columns ask for enough shared memory that at most
-  // four are resident per SM (4 x 128 = the 512 columns), so no allocation waits
-  // (4 x (55 KB + 1 KB reserved) fits the SM's 228 KB, a fifth does not)
-  return COLS > 64 && bytes < 55 * 1024 ? 55 * 1024 : bytes;
+  constexpr size_t bytes = 27u * KC * 2u * N * 16u + 2u * (size_t)KG * IN.rows * 16u + 9 * 8 + 8;
+  // Ask for enough shared memory that one more CTA than the TMEM allows does
+  // not fit the SM (228 KB, 1 KB reserved per CTA), so no TMEM allocation
+  // waits for another CTA's release.
+  constexpr int cap = conv_ctas_per_sm<KG, N, MODE, IN_KIND, OUT_KIND>();
+  constexpr size_t floor_bytes = (size_t)(233472 / (cap + 1)) - 1024 + 16;
+  return bytes < floor_bytes ? floor_bytes : bytes;
 }
 
 template <int KG, int N, int MODE, int IN_KIND, int OUT_KIND>
@@ -498,7 +554,9 @@ cudaError_t launch_conv(const ConvArgs& a, int sms, cudaStream_t s) {
   static unsigned long long configured = 0;
   if (first_on_device(configured))
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int per_sm = (int)((227 * 1024) / smem);
+  const int by_smem = (int)(233472 / (smem + 1024));
+  const int cap = conv_ctas_per_sm<KG, N, MODE, IN_KIND, OUT_KIND>();
+  const int per_sm = by_smem < cap ? by_smem : cap;
   const int grid = a.nb < sms * per_sm ? a.nb : sms * per_sm;
   ++g_kernel_launches;
   kern<<<grid, kTcThreads, smem, s>>>(a);
