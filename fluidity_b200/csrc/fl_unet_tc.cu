@@ -451,12 +451,17 @@ __global__ void __launch_bounds__(256) k_tc_upadd2(const float* __restrict__ bt,
                                                    uint4* __restrict__ u2) {
   constexpr PadGeom L = geom4();
   __shared__ float c2[8][32];
+  __shared__ float wt[64][32];  // the 1x1 weights transposed: a warp's 32 output channels read one row
+  __shared__ float in[8][64];
   const int b = blockIdx.x;
+  for (int i = threadIdx.x; i < 64 * 32; i += 256) wt[i & 63][i >> 6] = __ldg(&w[i]);  // w[co][ci], coalesced
+  for (int i = threadIdx.x; i < 8 * 64; i += 256) in[i >> 6][i & 63] = bt[(size_t)b * 8 * 64 + i];
+  __syncthreads();
   {
     const int cell = threadIdx.x >> 5, co = threadIdx.x & 31;
-    const float* src = bt + ((size_t)b * 8 + cell) * 64;
     float acc = bias[co];
-    for (int ci = 0; ci < 64; ++ci) acc = fmaf(__ldg(&w[co * 64 + ci]), src[ci], acc);
+#pragma unroll 8
+    for (int ci = 0; ci < 64; ++ci) acc = fmaf(wt[ci][co], in[cell][ci], acc);
     c2[cell][co] = acc;
   }
   __syncthreads();
@@ -481,7 +486,9 @@ __global__ void __launch_bounds__(256) k_tc_upadd1(const uint4* __restrict__ d2,
   constexpr PadGeom L8 = geom8();
   __shared__ float din[64][33];
   __shared__ float c1[64][16];
+  __shared__ float wt[32][16];  // the 1x1 weights transposed (w[co][ci] -> wt[ci][co])
   const int b = blockIdx.x;
+  for (int i = threadIdx.x; i < 16 * 32; i += 256) wt[i & 31][i >> 5] = __ldg(&w[i]);
   for (int i = threadIdx.x; i < 64 * 4; i += 256) {
     const int gi = i & 3, c = i >> 2;
     const int x = c & 3, y = (c >> 2) & 3, z = c >> 4;
@@ -494,7 +501,8 @@ __global__ void __launch_bounds__(256) k_tc_upadd1(const uint4* __restrict__ d2,
   for (int i = threadIdx.x; i < 64 * 16; i += 256) {
     const int co = i & 15, c = i >> 4;
     float acc = bias[co];
-    for (int ci = 0; ci < 32; ++ci) acc = fmaf(__ldg(&w[co * 32 + ci]), din[c][ci], acc);
+#pragma unroll 8
+    for (int ci = 0; ci < 32; ++ci) acc = fmaf(wt[ci][co], din[c][ci], acc);
     c1[c][co] = acc;
   }
   __syncthreads();
