@@ -248,25 +248,38 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvArgs a) {
   const uint32_t tmem = *tmem_slot;
   const uint32_t w_addr = smem_u32(w_s), a_addr = smem_u32(smem + W_BYTES);
   auto bar = [&](int k) { return smem_u32(bars + k); };
-  const int nblk = (int)blockIdx.x < a.nb ? (a.nb - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+  // This CTA's blocks: blockIdx.x, blockIdx.x + gridDim.x, ..., skipping blocks whose
+  // window holds no residual (scale 0: their correction is zero whatever the network
+  // computes). Both roles walk the same sequence with their own cursor.
+  auto next_block = [&](int& j) -> int {
+    for (;;) {
+      const int b = (int)blockIdx.x + j * (int)gridDim.x;
+      if (b >= a.nb) return -1;
+      ++j;
+      if (a.scale == nullptr || __ldg(&a.scale[b]) != 0.0f) return b;
+    }
+  };
 
   if (warp == 4) {
     if (lane == 0) {
       bool ok = true;
-      int issued = -1, arrived = -1;  // last block whose operand copy was issued / was waited for
-      auto copy = [&](int k) {
+      int issued = -1, arrived = -1;  // last block (in this CTA's sequence) copied / waited for
+      auto copy = [&](int k, int blk) {
         const int st = k & 1;
-        bulk_copy_g2s(a_addr + (uint32_t)st * A_BYTES, a.in + (size_t)(blockIdx.x + k * gridDim.x) * (KG * IN.rows),
-                      A_BYTES, bar(kFull + st));
+        bulk_copy_g2s(a_addr + (uint32_t)st * A_BYTES, a.in + (size_t)blk * (KG * IN.rows), A_BYTES,
+                      bar(kFull + st));
         issued = k;
       };
-      if (nblk > 0) copy(0);
-      for (int k = 0; k < nblk && ok; ++k) {
+      int cursor = 0;
+      int bk = next_block(cursor);                 // block k of the sequence
+      int bn = bk >= 0 ? next_block(cursor) : -1;  // block k + 1
+      if (bk >= 0) copy(0, bk);
+      for (int k = 0; bk >= 0 && ok; ++k) {
         const int st = k & 1;
         const uint32_t u = (uint32_t)(k >> 1);
-        if (k + 1 < nblk) {  // the other stage is free once block k - 1's MMAs are done
+        if (bn >= 0) {  // the other stage is free once block k - 1's MMAs are done
           if (k >= 1 && !(ok = mbar_wait(bar(kEmpty + (st ^ 1)), (uint32_t)((k - 1) >> 1) & 1u))) break;
-          copy(k + 1);
+          copy(k + 1, bn);
         }
         if (!(ok = mbar_wait(bar(kFull + st), u & 1u))) break;
         arrived = k;
@@ -296,6 +309,8 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvArgs a) {
         }
         mma_commit(bar(kEmpty + st));
         mma_commit(bar(kAccF + st));
+        bk = bn;
+        bn = bk >= 0 ? next_block(cursor) : -1;
       }
       if (!ok) atomicExch(a.error, 1);
       // after a wait gave up: one more bounded wait for each copy still in flight
@@ -304,7 +319,10 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvArgs a) {
       if (!mbar_wait(bar(kDrain), 0u)) atomicExch(a.error, 1);
     }
   } else {
-    for (int k = 0; k < nblk; ++k) {
+    int cursor = 0;
+    for (int k = 0;; ++k) {
+      const int b = next_block(cursor);
+      if (b < 0) break;
       const int st = k & 1;
       const uint32_t u = (uint32_t)(k >> 1);
       if (!mbar_wait(bar(kAccF + st), u & 1u)) {
@@ -312,7 +330,6 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvArgs a) {
         break;
       }
       fence_after_sync();
-      const int b = blockIdx.x + k * gridDim.x;
       // warp w owns tile rows 32w..32w+31
 #pragma unroll 1
       for (int t = 0; t < TILES; ++t) {
@@ -370,9 +387,13 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvArgs a) {
 
 // Input window of block b in the 10^3 layout (one channel group: residual / s,
 // cell mask, six zero channels) and the block scale s (max |residual| over the window).
+// z_zero (not null when the network's output replaces z): a block whose window
+// holds no residual is skipped by every layer, so its correction, zero, is
+// written here.
+template <typename T>
 __global__ void __launch_bounds__(512) k_tc_gather(GridView g, const float* __restrict__ r_rb,
                                                    const unsigned char* __restrict__ type, uint4* __restrict__ x,
-                                                   float* __restrict__ scale) {
+                                                   float* __restrict__ scale, T* __restrict__ z_zero) {
   constexpr PadGeom W = geom10();
   __shared__ float red[16];
   const int b = blockIdx.x;
@@ -405,6 +426,7 @@ __global__ void __launch_bounds__(512) k_tc_gather(GridView g, const float* __re
   float sc = 0.0f;
 #pragma unroll
   for (int k = 0; k < 16; ++k) sc = fmaxf(sc, red[k]);
+  if (sc == 0.0f && z_zero != nullptr) z_zero[(size_t)b * 512 + threadIdx.x] = static_cast<T>(0.0f);
   uint4* dst = x + (size_t)b * W.rows;
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
@@ -635,10 +657,11 @@ cudaError_t unet_tc_apply(const GridView& g, const float* params, const __nv_bfl
   auto base = [&](long long off) { return act + off * cap; };
   auto wp = [&](int k) { return reinterpret_cast<const uint4*>(packed + L.w_off[k]); };
   ++g_kernel_launches;
-  k_tc_gather<<<nb, 512, 0, s>>>(g, r_rb, type, base(L.x), scale);
+  k_tc_gather<T><<<nb, 512, 0, s>>>(g, r_rb, type, base(L.x), scale, accumulate ? nullptr : z);
   ConvArgs a{};
   a.nb = nb;
   a.error = error;
+  a.scale = scale;  // every layer skips the blocks without residual
   cudaError_t e;
   // e1a: window (1 group) -> t8
   a.in = base(L.x); a.weights = wp(0); a.bias = params + P.bias[0]; a.out = base(L.t8);
@@ -668,7 +691,7 @@ cudaError_t unet_tc_apply(const GridView& g, const float* params, const __nv_bfl
   k_tc_upadd1<<<nb, 256, 0, s>>>(base(L.d2), base(L.s1), params + P.offset[7], params + P.bias[7], base(L.t8));
   // d1 + output layer: u1 (in t8) -> z
   a.in = base(L.t8); a.weights = wp(6); a.bias = params + P.bias[8]; a.out = nullptr;
-  a.w_out = params + P.offset[9]; a.b_out = params + P.bias[9]; a.scale = scale; a.type = type; a.z = z;
+  a.w_out = params + P.offset[9]; a.b_out = params + P.bias[9]; a.type = type; a.z = z;
   a.z_bf16 = sizeof(T) == 2;
   a.z_add = accumulate ? 1 : 0;
   return launch_conv<2, 16, kToCorrection, 8, 8>(a, sms, s);
