@@ -1,4 +1,4 @@
-// Minimal stand-in for absl::FunctionRef used by the oracle build only
+// Minimal stand-in for absl::FunctionRef where no absl installation exists
 // (a non-owning callable reference is approximated with std::function).
 #pragma once
 

@@ -1,7 +1,8 @@
-// Minimal stand-in for absl::Status, written for this repository's oracle build.
-// It provides only what the reference's CPU transfer and pressure operators use:
-// status codes, code-plus-message construction, ok()/code()/message() and the
-// *Error helper constructors. It is test infrastructure, never shipped code.
+// Minimal stand-in for absl::Status where no absl installation exists (the
+// backend adapter and the reference's CPU operators built in this repository;
+// inside the reference's own tree its absl is used instead). It provides only
+// what those use: status codes, code-plus-message construction,
+// ok()/code()/message() and the *Error helper constructors.
 #pragma once
 
 #include <ostream>
@@ -10,6 +11,8 @@
 #include <utility>
 
 namespace absl {
+
+using string_view = std::string_view;
 
 enum class StatusCode : int {
   kOk = 0,

@@ -1,4 +1,4 @@
-// Minimal stand-in for absl::StatusOr<T> used by the oracle build only.
+// Minimal stand-in for absl::StatusOr<T> where no absl installation exists.
 #pragma once
 
 #include <cassert>

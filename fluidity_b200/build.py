@@ -5,6 +5,12 @@ Every translation unit is compiled by nvcc with
 flags of EXTRA) and linked into one
 shared object with a C-ABI (include/fluidity_b200.h). The library is built in
 tree so it travels with the working copy; nothing is installed.
+
+When the FluidiTy sources are present ($FLUIDITY_REFERENCE, or the checkout
+beside this repository), the backend-table adapter (adapter/) is compiled
+against their headers with g++ into _lib/libfluidity_b200_backend.so, linked
+to the CUDA library. It leaves the reference's own symbols (the sparse grid
+view's accessors) to the program that loads it, as a plug-in of that tree does.
 """
 
 from __future__ import annotations
@@ -19,12 +25,13 @@ HERE = Path(__file__).resolve().parent
 SRC = HERE / "csrc"
 OUT = HERE / "_lib"
 LIB = OUT / "libfluidity_b200.so"
+BACKEND = OUT / "libfluidity_b200_backend.so"
 SOURCES = ["fl_grid.cu", "fl_p2g.cu", "fl_g2p.cu", "fl_pressure.cu", "fl_quanta.cu", "fl_context.cu", "fl_noalloc.cu",
-           "fl_unet.cu", "fl_unet_tc.cu", "fl_snapshot.cu", "fl_mac_pressure.cu"]
+           "fl_unet.cu", "fl_unet_tc.cu", "fl_snapshot.cu", "fl_mac_pressure.cu", "fl_boundary.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # Per-file flags: the reference-shaped pressure operator keeps every FP64
 # product apart from the sum it enters, as the reference's arithmetic does.
-EXTRA = {"fl_mac_pressure.cu": ["-fmad=false"]}
+EXTRA = {"fl_mac_pressure.cu": ["-fmad=false"], "fl_boundary.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -68,7 +75,29 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     if force or _stale(LIB, objs):
         cmd = [nvcc(), "-shared", *ARCH, "-o", str(LIB), *map(str, objs), "-lcudart"]
         subprocess.check_call(cmd)
+    build_backend(force)
     return LIB
+
+
+def reference_root() -> Path:
+    return Path(os.environ.get("FLUIDITY_REFERENCE", HERE.parent.parent / "reference"))
+
+
+def build_backend(force: bool = False) -> Path | None:
+    """The LiquidSubstepBackend3D adapter; None where the reference headers are absent."""
+    ref = reference_root() / "native" / "include"
+    if not ref.is_dir():
+        return None
+    ad = HERE / "adapter"
+    src = ad / "b200_liquid_substep_backend_3d.cc"
+    deps = [src, ad / "b200_liquid_substep_backend_3d.h", HERE.parent / "include" / "fluidity_b200.h", LIB]
+    deps += list((ad / "absl_shim").rglob("*.h"))
+    if force or _stale(BACKEND, deps):
+        cmd = ["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-o", str(BACKEND), str(src),
+               f"-I{ad / 'absl_shim'}", f"-I{ref}", f"-I{HERE.parent / 'include'}", f"-L{OUT}", "-lfluidity_b200",
+               "-Wl,-rpath,$ORIGIN"]
+        subprocess.check_call(cmd)
+    return BACKEND
 
 
 if __name__ == "__main__":

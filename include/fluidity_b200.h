@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-/* Status codes (absl::StatusCode numbering, as in native/src/*: transfers_3d.h:13-22,
+/* Status codes (absl::StatusCode numbering, as in the reference's transfers_3d.h:13-22,
  * mac_pressure_3d.h:88-100, operator_runtime.h:18-40). */
 #define FL_OK 0
 #define FL_INVALID_ARGUMENT 3
@@ -476,6 +476,147 @@ int fl_copy_to_device(void* device, const void* host, uint64_t bytes);
 
 /* Library information: compiled architecture (e.g. 1000) and whether a usable device exists. */
 int fl_runtime_info(int* compiled_architecture, int* device_count, int* device_major, int* device_minor);
+
+/* ---- bounded boundary-aware transfers: the liquid scheduler's backend operations ----
+ *
+ * The operations behind LiquidSubstepBackend3D's .deposit, .normalize,
+ * .predict_missing_face, .forces and .gather
+ * (native/include/fluidity/host/liquid_substep_backend_3d.h:121-194), as the
+ * reference's CPU table binds them (native/src/liquid_substep_3d_cpu.cc:
+ * 775-803, 847-849; numerics native/src/liquid_boundary_transfer_3d.cc:
+ * 56-308, 327-668, 785-805, 953-984) and its CUDA table replaces them
+ * (native/cuda/liquid_transfer_stages_3d_host.cc:375-620). They run on the
+ * reference's owned sparse grid: 4^3-cell blocks in strictly increasing (z,y,x)
+ * order, 192 face slots per block (normal axis, then local (z,y,x)), at most
+ * 1024 particles and 24576 face slots (liquid_boundary_transfer_3d.h:16-17).
+ *
+ * An fl_boundary reserves its device and pinned host storage for those caps
+ * when it is created; the operations allocate nothing. Each call copies its
+ * inputs to the device, runs its kernels in FP64 on one non-blocking stream and
+ * synchronizes it, and writes its outputs only on FL_OK (the reference's
+ * "errors publish nothing"). Codes follow the CPU operations: for several
+ * failing items the code is that of the first in the CPU loop order
+ * (particle, then component, then stencil sample). Deposit quanta, normalized
+ * faces and forces are bit-identical to the CPU operations; the gather's ghost
+ * fits use the device's hypot, so a filled ghost velocity can differ from the
+ * CPU's in its last bits.
+ *
+ * The record layouts below are byte-compatible with the reference's
+ * (LiquidBoundaryParticle3D, LiquidBoundaryFaceTag3D, MacFaceDepositQuanta3D,
+ * CompatibleMacFaceSample3D, LiquidPrescribedWallSample3D,
+ * LiquidBoundaryParticleGather3D: native/include/fluidity/base/
+ * liquid_boundary_transfer_types_3d.h:4-45, mac_transfer_types_3d.h:7-30), so a
+ * backend passes the scheduler's spans through unchanged. */
+typedef struct fl_boundary fl_boundary;
+
+typedef struct {
+  double origin[3];      /* world position of lattice point (0,0,0), m */
+  double h;              /* cell width, m (positive normal) */
+  const int32_t* blocks; /* block_count x (x, y, z), 4^3-cell blocks, strictly increasing (z,y,x) */
+  uint64_t block_count;  /* face slots = 192 x block_count */
+} fl_owned_grid;
+
+typedef struct {
+  double sorted_position[3]; /* m, position at the last sort */
+  double trial_position[3];  /* m, position used for this transfer */
+  double mass;               /* kg */
+  double velocity[3];        /* m/s */
+  double slopes[9];          /* APIC slope rows (x, y, z), 1/s */
+  int64_t side_tag;
+  uint8_t affine_enabled;
+  uint8_t pad[7];
+} fl_boundary_particle;
+
+typedef struct {
+  int64_t side_tag;
+  uint8_t structurally_eligible;
+  uint8_t pad[7];
+} fl_face_tag;
+
+typedef struct {
+  int64_t mass;     /* quanta */
+  int64_t momentum; /* quanta */
+  int64_t stress;   /* reserved, zero for liquid */
+} fl_face_quanta;
+
+typedef struct {
+  double mass_per_quantum;     /* kg, a positive normal power of two */
+  double momentum_per_quantum; /* kg m/s, a positive normal power of two */
+  uint64_t declared_capacity;  /* declared particle capacity, <= 1024 */
+} fl_quantization;
+
+typedef struct {
+  uint64_t face_slot;
+  uint8_t compatible;
+  uint8_t pad[7];
+  double normalized_weight;
+  double normalized_weight_gradient[3]; /* 1/m */
+  double centered_face_offset[3];       /* m */
+} fl_compatible_sample;
+
+typedef struct {
+  uint8_t available;
+  uint8_t pad[7];
+  int64_t side_tag;
+  double unit_normal[3];
+  double wall_velocity[3]; /* m/s */
+} fl_wall_sample;
+
+/* Validity: 0 missing, 1 valid, 2 predicted, 3 low mass (LiquidFaceValidity3D). */
+typedef struct {
+  double velocity_sample_time; /* s */
+  double wall_sample_time;     /* s */
+  const double* face_velocities;
+  const uint8_t* validity;
+  const fl_face_tag* face_tags;
+  const fl_wall_sample* walls;
+} fl_velocity_history;
+
+typedef struct {
+  double new_pic_velocity[3];
+  double grid_velocity_increment[3];
+  double particle_minus_old_pic_velocity[3];
+  double fitted_velocity_slopes[9]; /* rows, 1/s */
+  double velocity_gradient[9];      /* rows, 1/s */
+  uint8_t affine_enabled;
+  uint8_t old_pic_fallback;
+  uint8_t new_pic_fallback;
+  uint8_t low_mass_fallback;
+  uint8_t pad[4];
+} fl_gathered_particle;
+
+int fl_boundary_create(fl_boundary** out);
+int fl_boundary_destroy(fl_boundary* boundary);
+
+/* DepositCompatibleMacQuanta3D: quanta per face slot and 3 x 27 compatible
+ * samples per particle (particle, component, stencil (z,y,x) order). */
+int fl_boundary_deposit(fl_boundary* boundary, const fl_owned_grid* grid, const fl_boundary_particle* particles,
+                        uint64_t particle_count, const fl_face_tag* face_tags, const fl_quantization* quantization,
+                        fl_face_quanta* face_quanta, fl_compatible_sample* compatible_stencils,
+                        fl_measurement* measurement);
+
+/* NormalizeLiquidMacFaces3D: masses (kg), velocities (m/s, 0 unless valid), validity. */
+int fl_boundary_normalize(fl_boundary* boundary, const fl_face_quanta* face_quanta, uint64_t face_count,
+                          const fl_quantization* quantization, double minimum_face_mass, double* face_masses,
+                          double* face_velocities, uint8_t* validity, fl_measurement* measurement);
+
+/* The CPU table's .forces: predicted = old + dt * acceleration[normal axis], per slot. */
+int fl_boundary_forces(fl_boundary* boundary, const fl_owned_grid* grid, const double* old_face_velocities,
+                       const double acceleration[3], double step_duration, double* predicted_face_velocities,
+                       fl_measurement* measurement);
+
+/* The CPU table's .predict_missing_face: the old history continued at one slot
+ * (same-side donors within 2h, wall projection) plus dt * acceleration. */
+int fl_boundary_predict_face(fl_boundary* boundary, const fl_owned_grid* grid, const fl_velocity_history* old_history,
+                             uint64_t face_slot, int64_t side_tag, const double acceleration[3],
+                             double step_duration, double* predicted_face_velocity, fl_measurement* measurement);
+
+/* GatherLiquidBoundaryParticles3D: one record per particle in input order;
+ * fallback_counts = old PIC, new PIC and low-mass fallback particle counts. */
+int fl_boundary_gather(fl_boundary* boundary, const fl_owned_grid* grid, const fl_boundary_particle* particles,
+                       uint64_t particle_count, double old_time, double new_time,
+                       const fl_velocity_history* old_history, const fl_velocity_history* new_history,
+                       fl_gathered_particle* gathered, uint64_t fallback_counts[3], fl_measurement* measurement);
 
 #ifdef __cplusplus
 }

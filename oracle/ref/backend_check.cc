@@ -1,0 +1,294 @@
+// Table-against-table harness for the liquid scheduler's backend operations.
+// Test infrastructure only (the checker, never the product).
+//
+// Each bk_* entry runs ONE operation of a LiquidSubstepBackend3D table on host
+// arrays: which == 0 the reference's own CPU table (CpuLiquidSubstepBackend3D,
+// native/src/liquid_substep_3d_cpu.cc:703-859, compiled from its sources into
+// libfluidity_ref.so), which == 1 the B200 table
+// (B200LiquidBackend3D::operations(), fluidity_b200/adapter). Both receive the
+// same SparseMacGrid3D, the same spans and fresh reference workspaces, so a
+// test compares the two tables' outputs directly. The records are the
+// reference's own types, passed through as bytes (their layouts match the
+// C-ABI's, which the adapter checks at compile time). Every entry returns the
+// operation's absl status code (0 = OK) and writes its outputs only on OK.
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <span>
+#include <vector>
+
+#include "b200_liquid_substep_backend_3d.h"
+#include "fluidity/host/liquid_boundary_workspace_3d.h"
+#include "fluidity/host/mac_pressure_workspace_3d.h"
+#include "fluidity/host/sparse_mac_grid_3d.h"
+
+using namespace fluidity;
+
+namespace {
+
+constexpr std::size_t kParticles = 1024;
+constexpr std::size_t kFaces = 24576;
+constexpr std::size_t kCells = 4096;
+
+std::unique_ptr<B200LiquidBackend3D>& B200() {
+  static std::unique_ptr<B200LiquidBackend3D> backend;
+  return backend;
+}
+
+// The table for `which`, or nullptr (with *code set) when it cannot be made.
+const LiquidSubstepBackend3D* Table(int which, int* code) {
+  static LiquidSubstepBackend3D cpu = CpuLiquidSubstepBackend3D();
+  static LiquidSubstepBackend3D b200{};
+  *code = 0;
+  if (which == 0) return &cpu;
+  if (!B200()) {
+    auto made = B200LiquidBackend3D::Create();
+    if (!made.ok()) {
+      *code = static_cast<int>(made.status().code());
+      return nullptr;
+    }
+    B200() = std::move(*made);
+    b200 = B200()->operations();
+  }
+  return &b200;
+}
+
+int Code(const absl::Status& s) { return static_cast<int>(s.code()); }
+
+std::vector<BlockIndex3D> Blocks(const int32_t* blocks, uint64_t nb) {
+  std::vector<BlockIndex3D> out(nb);
+  for (uint64_t i = 0; i < nb; ++i) out[i] = {blocks[3 * i], blocks[3 * i + 1], blocks[3 * i + 2]};
+  return out;
+}
+
+absl::StatusOr<SparseMacGrid3D> Grid(const double origin[3], double h, const int32_t* blocks, uint64_t nb) {
+  return SparseMacGrid3D::Create({{origin[0], origin[1], origin[2]}, h}, Blocks(blocks, nb), nb);
+}
+
+absl::StatusOr<LiquidBoundaryWorkspace3D> Workspace() {
+  LiquidStateCapacities3D caps{};
+  caps.particles = kParticles;
+  caps.blocks = kFaces / 192;
+  caps.cells = kCells;
+  caps.faces = kFaces;
+  return LiquidBoundaryWorkspace3D::Create(caps);
+}
+
+template <typename T>
+std::span<const T> Span(const void* data, uint64_t count) {
+  return std::span<const T>(static_cast<const T*>(data), count);
+}
+
+LiquidBoundaryVelocityHistory3D History(double time, const double* velocities, const uint8_t* validity,
+                                        const void* tags, const void* walls, uint64_t faces) {
+  return LiquidBoundaryVelocityHistory3D{
+      .velocity_sample_time = time,
+      .wall_sample_time = time,
+      .face_velocities = std::span<const double>(velocities, faces),
+      .validity = Span<LiquidFaceValidity3D>(validity, faces),
+      .face_tags = Span<LiquidBoundaryFaceTag3D>(tags, faces),
+      .wall_samples = Span<LiquidPrescribedWallSample3D>(walls, faces),
+  };
+}
+
+}  // namespace
+
+extern "C" {
+
+// .deposit: quanta (3 x int64 per slot) and 81 compatible samples per particle.
+int bk_deposit(int which, const double origin[3], double h, const int32_t* blocks, uint64_t nb,
+               const void* particles, uint64_t n, const void* tags, double mass_q, double momentum_q,
+               uint64_t declared_capacity, void* quanta_out, void* stencils_out) {
+  int code = 0;
+  const auto* table = Table(which, &code);
+  if (!table) return code;
+  auto grid = Grid(origin, h, blocks, nb);
+  if (!grid.ok()) return Code(grid.status());
+  auto ws = Workspace();
+  if (!ws.ok()) return Code(ws.status());
+  const std::size_t faces = grid->face_count();
+  const LiquidBoundaryDepositViewInputs3D inputs{grid->view(), Span<LiquidBoundaryParticle3D>(particles, n),
+                                                 Span<LiquidBoundaryFaceTag3D>(tags, faces),
+                                                 MacDepositQuantization3D{mass_q, momentum_q, declared_capacity}};
+  auto r = table->deposit(table->context, inputs, *ws);
+  if (!r.ok()) return Code(r.status());
+  std::memcpy(quanta_out, r->face_quanta.data(), r->face_quanta.size_bytes());
+  std::memcpy(stencils_out, r->compatible_stencils.data(), r->compatible_stencils.size_bytes());
+  return 0;
+}
+
+// .normalize: masses, velocities and validity per slot.
+int bk_normalize(int which, const void* quanta, uint64_t count, double mass_q, double momentum_q,
+                 uint64_t declared_capacity, double minimum_face_mass, double* masses, double* velocities,
+                 uint8_t* validity) {
+  int code = 0;
+  const auto* table = Table(which, &code);
+  if (!table) return code;
+  auto ws = Workspace();
+  if (!ws.ok()) return Code(ws.status());
+  auto r = table->normalize(table->context, Span<MacFaceDepositQuanta3D>(quanta, count),
+                            MacDepositQuantization3D{mass_q, momentum_q, declared_capacity}, minimum_face_mass, *ws);
+  if (!r.ok()) return Code(r.status());
+  std::memcpy(masses, r->face_masses.data(), r->face_masses.size_bytes());
+  std::memcpy(velocities, r->face_velocities.data(), r->face_velocities.size_bytes());
+  std::memcpy(validity, r->validity.data(), r->validity.size_bytes());
+  return 0;
+}
+
+// .forces: predicted velocity per slot.
+int bk_forces(int which, const double origin[3], double h, const int32_t* blocks, uint64_t nb,
+              const double* old_velocities, const double acceleration[3], double dt, double* predicted) {
+  int code = 0;
+  const auto* table = Table(which, &code);
+  if (!table) return code;
+  auto grid = Grid(origin, h, blocks, nb);
+  if (!grid.ok()) return Code(grid.status());
+  const std::size_t faces = grid->face_count();
+  std::vector<double> out(faces, 0.0);
+  const auto s = table->forces(table->context, grid->view(), std::span<const double>(old_velocities, faces),
+                               Vec3{acceleration[0], acceleration[1], acceleration[2]}, dt, out);
+  if (!s.ok()) return Code(s);
+  std::memcpy(predicted, out.data(), sizeof(double) * faces);
+  return 0;
+}
+
+// .predict_missing_face on the old history at `time`.
+int bk_predict(int which, const double origin[3], double h, const int32_t* blocks, uint64_t nb, double time,
+               const double* velocities, const uint8_t* validity, const void* tags, const void* walls,
+               uint64_t slot, int64_t side, const double acceleration[3], double dt, double* predicted) {
+  int code = 0;
+  const auto* table = Table(which, &code);
+  if (!table) return code;
+  auto grid = Grid(origin, h, blocks, nb);
+  if (!grid.ok()) return Code(grid.status());
+  auto ws = Workspace();
+  if (!ws.ok()) return Code(ws.status());
+  const LiquidMissingFacePredictionInputs3D inputs{
+      grid->view(), History(time, velocities, validity, tags, walls, grid->face_count()), slot, side,
+      Vec3{acceleration[0], acceleration[1], acceleration[2]}, dt};
+  auto r = table->predict_missing_face(table->context, inputs, *ws);
+  if (!r.ok()) return Code(r.status());
+  *predicted = *r;
+  return 0;
+}
+
+// .gather: one record per particle; counts = old PIC, new PIC, low-mass fallbacks.
+int bk_gather(int which, const double origin[3], double h, const int32_t* blocks, uint64_t nb,
+              const void* particles, uint64_t n, double old_time, double new_time, const double* old_velocities,
+              const uint8_t* old_validity, const void* old_tags, const void* old_walls,
+              const double* new_velocities, const uint8_t* new_validity, const void* new_tags,
+              const void* new_walls, void* gathered, uint64_t counts[3]) {
+  int code = 0;
+  const auto* table = Table(which, &code);
+  if (!table) return code;
+  auto grid = Grid(origin, h, blocks, nb);
+  if (!grid.ok()) return Code(grid.status());
+  auto ws = Workspace();
+  if (!ws.ok()) return Code(ws.status());
+  const std::size_t faces = grid->face_count();
+  const LiquidBoundaryGatherViewInputs3D inputs{
+      grid->view(), Span<LiquidBoundaryParticle3D>(particles, n), old_time, new_time,
+      History(old_time, old_velocities, old_validity, old_tags, old_walls, faces),
+      History(new_time, new_velocities, new_validity, new_tags, new_walls, faces)};
+  auto r = table->gather(table->context, inputs, *ws);
+  if (!r.ok()) return Code(r.status());
+  std::memcpy(gathered, r->particles.data(), r->particles.size_bytes());
+  counts[0] = r->old_pic_fallback_particle_count;
+  counts[1] = r->new_pic_fallback_particle_count;
+  counts[2] = r->low_mass_fallback_particle_count;
+  return 0;
+}
+
+// .project on cells (x,y,z; volume, target divergence, bulk modulus (0 = +inf),
+// previous pressure, inward wall flux) and faces in owned-slot order (axis,x,y,z;
+// kind 0 sealed / 1 internal / 2 Dirichlet; area, inverse density, distance,
+// predicted velocity, wall velocity, jump or exterior pressure; explicit wall
+// flux, NaN when absent). diag: iterations, true residual, max |r|/V, max
+// defect, gauge count; measure: RHS norm, cell volume, inward explicit flux.
+int bk_project(int which, const double origin[3], double h, const int32_t* blocks, uint64_t nb, double dt,
+               const int32_t* cell_index, const double* cell_values, uint64_t nc, const int32_t* face_index,
+               const int32_t* face_kind, const double* face_values, const double* face_flux, uint64_t nf,
+               uint64_t max_iterations, double tolerance_scale, double* pressure, double* corrected_u,
+               double* rhs, double* residual, double* defect, double diag[5], double measure[3]) {
+  int code = 0;
+  const auto* table = Table(which, &code);
+  if (!table) return code;
+  auto grid = Grid(origin, h, blocks, nb);
+  if (!grid.ok()) return Code(grid.status());
+  auto ws = MacPressureWorkspace3D::Create(kCells, kFaces);
+  if (!ws.ok()) return Code(ws.status());
+  std::vector<MacPressureCell3D> cells(nc);
+  for (uint64_t i = 0; i < nc; ++i) {
+    const double* v = cell_values + 5 * i;
+    cells[i].cell_index = {cell_index[3 * i], cell_index[3 * i + 1], cell_index[3 * i + 2]};
+    cells[i].fluid_volume = v[0];
+    cells[i].target_divergence = v[1];
+    cells[i].bulk_modulus = v[2] == 0.0 ? HUGE_VAL : v[2];
+    cells[i].previous_pressure = v[3];
+    cells[i].integrated_inward_wall_flux = v[4];
+  }
+  std::vector<MacPressureFace3D> faces(nf);
+  for (uint64_t f = 0; f < nf; ++f) {
+    const double* v = face_values + 6 * f;
+    MacPressureFace3D face{};
+    face.face_index = {static_cast<FaceNormalAxis>(face_index[4 * f]),
+                       {face_index[4 * f + 1], face_index[4 * f + 2], face_index[4 * f + 3]}};
+    face.open_area = v[0];
+    face.inverse_density = v[1];
+    face.pressure_gradient_distance = v[2];
+    face.predicted_normal_velocity = v[3];
+    face.wall_normal_velocity = v[4];
+    if (face_kind[f] == 1) {
+      face.pressure_link = InternalMacPressureLink3D{v[5]};
+    } else if (face_kind[f] == 2) {
+      face.pressure_link = DirichletMacPressureLink3D{v[5]};
+    } else {
+      face.pressure_link = SealedMacPressureLink3D{};
+    }
+    if (face_flux && face_flux[f] == face_flux[f]) face.prescribed_wall_flux = face_flux[f];
+    faces[f] = face;
+  }
+  const LiquidPressureProblemView3D problem{cells, faces};
+  auto r = table->project(table->context, grid->view(), dt, problem,
+                          MacPressureSolverOptions3D{max_iterations, tolerance_scale}, *ws);
+  if (!r.ok()) return Code(r.status());
+  std::memcpy(pressure, r->cell_pressures.data(), r->cell_pressures.size_bytes());
+  std::memcpy(corrected_u, r->corrected_face_velocities.data(), r->corrected_face_velocities.size_bytes());
+  std::memcpy(rhs, r->integrated_rhs.data(), r->integrated_rhs.size_bytes());
+  std::memcpy(residual, r->true_residuals.data(), r->true_residuals.size_bytes());
+  std::memcpy(defect, r->cell_constraint_defects.data(), r->cell_constraint_defects.size_bytes());
+  diag[0] = static_cast<double>(r->diagnostics.iteration_count);
+  diag[1] = r->diagnostics.true_residual_l2;
+  diag[2] = r->diagnostics.max_volume_scaled_residual;
+  diag[3] = r->diagnostics.max_cell_constraint_defect;
+  diag[4] = static_cast<double>(r->gauge_cell_ordinals.size());
+  measure[0] = r->frozen_measurement.integrated_rhs_l2_m3_per_s;
+  measure[1] = r->frozen_measurement.pressure_cell_volume_m3;
+  measure[2] = r->frozen_measurement.inward_prescribed_wall_flux_m3_per_s;
+  return 0;
+}
+
+// Which operations each table fills (bit k: deposit, normalize, predict,
+// forces, gather, project, topology, update_particles).
+int bk_filled(int which, uint32_t* mask) {
+  int code = 0;
+  const auto* table = Table(which, &code);
+  if (!table) return code;
+  const void* ops[] = {reinterpret_cast<const void*>(table->deposit),
+                       reinterpret_cast<const void*>(table->normalize),
+                       reinterpret_cast<const void*>(table->predict_missing_face),
+                       reinterpret_cast<const void*>(table->forces),
+                       reinterpret_cast<const void*>(table->gather),
+                       reinterpret_cast<const void*>(table->project),
+                       reinterpret_cast<const void*>(table->topology),
+                       reinterpret_cast<const void*>(table->update_particles)};
+  *mask = 0;
+  for (int k = 0; k < 8; ++k)
+    if (ops[k]) *mask |= 1u << k;
+  return 0;
+}
+
+// Drops the B200 table's backend (its device storage) before the process exits.
+void bk_release() { B200().reset(); }
+
+}  // extern "C"

@@ -1,0 +1,212 @@
+"""ctypes view of the backend-table harness (oracle/_ref/libfluidity_backend_check.so)
+and the bounded 32^3 tank dam break the table tests run on.
+
+The harness runs one LiquidSubstepBackend3D operation through the reference's
+own CPU table (which=0) or the B200 table (which=1) on the same inputs. The
+numpy record dtypes below are the reference's record layouts
+(liquid_boundary_transfer_types_3d.h:4-45, mac_transfer_types_3d.h:7-30).
+
+Scene: a 32^3 tank (h = 1/32 m, walls on the lattice planes 0 and 32) with a
+4 x 8 x 4-cell water column in its low corner, 8 particles per cell (1024,
+the boundary path's particle cap), small seeded velocities and APIC slopes,
+trial positions moved less than half a cell. Faces inside the tank are
+structurally eligible; faces on or beyond the tank's walls are ineligible and
+carry a prescribed wall at rest (the inward normal of the first low wall they
+lie on or beyond). With mixed_sides the column's top two cell layers (y >= 6)
+carry side tag 1, as do the faces and walls there, so the compatible-support
+masks mix sides; a ghost of one side next to the other side's walls then has
+no support, so the gather runs on the one-sided scene. Active 4^3 blocks: x, z in [-1, 2],
+y in [-1, 3] (80 blocks, 15360 face slots).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+import oracle
+
+LIB_PATH = oracle.HERE / "_ref" / "libfluidity_backend_check.so"
+
+PARTICLE = np.dtype([("sorted", "<f8", 3), ("trial", "<f8", 3), ("mass", "<f8"), ("velocity", "<f8", 3),
+                     ("slopes", "<f8", 9), ("side", "<i8"), ("affine", "u1"), ("pad", "u1", 7)])
+TAG = np.dtype([("side", "<i8"), ("eligible", "u1"), ("pad", "u1", 7)])
+QUANTA = np.dtype([("mass", "<i8"), ("momentum", "<i8"), ("stress", "<i8")])
+SAMPLE = np.dtype([("slot", "<u8"), ("compatible", "u1"), ("pad", "u1", 7), ("weight", "<f8"),
+                   ("gradient", "<f8", 3), ("centered", "<f8", 3)])
+WALL = np.dtype([("available", "u1"), ("pad", "u1", 7), ("side", "<i8"), ("normal", "<f8", 3),
+                 ("velocity", "<f8", 3)])
+GATHERED = np.dtype([("new_pic", "<f8", 3), ("increment", "<f8", 3), ("retained", "<f8", 3), ("slopes", "<f8", 9),
+                     ("gradient", "<f8", 9), ("affine", "u1"), ("old_fallback", "u1"), ("new_fallback", "u1"),
+                     ("low_mass", "u1"), ("pad", "u1", 4)])
+assert (PARTICLE.itemsize, TAG.itemsize, QUANTA.itemsize, SAMPLE.itemsize, WALL.itemsize, GATHERED.itemsize) == (
+    168, 16, 24, 72, 64, 224)
+
+CPU, B200 = 0, 1
+MASS_Q = 2.0 ** -40
+MOMENTUM_Q = 2.0 ** -40
+N = 32
+H = 1.0 / N
+DT = 1.0 / 240.0
+GRAVITY = (0.0, -9.81, 0.0)
+
+
+def available() -> bool:
+    return LIB_PATH.exists()
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(str(LIB_PATH))
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def _d3(v):
+    return (ctypes.c_double * 3)(*[float(x) for x in v])
+
+
+def filled(which):
+    m = ctypes.c_uint32(0)
+    code = lib().bk_filled(ctypes.c_int(which), ctypes.byref(m))
+    return code, m.value
+
+
+class Scene:
+    """The bounded tank dam break, its face tags and walls."""
+
+    def __init__(self, seed: int = 7, mixed_sides: bool = True):
+        rng = np.random.default_rng(seed)
+        self.origin = np.zeros(3)
+        bz, by, bx = np.meshgrid(np.arange(-1, 3), np.arange(-1, 4), np.arange(-1, 3), indexing="ij")
+        self.blocks = np.stack([bx.ravel(), by.ravel(), bz.ravel()], 1).astype(np.int32)  # (z,y,x) order
+        self.faces = 192 * len(self.blocks)
+        cz, cy, cx = np.meshgrid(np.arange(4), np.arange(8), np.arange(4), indexing="ij")
+        cells = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], 1).astype(np.float64)
+        sub = np.array([[i, j, k] for k in (0.25, 0.75) for j in (0.25, 0.75) for i in (0.25, 0.75)])
+        pos = (cells[:, None, :] + sub[None] + rng.uniform(-0.2, 0.2, (len(cells), 8, 3))).reshape(-1, 3)
+        n = len(pos)
+        p = np.zeros(n, PARTICLE)
+        p["sorted"] = pos * H
+        trial = pos + rng.uniform(-0.3, 0.3, pos.shape)
+        trial = np.clip(trial, 0.02, None)
+        trial = np.minimum(np.maximum(trial, pos - 0.45), pos + 0.45)
+        p["trial"] = trial * H
+        p["mass"] = 1000.0 * H ** 3 / 8
+        p["velocity"] = rng.uniform(-0.5, 0.5, (n, 3))
+        p["slopes"] = rng.uniform(-2.0, 2.0, (n, 9))
+        p["side"] = (pos[:, 1] >= 6.0).astype(np.int64) if mixed_sides else 0
+        p["affine"] = (np.arange(n) % 16 != 5).astype(np.uint8)
+        self.particles = p
+        # face slots: block ordinal, axis, local (z,y,x)
+        slot = np.arange(self.faces)
+        blk = self.blocks[slot // 192]
+        axis = (slot % 192) // 64
+        local = slot % 64
+        lat = blk * 4 + np.stack([local % 4, (local // 4) % 4, local // 16], 1)
+        self.axis, self.lattice = axis, lat
+        inside = np.ones(self.faces, bool)
+        for a in range(3):
+            on = axis == a
+            inside &= np.where(on, (lat[:, a] > 0) & (lat[:, a] < N), (lat[:, a] >= 0) & (lat[:, a] < N))
+        tags = np.zeros(self.faces, TAG)
+        tags["eligible"] = inside.astype(np.uint8)
+        tags["side"] = (lat[:, 1] >= 6).astype(np.int64) if mixed_sides else 0
+        self.tags = tags
+        # every ineligible face is a prescribed wall at rest, its normal the
+        # inward normal of the first low tank wall it lies on or beyond
+        walls = np.zeros(self.faces, WALL)
+        walls["available"] = (~inside).astype(np.uint8)
+        walls["side"] = tags["side"]
+        normal_axis = np.full(self.faces, -1)
+        for a in (2, 1, 0):
+            low = np.where(axis == a, lat[:, a] <= 0, lat[:, a] < 0)
+            normal_axis = np.where(low, a, normal_axis)
+        normal_axis = np.where((normal_axis < 0) & ~inside, axis, normal_axis)
+        rows = np.nonzero(~inside)[0]
+        walls["normal"][rows, normal_axis[rows]] = 1.0
+        self.walls = walls
+
+    def grid_args(self):
+        return (_d3(self.origin), ctypes.c_double(H), _p(self.blocks), ctypes.c_uint64(len(self.blocks)))
+
+
+def deposit(which, s: Scene, particles=None, tags=None, capacity=1024):
+    particles = s.particles if particles is None else particles
+    tags = s.tags if tags is None else tags
+    q = np.zeros(s.faces, QUANTA)
+    st = np.zeros((len(particles), 3, 27), SAMPLE)
+    code = lib().bk_deposit(ctypes.c_int(which), *s.grid_args(), _p(particles), ctypes.c_uint64(len(particles)),
+                            _p(tags), ctypes.c_double(MASS_Q), ctypes.c_double(MOMENTUM_Q), ctypes.c_uint64(capacity),
+                            _p(q), _p(st))
+    return code, q, st
+
+
+def normalize(which, quanta, min_mass, capacity=1024):
+    n = len(quanta)
+    m, v, val = np.zeros(n), np.zeros(n), np.zeros(n, np.uint8)
+    code = lib().bk_normalize(ctypes.c_int(which), _p(quanta), ctypes.c_uint64(n), ctypes.c_double(MASS_Q),
+                              ctypes.c_double(MOMENTUM_Q), ctypes.c_uint64(capacity), ctypes.c_double(min_mass),
+                              _p(m), _p(v), _p(val))
+    return code, m, v, val
+
+
+def forces(which, s: Scene, old, acceleration=GRAVITY, dt=DT):
+    out = np.zeros(s.faces)
+    code = lib().bk_forces(ctypes.c_int(which), *s.grid_args(), _p(np.ascontiguousarray(old)), _d3(acceleration),
+                           ctypes.c_double(dt), _p(out))
+    return code, out
+
+
+def predict(which, s: Scene, velocities, validity, slot, side, acceleration=GRAVITY, dt=DT, time=0.0):
+    out = ctypes.c_double(np.nan)
+    code = lib().bk_predict(ctypes.c_int(which), *s.grid_args(), ctypes.c_double(time), _p(velocities),
+                            _p(validity), _p(s.tags), _p(s.walls), ctypes.c_uint64(slot), ctypes.c_int64(side),
+                            _d3(acceleration), ctypes.c_double(dt), ctypes.byref(out))
+    return code, out.value
+
+
+def gather(which, s: Scene, old, new, t0=0.0, t1=DT, particles=None):
+    """old/new: (velocities, validity) per slot; tags and walls are the scene's."""
+    particles = s.particles if particles is None else particles
+    out = np.zeros(len(particles), GATHERED)
+    counts = (ctypes.c_uint64 * 3)()
+    code = lib().bk_gather(ctypes.c_int(which), *s.grid_args(), _p(particles), ctypes.c_uint64(len(particles)),
+                           ctypes.c_double(t0), ctypes.c_double(t1), _p(old[0]), _p(old[1]), _p(s.tags),
+                           _p(s.walls), _p(new[0]), _p(new[1]), _p(s.tags), _p(s.walls), _p(out), counts)
+    return code, out, np.array(counts[:], np.uint64)
+
+
+def project(which, system, h, dt, max_iterations=256, tolerance_scale=1.0, face_flux=None):
+    """system: oracle.box_system.box_pressure_system output (faces in owned-slot order)."""
+    ci, cv = system["cells_idx"], system["cells_val"]
+    fi, fk, fv = system["faces_idx"], system["faces_kind"], system["faces_val"]
+    lat = fi[:, 1:4].astype(np.int64)
+    owners = np.unique(np.floor_divide(lat, 4), axis=0)
+    owners = owners[np.lexsort((owners[:, 0], owners[:, 1], owners[:, 2]))].astype(np.int32)
+    nc, nf = len(ci), len(fi)
+    outs = [np.zeros(nc), np.zeros(nf), np.zeros(nc), np.zeros(nc), np.zeros(nc)]
+    diag, meas = (ctypes.c_double * 5)(), (ctypes.c_double * 3)()
+    flux = None if face_flux is None else np.ascontiguousarray(face_flux, np.float64)
+    code = lib().bk_project(ctypes.c_int(which), _d3((0, 0, 0)), ctypes.c_double(h), _p(owners),
+                            ctypes.c_uint64(len(owners)), ctypes.c_double(dt), _p(np.ascontiguousarray(ci, np.int32)),
+                            _p(np.ascontiguousarray(cv, np.float64)), ctypes.c_uint64(nc),
+                            _p(np.ascontiguousarray(fi, np.int32)), _p(np.ascontiguousarray(fk, np.int32)),
+                            _p(np.ascontiguousarray(fv, np.float64)), _p(flux), ctypes.c_uint64(nf),
+                            ctypes.c_uint64(max_iterations), ctypes.c_double(tolerance_scale), *map(_p, outs), diag,
+                            meas)
+    keys = ("pressure", "corrected_u", "rhs", "residual", "defect")
+    return code, dict(zip(keys, outs), diag=np.array(diag[:]), measure=np.array(meas[:]))
+
+
+def release():
+    if _lib is not None:
+        _lib.bk_release()

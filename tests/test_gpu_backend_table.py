@@ -1,0 +1,198 @@
+"""The B200 liquid-scheduler backend table against the reference's own CPU table.
+
+Both tables (LiquidSubstepBackend3D, liquid_substep_backend_3d.h:47-260) run
+the same operation on the same inputs through oracle/_ref/
+libfluidity_backend_check.so: the CPU table is CpuLiquidSubstepBackend3D
+compiled from the reference's sources (liquid_substep_3d_cpu.cc:703-859), the
+B200 table is fluidity_b200/adapter over the library's FP64 boundary kernels
+and its MAC pressure solver. Scene: the bounded 32^3 tank dam break of
+tests/backend_tables.py (1024 particles, 80 blocks of 4^3 cells).
+
+Bars: deposit quanta and compatible stencils, normalized faces and forces
+bit-identical; the gather's flags and fallback counts identical and its
+values within 1e-12 of the largest magnitude (the ghost fits' hypot is the
+device's); predicted faces within 1e-12 relative; the projection within the
+solvers' common gate; error codes identical, including which of several
+failing particles decides the code.
+"""
+
+import numpy as np
+import pytest
+
+import backend_tables as bt
+from oracle.box_system import box_pressure_system
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not bt.available(), reason="backend harness not built")]
+
+CPU, B200 = bt.CPU, bt.B200
+
+
+@pytest.fixture(scope="module")
+def scene():
+    yield bt.Scene()
+    bt.release()
+
+
+@pytest.fixture(scope="module")
+def one_sided():
+    return bt.Scene(mixed_sides=False)
+
+
+@pytest.fixture(scope="module")
+def deposited(scene):
+    code, q, st = bt.deposit(CPU, scene)
+    assert code == 0
+    return q, st
+
+
+@pytest.fixture(scope="module")
+def histories(one_sided):
+    """On the one-sided scene: old history, the CPU table's normalized deposit
+    (some faces low-mass); new, the CPU forces on it, perturbed on valid faces
+    as a projection would, with missing faces next to the water marked
+    predicted."""
+    scene = one_sided
+    code, q, _ = bt.deposit(CPU, scene)
+    assert code == 0
+    min_mass = 0.1 * float(scene.particles["mass"][0])
+    code, m, v, val = bt.normalize(CPU, q, min_mass)
+    assert code == 0
+    code, pred = bt.forces(CPU, scene, v)
+    assert code == 0
+    rng = np.random.default_rng(3)
+    new_v = pred + np.where(val == 1, rng.uniform(-0.05, 0.05, len(pred)), 0.0)
+    new_val = val.copy()
+    missing_inside = np.nonzero((val == 0) & (scene.tags["eligible"] == 1) & (scene.lattice[:, 1] < 10)
+                                & (scene.lattice[:, 0] < 6) & (scene.lattice[:, 2] < 6))[0]
+    marked = []
+    for slot in missing_inside[::2][:40]:
+        side = int(scene.tags["side"][slot])
+        c, value = bt.predict(CPU, scene, v, val, int(slot), side)
+        if c == 0:
+            new_v[slot] = value
+            new_val[slot] = 2
+            marked.append(int(slot))
+    assert len(marked) >= 10
+    return dict(min_mass=min_mass, old=(v, val), new=(new_v, new_val), masses=m, predicted_slots=marked,
+                missing=missing_inside)
+
+
+def test_tables_fill_the_transfer_and_projection_operations():
+    code, cpu = bt.filled(CPU)
+    assert code == 0 and cpu == 0xFF
+    code, b200 = bt.filled(B200)
+    assert code == 0
+    assert b200 == 0x3F  # deposit, normalize, predict, forces, gather, project; no topology or particle update
+
+
+def test_deposit_is_bit_identical(scene, deposited):
+    q_cpu, st_cpu = deposited
+    code, q, st = bt.deposit(B200, scene)
+    assert code == 0
+    assert np.array_equal(q, q_cpu)
+    for f in ("slot", "compatible", "weight", "gradient", "centered"):
+        assert np.array_equal(st[f], st_cpu[f]), f
+    # the scene exercises partial support: walls, outside faces and mixed sides
+    frac = st_cpu["compatible"].mean()
+    assert 0.5 < frac < 1.0
+    assert np.count_nonzero(q_cpu["mass"]) > 500
+
+
+def test_normalize_and_forces_are_bit_identical(scene, deposited, histories):
+    q, _ = deposited
+    cpu = bt.normalize(CPU, q, histories["min_mass"])
+    b200 = bt.normalize(B200, q, histories["min_mass"])
+    assert cpu[0] == 0 and b200[0] == 0
+    for a, b in zip(cpu[1:], b200[1:]):
+        assert np.array_equal(a, b)
+    val = cpu[3]
+    assert {0, 1, 3} <= set(np.unique(val).tolist())  # missing, valid and low-mass faces all occur
+    c0, f_cpu = bt.forces(CPU, scene, cpu[2])
+    c1, f_b200 = bt.forces(B200, scene, cpu[2])
+    assert c0 == 0 and c1 == 0
+    assert np.array_equal(f_cpu, f_b200)
+
+
+def test_predict_missing_face_matches(scene, one_sided, histories):
+    v, val = histories["old"]
+    checked = 0
+    for slot in histories["missing"][:60]:
+        for sc, side in ((one_sided, 0), (scene, 0), (scene, 1)):
+            c0, a = bt.predict(CPU, sc, v, val, int(slot), side)
+            c1, b = bt.predict(B200, sc, v, val, int(slot), side)
+            assert c0 == c1, (slot, side)
+            if c0 == 0:
+                assert abs(a - b) <= 1e-12 * max(abs(a), 1.0), (slot, side, a, b)
+                checked += 1
+    assert checked >= 60
+
+
+def test_gather_matches(one_sided, histories):
+    c0, g_cpu, n_cpu = bt.gather(CPU, one_sided, histories["old"], histories["new"])
+    c1, g, n = bt.gather(B200, one_sided, histories["old"], histories["new"])
+    assert c0 == 0 and c1 == 0
+    assert np.array_equal(n, n_cpu)
+    for f in ("affine", "old_fallback", "new_fallback", "low_mass"):
+        assert np.array_equal(g[f], g_cpu[f]), f
+    for f in ("new_pic", "increment", "retained", "slopes", "gradient"):
+        scale = max(np.abs(g_cpu[f]).max(), 1.0)
+        err = np.abs(g[f] - g_cpu[f]).max() / scale
+        assert err <= 1e-12, (f, err)
+    print(f"gather: fallback counts {n_cpu.tolist()}, affine on {int(g_cpu['affine'].sum())} of {len(g_cpu)}")
+    assert n_cpu[0] > 0 and n_cpu[2] > 0 and g_cpu["affine"].sum() > 100
+
+
+def test_error_codes_follow_the_cpu_order(scene):
+    p = scene.particles.copy()
+    p["velocity"][700, 1] = np.nan  # InvalidArgument at particle 700
+    p["trial"][300, 0] = p["sorted"][300, 0] + 0.75 * bt.H  # moved beyond half a cell: FailedPrecondition at 300
+    for which in (CPU, B200):
+        assert bt.deposit(which, scene, particles=p)[0] == 9
+    p["trial"][300, 0] = p["sorted"][300, 0]
+    for which in (CPU, B200):
+        assert bt.deposit(which, scene, particles=p)[0] == 3
+    assert bt.deposit(CPU, scene, capacity=512)[0] == bt.deposit(B200, scene, capacity=512)[0] == 8
+    q = np.zeros(scene.faces, bt.QUANTA)
+    q["mass"][5] = -1
+    assert bt.normalize(CPU, q, 0.0)[0] == bt.normalize(B200, q, 0.0)[0] == 3
+    # a side with no compatible support anywhere in a stencil
+    p = scene.particles.copy()
+    p["side"][10] = 7
+    assert bt.deposit(CPU, scene, particles=p)[0] == bt.deposit(B200, scene, particles=p)[0] == 9
+
+
+def _dam_break_system():
+    import oracle
+    from fluidity_b200 import scenes
+    from helpers import box_for, soa_to_xvc
+
+    soa, m = scenes.dam_break(32)
+    x, v, c = soa_to_xvc(soa)
+    box = box_for(32)
+    fm, fq = oracle.p2g(box, x, v, c, m)
+    u_pred, _ = oracle.normalize_forces(box, fm, fq, 0.0, scenes.DT, scenes.GRAVITY)
+    ct = oracle.classify_cells(box, x)
+    return box, box_pressure_system(box, ct, u_pred), scenes.DT
+
+
+def test_project_matches_within_the_gate():
+    box, s, dt = _dam_break_system()
+    flux = np.full(len(s["faces_idx"]), np.nan)
+    sealed = np.nonzero(s["faces_kind"] == 0)[0]
+    flux[sealed[::5]] = 1e-7  # explicit wall flux on some sealed faces
+    c0, cpu = bt.project(CPU, s, box.h, dt, tolerance_scale=1e-3, face_flux=flux)
+    c1, b200 = bt.project(B200, s, box.h, dt, tolerance_scale=1e-3, face_flux=flux)
+    assert c0 == 0 and c1 == 0
+    np.testing.assert_allclose(b200["rhs"], cpu["rhs"], rtol=1e-12, atol=1e-18)
+    rhs_l2 = np.linalg.norm(cpu["rhs"])
+    gate = 1e-3 * (2e-6 + 2e-6 * rhs_l2)
+    assert cpu["diag"][1] <= gate and b200["diag"][1] <= gate
+    pmax = np.abs(cpu["pressure"]).max()
+    dp = np.abs(b200["pressure"] - cpu["pressure"]).max() / pmax
+    du = np.abs(b200["corrected_u"] - cpu["corrected_u"]).max() / np.abs(cpu["corrected_u"]).max()
+    print(f"project: {len(cpu['pressure'])} cells, iterations cpu {cpu['diag'][0]:.0f} b200 {b200['diag'][0]:.0f}, "
+          f"max |dp|/|p| {dp:.2e}, max |du|/|u| {du:.2e}")
+    assert dp <= 1e-5 and du <= 1e-5
+    np.testing.assert_allclose(b200["measure"][:2], cpu["measure"][:2], rtol=1e-12)
+    assert abs(b200["measure"][2] - cpu["measure"][2]) <= 1e-12 * max(abs(cpu["measure"][2]), 1e-12)
+    assert b200["diag"][4] == cpu["diag"][4] == 0
