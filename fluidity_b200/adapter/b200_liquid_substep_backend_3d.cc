@@ -335,8 +335,8 @@ struct B200BackendOps3D {
     const double rel_tol = options.cpu_residual_tolerance_scale < 1.0 ? 2e-6 * options.cpu_residual_tolerance_scale
                                                                        : 0.0;
     fl_mac_pressure_diagnostics d{};
-    const int code = fl_project_mac_pressure_3d(
-        h, step_duration, s.cell_index.data(), s.cell_values.data(), nc, s.face_index.data(), s.face_kind.data(),
+    const int code = fl_boundary_project(
+        self.boundary_, h, step_duration, s.cell_index.data(), s.cell_values.data(), nc, s.face_index.data(), s.face_kind.data(),
         s.face_values.data(), nf, static_cast<int>(options.max_iterations), rel_tol, bank.pressures.data(),
         bank.velocities.data(), bank.rhs.data(), bank.residuals.data(), bank.defects.data(),
         reinterpret_cast<std::uint64_t*>(bank.gauges.data()), &d, nullptr

@@ -11,7 +11,7 @@
 //   .predict_missing_face  fl_boundary_predict_face   (LiquidBoundaryWorkspace3D::ContinueFace + dt a)
 //   .forces                fl_boundary_forces         (the CPU table's ApplyForces)
 //   .gather                fl_boundary_gather         (GatherLiquidBoundaryParticles3D)
-//   .project               fl_project_mac_pressure_3d (ProjectMacPressure3D over a pressure problem)
+//   .project               fl_boundary_project        (ProjectMacPressure3D over a pressure problem)
 //   .initialize, publication and growth hooks: no device state outlives a call
 //
 // The scene-geometry, topology and particle-update operations (.sample_*,

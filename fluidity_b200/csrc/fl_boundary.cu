@@ -871,6 +871,7 @@ struct fl_boundary {
   char* dev = nullptr;
   char* pin = nullptr;
   int device = -1;
+  fl::MpScratch pressure;  // the bounded projection's scratch, reserved for its caps
 };
 
 namespace {
@@ -1017,7 +1018,7 @@ extern "C" int fl_boundary_create(fl_boundary** out) {
             cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreate(&b->e0) == cudaSuccess && cudaEventCreate(&b->e1) == cudaSuccess &&
             cudaMalloc(&b->dev, kRegions.total) == cudaSuccess &&
-            cudaMallocHost(&b->pin, kRegions.staged) == cudaSuccess;
+            cudaMallocHost(&b->pin, kRegions.staged) == cudaSuccess && b->pressure.reserve_caps();
   if (!ok) {
     cudaGetLastError();
     fl_boundary_destroy(b);
@@ -1031,6 +1032,7 @@ extern "C" int fl_boundary_destroy(fl_boundary* b) {
   if (!b) return FL_INVALID_ARGUMENT;
   if (b->device >= 0) cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  b->pressure.destroy();
   if (b->pin) cudaFreeHost(b->pin);
   if (b->dev) cudaFree(b->dev);
   if (b->e0) cudaEventDestroy(b->e0);
@@ -1235,4 +1237,20 @@ extern "C" int fl_boundary_gather(fl_boundary* b, const fl_owned_grid* grid, con
   if (counts)
     for (int k = 0; k < 3; ++k) counts[k] = c[k];
   return FL_OK;
+}
+
+extern "C" int fl_boundary_project(fl_boundary* b, double h, double dt, const int32_t* cell_index,
+                                   const double* cell_values, uint64_t cell_count, const int32_t* face_index,
+                                   const int32_t* face_kind, const double* face_values, uint64_t face_count,
+                                   int max_iterations, double rel_tol, double* pressure, double* corrected_u,
+                                   double* rhs, double* residual, double* defect, uint64_t* gauge_ordinals,
+                                   fl_mac_pressure_diagnostics* diagnostics, fl_measurement* measurement) {
+  if (!b) return FL_INVALID_ARGUMENT;
+  if (cudaSetDevice(b->device) != cudaSuccess) {
+    cudaGetLastError();
+    return FL_INTERNAL;
+  }
+  return fl::mp_project(b->pressure, b->stream, h, dt, cell_index, cell_values, cell_count, face_index, face_kind,
+                        face_values, face_count, max_iterations, rel_tol, pressure, corrected_u, rhs, residual,
+                        defect, gauge_ordinals, diagnostics, measurement);
 }

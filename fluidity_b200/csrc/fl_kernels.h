@@ -213,3 +213,49 @@ void context_attach_snapshot_queue(::fl_context* c, int delta);
 // FL_OK when an sm_100 device is current, else FL_FAILED_PRECONDITION.
 int check_device();
 }  // namespace fl
+
+// ---- bounded MAC pressure projection (fl_mac_pressure.cu) ----
+#include <vector>
+
+#include "../../include/fluidity_b200.h"
+namespace fl {
+// A face of the reference's owned sparse grid as (4^3 block z, y, x, normal
+// axis, local z, y, x): its owned-slot order.
+struct OwnedFaceKey {
+  int32_t v[7];
+  bool operator<(const OwnedFaceKey& o) const {
+    for (int k = 0; k < 7; ++k)
+      if (v[k] != o.v[k]) return v[k] < o.v[k];
+    return false;
+  }
+  bool operator==(const OwnedFaceKey& o) const {
+    for (int k = 0; k < 7; ++k)
+      if (v[k] != o.v[k]) return false;
+    return true;
+  }
+};
+// Host and device scratch of one projection. reserve_caps() sizes every part
+// for the operator's caps (4096 cells, 24576 faces) once, after which
+// projections through it allocate nothing; a scratch left empty grows for the
+// call.
+struct MpScratch {
+  std::vector<OwnedFaceKey> incident;
+  std::vector<int> tail, head, cell_off, cell_ent, fill, parent, root, comp_of, gauges, comp_cell_off, comp_cells,
+      comp_face_off, comp_faces, host_ints;
+  std::vector<unsigned char> anchored, pinned;
+  std::vector<double> hp, hr, hd, hb, hu;
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  bool reserve_caps();
+  void release();  // the device arena
+  void destroy();  // arena and events
+};
+// fl_project_mac_pressure_3d's work on a caller's scratch and stream (NULL:
+// the default stream).
+int mp_project(MpScratch& scratch, cudaStream_t stream, double h, double dt, const int32_t* cell_index,
+               const double* cell_values, uint64_t cell_count, const int32_t* face_index, const int32_t* face_kind,
+               const double* face_values, uint64_t face_count, int max_iterations, double rel_tol, double* pressure,
+               double* corrected_u, double* rhs, double* residual, double* defect, uint64_t* gauge_ordinals,
+               fl_mac_pressure_diagnostics* diagnostics, fl_measurement* measurement);
+}  // namespace fl

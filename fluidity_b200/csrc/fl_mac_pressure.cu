@@ -382,10 +382,6 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
   }
 }
 
-int64_t cell_key(const int32_t* c) {
-  return ((int64_t)c[2] << 42) ^ (((int64_t)c[1] & 0x1fffff) << 21) ^ ((int64_t)c[0] & 0x1fffff);
-}
-
 bool cell_less(const int32_t* a, const int32_t* b) {
   if (a[2] != b[2]) return a[2] < b[2];
   if (a[1] != b[1]) return a[1] < b[1];
@@ -410,19 +406,7 @@ int find_cell(const int32_t* cells, int nc, int32_t x, int32_t y, int32_t z) {
 // (SparseMacGrid3D::FaceSlot, sparse_mac_grid_3d.cc:388-409): blocks in
 // (z,y,x) order, then the normal axis, then the local (z,y,x) position; the
 // face at lattice index (i,j,k) is owned by the block of cell (i,j,k).
-struct FaceKey {
-  int32_t v[7];
-  bool operator<(const FaceKey& o) const {
-    for (int k = 0; k < 7; ++k)
-      if (v[k] != o.v[k]) return v[k] < o.v[k];
-    return false;
-  }
-  bool operator==(const FaceKey& o) const {
-    for (int k = 0; k < 7; ++k)
-      if (v[k] != o.v[k]) return false;
-    return true;
-  }
-};
+using FaceKey = OwnedFaceKey;
 
 FaceKey face_key(int axis, int64_t x, int64_t y, int64_t z) {
   auto fdiv = [](int64_t a) { return (int32_t)(a >= 0 ? a / 4 : -((-a + 3) / 4)); };
@@ -436,6 +420,68 @@ int find_root(std::vector<int>& parent, int c) {
 }
 
 }  // namespace
+
+// Device arena bytes for nc cells, nf faces, ent cell-face entries, ncomp
+// unanchored components, comp_faces component face entries.
+size_t mp_arena_bytes(size_t nc, size_t nf, size_t ent, size_t ncomp, size_t comp_faces) {
+  const size_t nd_in = 5 * nc + 6 * nf;
+  const size_t nd_work = 3 * nf + 6 * nc + nf + ent;
+  const size_t ni = 3 * nf + (nc + 1) + ent + nc + (ncomp + 1) + nc + (ncomp + 1) + comp_faces;
+  return sizeof(double) * (nd_in + nd_work) + sizeof(MpStatus) + sizeof(int) * (ni + ent) + nc + 64;
+}
+
+bool MpScratch::reserve_caps() {
+  const size_t nc = kMpMaxCells, nf = kMpMaxFaces;
+  try {
+    incident.reserve(6 * nc);
+    tail.reserve(nf);
+    head.reserve(nf);
+    cell_off.reserve(nc + 1);
+    cell_ent.reserve(2 * nf);
+    fill.reserve(nc);
+    parent.reserve(nc);
+    root.reserve(nc);
+    comp_of.reserve(nc);
+    gauges.reserve(nc);
+    comp_cell_off.reserve(nc + 1);
+    comp_cells.reserve(nc);
+    comp_face_off.reserve(nc + 1);
+    comp_faces.reserve(2 * nf);
+    host_ints.reserve(4 * nf + 5 * nc + 3);
+    anchored.reserve(nc);
+    pinned.reserve(nc);
+    for (auto* v : {&hp, &hr, &hd, &hb}) v->reserve(nc);
+    hu.reserve(nf);
+  } catch (...) {
+    return false;
+  }
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  arena_bytes = mp_arena_bytes(nc, nf, 2 * nf, nc, 2 * nf);
+  if (cudaMalloc(&arena, arena_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    arena = nullptr;
+    arena_bytes = 0;
+    return false;
+  }
+  return true;
+}
+
+void MpScratch::release() {
+  if (arena) cudaFree(arena);
+  arena = nullptr;
+  arena_bytes = 0;
+}
+
+void MpScratch::destroy() {
+  release();
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  e0 = e1 = nullptr;
+}
+
 }  // namespace fl
 
 using namespace fl;
@@ -446,6 +492,21 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
                                           double rel_tol, double* pressure, double* corrected_u, double* rhs,
                                           double* residual, double* defect, uint64_t* gauge_ordinals,
                                           fl_mac_pressure_diagnostics* diagnostics, fl_measurement* measurement) {
+  MpScratch scratch;  // grows for this call and is released after it
+  const int st = fl::mp_project(scratch, nullptr, h, dt, cell_index, cell_values, cell_count, face_index, face_kind,
+                                face_values, face_count, max_iterations, rel_tol, pressure, corrected_u, rhs,
+                                residual, defect, gauge_ordinals, diagnostics, measurement);
+  scratch.destroy();
+  return st;
+}
+
+namespace fl {
+
+int mp_project(MpScratch& X, cudaStream_t stream, double h, double dt, const int32_t* cell_index,
+               const double* cell_values, uint64_t cell_count, const int32_t* face_index, const int32_t* face_kind,
+               const double* face_values, uint64_t face_count, int max_iterations, double rel_tol, double* pressure,
+               double* corrected_u, double* rhs, double* residual, double* defect, uint64_t* gauge_ordinals,
+               fl_mac_pressure_diagnostics* diagnostics, fl_measurement* measurement) {
   if (!(h > 0.0) || !std::isfinite(h) || !(dt > 0.0) || !std::isfinite(dt) || !(rel_tol >= 0.0) ||
       !std::isfinite(rel_tol))
     return FL_INVALID_ARGUMENT;
@@ -465,8 +526,8 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   // faces once), unique and in the reference's owned-slot order, as
   // PrepareMacPressureSystem3D requires (mac_pressure_3d_system.cc:223-239).
   {
-    std::vector<FaceKey> incident;
-    incident.reserve((size_t)6 * nc);
+    auto& incident = X.incident;
+    incident.clear();
     for (int i = 0; i < nc; ++i) {
       const int32_t* c = cell_index + 3 * i;
       for (int a = 0; a < 3; ++a) {
@@ -488,7 +549,10 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   // Face endpoints and the link rules (internal: two cells; Dirichlet: one
   // cell and an open aperture; sealed: closed; the aperture within the full
   // face, mac_pressure_3d_arithmetic.h:182).
-  std::vector<int> tail(nf), head(nf);
+  auto& tail = X.tail;
+  auto& head = X.head;
+  tail.assign(nf, -1);
+  head.assign(nf, -1);
   for (int f = 0; f < nf; ++f) {
     const int32_t* fi = face_index + 4 * f;
     const double* v = face_values + 6 * f;
@@ -510,15 +574,18 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   int st = check_device();
   if (st != FL_OK) return st;
   // Per-cell face lists in increasing face order.
-  std::vector<int> cell_off(nc + 1, 0), cell_ent;
+  auto& cell_off = X.cell_off;
+  auto& cell_ent = X.cell_ent;
+  cell_off.assign(nc + 1, 0);
   for (int f = 0; f < nf; ++f) {
     if (tail[f] >= 0) ++cell_off[tail[f] + 1];
     if (head[f] >= 0) ++cell_off[head[f] + 1];
   }
   for (int i = 0; i < nc; ++i) cell_off[i + 1] += cell_off[i];
-  cell_ent.resize(std::max(cell_off[nc], 1));
+  cell_ent.assign(std::max(cell_off[nc], 1), 0);
   {
-    std::vector<int> fill(cell_off.begin(), cell_off.end() - 1);
+    auto& fill = X.fill;
+    fill.assign(cell_off.begin(), cell_off.end() - 1);
     for (int f = 0; f < nf; ++f) {
       if (tail[f] >= 0) cell_ent[fill[tail[f]]++] = f << 1;
       if (head[f] >= 0) cell_ent[fill[head[f]]++] = (f << 1) | 1;
@@ -527,7 +594,8 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   // Components over conducting two-cell faces (union towards the smaller
   // ordinal, so a component's root is its first cell); anchors are compliant
   // cells and Dirichlet faces; every unanchored component pins its root.
-  std::vector<int> parent(nc);
+  auto& parent = X.parent;
+  parent.resize(nc);
   for (int i = 0; i < nc; ++i) parent[i] = i;
   for (int f = 0; f < nf; ++f) {
     const double* v = face_values + 6 * f;
@@ -537,8 +605,12 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
       parent[std::max(a, b)] = std::min(a, b);
     }
   }
-  std::vector<int> root(nc);
-  std::vector<unsigned char> anchored(nc, 0), pinned(nc, 0);
+  auto& root = X.root;
+  auto& anchored = X.anchored;
+  auto& pinned = X.pinned;
+  root.resize(nc);
+  anchored.assign(nc, 0);
+  pinned.assign(nc, 0);
   for (int i = 0; i < nc; ++i) {
     root[i] = find_root(parent, i);
     const double* v = cell_values + 5 * i;
@@ -546,7 +618,10 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   }
   for (int f = 0; f < nf; ++f)
     if (face_kind[f] == kLinkDirichlet) anchored[root[tail[f] >= 0 ? tail[f] : head[f]]] = 1;
-  std::vector<int> comp_of(nc, -1), gauges;
+  auto& comp_of = X.comp_of;
+  auto& gauges = X.gauges;
+  comp_of.assign(nc, -1);
+  gauges.clear();
   for (int i = 0; i < nc; ++i)
     if (root[i] == i && !anchored[i]) {
       pinned[i] = 1;
@@ -554,35 +629,55 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
       gauges.push_back(i);
     }
   const int ncomp = (int)gauges.size();
-  std::vector<int> comp_cell_off(ncomp + 1, 0), comp_cells, comp_face_off(ncomp + 1, 0), comp_faces;
+  // Each unanchored component's cells (ascending) and its faces that do not
+  // join two cells of the component (ascending), by counting then filling.
+  auto& comp_cell_off = X.comp_cell_off;
+  auto& comp_cells = X.comp_cells;
+  auto& comp_face_off = X.comp_face_off;
+  auto& comp_faces = X.comp_faces;
+  comp_cell_off.assign(ncomp + 1, 0);
+  comp_face_off.assign(ncomp + 1, 0);
+  for (int i = 0; i < nc; ++i)
+    if (comp_of[root[i]] >= 0) ++comp_cell_off[comp_of[root[i]] + 1];
+  for (int f = 0; f < nf; ++f) {
+    const int tl = tail[f], hd = head[f];
+    if (tl >= 0 && hd >= 0 && root[tl] == root[hd]) continue;
+    if (tl >= 0 && comp_of[root[tl]] >= 0) ++comp_face_off[comp_of[root[tl]] + 1];
+    if (hd >= 0 && comp_of[root[hd]] >= 0) ++comp_face_off[comp_of[root[hd]] + 1];
+  }
+  for (int k = 0; k < ncomp; ++k) {
+    comp_cell_off[k + 1] += comp_cell_off[k];
+    comp_face_off[k + 1] += comp_face_off[k];
+  }
+  comp_cells.assign(comp_cell_off[ncomp], 0);
+  comp_faces.assign(comp_face_off[ncomp], 0);
   {
-    std::vector<std::vector<int>> cc(ncomp), cf(ncomp);
+    auto& fill = X.fill;
+    fill.assign(comp_cell_off.begin(), comp_cell_off.end() - 1);
     for (int i = 0; i < nc; ++i)
-      if (comp_of[root[i]] >= 0) cc[comp_of[root[i]]].push_back(i);
+      if (comp_of[root[i]] >= 0) comp_cells[fill[comp_of[root[i]]]++] = i;
+    fill.assign(comp_face_off.begin(), comp_face_off.end() - 1);
     for (int f = 0; f < nf; ++f) {
       const int tl = tail[f], hd = head[f];
       if (tl >= 0 && hd >= 0 && root[tl] == root[hd]) continue;
-      if (tl >= 0 && comp_of[root[tl]] >= 0) cf[comp_of[root[tl]]].push_back(f << 1);
-      if (hd >= 0 && comp_of[root[hd]] >= 0) cf[comp_of[root[hd]]].push_back((f << 1) | 1);
-    }
-    for (int k = 0; k < ncomp; ++k) {
-      comp_cell_off[k + 1] = comp_cell_off[k] + (int)cc[k].size();
-      comp_face_off[k + 1] = comp_face_off[k] + (int)cf[k].size();
-      comp_cells.insert(comp_cells.end(), cc[k].begin(), cc[k].end());
-      comp_faces.insert(comp_faces.end(), cf[k].begin(), cf[k].end());
+      if (tl >= 0 && comp_of[root[tl]] >= 0) comp_faces[fill[comp_of[root[tl]]]++] = f << 1;
+      if (hd >= 0 && comp_of[root[hd]] >= 0) comp_faces[fill[comp_of[root[hd]]]++] = (f << 1) | 1;
     }
   }
   // One device arena: inputs, index lists, work arrays and the status.
-  const size_t nd_in = (size_t)5 * nc + (size_t)6 * nf;
-  const size_t nd_work = (size_t)3 * nf + (size_t)6 * nc + (size_t)nf + cell_ent.size();
-  const size_t ni = (size_t)3 * nf + (nc + 1) + cell_ent.size() + nc + (ncomp + 1) + comp_cells.size() + (ncomp + 1) +
-                    comp_faces.size();
-  const size_t bytes = sizeof(double) * (nd_in + nd_work) + sizeof(MpStatus) + sizeof(int) * (ni + cell_ent.size()) +
-                       nc + 64;
-  char* arena = nullptr;
-  if (cudaMalloc(&arena, bytes) != cudaSuccess) {
+  const size_t bytes = mp_arena_bytes(nc, nf, cell_ent.size(), ncomp, comp_faces.size());
+  if (X.arena_bytes < bytes) {
+    X.release();
+    if (cudaMalloc(&X.arena, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      X.arena = nullptr;
+      return FL_RESOURCE_EXHAUSTED;
+    }
+    X.arena_bytes = bytes;
+  }
+  if (!X.e0 && (cudaEventCreate(&X.e0) != cudaSuccess || cudaEventCreate(&X.e1) != cudaSuccess)) {
     cudaGetLastError();
-    return FL_RESOURCE_EXHAUSTED;
+    return FL_INTERNAL;
   }
   MpSystem S{};
   S.nc = nc;
@@ -592,7 +687,7 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   S.dt = dt;
   S.rel_tol = rel_tol;
   S.max_iterations = max_iterations;
-  double* dp = reinterpret_cast<double*>(arena);
+  double* dp = reinterpret_cast<double*>(X.arena);
   auto take_d = [&](size_t n) {
     double* r = dp;
     dp += n;
@@ -613,8 +708,8 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   S.ent_cond = take_d(cell_ent.size());
   S.out = reinterpret_cast<MpStatus*>(dp);
   int* ip = reinterpret_cast<int*>(S.out + 1);
-  std::vector<int> host_ints;
-  host_ints.reserve(ni);
+  auto& host_ints = X.host_ints;
+  host_ints.clear();
   auto put = [&](const int* src, size_t n) {
     int* r = ip + host_ints.size();
     host_ints.insert(host_ints.end(), src, src + n);
@@ -635,18 +730,16 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
   S.pinned = d_pinned;
   S.cell_values = d_cells;
   S.face_values = d_faces;
-  cudaStream_t s = 0;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaStream_t s = stream;
   MpStatus res{};
   float ms = 0.0f;
-  bool ok = cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess &&
-            cudaMemcpyAsync(d_cells, cell_values, sizeof(double) * 5 * nc, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+  bool ok = cudaMemcpyAsync(d_cells, cell_values, sizeof(double) * 5 * nc, cudaMemcpyHostToDevice, s) == cudaSuccess &&
             (nf == 0 || cudaMemcpyAsync(d_faces, face_values, sizeof(double) * 6 * nf, cudaMemcpyHostToDevice, s) ==
                             cudaSuccess) &&
             cudaMemcpyAsync(ip, host_ints.data(), sizeof(int) * host_ints.size(), cudaMemcpyHostToDevice, s) ==
                 cudaSuccess &&
             cudaMemcpyAsync(d_pinned, pinned.data(), nc, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-            cudaEventRecord(e0, s) == cudaSuccess;
+            cudaEventRecord(X.e0, s) == cudaSuccess;
   if (ok) {
     const size_t vec_bytes = sizeof(double) * 6 * (size_t)nc;
     static unsigned long long configured = 0;
@@ -655,27 +748,25 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
                            (int)(sizeof(double) * 6 * kMpMaxCells));
     ++g_kernel_launches;
     k_mac_pressure<<<1, kMpThreads, vec_bytes, s>>>(S);
-    ok = cudaGetLastError() == cudaSuccess && cudaEventRecord(e1, s) == cudaSuccess &&
+    ok = cudaGetLastError() == cudaSuccess && cudaEventRecord(X.e1, s) == cudaSuccess &&
          cudaMemcpyAsync(&res, S.out, sizeof(MpStatus), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
-         cudaStreamSynchronize(s) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+         cudaStreamSynchronize(s) == cudaSuccess && cudaEventElapsedTime(&ms, X.e0, X.e1) == cudaSuccess;
   }
-  std::vector<double> hp, hr, hd, hb, hu;
+  auto &hp = X.hp, &hr = X.hr, &hd = X.hd, &hb = X.hb, &hu = X.hu;
   if (ok && res.status == FL_OK) {
     hp.resize(nc);
     hr.resize(nc);
     hd.resize(nc);
     hb.resize(nc);
     hu.resize(std::max(nf, 1));
-    ok = cudaMemcpy(hp.data(), S.p, sizeof(double) * nc, cudaMemcpyDeviceToHost) == cudaSuccess &&
-         cudaMemcpy(hr.data(), S.residual, sizeof(double) * nc, cudaMemcpyDeviceToHost) == cudaSuccess &&
-         cudaMemcpy(hd.data(), S.defect, sizeof(double) * nc, cudaMemcpyDeviceToHost) == cudaSuccess &&
-         cudaMemcpy(hb.data(), S.rhs, sizeof(double) * nc, cudaMemcpyDeviceToHost) == cudaSuccess &&
-         (nf == 0 ||
-          cudaMemcpy(hu.data(), S.corrected_u, sizeof(double) * nf, cudaMemcpyDeviceToHost) == cudaSuccess);
+    ok = cudaMemcpyAsync(hp.data(), S.p, sizeof(double) * nc, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         cudaMemcpyAsync(hr.data(), S.residual, sizeof(double) * nc, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         cudaMemcpyAsync(hd.data(), S.defect, sizeof(double) * nc, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         cudaMemcpyAsync(hb.data(), S.rhs, sizeof(double) * nc, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         (nf == 0 || cudaMemcpyAsync(hu.data(), S.corrected_u, sizeof(double) * nf, cudaMemcpyDeviceToHost, s) ==
+                         cudaSuccess) &&
+         cudaStreamSynchronize(s) == cudaSuccess;
   }
-  if (e0) cudaEventDestroy(e0);
-  if (e1) cudaEventDestroy(e1);
-  cudaFree(arena);
   if (!ok) {
     cudaGetLastError();
     return FL_INTERNAL;
@@ -702,3 +793,5 @@ extern "C" int fl_project_mac_pressure_3d(double h, double dt, const int32_t* ce
     for (int k = 0; k < ncomp; ++k) gauge_ordinals[k] = (uint64_t)gauges[k];
   return FL_OK;
 }
+
+}  // namespace fl

@@ -611,6 +611,16 @@ int fl_boundary_predict_face(fl_boundary* boundary, const fl_owned_grid* grid, c
                              uint64_t face_slot, int64_t side_tag, const double acceleration[3],
                              double step_duration, double* predicted_face_velocity, fl_measurement* measurement);
 
+/* fl_project_mac_pressure_3d on the boundary object's scratch and stream, which
+ * are reserved for the operator's caps when the object is created: the
+ * projection allocates nothing. Same arguments, outputs and codes. */
+int fl_boundary_project(fl_boundary* boundary, double h, double dt, const int32_t* cell_index,
+                        const double* cell_values, uint64_t cell_count, const int32_t* face_index,
+                        const int32_t* face_kind, const double* face_values, uint64_t face_count, int max_iterations,
+                        double rel_tol, double* pressure, double* corrected_u, double* rhs, double* residual,
+                        double* defect, uint64_t* gauge_ordinals, fl_mac_pressure_diagnostics* diagnostics,
+                        fl_measurement* measurement);
+
 /* GatherLiquidBoundaryParticles3D: one record per particle in input order;
  * fallback_counts = old PIC, new PIC and low-mass fallback particle counts. */
 int fl_boundary_gather(fl_boundary* boundary, const fl_owned_grid* grid, const fl_boundary_particle* particles,

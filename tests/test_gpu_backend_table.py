@@ -196,3 +196,25 @@ def test_project_matches_within_the_gate():
     np.testing.assert_allclose(b200["measure"][:2], cpu["measure"][:2], rtol=1e-12)
     assert abs(b200["measure"][2] - cpu["measure"][2]) <= 1e-12 * max(abs(cpu["measure"][2]), 1e-12)
     assert b200["diag"][4] == cpu["diag"][4] == 0
+
+
+def test_operations_repeat_bitwise_without_growing_device_memory(one_sided, histories):
+    """The B200 table reserves its storage when it is made: repeated attempts
+    leave the device's free memory unchanged and repeat bit for bit."""
+    import torch
+
+    box, s, dt = _dam_break_system()
+
+    def attempt():
+        return (bt.deposit(B200, one_sided)[1], bt.gather(B200, one_sided, histories["old"], histories["new"])[1],
+                bt.project(B200, s, box.h, dt)[1]["pressure"])
+
+    first = attempt()
+    torch.cuda.synchronize()
+    free = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        again = attempt()
+        for a, b in zip(first, again):
+            assert np.array_equal(a, b)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free
