@@ -232,11 +232,15 @@ def runtime_info():
                 minor=vals[3].value)
 
 
-def default_pressure_options(precision: int = 0, rel_tol: float = 1e-6, levels: int = 0, pre: int = 2,
+def default_pressure_options(precision: int = 0, rel_tol: float = 1e-6, levels: int = 0, pre: int = 1,
                              post: int = 2, coarse_sweeps: int = 4, max_iterations: int = 400,
                              max_refinements: int = 6, inner_rtol: float = 1e-3,
                              warm_start: int = 0, preconditioner: int = 0, stall_limit: int = 3,
                              stall_ratio: float = 0.9) -> PressureOptions:
+    """Solver options. One pre-smoothing and two post-smoothing sweeps per level: fewer V-cycle
+    kernels for slightly more flexible-CG iterations, the fastest of the sweep counts measured
+    (3.09 vs 3.24 ms per projection at the 256^3 splash, 1.19 vs 1.30 ms at the 128^3 dam break,
+    against two and two)."""
     o = PressureOptions()
     o.warm_start = warm_start
     o.preconditioner, o.stall_limit, o.stall_ratio = preconditioner, stall_limit, stall_ratio
