@@ -22,11 +22,11 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-5
 
 
-def _compare_step(ctx, n, state_in, precision=0, levels=0):
+def _compare_step(ctx, n, state_in, precision=0, levels=0, pre=1, post=2):
     """Runs one GPU step from state_in and one oracle step; returns errors."""
     ctx.upload(state_in)
     code, diag = ctx.step(fb.transfer_params(scenes.DT, scenes.DENSITY / n ** 3 / 8),
-                          fb.default_pressure_options(precision=precision, levels=levels))
+                          fb.default_pressure_options(precision=precision, levels=levels, pre=pre, post=post))
     assert code == fb.OK, diag.as_dict()
     f = read_fields(ctx, n)
     out = ctx.download()
@@ -91,14 +91,14 @@ def test_dam_break_128_steps_10_and_200_match_oracle_replay():
     oracle from the GPU state of the step before."""
     ctx, soa, m = dam_break_context(128)
     tp = fb.transfer_params(scenes.DT, m)
-    opt = fb.default_pressure_options(levels=4)
+    opt = fb.default_pressure_options(levels=4, pre=2, post=2)
     done = 0
     for check in (10, 200):
         while done < check - 1:
             code, _ = ctx.step(tp, opt)
             assert code == fb.OK
             done += 1
-        errs, diag, _, _ = _compare_step(ctx, 128, ctx.download(), levels=4)
+        errs, diag, _, _ = _compare_step(ctx, 128, ctx.download(), levels=4, pre=2, post=2)
         done += 1
         assert diag.relative_residual <= 1e-6
         for k, e in errs.items():
@@ -108,7 +108,7 @@ def test_dam_break_128_steps_10_and_200_match_oracle_replay():
 def test_dam_break_128_first_step_matches_oracle():
     """128^3 with the 4-level V-cycle (2 pre + 2 post red-black sweeps)."""
     ctx, soa, _ = dam_break_context(128)
-    errs, diag, _, _ = _compare_step(ctx, 128, soa, levels=4)
+    errs, diag, _, _ = _compare_step(ctx, 128, soa, levels=4, pre=2, post=2)
     assert diag.levels == 4
     for k, e in errs.items():
         assert e <= TOL, (k, e, errs)
