@@ -166,21 +166,33 @@ def _traffic_per_launch(particles: int, cells: int):
 
 # Algorithmic bytes per allocated cell (active blocks x 512) of one flexible-CG
 # iteration, each array element counted once per kernel, V-cycle x and
-# coefficients in BF16 (FP32 storage: 158, the x and k accesses at 4 B):
+# coefficients in BF16:
 #   k_dots 10 (z, r, r_prev) + k_direction_tiled 15 (z, d_old, mask -> d, q)
 #   + k_update 24 (d, q, r, e -> e, r_next)                                   = 49
-#   level 0: from-zero sweep 5.5, six sweeps 6.5, prolongation sweep 6.75
-#            (mask, b, diag of the colour; x of the other colour; x written),
-#            restriction 11.9 (mask, diag, b, x; coarse b and seed)            = 63.2
-#   levels >= 1: ~106 B per coarse cell per V-cycle, 1/8 per level             = 15.5
-_PRESSURE_BYTES_PER_CELL_ITER = {1: 128.0, 0: 158.0}
+#   level 0, per sweep the colour's mask, b and diag, the other colour's x and
+#   the colour's x written: the from-zero sweep 5.5, a sweep 6.5, the
+#   prolongation sweep 6.75; the restriction 11.9 (mask, diag, b, x; coarse b
+#   and seed). With `pre` pre- and `post` post-smoothing sweeps:
+#   5.5 + 6.5 + 13 (pre - 1) + 6.75 + 6.5 (2 post - 1) + 11.9
+#   (63.2 for two and two, 50.2 for one and two)
+#   levels >= 1: ~106 B per coarse cell per V-cycle at two and two, 1/8 per
+#   level (15.5), scaled with level 0's sweeps
+# FP32 storage reads x and the coefficients at 4 B: the V-cycle part x 109/78.65
+# (158 B in all for two and two, against 128 in BF16).
+def _pressure_bytes_per_cell_iter(precision: int, pre: int, post: int) -> float:
+    level0 = 5.5 + 6.5 + 13.0 * (pre - 1) + 6.75 + 6.5 * (2 * post - 1) + 11.9
+    vcycle = level0 + 15.5 * level0 / 63.15
+    if precision == 0:
+        vcycle *= 109.0 / 78.65
+    return round(49.0 + vcycle, 1)
 
 
-def _pressure_roofline(cells: int, iterations: float, pressure_ms: float, peak: float, precision: int):
+def _pressure_roofline(cells: int, iterations: float, pressure_ms: float, peak: float, precision: int,
+                       pre: int, post: int):
     """Iteration bytes over the whole projection's time (setup, FP64 residuals,
     correction and export included in the time but not in the bytes): a lower
     bound on the solver's achieved bandwidth."""
-    per = _PRESSURE_BYTES_PER_CELL_ITER[precision]
+    per = _pressure_bytes_per_cell_iter(precision, pre, post)
     moved = per * cells * iterations
     achieved = moved / (pressure_ms / 1e3) / 1e9
     return {"bytes_per_cell_per_iteration": per, "cells": cells, "iterations": iterations,
@@ -343,7 +355,7 @@ def run_ours(args, world, rank, local):
                                "achieved": round((p2g_bytes + g2p_bytes) / ((p2g_ms + g2p_ms) / 1e3) / 1e9, 1),
                                "frac": round((p2g_bytes + g2p_bytes) / ((p2g_ms + g2p_ms) / 1e3) / 1e9 / peak, 4)},
         "pressure_roofline": _pressure_roofline(ncell, float(np.mean(iters)), phases[2] / args.steps, peak,
-                                                args.precision),
+                                                args.precision, opt.pre_sweeps, opt.post_sweeps),
         "particles_per_s": round(value * npart, 1),
         "pressure": {"mean_iterations": float(np.mean(iters)), "max_relative_residual": float(max(residuals)),
                      "vcycle_storage": "bf16" if args.precision == 1 else "fp32", "inner_rtol": 1e-3},
@@ -422,7 +434,8 @@ def column_drop_512(peak, learned_params, steps=5, warmup=3):
            "transfers_roofline": {"algorithmic_bytes": int(tb),
                                   "achieved": round(tb / ((p2g_ms + g2p_ms) / 1e3) / 1e9, 1),
                                   "frac": round(tb / ((p2g_ms + g2p_ms) / 1e3) / 1e9 / peak, 4)},
-           "pressure_roofline": _pressure_roofline(ncell, float(np.mean(iters)), pr_ms, peak, 1),
+           "pressure_roofline": _pressure_roofline(ncell, float(np.mean(iters)), pr_ms, peak, 1, opt.pre_sweeps,
+                                                   opt.post_sweeps),
            "mean_iterations": float(np.mean(iters)), "scene_seconds": round(gen_s, 1),
            "data": "synthetic (seeded column_drop scene, generated on the host z-slab by z-slab)"}
     variants = {"mgpcg_fp32": dict(precision=0), "mgpcg_bf16": dict(precision=1)}
