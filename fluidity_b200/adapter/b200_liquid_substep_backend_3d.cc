@@ -60,6 +60,16 @@ static_assert(offsetof(LiquidBoundaryParticleGather3D, affine_enabled) ==
 static_assert(offsetof(LiquidBoundaryParticleGather3D, low_mass_fallback) ==
               offsetof(fl_gathered_particle, low_mass_fallback));
 static_assert(sizeof(LiquidFaceValidity3D) == 1);
+static_assert(sizeof(LiquidCenterDistance3D) == sizeof(fl_center_sample));
+static_assert(offsetof(LiquidCenterDistance3D, signed_distance) == offsetof(fl_center_sample, signed_distance));
+static_assert(sizeof(FrozenLiquidCell3D) == sizeof(fl_frozen_cell));
+static_assert(offsetof(FrozenLiquidCell3D, curvature) == offsetof(fl_frozen_cell, curvature));
+static_assert(sizeof(LiquidAirCellPressure3D) == sizeof(fl_air_cell_pressure));
+static_assert(offsetof(LiquidAirCellPressure3D, gas_gauge_pressure) ==
+              offsetof(fl_air_cell_pressure, gas_gauge_pressure));
+static_assert(sizeof(LiquidInternalInterface3D) == sizeof(fl_internal_interface));
+static_assert(offsetof(LiquidInternalInterface3D, normal_viscous_jump_tail_to_head) ==
+              offsetof(fl_internal_interface, normal_viscous_jump_tail_to_head));
 
 absl::Status Code(absl::StatusCode code) { return absl::Status(code, ""); }
 
@@ -245,6 +255,128 @@ struct B200BackendOps3D {
     return LiquidBoundaryGatherView3D{bank.particles, counts[0], counts[1], counts[2]};
   }
 
+
+  // The frozen view and the fields with their optional values unpacked into
+  // the C-ABI's records; cells, centre samples, air pressures and interfaces
+  // pass through (byte-compatible). Results are packed into the reference's
+  // pressure-cell and link records.
+  static absl::StatusOr<LiquidPressureProblemView3D> Links(
+      void* context,
+      const FrozenLiquidBoundaryGeometryView3D& geometry,
+      const LiquidPressureFields3D& fields,
+      LiquidBoundaryWorkspace3D&
+  ) {
+    auto& self = Self(context);
+    const std::size_t nc = geometry.cells.size(), nf = geometry.faces.size();
+    if (nc > kPressureCells || nf > kFaces) return Code(absl::StatusCode::kResourceExhausted);
+    // field extents (LinksCore, liquid_boundary_geometry_3d.cc:1086-1094), after the view checks the C-ABI makes
+    const bool extents_ok = fields.cells.size() == nc && fields.predicted_face_velocities.size() == nf &&
+                            (fields.wetted_piston_face_fluxes.empty() || fields.wetted_piston_face_fluxes.size() == nf);
+    auto& st = self.link_staging_;
+    st.faces.resize(nf);
+    for (std::size_t f = 0; f < nf; ++f) {
+      const FrozenLiquidFace3D& face = geometry.faces[f];
+      fl_frozen_face& o = st.faces[f];
+      o = fl_frozen_face{};
+      o.axis = static_cast<std::int32_t>(face.face_index.axis);
+      o.lattice[0] = face.face_index.lattice_index.x;
+      o.lattice[1] = face.face_index.lattice_index.y;
+      o.lattice[2] = face.face_index.lattice_index.z;
+      o.face_slot = face.face_slot;
+      o.open_area = face.open_area;
+      o.blocked_area = face.blocked_area;
+      o.wall_normal_velocity = face.wall_normal_velocity;
+      o.has_prescribed_wall_flux = face.prescribed_wall_flux.has_value();
+      o.prescribed_wall_flux = face.prescribed_wall_flux.value_or(0.0);
+      o.is_low_x_piston_face = face.is_low_x_piston_face;
+    }
+    const std::size_t nfields = std::min(fields.cells.size(), nc);
+    st.fields.resize(nc);
+    for (std::size_t i = 0; i < nfields; ++i) {
+      const LiquidPressureCellFields3D& c = fields.cells[i];
+      st.fields[i] = fl_pressure_cell_fields{c.target_divergence, c.bulk_modulus, c.previous_pressure,
+                                             c.density.value_or(0.0), static_cast<std::uint8_t>(c.density.has_value()),
+                                             {}};
+    }
+    const bool wetted = !fields.wetted_piston_face_fluxes.empty();
+    st.wetted.resize(wetted ? nf : 0);
+    st.has_wetted.resize(wetted ? nf : 0);
+    for (std::size_t f = 0; wetted && f < std::min(nf, fields.wetted_piston_face_fluxes.size()); ++f) {
+      st.wetted[f] = fields.wetted_piston_face_fluxes[f].value_or(0.0);
+      st.has_wetted[f] = fields.wetted_piston_face_fluxes[f].has_value();
+    }
+    const fl_owned_grid grid = OwnedGrid(geometry.mac_grid);
+    const fl_frozen_geometry g{&grid,
+                               reinterpret_cast<const fl_center_sample*>(geometry.center_distances.data()),
+                               geometry.center_distances.size(),
+                               reinterpret_cast<const fl_frozen_cell*>(geometry.cells.data()),
+                               nc,
+                               st.faces.data(),
+                               nf,
+                               geometry.step_duration,
+                               geometry.liquid_density,
+                               geometry.surface_tension};
+    const fl_pressure_fields pf{st.fields.data(),
+                                fields.predicted_face_velocities.data(),
+                                fields.ambient_pressure,
+                                wetted ? st.wetted.data() : nullptr,
+                                wetted ? st.has_wetted.data() : nullptr,
+                                reinterpret_cast<const fl_air_cell_pressure*>(fields.air_cell_pressures.data()),
+                                fields.air_cell_pressures.size(),
+                                reinterpret_cast<const fl_internal_interface*>(fields.internal_interfaces.data()),
+                                fields.internal_interfaces.size()};
+    st.cells_out.resize(nc);
+    st.faces_out.resize(nf);
+    std::uint64_t lower = 0;
+    int code = FL_OK;
+    if (!extents_ok) {
+      // the view checks still decide the code when they fail first
+      fl_pressure_fields probe = pf;
+      probe.ambient_pressure = std::nan("");
+      code = fl_boundary_links(self.boundary_, &g, &probe, st.cells_out.data(), st.faces_out.data(), &lower, nullptr);
+      return FromFl(code);
+    }
+    code = fl_boundary_links(self.boundary_, &g, &pf, st.cells_out.data(), st.faces_out.data(), &lower, nullptr);
+    if (code != FL_OK) return FromFl(code);
+    auto& bank = self.links_[1 - self.links_bank_];
+    bank.cells.resize(nc);
+    bank.faces.resize(nf);
+    for (std::size_t i = 0; i < nc; ++i) {
+      const fl_pressure_cell& c = st.cells_out[i];
+      bank.cells[i] = MacPressureCell3D{{c.cell_index[0], c.cell_index[1], c.cell_index[2]},
+                                        c.fluid_volume,
+                                        c.target_divergence,
+                                        c.bulk_modulus,
+                                        c.previous_pressure,
+                                        c.integrated_inward_wall_flux};
+    }
+    for (std::size_t f = 0; f < nf; ++f) {
+      const fl_pressure_link& l = st.faces_out[f];
+      MacPressureFace3D face{};
+      face.face_index = {static_cast<FaceNormalAxis>(l.axis), {l.lattice[0], l.lattice[1], l.lattice[2]}};
+      face.open_area = l.open_area;
+      face.inverse_density = l.inverse_density;
+      face.pressure_gradient_distance = l.pressure_gradient_distance;
+      face.predicted_normal_velocity = l.predicted_normal_velocity;
+      face.wall_normal_velocity = l.wall_normal_velocity;
+      if (l.link_kind == 1) {
+        face.pressure_link = InternalMacPressureLink3D{l.link_value};
+      } else if (l.link_kind == 2) {
+        face.pressure_link = DirichletMacPressureLink3D{l.link_value};
+      } else {
+        face.pressure_link = SealedMacPressureLink3D{};
+      }
+      if (l.has_prescribed_wall_flux) face.prescribed_wall_flux = l.prescribed_wall_flux;
+      bank.faces[f] = face;
+    }
+    self.links_bank_ = 1 - self.links_bank_;
+    LiquidPressureProblemView3D view{};
+    view.cells = bank.cells;
+    view.faces = bank.faces;
+    view.lower_theta_regularization_count = lower;
+    return view;
+  }
+
   // The pressure problem in the C-ABI's records: bulk modulus +inf as 0 (no
   // compliance) and any other non-positive or non-finite value as NaN (an
   // invalid cell, as the reference rejects it); an explicit wall flux on the
@@ -401,6 +533,11 @@ absl::StatusOr<std::unique_ptr<B200LiquidBackend3D>> B200LiquidBackend3D::Create
          Reserve(self->projections_[k].defects, kPressureCells) &&
          Reserve(self->projections_[k].gauges, kPressureCells);
   }
+  for (int k = 0; k < 2; ++k)
+    ok = ok && Reserve(self->links_[k].cells, kPressureCells) && Reserve(self->links_[k].faces, kFaces);
+  auto& ls = self->link_staging_;
+  ok = ok && Reserve(ls.faces, kFaces) && Reserve(ls.fields, kPressureCells) && Reserve(ls.wetted, kFaces) &&
+       Reserve(ls.has_wetted, kFaces) && Reserve(ls.cells_out, kPressureCells) && Reserve(ls.faces_out, kFaces);
   auto& s = self->staging_;
   ok = ok && Reserve(s.cell_index, 3 * kPressureCells) && Reserve(s.cell_values, 5 * kPressureCells) &&
        Reserve(s.face_index, 4 * kFaces) && Reserve(s.face_kind, kFaces) && Reserve(s.face_values, 6 * kFaces);
@@ -427,6 +564,7 @@ LiquidSubstepBackend3D B200LiquidBackend3D::operations() {
   table.predict_missing_face = &B200BackendOps3D::PredictMissingFace;
   table.forces = &B200BackendOps3D::Forces;
   table.gather = &B200BackendOps3D::Gather;
+  table.links = &B200BackendOps3D::Links;
   table.project = &B200BackendOps3D::Project;
   return table;
 }

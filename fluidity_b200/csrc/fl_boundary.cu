@@ -815,6 +815,249 @@ __global__ void k_predict_face(Grid g, History h, long long slot, long long side
   rep->predicted = v;
 }
 
+
+// ---- pressure-link assembly (.links) ----
+
+__device__ __forceinline__ bool cell_less(const int32_t* a, const int32_t* b) {
+  return a[2] != b[2] ? a[2] < b[2] : (a[1] != b[1] ? a[1] < b[1] : a[0] < b[0]);
+}
+__device__ __forceinline__ bool cell_equal(const int32_t* a, const int32_t* b) {
+  return a[0] == b[0] && a[1] == b[1] && a[2] == b[2];
+}
+
+// Index of the record with cell key `key` in a (z,y,x)-sorted array of records
+// `stride` bytes apart whose cell index sits at their start, else -1.
+__device__ int find_cell_record(const void* base, int count, size_t stride, const int32_t* key) {
+  const char* p = static_cast<const char*>(base);
+  int lo = 0, hi = count;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (cell_less(reinterpret_cast<const int32_t*>(p + mid * stride), key))
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo < count && cell_equal(reinterpret_cast<const int32_t*>(p + lo * stride), key)) return lo;
+  return -1;
+}
+
+__device__ __forceinline__ bool positive_finite(double v) { return isfinite(v) && v > 0.0; }
+__device__ __forceinline__ bool normal_or_zero(double v) { return v == 0.0 || is_normal(v); }
+
+// C++20 std::lerp for a, b > 0 (the monotone, exact-at-the-ends formula of P0811).
+__device__ double lerp_positive(double a, double b, double t) {
+  if (t == 1.0) return b;
+  const double x = a + t * (b - a);
+  return (t > 1.0) == (b > a) ? (b < x ? x : b) : (b > x ? x : b);
+}
+
+// C++20 std::midpoint for doubles (P0811).
+__device__ double midpoint_double(double a, double b) {
+  const double lo = DBL_MIN * 2, hi = DBL_MAX / 2;
+  const double aa = a < 0 ? -a : a, ab = b < 0 ? -b : b;
+  if (aa <= hi && ab <= hi) return (a + b) / 2;
+  if (aa < lo) return a + b / 2;
+  if (ab < lo) return a / 2 + b;
+  return a / 2 + b / 2;
+}
+
+// sqrt((rho_t + rho_h) h^3 / (4 pi sigma)) with the operands scaled to their
+// mantissas first, as InternalLiquidCapillaryStepBound3D forms it
+// (liquid_boundary_geometry_3d.cc:1669-1698).
+__device__ int capillary_step_bound(double tail_density, double head_density, double h, double sigma, double* out) {
+  if (!positive_finite(tail_density) || !positive_finite(head_density) || !positive_finite(h) || !isfinite(sigma) ||
+      sigma < 0.0)
+    return kInvalidArgument;
+  if (sigma == 0.0) {
+    *out = INFINITY;
+    return kOk;
+  }
+  const double larger = tail_density < head_density ? head_density : tail_density;
+  const double smaller = head_density < tail_density ? head_density : tail_density;
+  const double ratio = smaller / larger;
+  int de, we, te;
+  const double sd = frexp(larger, &de) * (1.0 + ratio);
+  const double sw = frexp(h, &we);
+  const double st = frexp(sigma, &te);
+  const double square = sd * sw * sw * sw / (4.0 * 3.141592653589793 * st);
+  const int e = de + 3 * we - te;
+  const double bound = scalbn(sqrt(scalbn(square, e % 2)), e / 2);
+  if (!positive_finite(bound)) return kOutOfRange;
+  *out = bound;
+  return kOk;
+}
+
+struct LinksArgs {
+  double h, density, step_duration, sigma, ambient;
+  const fl_frozen_cell* cells;
+  int nc;
+  const fl_frozen_face* faces;
+  int nf;
+  const fl_pressure_cell_fields* fields;
+  const double* predicted;
+  const double* wetted;  // nullptr: no wetted piston fluxes
+  const uint8_t* has_wetted;
+  const fl_air_cell_pressure* air;
+  int nair;
+  const fl_internal_interface* interfaces;
+  int ninterfaces;
+  const fl_center_sample* centers;
+  int ncenters;
+  fl_pressure_link* out;
+  uint8_t* regularized;
+  Report* rep;
+};
+
+// One thread per frozen face: the face's stage, geometry and consume steps
+// of LinksCore (liquid_boundary_geometry_3d.cc:1139-1273), errors ordered by face.
+__global__ void k_links(LinksArgs a) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f == 0) a.rep->arch = compiled_arch();
+  if (f >= a.nf) return;
+  const fl_frozen_face& face = a.faces[f];
+  a.regularized[f] = 0;
+  if (!isfinite(a.predicted[f])) {
+    fail(a.rep, f, kInvalidArgument);
+    return;
+  }
+  fl_pressure_link link;
+  memset(&link, 0, sizeof(link));
+  link.axis = face.axis;
+  for (int d = 0; d < 3; ++d) link.lattice[d] = face.lattice[d];
+  link.open_area = face.open_area;
+  link.inverse_density = 1 / a.density;
+  link.pressure_gradient_distance = a.h;
+  link.predicted_normal_velocity = a.predicted[f];
+  link.wall_normal_velocity = face.wall_normal_velocity;
+  link.link_kind = 0;
+  link.has_prescribed_wall_flux = face.has_prescribed_wall_flux;
+  link.prescribed_wall_flux = face.has_prescribed_wall_flux ? face.prescribed_wall_flux : 0.0;
+  const int32_t head[3] = {face.lattice[0], face.lattice[1], face.lattice[2]};
+  int32_t tail[3] = {head[0], head[1], head[2]};
+  const bool tail_ok = head[face.axis] != INT32_MIN;
+  if (tail_ok) tail[face.axis] -= 1;
+  const int hf = find_cell_record(a.cells, a.nc, sizeof(fl_frozen_cell), head);
+  const int tf = tail_ok ? find_cell_record(a.cells, a.nc, sizeof(fl_frozen_cell), tail) : -1;
+  const bool has_head = hf >= 0, has_tail = tf >= 0;
+  if (a.wetted != nullptr) {
+    const bool receiver = face.is_low_x_piston_face && face.axis == 0 && face.open_area == 0 && has_head &&
+                          !has_tail && face.has_prescribed_wall_flux;
+    const bool has = a.has_wetted[f] != 0;
+    if (receiver != has) {
+      fail(a.rep, f, kInvalidArgument);
+      return;
+    }
+    if (has) {
+      const double flux = a.wetted[f], w = face.wall_normal_velocity;
+      const bool wrong = (flux > 0 && w <= 0) || (flux < 0 && w >= 0);
+      if (!isfinite(flux) || wrong) {
+        fail(a.rep, f, kInvalidArgument);
+        return;
+      }
+      link.has_prescribed_wall_flux = 1;
+      link.prescribed_wall_flux = flux;
+    }
+  }
+  // the certified internal interface on this face, if any
+  int lo = 0, hi = a.ninterfaces;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a.interfaces[mid].face_ordinal < (uint64_t)f)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo < a.ninterfaces && a.interfaces[lo].face_ordinal == (uint64_t)f) {
+    const fl_internal_interface& c = a.interfaces[lo];
+    if (!has_head || !has_tail || face.open_area <= 0.0 || !a.fields[hf].has_density || !a.fields[tf].has_density) {
+      fail(a.rep, f, kInvalidArgument);
+      return;
+    }
+    const double tail_density = a.fields[tf].density, head_density = a.fields[hf].density;
+    double bound = 0.0;
+    const int st = capillary_step_bound(tail_density, head_density, a.h, c.surface_tension, &bound);
+    if (st != kOk) {
+      fail(a.rep, f, st);
+      return;
+    }
+    if (a.step_duration > bound) {
+      fail(a.rep, f, kAborted);
+      return;
+    }
+    const double face_density = lerp_positive(head_density, tail_density, c.tail_fraction);
+    const double inverse_density = 1.0 / face_density;
+    const double jump = fma(-c.surface_tension, c.curvature_tail_to_head, c.normal_viscous_jump_tail_to_head);
+    if (!is_normal(inverse_density) || !isfinite(jump)) {
+      fail(a.rep, f, kOutOfRange);
+      return;
+    }
+    link.inverse_density = inverse_density;
+    link.link_kind = 1;
+    link.link_value = jump;
+    a.out[f] = link;
+    return;
+  }
+  if (!tail_ok) {
+    if (face.open_area > 0) {
+      fail(a.rep, f, kOutOfRange);
+      return;
+    }
+    a.out[f] = link;
+    return;
+  }
+  if (!has_head && !has_tail) {
+    fail(a.rep, f, kFailedPrecondition);
+    return;
+  }
+  if (face.open_area > 0) {
+    const bool hd = has_head && a.fields[hf].has_density, td = has_tail && a.fields[tf].has_density;
+    if (hd || td) {
+      const double head_density = hd ? a.fields[hf].density : a.density;
+      const double tail_density = td ? a.fields[tf].density : a.density;
+      const double face_density = has_head && has_tail ? midpoint_double(head_density, tail_density)
+                                                       : (has_head ? head_density : tail_density);
+      link.inverse_density = 1.0 / face_density;
+      if (!is_normal(link.inverse_density)) {
+        fail(a.rep, f, kOutOfRange);
+        return;
+      }
+    }
+  }
+  if (has_head && has_tail) {
+    link.link_kind = 1;
+    link.link_value = 0.0;
+  } else if (face.open_area > 0) {
+    const int32_t* air_cell = has_head ? tail : head;
+    const int ci = find_cell_record(a.centers, a.ncenters, sizeof(fl_center_sample), air_cell);
+    if (ci < 0 || a.centers[ci].signed_distance < 0) {
+      fail(a.rep, f, kFailedPrecondition);
+      return;
+    }
+    const double air_distance = a.centers[ci].signed_distance;
+    const fl_frozen_cell& liquid = a.cells[has_head ? hf : tf];
+    const int pi = find_cell_record(a.air, a.nair, sizeof(fl_air_cell_pressure), air_cell);
+    const double ambient = pi >= 0 ? a.air[pi].gas_gauge_pressure : a.ambient;
+    // the link arithmetic (liquid_boundary_geometry_math_3d.h:676-689)
+    const double mag = -liquid.center_distance < air_distance ? air_distance : -liquid.center_distance;
+    const double ls = -liquid.center_distance / mag;
+    const double theta = ls / (ls + air_distance / mag);
+    const double clamped = theta < 0.05 ? 0.05 : (1.0 < theta ? 1.0 : theta);
+    const double distance = clamped * a.h;
+    const double lift = a.sigma * liquid.curvature;
+    const double exterior = ambient + lift;
+    if ((a.sigma > 0 && liquid.curvature != 0 && lift == 0) || !normal_or_zero(lift) || !isfinite(exterior) ||
+        !is_normal(distance)) {
+      fail(a.rep, f, kOutOfRange);
+      return;
+    }
+    a.regularized[f] = theta < 0.05 ? 1 : 0;
+    link.pressure_gradient_distance = distance;
+    link.link_kind = 2;
+    link.link_value = exterior;
+  }
+  a.out[f] = link;
+}
+
 }  // namespace
 }  // namespace fl
 
@@ -872,6 +1115,8 @@ struct fl_boundary {
   char* pin = nullptr;
   int device = -1;
   fl::MpScratch pressure;  // the bounded projection's scratch, reserved for its caps
+  char* ldev = nullptr;    // pressure-link assembly: device arena
+  char* lpin = nullptr;    // and its pinned mirror
 };
 
 namespace {
@@ -1008,6 +1253,10 @@ unsigned grid_of(uint64_t n, unsigned block) { return (unsigned)((n + block - 1)
 
 }  // namespace
 
+namespace {
+size_t link_arena_bytes();  // the pressure-link assembly's staging, defined with its regions below
+}  // namespace
+
 extern "C" int fl_boundary_create(fl_boundary** out) {
   if (!out) return FL_INVALID_ARGUMENT;
   *out = nullptr;
@@ -1018,7 +1267,9 @@ extern "C" int fl_boundary_create(fl_boundary** out) {
             cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreate(&b->e0) == cudaSuccess && cudaEventCreate(&b->e1) == cudaSuccess &&
             cudaMalloc(&b->dev, kRegions.total) == cudaSuccess &&
-            cudaMallocHost(&b->pin, kRegions.staged) == cudaSuccess && b->pressure.reserve_caps();
+            cudaMallocHost(&b->pin, kRegions.staged) == cudaSuccess && b->pressure.reserve_caps() &&
+            cudaMalloc(&b->ldev, link_arena_bytes()) == cudaSuccess &&
+            cudaMallocHost(&b->lpin, link_arena_bytes()) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     fl_boundary_destroy(b);
@@ -1033,6 +1284,8 @@ extern "C" int fl_boundary_destroy(fl_boundary* b) {
   if (b->device >= 0) cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   b->pressure.destroy();
+  if (b->lpin) cudaFreeHost(b->lpin);
+  if (b->ldev) cudaFree(b->ldev);
   if (b->pin) cudaFreeHost(b->pin);
   if (b->dev) cudaFree(b->dev);
   if (b->e0) cudaEventDestroy(b->e0);
@@ -1253,4 +1506,282 @@ extern "C" int fl_boundary_project(fl_boundary* b, double h, double dt, const in
   return fl::mp_project(b->pressure, b->stream, h, dt, cell_index, cell_values, cell_count, face_index, face_kind,
                         face_values, face_count, max_iterations, rel_tol, pressure, corrected_u, rhs, residual,
                         defect, gauge_ordinals, diagnostics, measurement);
+}
+
+// ---- pressure-link assembly: host checks and launch ----
+
+namespace {
+
+constexpr int kMaxLinkCells = 4096;
+constexpr size_t kMaxCenters = 27 * (size_t)kMaxLinkCells;
+
+bool host_cell_less(const int32_t* a, const int32_t* b) {
+  return a[2] != b[2] ? a[2] < b[2] : (a[1] != b[1] ? a[1] < b[1] : a[0] < b[0]);
+}
+
+template <typename R>
+long long host_find_cell(const R* recs, uint64_t n, const int32_t* key) {
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) / 2;
+    if (host_cell_less(recs[mid].cell_index, key))
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo < n && !host_cell_less(key, recs[lo].cell_index)) return (long long)lo;
+  return -1;
+}
+
+// SparseMacGridView3D::FaceSlot (sparse_mac_grid_3d.cc:388-409): the owned slot
+// of face (axis, lattice) or the reference's status.
+int host_face_slot(const fl_owned_grid* g, int axis, const int64_t lat[3], uint64_t* slot) {
+  if (axis < 0 || axis > 2) return FL_INVALID_ARGUMENT;
+  auto fdiv = [](int64_t i) { return i >= 0 ? i / 4 : -1 - (-(i + 1)) / 4; };
+  const int64_t b[3] = {fdiv(lat[0]), fdiv(lat[1]), fdiv(lat[2])};
+  uint64_t lo = 0, hi = g->block_count;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) / 2;
+    const int32_t* m = g->blocks + 3 * mid;
+    const bool less = m[2] != b[2] ? m[2] < b[2] : (m[1] != b[1] ? m[1] < b[1] : m[0] < b[0]);
+    if (less)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo >= g->block_count) return FL_FAILED_PRECONDITION;
+  const int32_t* m = g->blocks + 3 * lo;
+  if (m[0] != b[0] || m[1] != b[1] || m[2] != b[2]) return FL_FAILED_PRECONDITION;
+  const int64_t local = ((lat[2] - 4 * b[2]) * 4 + (lat[1] - 4 * b[1])) * 4 + (lat[0] - 4 * b[0]);
+  *slot = lo * 192 + (uint64_t)axis * 64 + (uint64_t)local;
+  return FL_OK;
+}
+
+bool positive_finite_h(double v) { return std::isfinite(v) && v > 0.0; }
+
+// ValidateFrozenView (liquid_boundary_geometry_3d.cc:1289-1380) and the field
+// checks at the head of LinksCore (:1084-1135), in their order.
+// The capacity check of the bounded workspace comes first
+// (LiquidBoundaryWorkspace3D::BuildLinksWithBackend, :2151-2159).
+int check_links(const fl_frozen_geometry* G, const fl_pressure_fields* F) {
+  if (G->cell_count > (uint64_t)kMaxLinkCells || G->face_count > (uint64_t)kMaxFaces) return FL_RESOURCE_EXHAUSTED;
+  if (!positive_finite_h(G->step_duration) || !positive_finite_h(G->liquid_density) ||
+      !std::isfinite(G->surface_tension) || G->surface_tension < 0)
+    return FL_INVALID_ARGUMENT;
+  const double h = G->grid->h, area = h * h, volume = area * h, inv = 1 / G->liquid_density;
+  if (!std::isnormal(area) || !std::isnormal(volume) || !std::isnormal(inv)) return FL_OUT_OF_RANGE;
+  for (uint64_t i = 0; i < G->center_count; ++i)
+    if (!std::isfinite(G->centers[i].signed_distance) ||
+        (i > 0 && !host_cell_less(G->centers[i - 1].cell_index, G->centers[i].cell_index)))
+      return FL_INVALID_ARGUMENT;
+  for (uint64_t i = 0; i < G->cell_count; ++i) {
+    const fl_frozen_cell& c = G->cells[i];
+    if (!positive_finite_h(c.fluid_volume) || c.fluid_volume > volume || !std::isfinite(c.center_distance) ||
+        c.center_distance >= 0 || !std::isfinite(c.curvature))
+      return FL_INVALID_ARGUMENT;
+    if (i > 0 && !host_cell_less(G->cells[i - 1].cell_index, c.cell_index)) return FL_INVALID_ARGUMENT;
+  }
+  for (uint64_t i = 0; i < G->face_count; ++i) {
+    const fl_frozen_face& f = G->faces[i];
+    const int64_t lat[3] = {f.lattice[0], f.lattice[1], f.lattice[2]};
+    uint64_t slot = 0;
+    const int st = host_face_slot(G->grid, f.axis, lat, &slot);
+    if (st != FL_OK) return st;
+    if (slot != f.face_slot || (i > 0 && f.face_slot <= G->faces[i - 1].face_slot)) return FL_INVALID_ARGUMENT;
+    if (!std::isfinite(f.open_area) || f.open_area < 0 || f.open_area > area || f.blocked_area != area - f.open_area ||
+        !std::isfinite(f.wall_normal_velocity))
+      return FL_INVALID_ARGUMENT;
+    if (f.has_prescribed_wall_flux &&
+        (!std::isfinite(f.prescribed_wall_flux) || (f.blocked_area == 0 && f.prescribed_wall_flux != 0)))
+      return FL_INVALID_ARGUMENT;
+    const int32_t head[3] = {f.lattice[0], f.lattice[1], f.lattice[2]};
+    const bool tail_ok = head[f.axis] != INT32_MIN;
+    int32_t tail[3] = {head[0], head[1], head[2]};
+    if (tail_ok) tail[f.axis] -= 1;
+    const bool has_head = host_find_cell(G->cells, G->cell_count, head) >= 0;
+    const bool has_tail = tail_ok && host_find_cell(G->cells, G->cell_count, tail) >= 0;
+    if (!has_head && !has_tail) return FL_FAILED_PRECONDITION;
+    if (!tail_ok && f.open_area > 0) return FL_OUT_OF_RANGE;
+  }
+  // every incident owner present in the face union
+  for (uint64_t i = 0; i < G->cell_count; ++i)
+    for (int a = 0; a < 3; ++a)
+      for (int side = 0; side < 2; ++side) {
+        int64_t lat[3] = {G->cells[i].cell_index[0], G->cells[i].cell_index[1], G->cells[i].cell_index[2]};
+        lat[a] += side;
+        if (lat[a] > INT32_MAX) return FL_OUT_OF_RANGE;
+        uint64_t slot = 0;
+        const int st = host_face_slot(G->grid, a, lat, &slot);
+        if (st != FL_OK) return st;
+        uint64_t lo = 0, hi = G->face_count;
+        while (lo < hi) {
+          const uint64_t mid = (lo + hi) / 2;
+          if (G->faces[mid].face_slot < slot)
+            lo = mid + 1;
+          else
+            hi = mid;
+        }
+        if (lo >= G->face_count || G->faces[lo].face_slot != slot) return FL_FAILED_PRECONDITION;
+      }
+  if (F->air_count > G->center_count || F->interface_count > G->face_count || !std::isfinite(F->ambient_pressure))
+    return FL_INVALID_ARGUMENT;
+  for (uint64_t k = 0; k < F->interface_count; ++k) {
+    const fl_internal_interface& c = F->interfaces[k];
+    if (c.face_ordinal >= G->face_count || (k > 0 && F->interfaces[k - 1].face_ordinal >= c.face_ordinal) ||
+        !std::isfinite(c.tail_fraction) || c.tail_fraction < 0.0 || c.tail_fraction > 1.0 ||
+        !std::isfinite(c.surface_tension) || c.surface_tension < 0.0 || !std::isfinite(c.curvature_tail_to_head) ||
+        !std::isfinite(c.normal_viscous_jump_tail_to_head))
+      return FL_INVALID_ARGUMENT;
+  }
+  for (uint64_t k = 0; k < F->air_count; ++k) {
+    const fl_air_cell_pressure& p = F->air[k];
+    if (!std::isfinite(p.gas_gauge_pressure) ||
+        (k > 0 && !host_cell_less(F->air[k - 1].cell_index, p.cell_index)))
+      return FL_INVALID_ARGUMENT;
+    const long long c = host_find_cell(G->centers, G->center_count, p.cell_index);
+    if (c < 0) return FL_FAILED_PRECONDITION;
+    if (G->centers[c].signed_distance < 0.0 || host_find_cell(G->cells, G->cell_count, p.cell_index) >= 0)
+      return FL_INVALID_ARGUMENT;
+  }
+  for (uint64_t i = 0; i < G->cell_count; ++i) {
+    const fl_pressure_cell_fields& f = F->cells[i];
+    if (!std::isfinite(f.target_divergence) || !std::isfinite(f.previous_pressure) || std::isnan(f.bulk_modulus) ||
+        f.bulk_modulus <= 0 || (f.has_density && !positive_finite_h(f.density)))
+      return FL_INVALID_ARGUMENT;
+  }
+  return FL_OK;
+}
+
+}  // namespace
+
+namespace {
+
+struct LinkRegions {
+  size_t cells, faces, fields, pred, wet, has_wet, air, itf, cent, out, reg, report, total;
+  LinkRegions() {
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+      const size_t r = o;
+      o = align_up(o + bytes);
+      return r;
+    };
+    cells = take(sizeof(fl_frozen_cell) * kMaxLinkCells);
+    faces = take(sizeof(fl_frozen_face) * kMaxFaces);
+    fields = take(sizeof(fl_pressure_cell_fields) * kMaxLinkCells);
+    pred = take(sizeof(double) * kMaxFaces);
+    wet = take(sizeof(double) * kMaxFaces);
+    has_wet = take(kMaxFaces);
+    air = take(sizeof(fl_air_cell_pressure) * kMaxCenters);
+    itf = take(sizeof(fl_internal_interface) * kMaxFaces);
+    cent = take(sizeof(fl_center_sample) * kMaxCenters);
+    out = take(sizeof(fl_pressure_link) * kMaxFaces);
+    reg = take(kMaxFaces);
+    report = take(sizeof(Report));
+    total = o;
+  }
+};
+
+const LinkRegions kLinkRegions;
+
+size_t link_arena_bytes() { return kLinkRegions.total; }
+
+bool lupload(fl_boundary* b, size_t off, const void* src, size_t bytes) {
+  if (bytes == 0) return true;
+  std::memcpy(b->lpin + off, src, bytes);
+  return cudaMemcpyAsync(b->ldev + off, b->lpin + off, bytes, cudaMemcpyHostToDevice, b->stream) == cudaSuccess;
+}
+
+bool ldownload(fl_boundary* b, size_t off, size_t bytes) {
+  if (bytes == 0) return true;
+  return cudaMemcpyAsync(b->lpin + off, b->ldev + off, bytes, cudaMemcpyDeviceToHost, b->stream) == cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" int fl_boundary_links(fl_boundary* b, const fl_frozen_geometry* G, const fl_pressure_fields* F,
+                                 fl_pressure_cell* cells_out, fl_pressure_link* faces_out, uint64_t* lower_theta,
+                                 fl_measurement* m) {
+  if (!b || !G || !F) return FL_INVALID_ARGUMENT;
+  int st = check_grid(G->grid);
+  if (st != FL_OK) return st;
+  if ((G->center_count && !G->centers) || (G->cell_count && (!G->cells || !F->cells || !cells_out)) ||
+      (G->face_count && (!G->faces || !F->predicted_face_velocities || !faces_out)) || (F->air_count && !F->air) ||
+      (F->interface_count && !F->interfaces) || (F->wetted_piston_face_fluxes && !F->has_wetted_piston_face_flux))
+    return FL_INVALID_ARGUMENT;
+  if (G->center_count > kMaxCenters) return FL_RESOURCE_EXHAUSTED;
+  st = check_links(G, F);
+  if (st != FL_OK) return st;
+  const LinkRegions& R = kLinkRegions;
+  const uint64_t nf = G->face_count, nc = G->cell_count;
+  const Report clean{kNoError, 0, 0, 0.0};
+  bool ok = cudaSetDevice(b->device) == cudaSuccess && lupload(b, R.report, &clean, sizeof(clean)) &&
+            cudaEventRecord(b->e0, b->stream) == cudaSuccess &&
+            lupload(b, R.cells, G->cells, sizeof(fl_frozen_cell) * nc) &&
+            lupload(b, R.faces, G->faces, sizeof(fl_frozen_face) * nf) &&
+            lupload(b, R.fields, F->cells, sizeof(fl_pressure_cell_fields) * nc) &&
+            lupload(b, R.pred, F->predicted_face_velocities, sizeof(double) * nf) &&
+            (!F->wetted_piston_face_fluxes || (lupload(b, R.wet, F->wetted_piston_face_fluxes, sizeof(double) * nf) &&
+                                               lupload(b, R.has_wet, F->has_wetted_piston_face_flux, nf))) &&
+            lupload(b, R.air, F->air, sizeof(fl_air_cell_pressure) * F->air_count) &&
+            lupload(b, R.itf, F->interfaces, sizeof(fl_internal_interface) * F->interface_count) &&
+            lupload(b, R.cent, G->centers, sizeof(fl_center_sample) * G->center_count);
+  if (ok && nf) {
+    LinksArgs a;
+    a.h = G->grid->h;
+    a.density = G->liquid_density;
+    a.step_duration = G->step_duration;
+    a.sigma = G->surface_tension;
+    a.ambient = F->ambient_pressure;
+    a.cells = reinterpret_cast<const fl_frozen_cell*>(b->ldev + R.cells);
+    a.nc = (int)nc;
+    a.faces = reinterpret_cast<const fl_frozen_face*>(b->ldev + R.faces);
+    a.nf = (int)nf;
+    a.fields = reinterpret_cast<const fl_pressure_cell_fields*>(b->ldev + R.fields);
+    a.predicted = reinterpret_cast<const double*>(b->ldev + R.pred);
+    a.wetted = F->wetted_piston_face_fluxes ? reinterpret_cast<const double*>(b->ldev + R.wet) : nullptr;
+    a.has_wetted = reinterpret_cast<const uint8_t*>(b->ldev + R.has_wet);
+    a.air = reinterpret_cast<const fl_air_cell_pressure*>(b->ldev + R.air);
+    a.nair = (int)F->air_count;
+    a.interfaces = reinterpret_cast<const fl_internal_interface*>(b->ldev + R.itf);
+    a.ninterfaces = (int)F->interface_count;
+    a.centers = reinterpret_cast<const fl_center_sample*>(b->ldev + R.cent);
+    a.ncenters = (int)G->center_count;
+    a.out = reinterpret_cast<fl_pressure_link*>(b->ldev + R.out);
+    a.regularized = reinterpret_cast<uint8_t*>(b->ldev + R.reg);
+    a.rep = reinterpret_cast<Report*>(b->ldev + R.report);
+    ++g_kernel_launches;
+    k_links<<<grid_of(nf, 128), 128, 0, b->stream>>>(a);
+  }
+  ok = ok && cudaGetLastError() == cudaSuccess && cudaEventRecord(b->e1, b->stream) == cudaSuccess &&
+       ldownload(b, R.out, sizeof(fl_pressure_link) * nf) && ldownload(b, R.reg, nf) &&
+       ldownload(b, R.report, sizeof(Report)) && cudaStreamSynchronize(b->stream) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    cudaStreamSynchronize(b->stream);
+    return FL_INTERNAL;
+  }
+  const Report* r = reinterpret_cast<const Report*>(b->lpin + R.report);
+  if (m) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, b->e0, b->e1);
+    m->compiled_architecture = r->arch;
+    m->kernel_ms = ms;
+  }
+  if (nf && r->key != kNoError) return (int)(r->key & 0xff);
+  for (uint64_t i = 0; i < nc; ++i) {
+    fl_pressure_cell& c = cells_out[i];
+    std::memset(&c, 0, sizeof(c));
+    for (int d = 0; d < 3; ++d) c.cell_index[d] = G->cells[i].cell_index[d];
+    c.fluid_volume = G->cells[i].fluid_volume;
+    c.target_divergence = F->cells[i].target_divergence;
+    c.bulk_modulus = F->cells[i].bulk_modulus;
+    c.previous_pressure = F->cells[i].previous_pressure;
+    c.integrated_inward_wall_flux = 0.0;
+  }
+  std::memcpy(faces_out, b->lpin + R.out, sizeof(fl_pressure_link) * nf);
+  uint64_t count = 0;
+  const uint8_t* reg = reinterpret_cast<const uint8_t*>(b->lpin + R.reg);
+  for (uint64_t f = 0; f < nf; ++f) count += reg[f];
+  if (lower_theta) *lower_theta = count;
+  return FL_OK;
 }

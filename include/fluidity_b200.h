@@ -621,6 +621,104 @@ int fl_boundary_project(fl_boundary* boundary, double h, double dt, const int32_
                         double* defect, uint64_t* gauge_ordinals, fl_mac_pressure_diagnostics* diagnostics,
                         fl_measurement* measurement);
 
+/* ---- pressure-link assembly (.links) ----
+ * BuildLiquidPressureLinks3D (native/src/liquid_boundary_workspace_3d.cc:
+ * 189-195 -> liquid_boundary_geometry_3d.cc:1077-1286 after the frozen-view
+ * checks of :1289-1380 and the link arithmetic of base/
+ * liquid_boundary_geometry_math_3d.h:676-689): the frozen cells become
+ * pressure cells; each frozen face becomes a sealed, internal (two liquid
+ * endpoints, or a certified internal interface with its jump and mixed
+ * density) or Dirichlet air link (pressure-gradient distance theta h with
+ * theta clamped to [0.05, 1], exterior pressure = ambient or the air cell's
+ * gas pressure plus sigma * curvature). Records in frozen order. */
+typedef struct {
+  int32_t cell_index[3];
+  int32_t pad;
+  double signed_distance; /* m, negative in the liquid */
+} fl_center_sample;
+typedef struct {
+  int32_t cell_index[3];
+  int32_t pad;
+  double fluid_volume;    /* m^3 */
+  double center_distance; /* m, negative */
+  double curvature;       /* 1/m */
+} fl_frozen_cell;
+typedef struct {
+  int32_t axis;
+  int32_t lattice[3];
+  uint64_t face_slot;
+  double open_area;            /* m^2 */
+  double blocked_area;         /* m^2, h^2 - open_area */
+  double wall_normal_velocity; /* m/s */
+  double prescribed_wall_flux; /* m^3/s, when has_prescribed_wall_flux */
+  uint8_t has_prescribed_wall_flux;
+  uint8_t is_low_x_piston_face;
+  uint8_t pad[6];
+} fl_frozen_face;
+typedef struct {
+  const fl_owned_grid* grid;
+  const fl_center_sample* centers; /* strictly increasing (z,y,x) */
+  uint64_t center_count;
+  const fl_frozen_cell* cells; /* strictly increasing (z,y,x), <= 4096 */
+  uint64_t cell_count;
+  const fl_frozen_face* faces; /* strictly increasing owned slot, <= 24576 */
+  uint64_t face_count;
+  double step_duration;   /* s */
+  double liquid_density;  /* kg/m^3 */
+  double surface_tension; /* N/m */
+} fl_frozen_geometry;
+typedef struct {
+  double target_divergence; /* 1/s */
+  double bulk_modulus;      /* Pa, +inf for no compliance */
+  double previous_pressure; /* Pa */
+  double density;           /* kg/m^3, when has_density */
+  uint8_t has_density;
+  uint8_t pad[7];
+} fl_pressure_cell_fields;
+typedef struct {
+  int32_t cell_index[3];
+  int32_t pad;
+  double gas_gauge_pressure; /* Pa */
+} fl_air_cell_pressure;
+typedef struct {
+  uint64_t face_ordinal;
+  double tail_fraction;
+  double surface_tension;
+  double curvature_tail_to_head;
+  double normal_viscous_jump_tail_to_head;
+} fl_internal_interface;
+typedef struct {
+  const fl_pressure_cell_fields* cells;     /* frozen cell order */
+  const double* predicted_face_velocities;  /* frozen face order, m/s */
+  double ambient_pressure;                  /* Pa */
+  const double* wetted_piston_face_fluxes;  /* NULL, or one per face (m^3/s) */
+  const uint8_t* has_wetted_piston_face_flux;
+  const fl_air_cell_pressure* air; /* strictly increasing (z,y,x) */
+  uint64_t air_count;
+  const fl_internal_interface* interfaces; /* strictly increasing face ordinal */
+  uint64_t interface_count;
+} fl_pressure_fields;
+typedef struct {
+  int32_t cell_index[3];
+  int32_t pad;
+  double fluid_volume, target_divergence, bulk_modulus, previous_pressure, integrated_inward_wall_flux;
+} fl_pressure_cell;
+/* link_kind: 0 sealed, 1 internal (link_value = jump, Pa), 2 Dirichlet (exterior pressure, Pa). */
+typedef struct {
+  int32_t axis;
+  int32_t lattice[3];
+  double open_area, inverse_density, pressure_gradient_distance, predicted_normal_velocity, wall_normal_velocity;
+  double link_value;
+  double prescribed_wall_flux;
+  int32_t link_kind;
+  uint8_t has_prescribed_wall_flux;
+  uint8_t pad[3];
+} fl_pressure_link;
+
+int fl_boundary_links(fl_boundary* boundary, const fl_frozen_geometry* geometry, const fl_pressure_fields* fields,
+                      fl_pressure_cell* cells, fl_pressure_link* faces, uint64_t* lower_theta_regularization_count,
+                      fl_measurement* measurement);
+
 /* GatherLiquidBoundaryParticles3D: one record per particle in input order;
  * fallback_counts = old PIC, new PIC and low-mass fallback particle counts. */
 int fl_boundary_gather(fl_boundary* boundary, const fl_owned_grid* grid, const fl_boundary_particle* particles,

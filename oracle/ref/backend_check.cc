@@ -22,6 +22,9 @@
 #include "fluidity/host/mac_pressure_workspace_3d.h"
 #include "fluidity/host/sparse_mac_grid_3d.h"
 
+#include <cmath>
+#include <optional>
+
 using namespace fluidity;
 
 namespace {
@@ -268,8 +271,110 @@ int bk_project(int which, const double origin[3], double h, const int32_t* block
   return 0;
 }
 
+// .links on a frozen view given as plain arrays: centre samples (x,y,z; d),
+// frozen cells (x,y,z; volume, centre distance, curvature), frozen faces
+// (axis,x,y,z; slot; open area, blocked area, wall velocity, explicit flux or
+// NaN; piston flag), pressure fields per cell (target divergence, bulk
+// modulus, previous pressure, density or NaN), predicted velocities, wetted
+// piston fluxes (NULL, or per face with NaN for none), air pressures (x,y,z;
+// p) and interfaces (ordinal; tail fraction, sigma, curvature, viscous jump).
+// Outputs: cells (5 doubles each), faces (kind 0/1/2, value, inverse
+// density, distance, predicted, wall velocity, open area, flux or NaN: 8
+// doubles each) and the lower-theta count.
+int bk_links(int which, const double origin[3], double h, const int32_t* blocks, uint64_t nb,
+             const int32_t* center_index, const double* center_distance, uint64_t ncenters,
+             const int32_t* cell_index, const double* cell_values, uint64_t nc, const int32_t* face_index,
+             const uint64_t* face_slot, const double* face_values, const uint8_t* piston, uint64_t nf,
+             double step_duration, double density, double sigma, const double* field_values,
+             const double* predicted, double ambient, const double* wetted, const int32_t* air_index,
+             const double* air_pressure, uint64_t nair, const uint64_t* itf_ordinal, const double* itf_values,
+             uint64_t nitf, double* cells_out, double* faces_out, uint64_t* lower) {
+  int code = 0;
+  const auto* table = Table(which, &code);
+  if (!table) return code;
+  auto grid = Grid(origin, h, blocks, nb);
+  if (!grid.ok()) return Code(grid.status());
+  auto ws = Workspace();
+  if (!ws.ok()) return Code(ws.status());
+  std::vector<LiquidCenterDistance3D> centers(ncenters);
+  for (uint64_t i = 0; i < ncenters; ++i)
+    centers[i] = {{center_index[3 * i], center_index[3 * i + 1], center_index[3 * i + 2]}, center_distance[i]};
+  std::vector<FrozenLiquidCell3D> cells(nc);
+  for (uint64_t i = 0; i < nc; ++i)
+    cells[i] = {{cell_index[3 * i], cell_index[3 * i + 1], cell_index[3 * i + 2]}, cell_values[3 * i],
+                cell_values[3 * i + 1], cell_values[3 * i + 2]};
+  std::vector<FrozenLiquidFace3D> faces(nf);
+  for (uint64_t f = 0; f < nf; ++f) {
+    FrozenLiquidFace3D face{};
+    face.face_index = {static_cast<FaceNormalAxis>(face_index[4 * f]),
+                       {face_index[4 * f + 1], face_index[4 * f + 2], face_index[4 * f + 3]}};
+    face.face_slot = face_slot[f];
+    face.open_area = face_values[4 * f];
+    face.blocked_area = face_values[4 * f + 1];
+    face.wall_normal_velocity = face_values[4 * f + 2];
+    if (face_values[4 * f + 3] == face_values[4 * f + 3]) face.prescribed_wall_flux = face_values[4 * f + 3];
+    face.is_low_x_piston_face = piston[f] != 0;
+    faces[f] = face;
+  }
+  const FrozenLiquidBoundaryGeometryView3D geometry{grid->view(), centers, cells, faces, step_duration, density,
+                                                    sigma, 0.0};
+  std::vector<LiquidPressureCellFields3D> fields(nc);
+  for (uint64_t i = 0; i < nc; ++i) {
+    const double* v = field_values + 4 * i;
+    fields[i] = {v[0], v[1], v[2], v[3] == v[3] ? std::optional<double>(v[3]) : std::nullopt};
+  }
+  std::vector<std::optional<double>> wet;
+  if (wetted) {
+    wet.resize(nf);
+    for (uint64_t f = 0; f < nf; ++f)
+      if (wetted[f] == wetted[f]) wet[f] = wetted[f];
+  }
+  std::vector<LiquidAirCellPressure3D> air(nair);
+  for (uint64_t k = 0; k < nair; ++k)
+    air[k] = {{air_index[3 * k], air_index[3 * k + 1], air_index[3 * k + 2]}, air_pressure[k]};
+  std::vector<LiquidInternalInterface3D> itf(nitf);
+  for (uint64_t k = 0; k < nitf; ++k) {
+    const double* v = itf_values + 4 * k;
+    itf[k] = {itf_ordinal[k], v[0], v[1], v[2], v[3]};
+  }
+  LiquidPressureFields3D pf{};
+  pf.cells = fields;
+  pf.predicted_face_velocities = std::span<const double>(predicted, nf);
+  pf.ambient_pressure = ambient;
+  pf.wetted_piston_face_fluxes = wet;
+  pf.air_cell_pressures = air;
+  pf.internal_interfaces = itf;
+  auto r = table->links(table->context, geometry, pf, *ws);
+  if (!r.ok()) return Code(r.status());
+  for (uint64_t i = 0; i < nc; ++i) {
+    const auto& c = r->cells[i];
+    double* o = cells_out + 5 * i;
+    o[0] = c.fluid_volume;
+    o[1] = c.target_divergence;
+    o[2] = c.bulk_modulus;
+    o[3] = c.previous_pressure;
+    o[4] = c.integrated_inward_wall_flux;
+  }
+  for (uint64_t f = 0; f < nf; ++f) {
+    const auto& l = r->faces[f];
+    double* o = faces_out + 8 * f;
+    o[0] = static_cast<double>(l.pressure_link.index() == 0 ? 1 : (l.pressure_link.index() == 1 ? 2 : 0));
+    o[1] = l.pressure_link.index() == 0   ? std::get<InternalMacPressureLink3D>(l.pressure_link).pressure_jump
+           : l.pressure_link.index() == 1 ? std::get<DirichletMacPressureLink3D>(l.pressure_link).exterior_pressure
+                                          : 0.0;
+    o[2] = l.inverse_density;
+    o[3] = l.pressure_gradient_distance;
+    o[4] = l.predicted_normal_velocity;
+    o[5] = l.wall_normal_velocity;
+    o[6] = l.open_area;
+    o[7] = l.prescribed_wall_flux.value_or(std::nan(""));
+  }
+  *lower = r->lower_theta_regularization_count;
+  return 0;
+}
+
 // Which operations each table fills (bit k: deposit, normalize, predict,
-// forces, gather, project, topology, update_particles).
+// forces, gather, project, topology, update_particles, links).
 int bk_filled(int which, uint32_t* mask) {
   int code = 0;
   const auto* table = Table(which, &code);
@@ -281,9 +386,10 @@ int bk_filled(int which, uint32_t* mask) {
                        reinterpret_cast<const void*>(table->gather),
                        reinterpret_cast<const void*>(table->project),
                        reinterpret_cast<const void*>(table->topology),
-                       reinterpret_cast<const void*>(table->update_particles)};
+                       reinterpret_cast<const void*>(table->update_particles),
+                       reinterpret_cast<const void*>(table->links)};
   *mask = 0;
-  for (int k = 0; k < 8; ++k)
+  for (int k = 0; k < 9; ++k)
     if (ops[k]) *mask |= 1u << k;
   return 0;
 }

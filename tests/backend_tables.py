@@ -210,3 +210,128 @@ def project(which, system, h, dt, max_iterations=256, tolerance_scale=1.0, face_
 def release():
     if _lib is not None:
         _lib.bk_release()
+
+
+def _owned_slot(blocks, axis, lat):
+    """Owned slot of face (axis, lattice) in the sorted 4^3-block list, or -1."""
+    b = np.floor_divide(lat, 4)
+    key = {tuple(v): i for i, v in enumerate(blocks.tolist())}
+    o = key.get((int(b[0]), int(b[1]), int(b[2])), -1)
+    if o < 0:
+        return -1
+    loc = lat - 4 * b
+    return o * 192 + axis * 64 + int((loc[2] * 4 + loc[1]) * 4 + loc[0])
+
+
+class LinkScene:
+    """A pool in a 12 x 32 x 12-cell tank frozen for the pressure-link
+    assembly: cells x, z in [0, 12), y in [0, 6) (864 cells), a free surface
+    in the top cell layer at a seeded height per column (so theta runs from
+    0.01 to 0.95 and some air links are regularized to 0.05 h) with small
+    seeded curvatures, tank walls at the lattice
+    planes x, z = 0 and 12 and y = 0 (sealed, some with explicit wall fluxes
+    or a wall velocity), every incident face in
+    owned-slot order, centre samples on every cell within one of the pool,
+    predictor densities on the cells x < 3 (so faces between them can carry
+    certified internal interfaces), a few air cells with their own gas
+    pressure, surface tension 0.072 N/m."""
+
+    def __init__(self, seed: int = 5):
+        rng = np.random.default_rng(seed)
+        n, ny = 12, 6
+        bz, by, bx = np.meshgrid(np.arange(-1, 4), np.arange(-1, 3), np.arange(-1, 4), indexing="ij")
+        self.blocks = np.stack([bx.ravel(), by.ravel(), bz.ravel()], 1).astype(np.int32)
+        cz, cy, cx = np.meshgrid(np.arange(n), np.arange(ny), np.arange(n), indexing="ij")
+        ci = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], 1).astype(np.int32)  # (z,y,x) order
+        self.cell_index = ci
+        # the surface height of each column: the top cells' theta (surface - 5.5) runs from 0.01 to 0.95
+        surf = 5.5 + rng.uniform(0.01, 0.95, (n + 2, n + 2))
+        height = lambda x, z: surf[np.clip(x, -1, n) + 1, np.clip(z, -1, n) + 1]  # noqa: E731
+        dist = (ci[:, 1] + 0.5 - height(ci[:, 0], ci[:, 2])) * H
+        curv = np.where(ci[:, 1] == ny - 1, rng.uniform(-3.0, 3.0, len(ci)), 0.0)
+        self.cell_values = np.stack([np.full(len(ci), H ** 3), dist, curv], 1)
+        cells = {tuple(v) for v in ci.tolist()}
+        # centre samples: every cell within one of a pool cell, (z,y,x) sorted
+        near = set()
+        for x, y, z in ci.tolist():
+            for dz in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dx in (-1, 0, 1):
+                        near.add((x + dx, y + dy, z + dz))
+        near = sorted(near, key=lambda c: (c[2], c[1], c[0]))
+        self.center_index = np.array(near, np.int32)
+        ce = self.center_index
+        self.center_distance = (ce[:, 1] + 0.5 - height(ce[:, 0], ce[:, 2])) * H
+        # incident faces in owned-slot order
+        faces = set()
+        for x, y, z in ci.tolist():
+            for a in range(3):
+                for side in (0, 1):
+                    lat = [x, y, z]
+                    lat[a] += side
+                    faces.add((a, *lat))
+        recs = []
+        for a, x, y, z in faces:
+            slot = _owned_slot(self.blocks, a, np.array([x, y, z]))
+            assert slot >= 0
+            recs.append((slot, a, x, y, z))
+        recs.sort()
+        self.face_slot = np.array([r[0] for r in recs], np.uint64)
+        self.face_index = np.array([r[1:] for r in recs], np.int32)
+        nf = len(recs)
+        fv = np.zeros((nf, 4))
+        fv[:, 3] = np.nan
+        for f, (slot, a, x, y, z) in enumerate(recs):
+            wall = [x, y, z][a] == 0 or (a != 1 and [x, y, z][a] == n)
+            fv[f, 0] = 0.0 if wall else H * H
+            fv[f, 1] = H * H - fv[f, 0]
+            if wall and f % 7 == 0:
+                fv[f, 3] = 1e-8 * ((f % 3) - 1)
+            if wall and f % 11 == 0:
+                fv[f, 2] = 0.01
+        self.face_values = fv
+        self.piston = np.zeros(nf, np.uint8)
+        self.step_duration, self.density, self.sigma = DT, 1000.0, 0.072
+        fields = np.zeros((len(ci), 4))
+        fields[:, 0] = rng.uniform(-0.1, 0.1, len(ci))
+        fields[:, 1] = np.inf
+        fields[:, 2] = rng.uniform(0.0, 50.0, len(ci))
+        fields[:, 3] = np.where(ci[:, 0] < 3, 1000.0 + rng.uniform(-5.0, 5.0, len(ci)), np.nan)
+        fields[ci[:, 0] == 5, 1] = 2.2e9  # a compliant column
+        self.fields = fields
+        self.predicted = rng.uniform(-0.3, 0.3, nf)
+        self.ambient = 101.0
+        air = [c for c in near if c[1] >= ny and 0 <= c[0] < n and 0 <= c[2] < n][::13]
+        self.air_index = np.array(air, np.int32).reshape(-1, 3)
+        self.air_pressure = rng.uniform(90.0, 110.0, len(air))
+        # interfaces on x-faces between two cells x < 3 (both with densities)
+        ords = [f for f, (slot, a, x, y, z) in enumerate(recs) if a == 0 and 1 <= x <= 2 and (x - 1, y, z) in cells
+                and y < ny - 1][::5]
+        self.itf_ordinal = np.array(ords, np.uint64)
+        self.itf_values = np.stack([rng.uniform(0.0, 1.0, len(ords)), np.full(len(ords), 0.05),
+                                    rng.uniform(-2.0, 2.0, len(ords)), rng.uniform(-1.0, 1.0, len(ords))], 1)
+        self.wetted = None
+
+
+def links(which, s: LinkScene, **override):
+    """The table's .links on the scene (fields overridable by keyword)."""
+    a = dict(s.__dict__)
+    a.update(override)
+    nc, nf = len(a["cell_index"]), len(a["face_index"])
+    cells_out = np.zeros((nc, 5))
+    faces_out = np.zeros((nf, 8))
+    lower = ctypes.c_uint64(0)
+    c = lambda x, t: np.ascontiguousarray(x, t)  # noqa: E731
+    wet = None if a["wetted"] is None else c(a["wetted"], np.float64)
+    code = lib().bk_links(
+        ctypes.c_int(which), _d3((0, 0, 0)), ctypes.c_double(H), _p(c(a["blocks"], np.int32)),
+        ctypes.c_uint64(len(a["blocks"])), _p(c(a["center_index"], np.int32)), _p(c(a["center_distance"], np.float64)),
+        ctypes.c_uint64(len(a["center_index"])), _p(c(a["cell_index"], np.int32)), _p(c(a["cell_values"], np.float64)),
+        ctypes.c_uint64(nc), _p(c(a["face_index"], np.int32)), _p(c(a["face_slot"], np.uint64)),
+        _p(c(a["face_values"], np.float64)), _p(c(a["piston"], np.uint8)), ctypes.c_uint64(nf),
+        ctypes.c_double(a["step_duration"]), ctypes.c_double(a["density"]), ctypes.c_double(a["sigma"]),
+        _p(c(a["fields"], np.float64)), _p(c(a["predicted"], np.float64)), ctypes.c_double(a["ambient"]), _p(wet),
+        _p(c(a["air_index"], np.int32)), _p(c(a["air_pressure"], np.float64)), ctypes.c_uint64(len(a["air_index"])),
+        _p(c(a["itf_ordinal"], np.uint64)), _p(c(a["itf_values"], np.float64)), ctypes.c_uint64(len(a["itf_ordinal"])),
+        _p(cells_out), _p(faces_out), ctypes.byref(lower))
+    return code, cells_out, faces_out, lower.value

@@ -37,7 +37,7 @@ def test_b200_table_refuses_without_a_device():
 
 def test_cpu_table_runs_the_bounded_dam_break():
     code, mask = bt.filled(bt.CPU)
-    assert code == 0 and mask == 0xFF
+    assert code == 0 and mask == 0x1FF
     s = bt.Scene(mixed_sides=False)
     code, q, st = bt.deposit(bt.CPU, s)
     assert code == 0
@@ -49,3 +49,10 @@ def test_cpu_table_runs_the_bounded_dam_break():
     assert code == 0 and {0, 1, 3} <= set(np.unique(val).tolist())
     code, g, counts = bt.gather(bt.CPU, s, (v, val), (v, val))
     assert code == 0 and counts[0] == counts[1] > 0
+
+
+def test_cpu_table_assembles_the_links_of_the_frozen_pool():
+    s = bt.LinkScene()
+    code, cells, faces, lower = bt.links(bt.CPU, s)
+    assert code == 0 and lower > 0
+    assert np.array_equal(np.bincount(faces[:, 0].astype(int), minlength=3) > 0, [True, True, True])

@@ -8,8 +8,8 @@ B200 table is fluidity_b200/adapter over the library's FP64 boundary kernels
 and its MAC pressure solver. Scene: the bounded 32^3 tank dam break of
 tests/backend_tables.py (1024 particles, 80 blocks of 4^3 cells).
 
-Bars: deposit quanta and compatible stencils, normalized faces and forces
-bit-identical; the gather's flags and fallback counts identical and its
+Bars: deposit quanta and compatible stencils, normalized faces, forces and the
+pressure links (tests/backend_tables.LinkScene) bit-identical; the gather's flags and fallback counts identical and its
 values within 1e-12 of the largest magnitude (the ghost fits' hypot is the
 device's); predicted faces within 1e-12 relative; the projection within the
 solvers' common gate; error codes identical, including which of several
@@ -79,10 +79,11 @@ def histories(one_sided):
 
 def test_tables_fill_the_transfer_and_projection_operations():
     code, cpu = bt.filled(CPU)
-    assert code == 0 and cpu == 0xFF
+    assert code == 0 and cpu == 0x1FF
     code, b200 = bt.filled(B200)
     assert code == 0
-    assert b200 == 0x3F  # deposit, normalize, predict, forces, gather, project; no topology or particle update
+    # deposit, normalize, predict, forces, gather, project and links; no topology or particle update
+    assert b200 == 0x13F
 
 
 def test_deposit_is_bit_identical(scene, deposited):
@@ -218,3 +219,55 @@ def test_operations_repeat_bitwise_without_growing_device_memory(one_sided, hist
             assert np.array_equal(a, b)
     torch.cuda.synchronize()
     assert torch.cuda.mem_get_info()[0] == free
+
+
+def test_links_are_bit_identical():
+    s = bt.LinkScene()
+    c0, cells_cpu, faces_cpu, low_cpu = bt.links(CPU, s)
+    c1, cells, faces, low = bt.links(B200, s)
+    assert c0 == 0 and c1 == 0
+    assert np.array_equal(cells, cells_cpu)
+    assert np.array_equal(faces, faces_cpu, equal_nan=True)
+    assert low == low_cpu > 0
+    kinds = np.bincount(faces_cpu[:, 0].astype(int), minlength=3)
+    assert kinds[0] > 0 and kinds[1] > 0 and kinds[2] > 0
+    internal = faces_cpu[:, 0] == 1
+    assert np.count_nonzero(faces_cpu[internal, 1]) == len(s.itf_ordinal)  # the interfaces' jumps
+    assert np.isfinite(faces_cpu[:, 7]).sum() > 0  # explicit wall fluxes carried through
+    # the one-sided mobility of free-surface links where the liquid cell has a predictor density
+    assert len(np.unique(faces_cpu[:, 2])) > 2
+
+
+def test_links_error_codes_match():
+    s = bt.LinkScene()
+    nf = len(s.face_index)
+
+    def both(**kw):
+        a, b = bt.links(CPU, s, **kw)[0], bt.links(B200, s, **kw)[0]
+        assert a == b, (kw.keys(), a, b)
+        return a
+
+    pred = s.predicted.copy()
+    pred[100] = np.nan
+    assert both(predicted=pred) == 3
+    air_i = np.vstack([s.air_index, s.cell_index[:1]])
+    order = np.lexsort((air_i[:, 0], air_i[:, 1], air_i[:, 2]))
+    assert both(air_index=air_i[order], air_pressure=np.append(s.air_pressure, 100.0)[order]) == 3
+    itf = s.itf_values.copy()
+    itf[2, 1] = 1e6  # surface tension so large that the step exceeds the capillary bound
+    assert both(itf_values=itf) == 10
+    keep = np.ones(nf, bool)
+    keep[500] = False
+    assert both(face_index=s.face_index[keep], face_slot=s.face_slot[keep], face_values=s.face_values[keep],
+                piston=s.piston[keep], predicted=s.predicted[keep], itf_ordinal=np.array([], np.uint64),
+                itf_values=np.zeros((0, 4))) == 9
+    fv = s.face_values.copy()
+    fv[42, 0] = 2 * bt.H * bt.H
+    assert both(face_values=fv) == 3
+    cv = s.cell_values.copy()
+    cv[7, 1] = 0.0
+    assert both(cell_values=cv) == 3
+    assert both(wetted=np.full(nf, np.nan)) == 0
+    wet = np.full(nf, np.nan)
+    wet[3] = 1e-6
+    assert both(wetted=wet) == 3
