@@ -190,6 +190,7 @@ def library():
         lib.fl_unet_param_count.argtypes = []
         lib.fl_unet_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
         lib.fl_unet_destroy.argtypes = [vp]
+        lib.fl_unet_set_tensor_cores.argtypes = [vp, ctypes.c_int]
         lib.fl_unet_init_params.argtypes = [vp, ctypes.c_uint64, vp]
         lib.fl_unet_forward.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
         lib.fl_unet_backward.argtypes = [vp, vp, vp, ctypes.c_int, vp, vp]
@@ -565,11 +566,18 @@ class UNet:
     """Training handle of the learned block preconditioner (fl_unet_*). Tensors are
     device tensors (torch, float32, contiguous); calls are ordered on `stream`."""
 
-    def __init__(self, max_batch: int):
+    def __init__(self, max_batch: int, tensor_cores: bool = False):
         h = ctypes.c_void_p()
         _check(library().fl_unet_create(int(max_batch), ctypes.byref(h)), "fl_unet_create")
         self._h = h
         self.max_batch = int(max_batch)
+        if tensor_cores:
+            self.set_tensor_cores(True)
+
+    def set_tensor_cores(self, enable: bool):
+        """fl_unet_set_tensor_cores: the 3x3x3 training convolutions as BF16 GEMMs with
+        FP32 accumulation on the tensor cores (True) or the FP32 kernels (False)."""
+        _check(library().fl_unet_set_tensor_cores(self._h, 1 if enable else 0), "fl_unet_set_tensor_cores")
 
     @staticmethod
     def param_count() -> int:

@@ -27,7 +27,8 @@ OUT = HERE / "_lib"
 LIB = OUT / "libfluidity_b200.so"
 BACKEND = OUT / "libfluidity_b200_backend.so"
 SOURCES = ["fl_grid.cu", "fl_p2g.cu", "fl_g2p.cu", "fl_pressure.cu", "fl_quanta.cu", "fl_context.cu", "fl_noalloc.cu",
-           "fl_unet.cu", "fl_unet_tc.cu", "fl_snapshot.cu", "fl_mac_pressure.cu", "fl_boundary.cu"]
+           "fl_unet.cu", "fl_unet_tc.cu", "fl_snapshot.cu", "fl_mac_pressure.cu", "fl_boundary.cu",
+           "fl_unet_train_tc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # Per-file flags: the reference-shaped pressure operator keeps every FP64
 # product apart from the sum it enters, as the reference's arithmetic does.
@@ -73,7 +74,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         if verbose:
             sys.stdout.write(out.decode())
     if force or _stale(LIB, objs):
-        cmd = [nvcc(), "-shared", *ARCH, "-o", str(LIB), *map(str, objs), "-lcudart"]
+        cmd = [nvcc(), "-shared", *ARCH, "-o", str(LIB), *map(str, objs), "-lcudart", "-lcublas"]
         subprocess.check_call(cmd)
     build_backend(force)
     return LIB

@@ -535,6 +535,27 @@ void conv3_bwd_weight(const float* in, int cin, const float* g, int cout, int ba
   k_conv3_bwd_weight<S, VALID><<<dim3(cin, cout), kT, 0, s>>>(in, cin, g, cout, batch, dw, db);
 }
 
+// A 3x3x3 layer on the SIMT kernels (tc == nullptr) or as a tensor-core GEMM;
+// the first tensor-core failure is kept in `e` and the remaining layers skip.
+template <int S, bool VALID>
+void fwd3(UNetTcTrain* tc, cudaError_t& e, const float* in, int cin, const float* w, const float* bias, int cout,
+          float* out, int batch, int relu, cudaStream_t s) {
+  if (tc == nullptr) return conv3_fwd<S, VALID>(in, cin, w, bias, cout, out, batch, relu, s);
+  if (e == cudaSuccess) e = conv3_fwd_tc<S, VALID>(*tc, in, cin, w, bias, cout, out, batch, relu, s);
+}
+template <int S>
+void bwd3_data(UNetTcTrain* tc, cudaError_t& e, const float* g, int cout, const float* w, int cin, const float* act,
+               float* din, int batch, cudaStream_t s) {
+  if (tc == nullptr) return conv3_bwd_data<S>(g, cout, w, cin, act, din, batch, s);
+  if (e == cudaSuccess) e = conv3_bwd_data_tc<S>(*tc, g, cout, w, cin, act, din, batch, s);
+}
+template <int S, bool VALID>
+void bwd3_weight(UNetTcTrain* tc, cudaError_t& e, const float* in, int cin, const float* g, int cout, int batch,
+                 float* dw, float* db, cudaStream_t s) {
+  if (tc == nullptr) return conv3_bwd_weight<S, VALID>(in, cin, g, cout, batch, dw, db, s);
+  if (e == cudaSuccess) e = conv3_bwd_weight_tc<S, VALID>(*tc, in, cin, g, cout, batch, dw, db, s);
+}
+
 }  // namespace
 
 UNetLayout unet_layout() {
@@ -603,7 +624,8 @@ void configure_unet_kernels() {
 }
 
 // Forward pass of `batch` items; every activation is kept in `cache` (layout unet_cache_layout).
-cudaError_t unet_forward(const float* P, const float* x, int batch, float* cache, float* y, cudaStream_t s) {
+cudaError_t unet_forward(const float* P, const float* x, int batch, float* cache, float* y, cudaStream_t s,
+                         UNetTcTrain* tc) {
   configure_unet_kernels();
   const UNetLayout L = unet_layout();
   const UNetCache C = unet_cache_layout(batch);
@@ -612,31 +634,35 @@ cudaError_t unet_forward(const float* P, const float* x, int batch, float* cache
   if (x != A + C.x) cudaMemcpyAsync(A + C.x, x, sizeof(float) * 2000 * B, cudaMemcpyDeviceToDevice, s);
   auto W = [&](int l) { return P + L.offset[l]; };
   auto Bi = [&](int l) { return P + L.bias[l]; };
-  conv3_fwd<8, true>(A + C.x, 2, W(0), Bi(0), 16, A + C.e1a, batch, 1, s);
-  conv3_fwd<8, false>(A + C.e1a, 16, W(1), Bi(1), 16, A + C.s1, batch, 1, s);
+  cudaError_t tce = cudaSuccess;
+  fwd3<8, true>(tc, tce, A + C.x, 2, W(0), Bi(0), 16, A + C.e1a, batch, 1, s);
+  fwd3<8, false>(tc, tce, A + C.e1a, 16, W(1), Bi(1), 16, A + C.s1, batch, 1, s);
   g_kernel_launches += 1;
   k_pool<<<grid_for(B * 16 * 64), kT, 0, s>>>(A + C.s1, 8, B * 16 * 64, A + C.p1);
-  conv3_fwd<4, false>(A + C.p1, 16, W(2), Bi(2), 32, A + C.e2a, batch, 1, s);
-  conv3_fwd<4, false>(A + C.e2a, 32, W(3), Bi(3), 32, A + C.s2, batch, 1, s);
+  fwd3<4, false>(tc, tce, A + C.p1, 16, W(2), Bi(2), 32, A + C.e2a, batch, 1, s);
+  fwd3<4, false>(tc, tce, A + C.e2a, 32, W(3), Bi(3), 32, A + C.s2, batch, 1, s);
   g_kernel_launches += 1;
   k_pool<<<grid_for(B * 32 * 8), kT, 0, s>>>(A + C.s2, 4, B * 32 * 8, A + C.p2);
-  conv3_fwd<2, false>(A + C.p2, 32, W(4), Bi(4), 64, A + C.bt, batch, 1, s);
+  fwd3<2, false>(tc, tce, A + C.p2, 32, W(4), Bi(4), 64, A + C.bt, batch, 1, s);
   g_kernel_launches += 6;
   k_conv1_fwd<<<grid_for(B * 32 * 8), kT, 0, s>>>(A + C.bt, 64, W(5), Bi(5), 32, 8, B * 32 * 8, A + C.c2);
   k_up_add_relu<<<grid_for(B * 32 * 64), kT, 0, s>>>(A + C.c2, A + C.s2, 4, B * 32 * 64, A + C.u2);
-  conv3_fwd<4, false>(A + C.u2, 32, W(6), Bi(6), 32, A + C.d2, batch, 1, s);
+  fwd3<4, false>(tc, tce, A + C.u2, 32, W(6), Bi(6), 32, A + C.d2, batch, 1, s);
   k_conv1_fwd<<<grid_for(B * 16 * 64), kT, 0, s>>>(A + C.d2, 32, W(7), Bi(7), 16, 64, B * 16 * 64, A + C.c1);
   k_up_add_relu<<<grid_for(B * 16 * 512), kT, 0, s>>>(A + C.c1, A + C.s1, 8, B * 16 * 512, A + C.u1);
-  conv3_fwd<8, false>(A + C.u1, 16, W(8), Bi(8), 16, A + C.d1, batch, 1, s);
+  fwd3<8, false>(tc, tce, A + C.u1, 16, W(8), Bi(8), 16, A + C.d1, batch, 1, s);
   k_conv1_fwd<<<grid_for(B * 512), kT, 0, s>>>(A + C.d1, 16, W(9), Bi(9), 1, 512, B * 512, A + C.y);
   if (y != nullptr && y != A + C.y)
     cudaMemcpyAsync(y, A + C.y, sizeof(float) * 512 * B, cudaMemcpyDeviceToDevice, s);
+  if (tce != cudaSuccess) return tce;
   return cudaGetLastError();
 }
 
 // Gradient of sum(gy * y) with respect to the parameters, from the cache of the last forward.
-cudaError_t unet_backward(const float* P, float* cache, const float* gy, int batch, float* G, cudaStream_t s) {
+cudaError_t unet_backward(const float* P, float* cache, const float* gy, int batch, float* G, cudaStream_t s,
+                          UNetTcTrain* tc) {
   configure_unet_kernels();
+  cudaError_t tce = cudaSuccess;
   const UNetLayout L = unet_layout();
   const UNetCache C = unet_cache_layout(batch);
   float* A = cache;
@@ -649,8 +675,8 @@ cudaError_t unet_backward(const float* P, float* cache, const float* gy, int bat
   k_conv1_bwd_weight<<<dim3(16, 1), kT, 0, s>>>(A + C.d1, 16, gy, 1, 512, batch, GW(9), GB(9));
   k_conv1_bwd_data<<<grid_for(B * 16 * 512), kT, 0, s>>>(gy, 1, W(9), 16, 512, B * 16 * 512, A + C.d1, A + C.g8a);
   // d1 (conv3 16->16 on u1); gu1 pre-activation -> g8b
-  conv3_bwd_weight<8, false>(A + C.u1, 16, A + C.g8a, 16, batch, GW(8), GB(8), s);
-  conv3_bwd_data<8>(A + C.g8a, 16, W(8), 16, A + C.u1, A + C.g8b, batch, s);
+  bwd3_weight<8, false>(tc, tce, A + C.u1, 16, A + C.g8a, 16, batch, GW(8), GB(8), s);
+  bwd3_data<8>(tc, tce, A + C.g8a, 16, W(8), 16, A + C.u1, A + C.g8b, batch, s);
   // u1 = relu(up(c1) + s1): c1 = conv1(d2, 32->16)
   g_kernel_launches += 3;
   k_up_back<<<grid_for(B * 16 * 64), kT, 0, s>>>(A + C.g8b, 8, B * 16 * 64, A + C.g4c);
@@ -658,35 +684,36 @@ cudaError_t unet_backward(const float* P, float* cache, const float* gy, int bat
   k_conv1_bwd_data<<<grid_for(B * 32 * 64), kT, 0, s>>>(A + C.g4c, 16, W(7), 32, 64, B * 32 * 64, A + C.d2,
                                                         A + C.g4a);
   // d2 (conv3 32->32 on u2); gu2 pre-activation -> g4b
-  conv3_bwd_weight<4, false>(A + C.u2, 32, A + C.g4a, 32, batch, GW(6), GB(6), s);
-  conv3_bwd_data<4>(A + C.g4a, 32, W(6), 32, A + C.u2, A + C.g4b, batch, s);
+  bwd3_weight<4, false>(tc, tce, A + C.u2, 32, A + C.g4a, 32, batch, GW(6), GB(6), s);
+  bwd3_data<4>(tc, tce, A + C.g4a, 32, W(6), 32, A + C.u2, A + C.g4b, batch, s);
   // u2 = relu(up(c2) + s2): c2 = conv1(bt, 64->32)
   g_kernel_launches += 3;
   k_up_back<<<grid_for(B * 32 * 8), kT, 0, s>>>(A + C.g4b, 4, B * 32 * 8, A + C.g2b);
   k_conv1_bwd_weight<<<dim3(64, 32), kT, 0, s>>>(A + C.bt, 64, A + C.g2b, 32, 8, batch, GW(5), GB(5));
   k_conv1_bwd_data<<<grid_for(B * 64 * 8), kT, 0, s>>>(A + C.g2b, 32, W(5), 64, 8, B * 64 * 8, A + C.bt, A + C.g2a);
   // bt (conv3 32->64 on p2) -> gp2 (g2b, 32 channels)
-  conv3_bwd_weight<2, false>(A + C.p2, 32, A + C.g2a, 64, batch, GW(4), GB(4), s);
-  conv3_bwd_data<2>(A + C.g2a, 64, W(4), 32, nullptr, A + C.g2b, batch, s);
+  bwd3_weight<2, false>(tc, tce, A + C.p2, 32, A + C.g2a, 64, batch, GW(4), GB(4), s);
+  bwd3_data<2>(tc, tce, A + C.g2a, 64, W(4), 32, nullptr, A + C.g2b, batch, s);
   // s2 gradient: (gu2 + pool_back(gp2)) * (s2 > 0) -> g4a
   g_kernel_launches += 1;
   k_pool_back_add_mask<<<grid_for(B * 32 * 64), kT, 0, s>>>(A + C.g4b, A + C.g2b, A + C.s2, 4, B * 32 * 64,
                                                             A + C.g4a);
   // e2b (conv3 32->32 on e2a) -> ge2a (g4c)
-  conv3_bwd_weight<4, false>(A + C.e2a, 32, A + C.g4a, 32, batch, GW(3), GB(3), s);
-  conv3_bwd_data<4>(A + C.g4a, 32, W(3), 32, A + C.e2a, A + C.g4c, batch, s);
+  bwd3_weight<4, false>(tc, tce, A + C.e2a, 32, A + C.g4a, 32, batch, GW(3), GB(3), s);
+  bwd3_data<4>(tc, tce, A + C.g4a, 32, W(3), 32, A + C.e2a, A + C.g4c, batch, s);
   // e2a (conv3 16->32 on p1) -> gp1 (g4b, 16 channels)
-  conv3_bwd_weight<4, false>(A + C.p1, 16, A + C.g4c, 32, batch, GW(2), GB(2), s);
-  conv3_bwd_data<4>(A + C.g4c, 32, W(2), 16, nullptr, A + C.g4b, batch, s);
+  bwd3_weight<4, false>(tc, tce, A + C.p1, 16, A + C.g4c, 32, batch, GW(2), GB(2), s);
+  bwd3_data<4>(tc, tce, A + C.g4c, 32, W(2), 16, nullptr, A + C.g4b, batch, s);
   // s1 gradient: (gu1 + pool_back(gp1)) * (s1 > 0) -> g8a
   g_kernel_launches += 1;
   k_pool_back_add_mask<<<grid_for(B * 16 * 512), kT, 0, s>>>(A + C.g8b, A + C.g4b, A + C.s1, 8, B * 16 * 512,
                                                              A + C.g8a);
   // e1b (conv3 16->16 on e1a) -> ge1a (g8c)
-  conv3_bwd_weight<8, false>(A + C.e1a, 16, A + C.g8a, 16, batch, GW(1), GB(1), s);
-  conv3_bwd_data<8>(A + C.g8a, 16, W(1), 16, A + C.e1a, A + C.g8c, batch, s);
+  bwd3_weight<8, false>(tc, tce, A + C.e1a, 16, A + C.g8a, 16, batch, GW(1), GB(1), s);
+  bwd3_data<8>(tc, tce, A + C.g8a, 16, W(1), 16, A + C.e1a, A + C.g8c, batch, s);
   // e1a (valid conv3 2->16 on x)
-  conv3_bwd_weight<8, true>(A + C.x, 2, A + C.g8c, 16, batch, GW(0), GB(0), s);
+  bwd3_weight<8, true>(tc, tce, A + C.x, 2, A + C.g8c, 16, batch, GW(0), GB(0), s);
+  if (tce != cudaSuccess) return tce;
   return cudaGetLastError();
 }
 
@@ -857,6 +884,7 @@ struct fl_unet {
   int device = 0;
   int max_batch = 0;
   float* cache = nullptr;
+  fl::UNetTcTrain* tc = nullptr;  // set: the 3x3x3 training convolutions run on the tensor cores
 };
 
 namespace {
@@ -901,8 +929,35 @@ int fl_unet_create(int max_batch, fl_unet** out) {
 
 int fl_unet_destroy(fl_unet* u) {
   if (u == nullptr) return FL_OK;
+  if (u->tc != nullptr) {
+    fl::unet_tc_train_destroy(u->tc);
+    delete u->tc;
+  }
   cudaFree(u->cache);
   delete u;
+  return FL_OK;
+}
+
+int fl_unet_set_tensor_cores(fl_unet* u, int enable) {
+  if (u == nullptr || (enable != 0 && enable != 1)) return FL_INVALID_ARGUMENT;
+  if (!enable) {
+    if (u->tc != nullptr) {
+      fl::unet_tc_train_destroy(u->tc);
+      delete u->tc;
+      u->tc = nullptr;
+    }
+    return FL_OK;
+  }
+  if (u->tc != nullptr) return FL_OK;
+  int st = fl::check_device();
+  if (st != FL_OK) return st;
+  auto* t = new fl::UNetTcTrain();
+  if (fl::unet_tc_train_create(u->max_batch, t) != cudaSuccess) {
+    cudaGetLastError();
+    delete t;
+    return FL_RESOURCE_EXHAUSTED;
+  }
+  u->tc = t;
   return FL_OK;
 }
 
@@ -917,7 +972,8 @@ int fl_unet_forward(fl_unet* u, const float* params, const float* input, int bat
   if (u == nullptr || params == nullptr || input == nullptr || batch < 0) return FL_INVALID_ARGUMENT;
   if (batch > u->max_batch) return FL_RESOURCE_EXHAUSTED;
   if (batch == 0) return FL_OK;
-  return unet_code(fl::unet_forward(params, input, batch, u->cache, output, static_cast<cudaStream_t>(stream)));
+  return unet_code(
+      fl::unet_forward(params, input, batch, u->cache, output, static_cast<cudaStream_t>(stream), u->tc));
 }
 
 int fl_unet_backward(fl_unet* u, const float* params, const float* grad_output, int batch, float* grad_params,
@@ -926,7 +982,7 @@ int fl_unet_backward(fl_unet* u, const float* params, const float* grad_output, 
     return FL_INVALID_ARGUMENT;
   if (batch > u->max_batch) return FL_RESOURCE_EXHAUSTED;
   return unet_code(fl::unet_backward(params, u->cache, grad_output, batch, grad_params,
-                                     static_cast<cudaStream_t>(stream)));
+                                     static_cast<cudaStream_t>(stream), u->tc));
 }
 
 int fl_unet_masked_mse(const float* output, const float* target, const float* mask, int batch, int relative,

@@ -32,9 +32,34 @@ UNetLayout unet_layout();
 void configure_unet_kernels();
 UNetCache unet_cache_layout(int batch);
 
-cudaError_t unet_forward(const float* params, const float* x, int batch, float* cache, float* y, cudaStream_t s);
+// Scratch of the tensor-core training convolutions (fl_unet_train_tc.cu): the
+// cuBLAS handle, the BF16 im2col, packed-weight and gradient-row operands and
+// the FP32 GEMM result, sized for a batch of up to max_batch items.
+struct UNetTcTrain {
+  void* handle = nullptr;  // cublasHandle_t
+  __nv_bfloat16* col = nullptr;
+  __nv_bfloat16* w = nullptr;
+  __nv_bfloat16* g = nullptr;
+  float* out = nullptr;
+};
+cudaError_t unet_tc_train_create(int max_batch, UNetTcTrain* t);
+void unet_tc_train_destroy(UNetTcTrain* t);
+template <int S, bool VALID>
+cudaError_t conv3_fwd_tc(UNetTcTrain& t, const float* in, int cin, const float* w, const float* bias, int cout,
+                         float* out, int batch, int relu, cudaStream_t s);
+template <int S>
+cudaError_t conv3_bwd_data_tc(UNetTcTrain& t, const float* g, int cout, const float* w, int cin, const float* act,
+                              float* din, int batch, cudaStream_t s);
+template <int S, bool VALID>
+cudaError_t conv3_bwd_weight_tc(UNetTcTrain& t, const float* in, int cin, const float* g, int cout, int batch,
+                                float* dw, float* db, cudaStream_t s);
+
+// tc == nullptr: the FP32 SIMT convolutions; otherwise the 3x3x3 convolutions
+// run as BF16 tensor-core GEMMs with FP32 accumulation.
+cudaError_t unet_forward(const float* params, const float* x, int batch, float* cache, float* y, cudaStream_t s,
+                         UNetTcTrain* tc = nullptr);
 cudaError_t unet_backward(const float* params, float* cache, const float* grad_y, int batch, float* grad_params,
-                          cudaStream_t s);
+                          cudaStream_t s, UNetTcTrain* tc = nullptr);
 cudaError_t unet_masked_mse(const float* y, const float* target, const float* mask, int batch, int relative,
                             float* loss, float* grad, cudaStream_t s);
 cudaError_t unet_block_residual_loss(const float* y, const float* x, int batch, float* loss, float* grad,

@@ -7,7 +7,7 @@ after k flexible-CG iterations give, per block holding fluid, the input
 (p* - p_k) / s, s = max |r_k| over the window. Training runs entirely in the
 library's kernels (fl_unet_forward / fl_unet_backward / fl_unet_block_residual_loss
 or fl_unet_masked_mse / fl_adam_step) on batches of 64 items with Adam at lr
-1e-3. The default loss is the block residual |r_b - A_b y|^2 / |r_b|^2: the
+1e-3, the convolutions as BF16 tensor-core GEMMs with FP32 accumulation. The default loss is the block residual |r_b - A_b y|^2 / |r_b|^2: the
 network learns to invert the pressure operator on its block, a target it can
 see in its window (the error p* - p_k is dominated by global modes that a
 block-local network cannot see, and training on it ends at the zero
@@ -62,8 +62,11 @@ def collect_pairs(n: int = 128, pairs: int = 10000, steps_between: int = 4, caps
 
 
 def train(inputs, targets, masks, steps: int = 2000, batch: int = 64, lr: float = 1e-3, seed: int = 0,
-          params=None, loss_kind: str = "residual"):
+          params=None, loss_kind: str = "residual", tensor_cores: bool = True):
     """Adam on batches of the pairs; returns (params, losses per step).
+    tensor_cores: the 3x3x3 convolutions of the forward and backward passes as BF16 GEMMs
+    with FP32 accumulation on the tensor cores (the configured training precision); False
+    runs them in FP32 kernels.
     loss_kind "residual": |r_b - A_b y|^2 / |r_b|^2 per item (fl_unet_block_residual_loss: the network
     learns the inverse of the pressure operator on its block; the zero output scores 1);
     "error": the per-item relative squared error against the targets p* - p_k (fl_unet_masked_mse)."""
@@ -71,7 +74,7 @@ def train(inputs, targets, masks, steps: int = 2000, batch: int = 64, lr: float 
 
     n = inputs.shape[0]
     batch = min(batch, n)
-    net = fb.UNet(batch)
+    net = fb.UNet(batch, tensor_cores=tensor_cores)
     P = params if params is not None else torch.empty(fb.UNet.param_count(), dtype=torch.float32, device="cuda")
     if params is None:
         fb.UNet.init_params(P, seed)
