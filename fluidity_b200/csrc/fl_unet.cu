@@ -246,14 +246,16 @@ __global__ void __launch_bounds__(kT) k_conv3_bwd_weight(const float* __restrict
   }
 }
 
-// dw[co][ci] = sum g[b][co][o] in[b][ci][o]; db[co] likewise (ci == 0 CTA). One CTA per (ci, co).
-__global__ void __launch_bounds__(kT) k_conv1_bwd_weight(const float* __restrict__ in, int cin,
+// dw[co][ci] = sum g[b][co][o] in[b][ci][o]; db[co] likewise (ci == 0 CTA). One CTA of NT
+// threads per (ci, co): 1024 for the output layer, whose 16 CTAs each reduce a whole plane.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_conv1_bwd_weight(const float* __restrict__ in, int cin,
                                                          const float* __restrict__ g, int cout, int s3, int batch,
                                                          float* __restrict__ dw, float* __restrict__ db) {
-  __shared__ float red[2 * (kT / 32)];
+  __shared__ float red[2 * (NT / 32)];
   const int ci = blockIdx.x, co = blockIdx.y;
   float a = 0.0f, bs = 0.0f;
-  for (int idx = threadIdx.x; idx < batch * s3; idx += kT) {
+  for (int idx = threadIdx.x; idx < batch * s3; idx += NT) {
     const int b = idx / s3, o = idx % s3;
     const float gv = g[((size_t)b * cout + co) * s3 + o];
     a = fmaf(gv, in[((size_t)b * cin + ci) * s3 + o], a);
@@ -266,14 +268,14 @@ __global__ void __launch_bounds__(kT) k_conv1_bwd_weight(const float* __restrict
   }
   if ((threadIdx.x & 31) == 0) {
     red[threadIdx.x >> 5] = a;
-    red[kT / 32 + (threadIdx.x >> 5)] = bs;
+    red[NT / 32 + (threadIdx.x >> 5)] = bs;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     float s = 0.0f, t = 0.0f;
-    for (int k = 0; k < kT / 32; ++k) {
+    for (int k = 0; k < NT / 32; ++k) {
       s += red[k];
-      t += red[kT / 32 + k];
+      t += red[NT / 32 + k];
     }
     dw[co * cin + ci] = s;
     if (ci == 0) db[co] = t;
@@ -672,7 +674,7 @@ cudaError_t unet_backward(const float* P, float* cache, const float* gy, int bat
   auto GB = [&](int l) { return G + L.bias[l]; };
   // out layer (16 -> 1)
   g_kernel_launches += 2;
-  k_conv1_bwd_weight<<<dim3(16, 1), kT, 0, s>>>(A + C.d1, 16, gy, 1, 512, batch, GW(9), GB(9));
+  k_conv1_bwd_weight<1024><<<dim3(16, 1), 1024, 0, s>>>(A + C.d1, 16, gy, 1, 512, batch, GW(9), GB(9));
   k_conv1_bwd_data<<<grid_for(B * 16 * 512), kT, 0, s>>>(gy, 1, W(9), 16, 512, B * 16 * 512, A + C.d1, A + C.g8a);
   // d1 (conv3 16->16 on u1); gu1 pre-activation -> g8b
   bwd3_weight<8, false>(tc, tce, A + C.u1, 16, A + C.g8a, 16, batch, GW(8), GB(8), s);
@@ -680,7 +682,7 @@ cudaError_t unet_backward(const float* P, float* cache, const float* gy, int bat
   // u1 = relu(up(c1) + s1): c1 = conv1(d2, 32->16)
   g_kernel_launches += 3;
   k_up_back<<<grid_for(B * 16 * 64), kT, 0, s>>>(A + C.g8b, 8, B * 16 * 64, A + C.g4c);
-  k_conv1_bwd_weight<<<dim3(32, 16), kT, 0, s>>>(A + C.d2, 32, A + C.g4c, 16, 64, batch, GW(7), GB(7));
+  k_conv1_bwd_weight<kT><<<dim3(32, 16), kT, 0, s>>>(A + C.d2, 32, A + C.g4c, 16, 64, batch, GW(7), GB(7));
   k_conv1_bwd_data<<<grid_for(B * 32 * 64), kT, 0, s>>>(A + C.g4c, 16, W(7), 32, 64, B * 32 * 64, A + C.d2,
                                                         A + C.g4a);
   // d2 (conv3 32->32 on u2); gu2 pre-activation -> g4b
@@ -689,7 +691,7 @@ cudaError_t unet_backward(const float* P, float* cache, const float* gy, int bat
   // u2 = relu(up(c2) + s2): c2 = conv1(bt, 64->32)
   g_kernel_launches += 3;
   k_up_back<<<grid_for(B * 32 * 8), kT, 0, s>>>(A + C.g4b, 4, B * 32 * 8, A + C.g2b);
-  k_conv1_bwd_weight<<<dim3(64, 32), kT, 0, s>>>(A + C.bt, 64, A + C.g2b, 32, 8, batch, GW(5), GB(5));
+  k_conv1_bwd_weight<kT><<<dim3(64, 32), kT, 0, s>>>(A + C.bt, 64, A + C.g2b, 32, 8, batch, GW(5), GB(5));
   k_conv1_bwd_data<<<grid_for(B * 64 * 8), kT, 0, s>>>(A + C.g2b, 32, W(5), 64, 8, B * 64 * 8, A + C.bt, A + C.g2a);
   // bt (conv3 32->64 on p2) -> gp2 (g2b, 32 channels)
   bwd3_weight<2, false>(tc, tce, A + C.p2, 32, A + C.g2a, 64, batch, GW(4), GB(4), s);
@@ -949,6 +951,7 @@ int fl_unet_set_tensor_cores(fl_unet* u, int enable) {
     return FL_OK;
   }
   if (u->tc != nullptr) return FL_OK;
+  if (u->max_batch > fl::kUNetTcMaxBatch) return FL_OUT_OF_RANGE;  // 32-bit operand indexing
   int st = fl::check_device();
   if (st != FL_OK) return st;
   auto* t = new fl::UNetTcTrain();

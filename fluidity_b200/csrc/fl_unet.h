@@ -41,7 +41,11 @@ struct UNetTcTrain {
   __nv_bfloat16* w = nullptr;
   __nv_bfloat16* g = nullptr;
   float* out = nullptr;
+  float* part = nullptr;  // bias-gradient partial sums, 64 x 32
 };
+// Largest batch of the tensor-core path: its operands (at most 512 x 432 BF16
+// per item) stay below 2^31 elements, so every index is 32-bit.
+constexpr int kUNetTcMaxBatch = 8192;
 cudaError_t unet_tc_train_create(int max_batch, UNetTcTrain* t);
 void unet_tc_train_destroy(UNetTcTrain* t);
 template <int S, bool VALID>

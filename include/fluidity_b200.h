@@ -312,13 +312,15 @@ int64_t fl_unet_param_count(void);
 /* Training workspace for up to max_batch items (all activations of one forward). */
 int fl_unet_create(int max_batch, fl_unet** out);
 int fl_unet_destroy(fl_unet* net);
-/* He-uniform weights from a counter-based stream (SplitMix64 of seed and index), zero biases. */
 /* Training precision of fl_unet_forward / fl_unet_backward: 0 (default) the
  * FP32 convolution kernels; 1 each 3x3x3 convolution (forward, data and weight
  * gradients) as a GEMM of BF16 operands with FP32 accumulation on the tensor
  * cores (im2col operands formed by this library's kernels, the GEMM by
- * cuBLAS), parameters, activations, gradients and Adam in FP32. */
+ * cuBLAS), parameters, activations, gradients and Adam in FP32. Enabling
+ * reserves the operand buffers: FL_OUT_OF_RANGE for a workspace of more than
+ * 8192 items, FL_RESOURCE_EXHAUSTED if they cannot be allocated. */
 int fl_unet_set_tensor_cores(fl_unet* net, int enable);
+/* He-uniform weights from a counter-based stream (SplitMix64 of seed and index), zero biases. */
 int fl_unet_init_params(float* params, uint64_t seed, void* stream);
 /* FP32 forward pass; keeps the activations for fl_unet_backward. */
 int fl_unet_forward(fl_unet* net, const float* params, const float* input, int batch, float* output, void* stream);
