@@ -2,6 +2,7 @@
 
     python -m fluidity_b200.profile_step --scene splash --grid 256 --steps 2 [--precision 1] [--levels 0]
         [--warm-start 1] [--inner-rtol 1e-3] [--snapshot] [--unet N]
+    python -m fluidity_b200.profile_step --train-batch 256 [--train-reps 20]
 
 Prints, per step, the status, FCG iterations, FP64 relative residual, the
 CUDA-event phase times (topology+sort, P2G, pressure, G2P; ms) and the running
@@ -10,6 +11,10 @@ asynchronous snapshot queue (device check + D2H), whose copy time is printed.
 With --unet N the learned preconditioner (He-uniform weights, seed 1) is then
 applied to a random vector on the last step's cells through the tensor-core
 kernels: 3 untimed applications, then N timed with CUDA events.
+With --train-batch B no scene is run: one training forward + backward of the
+learned preconditioner on B random items (He-uniform weights, seed 1) is timed
+with the FP32 convolution kernels and with the tensor-core convolutions, 3
+untimed then --train-reps timed with CUDA events each.
 """
 
 from __future__ import annotations
@@ -18,6 +23,34 @@ import argparse
 
 import fluidity_b200 as fb
 from fluidity_b200 import scenes
+
+
+def time_training(batch: int, reps: int):
+    import torch
+
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    params = torch.empty(fb.UNet.param_count(), dtype=torch.float32, device="cuda")
+    fb.UNet.init_params(params, 1)
+    x = torch.randn((batch, 2000), generator=gen, device="cuda")
+    gy = torch.randn((batch, 512), generator=gen, device="cuda")
+    y = torch.empty((batch, 512), device="cuda")
+    grads = torch.empty_like(params)
+    for tc in (False, True):
+        net = fb.UNet(batch, tensor_cores=tc)
+        for _ in range(3):
+            net.forward(params, x, y)
+            net.backward(params, gy, grads)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            net.forward(params, x, y)
+            net.backward(params, gy, grads)
+        e1.record()
+        torch.cuda.synchronize()
+        net.close()
+        print(f"training forward+backward, {batch} items, {'tensor cores' if tc else 'FP32 kernels'}: "
+              f"{e0.elapsed_time(e1) / reps:.3f} ms", flush=True)
 
 
 def main():
@@ -31,7 +64,11 @@ def main():
     ap.add_argument("--inner-rtol", type=float, default=1e-3)
     ap.add_argument("--snapshot", action="store_true")
     ap.add_argument("--unet", type=int, default=0)
+    ap.add_argument("--train-batch", type=int, default=0)
+    ap.add_argument("--train-reps", type=int, default=20)
     args = ap.parse_args()
+    if args.train_batch > 0:
+        return time_training(args.train_batch, args.train_reps)
     soa, mass = scenes.SCENES[args.scene](args.grid)
     ctx = fb.LiquidContext(args.grid, capacity=soa.shape[1])
     ctx.upload(soa)
