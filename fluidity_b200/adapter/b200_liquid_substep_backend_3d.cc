@@ -63,6 +63,9 @@ static_assert(sizeof(LiquidFaceValidity3D) == 1);
 static_assert(sizeof(LiquidCenterDistance3D) == sizeof(fl_center_sample));
 static_assert(offsetof(LiquidCenterDistance3D, signed_distance) == offsetof(fl_center_sample, signed_distance));
 static_assert(sizeof(FrozenLiquidCell3D) == sizeof(fl_frozen_cell));
+static_assert(sizeof(CellIndex3D) == 3 * sizeof(std::int32_t));
+static_assert(sizeof(LiquidCornerDistance3D) == sizeof(fl_corner_sample));
+static_assert(offsetof(LiquidCornerDistance3D, signed_distance) == offsetof(fl_corner_sample, signed_distance));
 static_assert(offsetof(FrozenLiquidCell3D, curvature) == offsetof(fl_frozen_cell, curvature));
 static_assert(sizeof(LiquidAirCellPressure3D) == sizeof(fl_air_cell_pressure));
 static_assert(offsetof(LiquidAirCellPressure3D, gas_gauge_pressure) ==
@@ -260,6 +263,81 @@ struct B200BackendOps3D {
   // the C-ABI's records; cells, centre samples, air pressures and interfaces
   // pass through (byte-compatible). Results are packed into the reference's
   // pressure-cell and link records.
+  // FreezeLiquidBoundaryGeometry3D (liquid_boundary_workspace_3d.cc:186 ->
+  // liquid_boundary_geometry_3d.cc:2109-2143): the frozen view in this
+  // backend's freeze bank; the centre samples are copied there as the
+  // workspace's own freeze does.
+  static absl::StatusOr<FrozenLiquidBoundaryGeometryView3D> Freeze(
+      void* context,
+      const LiquidBoundaryGeometryViewInputs3D& inputs,
+      LiquidBoundaryWorkspace3D&
+  ) {
+    auto& self = Self(context);
+    const std::size_t n = inputs.cell_indices.size();
+    if (n > kPressureCells || inputs.center_distances.size() > 27 * kPressureCells)
+      return Code(absl::StatusCode::kResourceExhausted);
+    if (inputs.sampled_solid || std::holds_alternative<AxisAlignedLiquidTank3D>(inputs.obstacle))
+      return Code(absl::StatusCode::kUnimplemented);
+    fl_freeze_inputs in{};
+    const fl_owned_grid grid = OwnedGrid(inputs.mac_grid);
+    in.grid = &grid;
+    in.cell_indices = reinterpret_cast<const std::int32_t*>(inputs.cell_indices.data());
+    in.cell_count = n;
+    in.centers = reinterpret_cast<const fl_center_sample*>(inputs.center_distances.data());
+    in.center_count = inputs.center_distances.size();
+    in.corners = reinterpret_cast<const fl_corner_sample*>(inputs.corner_distances.data());
+    in.corner_count = inputs.corner_distances.size();
+    if (const auto* hs = std::get_if<TranslatingHalfspace3D>(&inputs.obstacle)) {
+      in.obstacle = fl_obstacle{FL_OBSTACLE_HALFSPACE, 0, {hs->unit_normal.x, hs->unit_normal.y, hs->unit_normal.z},
+                                hs->start_plane_coordinate, 0.0,
+                                {hs->wall_velocity.x, hs->wall_velocity.y, hs->wall_velocity.z}};
+    } else if (const auto* sl = std::get_if<TranslatingSlab3D>(&inputs.obstacle)) {
+      in.obstacle = fl_obstacle{FL_OBSTACLE_SLAB, 0, {sl->unit_normal.x, sl->unit_normal.y, sl->unit_normal.z},
+                                sl->start_center_coordinate, sl->half_width,
+                                {sl->wall_velocity.x, sl->wall_velocity.y, sl->wall_velocity.z}};
+    } else {
+      in.obstacle.kind = FL_OBSTACLE_NONE;
+    }
+    in.step_duration = inputs.step_duration;
+    in.liquid_density = inputs.liquid_density;
+    in.surface_tension = inputs.surface_tension;
+    in.has_exact_curvature = inputs.exact_outward_interface_curvature.has_value();
+    in.exact_curvature = inputs.exact_outward_interface_curvature.value_or(0.0);
+    auto& bank = self.frozen_[1 - self.frozen_bank_];
+    bank.cells.resize(n);
+    auto& fs = self.freeze_staging_.faces;
+    fs.resize(6 * n);
+    std::uint64_t nc = 0, nf = 0;
+    double bound = 0.0;
+    const int code = fl_boundary_freeze(self.boundary_, &in, reinterpret_cast<fl_frozen_cell*>(bank.cells.data()),
+                                        &nc, fs.data(), &nf, &bound, nullptr);
+    if (code != FL_OK) return FromFl(code);
+    bank.cells.resize(nc);
+    bank.faces.resize(nf);
+    for (std::size_t f = 0; f < nf; ++f) {
+      const fl_frozen_face& o = fs[f];
+      FrozenLiquidFace3D face{};
+      face.face_index = {static_cast<FaceNormalAxis>(o.axis), {o.lattice[0], o.lattice[1], o.lattice[2]}};
+      face.face_slot = o.face_slot;
+      face.open_area = o.open_area;
+      face.blocked_area = o.blocked_area;
+      face.wall_normal_velocity = o.wall_normal_velocity;
+      if (o.has_prescribed_wall_flux) face.prescribed_wall_flux = o.prescribed_wall_flux;
+      face.is_low_x_piston_face = o.is_low_x_piston_face != 0;
+      bank.faces[f] = face;
+    }
+    bank.centers.assign(inputs.center_distances.begin(), inputs.center_distances.end());
+    self.frozen_bank_ = 1 - self.frozen_bank_;
+    return FrozenLiquidBoundaryGeometryView3D{inputs.mac_grid,
+                                              bank.centers,
+                                              bank.cells,
+                                              bank.faces,
+                                              inputs.step_duration,
+                                              inputs.liquid_density,
+                                              inputs.surface_tension,
+                                              bound};
+  }
+
   static absl::StatusOr<LiquidPressureProblemView3D> Links(
       void* context,
       const FrozenLiquidBoundaryGeometryView3D& geometry,
@@ -534,7 +612,10 @@ absl::StatusOr<std::unique_ptr<B200LiquidBackend3D>> B200LiquidBackend3D::Create
          Reserve(self->projections_[k].gauges, kPressureCells);
   }
   for (int k = 0; k < 2; ++k)
-    ok = ok && Reserve(self->links_[k].cells, kPressureCells) && Reserve(self->links_[k].faces, kFaces);
+    ok = ok && Reserve(self->links_[k].cells, kPressureCells) && Reserve(self->links_[k].faces, kFaces) &&
+         Reserve(self->frozen_[k].centers, 27 * kPressureCells) && Reserve(self->frozen_[k].cells, kPressureCells) &&
+         Reserve(self->frozen_[k].faces, kFaces);
+  ok = ok && Reserve(self->freeze_staging_.faces, 6 * kPressureCells);
   auto& ls = self->link_staging_;
   ok = ok && Reserve(ls.faces, kFaces) && Reserve(ls.fields, kPressureCells) && Reserve(ls.wetted, kFaces) &&
        Reserve(ls.has_wetted, kFaces) && Reserve(ls.cells_out, kPressureCells) && Reserve(ls.faces_out, kFaces);
@@ -564,6 +645,7 @@ LiquidSubstepBackend3D B200LiquidBackend3D::operations() {
   table.predict_missing_face = &B200BackendOps3D::PredictMissingFace;
   table.forces = &B200BackendOps3D::Forces;
   table.gather = &B200BackendOps3D::Gather;
+  table.freeze = &B200BackendOps3D::Freeze;
   table.links = &B200BackendOps3D::Links;
   table.project = &B200BackendOps3D::Project;
   return table;

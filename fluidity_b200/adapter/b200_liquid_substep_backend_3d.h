@@ -11,17 +11,20 @@
 //   .predict_missing_face  fl_boundary_predict_face   (LiquidBoundaryWorkspace3D::ContinueFace + dt a)
 //   .forces                fl_boundary_forces         (the CPU table's ApplyForces)
 //   .gather                fl_boundary_gather         (GatherLiquidBoundaryParticles3D)
+//   .freeze                fl_boundary_freeze         (FreezeLiquidBoundaryGeometry3D: no obstacle,
+//                                                      halfspace or slab; open tanks and sampled
+//                                                      solids return kUnimplemented)
 //   .links                 fl_boundary_links          (BuildLiquidPressureLinks3D)
 //   .project               fl_boundary_project        (ProjectMacPressure3D over a pressure problem)
 //   .initialize, publication and growth hooks: no device state outlives a call
 //
 // The scene-geometry, topology and particle-update operations (.sample_*,
-// .topology, .freeze, .wetted_piston, .project_viscous, .update_particles)
+// .topology, .wetted_piston, .project_viscous, .update_particles)
 // are outside this library and stay null: the scheduler's
 // Create rejects a scene that needs them, and no CPU callback is substituted.
 //
 // Results borrow the backend's own two banks per region (deposit,
-// normalization, gather, links, projection), reserved at Create for the reference's
+// normalization, gather, freeze, links, projection), reserved at Create for the reference's
 // bounded capacities (1024 particles, 24576 faces, 4096 pressure cells); a
 // borrow expires on the next successful operation of the same region, as the
 // workspace's own do. Attempt operations allocate nothing; errors return
@@ -67,6 +70,11 @@ class B200LiquidBackend3D {
     std::vector<MacPressureCell3D> cells;
     std::vector<MacPressureFace3D> faces;
   };
+  struct FreezeBank {
+    std::vector<LiquidCenterDistance3D> centers;
+    std::vector<FrozenLiquidCell3D> cells;
+    std::vector<FrozenLiquidFace3D> faces;
+  };
   // Host staging of the link assembly's optional-valued records in the C-ABI's layout.
   struct LinkStaging {
     std::vector<fl_frozen_face> faces;
@@ -75,6 +83,10 @@ class B200LiquidBackend3D {
     std::vector<std::uint8_t> has_wetted;
     std::vector<fl_pressure_cell> cells_out;
     std::vector<fl_pressure_link> faces_out;
+  };
+  // Host staging of the freeze's face records in the C-ABI's layout.
+  struct FreezeStaging {
+    std::vector<fl_frozen_face> faces;
   };
   // Host staging of a pressure problem in the C-ABI's record layout.
   struct PressureStaging {
@@ -94,9 +106,12 @@ class B200LiquidBackend3D {
   GatherBank gathered_[2];
   ProjectionBank projections_[2];
   LinkBank links_[2];
+  FreezeBank frozen_[2];
   PressureStaging staging_;
   LinkStaging link_staging_;
-  int deposit_bank_ = 0, normalize_bank_ = 0, gather_bank_ = 0, projection_bank_ = 0, links_bank_ = 0;
+  FreezeStaging freeze_staging_;
+  int deposit_bank_ = 0, normalize_bank_ = 0, gather_bank_ = 0, projection_bank_ = 0, links_bank_ = 0,
+      frozen_bank_ = 0;
 };
 
 }  // namespace fluidity

@@ -28,9 +28,12 @@
 // Errors are ordered: a failing lane writes atomicMin((order << 8) | code) into
 // the report, where order follows the CPU loop (particle, component, sample,
 // old then new history), so the call returns the CPU's first error.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <limits>
+#include <memory>
 
 #include "fl_internal.cuh"
 #include "fl_kernels.h"
@@ -1117,6 +1120,8 @@ struct fl_boundary {
   fl::MpScratch pressure;  // the bounded projection's scratch, reserved for its caps
   char* ldev = nullptr;    // pressure-link assembly: device arena
   char* lpin = nullptr;    // and its pinned mirror
+  char* fdev = nullptr;    // geometry freeze: device arena
+  char* fpin = nullptr;    // and its pinned mirror
 };
 
 namespace {
@@ -1256,6 +1261,7 @@ unsigned grid_of(uint64_t n, unsigned block) { return (unsigned)((n + block - 1)
 namespace {
 size_t link_arena_bytes();  // the pressure-link assembly's staging, defined with its regions below
 }  // namespace
+size_t freeze_arena_bytes();  // the geometry freeze's staging, likewise
 
 extern "C" int fl_boundary_create(fl_boundary** out) {
   if (!out) return FL_INVALID_ARGUMENT;
@@ -1269,7 +1275,9 @@ extern "C" int fl_boundary_create(fl_boundary** out) {
             cudaMalloc(&b->dev, kRegions.total) == cudaSuccess &&
             cudaMallocHost(&b->pin, kRegions.staged) == cudaSuccess && b->pressure.reserve_caps() &&
             cudaMalloc(&b->ldev, link_arena_bytes()) == cudaSuccess &&
-            cudaMallocHost(&b->lpin, link_arena_bytes()) == cudaSuccess;
+            cudaMallocHost(&b->lpin, link_arena_bytes()) == cudaSuccess &&
+            cudaMalloc(&b->fdev, freeze_arena_bytes()) == cudaSuccess &&
+            cudaMallocHost(&b->fpin, freeze_arena_bytes()) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     fl_boundary_destroy(b);
@@ -1284,6 +1292,8 @@ extern "C" int fl_boundary_destroy(fl_boundary* b) {
   if (b->device >= 0) cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   b->pressure.destroy();
+  if (b->fpin) cudaFreeHost(b->fpin);
+  if (b->fdev) cudaFree(b->fdev);
   if (b->lpin) cudaFreeHost(b->lpin);
   if (b->ldev) cudaFree(b->ldev);
   if (b->pin) cudaFreeHost(b->pin);
@@ -1783,5 +1793,950 @@ extern "C" int fl_boundary_links(fl_boundary* b, const fl_frozen_geometry* G, co
   const uint8_t* reg = reinterpret_cast<const uint8_t*>(b->lpin + R.reg);
   for (uint64_t f = 0; f < nf; ++f) count += reg[f];
   if (lower_theta) *lower_theta = count;
+  return FL_OK;
+}
+
+// ---- geometry freeze (.freeze) ----
+//
+// The geometry queries of base/liquid_boundary_geometry_math_3d.h restated for
+// the obstacle kinds offered here (none, halfspace, slab): cell volumes
+// (:739-780), face areas (:782-847), curvature (:686-725) and the capillary
+// bound (:667-675). Positions are in cell widths; a clipping vertex carries
+// the liquid distance interpolated along the clipped edges. The host stages
+// the sample lookups in the reference's order (liquid_boundary_geometry_3d.cc:
+// 765-1075), one thread computes one query, and each query keeps its own
+// status so the host can report the first failure in ordinal order.
+namespace fl {
+namespace {
+
+constexpr int kPolyCap = 10;  // a tetrahedron face clipped twice has <= 5 vertices; a cap <= 2 per cut edge
+constexpr int kPolyhCap = 7;  // 4 faces + one cap per clip
+constexpr int kCutCap = 2 * kPolyhCap;
+constexpr double kNaN = __builtin_nan("");
+
+struct ClipVertex {
+  double p[3];  // position in cell widths
+  double d;     // interpolated liquid distance (m)
+};
+
+template <int N>
+struct VertexList {
+  ClipVertex v[N];
+  int n = 0;
+  bool overflow = false;
+  __device__ void push(const ClipVertex& x) {
+    if (n == N) {
+      overflow = true;
+      return;
+    }
+    v[n++] = x;
+  }
+};
+using Polygon = VertexList<kPolyCap>;
+
+struct Polyhedron {
+  Polygon f[kPolyhCap];
+  int n = 0;
+  bool overflow = false;
+};
+
+// A plane's clip distance: the liquid distance itself, or n . p - c.
+struct ClipPlane {
+  double n[3];
+  double c;
+  bool liquid;
+};
+
+__device__ __forceinline__ void cross3(const double* a, const double* b, double* o) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// Euclidean norm by scaling with the largest magnitude (the overflow-safe
+// textbook form, as the host's three-argument hypot evaluates it).
+__device__ __forceinline__ double norm3(double x, double y, double z) {
+  x = fabs(x);
+  y = fabs(y);
+  z = fabs(z);
+  const double a = x < y ? (y < z ? z : y) : (x < z ? z : x);
+  if (a == 0.0) return 0.0;
+  const double sx = x / a, sy = y / a, sz = z / a;
+  return a * sqrt(sx * sx + sy * sy + sz * sz);
+}
+
+__device__ __forceinline__ double clip_distance(const ClipVertex& v, const ClipPlane& pl) {
+  return pl.liquid ? v.d : dot3(pl.n, v.p) - pl.c;
+}
+
+// Keeps the part with distance <= 0; each crossing gets an intersection whose
+// weights are formed from the distances scaled by their larger magnitude.
+template <int NO, int NI>
+__device__ void clip_polygon(const VertexList<NI>& in, const ClipPlane& pl, VertexList<NO>& out,
+                             VertexList<kCutCap>* cuts) {
+  out.n = 0;
+  out.overflow = false;
+  if (in.overflow) {
+    out.overflow = true;
+    return;
+  }
+  if (in.n == 0) return;
+  ClipVertex prev = in.v[in.n - 1];
+  double dprev = clip_distance(prev, pl);
+  for (int k = 0; k < in.n; ++k) {
+    const ClipVertex cur = in.v[k];
+    const double dcur = clip_distance(cur, pl);
+    if ((dprev <= 0.0) != (dcur <= 0.0)) {
+      const double mag = fabs(dprev) < fabs(dcur) ? fabs(dcur) : fabs(dprev);
+      const double sp = dprev / mag, sc = dcur / mag;
+      const double diff = sp - sc;
+      const double wp = -sc / diff, wc = sp / diff;
+      ClipVertex x;
+      for (int a = 0; a < 3; ++a) x.p[a] = prev.p[a] * wp + cur.p[a] * wc;
+      x.d = wp * prev.d + wc * cur.d;
+      out.push(x);
+      if (cuts) cuts->push(x);
+    }
+    if (dcur <= 0.0) out.push(cur);
+    prev = cur;
+    dprev = dcur;
+  }
+}
+
+// Scales a direction by a power of two so its largest component is in
+// [1/2, 1), then to unit length.
+__device__ void unit_direction(const double* d, double* o) {
+  const double big = fmax(fmax(fabs(d[0]), fabs(d[1])), fabs(d[2]));
+  if (big == 0.0) {
+    o[0] = o[1] = o[2] = 0.0;
+    return;
+  }
+  int e = 0;
+  (void)frexp(big, &e);
+  double s[3];
+  for (int a = 0; a < 3; ++a) s[a] = ldexp(d[a], -e);
+  const double inv = 1 / norm3(s[0], s[1], s[2]);
+  for (int a = 0; a < 3; ++a) o[a] = s[a] * inv;
+}
+
+__device__ bool same_position(const ClipVertex& a, const ClipVertex& b) {
+  return a.p[0] == b.p[0] && a.p[1] == b.p[1] && a.p[2] == b.p[2];
+}
+
+// A tetrahedron as four triangles (the first polyhedron of a cell query).
+struct Tetrahedron {
+  VertexList<3> f[4];
+  int n = 4;
+  bool overflow = false;
+};
+
+// Clips every face of a convex polyhedron and closes it with the cap through
+// the distinct cut points, ordered by angle about their centroid.
+template <typename In>
+__device__ void clip_polyhedron(const In& in, const ClipPlane& pl, Polyhedron& out) {
+  out.n = 0;
+  out.overflow = false;
+  if (in.overflow) {
+    out.overflow = true;
+    return;
+  }
+  VertexList<kCutCap> cuts;
+  for (int k = 0; k < in.n; ++k) {
+    Polygon clipped;
+    clip_polygon(in.f[k], pl, clipped, &cuts);
+    if (clipped.overflow || cuts.overflow) {
+      out.overflow = true;
+      return;
+    }
+    if (clipped.n >= 3) {
+      if (out.n == kPolyhCap) {
+        out.overflow = true;
+        return;
+      }
+      out.f[out.n++] = clipped;
+    }
+  }
+  Polygon cap;
+  for (int k = 0; k < cuts.n; ++k) {
+    bool seen = false;
+    for (int j = 0; j < cap.n; ++j) seen = seen || same_position(cap.v[j], cuts.v[k]);
+    if (!seen) cap.push(cuts.v[k]);
+  }
+  if (cap.overflow) {
+    out.overflow = true;
+    return;
+  }
+  if (cap.n < 3) return;
+  double center[3] = {0.0, 0.0, 0.0};
+  const double w = 1.0 / cap.n;
+  for (int k = 0; k < cap.n; ++k)
+    for (int a = 0; a < 3; ++a) center[a] = center[a] + cap.v[k].p[a] * w;
+  double t[3], nrm[3] = {0.0, 0.0, 0.0}, d[3];
+  for (int a = 0; a < 3; ++a) d[a] = cap.v[0].p[a] - center[a];
+  unit_direction(d, t);
+  for (int k = 1; k < cap.n; ++k) {
+    double u[3], c[3];
+    for (int a = 0; a < 3; ++a) d[a] = cap.v[k].p[a] - center[a];
+    unit_direction(d, u);
+    cross3(t, u, c);
+    unit_direction(c, nrm);
+    if (norm3(nrm[0], nrm[1], nrm[2]) > 0.0) break;
+  }
+  double bt[3];
+  cross3(nrm, t, bt);
+  const double tl = norm3(t[0], t[1], t[2]), bl = norm3(bt[0], bt[1], bt[2]);
+  if (!(tl > 0.0 && bl > 0.0)) return;
+  double ut[3], ub[3];
+  const double it = 1 / tl, ib = 1 / bl;
+  for (int a = 0; a < 3; ++a) {
+    ut[a] = t[a] * it;
+    ub[a] = bt[a] * ib;
+  }
+  auto angle = [&](const ClipVertex& v) {
+    double e[3];
+    for (int a = 0; a < 3; ++a) e[a] = v.p[a] - center[a];
+    return atan2(dot3(e, ub), dot3(e, ut));
+  };
+  for (int k = 1; k < cap.n; ++k) {  // insertion sort, stable
+    const ClipVertex v = cap.v[k];
+    int j = k;
+    while (j > 0 && angle(v) < angle(cap.v[j - 1])) {
+      cap.v[j] = cap.v[j - 1];
+      --j;
+    }
+    cap.v[j] = v;
+  }
+  if (out.n == kPolyhCap) {
+    out.overflow = true;
+    return;
+  }
+  out.f[out.n++] = cap;
+}
+
+// Each coordinate row of a small set of vectors scaled by a power of two so
+// its largest entry is in [1/2, 1); returns the exponent taken out.
+template <int N>
+__device__ int normalize_row(double (*e)[3], int axis) {
+  double big = 0.0;
+  for (int k = 0; k < N; ++k) big = fmax(big, fabs(e[k][axis]));
+  if (big == 0.0) return 0;
+  int x = 0;
+  (void)frexp(big, &x);
+  for (int k = 0; k < N; ++k) e[k][axis] = ldexp(e[k][axis], -x);
+  return x;
+}
+
+// A scaled determinant times h^dim, with the exponents combined before the
+// rounding; NaN when a nonzero measure is not representable.
+__device__ double physical_measure(double det, int exp, double h, int dim) {
+  if (det == 0.0) return 0.0;
+  int he = 0;
+  const double hm = frexp(h, &he);
+  double m = det;
+  for (int a = 0; a < dim; ++a) m *= hm;
+  const double r = ldexp(m, exp + dim * he);
+  if (!isfinite(r) || r == 0.0) return kNaN;
+  return r;
+}
+
+// Volume as tetrahedra from the mean of all polygon vertices.
+__device__ double clipped_volume(const Polyhedron& ph, double h) {
+  if (ph.overflow) return kNaN;
+  double apex[3] = {0.0, 0.0, 0.0};
+  int count = 0;
+  for (int k = 0; k < ph.n; ++k) {
+    if (ph.f[k].overflow) return kNaN;
+    for (int j = 0; j < ph.f[k].n; ++j) {
+      for (int a = 0; a < 3; ++a) apex[a] = apex[a] + ph.f[k].v[j].p[a];
+      ++count;
+    }
+  }
+  if (count == 0) return 0.0;
+  const double inv = 1.0 / count;
+  for (int a = 0; a < 3; ++a) apex[a] = apex[a] * inv;
+  double vol = 0.0;
+  for (int k = 0; k < ph.n; ++k) {
+    const Polygon& pg = ph.f[k];
+    for (int j = 1; j + 1 < pg.n; ++j) {
+      double e[3][3];
+      for (int a = 0; a < 3; ++a) {
+        e[0][a] = pg.v[0].p[a] - apex[a];
+        e[1][a] = pg.v[j].p[a] - apex[a];
+        e[2][a] = pg.v[j + 1].p[a] - apex[a];
+      }
+      int x = 0;
+      for (int a = 0; a < 3; ++a) x += normalize_row<3>(e, a);
+      double c[3];
+      cross3(e[1], e[2], c);
+      vol += physical_measure(fabs(dot3(e[0], c)) / 6, x, h, 3);
+    }
+  }
+  return vol;
+}
+
+// Area of a planar polygon's triangle fan, each component of a triangle's
+// area vector with its own two coordinate rows scaled.
+template <int N>
+__device__ double clipped_area(const VertexList<N>& pg, double h) {
+  if (pg.overflow) return kNaN;
+  double area = 0.0;
+  for (int j = 1; j + 1 < pg.n; ++j) {
+    double e[2][3];
+    for (int a = 0; a < 3; ++a) {
+      e[0][a] = pg.v[j].p[a] - pg.v[0].p[a];
+      e[1][a] = pg.v[j + 1].p[a] - pg.v[0].p[a];
+    }
+    double w[3];
+    for (int a = 0; a < 3; ++a) {
+      double s[2][3] = {{e[0][0], e[0][1], e[0][2]}, {e[1][0], e[1][1], e[1][2]}};
+      const int f = (a + 1) % 3, g = (a + 2) % 3;
+      const int x = normalize_row<2>(s, f) + normalize_row<2>(s, g);
+      w[a] = physical_measure((s[0][f] * s[1][g] - s[0][g] * s[1][f]) / 2, x, h, 2);
+    }
+    area += norm3(w[0], w[1], w[2]);
+  }
+  return area;
+}
+
+// A polygon lying wholly on the kept side's boundary or beyond is closed.
+template <int N>
+__device__ double open_face_area(const VertexList<N>& pg, const ClipPlane& pl, double h) {
+  if (pg.overflow) return kNaN;
+  bool any = false;
+  for (int k = 0; k < pg.n; ++k) any = any || clip_distance(pg.v[k], pl) < 0.0;
+  if (!any) return 0.0;
+  Polygon c;
+  clip_polygon(pg, pl, c, nullptr);
+  return clipped_area(c, h);
+}
+
+struct FreezeObstacle {
+  int kind;  // FL_OBSTACLE_*
+  double n[3];
+  double coordinate, half_width;
+};
+
+// The obstacle's planes in the query's cell-width frame (anchor: the lattice
+// corner of the queried cell or face); present = false without an obstacle.
+struct LocalPlanes {
+  bool present, slab;
+  double n[3];
+  double low, high;
+};
+
+__device__ int local_planes(const FreezeObstacle& ob, const double origin[3], double h, const int32_t idx[3],
+                            LocalPlanes& lp) {
+  lp.present = ob.kind == FL_OBSTACLE_HALFSPACE || ob.kind == FL_OBSTACLE_SLAB;
+  lp.slab = ob.kind == FL_OBSTACLE_SLAB;
+  for (int a = 0; a < 3; ++a) lp.n[a] = ob.n[a];
+  const double hw = lp.slab ? ob.half_width : 0.0;
+  lp.low = ob.coordinate - hw;
+  lp.high = ob.coordinate + hw;
+  if (!lp.present) return FL_OK;
+  double anchor[3];
+  for (int a = 0; a < 3; ++a) anchor[a] = origin[a] + h * (double)idx[a];
+  const double proj = dot3(lp.n, anchor);
+  lp.low = (lp.low - proj) / h;
+  lp.high = (lp.high - proj) / h;
+  if (!finite3(anchor) || !isfinite(lp.low) || !isfinite(lp.high) || (lp.slab && lp.low >= lp.high))
+    return FL_OUT_OF_RANGE;
+  return FL_OK;
+}
+
+// The six tetrahedra of the cube around its 0-7 diagonal (corner bit a = offset along axis a).
+__constant__ int kCubeTets[6][4] = {{0, 1, 3, 7}, {0, 1, 5, 7}, {0, 2, 3, 7}, {0, 2, 6, 7}, {0, 4, 5, 7}, {0, 4, 6, 7}};
+
+struct CellQuery {
+  double corner[8];
+  int32_t index[3];
+  int32_t pad;
+};
+struct CellResult {
+  double low, high;  // liquid volume on each side of a slab (high: all of it otherwise), m^3
+  int32_t status;
+  int32_t pad;
+};
+struct FaceQuery {
+  int32_t axis;
+  int32_t lattice[3];
+};
+struct FaceResult {
+  double open, blocked;
+  int32_t status;
+  int32_t pad;
+};
+struct CurvatureQuery {
+  double d[27];  // centre distances, x fastest, the eight outer corners unused
+};
+struct CurvatureResult {
+  double curvature;
+  int32_t status;
+  int32_t pad;
+};
+
+struct FreezeArgs {
+  double origin[3];
+  double h;
+  FreezeObstacle obstacle;
+  const CellQuery* cq;
+  CellResult* cr;
+  int ncell;
+  const FaceQuery* fq;
+  FaceResult* fr;
+  int nface;
+  const CurvatureQuery* kq;
+  CurvatureResult* kr;
+  int ncurv;
+  double density, sigma;
+  double* capillary;  // [0] bound, [1] status
+  int* arch;
+};
+
+__global__ void k_freeze_cells(FreezeArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *a.arch = compiled_arch();
+  if (i >= a.ncell) return;
+  const CellQuery& q = a.cq[i];
+  CellResult r{0.0, 0.0, FL_OK, 0};
+  LocalPlanes lp;
+  r.status = local_planes(a.obstacle, a.origin, a.h, q.index, lp);
+  if (r.status != FL_OK) {
+    a.cr[i] = r;
+    return;
+  }
+  ClipVertex corner[8];
+  for (int c = 0; c < 8; ++c) {
+    for (int d = 0; d < 3; ++d) corner[c].p[d] = (double)((c >> d) & 1);
+    corner[c].d = q.corner[c];
+  }
+  const ClipPlane liquid{{0.0, 0.0, 0.0}, 0.0, true};
+  const ClipPlane above{{-lp.n[0], -lp.n[1], -lp.n[2]}, -lp.high, false};
+  const ClipPlane below{{lp.n[0], lp.n[1], lp.n[2]}, lp.low, false};
+  for (int t = 0; t < 6; ++t) {
+    const ClipVertex& A = corner[kCubeTets[t][0]];
+    const ClipVertex& B = corner[kCubeTets[t][1]];
+    const ClipVertex& C = corner[kCubeTets[t][2]];
+    const ClipVertex& D = corner[kCubeTets[t][3]];
+    if (!(A.d < 0.0 || B.d < 0.0 || C.d < 0.0 || D.d < 0.0)) continue;  // an all-zero tetrahedron holds no liquid
+    Tetrahedron tet;
+    const ClipVertex* faces[4][3] = {{&A, &B, &C}, {&A, &B, &D}, {&A, &C, &D}, {&B, &C, &D}};
+    for (int f = 0; f < 4; ++f)
+      for (int k = 0; k < 3; ++k) tet.f[f].push(*faces[f][k]);
+    Polyhedron wet;
+    clip_polyhedron(tet, liquid, wet);
+    if (!lp.present) {
+      r.high += clipped_volume(wet, a.h);
+    } else {
+      Polyhedron side;
+      clip_polyhedron(wet, above, side);
+      r.high += clipped_volume(side, a.h);
+      if (lp.slab) {
+        clip_polyhedron(wet, below, side);
+        r.low += clipped_volume(side, a.h);
+      }
+    }
+  }
+  a.cr[i] = r;
+}
+
+__global__ void k_freeze_faces(FreezeArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nface) return;
+  const FaceQuery& q = a.fq[i];
+  FaceResult r{0.0, 0.0, FL_OK, 0};
+  const double h = a.h, full = h * h;
+  if (q.axis < 0 || q.axis >= 3) {
+    r.status = FL_INVALID_ARGUMENT;
+    a.fr[i] = r;
+    return;
+  }
+  LocalPlanes lp;
+  r.status = local_planes(a.obstacle, a.origin, h, q.lattice, lp);
+  if (r.status != FL_OK) {
+    a.fr[i] = r;
+    return;
+  }
+  const int t0 = q.axis == 0 ? 1 : 0, t1 = q.axis == 2 ? 1 : 2;
+  ClipVertex v[4] = {};
+  v[1].p[t0] = 1.0;
+  v[2].p[t0] = 1.0;
+  v[2].p[t1] = 1.0;
+  v[3].p[t1] = 1.0;
+  const ClipPlane inside{{lp.n[0], lp.n[1], lp.n[2]}, lp.high, false};
+  const ClipPlane beyond{{-lp.n[0], -lp.n[1], -lp.n[2]}, -lp.low, false};
+  const ClipPlane above{{-lp.n[0], -lp.n[1], -lp.n[2]}, -lp.high, false};
+  const ClipPlane below{{lp.n[0], lp.n[1], lp.n[2]}, lp.low, false};
+  double geometric_open = 0.0, geometric_blocked = 0.0;
+  for (int tri = 0; tri < 2; ++tri) {
+    VertexList<3> pg;
+    pg.push(v[0]);
+    pg.push(v[tri + 1]);
+    pg.push(v[tri + 2]);
+    if (!lp.present) {
+      geometric_open += clipped_area(pg, h);
+      continue;
+    }
+    Polygon blocked;
+    clip_polygon(pg, inside, blocked, nullptr);
+    if (lp.slab) {
+      Polygon b2;
+      clip_polygon(blocked, beyond, b2, nullptr);
+      blocked = b2;
+    }
+    geometric_blocked += clipped_area(blocked, h);
+    geometric_open += open_face_area(pg, above, h);
+    if (lp.slab) geometric_open += open_face_area(pg, below, h);
+  }
+  r.open = full < geometric_open ? full : geometric_open;
+  r.blocked = full - r.open;
+  if (!isfinite(geometric_open) || !isfinite(geometric_blocked) ||
+      geometric_open / full > 1 + 64 * DBL_EPSILON || !(r.open == 0.0 || is_normal(r.open)) ||
+      !(r.blocked == 0.0 || is_normal(r.blocked)) || (geometric_blocked > 0 && r.blocked == 0.0))
+    r.status = FL_OUT_OF_RANGE;
+  a.fr[i] = r;
+}
+
+// Outward curvature from centred differences: div(grad d / |grad d|) with the
+// Hessian's mixed entries from the four edge neighbours of each plane.
+__global__ void k_freeze_curvature(FreezeArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.ncurv) return;
+  const double* d = a.kq[i].d;
+  const double h = a.h;
+  const int stride[3] = {1, 3, 9};
+  double g[3], H[3][3];
+  for (int ax = 0; ax < 3; ++ax) {
+    const double lo = d[13 - stride[ax]], hi = d[13 + stride[ax]];
+    g[ax] = (hi - lo) / (2 * h);
+    H[ax][ax] = ((hi - d[13]) + (lo - d[13])) / h / h;
+    for (int o = 0; o < ax; ++o) {
+      double mixed = 0.0;
+      for (int s = -1; s <= 1; s += 2)
+        for (int u = -1; u <= 1; u += 2) mixed += (double)(s * u) * (d[13 + s * stride[ax] + u * stride[o]] / 4);
+      H[ax][o] = mixed / h / h;
+      H[o][ax] = H[ax][o];
+    }
+  }
+  CurvatureResult r{0.0, FL_OK, 0};
+  const double norm = norm3(g[0], g[1], g[2]);
+  if (!finite3(g) || !isfinite(norm)) {
+    r.status = FL_OUT_OF_RANGE;
+  } else if (norm < 1e-8) {
+    r.status = FL_FAILED_PRECONDITION;
+  } else {
+    const double inv = 1 / norm;
+    const double nv[3] = {g[0] * inv, g[1] * inv, g[2] * inv};
+    double k = 0.0;
+    for (int ax = 0; ax < 3 && r.status == FL_OK; ++ax) {
+      if (!finite3(H[ax])) {
+        r.status = FL_OUT_OF_RANGE;
+        break;
+      }
+      k += (H[ax][ax] - nv[ax] * dot3(H[ax], nv)) / norm;
+    }
+    if (r.status == FL_OK && !isfinite(k)) r.status = FL_OUT_OF_RANGE;
+    r.curvature = k;
+  }
+  a.kr[i] = r;
+}
+
+// sqrt(rho h^3 / (4 pi sigma)): the step below which a capillary wave of the
+// cell's size stays resolved.
+__global__ void k_freeze_capillary(FreezeArgs a) {
+  const double pi = 3.141592653589793238462643383279502884;
+  const double h = a.h, volume = h * h * h;
+  const double square = a.density * volume / (4 * pi * a.sigma);
+  a.capillary[0] = is_normal(square) ? sqrt(square) : 0.0;
+  a.capillary[1] = is_normal(square) ? (double)FL_OK : (double)FL_OUT_OF_RANGE;
+}
+
+}  // namespace
+}  // namespace fl
+
+namespace {
+
+struct FreezeRegions {
+  size_t cq, cr, fq, fr, kq, kr, cap, arch, total;
+  FreezeRegions() {
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+      const size_t r = o;
+      o = align_up(o + bytes);
+      return r;
+    };
+    cq = take(sizeof(CellQuery) * kMaxLinkCells);
+    cr = take(sizeof(CellResult) * kMaxLinkCells);
+    fq = take(sizeof(FaceQuery) * kMaxFaces);
+    fr = take(sizeof(FaceResult) * kMaxFaces);
+    kq = take(sizeof(CurvatureQuery) * kMaxLinkCells);
+    kr = take(sizeof(CurvatureResult) * kMaxLinkCells);
+    cap = take(2 * sizeof(double));
+    arch = take(sizeof(int));
+    total = o;
+  }
+};
+
+const FreezeRegions kFreezeRegions;
+
+}  // namespace
+
+size_t freeze_arena_bytes() { return kFreezeRegions.total; }
+
+namespace {
+
+// OffsetCellIndex (liquid_boundary_geometry_3d.cc:47-60): one lattice step,
+// out of range past the int32 lattice.
+int offset_cell(const int32_t* in, int axis, int amount, int32_t* out) {
+  int64_t v = (int64_t)in[axis] + amount;
+  if (v < INT32_MIN || v > INT32_MAX) return FL_OUT_OF_RANGE;
+  out[0] = in[0];
+  out[1] = in[1];
+  out[2] = in[2];
+  out[axis] = (int32_t)v;
+  return FL_OK;
+}
+
+// LookupSignedDistance (:82-92) over either sample kind; FailedPrecondition when absent.
+template <typename R>
+int lookup_distance(const R* recs, uint64_t n, const int32_t* key, const int32_t* (*keyof)(const R&), double* out) {
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) / 2;
+    if (host_cell_less(keyof(recs[mid]), key))
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo >= n || host_cell_less(key, keyof(recs[lo]))) return FL_FAILED_PRECONDITION;
+  *out = recs[lo].signed_distance;
+  return FL_OK;
+}
+
+const int32_t* center_key(const fl_center_sample& s) { return s.cell_index; }
+const int32_t* corner_key(const fl_corner_sample& s) { return s.corner_index; }
+
+template <typename R>
+bool samples_valid(const R* recs, uint64_t n, const int32_t* (*keyof)(const R&)) {
+  for (uint64_t i = 0; i < n; ++i)
+    if (!std::isfinite(recs[i].signed_distance) || (i > 0 && !host_cell_less(keyof(recs[i - 1]), keyof(recs[i]))))
+      return false;
+  return true;
+}
+
+bool fupload(fl_boundary* b, size_t off, size_t bytes);
+bool fdownload(fl_boundary* b, size_t off, size_t bytes);
+
+}  // namespace
+
+namespace {
+
+bool fupload(fl_boundary* b, size_t off, size_t bytes) {
+  if (bytes == 0) return true;
+  return cudaMemcpyAsync(b->fdev + off, b->fpin + off, bytes, cudaMemcpyHostToDevice, b->stream) == cudaSuccess;
+}
+
+bool fdownload(fl_boundary* b, size_t off, size_t bytes) {
+  if (bytes == 0) return true;
+  return cudaMemcpyAsync(b->fpin + off, b->fdev + off, bytes, cudaMemcpyDeviceToHost, b->stream) == cudaSuccess;
+}
+
+template <typename T>
+T* fhost(fl_boundary* b, size_t off) {
+  return reinterpret_cast<T*>(b->fpin + off);
+}
+template <typename T>
+T* fdevp(fl_boundary* b, size_t off) {
+  return reinterpret_cast<T*>(b->fdev + off);
+}
+
+// One device phase: uploads of the staged queries, the kernel, the results
+// back; adds its event time to *ms. False on a CUDA failure.
+template <typename Launch>
+bool freeze_phase(fl_boundary* b, size_t qoff, size_t qbytes, size_t roff, size_t rbytes, Launch launch, float* ms) {
+  bool ok = cudaEventRecord(b->e0, b->stream) == cudaSuccess && fupload(b, qoff, qbytes);
+  if (ok) launch();
+  ok = ok && cudaGetLastError() == cudaSuccess && fdownload(b, roff, rbytes) &&
+       fdownload(b, kFreezeRegions.arch, sizeof(int)) && cudaEventRecord(b->e1, b->stream) == cudaSuccess &&
+       cudaStreamSynchronize(b->stream) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    cudaStreamSynchronize(b->stream);
+    return false;
+  }
+  float t = 0.0f;
+  cudaEventElapsedTime(&t, b->e0, b->e1);
+  *ms += t;
+  return true;
+}
+
+// ValidateObstacle (liquid_boundary_geometry_3d.cc:132-175) for the kinds offered here.
+int check_obstacle(const fl_obstacle& o, FreezeObstacle* out) {
+  out->kind = o.kind;
+  out->coordinate = o.coordinate;
+  out->half_width = o.kind == FL_OBSTACLE_SLAB ? o.half_width : 0.0;
+  for (int a = 0; a < 3; ++a) out->n[a] = o.unit_normal[a];
+  if (o.kind == FL_OBSTACLE_NONE) return FL_OK;
+  if (o.kind != FL_OBSTACLE_HALFSPACE && o.kind != FL_OBSTACLE_SLAB) return FL_INVALID_ARGUMENT;
+  double low = o.coordinate, high = o.coordinate;
+  if (o.kind == FL_OBSTACLE_SLAB) {
+    if (!(std::isfinite(o.half_width) && o.half_width > 0)) return FL_INVALID_ARGUMENT;
+    low = o.coordinate - o.half_width;
+    high = o.coordinate + o.half_width;
+    if (!std::isfinite(o.coordinate)) return FL_INVALID_ARGUMENT;
+    if (!std::isfinite(low) || !std::isfinite(high) || low >= high) return FL_OUT_OF_RANGE;
+  }
+  const double* n = o.unit_normal;
+  const double* v = o.wall_velocity;
+  const bool finite_n = std::isfinite(n[0]) && std::isfinite(n[1]) && std::isfinite(n[2]);
+  const bool finite_v = std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]);
+  if (!finite_n || !finite_v || !std::isfinite(low) || std::fabs((n[0] * n[0] + n[1] * n[1] + n[2] * n[2]) - 1.0) > 1e-12)
+    return FL_INVALID_ARGUMENT;
+  return FL_OK;
+}
+
+}  // namespace
+
+extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl_frozen_cell* cells_out,
+                                  uint64_t* cell_count, fl_frozen_face* faces_out, uint64_t* face_count,
+                                  double* capillary_step_bound, fl_measurement* m) {
+  if (!b || !in || !cell_count || !face_count || !capillary_step_bound) return FL_INVALID_ARGUMENT;
+  int st = check_grid(in->grid);
+  if (st != FL_OK) return st;
+  const uint64_t n = in->cell_count;
+  if ((n && (!in->cell_indices || !cells_out || !faces_out)) || (in->center_count && !in->centers) ||
+      (in->corner_count && !in->corners))
+    return FL_INVALID_ARGUMENT;
+  // the bounded workspace's capacity (FreezeWithBackend, :2109-2113), then FreezeCore (:772-797)
+  if (n > (uint64_t)kMaxLinkCells || in->center_count > kMaxCenters) return FL_RESOURCE_EXHAUSTED;
+  if (!positive_finite_h(in->step_duration) || !positive_finite_h(in->liquid_density) ||
+      !std::isfinite(in->surface_tension) || in->surface_tension < 0)
+    return FL_INVALID_ARGUMENT;
+  if (in->has_exact_curvature && !std::isfinite(in->exact_curvature)) return FL_INVALID_ARGUMENT;
+  FreezeObstacle ob;
+  st = check_obstacle(in->obstacle, &ob);
+  if (st != FL_OK) return st;
+  const fl_owned_grid* g = in->grid;
+  const double h = g->h, full_area = h * h, full_volume = full_area * h;
+  if (!std::isnormal(full_area) || !std::isnormal(full_volume) || !std::isnormal(1 / in->liquid_density))
+    return FL_OUT_OF_RANGE;
+  if (!samples_valid(in->centers, in->center_count, center_key) ||
+      !samples_valid(in->corners, in->corner_count, corner_key))
+    return FL_INVALID_ARGUMENT;
+  if (cudaSetDevice(b->device) != cudaSuccess) return FL_INTERNAL;
+  const FreezeRegions& R = kFreezeRegions;
+  FreezeArgs a{};
+  for (int k = 0; k < 3; ++k) a.origin[k] = g->origin[k];
+  a.h = h;
+  a.obstacle = ob;
+  a.cq = fdevp<CellQuery>(b, R.cq);
+  a.cr = fdevp<CellResult>(b, R.cr);
+  a.fq = fdevp<FaceQuery>(b, R.fq);
+  a.fr = fdevp<FaceResult>(b, R.fr);
+  a.kq = fdevp<CurvatureQuery>(b, R.kq);
+  a.kr = fdevp<CurvatureResult>(b, R.kr);
+  a.density = in->liquid_density;
+  a.sigma = in->surface_tension;
+  a.capillary = fdevp<double>(b, R.cap);
+  a.arch = fdevp<int>(b, R.arch);
+  float ms = 0.0f;
+  auto finish_measure = [&]() {
+    if (m) {
+      m->compiled_architecture = *fhost<int>(b, R.arch);
+      m->kernel_ms = ms;
+    }
+  };
+
+  // Cells: stage until the first staging failure, compute the staged prefix,
+  // then consume it in order (stage, compute and consume errors of one
+  // ordinal come before those of the next).
+  CellQuery* cq = fhost<CellQuery>(b, R.cq);
+  std::unique_ptr<double[]> centre(new double[n ? n : 1]);
+  uint64_t staged = 0;
+  int stage_error = FL_OK;
+  for (; staged < n; ++staged) {
+    const int32_t* idx = in->cell_indices + 3 * staged;
+    if (staged > 0 && !host_cell_less(in->cell_indices + 3 * (staged - 1), idx)) {
+      stage_error = FL_INVALID_ARGUMENT;
+      break;
+    }
+    stage_error = lookup_distance(in->centers, in->center_count, idx, center_key, &centre[staged]);
+    if (stage_error != FL_OK) break;
+    CellQuery& q = cq[staged];
+    for (int d = 0; d < 3; ++d) q.index[d] = idx[d];
+    q.pad = 0;
+    for (int c = 0; c < 8 && stage_error == FL_OK; ++c) {
+      int32_t ci[3] = {idx[0], idx[1], idx[2]};
+      for (int axis = 0; axis < 3 && stage_error == FL_OK; ++axis)
+        stage_error = offset_cell(ci, axis, (c >> axis) & 1, ci);
+      if (stage_error == FL_OK)
+        stage_error = lookup_distance(in->corners, in->corner_count, ci, corner_key, &q.corner[c]);
+    }
+    if (stage_error != FL_OK) break;
+  }
+  uint64_t kept = 0, nfaces = 0;
+  if (staged > 0) {
+    a.ncell = (int)staged;
+    if (!freeze_phase(
+            b, R.cq, sizeof(CellQuery) * staged, R.cr, sizeof(CellResult) * staged,
+            [&]() {
+              ++g_kernel_launches;
+              k_freeze_cells<<<grid_of(staged, 64), 64, 0, b->stream>>>(a);
+            },
+            &ms))
+      return FL_INTERNAL;
+  }
+  const CellResult* cr = fhost<CellResult>(b, R.cr);
+  for (uint64_t i = 0; i < staged; ++i) {
+    if (cr[i].status != FL_OK) return cr[i].status;
+    const double low = cr[i].low, high = cr[i].high, dc = centre[i];
+    if (low > 0 && high > 0 && dc < 0) return FL_FAILED_PRECONDITION;
+    const double unclamped = low + high;
+    if (!std::isfinite(unclamped) || unclamped < 0 || unclamped / full_volume > 1 + 64 * DBL_EPSILON)
+      return FL_OUT_OF_RANGE;
+    const double volume = std::min(full_volume, unclamped);
+    if (!(volume == 0.0 || std::isnormal(volume))) return FL_OUT_OF_RANGE;
+    if (dc >= 0 || volume == 0) continue;
+    fl_frozen_cell& c = cells_out[kept++];
+    std::memset(&c, 0, sizeof(c));
+    for (int d = 0; d < 3; ++d) c.cell_index[d] = in->cell_indices[3 * i + d];
+    c.fluid_volume = volume;
+    c.center_distance = dc;
+    c.curvature = 0.0;
+    for (int axis = 0; axis < 3; ++axis)
+      for (int side = 0; side < 2; ++side) {
+        int32_t lat[3];
+        st = offset_cell(c.cell_index, axis, side, lat);
+        if (st != FL_OK) return st;
+        const int64_t lat64[3] = {lat[0], lat[1], lat[2]};
+        uint64_t slot = 0;
+        st = host_face_slot(g, axis, lat64, &slot);
+        if (st != FL_OK) return st;
+        fl_frozen_face& f = faces_out[nfaces++];
+        std::memset(&f, 0, sizeof(f));
+        f.axis = axis;
+        for (int d = 0; d < 3; ++d) f.lattice[d] = lat[d];
+        f.face_slot = slot;
+      }
+  }
+  if (stage_error != FL_OK) return stage_error;
+  // faces by owned slot, one record per slot
+  std::stable_sort(faces_out, faces_out + nfaces,
+                   [](const fl_frozen_face& x, const fl_frozen_face& y) { return x.face_slot < y.face_slot; });
+  nfaces = (uint64_t)(std::unique(faces_out, faces_out + nfaces,
+                                  [](const fl_frozen_face& x, const fl_frozen_face& y) {
+                                    return x.face_slot == y.face_slot;
+                                  }) -
+                      faces_out);
+  if (nfaces > (uint64_t)kMaxFaces) return FL_RESOURCE_EXHAUSTED;
+  if (nfaces > 0) {
+    FaceQuery* fq = fhost<FaceQuery>(b, R.fq);
+    for (uint64_t f = 0; f < nfaces; ++f) {
+      fq[f].axis = faces_out[f].axis;
+      for (int d = 0; d < 3; ++d) fq[f].lattice[d] = faces_out[f].lattice[d];
+    }
+    a.nface = (int)nfaces;
+    if (!freeze_phase(
+            b, R.fq, sizeof(FaceQuery) * nfaces, R.fr, sizeof(FaceResult) * nfaces,
+            [&]() {
+              ++g_kernel_launches;
+              k_freeze_faces<<<grid_of(nfaces, 128), 128, 0, b->stream>>>(a);
+            },
+            &ms))
+      return FL_INTERNAL;
+    const FaceResult* fr = fhost<FaceResult>(b, R.fr);
+    for (uint64_t f = 0; f < nfaces; ++f) {
+      if (fr[f].status != FL_OK) return fr[f].status;
+      faces_out[f].open_area = fr[f].open;
+      faces_out[f].blocked_area = fr[f].blocked;
+      faces_out[f].wall_normal_velocity = in->obstacle.kind == FL_OBSTACLE_NONE ? 0.0
+                                                                               : in->obstacle.wall_velocity[faces_out[f].axis];
+    }
+  }
+  // Interface cells (:983-1009): a kept cell with an open face toward an air centre.
+  std::unique_ptr<uint8_t[]> needs(new uint8_t[kept ? kept : 1]());
+  for (uint64_t f = 0; f < nfaces; ++f) {
+    const fl_frozen_face& face = faces_out[f];
+    if (face.open_area == 0 || in->surface_tension == 0) continue;
+    const int32_t head[3] = {face.lattice[0], face.lattice[1], face.lattice[2]};
+    int32_t tail[3];
+    st = offset_cell(head, face.axis, -1, tail);
+    if (st != FL_OK) return st;
+    const long long hc = host_find_cell(cells_out, kept, head), tc = host_find_cell(cells_out, kept, tail);
+    if (hc >= 0 && tc >= 0) continue;
+    double air = 0.0;
+    st = lookup_distance(in->centers, in->center_count, hc >= 0 ? tail : head, center_key, &air);
+    if (st != FL_OK) return st;
+    if (air >= 0) needs[hc >= 0 ? hc : tc] = 1;
+  }
+  bool capillary = false;
+  for (uint64_t i = 0; i < kept; ++i) capillary = capillary || needs[i];
+  if (in->has_exact_curvature) {
+    if (capillary && in->exact_curvature != 0) {
+      const double lift = in->surface_tension * in->exact_curvature;
+      if (!std::isnormal(lift)) return FL_OUT_OF_RANGE;
+    }
+    for (uint64_t i = 0; i < kept; ++i)
+      if (needs[i]) cells_out[i].curvature = in->exact_curvature;
+  } else if (capillary) {
+    // StageCenteredCurvature (:177-215): the 19 centre samples of the
+    // derivative stencil, in z, y, x order; staging stops at its first failure.
+    CurvatureQuery* kq = fhost<CurvatureQuery>(b, R.kq);
+    std::unique_ptr<uint64_t[]> ordinal(new uint64_t[kept]);
+    uint64_t nk = 0;
+    int kstage = FL_OK;
+    for (uint64_t i = 0; i < kept && kstage == FL_OK; ++i) {
+      if (!needs[i]) continue;
+      CurvatureQuery& q = kq[nk];
+      for (int k = 0; k < 27; ++k) q.d[k] = 0.0;
+      for (int z = -1; z <= 1 && kstage == FL_OK; ++z)
+        for (int y = -1; y <= 1 && kstage == FL_OK; ++y)
+          for (int x = -1; x <= 1 && kstage == FL_OK; ++x) {
+            if (x != 0 && y != 0 && z != 0) continue;
+            int32_t idx[3] = {cells_out[i].cell_index[0], cells_out[i].cell_index[1], cells_out[i].cell_index[2]};
+            const int off[3] = {x, y, z};
+            for (int axis = 0; axis < 3 && kstage == FL_OK; ++axis) kstage = offset_cell(idx, axis, off[axis], idx);
+            if (kstage == FL_OK)
+              kstage = lookup_distance(in->centers, in->center_count, idx, center_key,
+                                       &q.d[(z + 1) * 9 + (y + 1) * 3 + x + 1]);
+          }
+      if (kstage == FL_OK) ordinal[nk++] = i;
+    }
+    if (nk > 0) {
+      a.ncurv = (int)nk;
+      if (!freeze_phase(
+              b, R.kq, sizeof(CurvatureQuery) * nk, R.kr, sizeof(CurvatureResult) * nk,
+              [&]() {
+                ++g_kernel_launches;
+                k_freeze_curvature<<<grid_of(nk, 64), 64, 0, b->stream>>>(a);
+              },
+              &ms))
+        return FL_INTERNAL;
+      const CurvatureResult* kr = fhost<CurvatureResult>(b, R.kr);
+      for (uint64_t k = 0; k < nk; ++k) {
+        if (kr[k].status != FL_OK) return kr[k].status;
+        cells_out[ordinal[k]].curvature = kr[k].curvature;
+      }
+    }
+    if (kstage != FL_OK) return kstage;
+  }
+  double bound = std::numeric_limits<double>::infinity();
+  if (capillary) {
+    if (!freeze_phase(
+            b, R.cap, 0, R.cap, 2 * sizeof(double),
+            [&]() {
+              ++g_kernel_launches;
+              k_freeze_capillary<<<1, 1, 0, b->stream>>>(a);
+            },
+            &ms))
+      return FL_INTERNAL;
+    const double* cap = fhost<double>(b, R.cap);
+    if ((int)cap[1] != FL_OK) return (int)cap[1];
+    bound = cap[0];
+    if (in->step_duration > bound) return FL_FAILED_PRECONDITION;
+  }
+  *cell_count = kept;
+  *face_count = nfaces;
+  *capillary_step_bound = bound;
+  finish_measure();
   return FL_OK;
 }

@@ -723,6 +723,58 @@ typedef struct {
   uint8_t pad[3];
 } fl_pressure_link;
 
+/* ---- geometry freeze (.freeze) ----
+ * FreezeLiquidBoundaryGeometry3D (native/src/liquid_boundary_workspace_3d.cc:
+ * 186 -> liquid_boundary_geometry_3d.cc:2109-2143 and FreezeCore :765-1075,
+ * with the geometry queries of base/liquid_boundary_geometry_math_3d.h:
+ * 657-847): each candidate cell's liquid volume from its eight corner
+ * distances (six diagonal tetrahedra clipped by the interpolated liquid
+ * plane and by the obstacle's planes), the kept cells' faces with their open
+ * and blocked areas, the outward curvature of interface cells (exact, or from
+ * the centred second differences of the centre distances) and the capillary
+ * step bound. Obstacles: none, a translating halfspace or a translating slab;
+ * open tanks and sampled solids are not offered here. The host stages the
+ * sample lookups and keeps the reference's error order; the device computes
+ * every volume, area, curvature and bound. */
+typedef struct {
+  int32_t corner_index[3]; /* the lattice corner at the cell's low corner */
+  int32_t pad;
+  double signed_distance; /* m, negative in the liquid */
+} fl_corner_sample;
+#define FL_OBSTACLE_NONE 0
+#define FL_OBSTACLE_HALFSPACE 1
+#define FL_OBSTACLE_SLAB 2
+typedef struct {
+  int32_t kind; /* FL_OBSTACLE_* */
+  int32_t pad;
+  double unit_normal[3];
+  double coordinate;       /* halfspace: start plane coordinate; slab: start centre coordinate (m) */
+  double half_width;       /* slab only (m) */
+  double wall_velocity[3]; /* m/s */
+} fl_obstacle;
+typedef struct {
+  const fl_owned_grid* grid;
+  const int32_t* cell_indices; /* 3 per candidate, strictly increasing (z,y,x), <= 4096 */
+  uint64_t cell_count;
+  const fl_center_sample* centers; /* strictly increasing (z,y,x) */
+  uint64_t center_count;
+  const fl_corner_sample* corners; /* strictly increasing (z,y,x) */
+  uint64_t corner_count;
+  fl_obstacle obstacle;
+  double step_duration;   /* s */
+  double liquid_density;  /* kg/m^3 */
+  double surface_tension; /* N/m */
+  double exact_curvature; /* 1/m, when has_exact_curvature */
+  uint8_t has_exact_curvature;
+  uint8_t pad[7];
+} fl_freeze_inputs;
+/* cells: room for cell_count records, faces: room for 6 * cell_count; both
+ * in frozen order (cells by (z,y,x), faces by owned slot). The capillary
+ * bound is +inf without a capillary interface. */
+int fl_boundary_freeze(fl_boundary* boundary, const fl_freeze_inputs* inputs, fl_frozen_cell* cells,
+                       uint64_t* cell_count, fl_frozen_face* faces, uint64_t* face_count,
+                       double* capillary_step_bound, fl_measurement* measurement);
+
 int fl_boundary_links(fl_boundary* boundary, const fl_frozen_geometry* geometry, const fl_pressure_fields* fields,
                       fl_pressure_cell* cells, fl_pressure_link* faces, uint64_t* lower_theta_regularization_count,
                       fl_measurement* measurement);

@@ -373,8 +373,70 @@ int bk_links(int which, const double origin[3], double h, const int32_t* blocks,
   return 0;
 }
 
+// .freeze on candidate cells with centre and corner samples (x,y,z; d),
+// obstacle kind 0 none / 1 halfspace / 2 slab (normal, coordinate, half
+// width, wall velocity) and the exact curvature (NaN for none). Outputs: cells
+// (x,y,z) + (volume, centre distance, curvature), faces (axis,x,y,z) + slot +
+// (open, blocked, wall velocity), the counts and the capillary bound.
+int bk_freeze(int which, const double origin[3], double h, const int32_t* blocks, uint64_t nb,
+              const int32_t* cell_index, uint64_t n, const int32_t* center_index, const double* center_distance,
+              uint64_t ncenters, const int32_t* corner_index, const double* corner_distance, uint64_t ncorners,
+              int obstacle_kind, const double normal[3], double coordinate, double half_width,
+              const double velocity[3], double step_duration, double density, double sigma, double exact_curvature,
+              int32_t* cells_index_out, double* cells_out, uint64_t* ncells_out, int32_t* faces_index_out,
+              uint64_t* faces_slot_out, double* faces_out, uint64_t* nfaces_out, double* capillary_bound) {
+  int code = 0;
+  const auto* table = Table(which, &code);
+  if (!table) return code;
+  auto grid = Grid(origin, h, blocks, nb);
+  if (!grid.ok()) return Code(grid.status());
+  auto ws = Workspace();
+  if (!ws.ok()) return Code(ws.status());
+  std::vector<CellIndex3D> cells(n);
+  for (uint64_t i = 0; i < n; ++i) cells[i] = {cell_index[3 * i], cell_index[3 * i + 1], cell_index[3 * i + 2]};
+  std::vector<LiquidCenterDistance3D> centers(ncenters);
+  for (uint64_t i = 0; i < ncenters; ++i)
+    centers[i] = {{center_index[3 * i], center_index[3 * i + 1], center_index[3 * i + 2]}, center_distance[i]};
+  std::vector<LiquidCornerDistance3D> corners(ncorners);
+  for (uint64_t i = 0; i < ncorners; ++i)
+    corners[i] = {{corner_index[3 * i], corner_index[3 * i + 1], corner_index[3 * i + 2]}, corner_distance[i]};
+  LiquidObstacle3D obstacle{};
+  const Vec3 nrm{normal[0], normal[1], normal[2]}, vel{velocity[0], velocity[1], velocity[2]};
+  if (obstacle_kind == 1) obstacle = TranslatingHalfspace3D{nrm, coordinate, vel};
+  if (obstacle_kind == 2) obstacle = TranslatingSlab3D{nrm, coordinate, half_width, vel};
+  LiquidBoundaryGeometryViewInputs3D in{grid->view(), cells, centers, corners, obstacle, step_duration, density,
+                                        sigma};
+  if (exact_curvature == exact_curvature) in.exact_outward_interface_curvature = exact_curvature;
+  auto r = table->freeze(table->context, in, *ws);
+  if (!r.ok()) return Code(r.status());
+  *ncells_out = r->cells.size();
+  for (std::size_t i = 0; i < r->cells.size(); ++i) {
+    const auto& c = r->cells[i];
+    cells_index_out[3 * i] = c.cell_index.x;
+    cells_index_out[3 * i + 1] = c.cell_index.y;
+    cells_index_out[3 * i + 2] = c.cell_index.z;
+    cells_out[3 * i] = c.fluid_volume;
+    cells_out[3 * i + 1] = c.center_distance;
+    cells_out[3 * i + 2] = c.curvature;
+  }
+  *nfaces_out = r->faces.size();
+  for (std::size_t f = 0; f < r->faces.size(); ++f) {
+    const auto& face = r->faces[f];
+    faces_index_out[4 * f] = static_cast<int32_t>(face.face_index.axis);
+    faces_index_out[4 * f + 1] = face.face_index.lattice_index.x;
+    faces_index_out[4 * f + 2] = face.face_index.lattice_index.y;
+    faces_index_out[4 * f + 3] = face.face_index.lattice_index.z;
+    faces_slot_out[f] = face.face_slot;
+    faces_out[3 * f] = face.open_area;
+    faces_out[3 * f + 1] = face.blocked_area;
+    faces_out[3 * f + 2] = face.wall_normal_velocity;
+  }
+  *capillary_bound = r->capillary_step_bound;
+  return 0;
+}
+
 // Which operations each table fills (bit k: deposit, normalize, predict,
-// forces, gather, project, topology, update_particles, links).
+// forces, gather, project, topology, update_particles, links, freeze).
 int bk_filled(int which, uint32_t* mask) {
   int code = 0;
   const auto* table = Table(which, &code);
@@ -387,9 +449,10 @@ int bk_filled(int which, uint32_t* mask) {
                        reinterpret_cast<const void*>(table->project),
                        reinterpret_cast<const void*>(table->topology),
                        reinterpret_cast<const void*>(table->update_particles),
-                       reinterpret_cast<const void*>(table->links)};
+                       reinterpret_cast<const void*>(table->links),
+                       reinterpret_cast<const void*>(table->freeze)};
   *mask = 0;
-  for (int k = 0; k < 9; ++k)
+  for (int k = 0; k < 10; ++k)
     if (ops[k]) *mask |= 1u << k;
   return 0;
 }

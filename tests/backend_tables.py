@@ -335,3 +335,72 @@ def links(which, s: LinkScene, **override):
         _p(c(a["itf_ordinal"], np.uint64)), _p(c(a["itf_values"], np.float64)), ctypes.c_uint64(len(a["itf_ordinal"])),
         _p(cells_out), _p(faces_out), ctypes.byref(lower))
     return code, cells_out, faces_out, lower.value
+
+
+class FreezeScene:
+    """Candidate cells of a 12 x 9 x 12-cell region (x, z in [0, 12), y in
+    [0, 9): 1296 candidates) holding a wobbly drop: the signed distance, in
+    cells, is |p - (6, 4.5, 6)| - 3.7 - 0.25 sin(2x/3) cos(z/2), times h,
+    sampled at every cell centre within one of the region and at every lattice
+    corner of the candidates. The region's outer cells are air, so every face
+    of a liquid cell opens onto a liquid or an air cell. Obstacles: none, a
+    translating halfspace whose plane cuts the drop's low-x, low-z side, or a
+    translating slab 2.4 h thick across it (thicker than a cell's diagonal, so
+    no cell holds liquid on both of its sides). Active 4^3 blocks: x, z in
+    [-1, 3], y in [-1, 2]."""
+
+    def __init__(self, obstacle: str = "none", sigma: float = 0.072, exact_curvature: float = float("nan")):
+        n, ny = 12, 9
+        bz, by, bx = np.meshgrid(np.arange(-1, 4), np.arange(-1, 3), np.arange(-1, 4), indexing="ij")
+        self.blocks = np.stack([bx.ravel(), by.ravel(), bz.ravel()], 1).astype(np.int32)
+
+        def distance(p):
+            r = np.sqrt((p[:, 0] - 6.0) ** 2 + (p[:, 1] - 4.5) ** 2 + (p[:, 2] - 6.0) ** 2)
+            return (r - 3.7 - 0.25 * np.sin(p[:, 0] / 1.5) * np.cos(p[:, 2] / 2.0)) * H
+
+        cz, cy, cx = np.meshgrid(np.arange(n), np.arange(ny), np.arange(n), indexing="ij")
+        self.cell_index = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], 1).astype(np.int32)
+        ez, ey, ex = np.meshgrid(np.arange(-1, n + 1), np.arange(-1, ny + 1), np.arange(-1, n + 1), indexing="ij")
+        self.center_index = np.stack([ex.ravel(), ey.ravel(), ez.ravel()], 1).astype(np.int32)
+        self.center_distance = distance(self.center_index + 0.5)
+        kz, ky, kx = np.meshgrid(np.arange(n + 1), np.arange(ny + 1), np.arange(n + 1), indexing="ij")
+        self.corner_index = np.stack([kx.ravel(), ky.ravel(), kz.ravel()], 1).astype(np.int32)
+        self.corner_distance = distance(self.corner_index.astype(np.float64))
+        self.kind, self.normal, self.coordinate, self.half_width = 0, (0.0, 0.0, 0.0), 0.0, 0.0
+        self.velocity = (0.0, 0.0, 0.0)
+        if obstacle == "halfspace":  # solid where n . x <= c
+            self.kind, self.normal, self.coordinate = 1, (0.8, 0.0, 0.6), 5.3 * H
+            self.velocity = (0.05, 0.0, -0.02)
+        elif obstacle == "slab":
+            self.kind, self.normal, self.coordinate, self.half_width = 2, (0.6, 0.0, 0.8), 8.1 * H, 1.2 * H
+            self.velocity = (0.0, 0.0, 0.1)
+        self.step_duration, self.density, self.sigma = DT, 1000.0, sigma
+        self.exact_curvature = exact_curvature
+
+
+def freeze(which, s: FreezeScene, **override):
+    """The table's .freeze on the scene: (code, cell indices, cell values
+    (volume, centre distance, curvature), face indices (axis, x, y, z), face
+    slots, face values (open, blocked, wall velocity), capillary bound)."""
+    a = dict(s.__dict__)
+    a.update(override)
+    n = len(a["cell_index"])
+    ci = np.zeros((n, 3), np.int32)
+    cv = np.zeros((n, 3))
+    fi = np.zeros((6 * n, 4), np.int32)
+    fs = np.zeros(6 * n, np.uint64)
+    fv = np.zeros((6 * n, 3))
+    nc, nf, bound = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_double(0.0)
+    c = lambda x, t: np.ascontiguousarray(x, t)  # noqa: E731
+    code = lib().bk_freeze(
+        ctypes.c_int(which), _d3((0, 0, 0)), ctypes.c_double(H), _p(c(a["blocks"], np.int32)),
+        ctypes.c_uint64(len(a["blocks"])), _p(c(a["cell_index"], np.int32)), ctypes.c_uint64(n),
+        _p(c(a["center_index"], np.int32)), _p(c(a["center_distance"], np.float64)),
+        ctypes.c_uint64(len(a["center_index"])), _p(c(a["corner_index"], np.int32)),
+        _p(c(a["corner_distance"], np.float64)), ctypes.c_uint64(len(a["corner_index"])), ctypes.c_int(a["kind"]),
+        _d3(a["normal"]), ctypes.c_double(a["coordinate"]), ctypes.c_double(a["half_width"]), _d3(a["velocity"]),
+        ctypes.c_double(a["step_duration"]), ctypes.c_double(a["density"]), ctypes.c_double(a["sigma"]),
+        ctypes.c_double(a["exact_curvature"]), _p(ci), _p(cv), ctypes.byref(nc), _p(fi), _p(fs), _p(fv),
+        ctypes.byref(nf), ctypes.byref(bound))
+    k, m = nc.value, nf.value
+    return code, ci[:k], cv[:k], fi[:m], fs[:m], fv[:m], bound.value

@@ -79,11 +79,11 @@ def histories(one_sided):
 
 def test_tables_fill_the_transfer_and_projection_operations():
     code, cpu = bt.filled(CPU)
-    assert code == 0 and cpu == 0x1FF
+    assert code == 0 and cpu == 0x3FF
     code, b200 = bt.filled(B200)
     assert code == 0
-    # deposit, normalize, predict, forces, gather, project and links; no topology or particle update
-    assert b200 == 0x13F
+    # deposit, normalize, predict, forces, gather, project, links and freeze; no topology or particle update
+    assert b200 == 0x33F
 
 
 def test_deposit_is_bit_identical(scene, deposited):
@@ -271,3 +271,88 @@ def test_links_error_codes_match():
     wet = np.full(nf, np.nan)
     wet[3] = 1e-6
     assert both(wetted=wet) == 3
+
+
+def _assert_frozen_equal(cpu, gpu):
+    code0, ci0, cv0, fi0, fs0, fv0, bound0 = cpu
+    code1, ci1, cv1, fi1, fs1, fv1, bound1 = gpu
+    assert code0 == 0 and code1 == 0
+    assert np.array_equal(ci1, ci0)  # the kept cells
+    assert np.array_equal(cv1[:, :2], cv0[:, :2])  # liquid volumes and centre distances, bitwise
+    assert np.array_equal(cv1[:, 2], cv0[:, 2])  # curvature, bitwise
+    assert np.array_equal(fi1, fi0) and np.array_equal(fs1, fs0)
+    assert np.array_equal(fv1, fv0)  # open and blocked areas, wall velocities
+    assert bound1 == bound0
+
+
+@pytest.mark.parametrize("obstacle", ["none", "halfspace", "slab"])
+def test_freeze_is_bit_identical(obstacle):
+    s = bt.FreezeScene(obstacle)
+    cpu, gpu = bt.freeze(CPU, s), bt.freeze(B200, s)
+    _assert_frozen_equal(cpu, gpu)
+    _, _, cv, _, _, fv, bound = cpu
+    vol = cv[:, 0] / bt.H ** 3
+    assert (vol < 0.99).sum() > 50 and (vol > 1 - 1e-12).sum() > 10  # cut and whole liquid cells
+    assert (cv[:, 2] != 0).sum() > 50 and np.isfinite(bound)  # interface cells with curvature
+    if obstacle != "none":
+        assert ((fv[:, 0] > 0) & (fv[:, 0] < bt.H ** 2)).sum() > 10  # partly blocked faces
+
+
+def test_freeze_with_exact_curvature_and_without_surface_tension():
+    _assert_frozen_equal(bt.freeze(CPU, bt.FreezeScene(exact_curvature=1.5)),
+                         bt.freeze(B200, bt.FreezeScene(exact_curvature=1.5)))
+    cpu = bt.freeze(CPU, bt.FreezeScene(sigma=0.0))
+    _assert_frozen_equal(cpu, bt.freeze(B200, bt.FreezeScene(sigma=0.0)))
+    assert np.all(cpu[2][:, 2] == 0) and cpu[6] == np.inf
+
+
+def test_freeze_error_codes_match():
+    s = bt.FreezeScene("halfspace")
+
+    def both(**kw):
+        a, b = bt.freeze(CPU, s, **kw)[0], bt.freeze(B200, s, **kw)[0]
+        assert a == b, (kw.keys(), a, b)
+        return a
+
+    swapped = s.cell_index.copy()
+    swapped[[10, 11]] = swapped[[11, 10]]
+    assert both(cell_index=swapped) == 3
+    # a missing centre sample of a candidate (deep in the liquid) and of a curvature stencil
+    keep = ~np.all(s.center_index == (5, 1, 5), axis=1)
+    assert both(center_index=s.center_index[keep], center_distance=s.center_distance[keep]) == 9
+    keep = ~np.all(s.corner_index == (6, 2, 6), axis=1)
+    assert both(corner_index=s.corner_index[keep], corner_distance=s.corner_distance[keep]) == 9
+    assert both(normal=(0.8, 0.0, 0.61)) == 3  # not a unit normal
+    assert both(kind=2, half_width=0.0) == 3
+    assert both(density=0.0) == 3
+    assert both(step_duration=1.0) == 9  # above the capillary bound
+    bad = s.corner_distance.copy()
+    bad[3] = np.nan
+    assert both(corner_distance=bad) == 3
+    many = np.repeat(s.cell_index, 4, axis=0)[:4097]
+    assert both(cell_index=many) == 8
+
+
+def test_freeze_then_links_on_device_match_the_cpu_pipeline():
+    """The frozen view of each table feeds that table's own link assembly."""
+    s = bt.FreezeScene()
+    out = []
+    for which in (CPU, B200):
+        code, ci, cv, fi, fs, fv, _ = bt.freeze(which, s)
+        assert code == 0
+        nc, nf = len(ci), len(fi)
+        fields = np.zeros((nc, 4))
+        fields[:, 1] = np.inf
+        fields[:, 3] = np.nan
+        face_values = np.concatenate([fv, np.full((nf, 1), np.nan)], 1)
+        ls = dict(blocks=s.blocks, center_index=s.center_index, center_distance=s.center_distance, cell_index=ci,
+                  cell_values=cv, face_index=fi, face_slot=fs, face_values=face_values,
+                  piston=np.zeros(nf, np.uint8), step_duration=s.step_duration, density=s.density, sigma=s.sigma,
+                  fields=fields, predicted=np.linspace(-0.1, 0.1, nf), ambient=0.0, air_index=np.zeros((0, 3)),
+                  air_pressure=np.zeros(0), itf_ordinal=np.zeros(0, np.uint64), itf_values=np.zeros((0, 4)),
+                  wetted=None)
+        out.append(bt.links(which, bt.LinkScene(), **ls))
+    (c0, cells0, faces0, low0), (c1, cells1, faces1, low1) = out
+    assert c0 == 0 and c1 == 0
+    assert np.array_equal(cells1, cells0) and np.array_equal(faces1, faces0, equal_nan=True) and low1 == low0
+    assert (faces0[:, 0] == 2).sum() > 50  # free-surface links with their theta distances
