@@ -276,8 +276,7 @@ struct B200BackendOps3D {
     const std::size_t n = inputs.cell_indices.size();
     if (n > kPressureCells || inputs.center_distances.size() > 27 * kPressureCells)
       return Code(absl::StatusCode::kResourceExhausted);
-    if (inputs.sampled_solid || std::holds_alternative<AxisAlignedLiquidTank3D>(inputs.obstacle))
-      return Code(absl::StatusCode::kUnimplemented);
+    if (inputs.sampled_solid) return Code(absl::StatusCode::kUnimplemented);
     fl_freeze_inputs in{};
     const fl_owned_grid grid = OwnedGrid(inputs.mac_grid);
     in.grid = &grid;
@@ -295,6 +294,10 @@ struct B200BackendOps3D {
       in.obstacle = fl_obstacle{FL_OBSTACLE_SLAB, 0, {sl->unit_normal.x, sl->unit_normal.y, sl->unit_normal.z},
                                 sl->start_center_coordinate, sl->half_width,
                                 {sl->wall_velocity.x, sl->wall_velocity.y, sl->wall_velocity.z}};
+    } else if (const auto* tk = std::get_if<AxisAlignedLiquidTank3D>(&inputs.obstacle)) {
+      in.obstacle.kind = FL_OBSTACLE_OPEN_TANK;
+      const double t[6] = {tk->start_low_x, tk->high_x, tk->floor_y, tk->low_z, tk->high_z, tk->piston_velocity_x};
+      for (int k = 0; k < 6; ++k) in.obstacle.tank[k] = t[k];
     } else {
       in.obstacle.kind = FL_OBSTACLE_NONE;
     }

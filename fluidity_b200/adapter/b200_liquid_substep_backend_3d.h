@@ -12,7 +12,7 @@
 //   .forces                fl_boundary_forces         (the CPU table's ApplyForces)
 //   .gather                fl_boundary_gather         (GatherLiquidBoundaryParticles3D)
 //   .freeze                fl_boundary_freeze         (FreezeLiquidBoundaryGeometry3D: no obstacle,
-//                                                      halfspace or slab; open tanks and sampled
+//                                                      halfspace, slab or open tank; sampled
 //                                                      solids return kUnimplemented)
 //   .links                 fl_boundary_links          (BuildLiquidPressureLinks3D)
 //   .project               fl_boundary_project        (ProjectMacPressure3D over a pressure problem)

@@ -1814,10 +1814,14 @@ extern "C" int fl_boundary_links(fl_boundary* b, const fl_frozen_geometry* G, co
 namespace fl {
 namespace {
 
-constexpr int kPolyCap = 10;  // a tetrahedron face clipped twice has <= 5 vertices; a cap <= 2 per cut edge
-constexpr int kPolyhCap = 7;  // 4 faces + one cap per clip
-constexpr int kCutCap = 2 * kPolyhCap;
+// Clipping-list capacities. With at most two planes after the liquid plane
+// (halfspace, slab) a tetrahedron face stays within 5 vertices and a cap
+// within 2 per cut edge; with the five planes of an open tank a face takes up
+// to 9 vertices and the polyhedron up to 10 faces.
+constexpr int kPolyCap = 10, kPolyhCap = 7;
+constexpr int kTankPolyCap = 20, kTankPolyhCap = 10;
 constexpr double kNaN = __builtin_nan("");
+constexpr double kInf = __builtin_inf();
 
 struct ClipVertex {
   double p[3];  // position in cell widths
@@ -1826,6 +1830,7 @@ struct ClipVertex {
 
 template <int N>
 struct VertexList {
+  static constexpr int kCap = N;
   ClipVertex v[N];
   int n = 0;
   bool overflow = false;
@@ -1839,17 +1844,24 @@ struct VertexList {
 };
 using Polygon = VertexList<kPolyCap>;
 
-struct Polyhedron {
-  Polygon f[kPolyhCap];
+template <int V, int F>
+struct PolyhedronT {
+  static constexpr int kVerts = V, kFaces = F;
+  VertexList<V> f[F];
   int n = 0;
   bool overflow = false;
 };
+using Polyhedron = PolyhedronT<kPolyCap, kPolyhCap>;
+using TankPolyhedron = PolyhedronT<kTankPolyCap, kTankPolyhCap>;
 
-// A plane's clip distance: the liquid distance itself, or n . p - c.
+// A plane's clip distance: the liquid distance itself, or n . p - c. An
+// axis-aligned plane (snap >= 0) pins its cut points' coordinate on that axis
+// to the plane's own.
 struct ClipPlane {
   double n[3];
   double c;
   bool liquid;
+  int snap = -1;
 };
 
 __device__ __forceinline__ void cross3(const double* a, const double* b, double* o) {
@@ -1876,9 +1888,9 @@ __device__ __forceinline__ double clip_distance(const ClipVertex& v, const ClipP
 
 // Keeps the part with distance <= 0; each crossing gets an intersection whose
 // weights are formed from the distances scaled by their larger magnitude.
-template <int NO, int NI>
+template <int NO, int NI, int NC = 1>
 __device__ void clip_polygon(const VertexList<NI>& in, const ClipPlane& pl, VertexList<NO>& out,
-                             VertexList<kCutCap>* cuts) {
+                             VertexList<NC>* cuts = nullptr) {
   out.n = 0;
   out.overflow = false;
   if (in.overflow) {
@@ -1899,6 +1911,7 @@ __device__ void clip_polygon(const VertexList<NI>& in, const ClipPlane& pl, Vert
       ClipVertex x;
       for (int a = 0; a < 3; ++a) x.p[a] = prev.p[a] * wp + cur.p[a] * wc;
       x.d = wp * prev.d + wc * cur.d;
+      if (pl.snap >= 0) x.p[pl.snap] = pl.c * pl.n[pl.snap];
       out.push(x);
       if (cuts) cuts->push(x);
     }
@@ -1937,31 +1950,32 @@ struct Tetrahedron {
 
 // Clips every face of a convex polyhedron and closes it with the cap through
 // the distinct cut points, ordered by angle about their centroid.
-template <typename In>
-__device__ void clip_polyhedron(const In& in, const ClipPlane& pl, Polyhedron& out) {
+template <typename In, typename Out>
+__device__ void clip_polyhedron(const In& in, const ClipPlane& pl, Out& out) {
+  using Face = VertexList<Out::kVerts>;
   out.n = 0;
   out.overflow = false;
   if (in.overflow) {
     out.overflow = true;
     return;
   }
-  VertexList<kCutCap> cuts;
+  VertexList<2 * Out::kFaces> cuts;
   for (int k = 0; k < in.n; ++k) {
-    Polygon clipped;
+    Face clipped;
     clip_polygon(in.f[k], pl, clipped, &cuts);
     if (clipped.overflow || cuts.overflow) {
       out.overflow = true;
       return;
     }
     if (clipped.n >= 3) {
-      if (out.n == kPolyhCap) {
+      if (out.n == Out::kFaces) {
         out.overflow = true;
         return;
       }
       out.f[out.n++] = clipped;
     }
   }
-  Polygon cap;
+  Face cap;
   for (int k = 0; k < cuts.n; ++k) {
     bool seen = false;
     for (int j = 0; j < cap.n; ++j) seen = seen || same_position(cap.v[j], cuts.v[k]);
@@ -2011,7 +2025,7 @@ __device__ void clip_polyhedron(const In& in, const ClipPlane& pl, Polyhedron& o
     }
     cap.v[j] = v;
   }
-  if (out.n == kPolyhCap) {
+  if (out.n == Out::kFaces) {
     out.overflow = true;
     return;
   }
@@ -2045,7 +2059,8 @@ __device__ double physical_measure(double det, int exp, double h, int dim) {
 }
 
 // Volume as tetrahedra from the mean of all polygon vertices.
-__device__ double clipped_volume(const Polyhedron& ph, double h) {
+template <typename Ph>
+__device__ double clipped_volume(const Ph& ph, double h) {
   if (ph.overflow) return kNaN;
   double apex[3] = {0.0, 0.0, 0.0};
   int count = 0;
@@ -2061,7 +2076,7 @@ __device__ double clipped_volume(const Polyhedron& ph, double h) {
   for (int a = 0; a < 3; ++a) apex[a] = apex[a] * inv;
   double vol = 0.0;
   for (int k = 0; k < ph.n; ++k) {
-    const Polygon& pg = ph.f[k];
+    const auto& pg = ph.f[k];
     for (int j = 1; j + 1 < pg.n; ++j) {
       double e[3][3];
       for (int a = 0; a < 3; ++a) {
@@ -2111,7 +2126,7 @@ __device__ double open_face_area(const VertexList<N>& pg, const ClipPlane& pl, d
   for (int k = 0; k < pg.n; ++k) any = any || clip_distance(pg.v[k], pl) < 0.0;
   if (!any) return 0.0;
   Polygon c;
-  clip_polygon(pg, pl, c, nullptr);
+  clip_polygon(pg, pl, c);
   return clipped_area(c, h);
 }
 
@@ -2119,7 +2134,200 @@ struct FreezeObstacle {
   int kind;  // FL_OBSTACLE_*
   double n[3];
   double coordinate, half_width;
+  double tank[6];  // open tank: start low x, high x, floor y, low z, high z, piston velocity x
 };
+
+// ---- open tank (base/liquid_boundary_math.h:94-296 for the certified plane
+// offsets, base/liquid_boundary_geometry_math_3d.h:440-624 for the clipping) ----
+
+struct SumResidual {
+  double value, residual;
+};
+
+// FastTwoSum with the larger magnitude first.
+__device__ SumResidual add_with_residual(double a, double b) {
+  if (fabs(a) < fabs(b)) {
+    const double t = a;
+    a = b;
+    b = t;
+  }
+  const double s = a + b;
+  if (!isfinite(s)) return {s, 0.0};
+  return {s, b - (s - a)};
+}
+
+__device__ double add_down(double a, double b) {
+  const SumResidual s = add_with_residual(a, b);
+  return s.residual < 0 ? nextafter(s.value, -kInf) : s.value;
+}
+
+__device__ double add_up(double a, double b) {
+  const SumResidual s = add_with_residual(a, b);
+  return s.residual > 0 ? nextafter(s.value, kInf) : s.value;
+}
+
+// Midpoint without overflow, correctly rounded (the P0811 formulation).
+__device__ double midpoint(double a, double b) {
+  const double lo = DBL_MIN * 2, hi = DBL_MAX / 2;
+  const double aa = a < 0 ? -a : a, ab = b < 0 ? -b : b;
+  if (aa <= hi && ab <= hi) return (a + b) / 2;
+  if (aa < lo) return a + b / 2;
+  if (ab < lo) return a / 2 + b;
+  return a / 2 + b / 2;
+}
+
+struct OffsetBounds {
+  double estimate, lower, upper;
+};
+
+// A rounded sum with outward-rounded bounds on its accumulated residuals, so
+// the sign of a tank plane's offset from a lattice plane can be certified.
+struct CertifiedSum {
+  double sum = 0.0, lower = 0.0, upper = 0.0;
+  __device__ void correct(double c) {
+    if (!isfinite(lower) || !isfinite(upper)) {
+      sum = kInf;
+      return;
+    }
+    lower = add_down(lower, c);
+    upper = add_up(upper, c);
+  }
+  __device__ void add(double term) {
+    if (!isfinite(sum) || !isfinite(term)) {
+      sum = kInf;
+      return;
+    }
+    const SumResidual s = add_with_residual(sum, term);
+    sum = s.value;
+    correct(s.residual);
+  }
+  __device__ void add_product(double l, double r) {
+    const double product = l * r;
+    add(product);
+    if (isfinite(product) && l != 0 && r != 0 && fabs(l) != 1 && fabs(r) != 1) {
+      correct(fma(l, r, -product));
+      if (fabs(product) <= 0x1p-969) {
+        const double tiny = 4.9406564584124654e-324;  // the smallest subnormal
+        lower = add_down(lower, -tiny);
+        upper = add_up(upper, tiny);
+      }
+    }
+  }
+  __device__ OffsetBounds bounds() const {
+    if (!isfinite(sum) || !isfinite(lower) || !isfinite(upper)) return {kInf, kInf, kInf};
+    return {sum + midpoint(lower, upper), add_down(sum, lower), add_up(sum, upper)};
+  }
+};
+
+constexpr int kSignUnresolved = 2;
+
+__device__ int certified_sign(const OffsetBounds& b) {
+  if (!isfinite(b.estimate) || !isfinite(b.lower) || !isfinite(b.upper)) return kSignUnresolved;
+  if (b.lower > 0) return 1;
+  if (b.upper < 0) return -1;
+  if (b.lower == 0 && b.upper == 0) return 0;
+  return kSignUnresolved;
+}
+
+// world - (origin + h * index), exactly enough to certify its sign.
+__device__ CertifiedSum tank_plane_offset(double world, double origin, double index, double h) {
+  CertifiedSum o;
+  o.add(world);
+  o.add(-origin);
+  o.add_product(-h, index);
+  return o;
+}
+
+__device__ int tank_plane_sign(double world, double origin, double index, double h, int* sign) {
+  const double translated = world - origin;
+  if (isinf(translated)) {
+    *sign = translated > 0 ? 1 : -1;
+    return FL_OK;
+  }
+  *sign = certified_sign(tank_plane_offset(world, origin, index, h).bounds());
+  return *sign == kSignUnresolved ? FL_OUT_OF_RANGE : FL_OK;
+}
+
+// The plane's coordinate in the cell's unit frame: 0 at or below the low
+// face, 1 at or beyond the high face, else the interior cut.
+__device__ int tank_clip_coordinate(double world, double origin, double index, double h, double* out) {
+  const double translated = world - origin;
+  if (isinf(translated)) {
+    *out = translated > 0 ? 1.0 : 0.0;
+    return FL_OK;
+  }
+  CertifiedSum o = tank_plane_offset(world, origin, index, h);
+  const OffsetBounds low = o.bounds();
+  const int low_side = certified_sign(low);
+  if (low_side == kSignUnresolved) return FL_OUT_OF_RANGE;
+  if (low_side <= 0) {
+    *out = 0.0;
+    return FL_OK;
+  }
+  o.add(-h);
+  const int high_side = certified_sign(o.bounds());
+  if (high_side == kSignUnresolved) return FL_OUT_OF_RANGE;
+  if (high_side >= 0) {
+    *out = 1.0;
+    return FL_OK;
+  }
+  const double c = low.estimate / h;
+  if (c <= 0 || c >= 1) return FL_OUT_OF_RANGE;
+  *out = c;
+  return FL_OK;
+}
+
+struct TankBounds {
+  double low[3] = {0.0, 0.0, 0.0};
+  double high[3] = {1.0, 1.0, 1.0};
+};
+
+// The tank's clip box in the unit frame of the queried cell or face (a face
+// skips its normal axis).
+__device__ int local_tank_bounds(const FreezeObstacle& ob, const double origin[3], double h, const int32_t idx[3],
+                                 int skip_axis, TankBounds& tb) {
+  const double lw[3] = {ob.tank[0], ob.tank[2], ob.tank[3]};
+  const double hw[3] = {ob.tank[1], kInf, ob.tank[4]};
+  for (int a = 0; a < 3; ++a) {
+    if (a == skip_axis) continue;
+    double lo = 0.0, hi = 0.0;
+    if (tank_clip_coordinate(lw[a], origin[a], (double)idx[a], h, &lo) != FL_OK ||
+        tank_clip_coordinate(hw[a], origin[a], (double)idx[a], h, &hi) != FL_OK)
+      return FL_OUT_OF_RANGE;
+    tb.low[a] = lo;
+    tb.high[a] = hi;
+    if (lo == hi && lo > 0 && hi < 1) return FL_OUT_OF_RANGE;
+  }
+  return FL_OK;
+}
+
+// Product of the box's extents (one axis excluded for a face), scaled by
+// powers of two before the multiply.
+__device__ double tank_box_measure(const TankBounds& tb, double h, int excluded) {
+  double mantissa = 1.0;
+  int exponent = 0, dim = 0;
+  for (int a = 0; a < 3; ++a) {
+    if (a == excluded) continue;
+    const double extent = tb.high[a] - tb.low[a];
+    if (extent <= 0) return 0.0;
+    int e = 0;
+    mantissa *= frexp(extent, &e);
+    exponent += e;
+    ++dim;
+  }
+  return physical_measure(mantissa, exponent, h, dim);
+}
+
+// Both ends of each cell edge resolvable in world coordinates.
+__device__ bool tank_cell_resolved(const double origin[3], double h, const int32_t idx[3]) {
+  for (int a = 0; a < 3; ++a) {
+    const double low = origin[a] + h * (double)idx[a];
+    const double high = origin[a] + h * ((double)idx[a] + 1);
+    if (!isfinite(low) || !isfinite(high) || low >= high) return false;
+    if (nextafter(low, high) - low > h || high - nextafter(high, low) > h) return false;
+  }
+  return true;
+}
 
 // The obstacle's planes in the query's cell-width frame (anchor: the lattice
 // corner of the queried cell or face); present = false without an obstacle.
@@ -2167,8 +2375,9 @@ struct FaceQuery {
 };
 struct FaceResult {
   double open, blocked;
+  double piston_velocity, wall_flux;  // open tank: the piston's share of a closed low-x face
   int32_t status;
-  int32_t pad;
+  int32_t is_piston;
 };
 struct CurvatureQuery {
   double d[27];  // centre distances, x fastest, the eight outer corners unused
@@ -2244,14 +2453,115 @@ __global__ void k_freeze_cells(FreezeArgs a) {
   a.cr[i] = r;
 }
 
+// Cell volumes inside an open tank: the liquid part of each tetrahedron
+// clipped to the tank's box in the cell's unit frame.
+__global__ void k_freeze_cells_tank(FreezeArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *a.arch = compiled_arch();
+  if (i >= a.ncell) return;
+  const CellQuery& q = a.cq[i];
+  CellResult r{0.0, 0.0, FL_OK, 0};
+  TankBounds tb;
+  if (!tank_cell_resolved(a.origin, a.h, q.index) ||
+      local_tank_bounds(a.obstacle, a.origin, a.h, q.index, -1, tb) != FL_OK) {
+    r.status = FL_OUT_OF_RANGE;
+    a.cr[i] = r;
+    return;
+  }
+  const double box = tank_box_measure(tb, a.h, -1);
+  bool all_liquid = true;
+  for (int c = 0; c < 8; ++c) all_liquid = all_liquid && q.corner[c] < 0;
+  if (!normal_or_zero(box)) {
+    r.status = FL_OUT_OF_RANGE;
+  } else if (box != 0.0 && all_liquid) {
+    r.high = box;
+  } else if (box != 0.0) {
+    ClipVertex corner[8];
+    for (int c = 0; c < 8; ++c) {
+      for (int d = 0; d < 3; ++d) corner[c].p[d] = (double)((c >> d) & 1);
+      corner[c].d = q.corner[c];
+    }
+    const ClipPlane liquid{{0.0, 0.0, 0.0}, 0.0, true};
+    for (int t = 0; t < 6; ++t) {
+      const ClipVertex& A = corner[kCubeTets[t][0]];
+      const ClipVertex& B = corner[kCubeTets[t][1]];
+      const ClipVertex& C = corner[kCubeTets[t][2]];
+      const ClipVertex& D = corner[kCubeTets[t][3]];
+      if (!(A.d < 0.0 || B.d < 0.0 || C.d < 0.0 || D.d < 0.0)) continue;
+      Tetrahedron tet;
+      const ClipVertex* faces[4][3] = {{&A, &B, &C}, {&A, &B, &D}, {&A, &C, &D}, {&B, &C, &D}};
+      for (int f = 0; f < 4; ++f)
+        for (int k = 0; k < 3; ++k) tet.f[f].push(*faces[f][k]);
+      TankPolyhedron cur, next;
+      clip_polyhedron(tet, liquid, cur);
+      // the low then high plane of each axis strictly inside the cell
+      for (int ax = 0; ax < 3; ++ax) {
+        ClipPlane pl{{0.0, 0.0, 0.0}, 0.0, false, ax};
+        if (tb.low[ax] > 0) {
+          pl.n[ax] = -1;
+          pl.c = -tb.low[ax];
+          clip_polyhedron(cur, pl, next);
+          cur = next;
+        }
+        if (tb.high[ax] < 1) {
+          pl.n[ax] = 1;
+          pl.c = tb.high[ax];
+          clip_polyhedron(cur, pl, next);
+          cur = next;
+        }
+      }
+      r.high += clipped_volume(cur, a.h);
+    }
+  }
+  a.cr[i] = r;
+}
+
 __global__ void k_freeze_faces(FreezeArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nface) return;
   const FaceQuery& q = a.fq[i];
-  FaceResult r{0.0, 0.0, FL_OK, 0};
+  FaceResult r{0.0, 0.0, 0.0, 0.0, FL_OK, 0};
   const double h = a.h, full = h * h;
   if (q.axis < 0 || q.axis >= 3) {
     r.status = FL_INVALID_ARGUMENT;
+    a.fr[i] = r;
+    return;
+  }
+  if (a.obstacle.kind == FL_OBSTACLE_OPEN_TANK) {
+    // The tank's walls close a face outside its planes; the piston owns the
+    // part of a closed low-x face inside the floor and z bounds.
+    TankBounds tb;
+    r.status = local_tank_bounds(a.obstacle, a.origin, h, q.lattice, q.axis, tb);
+    const double lw[3] = {a.obstacle.tank[0], a.obstacle.tank[2], a.obstacle.tank[3]};
+    const double hw[3] = {a.obstacle.tank[1], kInf, a.obstacle.tank[4]};
+    int low_sign = 0, high_sign = 0;
+    if (r.status == FL_OK &&
+        (tank_plane_sign(lw[q.axis], a.origin[q.axis], (double)q.lattice[q.axis], h, &low_sign) != FL_OK ||
+         tank_plane_sign(hw[q.axis], a.origin[q.axis], (double)q.lattice[q.axis], h, &high_sign) != FL_OK))
+      r.status = FL_OUT_OF_RANGE;
+    if (r.status == FL_OK) {
+      const bool piston_side = q.axis == 0 && low_sign >= 0;
+      const bool open = low_sign < 0 && high_sign > 0;
+      if (open || piston_side) {
+        const double transverse = tank_box_measure(tb, h, q.axis);
+        if (!normal_or_zero(transverse) || transverse > full) {
+          r.status = FL_OUT_OF_RANGE;
+        } else if (open) {
+          r.open = transverse;
+          for (int ax = 0; ax < 3; ++ax)
+            if (ax != q.axis && transverse == full && (tb.low[ax] > 0 || tb.high[ax] < 1)) r.status = FL_OUT_OF_RANGE;
+        } else if (transverse > 0) {
+          r.is_piston = 1;
+          r.piston_velocity = a.obstacle.tank[5];
+          r.wall_flux = transverse * r.piston_velocity;
+          if (!normal_or_zero(r.wall_flux) || (r.piston_velocity != 0 && r.wall_flux == 0)) r.status = FL_OUT_OF_RANGE;
+        }
+      }
+      if (r.status == FL_OK) {
+        r.blocked = full - r.open;
+        if (!normal_or_zero(r.blocked)) r.status = FL_OUT_OF_RANGE;
+      }
+    }
     a.fr[i] = r;
     return;
   }
@@ -2282,10 +2592,10 @@ __global__ void k_freeze_faces(FreezeArgs a) {
       continue;
     }
     Polygon blocked;
-    clip_polygon(pg, inside, blocked, nullptr);
+    clip_polygon(pg, inside, blocked);
     if (lp.slab) {
       Polygon b2;
-      clip_polygon(blocked, beyond, b2, nullptr);
+      clip_polygon(blocked, beyond, b2);
       blocked = b2;
     }
     geometric_blocked += clipped_area(blocked, h);
@@ -2475,12 +2785,28 @@ bool freeze_phase(fl_boundary* b, size_t qoff, size_t qbytes, size_t roff, size_
 }
 
 // ValidateObstacle (liquid_boundary_geometry_3d.cc:132-175) for the kinds offered here.
-int check_obstacle(const fl_obstacle& o, FreezeObstacle* out) {
+int check_obstacle(const fl_obstacle& o, double step, FreezeObstacle* out) {
   out->kind = o.kind;
   out->coordinate = o.coordinate;
   out->half_width = o.kind == FL_OBSTACLE_SLAB ? o.half_width : 0.0;
   for (int a = 0; a < 3; ++a) out->n[a] = o.unit_normal[a];
+  for (int k = 0; k < 6; ++k) out->tank[k] = o.tank[k];
   if (o.kind == FL_OBSTACLE_NONE) return FL_OK;
+  if (o.kind == FL_OBSTACLE_OPEN_TANK) {
+    // CheckTankStep (base/liquid_boundary_math.h:252-276)
+    const double* t = o.tank;
+    for (int k = 0; k < 6; ++k)
+      if (!std::isfinite(t[k])) return FL_INVALID_ARGUMENT;
+    if (t[0] >= t[1] || t[3] >= t[4]) return FL_INVALID_ARGUMENT;
+    const double displacement = t[5] * step;
+    const double end_x = std::fma(t[5], step, t[0]);
+    const double start_width = t[1] - t[0], end_width = t[1] - end_x, width_z = t[4] - t[3];
+    if (!std::isfinite(displacement) || !std::isfinite(end_x) || !std::isfinite(start_width) ||
+        !std::isfinite(end_width) || !std::isfinite(width_z))
+      return FL_OUT_OF_RANGE;
+    if (end_x >= t[1]) return FL_FAILED_PRECONDITION;
+    return FL_OK;
+  }
   if (o.kind != FL_OBSTACLE_HALFSPACE && o.kind != FL_OBSTACLE_SLAB) return FL_INVALID_ARGUMENT;
   double low = o.coordinate, high = o.coordinate;
   if (o.kind == FL_OBSTACLE_SLAB) {
@@ -2518,7 +2844,7 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
     return FL_INVALID_ARGUMENT;
   if (in->has_exact_curvature && !std::isfinite(in->exact_curvature)) return FL_INVALID_ARGUMENT;
   FreezeObstacle ob;
-  st = check_obstacle(in->obstacle, &ob);
+  st = check_obstacle(in->obstacle, in->step_duration, &ob);
   if (st != FL_OK) return st;
   const fl_owned_grid* g = in->grid;
   const double h = g->h, full_area = h * h, full_volume = full_area * h;
@@ -2585,7 +2911,10 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
             b, R.cq, sizeof(CellQuery) * staged, R.cr, sizeof(CellResult) * staged,
             [&]() {
               ++g_kernel_launches;
-              k_freeze_cells<<<grid_of(staged, 64), 64, 0, b->stream>>>(a);
+              if (ob.kind == FL_OBSTACLE_OPEN_TANK)
+                k_freeze_cells_tank<<<grid_of(staged, 32), 32, 0, b->stream>>>(a);
+              else
+                k_freeze_cells<<<grid_of(staged, 64), 64, 0, b->stream>>>(a);
             },
             &ms))
       return FL_INTERNAL;
@@ -2653,8 +2982,15 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
       if (fr[f].status != FL_OK) return fr[f].status;
       faces_out[f].open_area = fr[f].open;
       faces_out[f].blocked_area = fr[f].blocked;
-      faces_out[f].wall_normal_velocity = in->obstacle.kind == FL_OBSTACLE_NONE ? 0.0
-                                                                               : in->obstacle.wall_velocity[faces_out[f].axis];
+      if (ob.kind == FL_OBSTACLE_OPEN_TANK) {
+        faces_out[f].wall_normal_velocity = fr[f].piston_velocity;
+        faces_out[f].prescribed_wall_flux = fr[f].wall_flux;
+        faces_out[f].has_prescribed_wall_flux = 1;
+        faces_out[f].is_low_x_piston_face = (uint8_t)fr[f].is_piston;
+      } else {
+        faces_out[f].wall_normal_velocity =
+            ob.kind == FL_OBSTACLE_NONE ? 0.0 : in->obstacle.wall_velocity[faces_out[f].axis];
+      }
     }
   }
   // Interface cells (:983-1009): a kept cell with an open face toward an air centre.

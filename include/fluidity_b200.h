@@ -732,8 +732,9 @@ typedef struct {
  * plane and by the obstacle's planes), the kept cells' faces with their open
  * and blocked areas, the outward curvature of interface cells (exact, or from
  * the centred second differences of the centre distances) and the capillary
- * step bound. Obstacles: none, a translating halfspace or a translating slab;
- * open tanks and sampled solids are not offered here. The host stages the
+ * step bound. Obstacles: none, a translating halfspace, a translating slab or
+ * an open tank with its low-x piston (the piston's share of a closed face
+ * becomes a prescribed wall flux); sampled solids are not offered here. The host stages the
  * sample lookups and keeps the reference's error order; the device computes
  * every volume, area, curvature and bound. */
 typedef struct {
@@ -744,6 +745,7 @@ typedef struct {
 #define FL_OBSTACLE_NONE 0
 #define FL_OBSTACLE_HALFSPACE 1
 #define FL_OBSTACLE_SLAB 2
+#define FL_OBSTACLE_OPEN_TANK 3
 typedef struct {
   int32_t kind; /* FL_OBSTACLE_* */
   int32_t pad;
@@ -751,6 +753,9 @@ typedef struct {
   double coordinate;       /* halfspace: start plane coordinate; slab: start centre coordinate (m) */
   double half_width;       /* slab only (m) */
   double wall_velocity[3]; /* m/s */
+  /* open tank (AxisAlignedLiquidTank3D): start low x, high x, floor y, low z,
+   * high z (m; open above the floor) and the low-x piston's x velocity (m/s) */
+  double tank[6];
 } fl_obstacle;
 typedef struct {
   const fl_owned_grid* grid;

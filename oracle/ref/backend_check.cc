@@ -375,14 +375,17 @@ int bk_links(int which, const double origin[3], double h, const int32_t* blocks,
 
 // .freeze on candidate cells with centre and corner samples (x,y,z; d),
 // obstacle kind 0 none / 1 halfspace / 2 slab (normal, coordinate, half
-// width, wall velocity) and the exact curvature (NaN for none). Outputs: cells
+// width, wall velocity) / 3 open tank (low x, high x, floor y, low z, high z,
+// piston velocity) and the exact curvature (NaN for none). Face outputs add
+// the prescribed wall flux (NaN for none) and the piston flag. Outputs: cells
 // (x,y,z) + (volume, centre distance, curvature), faces (axis,x,y,z) + slot +
 // (open, blocked, wall velocity), the counts and the capillary bound.
 int bk_freeze(int which, const double origin[3], double h, const int32_t* blocks, uint64_t nb,
               const int32_t* cell_index, uint64_t n, const int32_t* center_index, const double* center_distance,
               uint64_t ncenters, const int32_t* corner_index, const double* corner_distance, uint64_t ncorners,
               int obstacle_kind, const double normal[3], double coordinate, double half_width,
-              const double velocity[3], double step_duration, double density, double sigma, double exact_curvature,
+              const double velocity[3], const double tank[6], double step_duration, double density, double sigma,
+              double exact_curvature,
               int32_t* cells_index_out, double* cells_out, uint64_t* ncells_out, int32_t* faces_index_out,
               uint64_t* faces_slot_out, double* faces_out, uint64_t* nfaces_out, double* capillary_bound) {
   int code = 0;
@@ -404,6 +407,7 @@ int bk_freeze(int which, const double origin[3], double h, const int32_t* blocks
   const Vec3 nrm{normal[0], normal[1], normal[2]}, vel{velocity[0], velocity[1], velocity[2]};
   if (obstacle_kind == 1) obstacle = TranslatingHalfspace3D{nrm, coordinate, vel};
   if (obstacle_kind == 2) obstacle = TranslatingSlab3D{nrm, coordinate, half_width, vel};
+  if (obstacle_kind == 3) obstacle = AxisAlignedLiquidTank3D{tank[0], tank[1], tank[2], tank[3], tank[4], tank[5]};
   LiquidBoundaryGeometryViewInputs3D in{grid->view(), cells, centers, corners, obstacle, step_duration, density,
                                         sigma};
   if (exact_curvature == exact_curvature) in.exact_outward_interface_curvature = exact_curvature;
@@ -427,9 +431,11 @@ int bk_freeze(int which, const double origin[3], double h, const int32_t* blocks
     faces_index_out[4 * f + 2] = face.face_index.lattice_index.y;
     faces_index_out[4 * f + 3] = face.face_index.lattice_index.z;
     faces_slot_out[f] = face.face_slot;
-    faces_out[3 * f] = face.open_area;
-    faces_out[3 * f + 1] = face.blocked_area;
-    faces_out[3 * f + 2] = face.wall_normal_velocity;
+    faces_out[5 * f] = face.open_area;
+    faces_out[5 * f + 1] = face.blocked_area;
+    faces_out[5 * f + 2] = face.wall_normal_velocity;
+    faces_out[5 * f + 3] = face.prescribed_wall_flux.value_or(std::nan(""));
+    faces_out[5 * f + 4] = face.is_low_x_piston_face ? 1.0 : 0.0;
   }
   *capillary_bound = r->capillary_step_bound;
   return 0;

@@ -346,11 +346,13 @@ class FreezeScene:
     of a liquid cell opens onto a liquid or an air cell. Obstacles: none, a
     translating halfspace whose plane cuts the drop's low-x, low-z side, or a
     translating slab 2.4 h thick across it (thicker than a cell's diagonal, so
-    no cell holds liquid on both of its sides). Active 4^3 blocks: x, z in
-    [-1, 3], y in [-1, 2]."""
+    no cell holds liquid on both of its sides); with the open tank the liquid
+    is instead a pool filling a tank whose walls and floor cut the lattice
+    cells. Active 4^3 blocks: x, z in [-1, 3], y in [-1, 2]."""
 
     def __init__(self, obstacle: str = "none", sigma: float = 0.072, exact_curvature: float = float("nan")):
         n, ny = 12, 9
+        self.tank = (0.0,) * 6
         bz, by, bx = np.meshgrid(np.arange(-1, 4), np.arange(-1, 3), np.arange(-1, 4), indexing="ij")
         self.blocks = np.stack([bx.ravel(), by.ravel(), bz.ravel()], 1).astype(np.int32)
 
@@ -374,6 +376,15 @@ class FreezeScene:
         elif obstacle == "slab":
             self.kind, self.normal, self.coordinate, self.half_width = 2, (0.6, 0.0, 0.8), 8.1 * H, 1.2 * H
             self.velocity = (0.0, 0.0, 0.1)
+        elif obstacle == "tank":
+            # a pool filling an open tank whose walls and floor cut the lattice
+            # cells (low x moves as a piston): distance (y - s(x, z)) h
+            self.kind, self.tank = 3, (0.3 * H, 11.6 * H, 0.45 * H, 0.2 * H, 11.7 * H, 0.05)
+            surface = lambda x, z: 4.4 + 0.7 * np.sin(x / 2.0) * np.cos(0.4 * z)  # noqa: E731
+            c = self.center_index + 0.5
+            self.center_distance = (c[:, 1] - surface(c[:, 0], c[:, 2])) * H
+            k = self.corner_index.astype(np.float64)
+            self.corner_distance = (k[:, 1] - surface(k[:, 0], k[:, 2])) * H
         self.step_duration, self.density, self.sigma = DT, 1000.0, sigma
         self.exact_curvature = exact_curvature
 
@@ -381,7 +392,8 @@ class FreezeScene:
 def freeze(which, s: FreezeScene, **override):
     """The table's .freeze on the scene: (code, cell indices, cell values
     (volume, centre distance, curvature), face indices (axis, x, y, z), face
-    slots, face values (open, blocked, wall velocity), capillary bound)."""
+    slots, face values (open, blocked, wall velocity, prescribed wall flux or
+    NaN, piston flag), capillary bound)."""
     a = dict(s.__dict__)
     a.update(override)
     n = len(a["cell_index"])
@@ -389,7 +401,7 @@ def freeze(which, s: FreezeScene, **override):
     cv = np.zeros((n, 3))
     fi = np.zeros((6 * n, 4), np.int32)
     fs = np.zeros(6 * n, np.uint64)
-    fv = np.zeros((6 * n, 3))
+    fv = np.zeros((6 * n, 5))
     nc, nf, bound = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_double(0.0)
     c = lambda x, t: np.ascontiguousarray(x, t)  # noqa: E731
     code = lib().bk_freeze(
@@ -399,7 +411,7 @@ def freeze(which, s: FreezeScene, **override):
         ctypes.c_uint64(len(a["center_index"])), _p(c(a["corner_index"], np.int32)),
         _p(c(a["corner_distance"], np.float64)), ctypes.c_uint64(len(a["corner_index"])), ctypes.c_int(a["kind"]),
         _d3(a["normal"]), ctypes.c_double(a["coordinate"]), ctypes.c_double(a["half_width"]), _d3(a["velocity"]),
-        ctypes.c_double(a["step_duration"]), ctypes.c_double(a["density"]), ctypes.c_double(a["sigma"]),
+        (ctypes.c_double * 6)(*[float(v) for v in a["tank"]]), ctypes.c_double(a["step_duration"]), ctypes.c_double(a["density"]), ctypes.c_double(a["sigma"]),
         ctypes.c_double(a["exact_curvature"]), _p(ci), _p(cv), ctypes.byref(nc), _p(fi), _p(fs), _p(fv),
         ctypes.byref(nf), ctypes.byref(bound))
     k, m = nc.value, nf.value

@@ -281,11 +281,11 @@ def _assert_frozen_equal(cpu, gpu):
     assert np.array_equal(cv1[:, :2], cv0[:, :2])  # liquid volumes and centre distances, bitwise
     assert np.array_equal(cv1[:, 2], cv0[:, 2])  # curvature, bitwise
     assert np.array_equal(fi1, fi0) and np.array_equal(fs1, fs0)
-    assert np.array_equal(fv1, fv0)  # open and blocked areas, wall velocities
+    assert np.array_equal(fv1, fv0, equal_nan=True)  # areas, wall velocities, piston fluxes and flags
     assert bound1 == bound0
 
 
-@pytest.mark.parametrize("obstacle", ["none", "halfspace", "slab"])
+@pytest.mark.parametrize("obstacle", ["none", "halfspace", "slab", "tank"])
 def test_freeze_is_bit_identical(obstacle):
     s = bt.FreezeScene(obstacle)
     cpu, gpu = bt.freeze(CPU, s), bt.freeze(B200, s)
@@ -296,6 +296,8 @@ def test_freeze_is_bit_identical(obstacle):
     assert (cv[:, 2] != 0).sum() > 50 and np.isfinite(bound)  # interface cells with curvature
     if obstacle != "none":
         assert ((fv[:, 0] > 0) & (fv[:, 0] < bt.H ** 2)).sum() > 10  # partly blocked faces
+    if obstacle == "tank":
+        assert fv[:, 4].sum() > 10 and np.isfinite(fv[:, 3]).all()  # piston faces; every face carries a flux
 
 
 def test_freeze_with_exact_curvature_and_without_surface_tension():
@@ -331,6 +333,17 @@ def test_freeze_error_codes_match():
     assert both(corner_distance=bad) == 3
     many = np.repeat(s.cell_index, 4, axis=0)[:4097]
     assert both(cell_index=many) == 8
+    t = bt.FreezeScene("tank")
+
+    def tank(**kw):
+        a, b = bt.freeze(CPU, t, **kw)[0], bt.freeze(B200, t, **kw)[0]
+        assert a == b, (kw.keys(), a, b)
+        return a
+
+    low, high = t.tank[0], t.tank[1]
+    assert tank(tank=(high, low) + t.tank[2:]) == 3  # walls out of order
+    assert tank(tank=t.tank[:5] + (1e4,)) == 9  # the piston passes the far wall within the step
+    assert tank(tank=t.tank[:2] + (np.inf,) + t.tank[3:]) == 3
 
 
 def test_freeze_then_links_on_device_match_the_cpu_pipeline():
