@@ -346,9 +346,10 @@ def test_freeze_error_codes_match():
     assert tank(tank=t.tank[:2] + (np.inf,) + t.tank[3:]) == 3
 
 
-def test_freeze_then_links_on_device_match_the_cpu_pipeline():
+@pytest.mark.parametrize("obstacle", ["none", "tank"])
+def test_freeze_then_links_on_device_match_the_cpu_pipeline(obstacle):
     """The frozen view of each table feeds that table's own link assembly."""
-    s = bt.FreezeScene()
+    s = bt.FreezeScene(obstacle)
     out = []
     for which in (CPU, B200):
         code, ci, cv, fi, fs, fv, _ = bt.freeze(which, s)
@@ -357,10 +358,9 @@ def test_freeze_then_links_on_device_match_the_cpu_pipeline():
         fields = np.zeros((nc, 4))
         fields[:, 1] = np.inf
         fields[:, 3] = np.nan
-        face_values = np.concatenate([fv, np.full((nf, 1), np.nan)], 1)
         ls = dict(blocks=s.blocks, center_index=s.center_index, center_distance=s.center_distance, cell_index=ci,
-                  cell_values=cv, face_index=fi, face_slot=fs, face_values=face_values,
-                  piston=np.zeros(nf, np.uint8), step_duration=s.step_duration, density=s.density, sigma=s.sigma,
+                  cell_values=cv, face_index=fi, face_slot=fs, face_values=fv[:, :4],
+                  piston=fv[:, 4].astype(np.uint8), step_duration=s.step_duration, density=s.density, sigma=s.sigma,
                   fields=fields, predicted=np.linspace(-0.1, 0.1, nf), ambient=0.0, air_index=np.zeros((0, 3)),
                   air_pressure=np.zeros(0), itf_ordinal=np.zeros(0, np.uint64), itf_values=np.zeros((0, 4)),
                   wetted=None)
