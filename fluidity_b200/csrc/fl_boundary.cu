@@ -2406,114 +2406,127 @@ struct FreezeArgs {
   int* arch;
 };
 
-__global__ void k_freeze_cells(FreezeArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *a.arch = compiled_arch();
-  if (i >= a.ncell) return;
-  const CellQuery& q = a.cq[i];
-  CellResult r{0.0, 0.0, FL_OK, 0};
-  LocalPlanes lp;
-  r.status = local_planes(a.obstacle, a.origin, a.h, q.index, lp);
-  if (r.status != FL_OK) {
-    a.cr[i] = r;
-    return;
+// One thread per (cell, tetrahedron), 32 cells per CTA: each thread clips its
+// tetrahedron; the cell's first thread sums the six contributions in
+// tetrahedron order (a tetrahedron without liquid adds +0, which leaves the
+// sum's bits unchanged) and writes the cell's result.
+constexpr int kFreezeCellsPerCta = 32;
+constexpr int kFreezeCellThreads = 6 * kFreezeCellsPerCta;
+
+__device__ void tet_corners(const CellQuery& q, int t, ClipVertex v[4]) {
+  for (int k = 0; k < 4; ++k) {
+    const int c = kCubeTets[t][k];
+    for (int d = 0; d < 3; ++d) v[k].p[d] = (double)((c >> d) & 1);
+    v[k].d = q.corner[c];
   }
-  ClipVertex corner[8];
-  for (int c = 0; c < 8; ++c) {
-    for (int d = 0; d < 3; ++d) corner[c].p[d] = (double)((c >> d) & 1);
-    corner[c].d = q.corner[c];
+}
+
+__device__ void tet_faces(const ClipVertex v[4], Tetrahedron& tet) {
+  const int f[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+  for (int k = 0; k < 4; ++k)
+    for (int j = 0; j < 3; ++j) tet.f[k].push(v[f[k][j]]);
+}
+
+__device__ void sum_cell(FreezeArgs& a, int cell, int tet, int status, double lo, double hi) {
+  __shared__ double s_lo[kFreezeCellThreads], s_hi[kFreezeCellThreads];
+  const int slot = threadIdx.x;
+  s_lo[slot] = lo;
+  s_hi[slot] = hi;
+  __syncthreads();
+  if (cell < a.ncell && tet == 0) {
+    CellResult r{0.0, 0.0, status, 0};
+    if (status == FL_OK)
+      for (int k = 0; k < 6; ++k) {
+        r.low += s_lo[slot + k];
+        r.high += s_hi[slot + k];
+      }
+    a.cr[cell] = r;
   }
-  const ClipPlane liquid{{0.0, 0.0, 0.0}, 0.0, true};
-  const ClipPlane above{{-lp.n[0], -lp.n[1], -lp.n[2]}, -lp.high, false};
-  const ClipPlane below{{lp.n[0], lp.n[1], lp.n[2]}, lp.low, false};
-  for (int t = 0; t < 6; ++t) {
-    const ClipVertex& A = corner[kCubeTets[t][0]];
-    const ClipVertex& B = corner[kCubeTets[t][1]];
-    const ClipVertex& C = corner[kCubeTets[t][2]];
-    const ClipVertex& D = corner[kCubeTets[t][3]];
-    if (!(A.d < 0.0 || B.d < 0.0 || C.d < 0.0 || D.d < 0.0)) continue;  // an all-zero tetrahedron holds no liquid
-    Tetrahedron tet;
-    const ClipVertex* faces[4][3] = {{&A, &B, &C}, {&A, &B, &D}, {&A, &C, &D}, {&B, &C, &D}};
-    for (int f = 0; f < 4; ++f)
-      for (int k = 0; k < 3; ++k) tet.f[f].push(*faces[f][k]);
-    Polyhedron wet;
-    clip_polyhedron(tet, liquid, wet);
-    if (!lp.present) {
-      r.high += clipped_volume(wet, a.h);
-    } else {
-      Polyhedron side;
-      clip_polyhedron(wet, above, side);
-      r.high += clipped_volume(side, a.h);
-      if (lp.slab) {
-        clip_polyhedron(wet, below, side);
-        r.low += clipped_volume(side, a.h);
+}
+
+__global__ void __launch_bounds__(kFreezeCellThreads) k_freeze_cells(FreezeArgs a) {
+  const int cell = blockIdx.x * kFreezeCellsPerCta + threadIdx.x / 6, t = threadIdx.x % 6;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.arch = compiled_arch();
+  double lo = 0.0, hi = 0.0;
+  int status = FL_OK;
+  if (cell < a.ncell) {
+    const CellQuery& q = a.cq[cell];
+    LocalPlanes lp;
+    status = local_planes(a.obstacle, a.origin, a.h, q.index, lp);
+    ClipVertex v[4];
+    tet_corners(q, t, v);
+    if (status == FL_OK && (v[0].d < 0.0 || v[1].d < 0.0 || v[2].d < 0.0 || v[3].d < 0.0)) {
+      Tetrahedron tet;
+      tet_faces(v, tet);
+      const ClipPlane liquid{{0.0, 0.0, 0.0}, 0.0, true};
+      Polyhedron wet;
+      clip_polyhedron(tet, liquid, wet);
+      if (!lp.present) {
+        hi = clipped_volume(wet, a.h);
+      } else {
+        const ClipPlane above{{-lp.n[0], -lp.n[1], -lp.n[2]}, -lp.high, false};
+        Polyhedron side;
+        clip_polyhedron(wet, above, side);
+        hi = clipped_volume(side, a.h);
+        if (lp.slab) {
+          const ClipPlane below{{lp.n[0], lp.n[1], lp.n[2]}, lp.low, false};
+          clip_polyhedron(wet, below, side);
+          lo = clipped_volume(side, a.h);
+        }
       }
     }
   }
-  a.cr[i] = r;
+  sum_cell(a, cell, t, status, lo, hi);
 }
 
 // Cell volumes inside an open tank: the liquid part of each tetrahedron
-// clipped to the tank's box in the cell's unit frame.
-__global__ void k_freeze_cells_tank(FreezeArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *a.arch = compiled_arch();
-  if (i >= a.ncell) return;
-  const CellQuery& q = a.cq[i];
-  CellResult r{0.0, 0.0, FL_OK, 0};
-  TankBounds tb;
-  if (!tank_cell_resolved(a.origin, a.h, q.index) ||
-      local_tank_bounds(a.obstacle, a.origin, a.h, q.index, -1, tb) != FL_OK) {
-    r.status = FL_OUT_OF_RANGE;
-    a.cr[i] = r;
-    return;
-  }
-  const double box = tank_box_measure(tb, a.h, -1);
-  bool all_liquid = true;
-  for (int c = 0; c < 8; ++c) all_liquid = all_liquid && q.corner[c] < 0;
-  if (!normal_or_zero(box)) {
-    r.status = FL_OUT_OF_RANGE;
-  } else if (box != 0.0 && all_liquid) {
-    r.high = box;
-  } else if (box != 0.0) {
-    ClipVertex corner[8];
-    for (int c = 0; c < 8; ++c) {
-      for (int d = 0; d < 3; ++d) corner[c].p[d] = (double)((c >> d) & 1);
-      corner[c].d = q.corner[c];
-    }
-    const ClipPlane liquid{{0.0, 0.0, 0.0}, 0.0, true};
-    for (int t = 0; t < 6; ++t) {
-      const ClipVertex& A = corner[kCubeTets[t][0]];
-      const ClipVertex& B = corner[kCubeTets[t][1]];
-      const ClipVertex& C = corner[kCubeTets[t][2]];
-      const ClipVertex& D = corner[kCubeTets[t][3]];
-      if (!(A.d < 0.0 || B.d < 0.0 || C.d < 0.0 || D.d < 0.0)) continue;
+// clipped to the tank's box in the cell's unit frame (low then high plane of
+// each axis strictly inside the cell).
+__global__ void __launch_bounds__(kFreezeCellThreads) k_freeze_cells_tank(FreezeArgs a) {
+  const int cell = blockIdx.x * kFreezeCellsPerCta + threadIdx.x / 6, t = threadIdx.x % 6;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.arch = compiled_arch();
+  double hi = 0.0;
+  int status = FL_OK;
+  if (cell < a.ncell) {
+    const CellQuery& q = a.cq[cell];
+    TankBounds tb;
+    if (!tank_cell_resolved(a.origin, a.h, q.index) ||
+        local_tank_bounds(a.obstacle, a.origin, a.h, q.index, -1, tb) != FL_OK)
+      status = FL_OUT_OF_RANGE;
+    const double box = status == FL_OK ? tank_box_measure(tb, a.h, -1) : 0.0;
+    bool all_liquid = true;
+    for (int c = 0; c < 8; ++c) all_liquid = all_liquid && q.corner[c] < 0;
+    if (status == FL_OK && !normal_or_zero(box)) status = FL_OUT_OF_RANGE;
+    ClipVertex v[4];
+    tet_corners(q, t, v);
+    if (status == FL_OK && box != 0.0 && all_liquid) {
+      hi = t == 0 ? box : 0.0;  // the whole box, once
+    } else if (status == FL_OK && box != 0.0 && (v[0].d < 0.0 || v[1].d < 0.0 || v[2].d < 0.0 || v[3].d < 0.0)) {
       Tetrahedron tet;
-      const ClipVertex* faces[4][3] = {{&A, &B, &C}, {&A, &B, &D}, {&A, &C, &D}, {&B, &C, &D}};
-      for (int f = 0; f < 4; ++f)
-        for (int k = 0; k < 3; ++k) tet.f[f].push(*faces[f][k]);
-      TankPolyhedron cur, next;
-      clip_polyhedron(tet, liquid, cur);
-      // the low then high plane of each axis strictly inside the cell
+      tet_faces(v, tet);
+      const ClipPlane liquid{{0.0, 0.0, 0.0}, 0.0, true};
+      TankPolyhedron buf[2];
+      int cur = 0;
+      clip_polyhedron(tet, liquid, buf[cur]);
       for (int ax = 0; ax < 3; ++ax) {
         ClipPlane pl{{0.0, 0.0, 0.0}, 0.0, false, ax};
         if (tb.low[ax] > 0) {
           pl.n[ax] = -1;
           pl.c = -tb.low[ax];
-          clip_polyhedron(cur, pl, next);
-          cur = next;
+          clip_polyhedron(buf[cur], pl, buf[1 - cur]);
+          cur = 1 - cur;
         }
         if (tb.high[ax] < 1) {
           pl.n[ax] = 1;
           pl.c = tb.high[ax];
-          clip_polyhedron(cur, pl, next);
-          cur = next;
+          clip_polyhedron(buf[cur], pl, buf[1 - cur]);
+          cur = 1 - cur;
         }
       }
-      r.high += clipped_volume(cur, a.h);
+      hi = clipped_volume(buf[cur], a.h);
     }
   }
-  a.cr[i] = r;
+  sum_cell(a, cell, t, status, 0.0, hi);
 }
 
 __global__ void k_freeze_faces(FreezeArgs a) {
@@ -2911,10 +2924,11 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
             b, R.cq, sizeof(CellQuery) * staged, R.cr, sizeof(CellResult) * staged,
             [&]() {
               ++g_kernel_launches;
+              const unsigned ctas = (unsigned)((staged + kFreezeCellsPerCta - 1) / kFreezeCellsPerCta);
               if (ob.kind == FL_OBSTACLE_OPEN_TANK)
-                k_freeze_cells_tank<<<grid_of(staged, 32), 32, 0, b->stream>>>(a);
+                k_freeze_cells_tank<<<ctas, kFreezeCellThreads, 0, b->stream>>>(a);
               else
-                k_freeze_cells<<<grid_of(staged, 64), 64, 0, b->stream>>>(a);
+                k_freeze_cells<<<ctas, kFreezeCellThreads, 0, b->stream>>>(a);
             },
             &ms))
       return FL_INTERNAL;

@@ -158,11 +158,14 @@ int device_ready() {
     cudaGetLastError();
     return FL_FAILED_PRECONDITION;
   }
-  int dev = 0;
+  int dev = 0, major = 0;
   cudaGetDevice(&dev);
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return FL_FAILED_PRECONDITION;
-  if (prop.major != 10) return FL_FAILED_PRECONDITION;  // image is sm_100a only
+  // one attribute query (a full property query costs milliseconds per call)
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return FL_FAILED_PRECONDITION;
+  }
+  if (major != 10) return FL_FAILED_PRECONDITION;  // image is sm_100a only
   return FL_OK;
 }
 

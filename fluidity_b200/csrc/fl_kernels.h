@@ -239,9 +239,9 @@ struct OwnedFaceKey {
 // projections through it allocate nothing; a scratch left empty grows for the
 // call.
 struct MpScratch {
-  std::vector<OwnedFaceKey> incident;
   std::vector<int> tail, head, cell_off, cell_ent, fill, parent, root, comp_of, gauges, comp_cell_off, comp_cells,
       comp_face_off, comp_faces, host_ints;
+  std::vector<int> lut;  // cell ordinal per lattice position of the cells' bounding box (-1: none), when it fits
   std::vector<unsigned char> anchored, pinned;
   std::vector<double> hp, hr, hd, hb, hu;
   char* arena = nullptr;

@@ -414,6 +414,23 @@ FaceKey face_key(int axis, int64_t x, int64_t y, int64_t z) {
   return FaceKey{{fdiv(z), fdiv(y), fdiv(x), axis, fmod(z), fmod(y), fmod(x)}};
 }
 
+// Largest cell bounding box (in lattice positions) given a dense ordinal lookup.
+constexpr size_t kMpLutCap = 1 << 20;
+
+// The owned-slot order of faces as two words: (block z, block y) and
+// (block x, axis, local z, y, x); int32 order kept by flipping sign bits.
+struct PackedFaceKey {
+  uint64_t hi, lo;
+  bool operator<(const PackedFaceKey& o) const { return hi != o.hi ? hi < o.hi : lo < o.lo; }
+};
+
+PackedFaceKey packed_face_key(int axis, int64_t x, int64_t y, int64_t z) {
+  const FaceKey k = face_key(axis, x, y, z);  // block z, y, x, axis, local z, y, x
+  auto u = [](int32_t v) { return (uint64_t)((uint32_t)v ^ 0x80000000u); };
+  const uint64_t local = (uint64_t)((k.v[3] << 6) | (k.v[4] << 4) | (k.v[5] << 2) | k.v[6]);
+  return PackedFaceKey{(u(k.v[0]) << 32) | u(k.v[1]), (u(k.v[2]) << 8) | local};
+}
+
 int find_root(std::vector<int>& parent, int c) {
   while (parent[c] != c) c = parent[c];
   return c;
@@ -433,7 +450,7 @@ size_t mp_arena_bytes(size_t nc, size_t nf, size_t ent, size_t ncomp, size_t com
 bool MpScratch::reserve_caps() {
   const size_t nc = kMpMaxCells, nf = kMpMaxFaces;
   try {
-    incident.reserve(6 * nc);
+    lut.reserve(kMpLutCap);
     tail.reserve(nf);
     head.reserve(nf);
     cell_off.reserve(nc + 1);
@@ -525,27 +542,43 @@ int mp_project(MpScratch& X, cudaStream_t stream, double h, double dt, const int
   // The faces must be exactly the cells' incident faces (six per cell, shared
   // faces once), unique and in the reference's owned-slot order, as
   // PrepareMacPressureSystem3D requires (mac_pressure_3d_system.cc:223-239).
-  {
-    auto& incident = X.incident;
-    incident.clear();
+  // Checked in the face loop below without building the incident set: the
+  // owned-slot keys strictly increase, every face touches a listed cell, and
+  // the faces' cell incidences number six per cell.
+  for (int i = 0; i < nc; ++i)
+    for (int a = 0; a < 3; ++a)
+      if (cell_index[3 * i + a] == INT32_MAX) return FL_OUT_OF_RANGE;  // its high face is off the lattice
+  // Cell lookups: a dense table over the cells' bounding box when it is small
+  // enough, else a binary search of the sorted cells.
+  int64_t lo[3], ext[3];
+  for (int a = 0; a < 3; ++a) {
+    int64_t mn = cell_index[a], mx = cell_index[a];
+    for (int i = 1; i < nc; ++i) {
+      mn = std::min<int64_t>(mn, cell_index[3 * i + a]);
+      mx = std::max<int64_t>(mx, cell_index[3 * i + a]);
+    }
+    lo[a] = mn;
+    ext[a] = mx - mn + 1;
+  }
+  const int64_t cap = (int64_t)kMpLutCap;
+  const bool dense = ext[0] <= cap && ext[1] <= cap && ext[2] <= cap && ext[0] * ext[1] <= cap &&
+                     ext[0] * ext[1] * ext[2] <= cap;
+  auto& lut = X.lut;
+  if (dense) {
+    lut.assign((size_t)(ext[0] * ext[1] * ext[2]), -1);
     for (int i = 0; i < nc; ++i) {
       const int32_t* c = cell_index + 3 * i;
-      for (int a = 0; a < 3; ++a) {
-        int64_t hi[3] = {c[0], c[1], c[2]};
-        hi[a] += 1;
-        if (hi[a] > INT32_MAX) return FL_OUT_OF_RANGE;
-        incident.push_back(face_key(a, c[0], c[1], c[2]));
-        incident.push_back(face_key(a, hi[0], hi[1], hi[2]));
-      }
-    }
-    std::sort(incident.begin(), incident.end());
-    incident.erase(std::unique(incident.begin(), incident.end()), incident.end());
-    if (incident.size() != (size_t)nf) return FL_INVALID_ARGUMENT;
-    for (int f = 0; f < nf; ++f) {
-      const int32_t* fi = face_index + 4 * f;
-      if (fi[0] < 0 || fi[0] > 2 || !(face_key(fi[0], fi[1], fi[2], fi[3]) == incident[f])) return FL_INVALID_ARGUMENT;
+      lut[(size_t)(((c[2] - lo[2]) * ext[1] + (c[1] - lo[1])) * ext[0] + (c[0] - lo[0]))] = i;
     }
   }
+  auto lookup = [&](int64_t x, int64_t y, int64_t z) {
+    if (!dense) return find_cell(cell_index, nc, (int32_t)x, (int32_t)y, (int32_t)z);
+    x -= lo[0];
+    y -= lo[1];
+    z -= lo[2];
+    if (x < 0 || y < 0 || z < 0 || x >= ext[0] || y >= ext[1] || z >= ext[2]) return -1;
+    return lut[(size_t)((z * ext[1] + y) * ext[0] + x)];
+  };
   // Face endpoints and the link rules (internal: two cells; Dirichlet: one
   // cell and an open aperture; sealed: closed; the aperture within the full
   // face, mac_pressure_3d_arithmetic.h:182).
@@ -553,17 +586,24 @@ int mp_project(MpScratch& X, cudaStream_t stream, double h, double dt, const int
   auto& head = X.head;
   tail.assign(nf, -1);
   head.assign(nf, -1);
+  PackedFaceKey prev{0, 0};
+  long long incidences = 0;
   for (int f = 0; f < nf; ++f) {
     const int32_t* fi = face_index + 4 * f;
     const double* v = face_values + 6 * f;
     if (fi[0] < 0 || fi[0] > 2 || face_kind[f] < kLinkSealed || face_kind[f] > kLinkDirichlet) return FL_INVALID_ARGUMENT;
+    const PackedFaceKey key = packed_face_key(fi[0], fi[1], fi[2], fi[3]);
+    if (f > 0 && !(prev < key)) return FL_INVALID_ARGUMENT;
+    prev = key;
     for (int k = 0; k < 6; ++k)
       if (!std::isfinite(v[k])) return FL_INVALID_ARGUMENT;
     if (v[0] < 0.0 || v[0] > h * h) return FL_INVALID_ARGUMENT;
-    int32_t tc[3] = {fi[1], fi[2], fi[3]};
+    int64_t tc[3] = {fi[1], fi[2], fi[3]};
     tc[fi[0]] -= 1;
-    tail[f] = find_cell(cell_index, nc, tc[0], tc[1], tc[2]);
-    head[f] = find_cell(cell_index, nc, fi[1], fi[2], fi[3]);
+    tail[f] = tc[fi[0]] < INT32_MIN ? -1 : lookup(tc[0], tc[1], tc[2]);
+    head[f] = lookup(fi[1], fi[2], fi[3]);
+    if (tail[f] < 0 && head[f] < 0) return FL_INVALID_ARGUMENT;
+    incidences += (tail[f] >= 0) + (head[f] >= 0);
     const bool both = tail[f] >= 0 && head[f] >= 0, one = (tail[f] >= 0) != (head[f] >= 0);
     const int kind = face_kind[f];
     if (kind == kLinkInternal && !both) return FL_INVALID_ARGUMENT;
@@ -571,6 +611,7 @@ int mp_project(MpScratch& X, cudaStream_t stream, double h, double dt, const int
     if (kind == kLinkSealed && v[0] != 0.0) return FL_INVALID_ARGUMENT;
     if (v[0] > 0.0 && !(v[2] > 0.0)) return FL_INVALID_ARGUMENT;
   }
+  if (incidences != 6LL * nc) return FL_INVALID_ARGUMENT;
   int st = check_device();
   if (st != FL_OK) return st;
   // Per-cell face lists in increasing face order.

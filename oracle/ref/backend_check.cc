@@ -11,6 +11,7 @@
 // reference's own types, passed through as bytes (their layouts match the
 // C-ABI's, which the adapter checks at compile time). Every entry returns the
 // operation's absl status code (0 = OK) and writes its outputs only on OK.
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -28,6 +29,19 @@
 using namespace fluidity;
 
 namespace {
+
+// Host time of the last table operation alone (the harness's own record
+// conversion, grid and workspace set-up excluded), in ms.
+double g_last_op_ms = 0.0;
+
+template <typename F>
+auto TimedOp(F&& op) {
+  const auto t0 = std::chrono::steady_clock::now();
+  auto r = op();
+  g_last_op_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return r;
+}
+
 
 constexpr std::size_t kParticles = 1024;
 constexpr std::size_t kFaces = 24576;
@@ -113,7 +127,7 @@ int bk_deposit(int which, const double origin[3], double h, const int32_t* block
   const LiquidBoundaryDepositViewInputs3D inputs{grid->view(), Span<LiquidBoundaryParticle3D>(particles, n),
                                                  Span<LiquidBoundaryFaceTag3D>(tags, faces),
                                                  MacDepositQuantization3D{mass_q, momentum_q, declared_capacity}};
-  auto r = table->deposit(table->context, inputs, *ws);
+  auto r = TimedOp([&] { return table->deposit(table->context, inputs, *ws); });
   if (!r.ok()) return Code(r.status());
   std::memcpy(quanta_out, r->face_quanta.data(), r->face_quanta.size_bytes());
   std::memcpy(stencils_out, r->compatible_stencils.data(), r->compatible_stencils.size_bytes());
@@ -129,8 +143,10 @@ int bk_normalize(int which, const void* quanta, uint64_t count, double mass_q, d
   if (!table) return code;
   auto ws = Workspace();
   if (!ws.ok()) return Code(ws.status());
-  auto r = table->normalize(table->context, Span<MacFaceDepositQuanta3D>(quanta, count),
+  auto r = TimedOp([&] {
+    return table->normalize(table->context, Span<MacFaceDepositQuanta3D>(quanta, count),
                             MacDepositQuantization3D{mass_q, momentum_q, declared_capacity}, minimum_face_mass, *ws);
+  });
   if (!r.ok()) return Code(r.status());
   std::memcpy(masses, r->face_masses.data(), r->face_masses.size_bytes());
   std::memcpy(velocities, r->face_velocities.data(), r->face_velocities.size_bytes());
@@ -148,8 +164,8 @@ int bk_forces(int which, const double origin[3], double h, const int32_t* blocks
   if (!grid.ok()) return Code(grid.status());
   const std::size_t faces = grid->face_count();
   std::vector<double> out(faces, 0.0);
-  const auto s = table->forces(table->context, grid->view(), std::span<const double>(old_velocities, faces),
-                               Vec3{acceleration[0], acceleration[1], acceleration[2]}, dt, out);
+  const auto s = TimedOp([&] { return table->forces(table->context, grid->view(), std::span<const double>(old_velocities, faces),
+                               Vec3{acceleration[0], acceleration[1], acceleration[2]}, dt, out); });
   if (!s.ok()) return Code(s);
   std::memcpy(predicted, out.data(), sizeof(double) * faces);
   return 0;
@@ -169,7 +185,7 @@ int bk_predict(int which, const double origin[3], double h, const int32_t* block
   const LiquidMissingFacePredictionInputs3D inputs{
       grid->view(), History(time, velocities, validity, tags, walls, grid->face_count()), slot, side,
       Vec3{acceleration[0], acceleration[1], acceleration[2]}, dt};
-  auto r = table->predict_missing_face(table->context, inputs, *ws);
+  auto r = TimedOp([&] { return table->predict_missing_face(table->context, inputs, *ws); });
   if (!r.ok()) return Code(r.status());
   *predicted = *r;
   return 0;
@@ -193,7 +209,7 @@ int bk_gather(int which, const double origin[3], double h, const int32_t* blocks
       grid->view(), Span<LiquidBoundaryParticle3D>(particles, n), old_time, new_time,
       History(old_time, old_velocities, old_validity, old_tags, old_walls, faces),
       History(new_time, new_velocities, new_validity, new_tags, new_walls, faces)};
-  auto r = table->gather(table->context, inputs, *ws);
+  auto r = TimedOp([&] { return table->gather(table->context, inputs, *ws); });
   if (!r.ok()) return Code(r.status());
   std::memcpy(gathered, r->particles.data(), r->particles.size_bytes());
   counts[0] = r->old_pic_fallback_particle_count;
@@ -252,8 +268,10 @@ int bk_project(int which, const double origin[3], double h, const int32_t* block
     faces[f] = face;
   }
   const LiquidPressureProblemView3D problem{cells, faces};
-  auto r = table->project(table->context, grid->view(), dt, problem,
+  auto r = TimedOp([&] {
+    return table->project(table->context, grid->view(), dt, problem,
                           MacPressureSolverOptions3D{max_iterations, tolerance_scale}, *ws);
+  });
   if (!r.ok()) return Code(r.status());
   std::memcpy(pressure, r->cell_pressures.data(), r->cell_pressures.size_bytes());
   std::memcpy(corrected_u, r->corrected_face_velocities.data(), r->corrected_face_velocities.size_bytes());
@@ -344,7 +362,7 @@ int bk_links(int which, const double origin[3], double h, const int32_t* blocks,
   pf.wetted_piston_face_fluxes = wet;
   pf.air_cell_pressures = air;
   pf.internal_interfaces = itf;
-  auto r = table->links(table->context, geometry, pf, *ws);
+  auto r = TimedOp([&] { return table->links(table->context, geometry, pf, *ws); });
   if (!r.ok()) return Code(r.status());
   for (uint64_t i = 0; i < nc; ++i) {
     const auto& c = r->cells[i];
@@ -411,7 +429,7 @@ int bk_freeze(int which, const double origin[3], double h, const int32_t* blocks
   LiquidBoundaryGeometryViewInputs3D in{grid->view(), cells, centers, corners, obstacle, step_duration, density,
                                         sigma};
   if (exact_curvature == exact_curvature) in.exact_outward_interface_curvature = exact_curvature;
-  auto r = table->freeze(table->context, in, *ws);
+  auto r = TimedOp([&] { return table->freeze(table->context, in, *ws); });
   if (!r.ok()) return Code(r.status());
   *ncells_out = r->cells.size();
   for (std::size_t i = 0; i < r->cells.size(); ++i) {
@@ -462,6 +480,9 @@ int bk_filled(int which, uint32_t* mask) {
     if (ops[k]) *mask |= 1u << k;
   return 0;
 }
+
+// Host time of the last table operation, ms.
+double bk_last_op_ms() { return g_last_op_ms; }
 
 // Drops the B200 table's backend (its device storage) before the process exits.
 void bk_release() { B200().reset(); }

@@ -74,6 +74,13 @@ def _d3(v):
     return (ctypes.c_double * 3)(*[float(x) for x in v])
 
 
+def last_op_ms() -> float:
+    """Host time of the harness's last table operation alone, ms."""
+    f = lib().bk_last_op_ms
+    f.restype = ctypes.c_double
+    return float(f())
+
+
 def filled(which):
     m = ctypes.c_uint32(0)
     code = lib().bk_filled(ctypes.c_int(which), ctypes.byref(m))

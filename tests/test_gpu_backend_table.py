@@ -369,3 +369,44 @@ def test_freeze_then_links_on_device_match_the_cpu_pipeline(obstacle):
     assert c0 == 0 and c1 == 0
     assert np.array_equal(cells1, cells0) and np.array_equal(faces1, faces0, equal_nan=True) and low1 == low0
     assert (faces0[:, 0] == 2).sum() > 50  # free-surface links with their theta distances
+
+
+def test_operation_times_against_the_cpu_table(scene, one_sided, histories):
+    """Each operation of both tables timed on the host clock around the table
+    call alone (the B200 call includes its uploads, kernels, downloads and
+    record conversion; the harness's own set-up is excluded), median of 15
+    after 3 warm-up calls; printed for the record. The B200 table must not be
+    slower than the CPU table on the operations whose work grows with the
+    scene (deposit, gather, freeze, project)."""
+
+    box, system, dt = _dam_break_system()
+    q = bt.deposit(CPU, scene)[1]
+    ls = bt.LinkScene()
+    fs = bt.FreezeScene("tank")
+    ops = {
+        "deposit (1024 particles)": lambda w: bt.deposit(w, scene),
+        "normalize (15360 faces)": lambda w: bt.normalize(w, q, 0.1 * float(scene.particles["mass"][0])),
+        "forces (15360 faces)": lambda w: bt.forces(w, one_sided, histories["old"][0]),
+        "gather (1024 particles)": lambda w: bt.gather(w, one_sided, histories["old"], histories["new"]),
+        "freeze (tank, 1296 candidates)": lambda w: bt.freeze(w, fs),
+        "links (864 cells, 2880 faces)": lambda w: bt.links(w, ls),
+        "project (3375 cells, to the gate)": lambda w: bt.project(w, system, box.h, dt),
+    }
+    rows = {}
+    for name, op in ops.items():
+        med = []
+        for which in (CPU, B200):
+            for _ in range(3):
+                assert op(which)[0] == 0
+            t = []
+            for _ in range(15):
+                op(which)
+                t.append(bt.last_op_ms())
+            med.append(float(np.median(t)))
+        rows[name] = med
+    print("\noperation | CPU table ms | B200 table ms | ratio")
+    for name, (c, g) in rows.items():
+        print(f"{name} | {c:.3f} | {g:.3f} | {c / g:.1f}x")
+    for name in ("deposit", "gather", "freeze", "project"):
+        c, g = next(v for k, v in rows.items() if k.startswith(name))
+        assert g <= c, (name, c, g)
