@@ -341,6 +341,97 @@ struct B200BackendOps3D {
                                               bound};
   }
 
+  // ComputeWettedPiston3D (wetted_piston_3d.cc:570-575): the view borrows
+  // this backend's piston bank.
+  static absl::StatusOr<WettedPistonView3D> WettedPiston(
+      void* context,
+      const WettedPistonInputs3D& inputs,
+      WettedPistonWorkspace3D&
+  ) {
+    auto& self = Self(context);
+    const auto& frozen = inputs.frozen;
+    const std::size_t nc = frozen.cells.size(), nf = frozen.faces.size(), np = inputs.particles.size();
+    if (nf > kFaces || nc > kPressureCells || np > kParticles) return Code(absl::StatusCode::kResourceExhausted);
+    auto& st = self.piston_staging_;
+    st.faces.resize(nf);
+    for (std::size_t f = 0; f < nf; ++f) {
+      const FrozenLiquidFace3D& face = frozen.faces[f];
+      fl_frozen_face& o = st.faces[f];
+      o = fl_frozen_face{};
+      o.axis = static_cast<std::int32_t>(face.face_index.axis);
+      o.lattice[0] = face.face_index.lattice_index.x;
+      o.lattice[1] = face.face_index.lattice_index.y;
+      o.lattice[2] = face.face_index.lattice_index.z;
+      o.face_slot = face.face_slot;
+      o.open_area = face.open_area;
+      o.blocked_area = face.blocked_area;
+      o.wall_normal_velocity = face.wall_normal_velocity;
+      o.has_prescribed_wall_flux = face.prescribed_wall_flux.has_value();
+      o.prescribed_wall_flux = face.prescribed_wall_flux.value_or(0.0);
+      o.is_low_x_piston_face = face.is_low_x_piston_face;
+    }
+    st.positions.resize(3 * np);
+    for (std::size_t i = 0; i < np; ++i) {
+      st.positions[3 * i] = inputs.particles[i].world_position.x;
+      st.positions[3 * i + 1] = inputs.particles[i].world_position.y;
+      st.positions[3 * i + 2] = inputs.particles[i].world_position.z;
+    }
+    fl_piston_field field{};
+    field.kind = -1;  // the covariance drop: not a piston field
+    if (const auto* sphere = std::get_if<LiquidAnalyticSphere3D>(&inputs.field)) {
+      field.kind = FL_PISTON_FIELD_SPHERE;
+      field.sphere_center[0] = sphere->world_center.x;
+      field.sphere_center[1] = sphere->world_center.y;
+      field.sphere_center[2] = sphere->world_center.z;
+      field.radius = sphere->radius;
+    } else if (const auto* u = std::get_if<LiquidParticleSphereUnion3D>(&inputs.field)) {
+      field.kind = FL_PISTON_FIELD_PARTICLE_UNION;
+      field.radius = u->radius;
+    } else if (const auto* plane = std::get_if<LiquidHorizontalPlaneSurface3D>(&inputs.field)) {
+      field.kind = FL_PISTON_FIELD_PLANE;
+      field.plane_height_y = plane->world_surface_height_y;
+    }
+    const double tank[6] = {inputs.tank.start_low_x, inputs.tank.high_x, inputs.tank.floor_y,
+                            inputs.tank.low_z,       inputs.tank.high_z, inputs.tank.piston_velocity_x};
+    st.patches.resize(kFaces);
+    st.fluxes.resize(nf);
+    st.has_flux.resize(nf);
+    const fl_owned_grid grid = OwnedGrid(frozen.mac_grid);
+    std::uint64_t count = 0, attached = 0;
+    double whole_area[2], whole_flux[2];
+    fl_measurement measured{};
+    const int code = fl_boundary_wetted_piston(
+        self.boundary_, &grid, reinterpret_cast<const fl_frozen_cell*>(frozen.cells.data()), nc, st.faces.data(), nf,
+        &field, st.positions.data(), np, tank, st.patches.data(), st.patches.size(), &count, st.fluxes.data(),
+        st.has_flux.data(), whole_area, whole_flux, &attached, &measured);
+    if (code != FL_OK) return FromFl(code);
+    auto& bank = self.pistons_[1 - self.piston_bank_];
+    bank.patches.resize(count);
+    for (std::size_t k = 0; k < count; ++k) {
+      const fl_piston_patch& o = st.patches[k];
+      WettedPistonPatch3D p{};
+      p.lattice_y = o.lattice_y;
+      p.lattice_z = o.lattice_z;
+      p.area = {o.area[0], o.area[1]};
+      if (o.has_receiver) p.receiver_face_ordinal = static_cast<std::size_t>(o.receiver_face_ordinal);
+      p.receiver_area = {o.receiver_area[0], o.receiver_area[1]};
+      p.receiver_flux = {o.receiver_flux[0], o.receiver_flux[1]};
+      bank.patches[k] = p;
+    }
+    bank.face_fluxes.resize(nf);
+    for (std::size_t f = 0; f < nf; ++f)
+      bank.face_fluxes[f] = st.has_flux[f] ? std::optional<double>(st.fluxes[f]) : std::nullopt;
+    self.piston_bank_ = 1 - self.piston_bank_;
+    WettedPistonView3D view{};
+    view.patches = bank.patches;
+    view.face_fluxes = bank.face_fluxes;
+    view.whole_area = {whole_area[0], whole_area[1]};
+    view.whole_flux = {whole_flux[0], whole_flux[1]};
+    view.attached_patch_count = attached;
+    view.compiled_architecture = measured.compiled_architecture;
+    return view;
+  }
+
   static absl::StatusOr<LiquidPressureProblemView3D> Links(
       void* context,
       const FrozenLiquidBoundaryGeometryView3D& geometry,
@@ -619,6 +710,11 @@ absl::StatusOr<std::unique_ptr<B200LiquidBackend3D>> B200LiquidBackend3D::Create
          Reserve(self->frozen_[k].centers, 27 * kPressureCells) && Reserve(self->frozen_[k].cells, kPressureCells) &&
          Reserve(self->frozen_[k].faces, kFaces);
   ok = ok && Reserve(self->freeze_staging_.faces, 6 * kPressureCells);
+  for (int k = 0; k < 2; ++k)
+    ok = ok && Reserve(self->pistons_[k].patches, kFaces) && Reserve(self->pistons_[k].face_fluxes, kFaces);
+  auto& ps = self->piston_staging_;
+  ok = ok && Reserve(ps.faces, kFaces) && Reserve(ps.positions, 3 * kParticles) && Reserve(ps.patches, kFaces) &&
+       Reserve(ps.fluxes, kFaces) && Reserve(ps.has_flux, kFaces);
   auto& ls = self->link_staging_;
   ok = ok && Reserve(ls.faces, kFaces) && Reserve(ls.fields, kPressureCells) && Reserve(ls.wetted, kFaces) &&
        Reserve(ls.has_wetted, kFaces) && Reserve(ls.cells_out, kPressureCells) && Reserve(ls.faces_out, kFaces);
@@ -649,6 +745,7 @@ LiquidSubstepBackend3D B200LiquidBackend3D::operations() {
   table.forces = &B200BackendOps3D::Forces;
   table.gather = &B200BackendOps3D::Gather;
   table.freeze = &B200BackendOps3D::Freeze;
+  table.wetted_piston = &B200BackendOps3D::WettedPiston;
   table.links = &B200BackendOps3D::Links;
   table.project = &B200BackendOps3D::Project;
   return table;

@@ -14,12 +14,13 @@
 //   .freeze                fl_boundary_freeze         (FreezeLiquidBoundaryGeometry3D: no obstacle,
 //                                                      halfspace, slab or open tank; sampled
 //                                                      solids return kUnimplemented)
+//   .wetted_piston         fl_boundary_wetted_piston  (ComputeWettedPiston3D)
 //   .links                 fl_boundary_links          (BuildLiquidPressureLinks3D)
 //   .project               fl_boundary_project        (ProjectMacPressure3D over a pressure problem)
 //   .initialize, publication and growth hooks: no device state outlives a call
 //
 // The scene-geometry, topology and particle-update operations (.sample_*,
-// .topology, .wetted_piston, .project_viscous, .update_particles)
+// .topology, .project_viscous, .update_particles)
 // are outside this library and stay null: the scheduler's
 // Create rejects a scene that needs them, and no CPU callback is substituted.
 //
@@ -35,6 +36,7 @@
 #include <vector>
 
 #include "fluidity/host/liquid_substep_backend_3d.h"
+#include "fluidity/host/wetted_piston_3d.h"
 #include "fluidity_b200.h"
 
 namespace fluidity {
@@ -69,6 +71,18 @@ class B200LiquidBackend3D {
   struct LinkBank {
     std::vector<MacPressureCell3D> cells;
     std::vector<MacPressureFace3D> faces;
+  };
+  struct PistonBank {
+    std::vector<WettedPistonPatch3D> patches;
+    std::vector<std::optional<double>> face_fluxes;
+  };
+  // Host staging of the wetted piston's inputs and outputs in the C-ABI's layout.
+  struct PistonStaging {
+    std::vector<fl_frozen_face> faces;
+    std::vector<double> positions;
+    std::vector<fl_piston_patch> patches;
+    std::vector<double> fluxes;
+    std::vector<std::uint8_t> has_flux;
   };
   struct FreezeBank {
     std::vector<LiquidCenterDistance3D> centers;
@@ -107,11 +121,13 @@ class B200LiquidBackend3D {
   ProjectionBank projections_[2];
   LinkBank links_[2];
   FreezeBank frozen_[2];
+  PistonBank pistons_[2];
+  PistonStaging piston_staging_;
   PressureStaging staging_;
   LinkStaging link_staging_;
   FreezeStaging freeze_staging_;
   int deposit_bank_ = 0, normalize_bank_ = 0, gather_bank_ = 0, projection_bank_ = 0, links_bank_ = 0,
-      frozen_bank_ = 0;
+      frozen_bank_ = 0, piston_bank_ = 0;
 };
 
 }  // namespace fluidity

@@ -1127,6 +1127,8 @@ struct fl_boundary {
   char* lpin = nullptr;    // and its pinned mirror
   char* fdev = nullptr;    // geometry freeze: device arena
   char* fpin = nullptr;    // and its pinned mirror
+  char* pdev = nullptr;    // wetted piston: device arena
+  char* ppin = nullptr;    // and its pinned mirror (all but the interval banks)
 };
 
 namespace {
@@ -1267,6 +1269,8 @@ namespace {
 size_t link_arena_bytes();  // the pressure-link assembly's staging, defined with its regions below
 }  // namespace
 size_t freeze_arena_bytes();  // the geometry freeze's staging, likewise
+size_t piston_arena_bytes();  // the wetted piston's device arena
+size_t piston_pinned_bytes();  // and its staged part
 
 extern "C" int fl_boundary_create(fl_boundary** out) {
   if (!out) return FL_INVALID_ARGUMENT;
@@ -1282,7 +1286,9 @@ extern "C" int fl_boundary_create(fl_boundary** out) {
             cudaMalloc(&b->ldev, link_arena_bytes()) == cudaSuccess &&
             cudaMallocHost(&b->lpin, link_arena_bytes()) == cudaSuccess &&
             cudaMalloc(&b->fdev, freeze_arena_bytes()) == cudaSuccess &&
-            cudaMallocHost(&b->fpin, freeze_arena_bytes()) == cudaSuccess;
+            cudaMallocHost(&b->fpin, freeze_arena_bytes()) == cudaSuccess &&
+            cudaMalloc(&b->pdev, piston_arena_bytes()) == cudaSuccess &&
+            cudaMallocHost(&b->ppin, piston_pinned_bytes()) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     fl_boundary_destroy(b);
@@ -1297,6 +1303,8 @@ extern "C" int fl_boundary_destroy(fl_boundary* b) {
   if (b->device >= 0) cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   b->pressure.destroy();
+  if (b->ppin) cudaFreeHost(b->ppin);
+  if (b->pdev) cudaFree(b->pdev);
   if (b->fpin) cudaFreeHost(b->fpin);
   if (b->fdev) cudaFree(b->fdev);
   if (b->lpin) cudaFreeHost(b->lpin);
@@ -2145,7 +2153,7 @@ struct SumResidual {
 };
 
 // FastTwoSum with the larger magnitude first.
-__device__ SumResidual add_with_residual(double a, double b) {
+__host__ __device__ SumResidual add_with_residual(double a, double b) {
   if (fabs(a) < fabs(b)) {
     const double t = a;
     a = b;
@@ -2156,18 +2164,18 @@ __device__ SumResidual add_with_residual(double a, double b) {
   return {s, b - (s - a)};
 }
 
-__device__ double add_down(double a, double b) {
+__host__ __device__ double add_down(double a, double b) {
   const SumResidual s = add_with_residual(a, b);
   return s.residual < 0 ? nextafter(s.value, -kInf) : s.value;
 }
 
-__device__ double add_up(double a, double b) {
+__host__ __device__ double add_up(double a, double b) {
   const SumResidual s = add_with_residual(a, b);
   return s.residual > 0 ? nextafter(s.value, kInf) : s.value;
 }
 
 // Midpoint without overflow, correctly rounded (the P0811 formulation).
-__device__ double midpoint(double a, double b) {
+__host__ __device__ double midpoint(double a, double b) {
   const double lo = DBL_MIN * 2, hi = DBL_MAX / 2;
   const double aa = a < 0 ? -a : a, ab = b < 0 ? -b : b;
   if (aa <= hi && ab <= hi) return (a + b) / 2;
@@ -2184,7 +2192,7 @@ struct OffsetBounds {
 // the sign of a tank plane's offset from a lattice plane can be certified.
 struct CertifiedSum {
   double sum = 0.0, lower = 0.0, upper = 0.0;
-  __device__ void correct(double c) {
+  __host__ __device__ void correct(double c) {
     if (!isfinite(lower) || !isfinite(upper)) {
       sum = kInf;
       return;
@@ -2192,7 +2200,7 @@ struct CertifiedSum {
     lower = add_down(lower, c);
     upper = add_up(upper, c);
   }
-  __device__ void add(double term) {
+  __host__ __device__ void add(double term) {
     if (!isfinite(sum) || !isfinite(term)) {
       sum = kInf;
       return;
@@ -2201,7 +2209,7 @@ struct CertifiedSum {
     sum = s.value;
     correct(s.residual);
   }
-  __device__ void add_product(double l, double r) {
+  __host__ __device__ void add_product(double l, double r) {
     const double product = l * r;
     add(product);
     if (isfinite(product) && l != 0 && r != 0 && fabs(l) != 1 && fabs(r) != 1) {
@@ -2213,7 +2221,7 @@ struct CertifiedSum {
       }
     }
   }
-  __device__ OffsetBounds bounds() const {
+  __host__ __device__ OffsetBounds bounds() const {
     if (!isfinite(sum) || !isfinite(lower) || !isfinite(upper)) return {kInf, kInf, kInf};
     return {sum + midpoint(lower, upper), add_down(sum, lower), add_up(sum, upper)};
   }
@@ -2221,7 +2229,7 @@ struct CertifiedSum {
 
 constexpr int kSignUnresolved = 2;
 
-__device__ int certified_sign(const OffsetBounds& b) {
+__host__ __device__ int certified_sign(const OffsetBounds& b) {
   if (!isfinite(b.estimate) || !isfinite(b.lower) || !isfinite(b.upper)) return kSignUnresolved;
   if (b.lower > 0) return 1;
   if (b.upper < 0) return -1;
@@ -2230,7 +2238,7 @@ __device__ int certified_sign(const OffsetBounds& b) {
 }
 
 // world - (origin + h * index), exactly enough to certify its sign.
-__device__ CertifiedSum tank_plane_offset(double world, double origin, double index, double h) {
+__host__ __device__ CertifiedSum tank_plane_offset(double world, double origin, double index, double h) {
   CertifiedSum o;
   o.add(world);
   o.add(-origin);
@@ -2238,7 +2246,7 @@ __device__ CertifiedSum tank_plane_offset(double world, double origin, double in
   return o;
 }
 
-__device__ int tank_plane_sign(double world, double origin, double index, double h, int* sign) {
+__host__ __device__ int tank_plane_sign(double world, double origin, double index, double h, int* sign) {
   const double translated = world - origin;
   if (isinf(translated)) {
     *sign = translated > 0 ? 1 : -1;
@@ -2250,7 +2258,7 @@ __device__ int tank_plane_sign(double world, double origin, double index, double
 
 // The plane's coordinate in the cell's unit frame: 0 at or below the low
 // face, 1 at or beyond the high face, else the interior cut.
-__device__ int tank_clip_coordinate(double world, double origin, double index, double h, double* out) {
+__host__ __device__ int tank_clip_coordinate(double world, double origin, double index, double h, double* out) {
   const double translated = world - origin;
   if (isinf(translated)) {
     *out = translated > 0 ? 1.0 : 0.0;
@@ -3093,5 +3101,688 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
   *face_count = nfaces;
   *capillary_step_bound = bound;
   finish_measure();
+  return FL_OK;
+}
+
+// ---- wetted piston (.wetted_piston) ----
+//
+// ComputeWettedPiston3D (wetted_piston_3d.cc:342-566) with the enclosure
+// arithmetic of base/wetted_piston_math_3d.h: the wet area of the open tank's
+// low-x piston, patch by lattice patch, under the liquid field (a horizontal
+// plane, an analytic sphere or a union of particle spheres), as outward-rounded
+// [lower, upper] bounds, and the signed fluxes handed to the piston's receiver
+// faces. The device computes the spheres' sections on the piston plane (one
+// thread per source) and each patch's banded area integral (one thread per
+// patch); the host enumerates the patches, finds the receivers and assigns the
+// patches in the reference's order.
+namespace fl {
+namespace {
+
+struct WBounds {
+  double lower = 0.0, upper = 0.0;
+};
+
+__host__ __device__ inline double smax(double a, double b) { return a < b ? b : a; }
+__host__ __device__ inline double smin(double a, double b) { return b < a ? b : a; }
+__host__ __device__ inline bool wfinite(WBounds b) { return isfinite(b.lower) && isfinite(b.upper) && b.lower <= b.upper; }
+__host__ __device__ inline WBounds wpoint(double v) { return {v, v}; }
+__host__ __device__ inline WBounds wadd(WBounds a, WBounds b) {
+  return {add_down(a.lower, b.lower), add_up(a.upper, b.upper)};
+}
+__host__ __device__ inline WBounds wneg(WBounds a) { return {-a.upper, -a.lower}; }
+__host__ __device__ inline WBounds wsub(WBounds a, WBounds b) { return wadd(a, wneg(b)); }
+
+// A rounded result moved one double outward when its exact residual lies
+// outward (or could have underflowed to zero).
+__host__ __device__ inline double directed(double rounded, double residual, double scale, bool up) {
+  if (!isfinite(rounded)) return rounded;
+  const bool uncertain = residual == 0 && fabs(scale) <= 0x1p-969;
+  if (uncertain || (up ? residual > 0 : residual < 0)) return nextafter(rounded, up ? kInf : -kInf);
+  return rounded;
+}
+
+__host__ __device__ inline double directed_product(double a, double b, bool up) {
+  const double p = a * b;
+  if (a == 0 || b == 0 || fabs(a) == 1 || fabs(b) == 1 || !isfinite(p)) return p;
+  return directed(p, fma(a, b, -p), p, up);
+}
+
+__host__ __device__ inline WBounds wmul_nonneg(WBounds a, WBounds b) {
+  return {smax(0.0, directed_product(a.lower, b.lower, false)), directed_product(a.upper, b.upper, true)};
+}
+
+__host__ __device__ inline WBounds area_to_flux(WBounds area, double v) {
+  const WBounds m = wmul_nonneg(area, wpoint(fabs(v)));
+  return v < 0 ? wneg(m) : m;
+}
+
+__host__ __device__ inline double directed_quotient(double value, double divisor, bool up) {
+  const double q = value / divisor;
+  if (value == 0 || divisor == 1 || !isfinite(q)) return q;
+  return directed(q, fma(-q, divisor, value), value, up);
+}
+
+__host__ __device__ inline WBounds wdiv(WBounds a, double d) {
+  return {directed_quotient(a.lower, d, false), directed_quotient(a.upper, d, true)};
+}
+
+__host__ __device__ inline double directed_root(double v, bool up) {
+  if (v <= 0) return 0.0;
+  const double r = sqrt(v);
+  return smax(0.0, directed(r, fma(-r, r, v), v, up));
+}
+
+__host__ __device__ inline WBounds wroot(WBounds a) { return {directed_root(a.lower, false), directed_root(a.upper, true)}; }
+__host__ __device__ inline WBounds wmax(WBounds a, WBounds b) { return {smax(a.lower, b.lower), smax(a.upper, b.upper)}; }
+__host__ __device__ inline WBounds wmin(WBounds a, WBounds b) { return {smin(a.lower, b.lower), smin(a.upper, b.upper)}; }
+__host__ __device__ inline WBounds wmag(WBounds a) {
+  return {smax(0.0, smax(a.lower, -a.upper)), smax(a.upper, -a.lower)};
+}
+__host__ __device__ inline WBounds wsquare(WBounds a) {
+  const WBounds m = wmag(a);
+  return wmul_nonneg(m, m);
+}
+
+// (world - origin) / h - index as an enclosure, in cell widths.
+__host__ __device__ inline WBounds lattice_offset(double world, double origin, double index, double h) {
+  const OffsetBounds b = tank_plane_offset(world, origin, index, h).bounds();
+  if (!isfinite(b.estimate) || !isfinite(b.lower) || !isfinite(b.upper)) return {kInf, kInf};
+  return wdiv({b.lower, b.upper}, h);
+}
+
+struct PistonField {
+  double origin[3], h;
+  double tank[6];  // start low x, high x, floor y, low z, high z, piston velocity x
+  double radius;   // sphere radius (m)
+  double plane_y;  // plane height (m)
+  int is_plane;
+};
+
+// A sphere's section by the piston plane, in cell widths (radius squared
+// zero: the sphere misses the plane).
+struct PistonDisk {
+  WBounds y, z, r2;
+  int status;
+};
+
+__host__ __device__ inline PistonDisk piston_section(const PistonField& f, const double c[3]) {
+  PistonDisk d{};
+  d.status = FL_OK;
+  const double h = f.h;
+  const WBounds dist = wmag(wsub(wpoint(c[0]), wpoint(f.tank[0])));
+  if (!wfinite(dist)) {
+    d.status = FL_OUT_OF_RANGE;
+    return d;
+  }
+  if (dist.lower >= f.radius) return d;
+  const WBounds R = wpoint(f.radius);
+  const WBounds less = wmax(wpoint(0.0), wsub(R, dist));
+  const WBounds more = wadd(wdiv(R, h), wdiv(dist, h));
+  const WBounds r2 = wmul_nonneg(wdiv(less, h), more);
+  const WBounds cy = lattice_offset(c[1], f.origin[1], 0.0, h), cz = lattice_offset(c[2], f.origin[2], 0.0, h);
+  if (!wfinite(r2) || !wfinite(cy) || !wfinite(cz) || r2.upper <= 0) {
+    d.status = FL_OUT_OF_RANGE;
+    return d;
+  }
+  d.y = cy;
+  d.z = cz;
+  d.r2 = r2;
+  return d;
+}
+
+struct PistonInterval {
+  double low, high;
+};
+
+__host__ __device__ inline bool interval_less(PistonInterval a, PistonInterval b) {
+  return a.low < b.low || (a.low == b.low && a.high < b.high);
+}
+
+__host__ __device__ inline void sift(PistonInterval* v, size_t count, size_t root) {
+  while (root < count / 2) {
+    size_t child = root * 2 + 1;
+    if (child + 1 < count && interval_less(v[child], v[child + 1])) ++child;
+    if (!interval_less(v[root], v[child])) break;
+    const PistonInterval t = v[root];
+    v[root] = v[child];
+    v[child] = t;
+    root = child;
+  }
+}
+
+// Length of a union of intervals (heap sort, then a sweep), lower or upper bound.
+__host__ __device__ inline double union_length(PistonInterval* v, size_t count, bool upper) {
+  if (count == 0) return 0.0;
+  for (size_t start = count / 2; start > 0; --start) sift(v, count, start - 1);
+  for (size_t end = count - 1; end > 0; --end) {
+    const PistonInterval t = v[0];
+    v[0] = v[end];
+    v[end] = t;
+    sift(v, end, 0);
+  }
+  WBounds length;
+  PistonInterval cur = v[0];
+  for (size_t k = 1; k < count; ++k) {
+    const PistonInterval nx = v[k];
+    if (nx.low <= cur.high) {
+      cur.high = smax(cur.high, nx.high);
+      continue;
+    }
+    length = wadd(length, wsub(wpoint(cur.high), wpoint(cur.low)));
+    cur = nx;
+  }
+  length = wadd(length, wsub(wpoint(cur.high), wpoint(cur.low)));
+  return upper ? length.upper : length.lower;
+}
+
+__host__ __device__ inline WBounds world_area(WBounds lattice_area, double h) {
+  return wmul_nonneg(wmul_nonneg(lattice_area, wpoint(h)), wpoint(h));
+}
+
+__host__ __device__ inline WBounds width_of(WBounds lo, WBounds hi) { return wmax(wpoint(0.0), wsub(hi, lo)); }
+__host__ __device__ inline WBounds nearest_of(WBounds c, WBounds lo, WBounds hi) {
+  return wmax(wpoint(0.0), wmax(wsub(lo, c), wsub(c, hi)));
+}
+__host__ __device__ inline WBounds farthest_of(WBounds c, WBounds lo, WBounds hi) {
+  return wmax(wmag(wsub(c, lo)), wmag(wsub(c, hi)));
+}
+__host__ __device__ inline WBounds gap_of(WBounds r2, WBounds dy, WBounds dz) {
+  return wsub(wsub(r2, wsquare(dy)), wsquare(dz));
+}
+
+struct PatchResult {
+  WBounds area;
+  double midpoint_flux;
+  int cross_lower;  // every wet source crosses the patch's lower edge
+  int status;
+};
+
+constexpr int kPistonBands = 64;
+
+// IntegratePatch + MeasurePatch (wetted_piston_math_3d.h:280-424): the wet
+// area of patch (py, pz) as an enclosure, by 64 z-bands of interval unions.
+__host__ __device__ inline PatchResult measure_patch(const PistonField& f, int32_t py, int32_t pz,
+                                                     const PistonDisk* disks, size_t nd, PistonInterval* inner,
+                                                     PistonInterval* outer) {
+  PatchResult m{};
+  m.cross_lower = 1;
+  m.status = FL_OK;
+  // every successful measure carries the midpoint of its area times the piston velocity
+  auto finish = [&f](PatchResult& r) {
+    if (r.status != FL_OK) return r;
+    r.midpoint_flux = midpoint(r.area.lower, r.area.upper) * f.tank[5];
+    if (!isfinite(r.midpoint_flux)) r.status = FL_OUT_OF_RANGE;
+    return r;
+  };
+  const double h = f.h;
+  const WBounds floor_ = lattice_offset(f.tank[2], f.origin[1], (double)py, h);
+  const WBounds low_z = lattice_offset(f.tank[3], f.origin[2], (double)pz, h);
+  const WBounds high_z = lattice_offset(f.tank[4], f.origin[2], (double)pz, h);
+  const WBounds surface = f.is_plane ? lattice_offset(f.plane_y, f.origin[1], (double)py, h) : wpoint(1.0);
+  if (!wfinite(floor_) || !wfinite(low_z) || !wfinite(high_z) || !wfinite(surface)) {
+    m.status = FL_OUT_OF_RANGE;
+    return m;
+  }
+  const WBounds rlo_y = wmax(wpoint(0.0), floor_), rhi_y = wmin(wpoint(1.0), surface);
+  const WBounds rlo_z = wmax(wpoint(0.0), low_z), rhi_z = wmin(wpoint(1.0), high_z);
+  const WBounds yw = width_of(rlo_y, rhi_y), zw = width_of(rlo_z, rhi_z);
+  if (yw.upper == 0 || zw.upper == 0) return finish(m);
+  const WBounds rect = wmul_nonneg(yw, zw);
+  if (f.is_plane) {
+    m.area = world_area(rect, h);
+    m.cross_lower = floor_.upper <= 0 && surface.lower > 0 && zw.lower > 0;
+    if (!wfinite(m.area)) m.status = FL_OUT_OF_RANGE;
+  } else {
+    bool cross = floor_.upper <= 0 && zw.lower > 0;
+    bool wet = false;
+    for (size_t k = 0; k < nd; ++k) {
+      const PistonDisk& d = disks[k];
+      if (d.r2.upper == 0) continue;
+      const WBounds y = wsub(d.y, wpoint((double)py)), z = wsub(d.z, wpoint((double)pz));
+      const WBounds ny = nearest_of(y, rlo_y, rhi_y), nz = nearest_of(z, rlo_z, rhi_z);
+      const WBounds pg = gap_of(d.r2, ny, nz);
+      if (!wfinite(pg)) {
+        m.status = FL_OUT_OF_RANGE;
+        return m;
+      }
+      if (pg.upper <= 0) continue;
+      wet = true;
+      const WBounds eg = gap_of(d.r2, wmag(y), nz);
+      if (!wfinite(eg)) {
+        m.status = FL_OUT_OF_RANGE;
+        return m;
+      }
+      cross = cross && eg.lower > 0;
+    }
+    if (!wet) return finish(m);
+    WBounds area;
+    for (int band = 0; band < kPistonBands; ++band) {
+      const WBounds blo = wmax(rlo_z, wpoint((double)band / kPistonBands));
+      const WBounds bhi = wmin(rhi_z, wpoint((double)(band + 1) / kPistonBands));
+      const WBounds bw = width_of(blo, bhi);
+      if (bw.upper == 0) continue;
+      size_t ni = 0, no = 0;
+      for (size_t k = 0; k < nd; ++k) {
+        const PistonDisk& d = disks[k];
+        if (d.r2.upper == 0) continue;
+        const WBounds z = wsub(d.z, wpoint((double)pz));
+        const WBounds near2 = wsquare(nearest_of(z, blo, bhi)), far2 = wsquare(farthest_of(z, blo, bhi));
+        const WBounds outer2 = wsub(d.r2, near2), inner2 = wsub(d.r2, far2);
+        if (!wfinite(outer2) || !wfinite(inner2)) {
+          m.status = FL_OUT_OF_RANGE;
+          return m;
+        }
+        if (outer2.upper <= 0) continue;
+        const WBounds y = wsub(d.y, wpoint((double)py));
+        const double ro = directed_root(outer2.upper, true);
+        const double olo = wmax(rlo_y, wsub(y, wpoint(ro))).lower;
+        const double ohi = wmin(rhi_y, wadd(y, wpoint(ro))).upper;
+        if (olo < ohi) outer[no++] = {olo, ohi};
+        if (inner2.lower > 0) {
+          const double ri = directed_root(inner2.lower, false);
+          const double ilo = wmax(rlo_y, wsub(y, wpoint(ri))).upper;
+          const double ihi = wmin(rhi_y, wadd(y, wpoint(ri))).lower;
+          if (ilo < ihi) inner[ni++] = {ilo, ihi};
+        }
+      }
+      const WBounds len{union_length(inner, ni, false), union_length(outer, no, true)};
+      area = wadd(area, wmul_nonneg(len, bw));
+    }
+    m.area = world_area(wmin(area, rect), h);
+    m.cross_lower = cross;
+    if (!wfinite(m.area)) m.status = FL_OUT_OF_RANGE;
+  }
+  return finish(m);
+}
+
+__global__ void k_piston_sections(PistonField f, const double* centers, int n, PistonDisk* disks, int* arch) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *arch = compiled_arch();
+  if (i < n) disks[i] = piston_section(f, centers + 3 * i);
+}
+
+// Patches strided over the launched threads; each thread sorts its intervals
+// in its own two banks of nd records.
+__global__ void k_piston_patches(PistonField f, const PistonDisk* disks, int nd, const int32_t* patches, int np,
+                                 PistonInterval* banks, PatchResult* out) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  const int slots = gridDim.x * blockDim.x;
+  PistonInterval* inner = banks + (size_t)slot * 2 * (nd > 0 ? nd : 1);
+  PistonInterval* outer = inner + (nd > 0 ? nd : 1);
+  for (int p = slot; p < np; p += slots)
+    out[p] = measure_patch(f, patches[2 * p], patches[2 * p + 1], disks, (size_t)nd, inner, outer);
+}
+
+}  // namespace
+}  // namespace fl
+
+namespace {
+
+constexpr int kPistonSlots = 256;  // threads measuring patches at once, each with two interval banks
+
+struct PistonRegions {
+  size_t centers, disks, patches, results, arch, staged, banks, total;
+  PistonRegions() {
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+      const size_t r = o;
+      o = align_up(o + bytes);
+      return r;
+    };
+    centers = take(sizeof(double) * 3 * kMaxParticles);
+    disks = take(sizeof(PistonDisk) * kMaxParticles);
+    patches = take(sizeof(int32_t) * 2 * kMaxFaces);
+    results = take(sizeof(PatchResult) * kMaxFaces);
+    arch = take(sizeof(int));
+    staged = o;
+    banks = take(sizeof(PistonInterval) * 2 * kPistonSlots * kMaxParticles);
+    total = o;
+  }
+};
+
+const PistonRegions kPistonRegions;
+
+}  // namespace
+
+size_t piston_arena_bytes() { return kPistonRegions.total; }
+size_t piston_pinned_bytes() { return kPistonRegions.staged; }
+
+namespace {
+
+constexpr int64_t kFirstLattice = INT32_MIN;
+constexpr int64_t kPastLastLattice = (int64_t)INT32_MAX + 1;
+
+// CheckTankStep (base/liquid_boundary_math.h:252-276).
+int check_tank(const double* t, double step) {
+  for (int k = 0; k < 6; ++k)
+    if (!std::isfinite(t[k])) return FL_INVALID_ARGUMENT;
+  if (t[0] >= t[1] || t[3] >= t[4]) return FL_INVALID_ARGUMENT;
+  const double displacement = t[5] * step;
+  const double end_x = std::fma(t[5], step, t[0]);
+  const double start_width = t[1] - t[0], end_width = t[1] - end_x, width_z = t[4] - t[3];
+  if (!std::isfinite(displacement) || !std::isfinite(end_x) || !std::isfinite(start_width) ||
+      !std::isfinite(end_width) || !std::isfinite(width_z))
+    return FL_OUT_OF_RANGE;
+  if (end_x >= t[1]) return FL_FAILED_PRECONDITION;
+  return FL_OK;
+}
+
+bool patch_less(const int32_t* a, const int32_t* b) { return a[1] != b[1] ? a[1] < b[1] : a[0] < b[0]; }
+
+// AddIndex (wetted_piston_3d.cc:131-149): a sorted, deduplicated (z, y) insert.
+int add_patch(std::vector<int32_t>& idx, int32_t y, int32_t z) {
+  const int32_t key[2] = {y, z};
+  size_t lo = 0, hi = idx.size() / 2;
+  while (lo < hi) {
+    const size_t mid = (lo + hi) / 2;
+    if (patch_less(&idx[2 * mid], key))
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo < idx.size() / 2 && idx[2 * lo] == y && idx[2 * lo + 1] == z) return FL_OK;
+  if (idx.size() / 2 == (size_t)kMaxFaces) return FL_RESOURCE_EXHAUSTED;
+  idx.insert(idx.begin() + 2 * lo, key, key + 2);
+  return FL_OK;
+}
+
+// AddRectangle (:158-186): every patch the rectangle (in cell widths) touches.
+int add_rectangle(std::vector<int32_t>& idx, double low_y, double high_y, double low_z, double high_z) {
+  if (!(low_y < high_y && low_z < high_z)) return FL_OK;
+  if (low_y < kFirstLattice || low_z < kFirstLattice || high_y > kPastLastLattice || high_z > kPastLastLattice)
+    return FL_OUT_OF_RANGE;
+  const int64_t fy = (int64_t)std::floor(low_y), fz = (int64_t)std::floor(low_z);
+  const int64_t ey = (int64_t)std::ceil(high_y), ez = (int64_t)std::ceil(high_z);
+  const uint64_t rows = (uint64_t)(ey - fy), cols = (uint64_t)(ez - fz);
+  if (rows > (uint64_t)kMaxFaces || cols > (uint64_t)kMaxFaces / rows) return FL_RESOURCE_EXHAUSTED;
+  for (int64_t z = fz; z < ez; ++z)
+    for (int64_t y = fy; y < ey; ++y) {
+      const int st = add_patch(idx, (int32_t)y, (int32_t)z);
+      if (st != FL_OK) return st;
+    }
+  return FL_OK;
+}
+
+}  // namespace
+
+extern "C" int fl_boundary_wetted_piston(fl_boundary* b, const fl_owned_grid* grid, const fl_frozen_cell* cells,
+                                         uint64_t nc, const fl_frozen_face* faces, uint64_t nf,
+                                         const fl_piston_field* field, const double* particles, uint64_t np,
+                                         const double tank[6], fl_piston_patch* patches, uint64_t patch_capacity,
+                                         uint64_t* patch_count, double* face_fluxes, uint8_t* has_face_flux,
+                                         double whole_area[2], double whole_flux[2], uint64_t* attached,
+                                         fl_measurement* m) {
+  if (!b || !field || !tank || !patch_count || !whole_area || !whole_flux || !attached ||
+      (nc && !cells) || (nf && (!faces || !face_fluxes || !has_face_flux)) || (np && !particles) ||
+      (patch_capacity && !patches))
+    return FL_INVALID_ARGUMENT;
+  int st = check_grid(grid);
+  if (st != FL_OK) return st;
+  // the workspace's capacities, then Run (wetted_piston_3d.cc:351-383)
+  if (nf > (uint64_t)kMaxFaces || nc > (uint64_t)kMaxLinkCells || np > (uint64_t)kMaxParticles)
+    return FL_RESOURCE_EXHAUSTED;
+  st = check_tank(tank, 0.0);
+  if (st != FL_OK) return st;
+  const double h = grid->h;
+  const WBounds nominal = world_area(wpoint(1.0), h);
+  if (!wfinite(nominal) || nominal.lower <= 0) return FL_OUT_OF_RANGE;
+  for (uint64_t f = 0; f < nf; ++f) {
+    const int64_t lat[3] = {faces[f].lattice[0], faces[f].lattice[1], faces[f].lattice[2]};
+    uint64_t slot = 0;
+    if (host_face_slot(grid, faces[f].axis, lat, &slot) != FL_OK || slot != faces[f].face_slot ||
+        (f > 0 && faces[f - 1].face_slot >= slot))
+      return FL_INVALID_ARGUMENT;
+  }
+  for (uint64_t i = 0; i < nc; ++i)
+    if (!std::isfinite(cells[i].fluid_volume) || cells[i].fluid_volume <= 0 ||
+        (i > 0 && !host_cell_less(cells[i - 1].cell_index, cells[i].cell_index)))
+      return FL_INVALID_ARGUMENT;
+  PistonField pf{};
+  for (int a = 0; a < 3; ++a) pf.origin[a] = grid->origin[a];
+  pf.h = h;
+  for (int k = 0; k < 6; ++k) pf.tank[k] = tank[k];
+  if (field->kind == FL_PISTON_FIELD_PLANE) {
+    pf.is_plane = 1;
+    pf.plane_y = field->plane_height_y;
+    if (!std::isfinite(pf.plane_y)) return FL_INVALID_ARGUMENT;
+  } else {
+    if (field->kind != FL_PISTON_FIELD_SPHERE && field->kind != FL_PISTON_FIELD_PARTICLE_UNION)
+      return FL_INVALID_ARGUMENT;
+    pf.radius = field->radius;
+    const double* c = field->sphere_center;
+    if (!std::isfinite(pf.radius) || pf.radius <= 0 ||
+        (field->kind == FL_PISTON_FIELD_SPHERE &&
+         !(std::isfinite(c[0]) && std::isfinite(c[1]) && std::isfinite(c[2]))))
+      return FL_INVALID_ARGUMENT;
+  }
+  for (uint64_t i = 0; i < np; ++i)
+    if (!std::isfinite(particles[3 * i]) || !std::isfinite(particles[3 * i + 1]) || !std::isfinite(particles[3 * i + 2]))
+      return FL_INVALID_ARGUMENT;
+  // FindPistonOwnerLatticeX (:102-129): the cell whose half-open x span holds the piston plane.
+  auto side = [&](int64_t index, int* sg) { return tank_plane_sign(tank[0], grid->origin[0], (double)index, h, sg); };
+  int64_t lo = kFirstLattice, hi = kPastLastLattice;
+  int lo_side = 0, hi_side = 0;
+  if (side(lo, &lo_side) != FL_OK || side(hi, &hi_side) != FL_OK || lo_side < 0 || hi_side >= 0)
+    return FL_OUT_OF_RANGE;
+  while (hi - lo > 1) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    int sg = 0;
+    if (side(mid, &sg) != FL_OK) return FL_OUT_OF_RANGE;
+    if (sg < 0)
+      hi = mid;
+    else
+      lo = mid;
+  }
+  const int32_t px = (int32_t)lo;
+  const double velocity = tank[5];
+  std::vector<int32_t> idx;
+  idx.reserve(2 * (size_t)kMaxFaces);
+  for (uint64_t i = 0; i < nc; ++i)
+    if (cells[i].cell_index[0] == px) {
+      st = add_patch(idx, cells[i].cell_index[1], cells[i].cell_index[2]);
+      if (st != FL_OK) return st;
+    }
+  // sections of the field's spheres by the piston plane
+  const PistonRegions& R = kPistonRegions;
+  const int sources = field->kind == FL_PISTON_FIELD_SPHERE ? 1 : (field->kind == FL_PISTON_FIELD_PARTICLE_UNION ? (int)np : 0);
+  if (cudaSetDevice(b->device) != cudaSuccess) return FL_INTERNAL;
+  double* centers = reinterpret_cast<double*>(b->ppin + R.centers);
+  if (field->kind == FL_PISTON_FIELD_SPHERE)
+    for (int a = 0; a < 3; ++a) centers[a] = field->sphere_center[a];
+  else if (sources > 0)
+    std::memcpy(centers, particles, sizeof(double) * 3 * sources);
+  float ms = 0.0f;
+  auto phase = [&](size_t qoff, size_t qbytes, size_t roff, size_t rbytes, auto launch) {
+    bool ok = cudaEventRecord(b->e0, b->stream) == cudaSuccess &&
+              (qbytes == 0 || cudaMemcpyAsync(b->pdev + qoff, b->ppin + qoff, qbytes, cudaMemcpyHostToDevice,
+                                              b->stream) == cudaSuccess);
+    if (ok) launch();
+    ok = ok && cudaGetLastError() == cudaSuccess &&
+         (rbytes == 0 || cudaMemcpyAsync(b->ppin + roff, b->pdev + roff, rbytes, cudaMemcpyDeviceToHost, b->stream) ==
+                             cudaSuccess) &&
+         cudaMemcpyAsync(b->ppin + R.arch, b->pdev + R.arch, sizeof(int), cudaMemcpyDeviceToHost, b->stream) ==
+             cudaSuccess &&
+         cudaEventRecord(b->e1, b->stream) == cudaSuccess && cudaStreamSynchronize(b->stream) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      cudaStreamSynchronize(b->stream);
+      return false;
+    }
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, b->e0, b->e1);
+    ms += t;
+    return true;
+  };
+  PistonDisk* disks_d = reinterpret_cast<PistonDisk*>(b->pdev + R.disks);
+  int* arch_d = reinterpret_cast<int*>(b->pdev + R.arch);
+  if (sources > 0 &&
+      !phase(R.centers, sizeof(double) * 3 * sources, R.disks, sizeof(PistonDisk) * sources, [&]() {
+        ++g_kernel_launches;
+        k_piston_sections<<<grid_of(sources, 128), 128, 0, b->stream>>>(
+            pf, reinterpret_cast<const double*>(b->pdev + R.centers), sources, disks_d, arch_d);
+      }))
+    return FL_INTERNAL;
+  const PistonDisk* disks = reinterpret_cast<const PistonDisk*>(b->ppin + R.disks);
+  for (int k = 0; k < sources; ++k) {
+    if (disks[k].status != FL_OK) return disks[k].status;
+    if (!wfinite(disks[k].r2) || disks[k].r2.lower < 0 || !wfinite(disks[k].y) || !wfinite(disks[k].z))
+      return FL_OUT_OF_RANGE;
+  }
+  // AddSupport (:188-232): the patches each section's circumscribed square touches
+  {
+    const WBounds fl_ = lattice_offset(tank[2], grid->origin[1], 0.0, h);
+    const WBounds lz = lattice_offset(tank[3], grid->origin[2], 0.0, h);
+    const WBounds hz = lattice_offset(tank[4], grid->origin[2], 0.0, h);
+    if (!wfinite(fl_) || !wfinite(lz) || !wfinite(hz)) return FL_OUT_OF_RANGE;
+    if (pf.is_plane) {
+      if (pf.plane_y > tank[2]) {
+        const WBounds sf = lattice_offset(pf.plane_y, grid->origin[1], 0.0, h);
+        if (!wfinite(sf)) return FL_OUT_OF_RANGE;
+        st = add_rectangle(idx, fl_.lower, sf.upper, lz.lower, hz.upper);
+        if (st != FL_OK) return st;
+      }
+    } else {
+      for (int k = 0; k < sources; ++k) {
+        const PistonDisk& d = disks[k];
+        if (d.r2.upper == 0) continue;
+        const WBounds r = wroot(d.r2);
+        const WBounds ys = wadd(d.y, {-r.upper, r.upper}), zs = wadd(d.z, {-r.upper, r.upper});
+        if (!wfinite(ys) || !wfinite(zs)) return FL_OUT_OF_RANGE;
+        st = add_rectangle(idx, std::max(ys.lower, fl_.lower), ys.upper, std::max(zs.lower, lz.lower),
+                           std::min(zs.upper, hz.upper));
+        if (st != FL_OK) return st;
+      }
+    }
+  }
+  const size_t npatch = idx.size() / 2;
+  if (npatch > patch_capacity) return FL_RESOURCE_EXHAUSTED;
+  for (uint64_t f = 0; f < nf; ++f) has_face_flux[f] = 0, face_fluxes[f] = 0.0;
+  for (size_t k = 0; k < npatch; ++k) {
+    fl_piston_patch& rec = patches[k];
+    std::memset(&rec, 0, sizeof(rec));
+    rec.lattice_y = idx[2 * k];
+    rec.lattice_z = idx[2 * k + 1];
+    const int32_t key[3] = {px, rec.lattice_y, rec.lattice_z};
+    if (host_find_cell(cells, nc, key) < 0) continue;
+    // FindReceiverFaceOrdinal (:234-256): the piston face of the selected cell
+    const int64_t lat[3] = {px, rec.lattice_y, rec.lattice_z};
+    uint64_t slot = 0;
+    if (host_face_slot(grid, 0, lat, &slot) != FL_OK) return FL_FAILED_PRECONDITION;
+    uint64_t a = 0, e = nf;
+    while (a < e) {
+      const uint64_t mid = (a + e) / 2;
+      if (faces[mid].face_slot < slot)
+        a = mid + 1;
+      else
+        e = mid;
+    }
+    const int32_t tail_key[3] = {px - 1, rec.lattice_y, rec.lattice_z};
+    const bool has_tail = (int64_t)px > kFirstLattice && host_find_cell(cells, nc, tail_key) >= 0;
+    if (a == nf || faces[a].face_slot != slot || has_tail) return FL_FAILED_PRECONDITION;
+    const fl_frozen_face& face = faces[a];
+    const double flux = face.prescribed_wall_flux;
+    if (face.open_area != 0 || face.blocked_area != h * h || face.wall_normal_velocity != velocity ||
+        !face.has_prescribed_wall_flux || !std::isfinite(flux) || (velocity == 0 && flux != 0) ||
+        (velocity > 0 && flux <= 0) || (velocity < 0 && flux >= 0))
+      return FL_FAILED_PRECONDITION;
+    rec.has_receiver = 1;
+    rec.receiver_face_ordinal = a;
+    has_face_flux[a] = 1;
+    face_fluxes[a] = 0.0;
+  }
+  for (uint64_t f = 0; f < nf; ++f)
+    if (faces[f].has_prescribed_wall_flux && faces[f].prescribed_wall_flux != 0 && !has_face_flux[f])
+      return FL_FAILED_PRECONDITION;
+  // every patch's wet area on the device
+  PatchResult* res = reinterpret_cast<PatchResult*>(b->ppin + R.results);
+  if (npatch > 0) {
+    std::memcpy(b->ppin + R.patches, idx.data(), sizeof(int32_t) * idx.size());
+    const int nd = sources;
+    if (!phase(R.patches, sizeof(int32_t) * idx.size(), R.results, sizeof(PatchResult) * npatch, [&]() {
+          ++g_kernel_launches;
+          const int threads = 64, blocks = (int)std::min<size_t>((npatch + threads - 1) / threads, kPistonSlots / threads);
+          k_piston_patches<<<blocks, threads, 0, b->stream>>>(
+              pf, disks_d, nd, reinterpret_cast<const int32_t*>(b->pdev + R.patches), (int)npatch,
+              reinterpret_cast<PistonInterval*>(b->pdev + R.banks), reinterpret_cast<PatchResult*>(b->pdev + R.results));
+        }))
+      return FL_INTERNAL;
+  }
+  WBounds whole;
+  for (size_t k = 0; k < npatch; ++k) {
+    if (res[k].status != FL_OK) return res[k].status;
+    if (!wfinite(res[k].area) || res[k].area.lower < 0 || res[k].area.upper > nominal.upper ||
+        !std::isfinite(res[k].midpoint_flux))
+      return FL_OUT_OF_RANGE;
+    patches[k].area[0] = res[k].area.lower;
+    patches[k].area[1] = res[k].area.upper;
+    whole = wadd(whole, res[k].area);
+  }
+  const WBounds wflux = area_to_flux(whole, velocity);
+  if (!wfinite(whole) || !wfinite(wflux)) return FL_OUT_OF_RANGE;
+  if (whole.upper > 0) {
+    const double width = add_up(whole.upper, -whole.lower);
+    const double limit = directed_quotient(whole.lower, 1000, false);
+    if (whole.lower <= 0 || width > limit) return FL_FAILED_PRECONDITION;
+  }
+  // AssignPatches (:285-328): per z column, a wet patch without a receiver
+  // joins the column's highest receiver when that lies directly below it.
+  uint64_t joined = 0;
+  for (size_t begin = 0; begin < npatch;) {
+    size_t end = begin;
+    long long highest = -1;
+    while (end < npatch && patches[end].lattice_z == patches[begin].lattice_z) {
+      if (patches[end].has_receiver) highest = (long long)end;
+      ++end;
+    }
+    for (size_t k = begin; k < end; ++k) {
+      fl_piston_patch& p = patches[k];
+      if (p.area[1] == 0) continue;
+      fl_piston_patch* recv = &p;
+      if (!p.has_receiver) {
+        if (highest < 0 || (int64_t)p.lattice_y - patches[highest].lattice_y != 1 || !res[k].cross_lower)
+          return FL_FAILED_PRECONDITION;
+        recv = &patches[highest];
+        p.has_receiver = 1;
+        p.receiver_face_ordinal = recv->receiver_face_ordinal;
+        ++joined;
+      }
+      const WBounds ra = wadd({recv->receiver_area[0], recv->receiver_area[1]}, {p.area[0], p.area[1]});
+      const WBounds rf = wadd({recv->receiver_flux[0], recv->receiver_flux[1]},
+                              area_to_flux({p.area[0], p.area[1]}, velocity));
+      recv->receiver_area[0] = ra.lower;
+      recv->receiver_area[1] = ra.upper;
+      recv->receiver_flux[0] = rf.lower;
+      recv->receiver_flux[1] = rf.upper;
+      double& acc = face_fluxes[recv->receiver_face_ordinal];
+      acc += res[k].midpoint_flux;
+      if (!wfinite(ra) || !wfinite(rf) || !std::isfinite(acc)) return FL_OUT_OF_RANGE;
+    }
+    begin = end;
+  }
+  WBounds assigned_area, assigned_flux;
+  for (size_t k = 0; k < npatch; ++k) {
+    const fl_piston_patch& p = patches[k];
+    if (p.receiver_area[1] == 0) continue;
+    const WBounds enc{p.receiver_flux[0], p.receiver_flux[1]};
+    const double given = face_fluxes[p.receiver_face_ordinal];
+    if (!wfinite(enc) || given < enc.lower || given > enc.upper) return FL_OUT_OF_RANGE;
+    assigned_area = wadd(assigned_area, {p.receiver_area[0], p.receiver_area[1]});
+    assigned_flux = wadd(assigned_flux, enc);
+  }
+  const bool area_ok =
+      wfinite(assigned_area) && assigned_area.upper >= whole.lower && assigned_area.lower <= whole.upper;
+  const bool flux_ok =
+      wfinite(assigned_flux) && assigned_flux.upper >= wflux.lower && assigned_flux.lower <= wflux.upper;
+  if (!area_ok || !flux_ok) return FL_OUT_OF_RANGE;
+  *patch_count = npatch;
+  whole_area[0] = whole.lower;
+  whole_area[1] = whole.upper;
+  whole_flux[0] = wflux.lower;
+  whole_flux[1] = wflux.upper;
+  *attached = joined;
+  if (m) {
+    m->compiled_architecture = *reinterpret_cast<int*>(b->ppin + R.arch);
+    m->kernel_ms = ms;
+  }
   return FL_OK;
 }

@@ -780,6 +780,45 @@ int fl_boundary_freeze(fl_boundary* boundary, const fl_freeze_inputs* inputs, fl
                        uint64_t* cell_count, fl_frozen_face* faces, uint64_t* face_count,
                        double* capillary_step_bound, fl_measurement* measurement);
 
+/* ---- wetted piston (.wetted_piston) ----
+ * ComputeWettedPiston3D (native/src/wetted_piston_3d.cc:342-571 with
+ * base/wetted_piston_math_3d.h): the wet area of the open tank's low-x piston
+ * under the liquid field, per lattice patch of the piston plane, as
+ * outward-rounded [lower, upper] enclosures, and each receiver face's signed
+ * flux (positive into the tank): the sum, in (z, y) patch order, of the
+ * midpoint-area fluxes of the patches assigned to it. Patches come in (z, y)
+ * order, including dry receivers; a wet patch without a receiver joins the
+ * receiver directly below it. Frozen cells and faces as fl_boundary_freeze
+ * returns them. */
+#define FL_PISTON_FIELD_SPHERE 0         /* LiquidAnalyticSphere3D */
+#define FL_PISTON_FIELD_PARTICLE_UNION 1 /* LiquidParticleSphereUnion3D over the particle positions */
+#define FL_PISTON_FIELD_PLANE 2          /* LiquidHorizontalPlaneSurface3D */
+typedef struct {
+  int32_t kind; /* FL_PISTON_FIELD_* */
+  int32_t pad;
+  double sphere_center[3]; /* m, analytic sphere */
+  double radius;           /* m, analytic sphere or each particle's sphere */
+  double plane_height_y;   /* m, plane */
+} fl_piston_field;
+typedef struct {
+  int32_t lattice_y, lattice_z;
+  double area[2]; /* m^2, [lower, upper] */
+  uint64_t receiver_face_ordinal;
+  uint8_t has_receiver;
+  uint8_t pad[7];
+  double receiver_area[2]; /* m^2 assigned to this receiver */
+  double receiver_flux[2]; /* m^3/s enclosure of its assigned flux */
+} fl_piston_patch;
+/* patches: room for patch_capacity records (at most 24576 are produced);
+ * face_fluxes / has_face_flux: one per frozen face. */
+int fl_boundary_wetted_piston(fl_boundary* boundary, const fl_owned_grid* grid, const fl_frozen_cell* cells,
+                              uint64_t cell_count, const fl_frozen_face* faces, uint64_t face_count,
+                              const fl_piston_field* field, const double* particle_positions,
+                              uint64_t particle_count, const double tank[6], fl_piston_patch* patches,
+                              uint64_t patch_capacity, uint64_t* patch_count, double* face_fluxes,
+                              uint8_t* has_face_flux, double whole_area[2], double whole_flux[2],
+                              uint64_t* attached_patch_count, fl_measurement* measurement);
+
 int fl_boundary_links(fl_boundary* boundary, const fl_frozen_geometry* geometry, const fl_pressure_fields* fields,
                       fl_pressure_cell* cells, fl_pressure_link* faces, uint64_t* lower_theta_regularization_count,
                       fl_measurement* measurement);

@@ -22,6 +22,7 @@
 #include "fluidity/host/liquid_boundary_workspace_3d.h"
 #include "fluidity/host/mac_pressure_workspace_3d.h"
 #include "fluidity/host/sparse_mac_grid_3d.h"
+#include "fluidity/host/wetted_piston_3d.h"
 
 #include <cmath>
 #include <optional>
@@ -459,8 +460,87 @@ int bk_freeze(int which, const double origin[3], double h, const int32_t* blocks
   return 0;
 }
 
+// .wetted_piston on a frozen view given as arrays (cells: x,y,z + volume,
+// centre distance, curvature; faces: axis,x,y,z + slot + open, blocked, wall
+// velocity, explicit flux or NaN, piston flag), a field (kind 0 sphere with
+// centre and radius, 1 particle union with radius over the positions, 2 plane
+// at a height; 3 the covariance drop) and the tank. Outputs: 9 doubles per
+// patch (y, z, area lower/upper, receiver ordinal or -1, receiver area
+// lower/upper, receiver flux lower/upper), face fluxes (NaN for none), the
+// whole area and flux enclosures and the attached count.
+int bk_wetted_piston(int which, const double origin[3], double h, const int32_t* blocks, uint64_t nb,
+                     const int32_t* cell_index, const double* cell_values, uint64_t nc, const int32_t* face_index,
+                     const uint64_t* face_slot, const double* face_values, uint64_t nf, int field_kind,
+                     const double center[3], double radius, double plane_y, const double* positions, uint64_t np,
+                     const double tank[6], double* patches_out, uint64_t* npatches, double* fluxes_out,
+                     double whole[4], uint64_t* attached) {
+  int code = 0;
+  const auto* table = Table(which, &code);
+  if (!table) return code;
+  auto grid = Grid(origin, h, blocks, nb);
+  if (!grid.ok()) return Code(grid.status());
+  LiquidStateCapacities3D caps{};
+  caps.particles = kParticles;
+  caps.blocks = kFaces / 192;
+  caps.cells = kCells;
+  caps.faces = kFaces;
+  auto ws = WettedPistonWorkspace3D::Create(caps);
+  if (!ws.ok()) return Code(ws.status());
+  std::vector<FrozenLiquidCell3D> cells(nc);
+  for (uint64_t i = 0; i < nc; ++i)
+    cells[i] = {{cell_index[3 * i], cell_index[3 * i + 1], cell_index[3 * i + 2]}, cell_values[3 * i],
+                cell_values[3 * i + 1], cell_values[3 * i + 2]};
+  std::vector<FrozenLiquidFace3D> faces(nf);
+  for (uint64_t f = 0; f < nf; ++f) {
+    FrozenLiquidFace3D face{};
+    face.face_index = {static_cast<FaceNormalAxis>(face_index[4 * f]),
+                       {face_index[4 * f + 1], face_index[4 * f + 2], face_index[4 * f + 3]}};
+    face.face_slot = face_slot[f];
+    face.open_area = face_values[5 * f];
+    face.blocked_area = face_values[5 * f + 1];
+    face.wall_normal_velocity = face_values[5 * f + 2];
+    if (face_values[5 * f + 3] == face_values[5 * f + 3]) face.prescribed_wall_flux = face_values[5 * f + 3];
+    face.is_low_x_piston_face = face_values[5 * f + 4] != 0;
+    faces[f] = face;
+  }
+  const std::vector<LiquidCenterDistance3D> centers;
+  const FrozenLiquidBoundaryGeometryView3D frozen{grid->view(), centers, cells, faces, 1.0 / 240.0, 1000.0, 0.0, 0.0};
+  std::vector<LiquidParticleState3D> particles(np);
+  for (uint64_t i = 0; i < np; ++i) particles[i].world_position = {positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]};
+  LiquidSceneField3D field = LiquidHorizontalPlaneSurface3D{plane_y};
+  if (field_kind == 0) field = LiquidAnalyticSphere3D{{center[0], center[1], center[2]}, radius};
+  if (field_kind == 1) field = LiquidParticleSphereUnion3D{radius};
+  if (field_kind == 3) field = LiquidIsolatedCovarianceDrop3D{radius, 1.0};
+  const AxisAlignedLiquidTank3D tk{tank[0], tank[1], tank[2], tank[3], tank[4], tank[5]};
+  const WettedPistonInputs3D inputs{field, particles, frozen, tk};
+  auto r = TimedOp([&] { return table->wetted_piston(table->context, inputs, *ws); });
+  if (!r.ok()) return Code(r.status());
+  *npatches = r->patches.size();
+  for (std::size_t k = 0; k < r->patches.size(); ++k) {
+    const auto& p = r->patches[k];
+    double* o = patches_out + 9 * k;
+    o[0] = p.lattice_y;
+    o[1] = p.lattice_z;
+    o[2] = p.area.lower;
+    o[3] = p.area.upper;
+    o[4] = p.receiver_face_ordinal ? static_cast<double>(*p.receiver_face_ordinal) : -1.0;
+    o[5] = p.receiver_area.lower;
+    o[6] = p.receiver_area.upper;
+    o[7] = p.receiver_flux.lower;
+    o[8] = p.receiver_flux.upper;
+  }
+  for (uint64_t f = 0; f < nf; ++f) fluxes_out[f] = r->face_fluxes[f].value_or(std::nan(""));
+  whole[0] = r->whole_area.lower;
+  whole[1] = r->whole_area.upper;
+  whole[2] = r->whole_flux.lower;
+  whole[3] = r->whole_flux.upper;
+  *attached = r->attached_patch_count;
+  return 0;
+}
+
 // Which operations each table fills (bit k: deposit, normalize, predict,
-// forces, gather, project, topology, update_particles, links, freeze).
+// forces, gather, project, topology, update_particles, links, freeze,
+// wetted_piston).
 int bk_filled(int which, uint32_t* mask) {
   int code = 0;
   const auto* table = Table(which, &code);
@@ -474,9 +554,10 @@ int bk_filled(int which, uint32_t* mask) {
                        reinterpret_cast<const void*>(table->topology),
                        reinterpret_cast<const void*>(table->update_particles),
                        reinterpret_cast<const void*>(table->links),
-                       reinterpret_cast<const void*>(table->freeze)};
+                       reinterpret_cast<const void*>(table->freeze),
+                       reinterpret_cast<const void*>(table->wetted_piston)};
   *mask = 0;
-  for (int k = 0; k < 10; ++k)
+  for (int k = 0; k < 11; ++k)
     if (ops[k]) *mask |= 1u << k;
   return 0;
 }

@@ -423,3 +423,54 @@ def freeze(which, s: FreezeScene, **override):
         ctypes.byref(nf), ctypes.byref(bound))
     k, m = nc.value, nf.value
     return code, ci[:k], cv[:k], fi[:m], fs[:m], fv[:m], bound.value
+
+
+class PistonScene:
+    """The open-tank pool frozen by the CPU table (FreezeScene("tank")) and a
+    liquid field over the low-x piston: a horizontal plane at 4.4 cells, an
+    analytic sphere of radius 3 cells centred 1.5 cells inside the piston, or
+    a union of 0.6-cell particle spheres on a 0.5-cell lattice in the 1.7
+    cells next to the piston (4 x 7 x 23 = 644 particles)."""
+
+    def __init__(self, field: str = "plane"):
+        fs = FreezeScene("tank")
+        code, ci, cv, fi, fslot, fv, _ = freeze(CPU, fs)
+        assert code == 0
+        self.blocks, self.tank = fs.blocks, fs.tank
+        self.cell_index, self.cell_values = ci, cv
+        self.face_index, self.face_slot, self.face_values = fi, fslot, fv
+        self.kind, self.center, self.radius, self.plane_y = 2, (0.0, 0.0, 0.0), 1.0, 4.4 * H
+        self.positions = np.zeros((0, 3))
+        x0 = fs.tank[0]
+        if field == "sphere":
+            self.kind, self.center, self.radius = 0, (x0 + 1.5 * H, 3.0 * H, 6.0 * H), 3.0 * H
+        elif field == "union":
+            self.kind, self.radius = 1, 0.6 * H
+            gx, gy, gz = np.meshgrid(x0 + H * (0.2 + 0.5 * np.arange(4)), H * (0.8 + 0.5 * np.arange(7)),
+                                     H * (0.5 + 0.5 * np.arange(23)), indexing="ij")
+            self.positions = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], 1)
+        elif field == "drop":
+            self.kind = 3
+
+
+def wetted_piston(which, s: PistonScene, **override):
+    """The table's .wetted_piston: (code, patches (n, 9), face fluxes (NaN
+    for none), whole area and flux enclosures (4,), attached count)."""
+    a = dict(s.__dict__)
+    a.update(override)
+    nf = len(a["face_index"])
+    patches = np.zeros((24576, 9))
+    fluxes = np.zeros(max(nf, 1))
+    whole = (ctypes.c_double * 4)()
+    npatch, attached = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    c = lambda x, t: np.ascontiguousarray(x, t)  # noqa: E731
+    pos = c(a["positions"], np.float64).reshape(-1, 3)
+    code = lib().bk_wetted_piston(
+        ctypes.c_int(which), _d3((0, 0, 0)), ctypes.c_double(H), _p(c(a["blocks"], np.int32)),
+        ctypes.c_uint64(len(a["blocks"])), _p(c(a["cell_index"], np.int32)), _p(c(a["cell_values"], np.float64)),
+        ctypes.c_uint64(len(a["cell_index"])), _p(c(a["face_index"], np.int32)), _p(c(a["face_slot"], np.uint64)),
+        _p(c(a["face_values"], np.float64)), ctypes.c_uint64(nf), ctypes.c_int(a["kind"]), _d3(a["center"]),
+        ctypes.c_double(a["radius"]), ctypes.c_double(a["plane_y"]), _p(pos), ctypes.c_uint64(len(pos)),
+        (ctypes.c_double * 6)(*[float(v) for v in a["tank"]]), _p(patches), ctypes.byref(npatch), _p(fluxes), whole,
+        ctypes.byref(attached))
+    return code, patches[:npatch.value], fluxes[:nf], np.array(whole[:]), attached.value

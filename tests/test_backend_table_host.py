@@ -37,7 +37,7 @@ def test_b200_table_refuses_without_a_device():
 
 def test_cpu_table_runs_the_bounded_dam_break():
     code, mask = bt.filled(bt.CPU)
-    assert code == 0 and mask == 0x3FF
+    assert code == 0 and mask == 0x7FF
     s = bt.Scene(mixed_sides=False)
     code, q, st = bt.deposit(bt.CPU, s)
     assert code == 0

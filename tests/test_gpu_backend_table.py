@@ -79,11 +79,12 @@ def histories(one_sided):
 
 def test_tables_fill_the_transfer_and_projection_operations():
     code, cpu = bt.filled(CPU)
-    assert code == 0 and cpu == 0x3FF
+    assert code == 0 and cpu == 0x7FF
     code, b200 = bt.filled(B200)
     assert code == 0
-    # deposit, normalize, predict, forces, gather, project, links and freeze; no topology or particle update
-    assert b200 == 0x33F
+    # deposit, normalize, predict, forces, gather, project, links, freeze and wetted piston;
+    # no topology or particle update
+    assert b200 == 0x73F
 
 
 def test_deposit_is_bit_identical(scene, deposited):
@@ -383,6 +384,7 @@ def test_operation_times_against_the_cpu_table(scene, one_sided, histories):
     q = bt.deposit(CPU, scene)[1]
     ls = bt.LinkScene()
     fs = bt.FreezeScene("tank")
+    ps = bt.PistonScene("union")
     ops = {
         "deposit (1024 particles)": lambda w: bt.deposit(w, scene),
         "normalize (15360 faces)": lambda w: bt.normalize(w, q, 0.1 * float(scene.particles["mass"][0])),
@@ -390,6 +392,7 @@ def test_operation_times_against_the_cpu_table(scene, one_sided, histories):
         "gather (1024 particles)": lambda w: bt.gather(w, one_sided, histories["old"], histories["new"]),
         "freeze (tank, 1296 candidates)": lambda w: bt.freeze(w, fs),
         "links (864 cells, 2880 faces)": lambda w: bt.links(w, ls),
+        "wetted piston (644 particle spheres)": lambda w: bt.wetted_piston(w, ps),
         "project (3375 cells, to the gate)": lambda w: bt.project(w, system, box.h, dt),
     }
     rows = {}
@@ -407,6 +410,43 @@ def test_operation_times_against_the_cpu_table(scene, one_sided, histories):
     print("\noperation | CPU table ms | B200 table ms | ratio")
     for name, (c, g) in rows.items():
         print(f"{name} | {c:.3f} | {g:.3f} | {c / g:.1f}x")
-    for name in ("deposit", "gather", "freeze", "project"):
+    for name in ("deposit", "gather", "freeze", "project", "wetted"):
         c, g = next(v for k, v in rows.items() if k.startswith(name))
         assert g <= c, (name, c, g)
+
+
+@pytest.mark.parametrize("field", ["plane", "union"])
+def test_wetted_piston_is_bit_identical(field):
+    s = bt.PistonScene(field)
+    c0, p0, f0, w0, a0 = bt.wetted_piston(CPU, s)
+    c1, p1, f1, w1, a1 = bt.wetted_piston(B200, s)
+    assert c0 == 0 and c1 == 0
+    assert np.array_equal(p1, p0)  # patches: indices, area enclosures, receivers, assigned area and flux
+    assert np.array_equal(f1, f0, equal_nan=True)  # each receiver face's summed midpoint flux
+    assert np.array_equal(w1, w0) and a1 == a0
+    assert a0 > 0 and (p0[:, 4] >= 0).sum() > 20 and w0[0] > 0
+
+
+def test_wetted_piston_error_codes_match():
+    s = bt.PistonScene("union")
+
+    def both(scene=s, **kw):
+        a, b = bt.wetted_piston(CPU, scene, **kw)[0], bt.wetted_piston(B200, scene, **kw)[0]
+        assert a == b, (kw.keys(), a, b)
+        return a
+
+    assert both(bt.PistonScene("sphere")) == 9  # a small sphere's banded enclosure is wider than 1/1000
+    assert both(bt.PistonScene("drop")) == 3  # not a field the piston can measure
+    assert both(radius=0.0) == 3
+    bad = s.positions.copy()
+    bad[5, 1] = np.nan
+    assert both(positions=bad) == 3
+    assert both(tank=(s.tank[1], s.tank[0]) + tuple(s.tank[2:])) == 3
+    swapped = s.face_slot.copy()
+    swapped[[3, 4]] = swapped[[4, 3]]
+    assert both(face_slot=swapped) == 3
+    fv = s.face_values.copy()
+    receivers = np.nonzero(fv[:, 4] == 1)[0]
+    fv[receivers[0], 2] = 0.0  # a receiver face whose wall velocity is not the piston's
+    assert both(face_values=fv) == 9
+    assert both(positions=np.repeat(s.positions, 2, axis=0)) == 8  # more particles than the bounded workspace
