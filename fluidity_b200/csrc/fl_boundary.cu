@@ -3299,100 +3299,102 @@ struct PatchResult {
 
 constexpr int kPistonBands = 64;
 
-// IntegratePatch + MeasurePatch (wetted_piston_math_3d.h:280-424): the wet
-// area of patch (py, pz) as an enclosure, by 64 z-bands of interval unions.
-__host__ __device__ inline PatchResult measure_patch(const PistonField& f, int32_t py, int32_t pz,
-                                                     const PistonDisk* disks, size_t nd, PistonInterval* inner,
-                                                     PistonInterval* outer) {
-  PatchResult m{};
-  m.cross_lower = 1;
-  m.status = FL_OK;
-  // every successful measure carries the midpoint of its area times the piston velocity
-  auto finish = [&f](PatchResult& r) {
-    if (r.status != FL_OK) return r;
-    r.midpoint_flux = midpoint(r.area.lower, r.area.upper) * f.tank[5];
-    if (!isfinite(r.midpoint_flux)) r.status = FL_OUT_OF_RANGE;
-    return r;
-  };
+// IntegratePatch + MeasurePatch (wetted_piston_math_3d.h:280-424), split so
+// that a patch's 64 z-bands run on 64 threads: the patch's frame (its
+// rectangle inside the tank's floor and z walls and under a plane surface),
+// the wet test over all sources, and one band's interval-union lengths times
+// its width; the band products are summed in band order.
+struct PatchFrame {
+  WBounds rlo_y, rhi_y, rlo_z, rhi_z, rect, floor_, surface, zw;
+  int status;
+  bool empty;  // a zero-width rectangle
+};
+
+__device__ PatchFrame patch_frame(const PistonField& f, int32_t py, int32_t pz) {
+  PatchFrame fr{};
+  fr.status = FL_OK;
   const double h = f.h;
-  const WBounds floor_ = lattice_offset(f.tank[2], f.origin[1], (double)py, h);
+  fr.floor_ = lattice_offset(f.tank[2], f.origin[1], (double)py, h);
   const WBounds low_z = lattice_offset(f.tank[3], f.origin[2], (double)pz, h);
   const WBounds high_z = lattice_offset(f.tank[4], f.origin[2], (double)pz, h);
-  const WBounds surface = f.is_plane ? lattice_offset(f.plane_y, f.origin[1], (double)py, h) : wpoint(1.0);
-  if (!wfinite(floor_) || !wfinite(low_z) || !wfinite(high_z) || !wfinite(surface)) {
-    m.status = FL_OUT_OF_RANGE;
-    return m;
+  fr.surface = f.is_plane ? lattice_offset(f.plane_y, f.origin[1], (double)py, h) : wpoint(1.0);
+  if (!wfinite(fr.floor_) || !wfinite(low_z) || !wfinite(high_z) || !wfinite(fr.surface)) {
+    fr.status = FL_OUT_OF_RANGE;
+    return fr;
   }
-  const WBounds rlo_y = wmax(wpoint(0.0), floor_), rhi_y = wmin(wpoint(1.0), surface);
-  const WBounds rlo_z = wmax(wpoint(0.0), low_z), rhi_z = wmin(wpoint(1.0), high_z);
-  const WBounds yw = width_of(rlo_y, rhi_y), zw = width_of(rlo_z, rhi_z);
-  if (yw.upper == 0 || zw.upper == 0) return finish(m);
-  const WBounds rect = wmul_nonneg(yw, zw);
-  if (f.is_plane) {
-    m.area = world_area(rect, h);
-    m.cross_lower = floor_.upper <= 0 && surface.lower > 0 && zw.lower > 0;
-    if (!wfinite(m.area)) m.status = FL_OUT_OF_RANGE;
-  } else {
-    bool cross = floor_.upper <= 0 && zw.lower > 0;
-    bool wet = false;
-    for (size_t k = 0; k < nd; ++k) {
-      const PistonDisk& d = disks[k];
-      if (d.r2.upper == 0) continue;
-      const WBounds y = wsub(d.y, wpoint((double)py)), z = wsub(d.z, wpoint((double)pz));
-      const WBounds ny = nearest_of(y, rlo_y, rhi_y), nz = nearest_of(z, rlo_z, rhi_z);
-      const WBounds pg = gap_of(d.r2, ny, nz);
-      if (!wfinite(pg)) {
-        m.status = FL_OUT_OF_RANGE;
-        return m;
-      }
-      if (pg.upper <= 0) continue;
-      wet = true;
-      const WBounds eg = gap_of(d.r2, wmag(y), nz);
-      if (!wfinite(eg)) {
-        m.status = FL_OUT_OF_RANGE;
-        return m;
-      }
-      cross = cross && eg.lower > 0;
+  fr.rlo_y = wmax(wpoint(0.0), fr.floor_);
+  fr.rhi_y = wmin(wpoint(1.0), fr.surface);
+  fr.rlo_z = wmax(wpoint(0.0), low_z);
+  fr.rhi_z = wmin(wpoint(1.0), high_z);
+  const WBounds yw = width_of(fr.rlo_y, fr.rhi_y);
+  fr.zw = width_of(fr.rlo_z, fr.rhi_z);
+  fr.empty = yw.upper == 0 || fr.zw.upper == 0;
+  if (!fr.empty) fr.rect = wmul_nonneg(yw, fr.zw);
+  return fr;
+}
+
+// Whether any source's section reaches the patch rectangle, and whether every
+// such source crosses the patch's lower edge.
+__device__ bool patch_wet(const PatchFrame& fr, int32_t py, int32_t pz, const PistonDisk* disks, int nd, int* status,
+                          bool* cross) {
+  *cross = fr.floor_.upper <= 0 && fr.zw.lower > 0;
+  bool wet = false;
+  for (int k = 0; k < nd; ++k) {
+    const PistonDisk& d = disks[k];
+    if (d.r2.upper == 0) continue;
+    const WBounds y = wsub(d.y, wpoint((double)py)), z = wsub(d.z, wpoint((double)pz));
+    const WBounds ny = nearest_of(y, fr.rlo_y, fr.rhi_y), nz = nearest_of(z, fr.rlo_z, fr.rhi_z);
+    const WBounds pg = gap_of(d.r2, ny, nz);
+    if (!wfinite(pg)) {
+      *status = FL_OUT_OF_RANGE;
+      return false;
     }
-    if (!wet) return finish(m);
-    WBounds area;
-    for (int band = 0; band < kPistonBands; ++band) {
-      const WBounds blo = wmax(rlo_z, wpoint((double)band / kPistonBands));
-      const WBounds bhi = wmin(rhi_z, wpoint((double)(band + 1) / kPistonBands));
-      const WBounds bw = width_of(blo, bhi);
-      if (bw.upper == 0) continue;
-      size_t ni = 0, no = 0;
-      for (size_t k = 0; k < nd; ++k) {
-        const PistonDisk& d = disks[k];
-        if (d.r2.upper == 0) continue;
-        const WBounds z = wsub(d.z, wpoint((double)pz));
-        const WBounds near2 = wsquare(nearest_of(z, blo, bhi)), far2 = wsquare(farthest_of(z, blo, bhi));
-        const WBounds outer2 = wsub(d.r2, near2), inner2 = wsub(d.r2, far2);
-        if (!wfinite(outer2) || !wfinite(inner2)) {
-          m.status = FL_OUT_OF_RANGE;
-          return m;
-        }
-        if (outer2.upper <= 0) continue;
-        const WBounds y = wsub(d.y, wpoint((double)py));
-        const double ro = directed_root(outer2.upper, true);
-        const double olo = wmax(rlo_y, wsub(y, wpoint(ro))).lower;
-        const double ohi = wmin(rhi_y, wadd(y, wpoint(ro))).upper;
-        if (olo < ohi) outer[no++] = {olo, ohi};
-        if (inner2.lower > 0) {
-          const double ri = directed_root(inner2.lower, false);
-          const double ilo = wmax(rlo_y, wsub(y, wpoint(ri))).upper;
-          const double ihi = wmin(rhi_y, wadd(y, wpoint(ri))).lower;
-          if (ilo < ihi) inner[ni++] = {ilo, ihi};
-        }
-      }
-      const WBounds len{union_length(inner, ni, false), union_length(outer, no, true)};
-      area = wadd(area, wmul_nonneg(len, bw));
+    if (pg.upper <= 0) continue;
+    wet = true;
+    const WBounds eg = gap_of(d.r2, wmag(y), nz);
+    if (!wfinite(eg)) {
+      *status = FL_OUT_OF_RANGE;
+      return false;
     }
-    m.area = world_area(wmin(area, rect), h);
-    m.cross_lower = cross;
-    if (!wfinite(m.area)) m.status = FL_OUT_OF_RANGE;
+    *cross = *cross && eg.lower > 0;
   }
-  return finish(m);
+  *status = FL_OK;
+  return wet;
+}
+
+// Band `band` of the patch: [inner, outer] union length of the sections'
+// chords times the band's width; used = false for a band outside the rectangle.
+__device__ int band_product(const PatchFrame& fr, int32_t py, int32_t pz, const PistonDisk* disks, int nd, int band,
+                            PistonInterval* inner, PistonInterval* outer, WBounds* prod, bool* used) {
+  const WBounds blo = wmax(fr.rlo_z, wpoint((double)band / kPistonBands));
+  const WBounds bhi = wmin(fr.rhi_z, wpoint((double)(band + 1) / kPistonBands));
+  const WBounds bw = width_of(blo, bhi);
+  *used = bw.upper != 0;
+  if (!*used) return FL_OK;
+  size_t ni = 0, no = 0;
+  for (int k = 0; k < nd; ++k) {
+    const PistonDisk& d = disks[k];
+    if (d.r2.upper == 0) continue;
+    const WBounds z = wsub(d.z, wpoint((double)pz));
+    const WBounds near2 = wsquare(nearest_of(z, blo, bhi)), far2 = wsquare(farthest_of(z, blo, bhi));
+    const WBounds outer2 = wsub(d.r2, near2), inner2 = wsub(d.r2, far2);
+    if (!wfinite(outer2) || !wfinite(inner2)) return FL_OUT_OF_RANGE;
+    if (outer2.upper <= 0) continue;
+    const WBounds y = wsub(d.y, wpoint((double)py));
+    const double ro = directed_root(outer2.upper, true);
+    const double olo = wmax(fr.rlo_y, wsub(y, wpoint(ro))).lower;
+    const double ohi = wmin(fr.rhi_y, wadd(y, wpoint(ro))).upper;
+    if (olo < ohi) outer[no++] = {olo, ohi};
+    if (inner2.lower > 0) {
+      const double ri = directed_root(inner2.lower, false);
+      const double ilo = wmax(fr.rlo_y, wsub(y, wpoint(ri))).upper;
+      const double ihi = wmin(fr.rhi_y, wadd(y, wpoint(ri))).lower;
+      if (ilo < ihi) inner[ni++] = {ilo, ihi};
+    }
+  }
+  const WBounds len{union_length(inner, ni, false), union_length(outer, no, true)};
+  *prod = wmul_nonneg(len, bw);
+  return FL_OK;
 }
 
 __global__ void k_piston_sections(PistonField f, const double* centers, int n, PistonDisk* disks, int* arch) {
@@ -3401,16 +3403,71 @@ __global__ void k_piston_sections(PistonField f, const double* centers, int n, P
   if (i < n) disks[i] = piston_section(f, centers + 3 * i);
 }
 
-// Patches strided over the launched threads; each thread sorts its intervals
-// in its own two banks of nd records.
-__global__ void k_piston_patches(PistonField f, const PistonDisk* disks, int nd, const int32_t* patches, int np,
-                                 PistonInterval* banks, PatchResult* out) {
-  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-  const int slots = gridDim.x * blockDim.x;
-  PistonInterval* inner = banks + (size_t)slot * 2 * (nd > 0 ? nd : 1);
-  PistonInterval* outer = inner + (nd > 0 ? nd : 1);
-  for (int p = slot; p < np; p += slots)
-    out[p] = measure_patch(f, patches[2 * p], patches[2 * p + 1], disks, (size_t)nd, inner, outer);
+// One CTA of 64 threads (one per band) per patch in flight, patches strided
+// over the CTAs; each thread sorts its band's intervals in its own two banks
+// of nd records.
+__global__ void __launch_bounds__(kPistonBands) k_piston_patches(PistonField f, const PistonDisk* disks, int nd,
+                                                                 const int32_t* patches, int np,
+                                                                 PistonInterval* banks, PatchResult* out) {
+  __shared__ WBounds prod[kPistonBands];
+  __shared__ int used[kPistonBands], bad[kPistonBands];
+  const int band = threadIdx.x;
+  const size_t ndc = nd > 0 ? (size_t)nd : 1;
+  PistonInterval* inner = banks + ((size_t)blockIdx.x * kPistonBands + band) * 2 * ndc;
+  PistonInterval* outer = inner + ndc;
+  for (int p = blockIdx.x; p < np; p += gridDim.x) {
+    const int32_t py = patches[2 * p], pz = patches[2 * p + 1];
+    const PatchFrame fr = patch_frame(f, py, pz);
+    PatchResult m{};
+    m.cross_lower = 1;
+    m.status = fr.status;
+    bool bands = false;
+    if (m.status == FL_OK && !fr.empty) {
+      if (f.is_plane) {
+        m.area = world_area(fr.rect, f.h);
+        m.cross_lower = fr.floor_.upper <= 0 && fr.surface.lower > 0 && fr.zw.lower > 0;
+        if (!wfinite(m.area)) m.status = FL_OUT_OF_RANGE;
+      } else {
+        bool cross = true;
+        int st = FL_OK;
+        const bool wet = patch_wet(fr, py, pz, disks, nd, &st, &cross);
+        m.status = st;
+        if (st == FL_OK && wet) {
+          bands = true;  // the same on every thread: all compute the frame and wet test alike
+          m.cross_lower = cross;
+        }
+      }
+    }
+    if (bands) {
+      WBounds pr;
+      bool u = false;
+      bad[band] = band_product(fr, py, pz, disks, nd, band, inner, outer, &pr, &u);
+      prod[band] = pr;
+      used[band] = u;
+      __syncthreads();
+      if (band == 0) {
+        WBounds area;
+        for (int k = 0; k < kPistonBands && m.status == FL_OK; ++k) {
+          if (bad[k] != FL_OK)
+            m.status = bad[k];
+          else if (used[k])
+            area = wadd(area, prod[k]);
+        }
+        if (m.status == FL_OK) {
+          m.area = world_area(wmin(area, fr.rect), f.h);
+          if (!wfinite(m.area)) m.status = FL_OUT_OF_RANGE;
+        }
+      }
+      __syncthreads();  // the shared band results are reused by the next patch
+    }
+    if (band == 0) {
+      if (m.status == FL_OK) {
+        m.midpoint_flux = midpoint(m.area.lower, m.area.upper) * f.tank[5];
+        if (!isfinite(m.midpoint_flux)) m.status = FL_OUT_OF_RANGE;
+      }
+      out[p] = m;
+    }
+  }
 }
 
 }  // namespace
@@ -3418,7 +3475,7 @@ __global__ void k_piston_patches(PistonField f, const PistonDisk* disks, int nd,
 
 namespace {
 
-constexpr int kPistonSlots = 256;  // threads measuring patches at once, each with two interval banks
+constexpr int kPistonCtas = 32;  // patches measured at once (64 band threads each, two interval banks per thread)
 
 struct PistonRegions {
   size_t centers, disks, patches, results, arch, staged, banks, total;
@@ -3435,7 +3492,7 @@ struct PistonRegions {
     results = take(sizeof(PatchResult) * kMaxFaces);
     arch = take(sizeof(int));
     staged = o;
-    banks = take(sizeof(PistonInterval) * 2 * kPistonSlots * kMaxParticles);
+    banks = take(sizeof(PistonInterval) * 2 * kPistonCtas * kPistonBands * kMaxParticles);
     total = o;
   }
 };
@@ -3700,8 +3757,8 @@ extern "C" int fl_boundary_wetted_piston(fl_boundary* b, const fl_owned_grid* gr
     const int nd = sources;
     if (!phase(R.patches, sizeof(int32_t) * idx.size(), R.results, sizeof(PatchResult) * npatch, [&]() {
           ++g_kernel_launches;
-          const int threads = 64, blocks = (int)std::min<size_t>((npatch + threads - 1) / threads, kPistonSlots / threads);
-          k_piston_patches<<<blocks, threads, 0, b->stream>>>(
+          const int blocks = (int)std::min<size_t>(npatch, kPistonCtas);
+          k_piston_patches<<<blocks, kPistonBands, 0, b->stream>>>(
               pf, disks_d, nd, reinterpret_cast<const int32_t*>(b->pdev + R.patches), (int)npatch,
               reinterpret_cast<PistonInterval*>(b->pdev + R.banks), reinterpret_cast<PatchResult*>(b->pdev + R.results));
         }))
