@@ -1,7 +1,7 @@
 // Bounded boundary-aware transfers on the reference's owned sparse grid: the
 // operations behind the liquid scheduler's backend table (.deposit, .normalize,
-// .predict_missing_face, .forces, .gather, .freeze, .links, and the bounded
-// projection's staging; liquid_substep_backend_3d.h:121-194).
+// .predict_missing_face, .forces, .gather, .freeze, .wetted_piston, .links,
+// and the bounded projection's staging; liquid_substep_backend_3d.h:121-194).
 //
 // Restated from the reference's CPU operations, which its CPU table binds
 // (liquid_substep_3d_cpu.cc:775-803, 847-849):
@@ -23,6 +23,7 @@
 //                      the queries of base/liquid_boundary_geometry_math_3d.h:
 //                      160-415 (clipping, measures), 657-847 (modes)
 //   pressure links     liquid_boundary_geometry_3d.cc:1077-1380
+//   wetted piston      wetted_piston_3d.cc:60-575 with base/wetted_piston_math_3d.h
 // The whole file is compiled without FMA contraction (-fmad=false), so every
 // expression rounds as the CPU's does; fma() appears only where the reference
 // calls std::fma.
