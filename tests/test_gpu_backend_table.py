@@ -450,3 +450,57 @@ def test_wetted_piston_error_codes_match():
     fv[receivers[0], 2] = 0.0  # a receiver face whose wall velocity is not the piston's
     assert both(face_values=fv) == 9
     assert both(positions=np.repeat(s.positions, 2, axis=0)) == 8  # more particles than the bounded workspace
+
+
+def test_freeze_and_wetted_piston_agree_on_seeded_scenes():
+    """Seeded variations: drops of other centres, radii and wobbles under each
+    obstacle kind, and tanks of other walls and piston speeds with particle
+    unions of other spacings; whenever the CPU table succeeds the B200 table
+    gives the same bits, and otherwise the same code."""
+    rng = np.random.default_rng(11)
+    agreed = pistons = 0
+    for trial in range(12):
+        kind = ["none", "halfspace", "slab", "tank"][trial % 4]
+        s = bt.FreezeScene(kind)
+        if kind == "tank":
+            t = list(s.tank)
+            t[0] = rng.uniform(0.05, 0.9) * bt.H
+            t[2] = rng.uniform(0.05, 0.9) * bt.H
+            t[5] = rng.uniform(-0.2, 0.2)
+            s.tank = tuple(t)
+        else:
+            c = np.array([rng.uniform(5.0, 7.0), rng.uniform(4.0, 5.0), rng.uniform(5.0, 7.0)])
+            r0, wob = rng.uniform(2.5, 3.8), rng.uniform(0.0, 0.4)
+
+            def dist(p):
+                r = np.linalg.norm(p - c, axis=1)
+                return (r - r0 - wob * np.sin(p[:, 0] / 1.5) * np.cos(p[:, 2] / 2.0)) * bt.H
+
+            s.center_distance = dist(s.center_index + 0.5)
+            s.corner_distance = dist(s.corner_index.astype(np.float64))
+            if kind == "halfspace":
+                a = rng.uniform(0.0, np.pi / 2)
+                s.normal, s.coordinate = (np.cos(a), 0.0, np.sin(a)), rng.uniform(4.0, 7.0) * bt.H
+            if kind == "slab":
+                a = rng.uniform(0.0, np.pi / 2)
+                s.normal, s.coordinate = (np.cos(a), 0.0, np.sin(a)), rng.uniform(6.0, 10.0) * bt.H
+        cpu, gpu = bt.freeze(CPU, s), bt.freeze(B200, s)
+        assert cpu[0] == gpu[0], (trial, kind, cpu[0], gpu[0])
+        if cpu[0] == 0:
+            _assert_frozen_equal(cpu, gpu)
+            agreed += 1
+        if kind == "tank" and cpu[0] == 0:
+            code, ci, cv, fi, fs, fv, _ = cpu
+            ps = bt.PistonScene("union")
+            gx, gy, gz = np.meshgrid(s.tank[0] + bt.H * (0.2 + 0.5 * np.arange(4)), bt.H * (0.8 + 0.5 * np.arange(7)),
+                                     bt.H * (0.5 + 0.5 * np.arange(23)), indexing="ij")
+            over = dict(blocks=s.blocks, tank=s.tank, cell_index=ci, cell_values=cv, face_index=fi, face_slot=fs,
+                        face_values=fv, positions=np.stack([gx.ravel(), gy.ravel(), gz.ravel()], 1),
+                        radius=0.65 * bt.H)
+            a, b = bt.wetted_piston(CPU, ps, **over), bt.wetted_piston(B200, ps, **over)
+            assert a[0] == b[0], (trial, a[0], b[0])
+            if a[0] == 0:
+                assert np.array_equal(b[1], a[1]) and np.array_equal(b[2], a[2], equal_nan=True)
+                assert np.array_equal(b[3], a[3]) and b[4] == a[4]
+                pistons += 1
+    assert agreed >= 8 and pistons >= 1
