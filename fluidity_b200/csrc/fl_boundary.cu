@@ -40,6 +40,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <vector>
 
 #include "fl_internal.cuh"
 #include "fl_kernels.h"
@@ -1130,6 +1131,18 @@ struct fl_boundary {
   char* fpin = nullptr;    // and its pinned mirror
   char* pdev = nullptr;    // wetted piston: device arena
   char* ppin = nullptr;    // and its pinned mirror (all but the interval banks)
+  // Host working storage of the freeze and the wetted piston, reserved at
+  // create so that an attempt allocates nothing; results reach the caller's
+  // buffers only on success.
+  std::vector<double> frz_centre;
+  std::vector<uint8_t> frz_needs;
+  std::vector<uint64_t> frz_ordinal;
+  std::vector<fl_frozen_cell> frz_cells;
+  std::vector<fl_frozen_face> frz_faces;
+  std::vector<int32_t> pst_idx;
+  std::vector<fl_piston_patch> pst_patches;
+  std::vector<double> pst_flux;
+  std::vector<uint8_t> pst_has;
 };
 
 namespace {
@@ -1290,6 +1303,19 @@ extern "C" int fl_boundary_create(fl_boundary** out) {
             cudaMallocHost(&b->fpin, freeze_arena_bytes()) == cudaSuccess &&
             cudaMalloc(&b->pdev, piston_arena_bytes()) == cudaSuccess &&
             cudaMallocHost(&b->ppin, piston_pinned_bytes()) == cudaSuccess;
+  try {
+    b->frz_centre.reserve(4096);
+    b->frz_needs.reserve(4096);
+    b->frz_ordinal.reserve(4096);
+    b->frz_cells.reserve(4096);
+    b->frz_faces.reserve(6 * 4096);
+    b->pst_idx.reserve(2 * (size_t)kMaxFaces);
+    b->pst_patches.reserve(kMaxFaces);
+    b->pst_flux.reserve(kMaxFaces);
+    b->pst_has.reserve(kMaxFaces);
+  } catch (...) {
+    ok = false;
+  }
   if (!ok) {
     cudaGetLastError();
     fl_boundary_destroy(b);
@@ -2903,7 +2929,13 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
   // then consume it in order (stage, compute and consume errors of one
   // ordinal come before those of the next).
   CellQuery* cq = fhost<CellQuery>(b, R.cq);
-  std::unique_ptr<double[]> centre(new double[n ? n : 1]);
+  b->frz_centre.assign(n ? n : 1, 0.0);
+  double* centre = b->frz_centre.data();
+  // working records, published to cells_out / faces_out on success
+  b->frz_cells.resize(n ? n : 1);
+  b->frz_faces.resize(6 * (n ? n : 1));
+  fl_frozen_cell* const kept_cells = b->frz_cells.data();
+  fl_frozen_face* const kept_faces = b->frz_faces.data();
   uint64_t staged = 0;
   int stage_error = FL_OK;
   for (; staged < n; ++staged) {
@@ -2953,7 +2985,7 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
     const double volume = std::min(full_volume, unclamped);
     if (!(volume == 0.0 || std::isnormal(volume))) return FL_OUT_OF_RANGE;
     if (dc >= 0 || volume == 0) continue;
-    fl_frozen_cell& c = cells_out[kept++];
+    fl_frozen_cell& c = kept_cells[kept++];
     std::memset(&c, 0, sizeof(c));
     for (int d = 0; d < 3; ++d) c.cell_index[d] = in->cell_indices[3 * i + d];
     c.fluid_volume = volume;
@@ -2968,7 +3000,7 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
         uint64_t slot = 0;
         st = host_face_slot(g, axis, lat64, &slot);
         if (st != FL_OK) return st;
-        fl_frozen_face& f = faces_out[nfaces++];
+        fl_frozen_face& f = kept_faces[nfaces++];
         std::memset(&f, 0, sizeof(f));
         f.axis = axis;
         for (int d = 0; d < 3; ++d) f.lattice[d] = lat[d];
@@ -2977,19 +3009,19 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
   }
   if (stage_error != FL_OK) return stage_error;
   // faces by owned slot, one record per slot
-  std::stable_sort(faces_out, faces_out + nfaces,
+  std::stable_sort(kept_faces, kept_faces + nfaces,
                    [](const fl_frozen_face& x, const fl_frozen_face& y) { return x.face_slot < y.face_slot; });
-  nfaces = (uint64_t)(std::unique(faces_out, faces_out + nfaces,
+  nfaces = (uint64_t)(std::unique(kept_faces, kept_faces + nfaces,
                                   [](const fl_frozen_face& x, const fl_frozen_face& y) {
                                     return x.face_slot == y.face_slot;
                                   }) -
-                      faces_out);
+                      kept_faces);
   if (nfaces > (uint64_t)kMaxFaces) return FL_RESOURCE_EXHAUSTED;
   if (nfaces > 0) {
     FaceQuery* fq = fhost<FaceQuery>(b, R.fq);
     for (uint64_t f = 0; f < nfaces; ++f) {
-      fq[f].axis = faces_out[f].axis;
-      for (int d = 0; d < 3; ++d) fq[f].lattice[d] = faces_out[f].lattice[d];
+      fq[f].axis = kept_faces[f].axis;
+      for (int d = 0; d < 3; ++d) fq[f].lattice[d] = kept_faces[f].lattice[d];
     }
     a.nface = (int)nfaces;
     if (!freeze_phase(
@@ -3003,29 +3035,30 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
     const FaceResult* fr = fhost<FaceResult>(b, R.fr);
     for (uint64_t f = 0; f < nfaces; ++f) {
       if (fr[f].status != FL_OK) return fr[f].status;
-      faces_out[f].open_area = fr[f].open;
-      faces_out[f].blocked_area = fr[f].blocked;
+      kept_faces[f].open_area = fr[f].open;
+      kept_faces[f].blocked_area = fr[f].blocked;
       if (ob.kind == FL_OBSTACLE_OPEN_TANK) {
-        faces_out[f].wall_normal_velocity = fr[f].piston_velocity;
-        faces_out[f].prescribed_wall_flux = fr[f].wall_flux;
-        faces_out[f].has_prescribed_wall_flux = 1;
-        faces_out[f].is_low_x_piston_face = (uint8_t)fr[f].is_piston;
+        kept_faces[f].wall_normal_velocity = fr[f].piston_velocity;
+        kept_faces[f].prescribed_wall_flux = fr[f].wall_flux;
+        kept_faces[f].has_prescribed_wall_flux = 1;
+        kept_faces[f].is_low_x_piston_face = (uint8_t)fr[f].is_piston;
       } else {
-        faces_out[f].wall_normal_velocity =
-            ob.kind == FL_OBSTACLE_NONE ? 0.0 : in->obstacle.wall_velocity[faces_out[f].axis];
+        kept_faces[f].wall_normal_velocity =
+            ob.kind == FL_OBSTACLE_NONE ? 0.0 : in->obstacle.wall_velocity[kept_faces[f].axis];
       }
     }
   }
   // Interface cells (:983-1009): a kept cell with an open face toward an air centre.
-  std::unique_ptr<uint8_t[]> needs(new uint8_t[kept ? kept : 1]());
+  b->frz_needs.assign(kept ? kept : 1, 0);
+  uint8_t* needs = b->frz_needs.data();
   for (uint64_t f = 0; f < nfaces; ++f) {
-    const fl_frozen_face& face = faces_out[f];
+    const fl_frozen_face& face = kept_faces[f];
     if (face.open_area == 0 || in->surface_tension == 0) continue;
     const int32_t head[3] = {face.lattice[0], face.lattice[1], face.lattice[2]};
     int32_t tail[3];
     st = offset_cell(head, face.axis, -1, tail);
     if (st != FL_OK) return st;
-    const long long hc = host_find_cell(cells_out, kept, head), tc = host_find_cell(cells_out, kept, tail);
+    const long long hc = host_find_cell(kept_cells, kept, head), tc = host_find_cell(kept_cells, kept, tail);
     if (hc >= 0 && tc >= 0) continue;
     double air = 0.0;
     st = lookup_distance(in->centers, in->center_count, hc >= 0 ? tail : head, center_key, &air);
@@ -3040,12 +3073,13 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
       if (!std::isnormal(lift)) return FL_OUT_OF_RANGE;
     }
     for (uint64_t i = 0; i < kept; ++i)
-      if (needs[i]) cells_out[i].curvature = in->exact_curvature;
+      if (needs[i]) kept_cells[i].curvature = in->exact_curvature;
   } else if (capillary) {
     // StageCenteredCurvature (:177-215): the 19 centre samples of the
     // derivative stencil, in z, y, x order; staging stops at its first failure.
     CurvatureQuery* kq = fhost<CurvatureQuery>(b, R.kq);
-    std::unique_ptr<uint64_t[]> ordinal(new uint64_t[kept]);
+    b->frz_ordinal.resize(kept);
+    uint64_t* ordinal = b->frz_ordinal.data();
     uint64_t nk = 0;
     int kstage = FL_OK;
     for (uint64_t i = 0; i < kept && kstage == FL_OK; ++i) {
@@ -3056,7 +3090,7 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
         for (int y = -1; y <= 1 && kstage == FL_OK; ++y)
           for (int x = -1; x <= 1 && kstage == FL_OK; ++x) {
             if (x != 0 && y != 0 && z != 0) continue;
-            int32_t idx[3] = {cells_out[i].cell_index[0], cells_out[i].cell_index[1], cells_out[i].cell_index[2]};
+            int32_t idx[3] = {kept_cells[i].cell_index[0], kept_cells[i].cell_index[1], kept_cells[i].cell_index[2]};
             const int off[3] = {x, y, z};
             for (int axis = 0; axis < 3 && kstage == FL_OK; ++axis) kstage = offset_cell(idx, axis, off[axis], idx);
             if (kstage == FL_OK)
@@ -3078,7 +3112,7 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
       const CurvatureResult* kr = fhost<CurvatureResult>(b, R.kr);
       for (uint64_t k = 0; k < nk; ++k) {
         if (kr[k].status != FL_OK) return kr[k].status;
-        cells_out[ordinal[k]].curvature = kr[k].curvature;
+        kept_cells[ordinal[k]].curvature = kr[k].curvature;
       }
     }
     if (kstage != FL_OK) return kstage;
@@ -3098,6 +3132,8 @@ extern "C" int fl_boundary_freeze(fl_boundary* b, const fl_freeze_inputs* in, fl
     bound = cap[0];
     if (in->step_duration > bound) return FL_FAILED_PRECONDITION;
   }
+  if (kept) std::memcpy(cells_out, kept_cells, sizeof(fl_frozen_cell) * kept);
+  if (nfaces) std::memcpy(faces_out, kept_faces, sizeof(fl_frozen_face) * nfaces);
   *cell_count = kept;
   *face_count = nfaces;
   *capillary_step_bound = bound;
@@ -3633,8 +3669,8 @@ extern "C" int fl_boundary_wetted_piston(fl_boundary* b, const fl_owned_grid* gr
   }
   const int32_t px = (int32_t)lo;
   const double velocity = tank[5];
-  std::vector<int32_t> idx;
-  idx.reserve(2 * (size_t)kMaxFaces);
+  std::vector<int32_t>& idx = b->pst_idx;  // reserved for every patch the workspace admits
+  idx.clear();
   for (uint64_t i = 0; i < nc; ++i)
     if (cells[i].cell_index[0] == px) {
       st = add_patch(idx, cells[i].cell_index[1], cells[i].cell_index[2]);
@@ -3714,9 +3750,15 @@ extern "C" int fl_boundary_wetted_piston(fl_boundary* b, const fl_owned_grid* gr
   }
   const size_t npatch = idx.size() / 2;
   if (npatch > patch_capacity) return FL_RESOURCE_EXHAUSTED;
-  for (uint64_t f = 0; f < nf; ++f) has_face_flux[f] = 0, face_fluxes[f] = 0.0;
+  // working outputs, published to the caller's buffers on success
+  b->pst_patches.resize(npatch);
+  b->pst_flux.assign(nf, 0.0);
+  b->pst_has.assign(nf, 0);
+  fl_piston_patch* const work = b->pst_patches.data();
+  double* const fluxes = b->pst_flux.data();
+  uint8_t* const has_flux = b->pst_has.data();
   for (size_t k = 0; k < npatch; ++k) {
-    fl_piston_patch& rec = patches[k];
+    fl_piston_patch& rec = work[k];
     std::memset(&rec, 0, sizeof(rec));
     rec.lattice_y = idx[2 * k];
     rec.lattice_z = idx[2 * k + 1];
@@ -3745,11 +3787,11 @@ extern "C" int fl_boundary_wetted_piston(fl_boundary* b, const fl_owned_grid* gr
       return FL_FAILED_PRECONDITION;
     rec.has_receiver = 1;
     rec.receiver_face_ordinal = a;
-    has_face_flux[a] = 1;
-    face_fluxes[a] = 0.0;
+    has_flux[a] = 1;
+    fluxes[a] = 0.0;
   }
   for (uint64_t f = 0; f < nf; ++f)
-    if (faces[f].has_prescribed_wall_flux && faces[f].prescribed_wall_flux != 0 && !has_face_flux[f])
+    if (faces[f].has_prescribed_wall_flux && faces[f].prescribed_wall_flux != 0 && !has_flux[f])
       return FL_FAILED_PRECONDITION;
   // every patch's wet area on the device
   PatchResult* res = reinterpret_cast<PatchResult*>(b->ppin + R.results);
@@ -3771,8 +3813,8 @@ extern "C" int fl_boundary_wetted_piston(fl_boundary* b, const fl_owned_grid* gr
     if (!wfinite(res[k].area) || res[k].area.lower < 0 || res[k].area.upper > nominal.upper ||
         !std::isfinite(res[k].midpoint_flux))
       return FL_OUT_OF_RANGE;
-    patches[k].area[0] = res[k].area.lower;
-    patches[k].area[1] = res[k].area.upper;
+    work[k].area[0] = res[k].area.lower;
+    work[k].area[1] = res[k].area.upper;
     whole = wadd(whole, res[k].area);
   }
   const WBounds wflux = area_to_flux(whole, velocity);
@@ -3788,18 +3830,18 @@ extern "C" int fl_boundary_wetted_piston(fl_boundary* b, const fl_owned_grid* gr
   for (size_t begin = 0; begin < npatch;) {
     size_t end = begin;
     long long highest = -1;
-    while (end < npatch && patches[end].lattice_z == patches[begin].lattice_z) {
-      if (patches[end].has_receiver) highest = (long long)end;
+    while (end < npatch && work[end].lattice_z == work[begin].lattice_z) {
+      if (work[end].has_receiver) highest = (long long)end;
       ++end;
     }
     for (size_t k = begin; k < end; ++k) {
-      fl_piston_patch& p = patches[k];
+      fl_piston_patch& p = work[k];
       if (p.area[1] == 0) continue;
       fl_piston_patch* recv = &p;
       if (!p.has_receiver) {
-        if (highest < 0 || (int64_t)p.lattice_y - patches[highest].lattice_y != 1 || !res[k].cross_lower)
+        if (highest < 0 || (int64_t)p.lattice_y - work[highest].lattice_y != 1 || !res[k].cross_lower)
           return FL_FAILED_PRECONDITION;
-        recv = &patches[highest];
+        recv = &work[highest];
         p.has_receiver = 1;
         p.receiver_face_ordinal = recv->receiver_face_ordinal;
         ++joined;
@@ -3811,7 +3853,7 @@ extern "C" int fl_boundary_wetted_piston(fl_boundary* b, const fl_owned_grid* gr
       recv->receiver_area[1] = ra.upper;
       recv->receiver_flux[0] = rf.lower;
       recv->receiver_flux[1] = rf.upper;
-      double& acc = face_fluxes[recv->receiver_face_ordinal];
+      double& acc = fluxes[recv->receiver_face_ordinal];
       acc += res[k].midpoint_flux;
       if (!wfinite(ra) || !wfinite(rf) || !std::isfinite(acc)) return FL_OUT_OF_RANGE;
     }
@@ -3819,10 +3861,10 @@ extern "C" int fl_boundary_wetted_piston(fl_boundary* b, const fl_owned_grid* gr
   }
   WBounds assigned_area, assigned_flux;
   for (size_t k = 0; k < npatch; ++k) {
-    const fl_piston_patch& p = patches[k];
+    const fl_piston_patch& p = work[k];
     if (p.receiver_area[1] == 0) continue;
     const WBounds enc{p.receiver_flux[0], p.receiver_flux[1]};
-    const double given = face_fluxes[p.receiver_face_ordinal];
+    const double given = fluxes[p.receiver_face_ordinal];
     if (!wfinite(enc) || given < enc.lower || given > enc.upper) return FL_OUT_OF_RANGE;
     assigned_area = wadd(assigned_area, {p.receiver_area[0], p.receiver_area[1]});
     assigned_flux = wadd(assigned_flux, enc);
@@ -3832,6 +3874,11 @@ extern "C" int fl_boundary_wetted_piston(fl_boundary* b, const fl_owned_grid* gr
   const bool flux_ok =
       wfinite(assigned_flux) && assigned_flux.upper >= wflux.lower && assigned_flux.lower <= wflux.upper;
   if (!area_ok || !flux_ok) return FL_OUT_OF_RANGE;
+  if (npatch) std::memcpy(patches, work, sizeof(fl_piston_patch) * npatch);
+  if (nf) {
+    std::memcpy(face_fluxes, fluxes, sizeof(double) * nf);
+    std::memcpy(has_face_flux, has_flux, nf);
+  }
   *patch_count = npatch;
   whole_area[0] = whole.lower;
   whole_area[1] = whole.upper;

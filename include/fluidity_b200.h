@@ -775,7 +775,8 @@ typedef struct {
 } fl_freeze_inputs;
 /* cells: room for cell_count records, faces: room for 6 * cell_count; both
  * in frozen order (cells by (z,y,x), faces by owned slot). The capillary
- * bound is +inf without a capillary interface. */
+ * bound is +inf without a capillary interface. Outputs are written only on
+ * FL_OK; a call allocates nothing. */
 int fl_boundary_freeze(fl_boundary* boundary, const fl_freeze_inputs* inputs, fl_frozen_cell* cells,
                        uint64_t* cell_count, fl_frozen_face* faces, uint64_t* face_count,
                        double* capillary_step_bound, fl_measurement* measurement);
@@ -810,7 +811,8 @@ typedef struct {
   double receiver_flux[2]; /* m^3/s enclosure of its assigned flux */
 } fl_piston_patch;
 /* patches: room for patch_capacity records (at most 24576 are produced);
- * face_fluxes / has_face_flux: one per frozen face. */
+ * face_fluxes / has_face_flux: one per frozen face. Outputs are written only
+ * on FL_OK; a call allocates nothing. */
 int fl_boundary_wetted_piston(fl_boundary* boundary, const fl_owned_grid* grid, const fl_frozen_cell* cells,
                               uint64_t cell_count, const fl_frozen_face* faces, uint64_t face_count,
                               const fl_piston_field* field, const double* particle_positions,

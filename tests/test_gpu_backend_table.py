@@ -206,10 +206,11 @@ def test_operations_repeat_bitwise_without_growing_device_memory(one_sided, hist
     import torch
 
     box, s, dt = _dam_break_system()
+    fs, ps = bt.FreezeScene("tank"), bt.PistonScene("union")
 
     def attempt():
         return (bt.deposit(B200, one_sided)[1], bt.gather(B200, one_sided, histories["old"], histories["new"])[1],
-                bt.project(B200, s, box.h, dt)[1]["pressure"])
+                bt.project(B200, s, box.h, dt)[1]["pressure"], bt.freeze(B200, fs)[2], bt.wetted_piston(B200, ps)[1])
 
     first = attempt()
     torch.cuda.synchronize()
