@@ -123,6 +123,27 @@ __device__ double cta_sum(double v, double* red) {
   for (int k = 0; k < kMpThreads / 32; ++k) s += red[k];
   return s;
 }
+// Two sums over the CTA in one pair of barriers, each exactly as cta_sum forms it.
+__device__ double2 cta_sum2(double a, double b, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) {
+    red[w] = a;
+    red[kMpThreads / 32 + w] = b;
+  }
+  __syncthreads();
+  double sa = 0.0, sb = 0.0;
+  for (int k = 0; k < kMpThreads / 32; ++k) {
+    sa += red[k];
+    sb += red[kMpThreads / 32 + k];
+  }
+  return make_double2(sa, sb);
+}
 __device__ double cta_max(double v, double* red) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -281,20 +302,28 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
   const double bnorm = sqrt(cta_sum(bb, red));
   // ||b - Ap||_2 <= rel_tol ||b||_2, or the reference's gate 2e-6 + 2e-6 ||b||_2
   const double limit = S.rel_tol > 0.0 ? S.rel_tol * bnorm : 2e-6 + 2e-6 * bnorm;
-  // Jacobi-preconditioned CG; the pinned rows stay at their warm start.
+  // Jacobi-preconditioned CG; the pinned rows stay at their warm start. The
+  // residual norm, the preconditioned residual z = r / diag and r.z of each
+  // iterate are formed in the pass that updates r (every thread visits its
+  // rows in the same order as a separate pass would, so the sums are the same
+  // bits), and both sums share one reduction.
+  __shared__ double red2[2 * (kMpThreads / 32)];
+  double rr = 0.0, rz = 0.0;
+  for (int i = t; i < nc; i += kMpThreads) rr += R[i] * R[i];
+  for (int i = t; i < nc; i += kMpThreads) {
+    const double zi = (S.pinned[i] || DG[i] == 0.0) ? 0.0 : R[i] / DG[i];
+    Z[i] = zi;
+    rz += R[i] * zi;
+  }
+  {
+    const double2 sums = cta_sum2(rr, rz, red2);
+    rr = sums.x;
+    rz = sums.y;
+  }
   double rz_prev = 0.0;
   int it = 0;
   for (; it < S.max_iterations; ++it) {
-    double rr = 0.0;
-    for (int i = t; i < nc; i += kMpThreads) rr += R[i] * R[i];
-    if (sqrt(cta_sum(rr, red)) <= limit) break;
-    double rz = 0.0;
-    for (int i = t; i < nc; i += kMpThreads) {
-      const double zi = (S.pinned[i] || DG[i] == 0.0) ? 0.0 : R[i] / DG[i];
-      Z[i] = zi;
-      rz += R[i] * zi;
-    }
-    rz = cta_sum(rz, red);
+    if (sqrt(rr) <= limit) break;
     const double beta = it == 0 ? 0.0 : rz / rz_prev;
     for (int i = t; i < nc; i += kMpThreads) D[i] = it == 0 ? Z[i] : Z[i] + beta * D[i];
     __syncthreads();
@@ -310,11 +339,20 @@ __global__ void __launch_bounds__(kMpThreads, 1) k_mac_pressure(MpSystem S) {
       break;
     }
     const double alpha = rz / dq;
+    double rr_next = 0.0, rz_next = 0.0;
     for (int i = t; i < nc; i += kMpThreads) {
       P[i] += alpha * D[i];
-      R[i] -= alpha * Q[i];
+      const double ri = R[i] - alpha * Q[i];
+      R[i] = ri;
+      rr_next += ri * ri;
+      const double zi = (S.pinned[i] || DG[i] == 0.0) ? 0.0 : ri / DG[i];
+      Z[i] = zi;
+      rz_next += ri * zi;
     }
+    const double2 sums = cta_sum2(rr_next, rz_next, red2);
     rz_prev = rz;
+    rr = sums.x;
+    rz = sums.y;
   }
   __syncthreads();
   // Evaluation: corrected faces, residuals b - Ap, physical defects and the
