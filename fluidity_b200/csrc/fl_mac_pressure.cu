@@ -160,19 +160,28 @@ __device__ double cta_max(double v, double* red) {
 // Entries are resolved once (other endpoint, conductance), so a row needs no
 // face lookup; the flux is c (x_tail - x_head) as in the face loop, with a
 // missing endpoint at zero.
+// Every cell lists exactly its six incident faces (the host checks the face
+// set), so row i's entries are 6i .. 6i+5: all twelve loads are issued
+// before the sum, which keeps the face order.
 __device__ double apply_row(const MpSystem& S, const double* x, int i) {
   const double xi = x[i];
   double out = S.compliance[i] * xi;
-  for (int e = S.cell_off[i]; e < S.cell_off[i + 1]; ++e) {
-    const double c = S.ent_cond[e];
-    if (c == 0.0) continue;
-    const int o = S.ent_other[e];
-    const int other = o >> 1;  // -1: no cell at the other end
+  double c[6];
+  int o[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    c[k] = S.ent_cond[6 * i + k];
+    o[k] = S.ent_other[6 * i + k];
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    if (c[k] == 0.0) continue;
+    const int other = o[k] >> 1;  // -1: no cell at the other end
     const double xo = other >= 0 ? x[other] : 0.0;
-    if (o & 1)
-      out -= c * (xo - xi);  // this cell is the head
+    if (o[k] & 1)
+      out -= c[k] * (xo - xi);  // this cell is the head
     else
-      out += c * (xi - xo);
+      out += c[k] * (xi - xo);
   }
   return out;
 }
