@@ -10,8 +10,9 @@
 // 462-515), ApplyForces (liquid_substep_3d_cpu.cc:156-178) and the stationary
 // wall condition.
 //
-// B200 design. One CTA per active 8^3 block, one thread per cell. Particles
-// are sorted by cell, so a thread walks its own cell's particles and
+// B200 design. One CTA of 256 threads per active 8^3 block, each thread
+// taking two cells in turn. Particles are sorted by cell, so a thread walks
+// one cell's particles at a time and
 // accumulates into registers: along the normal axis a particle of the cell
 // touches nodes cell-1..cell+1 or cell..cell+2, so 4 x 3 x 3 = 36 slots per
 // channel cover every particle of the cell with static register indexing.
@@ -31,7 +32,15 @@
 
 namespace fl {
 
-constexpr int kP2GThreads = 512;
+// 256 threads per CTA, each thread taking two cells of the block (cells t and
+// t + 256: the same warp shapes and warp tiles as one thread per cell). Two
+// CTAs fit one SM (123 registers), so one CTA's barriers and tile sums overlap
+// the other's particle loop, and with one 30 KB warp-tile set per CTA the SM
+// keeps ~190 KB of L1: a warp's particle loads touch 8 lines per instruction
+// (lanes walk different cells), and those lines are reused by the next ~8
+// particles of each cell only while they stay in L1.
+constexpr int kP2GThreads = 256;
+constexpr int kP2GPasses = kBlockCells / kP2GThreads;
 constexpr int kSlots = 36;
 
 template <int A>
@@ -163,7 +172,7 @@ struct WarpTile {
   static constexpr int size = tx * ty * tz;
 };
 constexpr int kWarpTileMax = 240;  // max over the three components (10 x 6 x 4)
-constexpr int kP2GWarps = kP2GThreads / 32;
+constexpr int kP2GWarps = kBlockCells / 32;  // warp tiles per component
 
 // The warp's partials summed per node, in a fixed order, into its tile:
 // along x within each 8-lane row (a lane keeps node x - 1 and, for x <= ex - 2,
@@ -233,13 +242,30 @@ __device__ __forceinline__ void block_tile(const float2* wtiles, float2* tile, i
   }
 }
 
-__global__ void __launch_bounds__(kP2GThreads, 1)
+template <int A>
+__device__ __forceinline__ void p2g_pass(const GridView& g, const ParticlesView& p, const unsigned int* order,
+                                         const int* cell_start, int b, int t, float2* wt, float2* tile,
+                                         DeviceReport* rep) {
+  const int base = b * kBlockCells;
+#pragma unroll 1
+  for (int pass = 0; pass < kP2GPasses; ++pass) {
+    const int l = t + pass * kP2GThreads;  // the cell: x = l & 7, y = (l >> 3) & 7, z = l >> 6
+    const int cell[3] = {g.coord[3 * b] * 8 + (l & 7), g.coord[3 * b + 1] * 8 + ((l >> 3) & 7),
+                         g.coord[3 * b + 2] * 8 + (l >> 6)};
+    float2 accW[kSlots / 2], accQ[kSlots / 2];
+    p2g_component<A>(g, p, order, cell_start[base + l], cell_start[base + l + 1], cell, accW, accQ, rep);
+    warp_tile<A>(accW, accQ, wt + (l >> 5) * kWarpTileMax, t & 31);
+  }
+  __syncthreads();
+  block_tile<A>(wt, tile + A * kTileFaces, t);
+  if (A < 2) __syncthreads();  // the next component overwrites the warp tiles
+}
+
+__global__ void __launch_bounds__(kP2GThreads, 2)
     k_p2g_tile(GridView g, ParticlesView p, const unsigned int* order, const int* cell_start, float2* tiles,
                DeviceReport* rep) {
-  // One set of warp tiles per component: each warp runs the three components'
-  // particle loops back to back and the CTA meets at a single barrier before
-  // the block tiles are summed, so a warp with few particles does not wait at
-  // every component.
+  // The components in turn through one warp-tile set: particle loops and warp
+  // tiles, a barrier, the block tile summed from the warp tiles, a barrier.
   extern __shared__ float2 wt_smem[];
   const int b = blockIdx.x;
   const int t = threadIdx.x;
@@ -249,29 +275,9 @@ __global__ void __launch_bounds__(kP2GThreads, 1)
     for (int n = t; n < 3 * kTileFaces; n += kP2GThreads) tile[n] = make_float2(0.0f, 0.0f);
     return;
   }
-  const int pbeg = cell_start[base + t], pend = cell_start[base + t + 1];
-  const int cell[3] = {g.coord[3 * b] * 8 + (t & 7), g.coord[3 * b + 1] * 8 + ((t >> 3) & 7),
-                       g.coord[3 * b + 2] * 8 + (t >> 6)};
-  const int wofs = (t >> 5) * kWarpTileMax;
-  {
-    float2 accW[kSlots / 2], accQ[kSlots / 2];
-    p2g_component<0>(g, p, order, pbeg, pend, cell, accW, accQ, rep);
-    warp_tile<0>(accW, accQ, wt_smem + wofs, t & 31);
-  }
-  {
-    float2 accW[kSlots / 2], accQ[kSlots / 2];
-    p2g_component<1>(g, p, order, pbeg, pend, cell, accW, accQ, rep);
-    warp_tile<1>(accW, accQ, wt_smem + kP2GWarps * kWarpTileMax + wofs, t & 31);
-  }
-  {
-    float2 accW[kSlots / 2], accQ[kSlots / 2];
-    p2g_component<2>(g, p, order, pbeg, pend, cell, accW, accQ, rep);
-    warp_tile<2>(accW, accQ, wt_smem + 2 * kP2GWarps * kWarpTileMax + wofs, t & 31);
-  }
-  __syncthreads();
-  block_tile<0>(wt_smem, tile, t);
-  block_tile<1>(wt_smem + kP2GWarps * kWarpTileMax, tile + kTileFaces, t);
-  block_tile<2>(wt_smem + 2 * kP2GWarps * kWarpTileMax, tile + 2 * kTileFaces, t);
+  p2g_pass<0>(g, p, order, cell_start, b, t, wt_smem, tile, rep);
+  p2g_pass<1>(g, p, order, cell_start, b, t, wt_smem, tile, rep);
+  p2g_pass<2>(g, p, order, cell_start, b, t, wt_smem, tile, rep);
 }
 
 __device__ __forceinline__ bool is_solid(const GridView& g, int x, int y, int z) {
@@ -360,10 +366,14 @@ cudaError_t launch_p2g(const GridView& g, const ParticlesView& p, const int* cel
                        const P2GMergeParams& prm, float* const out0[3], float* const out1[3], DeviceReport* rep,
                        cudaStream_t s, const unsigned int* order) {
   if (g.nb == 0) return cudaSuccess;
-  const size_t smem = sizeof(float2) * 3 * kP2GWarps * kWarpTileMax;
+  const size_t smem = sizeof(float2) * kP2GWarps * kWarpTileMax;
   static unsigned long long configured = 0;
-  if (first_on_device(configured))
+  if (first_on_device(configured)) {
     cudaFuncSetAttribute(k_p2g_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // two CTAs per SM: 2 x 30 KB of warp tiles in the 64 KB shared-memory
+    // carveout (28% of 228 KB); the rest of the SM's 256 KB stays L1
+    cudaFuncSetAttribute(k_p2g_tile, cudaFuncAttributePreferredSharedMemoryCarveout, 28);
+  }
   ++g_kernel_launches;
   k_p2g_tile<<<g.nb, kP2GThreads, smem, s>>>(g, p, order, cell_start, tiles, rep);
   ++g_kernel_launches;
